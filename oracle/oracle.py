@@ -1,0 +1,227 @@
+"""ctypes bindings of the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+``Oracle`` wraps oracle/liboracle.so (the C restatement of the reference's algorithm) and ``RefLib``
+wraps oracle/_ref/libkiwi_ref.so (the reference KIWI library built from its own sources by
+oracle/Makefile).  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this
+module; the product package (kiwi_b200) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libkiwi_ref.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class OrStats(C.Structure):
+    _fields_ = [("bbox_pairs", C.c_int64), ("sphere_pairs", C.c_int64), ("skipped_outside", C.c_int64),
+                ("neg_clamped", C.c_int64), ("neg_warned", C.c_int64)]
+
+
+class Oracle:
+    """The C restatement (oracle/kiwi_oracle.c)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
+        L = self.lib = C.CDLL(path)
+        L.or_full_integral_new.restype = C.c_double
+        L.or_full_integral_new.argtypes = [C.c_double] * 4
+        L.or_generic_full_integral.restype = C.c_double
+        L.or_generic_full_integral.argtypes = [C.c_int] + [C.c_double] * 4
+        L.or_gridded_integral.restype = C.c_double
+        L.or_gridded_integral.argtypes = [C.c_double] * 4
+        L.or_face_integral.restype = C.c_double
+        L.or_face_integral.argtypes = [C.c_double] * 3 + [C.c_int, C.c_double, C.c_double, C.c_int, _dp, C.c_int, _ip]
+        L.or_generic_edge_breaks.restype = C.c_int
+        L.or_generic_edge_breaks.argtypes = [C.c_int] + [C.c_double] * 3 + [_dp, C.c_int]
+        L.or_generic_vertex.restype = C.c_double
+        L.or_generic_vertex.argtypes = [C.c_int] + [C.c_double] * 4
+        L.or_sph_to_grid.restype = C.c_int
+        L.or_sph_to_grid.argtypes = ([C.c_int64] + [_dp] * 8 + [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                                                C.c_int, C.c_int64, C.c_int64] + [_dp] * 5 +
+                                     [C.POINTER(OrStats)])
+        L.or_map_voronoi.restype = C.c_int
+        L.or_map_voronoi.argtypes = ([C.c_int64, _i32p] + [_dp] * 8 + [C.c_int64, _i64p, _i64p, _dp, _i32p, _dp,
+                                                                      C.c_int, C.c_double, C.c_int] + [_dp] * 5 +
+                                     [_i64p])
+
+    def full_integral_new(self, h, phi, r0, R0):
+        return self.lib.or_full_integral_new(h, phi, r0, R0)
+
+    def generic_full_integral(self, kernel, H, phi, r0, R0):
+        return self.lib.or_generic_full_integral(kernel, H, phi, r0, R0)
+
+    def gridded_integral(self, h, phi, r0, R0):
+        return self.lib.or_gridded_integral(h, phi, r0, R0)
+
+    def face_integral(self, x0, y0, z0, verts, kernel=-1, h=1.0, support=None, tabulated=False):
+        v = _f64(verts).reshape(-1)
+        ov = C.c_int(0)
+        sup = support if support is not None else 2.0 * h
+        r = self.lib.or_face_integral(x0, y0, z0, kernel, h, sup, int(tabulated), _d(v), len(v) // 3, C.byref(ov))
+        return r, ov.value
+
+    def generic_edge_breaks(self, kernel, H, r0, R0):
+        out = np.zeros(8)
+        n = self.lib.or_generic_edge_breaks(kernel, H, r0, R0, _d(out), 8)
+        return out[:n]
+
+    def generic_vertex(self, kernel, H, r0, R0, phi):
+        return self.lib.or_generic_vertex(kernel, H, r0, R0, phi)
+
+    def sph_to_grid(self, P, bounds, shape, kernel=-1, support_in_h=2.0, tabulated=False, p_range=None):
+        """P: dict of arrays x y z vx vy vz m h.  Returns (density, vx, vy, vz, raw[4], stats)."""
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+        n = len(arrs[0])
+        nx, ny, nz = shape
+        nc = nx * ny * nz
+        outs = [np.zeros(nc) for _ in range(4)]
+        raw = np.zeros(4 * nc)
+        st = OrStats()
+        b = _f64(bounds)
+        pb, pe = (0, n) if p_range is None else p_range
+        rc = self.lib.or_sph_to_grid(n, *[_d(a) for a in arrs], _d(b), nx, ny, nz, kernel, support_in_h,
+                                     int(tabulated), pb, pe, *[_d(o) for o in outs], _d(raw), C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"or_sph_to_grid failed: {rc}")
+        return outs[0], outs[1], outs[2], outs[3], raw.reshape(4, nc), st
+
+    def map_voronoi(self, P, home, geo, kernel=-1, support_in_h=2.0, tabulated=False):
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+        n = len(arrs[0])
+        home = np.ascontiguousarray(home, dtype=np.int32)
+        fo = np.ascontiguousarray(geo["face_off"], dtype=np.int64)
+        vo = np.ascontiguousarray(geo["vert_off"], dtype=np.int64)
+        vx = _f64(geo["vxyz"]).reshape(-1)
+        fn = np.ascontiguousarray(geo["face_nbr"], dtype=np.int32)
+        vol = _f64(geo["volume"])
+        nc = len(vol)
+        outs = [np.zeros(nc) for _ in range(4)]
+        raw = np.zeros(4 * nc)
+        vis = C.c_int64(0)
+        rc = self.lib.or_map_voronoi(n, home.ctypes.data_as(_i32p), *[_d(a) for a in arrs], nc,
+                                     fo.ctypes.data_as(_i64p), vo.ctypes.data_as(_i64p), _d(vx),
+                                     fn.ctypes.data_as(_i32p), _d(vol), kernel, support_in_h, int(tabulated),
+                                     *[_d(o) for o in outs], _d(raw), C.byref(vis))
+        if rc != 0:
+            raise RuntimeError(f"or_map_voronoi failed: {rc}")
+        return outs[0], outs[1], outs[2], outs[3], raw.reshape(4, nc), vis.value
+
+
+KERNEL_NAMES = ["cubic_spline", "quartic_spline", "quintic_spline", "wendland_c2", "wendland_c4", "wendland_c6"]
+
+
+class RefLib:
+    """The reference library compiled from its own sources (oracle/_ref/libkiwi_ref.so)."""
+
+    def __init__(self, path: str = REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle` where the reference is present")
+        L = self.lib = C.CDLL(path)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref_full_integral_new.restype = C.c_double
+        L.ref_full_integral_new.argtypes = [C.c_double] * 4
+        L.ref_generic_full_integral.restype = C.c_double
+        L.ref_generic_full_integral.argtypes = [C.c_int] + [C.c_double] * 4
+        L.ref_gridded_integral.restype = C.c_double
+        L.ref_gridded_integral.argtypes = [C.c_double] * 4
+        L.ref_face_integral.restype = C.c_double
+        L.ref_face_integral.argtypes = [C.c_double] * 3 + [C.c_int, C.c_double, C.c_double, C.c_int, _dp, C.c_int, _ip]
+        L.ref_sph_to_grid.restype = C.c_int
+        L.ref_sph_to_grid.argtypes = ([C.c_long] + [_dp] * 8 + [_dp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_double,
+                                                               C.c_int, C.c_int, C.c_int] + [_dp] * 4)
+        L.ref_voronoi_build.restype = C.c_void_p
+        L.ref_voronoi_build.argtypes = ([C.c_long] + [_dp] * 8 + [_dp, C.c_int, C.c_double, C.c_int, C.c_char_p,
+                                                                 C.c_double, C.c_int, C.c_int, C.c_int])
+        L.ref_voronoi_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_long)]
+        L.ref_voronoi_copy.argtypes = [C.c_void_p, _ip, _dp, _dp, C.POINTER(C.c_long), C.POINTER(C.c_long), _dp, _ip,
+                                       _ip, _dp, _dp, _dp, _dp]
+        L.ref_voronoi_free.argtypes = [C.c_void_p]
+
+    def full_integral_new(self, h, phi, r0, R0):
+        return self.lib.ref_full_integral_new(h, phi, r0, R0)
+
+    def generic_full_integral(self, kernel, H, phi, r0, R0):
+        return self.lib.ref_generic_full_integral(kernel, H, phi, r0, R0)
+
+    def gridded_integral(self, h, phi, r0, R0):
+        return self.lib.ref_gridded_integral(h, phi, r0, R0)
+
+    def face_integral(self, x0, y0, z0, verts, kernel=-1, h=1.0, support=None, tabulated=False):
+        v = _f64(verts).reshape(-1)
+        ov = C.c_int(0)
+        sup = support if support is not None else 2.0 * h
+        r = self.lib.ref_face_integral(x0, y0, z0, kernel, h, sup, int(tabulated), _d(v), len(v) // 3, C.byref(ov))
+        return r, ov.value
+
+    def sph_to_grid(self, P, bounds, shape, kernel="cubic_spline", support_in_h=0.0, generic_path=False,
+                    tabulated=False, threads=0):
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+        n = len(arrs[0])
+        nx, ny, nz = shape
+        nc = nx * ny * nz
+        outs = [np.zeros(nc) for _ in range(4)]
+        b = _f64(bounds)
+        rc = self.lib.ref_sph_to_grid(n, *[_d(a) for a in arrs], _d(b), nx, ny, nz, kernel.encode(), support_in_h,
+                                      int(generic_path), int(tabulated), threads, *[_d(o) for o in outs])
+        if rc != 0:
+            raise RuntimeError("reference sph-to-grid failed: " + self.lib.ref_last_error().decode())
+        return tuple(outs)
+
+    def voronoi(self, P, bounds, buffer=False, spacing_fraction=0.0, lloyd=0, kernel="cubic_spline",
+                support_in_h=0.0, generic_path=False, threads=0, run_map=True):
+        """Cell geometry (CSR, as src/mapping.cpp builds it), home cells and, if run_map, the reference's
+        own mapping.dat values per cell."""
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+        n = len(arrs[0])
+        b = _f64(bounds)
+        hnd = self.lib.ref_voronoi_build(n, *[_d(a) for a in arrs], _d(b), int(buffer), spacing_fraction, lloyd,
+                                         kernel.encode(), support_in_h, int(generic_path), threads, int(run_map))
+        if not hnd:
+            raise RuntimeError("reference voronoi failed: " + self.lib.ref_last_error().decode())
+        sz = (C.c_long * 4)()
+        self.lib.ref_voronoi_sizes(hnd, sz)
+        nc, nf, nv, npart = sz[0], sz[1], sz[2], sz[3]
+        g = {
+            "id": np.zeros(nc, np.int32), "site": np.zeros(3 * nc), "volume": np.zeros(nc),
+            "face_off": np.zeros(nc + 1, np.int64), "vert_off": np.zeros(nf + 1, np.int64),
+            "vxyz": np.zeros(3 * nv), "face_nbr": np.zeros(nf, np.int32), "home": np.zeros(npart, np.int32),
+        }
+        res = [np.zeros(nc) for _ in range(4)]
+        lp = C.POINTER(C.c_long)
+        self.lib.ref_voronoi_copy(hnd, g["id"].ctypes.data_as(_ip), _d(g["site"]), _d(g["volume"]),
+                                  g["face_off"].ctypes.data_as(lp), g["vert_off"].ctypes.data_as(lp), _d(g["vxyz"]),
+                                  g["face_nbr"].ctypes.data_as(_ip), g["home"].ctypes.data_as(_ip),
+                                  *[_d(r) for r in res])
+        self.lib.ref_voronoi_free(hnd)
+        return g, (res if run_map else None)
+
+
+def load_oracle():
+    return Oracle()
+
+
+def load_ref():
+    """The reference library, or None when it was not built on this machine."""
+    try:
+        return RefLib()
+    except (FileNotFoundError, OSError):
+        return None

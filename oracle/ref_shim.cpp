@@ -1,0 +1,296 @@
+// C-ABI shim over the reference KIWI library, built from the reference's own sources by
+// oracle/Makefile into oracle/_ref/libkiwi_ref.so -- TEST INFRASTRUCTURE ONLY.
+//
+// It lets the tests and bench.py's CPU-baseline leg call the unmodified reference code:
+//  - the scalar integral API (include/kiwi/kernel_integral.hpp:72-193,
+//    include/kiwi/kernel_integral_generic.hpp:47-56);
+//  - run_sph_to_grid_stage (src/cartesian_grid.cpp:76) on arrays, through a temporary plain_ascii
+//    snapshot (written with 17 significant digits, so it reads back bit-exact) and a Config built in code;
+//  - the Voronoi cell geometry exactly as src/mapping.cpp:222-269 extracts it from Voro++, and
+//    run_mapping_stage (src/mapping.cpp:331) on arrays.
+#include <omp.h>
+#include <unistd.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kiwi/cartesian_grid.hpp"
+#include "kiwi/config.hpp"
+#include "kiwi/kernel_integral.hpp"
+#include "kiwi/kernel_integral_generic.hpp"
+#include "kiwi/kernel_spec.hpp"
+#include "kiwi/mapping.hpp"
+#include "kiwi/point_set.hpp"
+#include "kiwi/voro_grid.hpp"
+#include "voro++.hh"
+
+namespace {
+
+const kiwi::KernelSpec& kernel_by_index(int k) { return *kiwi::all_kernels().at(k); }
+
+std::string g_err;
+
+std::string make_tmpdir() {
+    char tmpl[] = "/tmp/kiwi_ref_XXXXXX";
+    char* d = mkdtemp(tmpl);
+    return d ? std::string(d) : std::string("/tmp");
+}
+
+void rm_rf(const std::string& dir) {
+    std::string cmd = "rm -rf '" + dir + "'";
+    int rc = std::system(cmd.c_str());
+    (void)rc;
+}
+
+void write_snapshot(const std::string& path, long n, const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz, const double* m, const double* h) {
+    FILE* f = std::fopen(path.c_str(), "w");
+    for (long i = 0; i < n; ++i)
+        std::fprintf(f, "%.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g 1\n", x[i], y[i], z[i], vx[i], vy[i],
+                     vz[i], m[i], h[i]);
+    std::fclose(f);
+}
+
+kiwi::Config base_config(const std::string& dir, const double b[6], const char* kernel, double support_in_h,
+                         int generic_path) {
+    kiwi::Config c;
+    c.run_name = "ref";
+    c.domain.x_min = b[0]; c.domain.x_max = b[1];
+    c.domain.y_min = b[2]; c.domain.y_max = b[3];
+    c.domain.z_min = b[4]; c.domain.z_max = b[5];
+    c.input_snapshot = dir + "/snap.txt";
+    c.input_snapshot_format = "plain_ascii";
+    c.work_folder = dir + "/runs";
+    c.kernel.name = kernel ? kernel : "cubic_spline";
+    c.kernel.support_radius_in_h = support_in_h;
+    c.kernel.generic_path = generic_path != 0;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_err.c_str(); }
+
+double ref_full_integral_new(double h, double phi, double r0, double R_0) {
+    return kiwi::full_integral_new(h, phi, r0, R_0);
+}
+
+double ref_generic_full_integral(int kernel, double H, double phi, double r0, double R_0) {
+    return kiwi::generic_full_integral(kernel_by_index(kernel), H, phi, r0, R_0);
+}
+
+double ref_gridded_integral(double h, double phi, double r0, double R_0) {
+    static kiwi::DensityLookupTable table = kiwi::generate_density_table();
+    return kiwi::gridded_integral(table, h, phi, r0, R_0);
+}
+
+// kernel < 0: compute_face_integral (support 2h); else compute_face_integral_generic with H = support.
+double ref_face_integral(double x0, double y0, double z0, int kernel, double h, double support, int tabulated,
+                         const double* verts, int n, int* out_vert) {
+    std::vector<double> v(verts, verts + 3 * n);
+    if (kernel < 0) {
+        static kiwi::DensityLookupTable table;
+        static bool have = false;
+        if (tabulated && !have) {
+            table = kiwi::generate_density_table();
+            have = true;
+        }
+        return kiwi::compute_face_integral(x0, y0, z0, h, tabulated != 0, &table, v, out_vert);
+    }
+    return kiwi::compute_face_integral_generic(x0, y0, z0, kernel_by_index(kernel), support, v, out_vert);
+}
+
+// run_sph_to_grid_stage on arrays. kernel: a kernel name accepted by get_kernel ("cubic_spline", ...).
+int ref_sph_to_grid(long n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
+                    const double* vz, const double* m, const double* h, const double bounds[6], int nx, int ny,
+                    int nz, const char* kernel, double support_in_h, int generic_path, int tabulated, int threads,
+                    double* density, double* gvx, double* gvy, double* gvz) {
+    std::string dir = make_tmpdir();
+    try {
+        write_snapshot(dir + "/snap.txt", n, x, y, z, vx, vy, vz, m, h);
+        kiwi::Config c = base_config(dir, bounds, kernel, support_in_h, generic_path);
+        c.cartesian_grid.resolution_x = nx;
+        c.cartesian_grid.resolution_y = ny;
+        c.cartesian_grid.resolution_z = nz;
+        c.cartesian_grid.use_tabulated_integral = tabulated != 0;
+        if (threads > 0) omp_set_num_threads(threads);
+        kiwi::CartesianGridResult g = kiwi::run_sph_to_grid_stage(c);
+        const size_t nc = static_cast<size_t>(nx) * ny * nz;
+        std::memcpy(density, g.density.data(), nc * sizeof(double));
+        std::memcpy(gvx, g.vx.data(), nc * sizeof(double));
+        std::memcpy(gvy, g.vy.data(), nc * sizeof(double));
+        std::memcpy(gvz, g.vz.data(), nc * sizeof(double));
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        rm_rf(dir);
+        return -1;
+    }
+    rm_rf(dir);
+    return 0;
+}
+
+// ---- Voronoi --------------------------------------------------------------------------------------
+
+struct RefVoronoi {
+    std::vector<int> id;
+    std::vector<double> site;               // 3 per cell
+    std::vector<double> volume;
+    std::vector<long> face_off, vert_off;   // CSR
+    std::vector<double> vxyz;               // absolute vertex coordinates
+    std::vector<int> face_nbr;              // resolved cell index or -1
+    std::vector<int> home;                  // per particle: cell index or -1
+    std::vector<double> density, vx, vy, vz;
+};
+
+// Builds the cell geometry the way src/mapping.cpp:222-269 does (same container and block setup), in
+// CSR form with vertices made absolute as src/mapping.cpp:168-175 does, plus each particle's home cell
+// as src/mapping.cpp:434-439 finds it.  Points: the final point set (after buffer/Lloyd) -- taken from
+// run_point_set_stage on the same snapshot, as run_mapping_stage does.  Then runs run_mapping_stage
+// itself and keeps its per-cell rows (matched by site id to the geometry order).
+void* ref_voronoi_build(long n, const double* x, const double* y, const double* z, const double* vx,
+                        const double* vy, const double* vz, const double* m, const double* h,
+                        const double bounds[6], int buffer_enabled, double spacing_fraction, int lloyd_iterations,
+                        const char* kernel, double support_in_h, int generic_path, int threads, int run_map) {
+    std::string dir = make_tmpdir();
+    auto* R = new RefVoronoi();
+    try {
+        write_snapshot(dir + "/snap.txt", n, x, y, z, vx, vy, vz, m, h);
+        kiwi::Config c = base_config(dir, bounds, kernel, support_in_h, generic_path);
+        c.buffer.enabled = buffer_enabled != 0;
+        c.buffer.strategy = "coverage_grid";
+        if (spacing_fraction > 0) c.buffer.coverage_grid.spacing_fraction = spacing_fraction;
+        c.lloyd.iterations = lloyd_iterations;
+        if (threads > 0) omp_set_num_threads(threads);
+        kiwi::PointSet pts = kiwi::run_point_set_stage(c);
+
+        const kiwi::Domain& d = c.domain;
+        voro::pre_container pcon(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, false, false, false);
+        for (size_t i = 0; i < pts.size(); ++i) pcon.put(pts.id[i], pts.x[i], pts.y[i], pts.z[i]);
+        int bx, by, bz;
+        kiwi::guess_scaled_blocks(pcon, c.grid_blocks.block_scale_factor, bx, by, bz);
+        voro::container con(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, bx, by, bz, false, false, false, 8);
+        pcon.setup(con);
+        int max_id = 0;
+        for (int pid : pts.id) max_id = std::max(max_id, pid);
+        std::vector<int> reverse(max_id + 1, -1);
+        std::vector<std::vector<int>> fvert_all, nlist_all;
+        std::vector<std::vector<double>> fcoord_all;
+        voro::voronoicell_neighbor cell;
+        voro::c_loop_all clo(con);
+        double px, py, pz;
+        if (clo.start()) do {
+            if (con.compute_cell(cell, clo)) {
+                int idx = static_cast<int>(R->id.size());
+                R->id.push_back(clo.pid());
+                reverse[clo.pid()] = idx;
+                clo.pos(px, py, pz);
+                R->site.push_back(px);
+                R->site.push_back(py);
+                R->site.push_back(pz);
+                std::vector<int> fv, nl;
+                std::vector<double> fc;
+                cell.face_vertices(fv);
+                cell.vertices(fc);
+                cell.neighbors(nl);
+                R->volume.push_back(cell.volume());
+                fvert_all.push_back(std::move(fv));
+                fcoord_all.push_back(std::move(fc));
+                nlist_all.push_back(std::move(nl));
+            }
+        } while (clo.inc());
+        R->face_off.push_back(0);
+        R->vert_off.push_back(0);
+        for (size_t ci = 0; ci < R->id.size(); ++ci) {
+            const std::vector<int>& fv = fvert_all[ci];
+            const std::vector<double>& fc = fcoord_all[ci];
+            const std::vector<int>& nl = nlist_all[ci];
+            const double sx = R->site[3 * ci], sy = R->site[3 * ci + 1], sz = R->site[3 * ci + 2];
+            size_t it = 0;
+            int fi = 0;
+            while (it < fv.size()) {
+                int cnt = fv[it];
+                for (int k = 0; k < cnt; ++k) {
+                    int ci2 = fv[it + 1 + k];
+                    R->vxyz.push_back(fc[3 * ci2] + sx);
+                    R->vxyz.push_back(fc[3 * ci2 + 1] + sy);
+                    R->vxyz.push_back(fc[3 * ci2 + 2] + sz);
+                }
+                R->vert_off.push_back(R->vert_off.back() + cnt);
+                int nb = nl[fi];
+                R->face_nbr.push_back(nb >= 0 && nb <= max_id ? reverse[nb] : -1);
+                it += cnt + 1;
+                ++fi;
+            }
+            R->face_off.push_back(R->face_off.back() + fi);
+        }
+        for (long i = 0; i < n; ++i) {
+            double fx, fy, fz;
+            int sid;
+            bool found = con.find_voronoi_cell(x[i], y[i], z[i], fx, fy, fz, sid);
+            R->home.push_back((found && sid >= 0 && sid <= max_id) ? reverse[sid] : -1);
+        }
+        if (run_map) {
+            kiwi::MappingResult mr = kiwi::run_mapping_stage(c);
+            const size_t nc = R->id.size();
+            R->density.assign(nc, 0.0);
+            R->vx.assign(nc, 0.0);
+            R->vy.assign(nc, 0.0);
+            R->vz.assign(nc, 0.0);
+            for (const auto& row : mr.cells) {
+                if (row.id < 0 || row.id > max_id || reverse[row.id] < 0) continue;
+                int ci = reverse[row.id];
+                R->density[ci] = row.density;
+                R->vx[ci] = row.vx;
+                R->vy[ci] = row.vy;
+                R->vz[ci] = row.vz;
+            }
+        }
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        rm_rf(dir);
+        delete R;
+        return nullptr;
+    }
+    rm_rf(dir);
+    return R;
+}
+
+// Sizes: [n_cells, n_faces, n_vertices, n_particles]
+void ref_voronoi_sizes(void* h, long* out4) {
+    auto* R = static_cast<RefVoronoi*>(h);
+    out4[0] = static_cast<long>(R->id.size());
+    out4[1] = static_cast<long>(R->face_nbr.size());
+    out4[2] = static_cast<long>(R->vxyz.size() / 3);
+    out4[3] = static_cast<long>(R->home.size());
+}
+
+void ref_voronoi_copy(void* h, int* id, double* site, double* volume, long* face_off, long* vert_off, double* vxyz,
+                      int* face_nbr, int* home, double* density, double* vx, double* vy, double* vz) {
+    auto* R = static_cast<RefVoronoi*>(h);
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(id, R->id);
+    cp(site, R->site);
+    cp(volume, R->volume);
+    cp(face_off, R->face_off);
+    cp(vert_off, R->vert_off);
+    cp(vxyz, R->vxyz);
+    cp(face_nbr, R->face_nbr);
+    cp(home, R->home);
+    cp(density, R->density);
+    cp(vx, R->vx);
+    cp(vy, R->vy);
+    cp(vz, R->vz);
+}
+
+void ref_voronoi_free(void* h) { delete static_cast<RefVoronoi*>(h); }
+
+}  // extern "C"
