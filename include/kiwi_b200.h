@@ -1,0 +1,141 @@
+/* kiwi_b200: C ABI of the B200-native KIWI kernel-integral engine (libkiwi_b200.so).
+ *
+ * Every entry point below replaces a piece of the reference's C++ kernel-integral layer or one of its
+ * two mapping stages; the comment on each names the reference interface (path within mapetkova/kiwi,
+ * file:line).  Conventions:
+ *   - plain pointers and sizes only; all arrays are caller-owned;
+ *   - return value 0 (KIWI_OK) or a negative KIWI_ERR_* code; kiwi_last_error() explains it.  This is
+ *     the C form of the reference's exceptions (std::runtime_error / ConfigError, turned into one
+ *     "[kiwi] error: <what>" line by src/main.cpp:241-244);
+ *   - one context per host thread; every call is synchronous with respect to the host unless its name
+ *     ends in _device, in which case it is stream-ordered on the context's stream;
+ *   - results are deterministic: each cell's sum is taken over its particles in ascending particle
+ *     order, with no floating-point atomics, so repeated calls are bitwise identical;
+ *   - there is no CPU fallback: without a usable sm_100 GPU every call fails with KIWI_ERR_NODEV.
+ */
+#ifndef KIWI_B200_H
+#define KIWI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KIWI_OK 0
+#define KIWI_ERR_ARG (-1)         /* invalid argument (the reference's ConfigError / runtime_error) */
+#define KIWI_ERR_CUDA (-2)        /* a CUDA call failed */
+#define KIWI_ERR_NODEV (-3)       /* no usable GPU */
+#define KIWI_ERR_ALLOC (-4)       /* device memory allocation failed */
+#define KIWI_ERR_LIMIT (-5)       /* a bounded device loop hit its iteration cap */
+#define KIWI_ERR_UNSUPPORTED (-6) /* option not available in this build */
+
+/* Arithmetic forms of the cell integrals. */
+#define KIWI_FP64 0       /* all-FP64, the reference's arithmetic operation by operation */
+#define KIWI_FP32_MIXED 1 /* FP32 bulk with FP64 islands and FP64 per-cell totals */
+
+typedef struct KiwiCtx KiwiCtx;
+
+/* Particle snapshot, SoA (the SPHSnapshot fields the hot path reads, include/kiwi/snapshot.hpp:70-77). */
+typedef struct KiwiParticles {
+    int64_t n;
+    const double *x, *y, *z;    /* positions */
+    const double *vx, *vy, *vz; /* velocities */
+    const double *m, *h;        /* mass, smoothing length (h <= 0: no contribution, as the reference) */
+} KiwiParticles;
+
+/* Uniform Cartesian grid (Domain + CartesianGridConfig resolved nx/ny/nz, include/kiwi/config.hpp:24-30,
+ * 209-216; src/cartesian_grid.cpp:89-97).  Cell (ix,iy,iz) is stored at (ix*ny + iy)*nz + iz. */
+typedef struct KiwiCartGrid {
+    double bounds[6]; /* x_min, x_max, y_min, y_max, z_min, z_max */
+    int32_t nx, ny, nz;
+} KiwiCartGrid;
+
+/* Kernel selection (KernelConfig + the dispatch of make_kernel_integrator,
+ * include/kiwi/kernel_integrator.hpp:14-45 and src/config.cpp:267-277): the cubic closed form is used iff
+ * kernel == M4, the support is 2h and generic_path == 0; otherwise the generic table-driven integral. */
+typedef struct KiwiKernelSel {
+    int32_t kernel;       /* kiwi_kernel_index(): 0 M4, 1 M5, 2 M6, 3 WC2, 4 WC4, 5 WC6 */
+    double support_in_h;  /* kernel support radius in units of h; 0 = the kernel's default radkern */
+    int32_t generic_path; /* force the generic integral for M4 */
+    int32_t tabulated;    /* cubic path only: trilinear lookup table instead of the closed form */
+} KiwiKernelSel;
+
+typedef struct KiwiStats {
+    int64_t bbox_pairs;      /* (particle, cell) pairs in the clamped support bounding boxes */
+    int64_t sphere_pairs;    /* of those, cells whose closest point lies within the support radius */
+    int64_t evaluated_pairs; /* pairs whose integral was evaluated */
+    int64_t skipped_outside; /* particles whose support misses the grid (src/cartesian_grid.cpp:234-237) */
+    int64_t neg_clamped;     /* pair integrals < 0 clamped to 0 (src/cartesian_grid.cpp:264-269) */
+    int64_t neg_warned;      /* of those, <= -0.01 (the reference prints a warning for each) */
+    int64_t fp64_fallback;   /* FP32-mixed form: edges evaluated in FP64 */
+    int64_t tile_pairs;      /* (tile, particle) list entries built by the binning step */
+    double gather_ms;        /* device time of the cell-integral kernel(s) of this call (CUDA events) */
+    double total_ms;         /* device time of the whole call, copies included for the host variants */
+} KiwiStats;
+
+/* ---- context --------------------------------------------------------------------------------- */
+int kiwi_ctx_create(int device, KiwiCtx** out);
+void kiwi_ctx_destroy(KiwiCtx* ctx);
+const char* kiwi_last_error(const KiwiCtx* ctx); /* message of the last failed call on ctx */
+void* kiwi_ctx_stream(KiwiCtx* ctx);             /* the context's cudaStream_t */
+int kiwi_ctx_synchronize(KiwiCtx* ctx);
+const char* kiwi_version(void);
+
+/* ---- kernel tables (include/kiwi/kernel_spec.hpp:18-44, src/kernel_spec_data.cpp:175-187) ----- */
+/* get_kernel(name): index 0..5 for a key or alias ("M4", "cubic_spline", "wendland_c4", ...), -1 if
+ * unknown (the reference throws std::invalid_argument). */
+int kiwi_kernel_index(const char* name);
+/* Kernel constants: out7 = {nreg, A2_pi, A3_pi, radkern, hfact, c[0], c[1]}. */
+int kiwi_kernel_info(int kernel, double* out7);
+
+/* ---- scalar integral layer, batched on the GPU ----------------------------------------------- */
+/* full_integral_new(h, phi, r0, R_0) (include/kiwi/kernel_integral.hpp:80) when kernel < 0, with arg0 = h;
+ * generic_full_integral(K, H, phi, r0, R_0) (include/kiwi/kernel_integral_generic.hpp:56) when
+ * kernel >= 0, with arg0 = H.  Host arrays of length n. */
+int kiwi_full_integral_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi,
+                             const double* r0, const double* R_0, double* out);
+
+/* compute_face_integral / compute_face_integral_generic (include/kiwi/kernel_integral.hpp:182-193) for
+ * n_faces independent (particle, face) items.  particle: 4 doubles per item (x0, y0, z0, h); face i has
+ * vertices vert_off[i]..vert_off[i+1]-1 of verts (xyz each, absolute, in the face's winding).  out_vert
+ * (may be NULL) receives the reference's out_vert per item. */
+int kiwi_face_integral_batch(KiwiCtx* ctx, const KiwiKernelSel* kernel, int64_t n_faces, const double* particle,
+                             const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert);
+
+/* ---- sph-to-grid stage (run_sph_to_grid_stage, src/cartesian_grid.cpp:76-321) ---------------- */
+/* Host arrays in, host arrays out (density, vx, vy, vz as CartesianGridResult holds them,
+ * include/kiwi/cartesian_grid.hpp:53-71).  raw4 (may be NULL): the unnormalised sums
+ * sum m*Msum, sum m*Msum*v{x,y,z} (4 * ncells doubles). */
+int kiwi_sph_to_grid(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                     const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy,
+                     double* vz, double* raw4, KiwiStats* stats);
+
+/* Same with every pointer (particles and outputs) in device memory, on the context's stream. */
+int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                            const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy,
+                            double* vz, double* raw4, KiwiStats* stats);
+
+/* ---- Voronoi map stage (run_mapping_stage's particle loop, src/mapping.cpp:105-206, 400-502) --- */
+/* Cell geometry in CSR form: the plain data of CellFaceGeometry (src/mapping.cpp:49-54) with vertex
+ * coordinates made absolute as src/mapping.cpp:168-175 does and neighbour ids resolved to cell indices. */
+typedef struct KiwiVoronoiCells {
+    int64_t n_cells;
+    const int64_t* face_off; /* n_cells + 1 */
+    const int64_t* vert_off; /* n_faces + 1 */
+    const double* vxyz;      /* 3 per vertex */
+    const int32_t* face_nbr; /* neighbour cell index, or -1 for a wall / unresolved neighbour */
+    const double* volume;    /* n_cells */
+} KiwiVoronoiCells;
+
+/* home_cell: per particle the cell containing it (container::find_voronoi_cell resolved through
+ * reverse_id_list, src/mapping.cpp:434-439), or -1 (skipped, "unresolved").  Outputs per cell in the
+ * geometry's order: density = M/volume (0 if volume <= 0), velocity = P/M or the mean velocity. */
+int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                     const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
+                     double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

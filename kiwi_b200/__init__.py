@@ -1,0 +1,365 @@
+"""kiwi_b200: B200-native KIWI kernel-integral engine -- Python host binding over the C ABI.
+
+The names mirror the reference's C++ kernel-integral layer and stages (mapetkova/kiwi):
+
+  get_kernel(name)                                      include/kiwi/kernel_spec.hpp:41-44
+  full_integral_new(h, phi, r0, R_0)                    include/kiwi/kernel_integral.hpp:80
+  generic_full_integral(K, H, phi, r0, R_0)             include/kiwi/kernel_integral_generic.hpp:56
+  compute_face_integral(x0, y0, z0, h, verts)           include/kiwi/kernel_integral.hpp:182-184
+  compute_face_integral_generic(x0, y0, z0, K, H, v)    include/kiwi/kernel_integral.hpp:192-193
+  KernelIntegrator / make_kernel_integrator             include/kiwi/kernel_integrator.hpp:14-45
+  sph_to_grid(...) -> CartesianGridResult               src/cartesian_grid.cpp:76-321 (the stage's compute)
+
+Every call runs on the GPU through libkiwi_b200.so (hand-written sm_100a kernels).  There is no CPU
+fallback: if the library or a usable GPU is missing, calls raise KiwiError.  Scalar functions accept
+NumPy arrays and evaluate them as one batched launch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkiwi_b200.so")
+
+KIWI_FP64 = 0
+KIWI_FP32_MIXED = 1
+PRECISIONS = {"fp64": KIWI_FP64, "fp32_mixed": KIWI_FP32_MIXED}
+
+KERNEL_KEYS = ["M4", "M5", "M6", "WC2", "WC4", "WC6"]
+KERNEL_NAMES = ["cubic_spline", "quartic_spline", "quintic_spline", "wendland_c2", "wendland_c4", "wendland_c6"]
+
+_ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "no usable GPU", -4: "device allocation failed",
+           -5: "iteration limit hit", -6: "unsupported option"}
+
+
+class KiwiError(RuntimeError):
+    """Raised for any failed call: the Python form of the reference's `[kiwi] error: <what>`."""
+
+    def __init__(self, code: int, what: str):
+        super().__init__(f"[kiwi] error: {what}")
+        self.code = code
+
+
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+
+class KiwiParticles(C.Structure):
+    _fields_ = [("n", C.c_int64)] + [(k, _dp) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+
+
+class KiwiCartGrid(C.Structure):
+    _fields_ = [("bounds", C.c_double * 6), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32)]
+
+
+class KiwiKernelSel(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("support_in_h", C.c_double), ("generic_path", C.c_int32),
+                ("tabulated", C.c_int32)]
+
+
+class KiwiStats(C.Structure):
+    _fields_ = [("bbox_pairs", C.c_int64), ("sphere_pairs", C.c_int64), ("evaluated_pairs", C.c_int64),
+                ("skipped_outside", C.c_int64), ("neg_clamped", C.c_int64), ("neg_warned", C.c_int64),
+                ("fp64_fallback", C.c_int64), ("tile_pairs", C.c_int64), ("gather_ms", C.c_double),
+                ("total_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KiwiVoronoiCells(C.Structure):
+    _fields_ = [("n_cells", C.c_int64), ("face_off", _i64p), ("vert_off", _i64p), ("vxyz", _dp),
+                ("face_nbr", _i32p), ("volume", _dp)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads libkiwi_b200.so (built in-tree by kiwi_b200.build); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise KiwiError(-6, f"{path} is missing: build it with `python -m kiwi_b200.build`")
+    L = C.CDLL(path)
+    L.kiwi_version.restype = C.c_char_p
+    L.kiwi_ctx_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+    L.kiwi_ctx_destroy.argtypes = [C.c_void_p]
+    L.kiwi_last_error.restype = C.c_char_p
+    L.kiwi_last_error.argtypes = [C.c_void_p]
+    L.kiwi_ctx_stream.restype = C.c_void_p
+    L.kiwi_ctx_stream.argtypes = [C.c_void_p]
+    L.kiwi_ctx_synchronize.argtypes = [C.c_void_p]
+    L.kiwi_kernel_index.argtypes = [C.c_char_p]
+    L.kiwi_kernel_info.argtypes = [C.c_int, _dp]
+    L.kiwi_full_integral_batch.argtypes = [C.c_void_p, C.c_int, C.c_int64, _dp, _dp, _dp, _dp, _dp]
+    L.kiwi_face_integral_batch.argtypes = [C.c_void_p, C.POINTER(KiwiKernelSel), C.c_int64, _dp, _i64p, _dp, _dp,
+                                           _i32p]
+    sig = [C.c_void_p, C.POINTER(KiwiParticles), C.POINTER(KiwiCartGrid), C.POINTER(KiwiKernelSel), C.c_int,
+           _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
+    L.kiwi_sph_to_grid.argtypes = sig
+    L.kiwi_sph_to_grid_device.argtypes = sig
+    L.kiwi_map_voronoi.argtypes = [C.c_void_p, C.POINTER(KiwiParticles), _i32p, C.POINTER(KiwiVoronoiCells),
+                                   C.POINTER(KiwiKernelSel), C.c_int, _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
+    _lib = L
+    return L
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+class KernelSpec:
+    """A kernel of the table (the KernelSpec of include/kiwi/kernel_spec.hpp:18-44)."""
+
+    def __init__(self, index: int):
+        out = (C.c_double * 7)()
+        rc = load_library().kiwi_kernel_info(index, out)
+        if rc != 0:
+            raise KiwiError(rc, f"unknown kernel index {index}")
+        self.index = index
+        self.key = KERNEL_KEYS[index]
+        self.name = KERNEL_NAMES[index]
+        self.nreg = int(out[0])
+        self.A2_pi, self.A3_pi, self.radkern, self.hfact = out[1], out[2], out[3], out[4]
+
+    def __repr__(self):
+        return f"KernelSpec({self.key})"
+
+
+def get_kernel(name: str) -> KernelSpec:
+    """Kernel by key or alias, case-insensitive; unknown names raise (std::invalid_argument)."""
+    k = load_library().kiwi_kernel_index(str(name).encode())
+    if k < 0:
+        raise KiwiError(-1, f"kernel.name: unknown kernel '{name}' (expected one of: cubic_spline, quartic_spline, "
+                            "quintic_spline, wendland_c2, wendland_c4, wendland_c6)")
+    return KernelSpec(k)
+
+
+class Context:
+    """One GPU context (stream, scratch memory).  One per host thread."""
+
+    def __init__(self, device: int = 0):
+        L = load_library()
+        h = C.c_void_p()
+        rc = L.kiwi_ctx_create(int(device), C.byref(h))
+        if rc != 0:
+            raise KiwiError(rc, f"kiwi_ctx_create(device={device}) failed: {_ERRORS.get(rc, rc)}")
+        self._h = h
+        self._L = L
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self) -> int:
+        return self._L.kiwi_ctx_stream(self._h)
+
+    def check(self, rc: int, what: str = ""):
+        if rc != 0:
+            msg = self._L.kiwi_last_error(self._h).decode()
+            raise KiwiError(rc, (what + ": " if what else "") + (msg or _ERRORS.get(rc, str(rc))))
+
+    def synchronize(self):
+        self.check(self._L.kiwi_ctx_synchronize(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.kiwi_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(int(os.environ.get("KIWI_DEVICE", "0")))
+    return _default_ctx
+
+
+# ---------------------------------------------------------------------------------------------- scalar API
+
+def _batch(fn_kernel: int, arg0, phi, r0, R0, ctx=None):
+    ctx = ctx or default_context()
+    a0, ph, a, b = np.broadcast_arrays(_f64(arg0), _f64(phi), _f64(r0), _f64(R0))
+    shape = a0.shape
+    a0, ph, a, b = (_f64(x).reshape(-1) for x in (a0, ph, a, b))
+    out = np.empty(a0.size)
+    ctx.check(ctx._L.kiwi_full_integral_batch(ctx.handle, fn_kernel, a0.size, _p(a0), _p(ph), _p(a), _p(b), _p(out)),
+              "full_integral")
+    return out.reshape(shape) if shape else float(out[0])
+
+
+def full_integral_new(h, phi, r0, R_0, ctx=None):
+    """Closed-form cubic-spline vertex-pyramid integral (src/kernel_integral.cpp:410-418), batched."""
+    return _batch(-1, h, phi, r0, R_0, ctx)
+
+
+def generic_full_integral(K, H, phi, r0, R_0, ctx=None):
+    """Generic-kernel vertex-pyramid integral (src/kernel_integral_generic.cpp:216-221), batched."""
+    k = K.index if isinstance(K, KernelSpec) else get_kernel(K).index
+    return _batch(k, H, phi, r0, R_0, ctx)
+
+
+def _sel(kernel=0, support_in_h=0.0, generic_path=False, tabulated=False) -> KiwiKernelSel:
+    k = kernel.index if isinstance(kernel, KernelSpec) else (kernel if isinstance(kernel, int) else get_kernel(kernel).index)
+    return KiwiKernelSel(k, float(support_in_h), int(bool(generic_path)), int(bool(tabulated)))
+
+
+def face_integrals(particles, faces, kernel=0, support_in_h=0.0, generic_path=False, ctx=None):
+    """Batched face integrals: particles (n, 4) = (x0, y0, z0, h); faces: list of (nv, 3) vertex arrays in
+    the face's winding.  Returns (values, out_vert)."""
+    ctx = ctx or default_context()
+    part = _f64(particles).reshape(-1, 4)
+    n = part.shape[0]
+    if len(faces) != n:
+        raise KiwiError(-1, "one face per particle row is required")
+    nv = np.array([len(np.asarray(f).reshape(-1, 3)) for f in faces], dtype=np.int64)
+    off = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(nv, out=off[1:])
+    verts = _f64(np.concatenate([_f64(f).reshape(-1) for f in faces]) if n else np.zeros(0))
+    out = np.empty(n)
+    ov = np.empty(n, dtype=np.int32)
+    sel = _sel(kernel, support_in_h, generic_path)
+    ctx.check(ctx._L.kiwi_face_integral_batch(ctx.handle, C.byref(sel), n, _p(part), off.ctypes.data_as(_i64p),
+                                              _p(verts), _p(out), ov.ctypes.data_as(_i32p)), "face_integral")
+    return out, ov
+
+
+def compute_face_integral(x0, y0, z0, h, vertices, out_vert=False, ctx=None):
+    """compute_face_integral(x0, y0, z0, h, false, nullptr, vertices, &out_vert): cubic spline, support 2h."""
+    v, ov = face_integrals([[x0, y0, z0, h]], [vertices], kernel=0, support_in_h=2.0, ctx=ctx)
+    return (float(v[0]), int(ov[0])) if out_vert else float(v[0])
+
+
+def compute_face_integral_generic(x0, y0, z0, K, H, vertices, out_vert=False, ctx=None):
+    """compute_face_integral_generic(x0, y0, z0, K, H, vertices, &out_vert)."""
+    k = K if isinstance(K, KernelSpec) else get_kernel(K)
+    # H is passed as h = H / support_in_h with support_in_h = 1 on the generic path
+    v, ov = face_integrals([[x0, y0, z0, H]], [vertices], kernel=k.index, support_in_h=1.0, generic_path=True, ctx=ctx)
+    return (float(v[0]), int(ov[0])) if out_vert else float(v[0])
+
+
+@dataclass
+class KernelIntegrator:
+    """Dispatch of make_kernel_integrator (include/kiwi/kernel_integrator.hpp:35-45)."""
+    kernel: int = 0
+    support_in_h: float = 0.0
+    generic_path: bool = False
+    tabulated: bool = False
+
+    @property
+    def generic(self) -> bool:
+        s = self.support_in_h or KernelSpec(self.kernel).radkern
+        return self.generic_path or self.kernel != 0 or s != 2.0
+
+    def support(self, h):
+        return (self.support_in_h or KernelSpec(self.kernel).radkern) * h
+
+    def sel(self) -> KiwiKernelSel:
+        return _sel(self.kernel, self.support_in_h, self.generic_path, self.tabulated)
+
+
+def make_kernel_integrator(name="cubic_spline", support_radius_in_h=0.0, generic_path=False,
+                           use_tabulated_integral=False) -> KernelIntegrator:
+    return KernelIntegrator(get_kernel(name).index, float(support_radius_in_h), bool(generic_path),
+                            bool(use_tabulated_integral))
+
+
+# ---------------------------------------------------------------------------------------------- stages
+
+@dataclass
+class CartesianGridResult:
+    """include/kiwi/cartesian_grid.hpp:53-71; arrays are flat, x-major: (ix*ny + iy)*nz + iz."""
+    nx: int
+    ny: int
+    nz: int
+    bounds: tuple
+    density: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+    raw: np.ndarray | None = None
+    stats: dict = field(default_factory=dict)
+
+
+def _particles_struct(P: dict, device: bool = False):
+    keys = ("x", "y", "z", "vx", "vy", "vz", "m", "h")
+    if device:
+        ptrs = [C.cast(C.c_void_p(int(P[k].data_ptr())), _dp) for k in keys]
+        n = int(P["x"].numel())
+        keep = None
+    else:
+        keep = [_f64(P[k]) for k in keys]
+        n = len(keep[0])
+        for a in keep:
+            if len(a) != n:
+                raise KiwiError(-1, "particle arrays differ in length")
+        ptrs = [_p(a) for a in keep]
+    return KiwiParticles(n, *ptrs), keep
+
+
+def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", raw=False, ctx=None):
+    """Density and mass-weighted velocity of an SPH snapshot on a Cartesian grid -- the compute of
+    run_sph_to_grid_stage (src/cartesian_grid.cpp:76-321) on host arrays.  `particles` maps x y z vx vy
+    vz m h to 1-D arrays; `bounds` = (x_min, x_max, y_min, y_max, z_min, z_max); `shape` = (nx, ny, nz);
+    `kernel` a KernelIntegrator (default: cubic spline)."""
+    ctx = ctx or default_context()
+    ki = kernel or KernelIntegrator()
+    Ps, keep = _particles_struct(particles)
+    nx, ny, nz = (int(s) for s in shape)
+    grid = KiwiCartGrid((C.c_double * 6)(*[float(b) for b in bounds]), nx, ny, nz)
+    nc = nx * ny * nz
+    outs = [np.empty(nc) for _ in range(4)]
+    rawa = np.empty(4 * nc) if raw else None
+    st = KiwiStats()
+    sel = ki.sel()
+    ctx.check(ctx._L.kiwi_sph_to_grid(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
+                                      PRECISIONS.get(precision, precision), *[_p(o) for o in outs], _p(rawa),
+                                      C.byref(st)), "sph-to-grid")
+    return CartesianGridResult(nx, ny, nz, tuple(bounds), *outs, raw=rawa.reshape(4, nc) if raw else None,
+                               stats=st.as_dict())
+
+
+def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, precision="fp64", ctx=None):
+    """Device variant: `particles` and `out` (density, vx, vy, vz[, raw4]) hold CUDA tensors (float64,
+    contiguous).  Runs on the context's stream and returns the call's stats."""
+    ctx = ctx or default_context()
+    ki = kernel or KernelIntegrator()
+    Ps, _ = _particles_struct(particles, device=True)
+    nx, ny, nz = (int(s) for s in shape)
+    grid = KiwiCartGrid((C.c_double * 6)(*[float(b) for b in bounds]), nx, ny, nz)
+    st = KiwiStats()
+    sel = ki.sel()
+
+    def dp(t):
+        return C.cast(C.c_void_p(int(t.data_ptr())), _dp) if t is not None else None
+
+    ctx.check(ctx._L.kiwi_sph_to_grid_device(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
+                                             PRECISIONS.get(precision, precision), dp(out.get("density")),
+                                             dp(out.get("vx")), dp(out.get("vy")), dp(out.get("vz")),
+                                             dp(out.get("raw4")), C.byref(st)), "sph-to-grid")
+    return st.as_dict()
+
+
+def version() -> str:
+    return load_library().kiwi_version().decode()

@@ -1,0 +1,447 @@
+// The C ABI (include/kiwi_b200.h): context management, the batched scalar integral API, and the
+// sph-to-grid pipeline -- particle binning into cell tiles, then the cell-integral gather.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "../../include/kiwi_b200.h"
+#include "engine.hpp"
+#include "kernel_tables.h"
+#include "prims.cuh"
+
+using namespace kiwi_b200;
+
+namespace {
+
+// ------------------------------------------------------------------ binning kernels
+
+struct TileBox {
+    int x0, x1, y0, y1, z0, z1;  // inclusive tile ranges
+};
+
+// Per particle: the number of cell tiles its clamped support box touches (0 if none).
+__global__ void k_tile_counts(CartGeom g, DevParticles P, uint32_t* __restrict__ counts, TileBox* __restrict__ boxes,
+                              DevStats* __restrict__ st) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long outside_count = 0;
+    if (i < P.n) {
+        CellBox b;
+        bool outside = false;
+        uint32_t c = 0;
+        TileBox tb{0, -1, 0, -1, 0, -1};
+        if (particle_cell_box(g, P.x[i], P.y[i], P.z[i], P.h[i], b, &outside)) {
+            tb.x0 = b.x0 / kTileX; tb.x1 = b.x1 / kTileX;
+            tb.y0 = b.y0 / kTileY; tb.y1 = b.y1 / kTileY;
+            tb.z0 = b.z0 / kTileZ; tb.z1 = b.z1 / kTileZ;
+            c = (uint32_t)((tb.x1 - tb.x0 + 1) * (tb.y1 - tb.y0 + 1) * (tb.z1 - tb.z0 + 1));
+        }
+        if (outside) outside_count = 1;
+        counts[i] = c;
+        boxes[i] = tb;
+    }
+    for (int o = 16; o > 0; o >>= 1) outside_count += __shfl_down_sync(0xffffffffu, outside_count, o);
+    if ((threadIdx.x & 31) == 0 && outside_count) atomicAdd(&st->skipped_outside, outside_count);
+}
+
+// One thread per (particle, tile) entry: key = tile id, value = particle index, written in particle
+// order (the offsets are the exclusive scan of the counts).
+__global__ void k_tile_emit(CartGeom g, int64_t n, const int64_t* __restrict__ offs, const TileBox* __restrict__ boxes,
+                            int64_t total, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= total) return;
+    // particle = last p with offs[p] <= k
+    int64_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (offs[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    const TileBox tb = boxes[lo];
+    const int64_t q = k - offs[lo];
+    const int dz = tb.z1 - tb.z0 + 1, dy = tb.y1 - tb.y0 + 1;
+    const int tz = tb.z0 + (int)(q % dz), ty = tb.y0 + (int)((q / dz) % dy), tx = tb.x0 + (int)(q / ((int64_t)dz * dy));
+    keys[k] = (uint32_t)(((int64_t)tx * g.nty + ty) * g.ntz + tz);
+    vals[k] = (uint32_t)lo;
+}
+
+// range[2t], range[2t+1] = [begin, end) of tile t in the sorted key array (zero-length if absent).
+__global__ void k_tile_ranges(const uint32_t* __restrict__ keys, int64_t total, int64_t* __restrict__ range) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const uint32_t k = keys[i];
+    if (i == 0 || keys[i - 1] != k) range[2 * (int64_t)k] = i;
+    if (i == total - 1 || keys[i + 1] != k) range[2 * (int64_t)k + 1] = i + 1;
+}
+
+int resolve_kernel(KiwiCtx* ctx, const KiwiKernelSel* sel, KernelChoice* out) {
+    const int k = sel ? sel->kernel : 0;
+    if (k < 0 || k >= KIWI_NUM_KERNELS) return set_err(ctx, KIWI_ERR_ARG, "unknown kernel index %d", k);
+    double sup = sel ? sel->support_in_h : 0.0;
+    if (sup < 0.0) return set_err(ctx, KIWI_ERR_ARG, "kernel.support_radius_in_h must be > 0 (or 0 for the default)");
+    if (sup == 0.0) sup = kiwi_kernel_tables[k].radkern;
+    const bool generic_path = sel && sel->generic_path;
+    // Config::use_generic_kernel_path (src/config.cpp:275-277)
+    const bool generic = generic_path || k != 0 || sup != 2.0;
+    const bool tab = sel && sel->tabulated;
+    if (generic && tab)
+        return set_err(ctx, KIWI_ERR_ARG,
+                       "use_tabulated_integral is only available for the cubic spline kernel with its default support "
+                       "radius (and kernel.generic_path unset)");
+    if (tab) return set_err(ctx, KIWI_ERR_UNSUPPORTED, "the tabulated integral is not available in this build");
+    out->cubic = !generic;
+    out->tabulated = tab;
+    out->kernel = k;
+    out->support_in_h = sup;
+    return KIWI_OK;
+}
+
+int make_geom(KiwiCtx* ctx, const KiwiCartGrid* grid, double support_in_h, CartGeom* g) {
+    if (!grid) return set_err(ctx, KIWI_ERR_ARG, "grid is null");
+    const double* b = grid->bounds;
+    if (!(b[0] < b[1])) return set_err(ctx, KIWI_ERR_ARG, "domain.x_min must be < domain.x_max");
+    if (!(b[2] < b[3])) return set_err(ctx, KIWI_ERR_ARG, "domain.y_min must be < domain.y_max");
+    if (!(b[4] < b[5])) return set_err(ctx, KIWI_ERR_ARG, "domain.z_min must be < domain.z_max");
+    if (grid->nx <= 0 || grid->ny <= 0 || grid->nz <= 0)
+        return set_err(ctx, KIWI_ERR_ARG, "cartesian_grid resolution (resolved nx/ny/nz) must be > 0");
+    g->x_min = b[0];
+    g->y_min = b[2];
+    g->z_min = b[4];
+    g->nx = grid->nx;
+    g->ny = grid->ny;
+    g->nz = grid->nz;
+    g->dpx = (b[1] - b[0]) / grid->nx;
+    g->dpy = (b[3] - b[2]) / grid->ny;
+    g->dpz = (b[5] - b[4]) / grid->nz;
+    g->hpx = 0.5 * g->dpx;
+    g->hpy = 0.5 * g->dpy;
+    g->hpz = 0.5 * g->dpz;
+    g->cell_volume = g->dpx * g->dpy * g->dpz;
+    g->ntx = (g->nx + kTileX - 1) / kTileX;
+    g->nty = (g->ny + kTileY - 1) / kTileY;
+    g->ntz = (g->nz + kTileZ - 1) / kTileZ;
+    g->support_in_h = support_in_h;
+    const int64_t nt = (int64_t)g->ntx * g->nty * g->ntz;
+    if (nt >= (1LL << 31)) return set_err(ctx, KIWI_ERR_ARG, "grid too large (%lld tiles)", (long long)nt);
+    return KIWI_OK;
+}
+
+int check_ctx(KiwiCtx* ctx) {
+    if (!ctx) return KIWI_ERR_ARG;
+    KIWI_CUDA(ctx, cudaSetDevice(ctx->device));
+    return KIWI_OK;
+}
+
+// The full device pipeline of one sph-to-grid call: mean velocity, binning, gather.
+int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
+                    const CartOutputs& out_in, KiwiStats* stats) {
+    DevStats* d_stats = nullptr;
+    double* d_meanv = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_STATS, 1, &d_stats));
+    KIWI_TRY(scratch_t(ctx, S_MEANV, 4, &d_meanv));
+    KIWI_CUDA(ctx, cudaMemsetAsync(d_stats, 0, sizeof(DevStats), ctx->stream));
+    CartOutputs out = out_in;
+    out.meanv = d_meanv;
+    KIWI_TRY(fp64_mean_velocity(ctx, P, d_meanv));
+
+    const int64_t n = P.n;
+    const int64_t ntiles = (int64_t)g.ntx * g.nty * g.ntz;
+    uint32_t* counts = nullptr;
+    TileBox* boxes = nullptr;
+    int64_t* offs = nullptr;
+    int64_t* range = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_COUNT, (size_t)std::max<int64_t>(n, 1), &counts));
+    KIWI_TRY(scratch_t(ctx, S_BOX, (size_t)std::max<int64_t>(n, 1), &boxes));
+    KIWI_TRY(scratch_t(ctx, S_OFFS, (size_t)std::max<int64_t>(n, 1) + 1, &offs));
+    KIWI_TRY(scratch_t(ctx, S_TILE_RANGE, (size_t)(2 * ntiles), &range));
+    int64_t* d_total = offs + std::max<int64_t>(n, 1);
+    KIWI_CUDA(ctx, cudaMemsetAsync(range, 0, sizeof(int64_t) * 2 * ntiles, ctx->stream));
+    if (n > 0) {
+        k_tile_counts<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g, P, counts, boxes, d_stats);
+        KIWI_LAUNCHED(ctx);
+    }
+    KIWI_TRY(exclusive_scan<uint32_t>(ctx, counts, n, offs, d_total));
+    int64_t total = 0;
+    KIWI_CUDA(ctx, cudaMemcpyAsync(&total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (total >= (1LL << 32)) return set_err(ctx, KIWI_ERR_LIMIT, "too many (tile, particle) entries: %lld", (long long)total);
+
+    uint32_t *k0, *v0, *k1, *v1;
+    KIWI_TRY(scratch_t(ctx, S_KEYS0, (size_t)std::max<int64_t>(total, 1), &k0));
+    KIWI_TRY(scratch_t(ctx, S_VALS0, (size_t)std::max<int64_t>(total, 1), &v0));
+    KIWI_TRY(scratch_t(ctx, S_KEYS1, (size_t)std::max<int64_t>(total, 1), &k1));
+    KIWI_TRY(scratch_t(ctx, S_VALS1, (size_t)std::max<int64_t>(total, 1), &v1));
+    const uint32_t* sorted_vals = v0;
+    if (total > 0) {
+        k_tile_emit<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(g, n, offs, boxes, total, k0, v0);
+        KIWI_LAUNCHED(ctx);
+        int key_bits = 1;
+        while ((1LL << key_bits) < ntiles) ++key_bits;
+        bool second = false;
+        KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, total, key_bits, &second));
+        const uint32_t* sk = second ? k1 : k0;
+        sorted_vals = second ? v1 : v0;
+        k_tile_ranges<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(sk, total, range);
+        KIWI_LAUNCHED(ctx);
+    }
+    TileLists tl{sorted_vals, range, ntiles};
+
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    if (precision == KIWI_FP64) {
+        KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl, out, d_stats));
+    } else {
+        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "precision %d is not available in this build", precision);
+    }
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+
+    DevStats hs;
+    KIWI_CUDA(ctx, cudaMemcpyAsync(&hs, d_stats, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+        stats->bbox_pairs = (int64_t)hs.bbox_pairs;
+        stats->sphere_pairs = (int64_t)hs.sphere_pairs;
+        stats->evaluated_pairs = (int64_t)hs.evaluated_pairs;
+        stats->skipped_outside = (int64_t)hs.skipped_outside;
+        stats->neg_clamped = (int64_t)hs.neg_clamped;
+        stats->neg_warned = (int64_t)hs.neg_warned;
+        stats->fp64_fallback = (int64_t)hs.fp64_fallback;
+        stats->tile_pairs = total;
+        stats->gather_ms = ms;
+    }
+    return KIWI_OK;
+}
+
+bool particles_ok(KiwiCtx* ctx, const KiwiParticles* p, int* rc) {
+    if (!p) {
+        *rc = set_err(ctx, KIWI_ERR_ARG, "particles is null");
+        return false;
+    }
+    if (p->n < 0 || p->n >= (1LL << 32)) {
+        *rc = set_err(ctx, KIWI_ERR_ARG, "particle count %lld out of range", (long long)p->n);
+        return false;
+    }
+    if (p->n > 0 && (!p->x || !p->y || !p->z || !p->vx || !p->vy || !p->vz || !p->m || !p->h)) {
+        *rc = set_err(ctx, KIWI_ERR_ARG, "a particle array is null");
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* kiwi_version(void) { return "kiwi_b200 0.1.0 (sm_100a)"; }
+
+int kiwi_ctx_create(int device, KiwiCtx** out) {
+    if (!out) return KIWI_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return KIWI_ERR_NODEV;
+    }
+    if (device < 0 || device >= ndev) return KIWI_ERR_NODEV;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) return KIWI_ERR_NODEV;
+    KiwiCtx* ctx = new KiwiCtx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return KIWI_ERR_CUDA;
+    }
+    for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+    if (fp64_init_tables(ctx) != KIWI_OK) {
+        kiwi_ctx_destroy(ctx);
+        return KIWI_ERR_CUDA;
+    }
+    *out = ctx;
+    return KIWI_OK;
+}
+
+void kiwi_ctx_destroy(KiwiCtx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < KiwiCtx::kSlots; ++i)
+        if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
+    for (auto& ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* kiwi_last_error(const KiwiCtx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* kiwi_ctx_stream(KiwiCtx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int kiwi_ctx_synchronize(KiwiCtx* ctx) {
+    KIWI_TRY(check_ctx(ctx));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return KIWI_OK;
+}
+
+int kiwi_kernel_index(const char* name) {
+    if (!name) return -1;
+    std::string n(name);
+    std::transform(n.begin(), n.end(), n.begin(), [](unsigned char c) { return (char)std::tolower(c); });
+    std::replace(n.begin(), n.end(), '-', '_');
+    std::replace(n.begin(), n.end(), ' ', '_');
+    // the aliases accepted by get_kernel (src/kernel_spec_data.cpp:175-187)
+    static const char* const names[KIWI_NUM_KERNELS][3] = {
+        {"cubic", "cubic_spline", "m4"},          {"quartic", "quartic_spline", "m5"},
+        {"quintic", "quintic_spline", "m6"},      {"wendland_c2", "wendlandc2", "wc2"},
+        {"wendland_c4", "wendlandc4", "wc4"},     {"wendland_c6", "wendlandc6", "wc6"}};
+    for (int k = 0; k < KIWI_NUM_KERNELS; ++k)
+        for (int a = 0; a < 3; ++a)
+            if (n == names[k][a]) return k;
+    return -1;
+}
+
+int kiwi_kernel_info(int kernel, double* out7) {
+    if (kernel < 0 || kernel >= KIWI_NUM_KERNELS || !out7) return KIWI_ERR_ARG;
+    const KiwiKernelTable& K = kiwi_kernel_tables[kernel];
+    out7[0] = K.nreg;
+    out7[1] = K.A2_pi;
+    out7[2] = K.A3_pi;
+    out7[3] = K.radkern;
+    out7[4] = K.hfact;
+    out7[5] = K.c[0];
+    out7[6] = K.c[1];
+    return KIWI_OK;
+}
+
+int kiwi_full_integral_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi,
+                             const double* r0, const double* R_0, double* out) {
+    KIWI_TRY(check_ctx(ctx));
+    if (kernel >= KIWI_NUM_KERNELS) return set_err(ctx, KIWI_ERR_ARG, "unknown kernel index %d", kernel);
+    if (n < 0 || (n > 0 && (!arg0 || !phi || !r0 || !R_0 || !out))) return set_err(ctx, KIWI_ERR_ARG, "bad arrays");
+    if (n == 0) return KIWI_OK;
+    double* d = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_MISC0, (size_t)(5 * n), &d));
+    const size_t b = sizeof(double) * n;
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d, arg0, b, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d + n, phi, b, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d + 2 * n, r0, b, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d + 3 * n, R_0, b, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_TRY(fp64_full_integral(ctx, kernel < 0 ? -1 : kernel, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(out, d + 4 * n, b, cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return KIWI_OK;
+}
+
+int kiwi_face_integral_batch(KiwiCtx* ctx, const KiwiKernelSel* kernel, int64_t n_faces, const double* particle,
+                             const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert) {
+    KIWI_TRY(check_ctx(ctx));
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    if (n_faces < 0 || (n_faces > 0 && (!particle || !vert_off || !verts || !out)))
+        return set_err(ctx, KIWI_ERR_ARG, "bad arrays");
+    if (n_faces == 0) return KIWI_OK;
+    const int64_t nv = vert_off[n_faces];
+    if (nv < 0 || vert_off[0] != 0) return set_err(ctx, KIWI_ERR_ARG, "vert_off must start at 0 and be non-decreasing");
+    for (int64_t i = 0; i < n_faces; ++i)
+        if (vert_off[i + 1] < vert_off[i]) return set_err(ctx, KIWI_ERR_ARG, "vert_off must be non-decreasing");
+    double *dp = nullptr, *dv = nullptr, *dout = nullptr;
+    int64_t* doff = nullptr;
+    int32_t* dov = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_MISC0, (size_t)(4 * n_faces), &dp));
+    KIWI_TRY(scratch_t(ctx, S_MISC1, (size_t)std::max<int64_t>(3 * nv, 1), &dv));
+    KIWI_TRY(scratch_t(ctx, S_MISC2, (size_t)(n_faces + 1), &doff));
+    KIWI_TRY(scratch_t(ctx, S_OUT, (size_t)n_faces, &dout));
+    KIWI_TRY(scratch_t(ctx, S_COUNT, (size_t)n_faces, &dov));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(dp, particle, sizeof(double) * 4 * n_faces, cudaMemcpyHostToDevice, ctx->stream));
+    if (nv > 0)
+        KIWI_CUDA(ctx, cudaMemcpyAsync(dv, verts, sizeof(double) * 3 * nv, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(doff, vert_off, sizeof(int64_t) * (n_faces + 1), cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_TRY(fp64_face_integral(ctx, kc, n_faces, dp, doff, dv, dout, dov));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(out, dout, sizeof(double) * n_faces, cudaMemcpyDeviceToHost, ctx->stream));
+    if (out_vert)
+        KIWI_CUDA(ctx, cudaMemcpyAsync(out_vert, dov, sizeof(int32_t) * n_faces, cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return KIWI_OK;
+}
+
+int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                            const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy,
+                            double* vz, double* raw4, KiwiStats* stats) {
+    KIWI_TRY(check_ctx(ctx));
+    int rc = KIWI_OK;
+    if (!particles_ok(ctx, particles, &rc)) return rc;
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    CartGeom g;
+    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+    DevParticles P{particles->n, particles->x, particles->y, particles->z, particles->vx,
+                   particles->vy, particles->vz, particles->m, particles->h};
+    CartOutputs out{density, vx, vy, vz, raw4, nullptr};
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    KIWI_TRY(sph_to_grid_dev(ctx, P, g, kc, precision, out, stats));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        stats->total_ms = ms;
+    }
+    return KIWI_OK;
+}
+
+int kiwi_sph_to_grid(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                     const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy, double* vz,
+                     double* raw4, KiwiStats* stats) {
+    KIWI_TRY(check_ctx(ctx));
+    int rc = KIWI_OK;
+    if (!particles_ok(ctx, particles, &rc)) return rc;
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    CartGeom g;
+    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+    const int64_t n = particles->n;
+    const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+    double* dpart = nullptr;
+    double* dout = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_PART, (size_t)std::max<int64_t>(8 * n, 1), &dpart));
+    KIWI_TRY(scratch_t(ctx, S_OUT, (size_t)(raw4 ? 8 : 4) * ncell, &dout));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    const double* src[8] = {particles->x, particles->y, particles->z, particles->vx,
+                            particles->vy, particles->vz, particles->m, particles->h};
+    for (int a = 0; a < 8 && n > 0; ++a)
+        KIWI_CUDA(ctx, cudaMemcpyAsync(dpart + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    DevParticles P{n, dpart, dpart + n, dpart + 2 * n, dpart + 3 * n, dpart + 4 * n, dpart + 5 * n, dpart + 6 * n,
+                   dpart + 7 * n};
+    CartOutputs out{dout, dout + ncell, dout + 2 * ncell, dout + 3 * ncell, raw4 ? dout + 4 * ncell : nullptr, nullptr};
+    KIWI_TRY(sph_to_grid_dev(ctx, P, g, kc, precision, out, stats));
+    double* dst[4] = {density, vx, vy, vz};
+    for (int a = 0; a < 4; ++a)
+        if (dst[a])
+            KIWI_CUDA(ctx, cudaMemcpyAsync(dst[a], dout + a * ncell, sizeof(double) * ncell, cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+    if (raw4)
+        KIWI_CUDA(ctx, cudaMemcpyAsync(raw4, dout + 4 * ncell, sizeof(double) * 4 * ncell, cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        stats->total_ms = ms;
+    }
+    return KIWI_OK;
+}
+
+int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                     const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
+                     double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats) {
+    (void)particles; (void)home_cell; (void)cells; (void)kernel; (void)precision;
+    (void)density; (void)vx; (void)vy; (void)vz; (void)raw4; (void)stats;
+    KIWI_TRY(check_ctx(ctx));
+    return set_err(ctx, KIWI_ERR_UNSUPPORTED, "kiwi_map_voronoi is not available in this build");
+}
+
+}  // extern "C"

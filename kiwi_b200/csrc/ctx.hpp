@@ -1,0 +1,110 @@
+// Host-side context of the C ABI: device, stream, events, error text and a grow-only scratch arena.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "../../include/kiwi_b200.h"
+
+struct KiwiCtx {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    std::string err;
+    // Scratch slots: each is grown on demand and reused by later calls on this context.
+    static constexpr int kSlots = 24;
+    void* slot_ptr[kSlots] = {};
+    size_t slot_bytes[kSlots] = {};
+};
+
+namespace kiwi_b200 {
+
+inline int set_err(KiwiCtx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    return code;
+}
+
+#define KIWI_CUDA(ctx, call)                                                                              \
+    do {                                                                                                  \
+        cudaError_t e_ = (call);                                                                          \
+        if (e_ != cudaSuccess)                                                                            \
+            return ::kiwi_b200::set_err((ctx), KIWI_ERR_CUDA, "%s failed: %s (%s:%d)", #call,              \
+                                        cudaGetErrorString(e_), __FILE__, __LINE__);                      \
+    } while (0)
+
+#define KIWI_LAUNCHED(ctx)                                                                                \
+    do {                                                                                                  \
+        cudaError_t e_ = cudaGetLastError();                                                              \
+        if (e_ != cudaSuccess)                                                                            \
+            return ::kiwi_b200::set_err((ctx), KIWI_ERR_CUDA, "kernel launch failed: %s (%s:%d)",          \
+                                        cudaGetErrorString(e_), __FILE__, __LINE__);                      \
+    } while (0)
+
+#define KIWI_TRY(expr)          \
+    do {                        \
+        int rc_ = (expr);       \
+        if (rc_ != KIWI_OK) return rc_; \
+    } while (0)
+
+// Device scratch of at least `bytes` in slot `slot` (grow-only; contents are not preserved on growth).
+inline int scratch(KiwiCtx* ctx, int slot, size_t bytes, void** out) {
+    if (bytes == 0) bytes = 256;
+    if (ctx->slot_bytes[slot] < bytes) {
+        if (ctx->slot_ptr[slot]) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->slot_ptr[slot]);
+            ctx->slot_ptr[slot] = nullptr;
+            ctx->slot_bytes[slot] = 0;
+        }
+        size_t want = bytes + bytes / 4;
+        cudaError_t e = cudaMalloc(&ctx->slot_ptr[slot], want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(ctx, KIWI_ERR_ALLOC, "cudaMalloc of %zu bytes of scratch failed: %s", want,
+                           cudaGetErrorString(e));
+        }
+        ctx->slot_bytes[slot] = want;
+    }
+    *out = ctx->slot_ptr[slot];
+    return KIWI_OK;
+}
+
+template <class T>
+inline int scratch_t(KiwiCtx* ctx, int slot, size_t count, T** out) {
+    void* p = nullptr;
+    int rc = scratch(ctx, slot, count * sizeof(T), &p);
+    *out = static_cast<T*>(p);
+    return rc;
+}
+
+// Scratch slot numbers (fixed so that a call never overwrites a buffer it still needs).
+enum ScratchSlot {
+    S_PART = 0,      // staged particle SoA (host entry points)
+    S_OUT,           // staged outputs
+    S_BOX,           // per-particle clamped bounding boxes
+    S_COUNT,         // per-particle tile counts
+    S_OFFS,          // per-particle tile-pair offsets
+    S_KEYS0,
+    S_VALS0,
+    S_KEYS1,
+    S_VALS1,
+    S_HIST,          // radix histograms
+    S_SCAN,          // scan partials
+    S_TILE_RANGE,    // per-tile [begin, end)
+    S_STATS,         // device counters
+    S_MEANV,         // mean velocity
+    S_MISC0,
+    S_MISC1,
+    S_MISC2,
+    S_MISC3,
+};
+
+}  // namespace kiwi_b200

@@ -1,0 +1,51 @@
+// Interfaces between the C-ABI layer (capi.cu) and the translation units holding the device kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "cart_common.cuh"
+#include "ctx.hpp"
+
+namespace kiwi_b200 {
+
+// Device SoA view of a particle snapshot.
+struct DevParticles {
+    int64_t n;
+    const double *x, *y, *z, *vx, *vy, *vz, *m, *h;
+};
+
+// Resolved kernel choice: cubic closed form (support 2h) or generic table `kernel` with support
+// support_in_h * h.
+struct KernelChoice {
+    bool cubic;
+    bool tabulated;
+    int kernel;
+    double support_in_h;
+};
+
+// Tile lists built by the binning step: tile t owns list[range[2t] .. range[2t+1]) (particle indices in
+// ascending order).
+struct TileLists {
+    const uint32_t* list;
+    const int64_t* range;
+    int64_t ntiles;
+};
+
+struct CartOutputs {
+    double *density, *vx, *vy, *vz;  // finalised fields (any may be null)
+    double* raw4;                     // optional raw sums, 4 * ncell
+    const double* meanv;              // device, 3 doubles: mean particle velocity
+};
+
+// kiwi_fp64.cu
+int fp64_init_tables(KiwiCtx* ctx);
+int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
+                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats);
+int fp64_full_integral(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi, const double* r0,
+                       const double* R0, double* out);
+int fp64_face_integral(KiwiCtx* ctx, const KernelChoice& k, int64_t n, const double* particle,
+                       const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert);
+int fp64_mean_velocity(KiwiCtx* ctx, const DevParticles& P, double* d_meanv);
+
+}  // namespace kiwi_b200

@@ -1,0 +1,303 @@
+// Plain (all-FP64) form: the cell-integral gather over Cartesian cell tiles, the batched scalar
+// integral API and the mean-velocity reduction.  Built with --fmad=false so that every product and sum
+// rounds exactly as in the reference's x86-64 build (see kiwi_math.cuh).
+#include <cuda_runtime.h>
+
+#include "engine.hpp"
+#include "kiwi_math.cuh"
+
+namespace kiwi_b200 {
+
+__constant__ KiwiKernelTable c_tables[KIWI_NUM_KERNELS];
+
+int fp64_init_tables(KiwiCtx* ctx) {
+    KIWI_CUDA(ctx, cudaMemcpyToSymbol(c_tables, kiwi_kernel_tables, sizeof(kiwi_kernel_tables)));
+    return KIWI_OK;
+}
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kPMax = 32;      // particles per chunk (one warp builds a chunk)
+constexpr int kChunkCap = 1024; // (particle, cell) pairs per chunk; >= kTileCells so one particle always fits
+static_assert(kChunkCap >= kTileCells, "a single particle's tile box must fit in one chunk");
+constexpr int kCellsPerThread = kTileCells / kThreads;
+static_assert(kTileCells % kThreads == 0, "tile cells must split evenly over the threads");
+
+template <bool CUBIC>
+__device__ __forceinline__ double pair_msum(int kernel, double x0, double y0, double z0, double h, double support,
+                                            double cx, double cy, double cz, double hx, double hy, double hz) {
+    if (CUBIC) {
+        CubicEval ev;
+        ev.h = h;
+        return box_cell_msum(x0, y0, z0, support, cx, cy, cz, hx, hy, hz, ev);
+    } else {
+        GenericEval ev;
+        ev.K = &c_tables[kernel];
+        ev.H = support;
+        return box_cell_msum(x0, y0, z0, support, cx, cy, cz, hx, hy, hz, ev);
+    }
+}
+
+__device__ __forceinline__ void add_stat(unsigned long long* dst, unsigned long long v) {
+    // warp-aggregate, then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// One CTA = one tile of kTileX x kTileY x kTileZ cells.  The tile's particle list (ascending particle
+// index) is walked in chunks of up to kPMax particles / kChunkCap pairs: all threads evaluate the
+// chunk's (particle, cell) pairs into shared memory, then each thread adds, for the cells it owns, the
+// chunk's values in particle order.  So every cell's sum runs over its particles in ascending order --
+// the summation order of the reference's single-threaded loop -- with no atomics.
+template <bool CUBIC>
+__global__ void __launch_bounds__(kThreads) k_cart_gather(CartGeom g, DevParticles P, int kernel,
+                                                          const uint32_t* __restrict__ list,
+                                                          const int64_t* __restrict__ range, CartOutputs out,
+                                                          DevStats* __restrict__ st) {
+    __shared__ double s_x[kPMax], s_y[kPMax], s_z[kPMax], s_h[kPMax], s_m[kPMax], s_vx[kPMax], s_vy[kPMax],
+        s_vz[kPMax];
+    __shared__ int s_lo[kPMax][3], s_dim[kPMax][3], s_start[kPMax];
+    __shared__ int s_np, s_total;
+    __shared__ double s_R[kChunkCap];
+
+    const int64_t t = blockIdx.x;
+    const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
+    const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    double acc[kCellsPerThread][4];
+#pragma unroll
+    for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
+
+    unsigned long long n_bbox = 0, n_sphere = 0, n_neg = 0, n_warn = 0;
+    const int64_t beg = range[2 * t], end = range[2 * t + 1];
+    const double sup_in_h = g.support_in_h;
+
+    for (int64_t pos = beg; pos < end;) {
+        if (warp == 0) {
+            const int64_t idx = pos + lane;
+            int size = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+            double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
+            if (idx < end) {
+                const uint32_t p = list[idx];
+                px = P.x[p]; py = P.y[p]; pz = P.z[p]; ph = P.h[p];
+                pm = P.m[p]; pvx = P.vx[p]; pvy = P.vy[p]; pvz = P.vz[p];
+                CellBox b;
+                bool outside;
+                particle_cell_box(g, px, py, pz, ph, b, &outside);
+                const int x0 = max(b.x0, bx), x1 = min(b.x1, bx + kTileX - 1);
+                const int y0 = max(b.y0, by), y1 = min(b.y1, by + kTileY - 1);
+                const int z0 = max(b.z0, bz), z1 = min(b.z1, bz + kTileZ - 1);
+                lo0 = x0 - bx; lo1 = y0 - by; lo2 = z0 - bz;
+                d0 = x1 - x0 + 1; d1 = y1 - y0 + 1; d2 = z1 - z0 + 1;
+                size = (d0 > 0 && d1 > 0 && d2 > 0) ? d0 * d1 * d2 : 0;
+            }
+            int incl = size;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const bool take = (idx < end) && incl <= kChunkCap;
+            const unsigned tm = __ballot_sync(0xffffffffu, take);
+            const int np = __popc(tm);
+            if (take) {
+                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph;
+                s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
+                s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
+                s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
+                s_start[lane] = incl - size;
+            }
+            if (lane == np - 1) {
+                s_np = np;
+                s_total = incl;
+            }
+        }
+        __syncthreads();
+        const int np = s_np, total = s_total;
+
+        for (int k = threadIdx.x; k < total; k += kThreads) {
+            int lo = 0, hi = np - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_start[mid] <= k) lo = mid; else hi = mid - 1;
+            }
+            const int j = lo;
+            const int q = k - s_start[j];
+            const int dz = s_dim[j][2], dy = s_dim[j][1];
+            const int qz = q % dz, qr = q / dz, qy = qr % dy, qx = qr / dy;
+            const int ix = bx + s_lo[j][0] + qx, iy = by + s_lo[j][1] + qy, iz = bz + s_lo[j][2] + qz;
+            const double x0 = s_x[j], y0 = s_y[j], z0 = s_z[j], h = s_h[j];
+            const double radius = mul_rn(sup_in_h, h);
+            const double cx = cell_centre(g.x_min, ix, g.dpx);
+            const double cy = cell_centre(g.y_min, iy, g.dpy);
+            const double cz = cell_centre(g.z_min, iz, g.dpz);
+            ++n_bbox;
+            {
+                const double ex = fmax(fabs(x0 - cx) - g.hpx, 0.0), ey = fmax(fabs(y0 - cy) - g.hpy, 0.0),
+                             ez = fmax(fabs(z0 - cz) - g.hpz, 0.0);
+                if (ex * ex + ey * ey + ez * ez < radius * radius) ++n_sphere;
+            }
+            double msum = pair_msum<CUBIC>(kernel, x0, y0, z0, h, CUBIC ? 2 * h : radius, cx, cy, cz, g.hpx, g.hpy,
+                                           g.hpz);
+            if (msum < 0.0) {
+                ++n_neg;
+                if (msum <= -0.01) ++n_warn;
+                msum = 0.0;
+            }
+            s_R[k] = msum;
+        }
+        __syncthreads();
+
+#pragma unroll
+        for (int c = 0; c < kCellsPerThread; ++c) {
+            const int li = threadIdx.x + c * kThreads;
+            const int lz = li % kTileZ, ly = (li / kTileZ) % kTileY, lx = li / (kTileZ * kTileY);
+            for (int j = 0; j < np; ++j) {
+                const int ox = lx - s_lo[j][0], oy = ly - s_lo[j][1], oz = lz - s_lo[j][2];
+                if (ox < 0 || oy < 0 || oz < 0 || ox >= s_dim[j][0] || oy >= s_dim[j][1] || oz >= s_dim[j][2]) continue;
+                const double msum = s_R[s_start[j] + (ox * s_dim[j][1] + oy) * s_dim[j][2] + oz];
+                if (msum == 0.0) continue;
+                const double mm = msum * s_m[j];
+                acc[c][0] += mm;
+                acc[c][1] += mm * s_vx[j];
+                acc[c][2] += mm * s_vy[j];
+                acc[c][3] += mm * s_vz[j];
+            }
+        }
+        __syncthreads();
+        pos += np;
+    }
+
+    const double mvx = out.meanv[0], mvy = out.meanv[1], mvz = out.meanv[2];
+    const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+#pragma unroll
+    for (int c = 0; c < kCellsPerThread; ++c) {
+        const int li = threadIdx.x + c * kThreads;
+        const int lz = li % kTileZ, ly = (li / kTileZ) % kTileY, lx = li / (kTileZ * kTileY);
+        const int ix = bx + lx, iy = by + ly, iz = bz + lz;
+        if (ix >= g.nx || iy >= g.ny || iz >= g.nz) continue;
+        const int64_t i3 = ((int64_t)ix * g.ny + iy) * g.nz + iz;
+        const double M = acc[c][0];
+        if (out.density) out.density[i3] = M / g.cell_volume;
+        const bool has = M > 0.0;
+        if (out.vx) out.vx[i3] = has ? acc[c][1] / M : mvx;
+        if (out.vy) out.vy[i3] = has ? acc[c][2] / M : mvy;
+        if (out.vz) out.vz[i3] = has ? acc[c][3] / M : mvz;
+        if (out.raw4) {
+            out.raw4[i3] = M;
+            out.raw4[ncell + i3] = acc[c][1];
+            out.raw4[2 * ncell + i3] = acc[c][2];
+            out.raw4[3 * ncell + i3] = acc[c][3];
+        }
+    }
+    add_stat(&st->bbox_pairs, n_bbox);
+    add_stat(&st->sphere_pairs, n_sphere);
+    add_stat(&st->evaluated_pairs, n_bbox);
+    add_stat(&st->neg_clamped, n_neg);
+    add_stat(&st->neg_warned, n_warn);
+}
+
+__global__ void k_full_integral(int kernel, int64_t n, const double* __restrict__ arg0, const double* __restrict__ phi,
+                                const double* __restrict__ r0, const double* __restrict__ R0, double* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = (kernel < 0) ? cubic_full_integral(arg0[i], phi[i], r0[i], R0[i])
+                          : generic_full_integral(&c_tables[kernel], arg0[i], phi[i], r0[i], R0[i]);
+}
+
+__global__ void k_face_integral(bool cubic, int kernel, double support_in_h, int64_t n,
+                                const double* __restrict__ particle, const int64_t* __restrict__ vert_off,
+                                const double* __restrict__ verts, double* __restrict__ out,
+                                int32_t* __restrict__ out_vert) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x0 = particle[4 * i], y0 = particle[4 * i + 1], z0 = particle[4 * i + 2], h = particle[4 * i + 3];
+    FlatVerts V{verts + 3 * vert_off[i]};
+    const int nv = (int)(vert_off[i + 1] - vert_off[i]);
+    int ov = 0;
+    double r;
+    if (cubic) {
+        CubicEval ev;
+        ev.h = h;
+        r = face_integral(x0, y0, z0, 2 * h, V, nv, &ov, ev);
+    } else {
+        GenericEval ev;
+        ev.K = &c_tables[kernel];
+        ev.H = mul_rn(support_in_h, h);
+        r = face_integral(x0, y0, z0, ev.H, V, nv, &ov, ev);
+    }
+    out[i] = r;
+    if (out_vert) out_vert[i] = ov;
+}
+
+// Mean particle velocity over all particles (src/cartesian_grid.cpp:205-207, 294-298), by one block
+// in a fixed reduction order, so it is bitwise repeatable.
+__global__ void k_mean_velocity(DevParticles P, double* __restrict__ meanv) {
+    __shared__ double sh[3][1024];
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int64_t i = threadIdx.x; i < P.n; i += blockDim.x) {
+        s0 += P.vx[i];
+        s1 += P.vy[i];
+        s2 += P.vz[i];
+    }
+    sh[0][threadIdx.x] = s0;
+    sh[1][threadIdx.x] = s1;
+    sh[2][threadIdx.x] = s2;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            sh[0][threadIdx.x] += sh[0][threadIdx.x + o];
+            sh[1][threadIdx.x] += sh[1][threadIdx.x + o];
+            sh[2][threadIdx.x] += sh[2][threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const double n = (double)P.n;
+        meanv[0] = P.n > 0 ? sh[0][0] / n : 0.0;
+        meanv[1] = P.n > 0 ? sh[1][0] / n : 0.0;
+        meanv[2] = P.n > 0 ? sh[2][0] / n : 0.0;
+    }
+}
+
+}  // namespace
+
+int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
+                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats) {
+    if (tl.ntiles <= 0) return KIWI_OK;
+    if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
+    if (k.cubic)
+        k_cart_gather<true><<<(unsigned)tl.ntiles, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out,
+                                                                              d_stats);
+    else
+        k_cart_gather<false><<<(unsigned)tl.ntiles, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out,
+                                                                               d_stats);
+    KIWI_LAUNCHED(ctx);
+    return KIWI_OK;
+}
+
+int fp64_full_integral(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi, const double* r0,
+                       const double* R0, double* out) {
+    if (n <= 0) return KIWI_OK;
+    k_full_integral<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(kernel, n, arg0, phi, r0, R0, out);
+    KIWI_LAUNCHED(ctx);
+    return KIWI_OK;
+}
+
+int fp64_face_integral(KiwiCtx* ctx, const KernelChoice& k, int64_t n, const double* particle,
+                       const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert) {
+    if (n <= 0) return KIWI_OK;
+    k_face_integral<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(k.cubic, k.kernel, k.support_in_h, n,
+                                                                          particle, vert_off, verts, out, out_vert);
+    KIWI_LAUNCHED(ctx);
+    return KIWI_OK;
+}
+
+int fp64_mean_velocity(KiwiCtx* ctx, const DevParticles& P, double* d_meanv) {
+    k_mean_velocity<<<1, 1024, 0, ctx->stream>>>(P, d_meanv);
+    KIWI_LAUNCHED(ctx);
+    return KIWI_OK;
+}
+
+}  // namespace kiwi_b200

@@ -1,0 +1,135 @@
+"""GPU parity of the sph-to-grid path (all-FP64 form) against the reference's own outputs (the committed
+fixtures under tests/golden/, made by the reference library) and against the CPU oracle, plus the
+invariants the reference's tests check (tests/synthetic_test.py:100-209, tests/real_data_test.py:142-196)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import random_particles
+from gpu_checks import FP64_REL, assert_grid_match, cell_errors
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "grid_*.npz")))
+
+
+def _load(fn):
+    d = np.load(fn)
+    P = {k: d[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+    return d, P
+
+
+def _integrator(kiwi, d):
+    k = int(d["kernel_index"])
+    return kiwi.KernelIntegrator(kernel=k, support_in_h=0.0, generic_path=bool(d["generic"]) and k == 0)
+
+
+@pytest.mark.parametrize("fn", GOLDEN, ids=[os.path.basename(f)[5:-4] for f in GOLDEN])
+def test_matches_reference_fixture(kiwi, ctx, fn):
+    d, P = _load(fn)
+    res = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=_integrator(kiwi, d), ctx=ctx)
+    assert_grid_match(res, d["out_density"], d["out_vx"], d["out_vy"], d["out_vz"], label=os.path.basename(fn))
+
+
+def test_padded_domain_conserves_mass(kiwi, ctx):
+    d, P = _load(os.path.join(ROOT, "tests", "golden", "grid_cubic_padded.npz"))
+    res = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), ctx=ctx)
+    b, s = d["bounds"], d["shape"]
+    vol = np.prod([(b[2 * i + 1] - b[2 * i]) / s[i] for i in range(3)])
+    total = res.density.sum() * vol
+    assert abs(total - P["m"].sum()) / P["m"].sum() < 1e-12
+
+
+def test_bulk_velocity_recovered_every_kernel(kiwi, ctx):
+    """tests/synthetic_test.py: a cloud with one bulk velocity; every cell with density carries it, and
+    with h scaled to a common support the grid holds the whole mass, for every kernel."""
+    rng = np.random.default_rng(12345)
+    n = 150
+    pos = rng.normal(size=(n, 3)) * 0.35 + 1.0
+    for k, radkern in enumerate([2.0, 2.5, 3.0, 2.0, 2.0, 2.0]):
+        P = {"x": pos[:, 0], "y": pos[:, 1], "z": pos[:, 2], "vx": np.full(n, 2.0), "vy": np.full(n, -1.0),
+             "vz": np.full(n, 0.5), "m": np.full(n, 0.01), "h": np.full(n, 0.12 * 2.0 / radkern)}
+        b = (-0.5, 2.5, -0.5, 2.5, -0.5, 2.5)
+        res = kiwi.sph_to_grid(P, b, (20, 20, 20), kernel=kiwi.KernelIntegrator(kernel=k), ctx=ctx)
+        vol = (3.0 / 20) ** 3
+        assert abs(res.density.sum() * vol - 1.5) / 1.5 < 1e-10, k
+        m = res.density > 1e-6 * res.density.max()
+        assert np.max(np.abs(res.vx[m] - 2.0)) < 1e-6 and np.max(np.abs(res.vy[m] + 1.0)) < 1e-6
+        assert np.all(np.isfinite(res.density)) and res.density.min() >= 0.0
+
+
+def test_generic_cubic_equals_fast_path(kiwi, ctx):
+    """tests/synthetic_test.py:173-180: kernel.generic_path reproduces the cubic fast path to 1e-8 of the peak."""
+    P = random_particles(200, 3)
+    b = (0, 2, 0, 2, 0, 2)
+    a = kiwi.sph_to_grid(P, b, (16, 16, 16), ctx=ctx)
+    g = kiwi.sph_to_grid(P, b, (16, 16, 16), kernel=kiwi.KernelIntegrator(generic_path=True), ctx=ctx)
+    assert np.max(np.abs(a.density - g.density)) / a.density.max() < 1e-8
+
+
+def test_matches_oracle_random_cases(kiwi, ctx, oracle):
+    for seed, shape, k in ((1, (9, 17, 11), -1), (2, (8, 8, 8), -1), (3, (24, 5, 7), 4)):
+        P = random_particles(120, seed)
+        b = (0.1, 1.9, 0.0, 2.0, -0.1, 2.1)
+        ki = kiwi.KernelIntegrator(kernel=max(k, 0))
+        res = kiwi.sph_to_grid(P, b, shape, kernel=ki, ctx=ctx)
+        dens, vx, vy, vz, _, st = oracle.sph_to_grid(P, b, shape, kernel=k, support_in_h=2.0)
+        assert_grid_match(res, dens, vx, vy, vz, label=f"seed{seed}")
+        assert res.stats["bbox_pairs"] == st.bbox_pairs
+        assert res.stats["sphere_pairs"] == st.sphere_pairs
+        assert res.stats["neg_clamped"] == st.neg_clamped
+        assert res.stats["skipped_outside"] == st.skipped_outside
+
+
+def test_deterministic_bitwise(kiwi, ctx):
+    P = random_particles(300, 9, hmin=0.02, hmax=0.5)
+    b = (0, 2, 0, 2, 0, 2)
+    r1 = kiwi.sph_to_grid(P, b, (20, 20, 20), raw=True, ctx=ctx)
+    r2 = kiwi.sph_to_grid(P, b, (20, 20, 20), raw=True, ctx=ctx)
+    assert np.array_equal(r1.raw, r2.raw) and np.array_equal(r1.density, r2.density)
+
+
+def test_edge_cases(kiwi, ctx):
+    b = (0, 1, 0, 1, 0, 1)
+    # empty snapshot
+    P0 = {k: np.zeros(0) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+    r = kiwi.sph_to_grid(P0, b, (4, 4, 4), ctx=ctx)
+    assert np.all(r.density == 0) and np.all(r.vx == 0)
+    # every particle outside the domain or with h <= 0: nothing mapped, velocities fall back to the mean
+    P = random_particles(50, 4, box=(3.0, 4.0))
+    P["h"][:10] = 0.0
+    r = kiwi.sph_to_grid(P, b, (4, 4, 4), ctx=ctx)
+    assert np.all(r.density == 0)
+    assert np.allclose(r.vx, P["vx"].mean(), rtol=1e-14, atol=1e-15)
+    assert r.stats["skipped_outside"] == 40
+    # a single particle, support far larger than the grid (every cell of a 1x1x1 grid)
+    P1 = {"x": np.array([0.5]), "y": np.array([0.5]), "z": np.array([0.5]), "vx": np.array([1.0]),
+          "vy": np.array([2.0]), "vz": np.array([3.0]), "m": np.array([2.0]), "h": np.array([10.0])}
+    r = kiwi.sph_to_grid(P1, b, (1, 1, 1), ctx=ctx)
+    assert r.density[0] > 0 and r.vx[0] == 1.0
+    # bad arguments raise, as the reference's ConfigError does
+    with pytest.raises(kiwi.KiwiError):
+        kiwi.sph_to_grid(P1, (1, 0, 0, 1, 0, 1), (4, 4, 4), ctx=ctx)
+    with pytest.raises(kiwi.KiwiError):
+        kiwi.sph_to_grid(P1, b, (0, 4, 4), ctx=ctx)
+
+
+def test_column_workload_subset_vs_oracle(kiwi, ctx, oracle):
+    """The 7,300-particle column workload on its full 100 x 100 x 410 grid: GPU vs oracle on a seeded subset
+    of particles (the oracle is single-threaded), plus linearity of the full GPU grid over a partition."""
+    from kiwi_b200.workloads import column_snapshot, subset
+    P, b = column_snapshot()
+    shape = (100, 100, 410)
+    idx = np.random.default_rng(0).choice(len(P["x"]), 6, replace=False)
+    Ps = subset(P, np.sort(idx))
+    res = kiwi.sph_to_grid(Ps, b, shape, raw=True, ctx=ctx)
+    dens, vx, vy, vz, raw, st = oracle.sph_to_grid(Ps, b, shape)
+    assert_grid_match(res, dens, vx, vy, vz, label="column subset")
+    full = kiwi.sph_to_grid(P, b, shape, raw=True, ctx=ctx)
+    half = np.arange(len(P["x"])) % 2 == 0
+    a = kiwi.sph_to_grid(subset(P, half), b, shape, raw=True, ctx=ctx)
+    c = kiwi.sph_to_grid(subset(P, ~half), b, shape, raw=True, ctx=ctx)
+    rel, low = cell_errors(a.raw[0] + c.raw[0], full.raw[0])
+    assert rel < 1e-11 and low < 1e-13, (rel, low)
