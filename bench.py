@@ -1,0 +1,329 @@
+#!/usr/bin/env python3
+"""Benchmark of the kernel-integral mapping hot path (sph-to-grid) on B200.
+
+Metric: particle-cell integrals per second -- a pair is one (particle, cell) pair whose cell's closest
+point lies within the particle's support radius (the cells that can receive mass); the bounding-box
+pair count the reference evaluates is reported beside it.
+
+Workload (one GPU): the 2,000,000-particle log-normal cube (sigma_ln rho = 1.5, P(k) ~ k^-4, 10 pc,
+domain padded by max 2h) on a 256^3 grid, cubic spline (M4) -- seeded synthetic input.  With N GPUs
+(torchrun, one process per GPU) each rank maps its own independently seeded snapshot of the same size
+(weak scaling, replicas: no data-path collective).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32_mixed] [--impl reference]
+
+One JSON line is printed by rank 0.  `value` is timed with CUDA events on the engine's stream with the
+inputs resident in HBM; `e2e` is the same metric through the public host API (pinned host arrays in,
+host arrays out, copies inside the timed region).  `cpu_baseline` / --impl reference time the
+reference's own OpenMP pair-integral loop (built from its sources into oracle/_ref) on a bounded particle
+sample of the same workload on this machine's host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic work of one evaluated (particle, cell) pair in the reference's evaluation order, measured
+# with the operation-counting oracle (`python oracle/count_work.py --workload lognormal --sample 60`):
+# 9,143 flops (+ - * / sqrt) and 435.6 transcendentals (sin cos acos atan atanh log pow).  Roofline
+# convention: a FP64 transcendental = 20 flop-equivalents.
+F_PAIR = 9143.0
+T_PAIR = 435.6
+TRANS_FLOPS = 20.0
+WORK_PER_PAIR = F_PAIR + TRANS_FLOPS * T_PAIR
+
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kiwi", choices=["kiwi", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed"])
+    ap.add_argument("--n", type=int, default=2_000_000)
+    ap.add_argument("--res", type=int, default=256)
+    ap.add_argument("--kernel", default="cubic_spline")
+    ap.add_argument("--seed", type=int, default=1002)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(n, res, seed, kernel_name):
+    from kiwi_b200.workloads import lognormal_cube
+    import kiwi_b200
+
+    hfact = kiwi_b200.get_kernel(kernel_name).hfact
+    P, bounds = lognormal_cube(n=n, seed=seed, mesh=min(res, 256), hfact=hfact)
+    return P, bounds, (res, res, res)
+
+
+def cpu_baseline(P, bounds, shape, kernel_name, target_s):
+    """The reference's own OpenMP pair loop (oracle/_ref) on a seeded particle sample sized to ~target_s."""
+    from oracle.oracle import load_ref
+
+    ref = load_ref()
+    if ref is None:
+        return None
+    threads = ref.max_threads()
+    n = len(P["x"])
+    rng = np.random.default_rng(99)
+    perm = rng.permutation(n)
+    Ps = {k: np.ascontiguousarray(v[perm]) for k, v in P.items()}
+    probe = min(n, max(64, 16 * threads))
+    t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads, p_range=(0, probe))
+    rate = probe / max(t, 1e-3)  # particles / s
+    m = int(min(n - probe, max(threads * 4, rate * target_s)))
+    t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads,
+                                       p_range=(probe, probe + m))
+    return {"value": sph / t, "unit": "pair-integrals/s", "cores": threads, "kind": "reference",
+            "sample": f"{m} of {n} particles (seeded permutation), {pairs} bounding-box / {sph} support pairs, "
+                      f"{t:.1f} s wall on {threads} OpenMP threads",
+            "bbox_pairs_per_s": pairs / t}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    P, bounds, shape = make_workload(args.n, args.res, args.seed, args.kernel)
+    from oracle.oracle import load_ref
+
+    ref = load_ref()
+    if ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkiwi_ref.so was not built"}))
+        return 0
+    threads = ref.max_threads()
+    n = len(P["x"])
+    perm = np.random.default_rng(99).permutation(n)
+    Ps = {k: np.ascontiguousarray(v[perm]) for k, v in P.items()}
+    t, _, _, _ = ref.pair_sample(Ps, bounds, shape, kernel=args.kernel, threads=threads, p_range=(0, 16 * threads))
+    per_step = int(max(threads * 4, 16 * threads / max(t, 1e-3) * 8.0))  # ~8 s of CPU work per step
+    pos = 16 * threads
+    for _ in range(args.warmup):
+        ref.pair_sample(Ps, bounds, shape, kernel=args.kernel, threads=threads, p_range=(pos, pos + per_step // 4))
+        pos += per_step // 4
+    tt, bb, ss = 0.0, 0, 0
+    for _ in range(args.steps):
+        t, b, s, _ = ref.pair_sample(Ps, bounds, shape, kernel=args.kernel, threads=threads,
+                                     p_range=(pos % n, min(n, pos % n + per_step)))
+        pos += per_step
+        tt += t
+        bb += b
+        ss += s
+    value = ss / tt
+    line = {"metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
+            "unit": "pair-integrals/s", "impl": "reference", "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"lognormal_cube n={args.n} grid={args.res}^3 kernel={args.kernel}",
+                       "sample_particles_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": "pair-integrals/s", "cores": threads, "kind": "reference",
+                             "sample": f"{per_step} particles per step of {n}; {bb} bbox / {ss} support pairs"},
+            "e2e": {"value": value, "unit": "pair-integrals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    ws, rank, local = dist_env()
+    import torch
+
+    import kiwi_b200
+
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    P, bounds, shape = make_workload(args.n, args.res, args.seed + 1000 * rank, args.kernel)
+    ki = kiwi_b200.make_kernel_integrator(args.kernel)
+    ctx = kiwi_b200.Context(dev.index)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    dP = {k: torch.from_numpy(v).to(dev) for k, v in P.items()}
+    nc = shape[0] * shape[1] * shape[2]
+    out = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, ctx=ctx)
+    peak_fp64 = kiwi_b200.measure_fp64_peak(ctx)
+
+    clocks = ClockSampler(dev.index)
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t_wall = time.perf_counter()
+    step_ms, gather_ms, sph_pairs, bbox_pairs, evaluated, launches = [], [], 0, 0, 0, 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()  # L2 flush between steps, outside the timed events
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        st = kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, ctx=ctx)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        gather_ms.append(st["gather_ms"])
+        sph_pairs += st["sphere_pairs"]
+        bbox_pairs += st["bbox_pairs"]
+        evaluated += st["evaluated_pairs"]
+        launches += st["launches"]
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+
+    tot_ms = float(np.sum(step_ms))
+    if ws > 1:
+        t = torch.tensor([tot_ms, float(sph_pairs), float(bbox_pairs)], dtype=torch.float64, device=dev)
+        tmax = t.clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        job_ms, job_pairs, job_bbox = float(tmax[0]), float(t[1]), float(t[2])
+    else:
+        job_ms, job_pairs, job_bbox = tot_ms, float(sph_pairs), float(bbox_pairs)
+    value = job_pairs / (job_ms * 1e-3)
+
+    # end to end through the public host API: pinned host arrays in, host arrays out
+    e2e = None
+    if args.e2e_steps > 0:
+        hP = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in P.items()}
+        hout = [torch.empty(nc, dtype=torch.float64).pin_memory().numpy() for _ in range(4)]
+        kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, ctx=ctx, out=hout)
+        e_ms, e_pairs = 0.0, 0
+        for _ in range(args.e2e_steps):
+            r = kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, ctx=ctx, out=hout)
+            e_ms += r.stats["total_ms"]
+            e_pairs += r.stats["sphere_pairs"]
+        e2e = {"value": e_pairs / (e_ms * 1e-3) * ws, "unit": "pair-integrals/s",
+               "h2d_bytes_per_step": int(8 * 8 * len(P["x"])), "d2h_bytes_per_step": int(4 * 8 * nc),
+               "ms_per_step": e_ms / args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(P, bounds, shape, args.kernel, args.cpu_seconds)
+
+    if rank == 0:
+        g_ms = float(np.mean(gather_ms))
+        evaluated_per_launch = evaluated / args.steps
+        achieved = evaluated_per_launch * WORK_PER_PAIR / (g_ms * 1e-3) / 1e12
+        line = {
+            "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
+            "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": job_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": f"lognormal_cube n={args.n} sigma_ln=1.5 P(k)~k^-4 10pc padded, "
+                                   f"grid {args.res}^3, kernel {args.kernel}",
+                       "precision": args.precision, "particles_per_gpu": args.n, "cells": nc,
+                       "l2": "flushed between timed steps (256 MB write) and inputs+outputs > L2",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "pairs": {"support_pairs_per_step": job_pairs / args.steps / ws,
+                      "bbox_pairs_per_step": job_bbox / args.steps / ws,
+                      "bbox_pairs_per_s": job_bbox / (job_ms * 1e-3)},
+            "roofline": {"bound": "fp64", "kernel": "k_cart_gather (FP64 cell-integral gather)",
+                         "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                         "frac": achieved / peak_fp64 if peak_fp64 else None, "traffic": None,
+                         "work_per_pair_flops": WORK_PER_PAIR,
+                         "peak_source": "measured FP64 FMA probe (kiwi_measure_fp64_peak) in this run",
+                         "gather_ms_per_launch": g_ms},
+            "clocks": clk, "gpu_launches": int(launches), "wall_s_timed_region": wall,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

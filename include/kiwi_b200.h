@@ -70,6 +70,7 @@ typedef struct KiwiStats {
     int64_t neg_warned;      /* of those, <= -0.01 (the reference prints a warning for each) */
     int64_t fp64_fallback;   /* FP32-mixed form: edges evaluated in FP64 */
     int64_t tile_pairs;      /* (tile, particle) list entries built by the binning step */
+    int64_t launches;        /* GPU kernels launched by this call */
     double gather_ms;        /* device time of the cell-integral kernel(s) of this call (CUDA events) */
     double total_ms;         /* device time of the whole call, copies included for the host variants */
 } KiwiStats;
@@ -81,6 +82,9 @@ const char* kiwi_last_error(const KiwiCtx* ctx); /* message of the last failed c
 void* kiwi_ctx_stream(KiwiCtx* ctx);             /* the context's cudaStream_t */
 int kiwi_ctx_synchronize(KiwiCtx* ctx);
 const char* kiwi_version(void);
+/* Measured FP64 FMA throughput of the context's GPU in TFLOP/s (a short probe kernel).  No counterpart in
+ * the reference: it provides the roofline denominator of the FP64 cell-integral kernels. */
+int kiwi_measure_fp64_peak(KiwiCtx* ctx, double* tflops);
 
 /* ---- kernel tables (include/kiwi/kernel_spec.hpp:18-44, src/kernel_spec_data.cpp:175-187) ----- */
 /* get_kernel(name): index 0..5 for a key or alias ("M4", "cubic_spline", "wendland_c4", ...), -1 if

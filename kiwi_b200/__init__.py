@@ -65,7 +65,7 @@ class KiwiKernelSel(C.Structure):
 class KiwiStats(C.Structure):
     _fields_ = [("bbox_pairs", C.c_int64), ("sphere_pairs", C.c_int64), ("evaluated_pairs", C.c_int64),
                 ("skipped_outside", C.c_int64), ("neg_clamped", C.c_int64), ("neg_warned", C.c_int64),
-                ("fp64_fallback", C.c_int64), ("tile_pairs", C.c_int64), ("gather_ms", C.c_double),
+                ("fp64_fallback", C.c_int64), ("tile_pairs", C.c_int64), ("launches", C.c_int64), ("gather_ms", C.c_double),
                 ("total_ms", C.c_double)]
 
     def as_dict(self):
@@ -318,18 +318,24 @@ def _particles_struct(P: dict, device: bool = False):
     return KiwiParticles(n, *ptrs), keep
 
 
-def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", raw=False, ctx=None):
+def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", raw=False, ctx=None, out=None):
     """Density and mass-weighted velocity of an SPH snapshot on a Cartesian grid -- the compute of
     run_sph_to_grid_stage (src/cartesian_grid.cpp:76-321) on host arrays.  `particles` maps x y z vx vy
     vz m h to 1-D arrays; `bounds` = (x_min, x_max, y_min, y_max, z_min, z_max); `shape` = (nx, ny, nz);
-    `kernel` a KernelIntegrator (default: cubic spline)."""
+    `kernel` a KernelIntegrator (default: cubic spline); `out`: optional preallocated float64 arrays
+    (density, vx, vy, vz), e.g. in pinned memory."""
     ctx = ctx or default_context()
     ki = kernel or KernelIntegrator()
     Ps, keep = _particles_struct(particles)
     nx, ny, nz = (int(s) for s in shape)
     grid = KiwiCartGrid((C.c_double * 6)(*[float(b) for b in bounds]), nx, ny, nz)
     nc = nx * ny * nz
-    outs = [np.empty(nc) for _ in range(4)]
+    if out is not None:
+        outs = list(out)
+        if len(outs) != 4 or any(o.dtype != np.float64 or o.size != nc or not o.flags.c_contiguous for o in outs):
+            raise KiwiError(-1, "out must be 4 contiguous float64 arrays of nx*ny*nz cells")
+    else:
+        outs = [np.empty(nc) for _ in range(4)]
     rawa = np.empty(4 * nc) if raw else None
     st = KiwiStats()
     sel = ki.sel()
@@ -363,3 +369,12 @@ def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, p
 
 def version() -> str:
     return load_library().kiwi_version().decode()
+
+
+def measure_fp64_peak(ctx=None) -> float:
+    """Measured FP64 FMA throughput (TFLOP/s) of the context's GPU."""
+    ctx = ctx or default_context()
+    v = C.c_double(0.0)
+    ctx._L.kiwi_measure_fp64_peak.argtypes = [C.c_void_p, _dp]
+    ctx.check(ctx._L.kiwi_measure_fp64_peak(ctx.handle, C.byref(v)), "fp64 peak")
+    return v.value

@@ -137,6 +137,7 @@ int check_ctx(KiwiCtx* ctx) {
 // The full device pipeline of one sph-to-grid call: mean velocity, binning, gather.
 int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
                     const CartOutputs& out_in, KiwiStats* stats) {
+    const int64_t launches0 = ctx->launches;
     DevStats* d_stats = nullptr;
     double* d_meanv = nullptr;
     KIWI_TRY(scratch_t(ctx, S_STATS, 1, &d_stats));
@@ -211,6 +212,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         stats->fp64_fallback = (int64_t)hs.fp64_fallback;
         stats->tile_pairs = total;
         stats->gather_ms = ms;
+        stats->launches = ctx->launches - launches0;
     }
     return KIWI_OK;
 }
@@ -284,6 +286,12 @@ int kiwi_ctx_synchronize(KiwiCtx* ctx) {
     KIWI_TRY(check_ctx(ctx));
     KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return KIWI_OK;
+}
+
+int kiwi_measure_fp64_peak(KiwiCtx* ctx, double* tflops) {
+    KIWI_TRY(check_ctx(ctx));
+    if (!tflops) return set_err(ctx, KIWI_ERR_ARG, "tflops is null");
+    return fp64_measure_peak(ctx, tflops);
 }
 
 int kiwi_kernel_index(const char* name) {

@@ -14,6 +14,7 @@ struct KiwiCtx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     std::string err;
+    int64_t launches = 0;  // kernels launched on this context (for the stats of a call)
     // Scratch slots: each is grown on demand and reused by later calls on this context.
     static constexpr int kSlots = 24;
     void* slot_ptr[kSlots] = {};
@@ -42,6 +43,7 @@ inline int set_err(KiwiCtx* ctx, int code, const char* fmt, ...) {
 
 #define KIWI_LAUNCHED(ctx)                                                                                \
     do {                                                                                                  \
+        ++(ctx)->launches;                                                                                \
         cudaError_t e_ = cudaGetLastError();                                                              \
         if (e_ != cudaSuccess)                                                                            \
             return ::kiwi_b200::set_err((ctx), KIWI_ERR_CUDA, "kernel launch failed: %s (%s:%d)",          \

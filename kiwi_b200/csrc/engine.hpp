@@ -47,5 +47,6 @@ int fp64_full_integral(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, 
 int fp64_face_integral(KiwiCtx* ctx, const KernelChoice& k, int64_t n, const double* particle,
                        const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert);
 int fp64_mean_velocity(KiwiCtx* ctx, const DevParticles& P, double* d_meanv);
+int fp64_measure_peak(KiwiCtx* ctx, double* tflops);
 
 }  // namespace kiwi_b200

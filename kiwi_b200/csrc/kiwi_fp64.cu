@@ -261,7 +261,39 @@ __global__ void k_mean_velocity(DevParticles P, double* __restrict__ meanv) {
     }
 }
 
+// FP64 FMA throughput probe: 8 independent fma chains per thread.
+__global__ void __launch_bounds__(256) k_dfma_peak(int iters, double seed, double* __restrict__ sink) {
+    double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+           a7 = a0 + 7;
+    const double m = 0.999999, c = 1e-7;
+    for (int i = 0; i < iters; ++i) {
+        a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+        a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+    const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 12345.678) sink[threadIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace
+
+int fp64_measure_peak(KiwiCtx* ctx, double* tflops) {
+    int sms = 0;
+    KIWI_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    double* sink = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_MISC0, 256, &sink));
+    const int blocks = sms * 8, iters = 1 << 14;
+    k_dfma_peak<<<blocks, 256, 0, ctx->stream>>>(256, 1.0, sink);  // warm-up
+    KIWI_LAUNCHED(ctx);
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    k_dfma_peak<<<blocks, 256, 0, ctx->stream>>>(iters, 1.0, sink);
+    KIWI_LAUNCHED(ctx);
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    KIWI_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * 256.0 / (ms * 1e-3) / 1e12;
+    return KIWI_OK;
+}
 
 int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
                      const TileLists& tl, const CartOutputs& out, DevStats* d_stats) {

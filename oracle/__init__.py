@@ -1,0 +1,1 @@
+"""CPU checkers of the kernel-integral path -- test infrastructure only (see oracle/oracle.py)."""

@@ -1,0 +1,98 @@
+// Operation-counting instance of the oracle -- TEST / MEASUREMENT INFRASTRUCTURE ONLY.
+//
+// oracle_core.inc compiled with R = Counted, a double that counts every arithmetic operation it takes
+// part in: each +, -, *, / and sqrt is one flop; each sin, cos, acos, atan, atanh, log and pow is one
+// transcendental (sincos counts as two).  Running it over a sample of a workload's (particle, cell)
+// pairs gives the algorithmic work per pair, F_pair (flops) and T_pair (transcendentals), of the
+// reference's evaluation order -- the numerator of the cell-integral kernel's roofline.
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../kiwi_b200/csrc/kernel_tables.h"
+
+extern "C" {
+typedef struct OrStats {
+    int64_t bbox_pairs, sphere_pairs, skipped_outside, neg_clamped, neg_warned;
+} OrStats;
+}
+
+static thread_local uint64_t g_flops = 0, g_trans = 0;
+
+struct Counted {
+    double v;
+    Counted() = default;
+    constexpr Counted(double x) : v(x) {}
+    explicit operator double() const { return v; }
+    explicit operator int() const { return (int)v; }
+};
+static inline Counted mk(double x) { return Counted(x); }
+#define BIN(op)                                                                            \
+    static inline Counted operator op(Counted a, Counted b) { ++g_flops; return mk(a.v op b.v); } \
+    static inline Counted operator op(Counted a, double b) { ++g_flops; return mk(a.v op b); }    \
+    static inline Counted operator op(double a, Counted b) { ++g_flops; return mk(a op b.v); }    \
+    static inline Counted operator op(Counted a, int b) { ++g_flops; return mk(a.v op b); }       \
+    static inline Counted operator op(int a, Counted b) { ++g_flops; return mk(a op b.v); }
+BIN(+)
+BIN(-)
+BIN(*)
+BIN(/)
+#undef BIN
+static inline Counted operator-(Counted a) { return mk(-a.v); }
+#define CMP(op)                                                                  \
+    static inline bool operator op(Counted a, Counted b) { return a.v op b.v; }  \
+    static inline bool operator op(Counted a, double b) { return a.v op b; }     \
+    static inline bool operator op(double a, Counted b) { return a op b.v; }
+CMP(<)
+CMP(>)
+CMP(<=)
+CMP(>=)
+CMP(==)
+CMP(!=)
+#undef CMP
+#define ASG(op, bop)                                                                         \
+    static inline Counted& operator op(Counted& a, Counted b) { a = a bop b; return a; }     \
+    static inline Counted& operator op(Counted& a, double b) { a = a bop b; return a; }
+ASG(+=, +)
+ASG(-=, -)
+ASG(*=, *)
+ASG(/=, /)
+#undef ASG
+
+static inline Counted c_sqrt(Counted a) { ++g_flops; return mk(sqrt(a.v)); }
+static inline Counted c_acos(Counted a) { ++g_trans; return mk(acos(a.v)); }
+static inline Counted c_atan(Counted a) { ++g_trans; return mk(atan(a.v)); }
+static inline Counted c_log(Counted a) { ++g_trans; return mk(log(a.v)); }
+static inline Counted c_sin(Counted a) { ++g_trans; return mk(sin(a.v)); }
+static inline Counted c_cos(Counted a) { ++g_trans; return mk(cos(a.v)); }
+static inline Counted c_atanh(Counted a) { ++g_trans; return mk(atanh(a.v)); }
+static inline Counted c_pow(Counted a, Counted b) { ++g_trans; return mk(pow(a.v, b.v)); }
+static inline Counted c_fabs(Counted a) { return mk(fabs(a.v)); }
+static inline Counted c_fmin(Counted a, Counted b) { return mk(fmin(a.v, b.v)); }
+static inline Counted c_floor(Counted a) { return mk(floor(a.v)); }
+static inline void c_sincos(Counted a, Counted* s, Counted* c) { g_trans += 2; s->v = sin(a.v); c->v = cos(a.v); }
+
+typedef Counted R;
+#define R_PI Counted(M_PI)
+#define Q(a, b) Counted((double)(a) / (double)(b))
+#define F_SQRT c_sqrt
+#define F_ACOS c_acos
+#define F_ATAN c_atan
+#define F_LOG c_log
+#define F_SIN c_sin
+#define F_COS c_cos
+#define F_FABS c_fabs
+#define F_ATANH c_atanh
+#define F_POW c_pow
+#define F_FMIN c_fmin
+#define F_FLOOR c_floor
+#define F_SINCOS c_sincos
+#define API(name) orc_##name
+
+extern "C" {
+#include "oracle_core.inc"
+
+void orc_reset(void) { g_flops = g_trans = 0; }
+void orc_counts(uint64_t* flops, uint64_t* trans) { *flops = g_flops; *trans = g_trans; }
+}

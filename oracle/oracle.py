@@ -14,6 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
+ORACLE_Q_SO = os.path.join(HERE, "liboracle_q.so")
 REF_SO = os.path.join(HERE, "_ref", "libkiwi_ref.so")
 
 _dp = C.POINTER(C.c_double)
@@ -36,12 +37,18 @@ class OrStats(C.Structure):
 
 
 class Oracle:
-    """The C restatement (oracle/kiwi_oracle.c)."""
+    """The C restatement (oracle/kiwi_oracle.c, FP64, bit-identical to the reference).  With quad=True the
+    same algorithm in __float128 with exact constants (oracle/kiwi_oracle_q.c): the error yardstick."""
 
-    def __init__(self, path: str = ORACLE_SO):
+    def __init__(self, path: str | None = None, quad: bool = False, prefix: str | None = None):
+        path = path or (ORACLE_Q_SO if quad else ORACLE_SO)
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
         L = self.lib = C.CDLL(path)
+        pfx = prefix or ("orq_" if quad else "or_")
+        for name in ("full_integral_new", "generic_full_integral", "gridded_integral", "face_integral",
+                     "generic_edge_breaks", "generic_vertex", "sph_to_grid", "map_voronoi"):
+            setattr(L, "or_" + name, getattr(L, pfx + name))
         L.or_full_integral_new.restype = C.c_double
         L.or_full_integral_new.argtypes = [C.c_double] * 4
         L.or_generic_full_integral.restype = C.c_double
@@ -155,6 +162,30 @@ class RefLib:
         L.ref_voronoi_copy.argtypes = [C.c_void_p, _ip, _dp, _dp, C.POINTER(C.c_long), C.POINTER(C.c_long), _dp, _ip,
                                        _ip, _dp, _dp, _dp, _dp]
         L.ref_voronoi_free.argtypes = [C.c_void_p]
+        L.ref_pair_sample.restype = C.c_double
+        L.ref_pair_sample.argtypes = ([C.c_long] + [_dp] * 5 + [_dp, C.c_int, C.c_int, C.c_int, C.c_char_p, C.c_double,
+                                                              C.c_int, C.c_int, C.c_long, C.c_long,
+                                                              C.POINTER(C.c_long), C.POINTER(C.c_long), _dp])
+        L.ref_max_threads.restype = C.c_int
+
+    def max_threads(self):
+        return self.lib.ref_max_threads()
+
+    def pair_sample(self, P, bounds, shape, kernel="cubic_spline", support_in_h=0.0, generic_path=False, threads=0,
+                    p_range=None):
+        """The reference's pair-integral loop over a particle range, OpenMP: (seconds, bbox pairs, sphere
+        pairs, checksum)."""
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "m", "h")]
+        n = len(arrs[0])
+        pb, pe = (0, n) if p_range is None else p_range
+        pairs = C.c_long(0)
+        sphere = C.c_long(0)
+        cs = C.c_double(0)
+        b = _f64(bounds)
+        t = self.lib.ref_pair_sample(n, *[_d(a) for a in arrs], _d(b), *[int(s) for s in shape], kernel.encode(),
+                                     support_in_h, int(generic_path), threads, pb, pe, C.byref(pairs), C.byref(sphere),
+                                     C.byref(cs))
+        return t, pairs.value, sphere.value, cs.value
 
     def full_integral_new(self, h, phi, r0, R0):
         return self.lib.ref_full_integral_new(h, phi, r0, R0)
@@ -217,6 +248,30 @@ class RefLib:
 
 def load_oracle():
     return Oracle()
+
+
+ORACLE_COUNT_SO = os.path.join(HERE, "liboracle_count.so")
+
+
+class CountingOracle(Oracle):
+    """The oracle over an operation-counting double (oracle/kiwi_oracle_count.cpp)."""
+
+    def __init__(self, path: str = ORACLE_COUNT_SO):
+        super().__init__(path=path, prefix="orc_")
+        self.lib.orc_counts.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+
+    def reset(self):
+        self.lib.orc_reset()
+
+    def counts(self):
+        f, t = C.c_uint64(0), C.c_uint64(0)
+        self.lib.orc_counts(C.byref(f), C.byref(t))
+        return f.value, t.value
+
+
+def load_truth():
+    """The __float128 oracle (the error yardstick)."""
+    return Oracle(quad=True)
 
 
 def load_ref():

@@ -23,6 +23,7 @@
 #include "kiwi/config.hpp"
 #include "kiwi/kernel_integral.hpp"
 #include "kiwi/kernel_integral_generic.hpp"
+#include "kiwi/kernel_integrator.hpp"
 #include "kiwi/kernel_spec.hpp"
 #include "kiwi/mapping.hpp"
 #include "kiwi/point_set.hpp"
@@ -135,6 +136,77 @@ int ref_sph_to_grid(long n, const double* x, const double* y, const double* z, c
     rm_rf(dir);
     return 0;
 }
+
+// The reference's per-(particle, cell) work of run_sph_to_grid_stage (src/cartesian_grid.cpp:188-281)
+// over the particles [p_begin, p_end), OpenMP-parallel over particles with schedule(dynamic, 256) as
+// the reference's loop is, through the KernelIntegrator the reference's make_kernel_integrator builds
+// (include/kiwi/kernel_integrator.hpp:35-45).  The six box faces are wound as src/cartesian_grid.cpp:54-72
+// winds them.  Only the per-cell accumulation differs: each thread sums m*Msum into one scalar instead
+// of a full-size grid replica, so that the time measured is that of the pair integrals.
+// Returns wall seconds; *pairs_out = bounding-box pairs evaluated, *sphere_out = those whose cell's
+// closest point lies within the support radius; *checksum = sum of m*Msum.
+double ref_pair_sample(long n, const double* x, const double* y, const double* z, const double* m, const double* h,
+                       const double bounds[6], int nx, int ny, int nz, const char* kernel, double support_in_h,
+                       int generic_path, int threads, long p_begin, long p_end, long* pairs_out, long* sphere_out,
+                       double* checksum) {
+    std::string dir = make_tmpdir();
+    kiwi::Config c = base_config(dir, bounds, kernel, support_in_h, generic_path);
+    rm_rf(dir);
+    kiwi::DensityLookupTable table;
+    const kiwi::KernelIntegrator ki = kiwi::make_kernel_integrator(c, false, &table);
+    if (threads > 0) omp_set_num_threads(threads);
+    const double dpx = (bounds[1] - bounds[0]) / nx, dpy = (bounds[3] - bounds[2]) / ny, dpz = (bounds[5] - bounds[4]) / nz;
+    const double hpx = 0.5 * dpx, hpy = 0.5 * dpy, hpz = 0.5 * dpz;
+    long pairs = 0, sphere = 0;
+    double sum = 0.0;
+    if (p_end < 0 || p_end > n) p_end = n;
+    const double t0 = omp_get_wtime();
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : pairs, sphere, sum)
+    for (long i = p_begin; i < p_end; ++i) {
+        if (h[i] <= 0.0) continue;
+        const double radius = ki.support(h[i]);
+        int ix0 = std::max(static_cast<int>(std::floor((x[i] - radius - bounds[0]) / dpx)), 0);
+        int ix1 = std::min(static_cast<int>(std::floor((x[i] + radius - bounds[0]) / dpx)), nx - 1);
+        int iy0 = std::max(static_cast<int>(std::floor((y[i] - radius - bounds[2]) / dpy)), 0);
+        int iy1 = std::min(static_cast<int>(std::floor((y[i] + radius - bounds[2]) / dpy)), ny - 1);
+        int iz0 = std::max(static_cast<int>(std::floor((z[i] - radius - bounds[4]) / dpz)), 0);
+        int iz1 = std::min(static_cast<int>(std::floor((z[i] + radius - bounds[4]) / dpz)), nz - 1);
+        for (int ix = ix0; ix <= ix1; ++ix) {
+            const double cx = bounds[0] + (ix + 0.5) * dpx;
+            for (int iy = iy0; iy <= iy1; ++iy) {
+                const double cy = bounds[2] + (iy + 0.5) * dpy;
+                for (int iz = iz0; iz <= iz1; ++iz) {
+                    const double cz = bounds[4] + (iz + 0.5) * dpz;
+                    const double xm = cx - hpx, xp = cx + hpx, ym = cy - hpy, yp = cy + hpy, zm = cz - hpz, zp = cz + hpz;
+                    std::vector<double> faces[6];
+                    faces[0] = {xp, ym, zp, xp, yp, zp, xp, yp, zm, xp, ym, zm};
+                    faces[1] = {xm, yp, zm, xm, yp, zp, xm, ym, zp, xm, ym, zm};
+                    faces[2] = {xp, yp, zm, xp, yp, zp, xm, yp, zp, xm, yp, zm};
+                    faces[3] = {xm, ym, zp, xp, ym, zp, xp, ym, zm, xm, ym, zm};
+                    faces[4] = {xm, yp, zp, xp, yp, zp, xp, ym, zp, xm, ym, zp};
+                    faces[5] = {xp, ym, zm, xp, yp, zm, xm, yp, zm, xm, ym, zm};
+                    double Msum = 0.0;
+                    for (int f = 0; f < 6; ++f) Msum += ki.face(x[i], y[i], z[i], h[i], faces[f]);
+                    if (Msum < 0.0) Msum = 0.0;
+                    sum += Msum * m[i];
+                    ++pairs;
+                    {
+                        const double ex = std::max(std::fabs(x[i] - cx) - hpx, 0.0), ey = std::max(std::fabs(y[i] - cy) - hpy, 0.0),
+                                     ez = std::max(std::fabs(z[i] - cz) - hpz, 0.0);
+                        if (ex * ex + ey * ey + ez * ez < radius * radius) ++sphere;
+                    }
+                }
+            }
+        }
+    }
+    const double t1 = omp_get_wtime();
+    if (pairs_out) *pairs_out = pairs;
+    if (sphere_out) *sphere_out = sphere;
+    if (checksum) *checksum = sum;
+    return t1 - t0;
+}
+
+int ref_max_threads() { return omp_get_max_threads(); }
 
 // ---- Voronoi --------------------------------------------------------------------------------------
 

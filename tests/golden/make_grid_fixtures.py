@@ -2,8 +2,11 @@
 """Generates the sph-to-grid golden fixtures ``grid_*.npz`` by running the reference library itself
 (oracle/_ref/libkiwi_ref.so, built from the reference sources by oracle/Makefile) on small seeded cases.
 
-Each fixture holds the particle arrays, the grid (bounds, shape), the kernel selection and the
-reference's output fields (density, vx, vy, vz) as run_sph_to_grid_stage computed them with one thread.
+Each fixture holds the particle arrays, the grid (bounds, shape), the kernel selection, the reference's
+output fields (density, vx, vy, vz) as run_sph_to_grid_stage computed them with one thread, and
+``truth_raw``: the raw per-cell sums (sum m*Msum, sum m*Msum*v) of the same algorithm evaluated in
+__float128 with exact constants (oracle/liboracle_q.so) -- the yardstick against which the reference's
+and the GPU's FP64 errors are both measured.
 Run from the repository root:  python tests/golden/make_grid_fixtures.py
 """
 import os
@@ -13,7 +16,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
-from oracle.oracle import KERNEL_NAMES, RefLib  # noqa: E402
+from oracle.oracle import KERNEL_NAMES, Oracle, RefLib  # noqa: E402
 
 RADKERN = [2.0, 2.5, 3.0, 2.0, 2.0, 2.0]
 
@@ -26,6 +29,23 @@ def particles(n, seed, lo, hi, hmin, hmax):
     P["m"] = rng.uniform(0.02, 0.08, n)
     P["h"] = rng.uniform(hmin, hmax, n)
     return P
+
+
+def _truth_part(args):
+    P, bounds, shape, kern, sup, lo, hi = args
+    q = Oracle(quad=True)
+    return q.sph_to_grid(P, bounds, shape, kernel=kern, support_in_h=sup, p_range=(lo, hi))[4]
+
+
+def truth_raw(P, bounds, shape, kern, sup, workers=8):
+    """Raw sums in __float128 (rounded once to double per particle range), split over processes."""
+    import multiprocessing as mp
+    n = len(P["x"])
+    cuts = np.linspace(0, n, workers + 1).astype(int)
+    jobs = [(P, bounds, shape, kern, sup, int(cuts[i]), int(cuts[i + 1])) for i in range(workers)]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        parts = pool.map(_truth_part, jobs)
+    return np.sum(parts, axis=0)
 
 
 def main():
@@ -53,9 +73,10 @@ def main():
     for name, P, bounds, shape, k, generic in cases:
         d, vx, vy, vz = ref.sph_to_grid(P, bounds, shape, kernel=KERNEL_NAMES[k], generic_path=generic and k == 0,
                                         threads=1)
+        tr = truth_raw(P, bounds, shape, k if (generic or k > 0) else -1, RADKERN[k])
         np.savez_compressed(os.path.join(out_dir, f"grid_{name}.npz"), **P, bounds=np.array(bounds, float),
                             shape=np.array(shape), kernel_index=k, support_in_h=RADKERN[k], generic=generic,
-                            out_density=d, out_vx=vx, out_vy=vy, out_vz=vz)
+                            out_density=d, out_vx=vx, out_vy=vy, out_vz=vz, truth_raw=tr)
         print(name, d.sum() * np.prod([(bounds[2 * i + 1] - bounds[2 * i]) / shape[i] for i in range(3)]))
 
 
