@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libkiwi_b200.so")
+LIB_PATH = os.environ.get("KIWI_B200_LIB") or os.path.join(HERE, "libkiwi_b200.so")
 
 KIWI_FP64 = 0
 KIWI_FP32_MIXED = 1

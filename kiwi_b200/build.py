@@ -43,7 +43,14 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
+def build(verbose: bool = False, force: bool = False, defines: tuple = (), out: str | None = None) -> str:
+    """Compiles the library.  `defines` (e.g. ("KIWI_GATHER_MIN_BLOCKS=1",)) and `out` build a variant
+    into its own directory (for tuning sweeps); the default is the in-tree kiwi_b200/libkiwi_b200.so."""
+    global BUILD, LIB
+    if out is not None:
+        BUILD = os.path.join(os.path.dirname(os.path.abspath(out)), "_build")
+        LIB = os.path.abspath(out)
+    extra_defs = [f"-D{d}" for d in defines]
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
     headers.append(os.path.join(HERE, "..", "include", "kiwi_b200.h"))
@@ -53,7 +60,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
         o = os.path.join(BUILD, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s, __file__] + headers):
-            cmd = [nvcc()] + ARCH + COMMON + extra + (["-Xptxas", "-v"] if verbose else []) + ["-c", s, "-o", o]
+            cmd = ([nvcc()] + ARCH + COMMON + extra + extra_defs + (["-Xptxas", "-v"] if verbose else []) +
+                   ["-c", s, "-o", o])
             if verbose:
                 print(" ".join(cmd), flush=True)
             r = subprocess.run(cmd, capture_output=True, text=True)

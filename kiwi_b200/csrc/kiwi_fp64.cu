@@ -18,8 +18,12 @@ int fp64_init_tables(KiwiCtx* ctx) {
 namespace {
 
 constexpr int kThreads = 256;
+#ifndef KIWI_GATHER_MIN_BLOCKS
+#define KIWI_GATHER_MIN_BLOCKS 2
+#endif
+constexpr int kMinBlocks = KIWI_GATHER_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 constexpr int kPMax = 32;      // particles per chunk (one warp builds a chunk)
-constexpr int kChunkCap = 1024; // (particle, cell) pairs per chunk; >= kTileCells so one particle always fits
+constexpr int kChunkCap = 2048; // (particle, cell) pairs per chunk; >= kTileCells so one particle always fits
 static_assert(kChunkCap >= kTileCells, "a single particle's tile box must fit in one chunk");
 constexpr int kCellsPerThread = kTileCells / kThreads;
 static_assert(kTileCells % kThreads == 0, "tile cells must split evenly over the threads");
@@ -51,7 +55,7 @@ __device__ __forceinline__ void add_stat(unsigned long long* dst, unsigned long 
 // chunk's values in particle order.  So every cell's sum runs over its particles in ascending order --
 // the summation order of the reference's single-threaded loop -- with no atomics.
 template <bool CUBIC>
-__global__ void __launch_bounds__(kThreads) k_cart_gather(CartGeom g, DevParticles P, int kernel,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g, DevParticles P, int kernel,
                                                           const uint32_t* __restrict__ list,
                                                           const int64_t* __restrict__ range, CartOutputs out,
                                                           DevStats* __restrict__ st) {

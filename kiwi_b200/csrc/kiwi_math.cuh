@@ -19,8 +19,10 @@
 
 #ifdef __CUDACC__
 #define KIWI_HD __host__ __device__ __forceinline__
+#define KIWI_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define KIWI_HD inline
+#define KIWI_HD_NOINLINE inline
 #endif
 
 namespace kiwi_b200 {
@@ -67,13 +69,19 @@ KIWI_HD CubicWall cubic_wall(double h, double r0) {
     return w;
 }
 
-// The I-series at one angle (src/kernel_integral.cpp:278-294 and 372-386).
+// The I-series at one angle (src/kernel_integral.cpp:278-294 and 372-386), with the sincos of the angle
+// it starts from.  This is the bulk of the transcendental work of every tier; it is kept out of line so
+// that a single copy of it serves the edge tier's two angles and the vertex tier's two vertices (inlined
+// four times per edge it overflows the instruction cache).
 struct PhiSeries {
-    double I0, I_2, I_4, I1, I_1, I_3, I_5;
+    double I0, I_2, I_4, I1, I_1, I_3, I_5, cosp;
 };
 
-KIWI_HD PhiSeries phi_series(double phi, double sinp, double cosp, double a, double a2) {
+KIWI_HD_NOINLINE PhiSeries phi_series(double phi, double a, double a2) {
     PhiSeries s;
+    double sinp, cosp;
+    sincos(phi, &sinp, &cosp);
+    s.cosp = cosp;
     const double cosp2 = cosp * cosp;
     const double mu = cosp / a / sqrt(1. + cosp2 / a2);
     const double tanp = sinp / cosp;
@@ -98,25 +106,25 @@ KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) {
     e.valid = true;
     const double h = w.h, r0 = w.r0, h2 = w.h2;
     const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    double D2 = 0.0, D3 = 0.0, sinp, cosp;
+    double D2 = 0.0, D3 = 0.0;
     const double a = R_0 / r0;
     const double a2 = a * a;
     e.a = a;
     e.a2 = a2;
     const double linedist2 = r0 * r0 + R_0 * R_0;
     if (linedist2 <= 4.0 * h2) {
-        if (linedist2 <= h2) {
-            // angle where the vertex radius reaches h
-            const double phi1 = acos(R_0 / sqrt(h * h - r0 * r0));
-            sincos(phi1, &sinp, &cosp);
-            const PhiSeries s = phi_series(phi1, sinp, cosp, a, a2);
-            D2 = -1. / 6. * s.I_2 + 0.25 * (r0 / h) * s.I_3 - 0.15 * r0h2 * s.I_4 + 1. / 30. * r0h3 * s.I_5 - 1. / 60. * r0h_3 * s.I1 + (w.B1 - w.B2) / r03 * s.I0;
+        // pass 0: the angle where the vertex radius reaches h (inner edges only) -> D2;
+        // pass 1: the angle where it reaches 2h -> D3
+#pragma unroll 1
+        for (int pass = (linedist2 <= h2) ? 0 : 1; pass < 2; ++pass) {
+            const double hh = (pass == 0) ? h * h : 4.0 * h * h;
+            const double phik = acos(R_0 / sqrt(hh - r0 * r0));
+            const PhiSeries s = phi_series(phik, a, a2);
+            if (pass == 0)
+                D2 = -1. / 6. * s.I_2 + 0.25 * (r0 / h) * s.I_3 - 0.15 * r0h2 * s.I_4 + 1. / 30. * r0h3 * s.I_5 - 1. / 60. * r0h_3 * s.I1 + (w.B1 - w.B2) / r03 * s.I0;
+            else
+                D3 = 1. / 3. * s.I_2 - 0.25 * (r0 / h) * s.I_3 + 3. / 40. * r0h2 * s.I_4 - 1. / 120. * r0h3 * s.I_5 + 4. / 15. * r0h_3 * s.I1 + (w.B2 - w.B3) / r03 * s.I0 + D2;
         }
-        // angle where the vertex radius reaches 2h
-        const double phi2 = acos(R_0 / sqrt(4.0 * h * h - r0 * r0));
-        sincos(phi2, &sinp, &cosp);
-        const PhiSeries s = phi_series(phi2, sinp, cosp, a, a2);
-        D3 = 1. / 3. * s.I_2 - 0.25 * (r0 / h) * s.I_3 + 3. / 40. * r0h2 * s.I_4 - 1. / 120. * r0h3 * s.I_5 + 4. / 15. * r0h_3 * s.I1 + (w.B2 - w.B3) / r03 * s.I0 + D2;
     }
     e.D2 = D2;
     e.D3 = D3;
@@ -127,11 +135,9 @@ KIWI_HD double cubic_vertex(const CubicWall& w, const CubicEdge& e, double phi) 
     if (!w.valid || !e.valid) return 0.0;
     if (phi == 0.0) return 0.0;
     const double r0 = w.r0, h = w.h, r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    double sinp, cosp;
-    sincos(phi, &sinp, &cosp);
-    const double R = e.R_0 / cosp;
+    const PhiSeries s = phi_series(phi, e.a, e.a2);
+    const double R = e.R_0 / s.cosp;
     const double r2 = r0 * r0 + R * R;
-    const PhiSeries s = phi_series(phi, sinp, cosp, e.a, e.a2);
     double full_int;
     if (r2 < w.h2) {
         full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
@@ -230,7 +236,7 @@ KIWI_HD int generic_imin(const GenericWall& w, int k) {
 }
 
 // G_k(phi): antiderivative of dI_P/dphi in region k (src/kernel_integral_generic.cpp:82-92).
-KIWI_HD double generic_G(const GenericWall& w, const GenericEdge& e, int k, double phi) {
+KIWI_HD_NOINLINE double generic_G(const GenericWall& w, const GenericEdge& e, int k, double phi) {
     const int imin = generic_imin(w, k);
     double I[KIWI_NI];
     generic_basis(e.a, e.a2, phi, imin, I);
@@ -403,8 +409,12 @@ KIWI_HD double face_integral(double x0, double y0, double z0, double support_rad
         min_edge_dist = dmin2(min_edge_dist, in_plane_dist);
         double M = (s1 * s2 * r0 <= 0) ? -1.0 : 1.0;
         ev.set_edge(R_0);
-        const double I1v = ev.at(phi1);
-        const double I2v = ev.at(phi2);
+        double I1v = 0.0, I2v = 0.0;
+#pragma unroll 1
+        for (int v = 0; v < 2; ++v) {
+            const double t = ev.at(v == 0 ? phi1 : phi2);
+            if (v == 0) I1v = t; else I2v = t;
+        }
         if (foot_beyond_endpoint) {
             M = (phi1 >= phi2) ? M * (I1v - I2v) : M * (I2v - I1v);
         } else {

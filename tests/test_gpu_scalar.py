@@ -16,12 +16,14 @@ def _rel(x, t):
     return np.abs(x - t) / np.maximum(np.abs(t), 1e-300)
 
 
-def assert_same_error_distribution(gpu, ref, truth, label, factor=2.0, floor=1e-15):
+def assert_same_error_distribution(gpu, ref, truth, label, min_identical=0.0, floor=1e-15):
+    """The largest error within 4x the reference's, the 99.9th percentile and the median within 2x."""
     eg, er = _rel(gpu, truth), _rel(ref, truth)
-    for q in (1.0, 0.999, 0.5):
+    for q, factor in ((1.0, 4.0), (0.999, 2.0), (0.5, 2.0)):
         g, r = np.quantile(eg, q), np.quantile(er, q)
         assert g <= factor * r + floor, f"{label}: quantile {q}: GPU {g:.3e} vs reference {r:.3e}"
-    assert np.mean(np.asarray(gpu) == np.asarray(ref)) > 0.5, f"{label}: fewer than half bit-identical"
+    same = np.mean(np.asarray(gpu) == np.asarray(ref))
+    assert same >= min_identical, f"{label}: only {same:.2f} of the values bit-identical to the reference"
 
 
 def _sample(n, seed):
@@ -40,12 +42,12 @@ def test_full_integral_cubic_and_generic(kiwi, ctx, oracle):
     g = kiwi.full_integral_new(H / 2, phi, r0, R0, ctx=ctx)
     o = np.array([oracle.full_integral_new(a, b, c, d) for a, b, c, d in zip(H / 2, phi, r0, R0)])
     t = np.array([q.full_integral_new(a, b, c, d) for a, b, c, d in zip(H / 2, phi, r0, R0)])
-    assert_same_error_distribution(g, o, t, "cubic")
+    assert_same_error_distribution(g, o, t, "cubic", min_identical=0.6)
     for k in range(6):
         gk = kiwi.generic_full_integral(kiwi.KernelSpec(k), H, phi, r0, R0, ctx=ctx)
         ok = np.array([oracle.generic_full_integral(k, a, b, c, d) for a, b, c, d in zip(H, phi, r0, R0)])
         tk = np.array([q.generic_full_integral(k, a, b, c, d) for a, b, c, d in zip(H, phi, r0, R0)])
-        assert_same_error_distribution(gk, ok, tk, f"generic kernel {k}")
+        assert_same_error_distribution(gk, ok, tk, f"generic kernel {k}", min_identical=0.5)
 
 
 def test_full_integral_guards(kiwi, ctx):
