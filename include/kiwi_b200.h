@@ -16,6 +16,7 @@
 #ifndef KIWI_B200_H
 #define KIWI_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -119,6 +120,28 @@ int kiwi_sph_to_grid(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCar
 int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                             const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy,
                             double* vz, double* raw4, KiwiStats* stats);
+
+/* Allocation-free variant of kiwi_sph_to_grid_device.  It has no counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: codes that hand all device memory to their own pool
+ * allocator (an SPH simulation mapping its particles in situ between steps, a rank with a hard memory
+ * budget) and latency-sensitive callers that cannot absorb the device-wide synchronisation a cudaMalloc
+ * or cudaFree may cause.  It allocates nothing: every scratch buffer comes from one fixed device array of
+ * KIWI_NOALLOC_SCRATCH_BYTES inside the library, which every GPU that loads the library holds until the
+ * process exits.  The caller passes the particle arrays and the output arrays, all in device memory, and
+ * the stream to run on (NULL: the legacy default stream); no KiwiCtx is needed.  It works on the current
+ * device.  Its first call on a device does a one-off set-up there (the scratch array's device address,
+ * the kernel tables, two timing events); make that first call before any stream capture.  Inputs whose
+ * scratch needs exceed the array (roughly 36 bytes per particle plus 18 bytes per (tile, particle)
+ * entry plus 16 bytes per 8x8x8-cell tile) are rejected with KIWI_ERR_LIMIT and a message in err (if
+ * err_len > 0).  Every call reuses the same array and leaves the last call's contents in it, so calls
+ * whose GPU work overlaps -- on different streams or from different host threads -- race and must be
+ * serialised by the caller.  Results equal kiwi_sph_to_grid_device's. */
+#define KIWI_NOALLOC_SCRATCH_BYTES (32u << 20)
+int kiwi_sph_to_grid_device_noalloc(void* stream, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                                    const KiwiKernelSel* kernel, int precision, double* density, double* vx,
+                                    double* vy, double* vz, double* raw4, KiwiStats* stats, char* err,
+                                    size_t err_len);
 
 /* ---- Voronoi map stage (run_mapping_stage's particle loop, src/mapping.cpp:105-206, 400-502) --- */
 /* Cell geometry in CSR form: the plain data of CellFaceGeometry (src/mapping.cpp:49-54) with vertex

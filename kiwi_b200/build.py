@@ -26,6 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("capi.cu", ["--fmad=false"]),
     ("kiwi_fp64.cu", ["--fmad=false"]),
+    ("noalloc.cu", ["--fmad=false"]),
 ]
 
 

@@ -76,6 +76,10 @@ __global__ void k_tile_ranges(const uint32_t* __restrict__ keys, int64_t total, 
     if (i == total - 1 || keys[i + 1] != k) range[2 * (int64_t)k + 1] = i + 1;
 }
 
+}  // namespace
+
+namespace kiwi_b200 {
+
 int resolve_kernel(KiwiCtx* ctx, const KiwiKernelSel* sel, KernelChoice* out) {
     const int k = sel ? sel->kernel : 0;
     if (k < 0 || k >= KIWI_NUM_KERNELS) return set_err(ctx, KIWI_ERR_ARG, "unknown kernel index %d", k);
@@ -233,7 +237,7 @@ bool particles_ok(KiwiCtx* ctx, const KiwiParticles* p, int* rc) {
     return true;
 }
 
-}  // namespace
+}  // namespace kiwi_b200
 
 extern "C" {
 

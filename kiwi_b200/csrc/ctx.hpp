@@ -19,6 +19,10 @@ struct KiwiCtx {
     static constexpr int kSlots = 24;
     void* slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
+    // Fixed arena mode (used only by the allocation-free entry point): when `arena` is set, scratch
+    // slots are carved from it instead of allocated, and a request that does not fit is an error.
+    unsigned char* arena = nullptr;
+    size_t arena_bytes = 0, arena_used = 0;
 };
 
 namespace kiwi_b200 {
@@ -59,6 +63,16 @@ inline int set_err(KiwiCtx* ctx, int code, const char* fmt, ...) {
 // Device scratch of at least `bytes` in slot `slot` (grow-only; contents are not preserved on growth).
 inline int scratch(KiwiCtx* ctx, int slot, size_t bytes, void** out) {
     if (bytes == 0) bytes = 256;
+    if (ctx->arena && ctx->slot_bytes[slot] < bytes) {
+        const size_t start = (ctx->arena_used + 255) & ~(size_t)255;
+        if (start > ctx->arena_bytes || bytes > ctx->arena_bytes - start)
+            return set_err(ctx, KIWI_ERR_LIMIT,
+                           "input too large for the fixed scratch area: it needs more than %zu bytes (%zu requested "
+                           "at offset %zu)", ctx->arena_bytes, bytes, start);
+        ctx->slot_ptr[slot] = ctx->arena + start;
+        ctx->slot_bytes[slot] = bytes;
+        ctx->arena_used = start + bytes;
+    }
     if (ctx->slot_bytes[slot] < bytes) {
         if (ctx->slot_ptr[slot]) {
             cudaStreamSynchronize(ctx->stream);

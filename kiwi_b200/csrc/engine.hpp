@@ -38,6 +38,13 @@ struct CartOutputs {
     const double* meanv;              // device, 3 doubles: mean particle velocity
 };
 
+// capi.cu: argument resolution and the device pipeline of one sph-to-grid call
+int resolve_kernel(KiwiCtx* ctx, const KiwiKernelSel* sel, KernelChoice* out);
+int make_geom(KiwiCtx* ctx, const KiwiCartGrid* grid, double support_in_h, CartGeom* g);
+bool particles_ok(KiwiCtx* ctx, const KiwiParticles* p, int* rc);
+int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
+                    const CartOutputs& out, KiwiStats* stats);
+
 // kiwi_fp64.cu
 int fp64_init_tables(KiwiCtx* ctx);
 int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
