@@ -35,12 +35,13 @@ sys.path.insert(0, ROOT)
 
 # Algorithmic work of one evaluated (particle, cell) pair in the reference's evaluation order, measured
 # with the operation-counting oracle (`python oracle/count_work.py --workload lognormal --sample 60`):
-# 9,143 flops (+ - * / sqrt) and 435.6 transcendentals (sin cos acos atan atanh log pow).  Roofline
-# convention: a FP64 transcendental = 20 flop-equivalents.
-F_PAIR = 9143.0
-T_PAIR = 435.6
+# per support pair (the cells the support reaches, evaluated by default) 10,166 flops (+ - * / sqrt) and
+# 481.9 transcendentals (sin cos acos atan atanh log pow); per bounding-box pair (every cell of the box,
+# --full-box) 9,143 flops and 435.6 transcendentals.  Roofline convention: one FP64 transcendental =
+# 20 flop-equivalents.
 TRANS_FLOPS = 20.0
-WORK_PER_PAIR = F_PAIR + TRANS_FLOPS * T_PAIR
+WORK_PER_SUPPORT_PAIR = 10166.4 + TRANS_FLOPS * 481.9
+WORK_PER_BBOX_PAIR = 9142.7 + TRANS_FLOPS * 435.6
 
 L2_BYTES = 126 * 1024 * 1024
 
@@ -52,6 +53,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kiwi", choices=["kiwi", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed"])
+    ap.add_argument("--full-box", action="store_true",
+                    help="evaluate every cell of each support bounding box, as the reference does")
     ap.add_argument("--n", type=int, default=2_000_000)
     ap.add_argument("--res", type=int, default=256)
     ap.add_argument("--kernel", default="cubic_spline")
@@ -229,7 +232,7 @@ def main():
     torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, ctx=ctx)
+        kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx)
     peak_fp64 = kiwi_b200.measure_fp64_peak(ctx)
 
     clocks = ClockSampler(dev.index)
@@ -245,7 +248,7 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        st = kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, ctx=ctx)
+        st = kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx)
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()
@@ -277,10 +280,10 @@ def main():
     if args.e2e_steps > 0:
         hP = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in P.items()}
         hout = [torch.empty(nc, dtype=torch.float64).pin_memory().numpy() for _ in range(4)]
-        kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, ctx=ctx, out=hout)
+        kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx, out=hout)
         e_ms, e_pairs = 0.0, 0
         for _ in range(args.e2e_steps):
-            r = kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, ctx=ctx, out=hout)
+            r = kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx, out=hout)
             e_ms += r.stats["total_ms"]
             e_pairs += r.stats["sphere_pairs"]
         e2e = {"value": e_pairs / (e_ms * 1e-3) * ws, "unit": "pair-integrals/s",
@@ -294,7 +297,8 @@ def main():
     if rank == 0:
         g_ms = float(np.mean(gather_ms))
         evaluated_per_launch = evaluated / args.steps
-        achieved = evaluated_per_launch * WORK_PER_PAIR / (g_ms * 1e-3) / 1e12
+        work_per_pair = WORK_PER_BBOX_PAIR if args.full_box else WORK_PER_SUPPORT_PAIR
+        achieved = evaluated_per_launch * work_per_pair / (g_ms * 1e-3) / 1e12
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -312,7 +316,7 @@ def main():
             "roofline": {"bound": "fp64", "kernel": "k_cart_gather (FP64 cell-integral gather)",
                          "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp64 if peak_fp64 else None, "traffic": None,
-                         "work_per_pair_flops": WORK_PER_PAIR,
+                         "work_per_pair_flops": work_per_pair, "evaluated_pairs_per_launch": evaluated_per_launch,
                          "peak_source": "measured FP64 FMA probe (kiwi_measure_fp64_peak) in this run",
                          "gather_ms_per_launch": g_ms},
             "clocks": clk, "gpu_launches": int(launches), "wall_s_timed_region": wall,

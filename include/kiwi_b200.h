@@ -31,9 +31,15 @@ extern "C" {
 #define KIWI_ERR_LIMIT (-5)       /* a bounded device loop hit its iteration cap */
 #define KIWI_ERR_UNSUPPORTED (-6) /* option not available in this build */
 
-/* Arithmetic forms of the cell integrals. */
+/* Arithmetic forms of the cell integrals (the low byte of a `precision` argument). */
 #define KIWI_FP64 0       /* all-FP64, the reference's arithmetic operation by operation */
 #define KIWI_FP32_MIXED 1 /* FP32 bulk with FP64 islands and FP64 per-cell totals */
+#define KIWI_FORM_MASK 0xff
+/* Flag: evaluate every cell of each particle's support bounding box, as the reference does
+ * (src/cartesian_grid.cpp:213-243).  Without it only cells whose closest point lies within the support
+ * radius are evaluated; the others hold no kernel mass and the reference's values for them are
+ * rounding noise around zero (clamped at 0). */
+#define KIWI_FULL_BOX 0x100
 
 typedef struct KiwiCtx KiwiCtx;
 

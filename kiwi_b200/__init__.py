@@ -318,7 +318,19 @@ def _particles_struct(P: dict, device: bool = False):
     return KiwiParticles(n, *ptrs), keep
 
 
-def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", raw=False, ctx=None, out=None):
+KIWI_FULL_BOX = 0x100
+
+
+def precision_code(precision="fp64", full_box=False) -> int:
+    """The C ABI's precision argument: the arithmetic form, plus KIWI_FULL_BOX to evaluate every cell of
+    each particle's support bounding box as the reference does (default: only the cells the support
+    reaches)."""
+    code = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    return code | (KIWI_FULL_BOX if full_box else 0)
+
+
+def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", raw=False, ctx=None, out=None,
+                full_box=False):
     """Density and mass-weighted velocity of an SPH snapshot on a Cartesian grid -- the compute of
     run_sph_to_grid_stage (src/cartesian_grid.cpp:76-321) on host arrays.  `particles` maps x y z vx vy
     vz m h to 1-D arrays; `bounds` = (x_min, x_max, y_min, y_max, z_min, z_max); `shape` = (nx, ny, nz);
@@ -340,13 +352,14 @@ def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", r
     st = KiwiStats()
     sel = ki.sel()
     ctx.check(ctx._L.kiwi_sph_to_grid(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
-                                      PRECISIONS.get(precision, precision), *[_p(o) for o in outs], _p(rawa),
+                                      precision_code(precision, full_box), *[_p(o) for o in outs], _p(rawa),
                                       C.byref(st)), "sph-to-grid")
     return CartesianGridResult(nx, ny, nz, tuple(bounds), *outs, raw=rawa.reshape(4, nc) if raw else None,
                                stats=st.as_dict())
 
 
-def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, precision="fp64", ctx=None):
+def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, precision="fp64", ctx=None,
+                       full_box=False):
     """Device variant: `particles` and `out` (density, vx, vy, vz[, raw4]) hold CUDA tensors (float64,
     contiguous).  Runs on the context's stream and returns the call's stats."""
     ctx = ctx or default_context()
@@ -361,7 +374,7 @@ def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, p
         return C.cast(C.c_void_p(int(t.data_ptr())), _dp) if t is not None else None
 
     ctx.check(ctx._L.kiwi_sph_to_grid_device(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
-                                             PRECISIONS.get(precision, precision), dp(out.get("density")),
+                                             precision_code(precision, full_box), dp(out.get("density")),
                                              dp(out.get("vx")), dp(out.get("vy")), dp(out.get("vz")),
                                              dp(out.get("raw4")), C.byref(st)), "sph-to-grid")
     return st.as_dict()

@@ -54,15 +54,37 @@ __device__ __forceinline__ void add_stat(unsigned long long* dst, unsigned long 
 // chunk's (particle, cell) pairs into shared memory, then each thread adds, for the cells it owns, the
 // chunk's values in particle order.  So every cell's sum runs over its particles in ascending order --
 // the summation order of the reference's single-threaded loop -- with no atomics.
-template <bool CUBIC>
+// Chunk pair k -> (chunk particle j, global cell ix, iy, iz): j is the last particle whose pair range
+// starts at or before k; the cell runs z fastest within the particle's box inside the tile.
+__device__ __forceinline__ void decode_pair(int k, int np, const int* s_start, const int (*s_lo)[3],
+                                            const int (*s_dim)[3], int bx, int by, int bz, int& j, int& ix, int& iy,
+                                            int& iz) {
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_start[mid] <= k) lo = mid; else hi = mid - 1;
+    }
+    j = lo;
+    const int q = k - s_start[j];
+    const int dz = s_dim[j][2], dy = s_dim[j][1];
+    const int qz = q % dz, qr = q / dz, qy = qr % dy, qx = qr / dy;
+    ix = bx + s_lo[j][0] + qx;
+    iy = by + s_lo[j][1] + qy;
+    iz = bz + s_lo[j][2] + qz;
+}
+
+template <bool CUBIC, bool CULL>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g, DevParticles P, int kernel,
                                                           const uint32_t* __restrict__ list,
                                                           const int64_t* __restrict__ range, CartOutputs out,
                                                           DevStats* __restrict__ st) {
+    static_assert(kChunkCap / kThreads <= 32, "per-thread keep mask is 32 bits");
     __shared__ double s_x[kPMax], s_y[kPMax], s_z[kPMax], s_h[kPMax], s_m[kPMax], s_vx[kPMax], s_vy[kPMax],
         s_vz[kPMax];
     __shared__ int s_lo[kPMax][3], s_dim[kPMax][3], s_start[kPMax];
     __shared__ int s_np, s_total;
+    __shared__ int s_wsum[kThreads / 32];
+    __shared__ unsigned short s_list[kChunkCap];
     __shared__ double s_R[kChunkCap];
 
     const int64_t t = blockIdx.x;
@@ -74,7 +96,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
 #pragma unroll
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
 
-    unsigned long long n_bbox = 0, n_sphere = 0, n_neg = 0, n_warn = 0;
+    unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
     const int64_t beg = range[2 * t], end = range[2 * t + 1];
     const double sup_in_h = g.support_in_h;
 
@@ -120,28 +142,55 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
         __syncthreads();
         const int np = s_np, total = s_total;
 
-        for (int k = threadIdx.x; k < total; k += kThreads) {
-            int lo = 0, hi = np - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (s_start[mid] <= k) lo = mid; else hi = mid - 1;
-            }
-            const int j = lo;
-            const int q = k - s_start[j];
-            const int dz = s_dim[j][2], dy = s_dim[j][1];
-            const int qz = q % dz, qr = q / dz, qy = qr % dy, qx = qr / dy;
-            const int ix = bx + s_lo[j][0] + qx, iy = by + s_lo[j][1] + qy, iz = bz + s_lo[j][2] + qz;
+        // Pass 1: which of the chunk's box pairs are evaluated.  With culling, only cells whose closest
+        // point lies within the support radius (the cells that can hold mass; the reference's other
+        // bounding-box cells evaluate to rounding noise around zero); the rest get 0.
+        unsigned keep = 0;
+#pragma unroll
+        for (int i = 0; i < kChunkCap / kThreads; ++i) {
+            const int k = threadIdx.x + i * kThreads;
+            if (k >= total) break;
+            int j, ix, iy, iz;
+            decode_pair(k, np, s_start, s_lo, s_dim, bx, by, bz, j, ix, iy, iz);
+            const double radius = mul_rn(sup_in_h, s_h[j]);
+            const double ex = fmax(fabs(s_x[j] - cell_centre(g.x_min, ix, g.dpx)) - g.hpx, 0.0);
+            const double ey = fmax(fabs(s_y[j] - cell_centre(g.y_min, iy, g.dpy)) - g.hpy, 0.0);
+            const double ez = fmax(fabs(s_z[j] - cell_centre(g.z_min, iz, g.dpz)) - g.hpz, 0.0);
+            const bool in = ex * ex + ey * ey + ez * ez < radius * radius;
+            ++n_bbox;
+            n_sphere += in;
+            if (!CULL || in) keep |= 1u << i;
+            else s_R[k] = 0.0;
+        }
+        // compact the kept pairs into s_list (block-wide exclusive scan of the per-thread counts)
+        const int nkeep = __popc(keep);
+        int incl = nkeep;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_wsum[warp] = incl;
+        __syncthreads();
+        int base = incl - nkeep;
+        for (int w = 0; w < warp; ++w) base += s_wsum[w];
+        int m_total = 0;
+        for (int w = 0; w < kThreads / 32; ++w) m_total += s_wsum[w];
+#pragma unroll
+        for (int i = 0; i < kChunkCap / kThreads; ++i)
+            if (keep & (1u << i)) s_list[base++] = (unsigned short)(threadIdx.x + i * kThreads);
+        __syncthreads();
+
+        // Pass 2: the cell integrals of the kept pairs.
+        for (int li = threadIdx.x; li < m_total; li += kThreads) {
+            const int k = s_list[li];
+            int j, ix, iy, iz;
+            decode_pair(k, np, s_start, s_lo, s_dim, bx, by, bz, j, ix, iy, iz);
             const double x0 = s_x[j], y0 = s_y[j], z0 = s_z[j], h = s_h[j];
             const double radius = mul_rn(sup_in_h, h);
             const double cx = cell_centre(g.x_min, ix, g.dpx);
             const double cy = cell_centre(g.y_min, iy, g.dpy);
             const double cz = cell_centre(g.z_min, iz, g.dpz);
-            ++n_bbox;
-            {
-                const double ex = fmax(fabs(x0 - cx) - g.hpx, 0.0), ey = fmax(fabs(y0 - cy) - g.hpy, 0.0),
-                             ez = fmax(fabs(z0 - cz) - g.hpz, 0.0);
-                if (ex * ex + ey * ey + ez * ez < radius * radius) ++n_sphere;
-            }
+            ++n_eval;
             double msum = pair_msum<CUBIC>(kernel, x0, y0, z0, h, CUBIC ? 2 * h : radius, cx, cy, cz, g.hpx, g.hpy,
                                            g.hpz);
             if (msum < 0.0) {
@@ -197,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
     }
     add_stat(&st->bbox_pairs, n_bbox);
     add_stat(&st->sphere_pairs, n_sphere);
-    add_stat(&st->evaluated_pairs, n_bbox);
+    add_stat(&st->evaluated_pairs, n_eval);
     add_stat(&st->neg_clamped, n_neg);
     add_stat(&st->neg_warned, n_warn);
 }
@@ -300,15 +349,18 @@ int fp64_measure_peak(KiwiCtx* ctx, double* tflops) {
 }
 
 int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
-                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats) {
+                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box) {
     if (tl.ntiles <= 0) return KIWI_OK;
     if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
-    if (k.cubic)
-        k_cart_gather<true><<<(unsigned)tl.ntiles, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out,
-                                                                              d_stats);
+    const dim3 grid((unsigned)tl.ntiles);
+    if (k.cubic && !full_box)
+        k_cart_gather<true, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+    else if (k.cubic)
+        k_cart_gather<true, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+    else if (!full_box)
+        k_cart_gather<false, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
     else
-        k_cart_gather<false><<<(unsigned)tl.ntiles, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out,
-                                                                               d_stats);
+        k_cart_gather<false, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

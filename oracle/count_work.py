@@ -36,13 +36,16 @@ def main():
     idx = np.sort(np.random.default_rng(7).choice(len(P["x"]), a.sample, replace=False))
     Ps = subset(P, idx)
     co = CountingOracle()
-    co.reset()
     sup = [2.0, 2.5, 3.0, 2.0, 2.0, 2.0][max(a.kernel, 0)]
-    st = co.sph_to_grid(Ps, b, shape, kernel=a.kernel, support_in_h=sup)[5]
-    f, t = co.counts()
-    out = {"workload": a.workload, "kernel": a.kernel, "sample_particles": a.sample, "bbox_pairs": st.bbox_pairs,
-           "sphere_pairs": st.sphere_pairs, "flops": f, "transcendentals": t,
-           "F_pair_bbox": f / st.bbox_pairs, "T_pair_bbox": t / st.bbox_pairs}
+    out = {"workload": a.workload, "kernel": a.kernel, "sample_particles": a.sample}
+    for label, only in (("bbox", 0), ("support", 1)):
+        co.lib.orc_set_support_cells_only(only)
+        co.reset()
+        st = co.sph_to_grid(Ps, b, shape, kernel=a.kernel, support_in_h=sup)[5]
+        f, t = co.counts()
+        n = st.sphere_pairs if only else st.bbox_pairs
+        out.update({f"{label}_pairs": n, f"F_pair_{label}": f / n, f"T_pair_{label}": t / n})
+    co.lib.orc_set_support_cells_only(0)
     print(json.dumps(out))
 
 

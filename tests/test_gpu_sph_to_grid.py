@@ -38,10 +38,12 @@ def _vol(d):
     return np.prod([(b[2 * i + 1] - b[2 * i]) / s[i] for i in range(3)])
 
 
+@pytest.mark.parametrize("full_box", [False, True], ids=["support_cells", "full_box"])
 @pytest.mark.parametrize("fn", GOLDEN, ids=[os.path.basename(f)[5:-4] for f in GOLDEN])
-def test_matches_reference_fixture(kiwi, ctx, fn):
+def test_matches_reference_fixture(kiwi, ctx, fn, full_box):
     d, P = _load(fn)
-    res = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=_integrator(kiwi, d), raw=True, ctx=ctx)
+    res = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=_integrator(kiwi, d), raw=True, ctx=ctx,
+                           full_box=full_box)
     tr = d["truth_raw"]
     truth_density = tr[0] / _vol(d)
     assert_within_envelope(res.density, d["out_density"], truth_density, label=os.path.basename(fn))
