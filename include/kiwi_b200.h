@@ -31,9 +31,17 @@ extern "C" {
 #define KIWI_ERR_LIMIT (-5)       /* a bounded device loop hit its iteration cap */
 #define KIWI_ERR_UNSUPPORTED (-6) /* option not available in this build */
 
-/* Arithmetic forms of the cell integrals (the low byte of a `precision` argument). */
-#define KIWI_FP64 0       /* all-FP64, the reference's arithmetic operation by operation */
-#define KIWI_FP32_MIXED 1 /* FP32 bulk with FP64 islands and FP64 per-cell totals */
+/* Arithmetic forms of the cell integrals (the low byte of a `precision` argument).
+ * KIWI_FP64: all FP64.  For the cubic closed form the vertex-pyramid tiers are shared between the cells
+ * of a particle's box (each edge tier once per plane and edge line, each vertex pyramid once per lattice
+ * point), which is algebraically the reference's per-cell sum; for the generic kernels it is the
+ * reference's per-cell evaluation order.
+ * KIWI_FP64_REFERENCE_ORDER: all FP64 in the reference's per-cell evaluation order, operation by
+ * operation (6 faces x 4 edges x 2 vertices per cell, src/kernel_integral.cpp:471-647).
+ * KIWI_FP32_MIXED: FP32 bulk with FP64 islands and FP64 per-cell totals. */
+#define KIWI_FP64 0
+#define KIWI_FP32_MIXED 1
+#define KIWI_FP64_REFERENCE_ORDER 2
 #define KIWI_FORM_MASK 0xff
 /* Flag: evaluate every cell of each particle's support bounding box, as the reference does
  * (src/cartesian_grid.cpp:213-243).  Without it only cells whose closest point lies within the support

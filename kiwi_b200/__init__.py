@@ -27,7 +27,8 @@ LIB_PATH = os.environ.get("KIWI_B200_LIB") or os.path.join(HERE, "libkiwi_b200.s
 
 KIWI_FP64 = 0
 KIWI_FP32_MIXED = 1
-PRECISIONS = {"fp64": KIWI_FP64, "fp32_mixed": KIWI_FP32_MIXED}
+KIWI_FP64_REFERENCE_ORDER = 2
+PRECISIONS = {"fp64": KIWI_FP64, "fp32_mixed": KIWI_FP32_MIXED, "fp64_reference_order": KIWI_FP64_REFERENCE_ORDER}
 
 KERNEL_KEYS = ["M4", "M5", "M6", "WC2", "WC4", "WC6"]
 KERNEL_NAMES = ["cubic_spline", "quartic_spline", "quintic_spline", "wendland_c2", "wendland_c4", "wendland_c6"]

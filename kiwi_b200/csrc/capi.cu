@@ -196,8 +196,8 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     const int form = precision & KIWI_FORM_MASK;
     const bool full_box = (precision & KIWI_FULL_BOX) != 0;
-    if (form == KIWI_FP64) {
-        KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl, out, d_stats, full_box));
+    if (form == KIWI_FP64 || form == KIWI_FP64_REFERENCE_ORDER) {
+        KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl, out, d_stats, full_box, form == KIWI_FP64_REFERENCE_ORDER));
     } else {
         return set_err(ctx, KIWI_ERR_UNSUPPORTED, "precision %d is not available in this build", precision);
     }

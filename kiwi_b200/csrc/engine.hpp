@@ -48,7 +48,8 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
 // kiwi_fp64.cu
 int fp64_init_tables(KiwiCtx* ctx);
 int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
-                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box);
+                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box,
+                     bool reference_order);
 int fp64_full_integral(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi, const double* r0,
                        const double* R0, double* out);
 int fp64_face_integral(KiwiCtx* ctx, const KernelChoice& k, int64_t n, const double* particle,

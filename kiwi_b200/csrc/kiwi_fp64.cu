@@ -5,6 +5,7 @@
 
 #include "engine.hpp"
 #include "kiwi_math.cuh"
+#include "lattice.cuh"
 
 namespace kiwi_b200 {
 
@@ -251,6 +252,246 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
     add_stat(&st->neg_warned, n_warn);
 }
 
+// ------------------------------------------------------------------ lattice-factorised gather (cubic)
+
+constexpr int kLatMinBlocks = 2;
+constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
+
+// Position of the smallest j with s_off[j] <= it among the chunk's np particles (s_off ascending).
+__device__ __forceinline__ int chunk_search(const int* s_off, int np, int it) {
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
+// the edge and corner tables in shared memory.  Per chunk: (A) the edge tiers of every (plane, edge
+// line) of every particle's box, (B) the corner values of every (plane, lattice point), (C) each thread
+// assembles the cells it owns from the corner values, particle by particle in list order, and adds them
+// to its accumulators -- the same fixed per-cell summation order as k_cart_gather, no atomics.
+template <bool CULL>
+__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGeom g, DevParticles P,
+                                                                          const uint32_t* __restrict__ list,
+                                                                          const int64_t* __restrict__ range,
+                                                                          CartOutputs out, DevStats* __restrict__ st) {
+    __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
+        s_vy[kLatPMax], s_vz[kLatPMax];
+    __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
+    __shared__ int s_np, s_etot, s_stot;
+    extern __shared__ double s_dyn[];
+    double* s_D2 = s_dyn;
+    double* s_D3 = s_dyn + kLatECap;
+    double* s_S = s_dyn + 2 * kLatECap;
+
+    const int64_t t = blockIdx.x;
+    const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
+    const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    double acc[kCellsPerThread][4];
+#pragma unroll
+    for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
+    unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
+    const int64_t beg = range[2 * t], end = range[2 * t + 1];
+
+    for (int64_t pos = beg; pos < end;) {
+        if (warp == 0) {
+            const int64_t idx = pos + lane;
+            int ne = 0, ns = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+            double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
+            if (idx < end) {
+                const uint32_t p = list[idx];
+                px = P.x[p]; py = P.y[p]; pz = P.z[p]; ph = P.h[p];
+                pm = P.m[p]; pvx = P.vx[p]; pvy = P.vy[p]; pvz = P.vz[p];
+                CellBox b;
+                bool outside;
+                particle_cell_box(g, px, py, pz, ph, b, &outside);
+                lo0 = max(b.x0, bx); lo1 = max(b.y0, by); lo2 = max(b.z0, bz);
+                d0 = min(b.x1, bx + kTileX - 1) - lo0 + 1;
+                d1 = min(b.y1, by + kTileY - 1) - lo1 + 1;
+                d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
+                const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
+                ne = 2 * (n0 * n1 + n0 * n2 + n1 * n2);
+                ns = 3 * n0 * n1 * n2;
+            }
+            int ie = ne, is = ns;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vs = __shfl_up_sync(0xffffffffu, is, o);
+                if (lane >= o) {
+                    ie += ve;
+                    is += vs;
+                }
+            }
+            const bool take = (idx < end) && ie <= kLatECap && is <= kLatSCap;
+            const int np = __popc(__ballot_sync(0xffffffffu, take));
+            if (take) {
+                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph;
+                s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
+                s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
+                s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
+                s_eoff[lane] = ie - ne;
+                s_soff[lane] = is - ns;
+            }
+            if (lane == np - 1) {
+                s_np = np;
+                s_etot = ie;
+                s_stot = is;
+            }
+        }
+        __syncthreads();
+        const int np = s_np, etot = s_etot, stot = s_stot;
+
+        // (A) edge tiers: block (a, b) holds r0 along axis a, R_0 along axis b
+        for (int it = threadIdx.x; it < etot; it += kThreads) {
+            const int j = chunk_search(s_eoff, np, it);
+            int e = it - s_eoff[j];
+            const int n[3] = {s_dim[j][0] + 1, s_dim[j][1] + 1, s_dim[j][2] + 1};
+            // blocks in order xy, xz, yx, yz, zx, zy
+            int a = 0, bax = 1;
+            {
+                const int sz[6] = {n[0] * n[1], n[0] * n[2], n[1] * n[0], n[1] * n[2], n[2] * n[0], n[2] * n[1]};
+                const int aa[6] = {0, 0, 1, 1, 2, 2}, bb[6] = {1, 2, 0, 2, 0, 1};
+                int blk = 0;
+                while (e >= sz[blk]) {
+                    e -= sz[blk];
+                    ++blk;
+                }
+                a = aa[blk];
+                bax = bb[blk];
+            }
+            const int p = e / n[bax], q = e % n[bax];
+            const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
+            const double pc[3] = {s_x[j], s_y[j], s_z[j]};
+            const double r0 = fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
+            const double R0 = fabs(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]));
+            const CubicWall w = cubic_wall(s_h[j], r0);
+            const CubicEdge ed = cubic_edge(w, R0);
+            s_D2[it] = ed.D2;
+            s_D3[it] = ed.D3;
+        }
+        __syncthreads();
+
+        // (B) corner values S_a(i, j, k) for the three plane orientations a
+        for (int it = threadIdx.x; it < stot; it += kThreads) {
+            const int jp = chunk_search(s_soff, np, it);
+            const int s = it - s_soff[jp];
+            const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+            const int L = n0 * n1 * n2;
+            const int axis = s / L, rem = s % L;
+            const int i = rem / (n1 * n2), jj = (rem / n2) % n1, k = rem % n2;
+            const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
+            const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
+            const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+            const int eb = s_eoff[jp];
+            const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
+            double r0, u1, u2;
+            int e1, e2;
+            if (axis == 0) {  // plane x = X_i, corner (y, z)
+                r0 = fabs(ux); u1 = uy; u2 = uz;
+                e1 = eb + i * n1 + jj;                    // xy[i][jj]
+                e2 = eb + nxy + i * n2 + k;               // xz[i][k]
+            } else if (axis == 1) {  // plane y = Y_jj, corner (x, z)
+                r0 = fabs(uy); u1 = ux; u2 = uz;
+                e1 = eb + nxy + nxz + jj * n0 + i;        // yx[jj][i]
+                e2 = eb + 2 * nxy + nxz + jj * n2 + k;    // yz[jj][k]
+            } else {  // plane z = Z_k, corner (x, y)
+                r0 = fabs(uz); u1 = ux; u2 = uy;
+                e1 = eb + 2 * nxy + nxz + nyz + k * n0 + i;       // zx[k][i]
+                e2 = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;  // zy[k][jj]
+            }
+            double f = 0.0;
+            const double sg = sgn(u1) * sgn(u2);
+            if (sg != 0.0 && r0 != 0.0) {
+                const double a1 = fabs(u1), a2 = fabs(u2);
+                f = lattice_vertex(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1]) +
+                    lattice_vertex(s_h[jp], r0, a2, a1, s_D2[e2], s_D3[e2]);
+            }
+            s_S[it] = sg * f;
+        }
+        __syncthreads();
+
+        // (C) cells: 6 faces x inclusion-exclusion over 4 corners, in particle order
+#pragma unroll
+        for (int c = 0; c < kCellsPerThread; ++c) {
+            const int li = threadIdx.x + c * kThreads;
+            const int gz = bz + li % kTileZ, gy = by + (li / kTileZ) % kTileY, gx = bx + li / (kTileZ * kTileY);
+            for (int j = 0; j < np; ++j) {
+                const int i = gx - s_lo[j][0], jj = gy - s_lo[j][1], k = gz - s_lo[j][2];
+                if (i < 0 || jj < 0 || k < 0 || i >= s_dim[j][0] || jj >= s_dim[j][1] || k >= s_dim[j][2]) continue;
+                ++n_bbox;
+                const double x0 = s_x[j], y0 = s_y[j], z0 = s_z[j];
+                const double radius = mul_rn(g.support_in_h, s_h[j]);
+                const double ex = fmax(fabs(x0 - cell_centre(g.x_min, gx, g.dpx)) - g.hpx, 0.0);
+                const double ey = fmax(fabs(y0 - cell_centre(g.y_min, gy, g.dpy)) - g.hpy, 0.0);
+                const double ez = fmax(fabs(z0 - cell_centre(g.z_min, gz, g.dpz)) - g.hpz, 0.0);
+                const bool in = ex * ex + ey * ey + ez * ez < radius * radius;
+                n_sphere += in;
+                if (CULL && !in) continue;
+                ++n_eval;
+                const int n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
+                const int L = (s_dim[j][0] + 1) * n1 * n2;
+                const double* Sx = s_S + s_soff[j];
+                const double* Sy = Sx + L;
+                const double* Sz = Sy + L;
+                auto at = [&](const double* S, int a, int b, int cc) { return S[(a * n1 + b) * n2 + cc]; };
+                const double sx1 = sgn(lattice_offset(g.x_min, g.dpx, gx + 1, x0)), sx0 = sgn(lattice_offset(g.x_min, g.dpx, gx, x0));
+                const double sy1 = sgn(lattice_offset(g.y_min, g.dpy, gy + 1, y0)), sy0 = sgn(lattice_offset(g.y_min, g.dpy, gy, y0));
+                const double sz1 = sgn(lattice_offset(g.z_min, g.dpz, gz + 1, z0)), sz0 = sgn(lattice_offset(g.z_min, g.dpz, gz, z0));
+                double msum = 0.0;
+                msum += sx1 * (at(Sx, i + 1, jj + 1, k + 1) - at(Sx, i + 1, jj, k + 1) - at(Sx, i + 1, jj + 1, k) + at(Sx, i + 1, jj, k));
+                msum -= sx0 * (at(Sx, i, jj + 1, k + 1) - at(Sx, i, jj, k + 1) - at(Sx, i, jj + 1, k) + at(Sx, i, jj, k));
+                msum += sy1 * (at(Sy, i + 1, jj + 1, k + 1) - at(Sy, i, jj + 1, k + 1) - at(Sy, i + 1, jj + 1, k) + at(Sy, i, jj + 1, k));
+                msum -= sy0 * (at(Sy, i + 1, jj, k + 1) - at(Sy, i, jj, k + 1) - at(Sy, i + 1, jj, k) + at(Sy, i, jj, k));
+                msum += sz1 * (at(Sz, i + 1, jj + 1, k + 1) - at(Sz, i, jj + 1, k + 1) - at(Sz, i + 1, jj, k + 1) + at(Sz, i, jj, k + 1));
+                msum -= sz0 * (at(Sz, i + 1, jj + 1, k) - at(Sz, i, jj + 1, k) - at(Sz, i + 1, jj, k) + at(Sz, i, jj, k));
+                if (msum < 0.0) {
+                    ++n_neg;
+                    if (msum <= -0.01) ++n_warn;
+                    msum = 0.0;
+                }
+                if (msum == 0.0) continue;
+                const double mm = msum * s_m[j];
+                acc[c][0] += mm;
+                acc[c][1] += mm * s_vx[j];
+                acc[c][2] += mm * s_vy[j];
+                acc[c][3] += mm * s_vz[j];
+            }
+        }
+        __syncthreads();
+        pos += np;
+    }
+
+    const double mvx = out.meanv[0], mvy = out.meanv[1], mvz = out.meanv[2];
+    const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+#pragma unroll
+    for (int c = 0; c < kCellsPerThread; ++c) {
+        const int li = threadIdx.x + c * kThreads;
+        const int ix = bx + li / (kTileZ * kTileY), iy = by + (li / kTileZ) % kTileY, iz = bz + li % kTileZ;
+        if (ix >= g.nx || iy >= g.ny || iz >= g.nz) continue;
+        const int64_t i3 = ((int64_t)ix * g.ny + iy) * g.nz + iz;
+        const double M = acc[c][0];
+        if (out.density) out.density[i3] = M / g.cell_volume;
+        const bool has = M > 0.0;
+        if (out.vx) out.vx[i3] = has ? acc[c][1] / M : mvx;
+        if (out.vy) out.vy[i3] = has ? acc[c][2] / M : mvy;
+        if (out.vz) out.vz[i3] = has ? acc[c][3] / M : mvz;
+        if (out.raw4) {
+            out.raw4[i3] = M;
+            out.raw4[ncell + i3] = acc[c][1];
+            out.raw4[2 * ncell + i3] = acc[c][2];
+            out.raw4[3 * ncell + i3] = acc[c][3];
+        }
+    }
+    add_stat(&st->bbox_pairs, n_bbox);
+    add_stat(&st->sphere_pairs, n_sphere);
+    add_stat(&st->evaluated_pairs, n_eval);
+    add_stat(&st->neg_clamped, n_neg);
+    add_stat(&st->neg_warned, n_warn);
+}
+
 __global__ void k_full_integral(int kernel, int64_t n, const double* __restrict__ arg0, const double* __restrict__ phi,
                                 const double* __restrict__ r0, const double* __restrict__ R0, double* __restrict__ out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -349,11 +590,22 @@ int fp64_measure_peak(KiwiCtx* ctx, double* tflops) {
 }
 
 int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
-                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box) {
+                     const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box,
+                     bool reference_order) {
     if (tl.ntiles <= 0) return KIWI_OK;
     if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
     const dim3 grid((unsigned)tl.ntiles);
-    if (k.cubic && !full_box)
+    if (k.cubic && !reference_order) {
+        if (full_box) {
+            KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)kLatDynSmem));
+            k_cart_lattice<false><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, out, d_stats);
+        } else {
+            KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)kLatDynSmem));
+            k_cart_lattice<true><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, out, d_stats);
+        }
+    } else if (k.cubic && !full_box)
         k_cart_gather<true, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
     else if (k.cubic)
         k_cart_gather<true, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);

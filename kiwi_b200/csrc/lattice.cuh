@@ -1,0 +1,82 @@
+// Lattice-factorised cell integrals for box cells (cubic spline closed form).
+//
+// The reference evaluates each (particle, cell) pair as 6 faces x 4 edges x 2 vertex pyramids
+// (src/kernel_integral.cpp:471-647, src/cartesian_grid.cpp:246-259).  For axis-aligned cells every one of
+// those vertex pyramids is determined by three lattice distances: the wall distance r0 = |X_p - x0| of
+// the face's plane, the in-plane distance R_0 = |Y_q - y0| from the particle's projection to the edge's
+// line, and the offset t = |Z_r - z0| of the vertex along the edge.  So neighbouring cells share them,
+// and a particle's whole box of cells needs only
+//   - one edge tier (D2, D3: src/kernel_integral.cpp:253-350) per (plane, edge line): 6 (n+1)^2 for an
+//     n^3 box, and
+//   - one "corner" value per (plane, lattice point): S(p, q, r) = sgn(u) sgn(v) [I(r0, |u|, |v|) +
+//     I(r0, |v|, |u|)], the cone mass of the rectangle spanned by the projection and the corner (two
+//     right-triangle vertex pyramids, src/kernel_integral.cpp:356-400), u and v the corner's in-plane
+//     offsets: 3 (n+1)^3;
+// after which a cell is 24 signed lookups: its mass is sum over its 6 faces of (outward-normal side sign)
+// x (inclusion-exclusion of S over the face's 4 corners).  This is algebraically the reference's sum --
+// the same 48 vertex-pyramid terms with the same signs (a face's edge/foot-beyond rule of
+// src/kernel_integral.cpp:613-631 is the 2-D inclusion-exclusion of a cumulative function) -- with
+// the vertex angle taken from the right triangle directly (phi = atan2(t, R_0), sin and cos from t, R_0
+// and their hypotenuse) instead of acos(R_0/r12) followed by sincos.
+#pragma once
+
+#include "cart_common.cuh"
+#include "kiwi_math.cuh"
+
+namespace kiwi_b200 {
+
+constexpr int kLatPMax = 32;     // particles per chunk
+constexpr int kLatECap = 1536;   // edge-tier entries per chunk (one full 8^3 particle box needs 486)
+constexpr int kLatSCap = 4096;   // corner values per chunk (one full 8^3 particle box needs 2187)
+
+// The I-series at an angle whose sine and cosine are given (no sincos); out of line for code size.
+KIWI_HD_NOINLINE PhiSeries phi_series_sc(double phi, double sinp, double cosp, double a, double a2) {
+    PhiSeries s;
+    s.cosp = cosp;
+    const double cosp2 = cosp * cosp;
+    const double mu = cosp / a / sqrt(1. + cosp2 / a2);
+    const double tanp = sinp / cosp;
+    s.I0 = phi;
+    s.I_2 = phi + a2 * tanp;
+    s.I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + 1. / cosp2);
+    const double u = sinp * sqrt(1 - mu * mu);
+    const double logs = log(1 + u) - log(1 - u);
+    s.I1 = atan(u / a);
+    s.I_1 = a / 2. * logs + s.I1;
+    s.I_3 = s.I_1 + a * (1. + a2) / 4. * (2 * u / (1 - u * u) + logs);
+    s.I_5 = s.I_3 + a * (1. + a2) * (1. + a2) / 16. * ((10 * u - 6 * u * u * u) / (1 - u * u) / (1 - u * u) + 3. * logs);
+    return s;
+}
+
+// Vertex-pyramid mass of the right triangle with legs R_0 (projection -> edge line) and t (along the
+// edge) in a wall at distance r0: the vertex tier of src/kernel_integral.cpp:356-400 at phi = atan2(t, R_0).
+__device__ __noinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
+    if (r0 == 0.0 || R_0 == 0.0 || t == 0.0) return 0.0;
+    const CubicWall w = cubic_wall(h, r0);
+    const double a = R_0 / r0;
+    const double a2 = a * a;
+    const double s2 = R_0 * R_0 + t * t;
+    const double rr = sqrt(s2);
+    const double phi = atan2(t, R_0);
+    const PhiSeries s = phi_series_sc(phi, t / rr, R_0 / rr, a, a2);
+    const double r2 = r0 * r0 + s2;
+    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+    double full_int;
+    if (r2 < w.h2) {
+        full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
+    } else if (r2 < 4.0 * w.h2) {
+        full_int = r0h3 / kPi * (0.25 * (4. / 3. * s.I_2 - (r0 / h) * s.I_3 + 0.3 * r0h2 * s.I_4 - 1. / 30. * r0h3 * s.I_5 + 1. / 15. * r0h_3 * s.I1) + w.B2 / r03 * s.I0 + D2);
+    } else {
+        full_int = r0h3 / kPi * (-0.25 * r0h_3 * s.I1 + w.B3 / r03 * s.I0 + D3);
+    }
+    return full_int;
+}
+
+// Offset of lattice plane P (global plane index) from the particle coordinate x0 along one axis.
+__device__ __forceinline__ double lattice_offset(double mn, double d, int P, double x0) {
+    return add_rn(mn, mul_rn((double)P, d)) - x0;
+}
+
+__device__ __forceinline__ double sgn(double v) { return (v > 0.0) ? 1.0 : ((v < 0.0) ? -1.0 : 0.0); }
+
+}  // namespace kiwi_b200

@@ -38,12 +38,13 @@ def _vol(d):
     return np.prod([(b[2 * i + 1] - b[2 * i]) / s[i] for i in range(3)])
 
 
+@pytest.mark.parametrize("form", ["fp64", "fp64_reference_order"])
 @pytest.mark.parametrize("full_box", [False, True], ids=["support_cells", "full_box"])
 @pytest.mark.parametrize("fn", GOLDEN, ids=[os.path.basename(f)[5:-4] for f in GOLDEN])
-def test_matches_reference_fixture(kiwi, ctx, fn, full_box):
+def test_matches_reference_fixture(kiwi, ctx, fn, full_box, form):
     d, P = _load(fn)
     res = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=_integrator(kiwi, d), raw=True, ctx=ctx,
-                           full_box=full_box)
+                           full_box=full_box, precision=form)
     tr = d["truth_raw"]
     truth_density = tr[0] / _vol(d)
     assert_within_envelope(res.density, d["out_density"], truth_density, label=os.path.basename(fn))
@@ -93,12 +94,13 @@ def test_generic_cubic_equals_fast_path(kiwi, ctx):
     assert np.max(np.abs(a.density - g.density)) / a.density.max() < 1e-8
 
 
-def test_matches_oracle_random_cases(kiwi, ctx, oracle):
+@pytest.mark.parametrize("form", ["fp64", "fp64_reference_order"])
+def test_matches_oracle_random_cases(kiwi, ctx, oracle, form):
     for seed, shape, k in ((1, (9, 17, 11), -1), (2, (8, 8, 8), -1), (3, (24, 5, 7), 4)):
         P = random_particles(120, seed)
         b = (0.1, 1.9, 0.0, 2.0, -0.1, 2.1)
         ki = kiwi.KernelIntegrator(kernel=max(k, 0))
-        res = kiwi.sph_to_grid(P, b, shape, kernel=ki, ctx=ctx)
+        res = kiwi.sph_to_grid(P, b, shape, kernel=ki, ctx=ctx, precision=form)
         dens, vx, vy, vz, _, st = oracle.sph_to_grid(P, b, shape, kernel=k, support_in_h=2.0)
         assert_band_tolerance(res.density, dens, RANDOM_TOLS, label=f"seed{seed}")
         assert res.stats["bbox_pairs"] == st.bbox_pairs
@@ -139,7 +141,8 @@ def test_edge_cases(kiwi, ctx):
         kiwi.sph_to_grid(P1, b, (0, 4, 4), ctx=ctx)
 
 
-def test_column_workload_subset_vs_oracle(kiwi, ctx, oracle):
+@pytest.mark.parametrize("form", ["fp64", "fp64_reference_order"])
+def test_column_workload_subset_vs_oracle(kiwi, ctx, oracle, form):
     """The 7,300-particle column workload on its full 100 x 100 x 410 grid: GPU vs oracle on a seeded subset
     of particles (the oracle is single-threaded), plus linearity of the full GPU grid over a partition."""
     from kiwi_b200.workloads import column_snapshot, subset
@@ -147,13 +150,13 @@ def test_column_workload_subset_vs_oracle(kiwi, ctx, oracle):
     shape = (100, 100, 410)
     idx = np.random.default_rng(0).choice(len(P["x"]), 6, replace=False)
     Ps = subset(P, np.sort(idx))
-    res = kiwi.sph_to_grid(Ps, b, shape, raw=True, ctx=ctx)
+    res = kiwi.sph_to_grid(Ps, b, shape, raw=True, ctx=ctx, precision=form)
     dens, vx, vy, vz, raw, st = oracle.sph_to_grid(Ps, b, shape)
     assert_band_tolerance(res.density, dens, COLUMN_TOLS, label="column subset")
     assert res.stats["bbox_pairs"] == st.bbox_pairs
-    full = kiwi.sph_to_grid(P, b, shape, raw=True, ctx=ctx)
+    full = kiwi.sph_to_grid(P, b, shape, raw=True, ctx=ctx, precision=form)
     half = np.arange(len(P["x"])) % 2 == 0
-    a = kiwi.sph_to_grid(subset(P, half), b, shape, raw=True, ctx=ctx)
-    c = kiwi.sph_to_grid(subset(P, ~half), b, shape, raw=True, ctx=ctx)
+    a = kiwi.sph_to_grid(subset(P, half), b, shape, raw=True, ctx=ctx, precision=form)
+    c = kiwi.sph_to_grid(subset(P, ~half), b, shape, raw=True, ctx=ctx, precision=form)
     errs = band_max_rel(a.raw[0] + c.raw[0], full.raw[0])
     assert max(errs[:3]) < 1e-12 and errs[3] < 1e-14, errs
