@@ -42,6 +42,15 @@ sys.path.insert(0, ROOT)
 TRANS_FLOPS = 20.0
 WORK_PER_SUPPORT_PAIR = 10166.4 + TRANS_FLOPS * 481.9
 WORK_PER_BBOX_PAIR = 9142.7 + TRANS_FLOPS * 435.6
+# The lattice-factorised kernel's own work items (orc_edge_cost / orc_lattice_vertex_cost of the counting
+# oracle, averaged over 3,000 random inputs per class): an edge tier beyond 2h 37 flops; between h and 2h
+# 127 flops + 6 transcendentals; within h 209 flops + 12; a vertex pyramid 121 flops + 4; the assembly of
+# one cell from 24 corner values ~60 flops.
+EDGE_OUTER = 37.0
+EDGE_MIDDLE = 127.0 + TRANS_FLOPS * 6
+EDGE_INNER = 209.0 + TRANS_FLOPS * 12
+VERTEX_PYRAMID = 121.0 + TRANS_FLOPS * 4
+CELL_ASSEMBLY = 60.0
 
 L2_BYTES = 126 * 1024 * 1024
 
@@ -145,9 +154,13 @@ def cpu_baseline(P, bounds, shape, kernel_name, target_s):
     rng = np.random.default_rng(99)
     perm = rng.permutation(n)
     Ps = {k: np.ascontiguousarray(v[perm]) for k, v in P.items()}
-    probe = min(n, max(64, 16 * threads))
-    t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads, p_range=(0, probe))
-    rate = probe / max(t, 1e-3)  # particles / s
+    warm = min(n, 16 * threads)
+    ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads, p_range=(0, warm))  # thread start-up
+    probe_end = min(n, warm + 128 * threads)
+    t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads,
+                                       p_range=(warm, probe_end))
+    rate = (probe_end - warm) / max(t, 1e-3)  # particles / s
+    probe = probe_end
     m = int(min(n - probe, max(threads * 4, rate * target_s)))
     t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads,
                                        p_range=(probe, probe + m))
@@ -242,6 +255,7 @@ def main():
     clocks.start()
     t_wall = time.perf_counter()
     step_ms, gather_ms, sph_pairs, bbox_pairs, evaluated, launches = [], [], 0, 0, 0, 0
+    items = {}
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()  # L2 flush between steps, outside the timed events
@@ -258,6 +272,8 @@ def main():
         bbox_pairs += st["bbox_pairs"]
         evaluated += st["evaluated_pairs"]
         launches += st["launches"]
+        for key in ("edge_tiers_outer", "edge_tiers_middle", "edge_tiers_inner", "vertex_pyramids"):
+            items[key] = items.get(key, 0) + st[key]
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
@@ -297,8 +313,18 @@ def main():
     if rank == 0:
         g_ms = float(np.mean(gather_ms))
         evaluated_per_launch = evaluated / args.steps
-        work_per_pair = WORK_PER_BBOX_PAIR if args.full_box else WORK_PER_SUPPORT_PAIR
-        achieved = evaluated_per_launch * work_per_pair / (g_ms * 1e-3) / 1e12
+        if items.get("vertex_pyramids", 0) > 0:
+            # lattice-factorised kernel: its own work items x their measured costs
+            kname = "k_cart_lattice (FP64 lattice-factorised cell-integral gather)"
+            work = (items["edge_tiers_outer"] * EDGE_OUTER + items["edge_tiers_middle"] * EDGE_MIDDLE +
+                    items["edge_tiers_inner"] * EDGE_INNER + items["vertex_pyramids"] * VERTEX_PYRAMID +
+                    evaluated * CELL_ASSEMBLY) / args.steps
+            work_per_pair = work / max(evaluated_per_launch, 1)
+        else:
+            kname = "k_cart_gather (FP64 cell-integral gather, reference evaluation order)"
+            work_per_pair = WORK_PER_BBOX_PAIR if args.full_box else WORK_PER_SUPPORT_PAIR
+            work = evaluated_per_launch * work_per_pair
+        achieved = work / (g_ms * 1e-3) / 1e12
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -313,7 +339,8 @@ def main():
             "pairs": {"support_pairs_per_step": job_pairs / args.steps / ws,
                       "bbox_pairs_per_step": job_bbox / args.steps / ws,
                       "bbox_pairs_per_s": job_bbox / (job_ms * 1e-3)},
-            "roofline": {"bound": "fp64", "kernel": "k_cart_gather (FP64 cell-integral gather)",
+            "roofline": {"bound": "fp64", "kernel": kname, "work_items_per_launch":
+                         {k: v / args.steps for k, v in items.items()},
                          "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp64 if peak_fp64 else None, "traffic": None,
                          "work_per_pair_flops": work_per_pair, "evaluated_pairs_per_launch": evaluated_per_launch,

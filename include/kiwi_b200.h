@@ -88,6 +88,9 @@ typedef struct KiwiStats {
     int64_t launches;        /* GPU kernels launched by this call */
     double gather_ms;        /* device time of the cell-integral kernel(s) of this call (CUDA events) */
     double total_ms;         /* device time of the whole call, copies included for the host variants */
+    /* work items of the lattice-factorised FP64 evaluation (0 for the other forms): edge tiers by the
+     * distance of the edge line (beyond 2h, between h and 2h, within h) and vertex pyramids */
+    int64_t edge_tiers_outer, edge_tiers_middle, edge_tiers_inner, vertex_pyramids;
 } KiwiStats;
 
 /* ---- context --------------------------------------------------------------------------------- */

@@ -67,7 +67,8 @@ class KiwiStats(C.Structure):
     _fields_ = [("bbox_pairs", C.c_int64), ("sphere_pairs", C.c_int64), ("evaluated_pairs", C.c_int64),
                 ("skipped_outside", C.c_int64), ("neg_clamped", C.c_int64), ("neg_warned", C.c_int64),
                 ("fp64_fallback", C.c_int64), ("tile_pairs", C.c_int64), ("launches", C.c_int64), ("gather_ms", C.c_double),
-                ("total_ms", C.c_double)]
+                ("total_ms", C.c_double), ("edge_tiers_outer", C.c_int64), ("edge_tiers_middle", C.c_int64),
+                ("edge_tiers_inner", C.c_int64), ("vertex_pyramids", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -219,6 +219,10 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         stats->tile_pairs = total;
         stats->gather_ms = ms;
         stats->launches = ctx->launches - launches0;
+        stats->edge_tiers_outer = (int64_t)hs.edge_outer;
+        stats->edge_tiers_middle = (int64_t)hs.edge_middle;
+        stats->edge_tiers_inner = (int64_t)hs.edge_inner;
+        stats->vertex_pyramids = (int64_t)hs.vertex_pyramids;
     }
     return KIWI_OK;
 }

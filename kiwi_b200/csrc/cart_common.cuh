@@ -85,6 +85,9 @@ __host__ __device__ __forceinline__ double cell_centre(double mn, int i, double 
 struct DevStats {
     unsigned long long bbox_pairs, sphere_pairs, evaluated_pairs, skipped_outside, neg_clamped, neg_warned,
         fp64_fallback, tile_pairs, limit_hit;
+    // work items of the lattice-factorised evaluation: edge tiers whose edge line lies outside 2h,
+    // between h and 2h, within h of the particle; vertex pyramids evaluated
+    unsigned long long edge_outer, edge_middle, edge_inner, vertex_pyramids;
 };
 
 }  // namespace kiwi_b200

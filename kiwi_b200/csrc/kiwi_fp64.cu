@@ -295,6 +295,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
 #pragma unroll
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
     unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
+    unsigned long long n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0;
     const int64_t beg = range[2 * t], end = range[2 * t + 1];
 
     for (int64_t pos = beg; pos < end;) {
@@ -371,6 +372,10 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
             const CubicEdge ed = cubic_edge(w, R0);
             s_D2[it] = ed.D2;
             s_D3[it] = ed.D3;
+            const double ld2 = r0 * r0 + R0 * R0;
+            if (!ed.valid || ld2 > 4.0 * w.h2) ++n_eo;
+            else if (ld2 > w.h2) ++n_em;
+            else ++n_ei;
         }
         __syncthreads();
 
@@ -408,6 +413,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
                 const double a1 = fabs(u1), a2 = fabs(u2);
                 f = lattice_vertex(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1]) +
                     lattice_vertex(s_h[jp], r0, a2, a1, s_D2[e2], s_D3[e2]);
+                n_vp += 2;
             }
             s_S[it] = sg * f;
         }
@@ -490,6 +496,10 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
     add_stat(&st->evaluated_pairs, n_eval);
     add_stat(&st->neg_clamped, n_neg);
     add_stat(&st->neg_warned, n_warn);
+    add_stat(&st->edge_outer, n_eo);
+    add_stat(&st->edge_middle, n_em);
+    add_stat(&st->edge_inner, n_ei);
+    add_stat(&st->vertex_pyramids, n_vp);
 }
 
 __global__ void k_full_integral(int kernel, int64_t n, const double* __restrict__ arg0, const double* __restrict__ phi,

@@ -96,3 +96,42 @@ extern "C" {
 void orc_reset(void) { g_flops = g_trans = 0; }
 void orc_counts(uint64_t* flops, uint64_t* trans) { *flops = g_flops; *trans = g_trans; }
 }
+
+// Per-item costs of the lattice-factorised evaluation (kiwi_b200/csrc/lattice.cuh): one edge tier
+// (wall tier + edge tier for a (plane, edge line)) and one lattice vertex pyramid (wall tier, the right-
+// triangle angle and its sine and cosine, the I-series and the region formula).
+extern "C" void orc_edge_cost(double h, double r0, double R0, uint64_t* f, uint64_t* t) {
+    g_flops = g_trans = 0;
+    Wall w = wall_constants(h, r0);
+    Edge e = edge_constants(&w, R0);
+    (void)e;
+    *f = g_flops;
+    *t = g_trans;
+}
+
+extern "C" void orc_lattice_vertex_cost(double h, double r0d, double R0d, double td, uint64_t* f, uint64_t* t) {
+    g_flops = g_trans = 0;
+    const Counted r0(r0d), R_0(R0d), tt(td);
+    Wall w = wall_constants(h, r0);
+    Edge e = edge_constants(&w, R_0);  // D2, D3 come from the shared edge tier: not counted here
+    g_flops = g_trans = 0;
+    w = wall_constants(h, r0);
+    const Counted a = R_0 / r0;
+    const Counted a2 = a * a;
+    const Counted s2 = R_0 * R_0 + tt * tt;
+    const Counted rr = c_sqrt(s2);
+    ++g_trans;  // atan2(t, R_0)
+    const Counted phi(atan2(td, R0d));
+    Series s = series_at(phi, tt / rr, R_0 / rr, a, a2);
+    const Counted r2 = r0 * r0 + s2;
+    Counted full;
+    if (r2 < w.h2)
+        full = w.r0h3 / R_PI * (Q(1, 6) * s.I_2 - Q(3, 40) * w.r0h2 * s.I_4 + Q(1, 40) * w.r0h3 * s.I_5 + w.B1 / w.r03 * s.I0);
+    else if (r2 < 4.0 * w.h2)
+        full = w.r0h3 / R_PI * (0.25 * (Q(4, 3) * s.I_2 - (r0 / h) * s.I_3 + Q(3, 10) * w.r0h2 * s.I_4 - Q(1, 30) * w.r0h3 * s.I_5 + Q(1, 15) * w.r0h_3 * s.I1) + w.B2 / w.r03 * s.I0 + e.D2);
+    else
+        full = w.r0h3 / R_PI * (-0.25 * w.r0h_3 * s.I1 + w.B3 / w.r03 * s.I0 + e.D3);
+    (void)full;
+    *f = g_flops;
+    *t = g_trans;
+}
