@@ -382,6 +382,49 @@ def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, p
     return st.as_dict()
 
 
+@dataclass
+class MappingResult:
+    """Per-cell results of the Voronoi map in the geometry's cell order (the MappingResult rows of
+    include/kiwi/mapping.hpp:17-30 without the site coordinates)."""
+    density: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+    raw: np.ndarray | None = None
+    stats: dict = field(default_factory=dict)
+
+
+def map_voronoi(particles: dict, home_cell, cells: dict, kernel=None, precision="fp64", raw=False, ctx=None):
+    """Density and mass-weighted velocity of an SPH snapshot on Voronoi cells -- the particle loop of
+    run_mapping_stage (src/mapping.cpp:400-502).  `cells` holds the CSR geometry: face_off (n_cells+1),
+    vert_off (n_faces+1), vxyz (absolute vertex coordinates, 3 per vertex, in each face's winding),
+    face_nbr (neighbour cell index or -1), volume.  `home_cell[i]` is the cell containing particle i, or -1."""
+    ctx = ctx or default_context()
+    ki = kernel or KernelIntegrator()
+    Ps, keep = _particles_struct(particles)
+    home = np.ascontiguousarray(home_cell, dtype=np.int32)
+    fo = np.ascontiguousarray(cells["face_off"], dtype=np.int64)
+    vo = np.ascontiguousarray(cells["vert_off"], dtype=np.int64)
+    vx_ = _f64(cells["vxyz"]).reshape(-1)
+    nb = np.ascontiguousarray(cells["face_nbr"], dtype=np.int32)
+    vol = _f64(cells["volume"])
+    nc = len(vol)
+    cs = KiwiVoronoiCells(nc, fo.ctypes.data_as(_i64p), vo.ctypes.data_as(_i64p), _p(vx_), nb.ctypes.data_as(_i32p),
+                          _p(vol))
+    outs = [np.empty(nc) for _ in range(4)]
+    rawa = np.empty(4 * nc) if raw else None
+    st = KiwiStats()
+    sel = ki.sel()
+    ctx.check(ctx._L.kiwi_map_voronoi(ctx.handle, C.byref(Ps), home.ctypes.data_as(_i32p), C.byref(cs), C.byref(sel),
+                                      precision_code(precision), *[_p(o) for o in outs], _p(rawa), C.byref(st)),
+              "map")
+    d = st.as_dict()
+    d["unresolved"] = d["skipped_outside"]
+    d["unmapped"] = d["tile_pairs"]
+    d["visited_pairs"] = d["evaluated_pairs"]
+    return MappingResult(*outs, raw=rawa.reshape(4, nc) if raw else None, stats=d)
+
+
 def version() -> str:
     return load_library().kiwi_version().decode()
 

@@ -27,6 +27,7 @@ UNITS = [
     ("capi.cu", ["--fmad=false"]),
     ("kiwi_fp64.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
+    ("voronoi.cu", ["--fmad=false"]),
 ]
 
 

@@ -268,7 +268,7 @@ int kiwi_ctx_create(int device, KiwiCtx** out) {
         return KIWI_ERR_CUDA;
     }
     for (auto& ev : ctx->ev) cudaEventCreate(&ev);
-    if (fp64_init_tables(ctx) != KIWI_OK) {
+    if (fp64_init_tables(ctx) != KIWI_OK || voronoi_init_tables(ctx) != KIWI_OK) {
         kiwi_ctx_destroy(ctx);
         return KIWI_ERR_CUDA;
     }
@@ -456,10 +456,82 @@ int kiwi_sph_to_grid(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCar
 int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
                      const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
                      double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats) {
-    (void)particles; (void)home_cell; (void)cells; (void)kernel; (void)precision;
-    (void)density; (void)vx; (void)vy; (void)vz; (void)raw4; (void)stats;
     KIWI_TRY(check_ctx(ctx));
-    return set_err(ctx, KIWI_ERR_UNSUPPORTED, "kiwi_map_voronoi is not available in this build");
+    int rc = KIWI_OK;
+    if (!particles_ok(ctx, particles, &rc)) return rc;
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    if ((precision & KIWI_FORM_MASK) != KIWI_FP64 && (precision & KIWI_FORM_MASK) != KIWI_FP64_REFERENCE_ORDER)
+        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "the Voronoi map is available in the FP64 form only");
+    if (!cells || cells->n_cells < 0 || (cells->n_cells > 0 && (!cells->face_off || !cells->vert_off ||
+                                                                 !cells->vxyz || !cells->face_nbr || !cells->volume)))
+        return set_err(ctx, KIWI_ERR_ARG, "cell geometry is incomplete");
+    if (particles->n > 0 && !home_cell) return set_err(ctx, KIWI_ERR_ARG, "home_cell is null");
+    if (cells->n_cells >= (1LL << 31)) return set_err(ctx, KIWI_ERR_ARG, "too many cells");
+    const int64_t n = particles->n, nc = cells->n_cells;
+    const int64_t nf = nc > 0 ? cells->face_off[nc] : 0;
+    const int64_t nv = nf > 0 ? cells->vert_off[nf] : 0;
+    if (nc > 0 && (cells->face_off[0] != 0 || nf < 0 || nv < 0 || (nf > 0 && cells->vert_off[0] != 0)))
+        return set_err(ctx, KIWI_ERR_ARG, "face_off / vert_off must start at 0");
+    for (int64_t c = 0; c < nc; ++c)
+        if (cells->face_off[c + 1] < cells->face_off[c]) return set_err(ctx, KIWI_ERR_ARG, "face_off must not decrease");
+    for (int64_t f = 0; f < nf; ++f) {
+        if (cells->vert_off[f + 1] < cells->vert_off[f]) return set_err(ctx, KIWI_ERR_ARG, "vert_off must not decrease");
+        if (cells->face_nbr[f] >= nc) return set_err(ctx, KIWI_ERR_ARG, "face_nbr out of range");
+    }
+    for (int64_t i = 0; i < n; ++i)
+        if (home_cell[i] >= nc) return set_err(ctx, KIWI_ERR_ARG, "home_cell out of range");
+    // stage particles, home cells and geometry
+    double* dpart = nullptr;
+    int32_t* dhome = nullptr;
+    unsigned char* dgeo = nullptr;
+    double* dout = nullptr;
+    const size_t b_fo = sizeof(int64_t) * (nc + 1), b_vo = sizeof(int64_t) * (nf + 1), b_v = sizeof(double) * 3 * nv;
+    const size_t b_nb = sizeof(int32_t) * nf, b_vol = sizeof(double) * nc;
+    auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    const size_t geo_bytes = al(b_fo) + al(b_vo) + al(b_v) + al(b_nb) + al(b_vol);
+    KIWI_TRY(scratch_t(ctx, S_PART, (size_t)std::max<int64_t>(8 * n, 1), &dpart));
+    KIWI_TRY(scratch_t(ctx, S_VOR_HOME, (size_t)std::max<int64_t>(n, 1), &dhome));
+    KIWI_TRY(scratch_t(ctx, S_VOR_CSR, geo_bytes, &dgeo));
+    KIWI_TRY(scratch_t(ctx, S_OUT, (size_t)(raw4 ? 8 : 4) * std::max<int64_t>(nc, 1), &dout));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    const double* src[8] = {particles->x, particles->y, particles->z, particles->vx,
+                            particles->vy, particles->vz, particles->m, particles->h};
+    for (int a = 0; a < 8 && n > 0; ++a)
+        KIWI_CUDA(ctx, cudaMemcpyAsync(dpart + a * n, src[a], sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    if (n > 0) KIWI_CUDA(ctx, cudaMemcpyAsync(dhome, home_cell, sizeof(int32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    unsigned char* q = dgeo;
+    int64_t* d_fo = (int64_t*)q; q += al(b_fo);
+    int64_t* d_vo = (int64_t*)q; q += al(b_vo);
+    double* d_v = (double*)q; q += al(b_v);
+    int32_t* d_nb = (int32_t*)q; q += al(b_nb);
+    double* d_vol = (double*)q;
+    if (nc > 0) {
+        KIWI_CUDA(ctx, cudaMemcpyAsync(d_fo, cells->face_off, b_fo, cudaMemcpyHostToDevice, ctx->stream));
+        KIWI_CUDA(ctx, cudaMemcpyAsync(d_vo, cells->vert_off, b_vo, cudaMemcpyHostToDevice, ctx->stream));
+        if (nv > 0) KIWI_CUDA(ctx, cudaMemcpyAsync(d_v, cells->vxyz, b_v, cudaMemcpyHostToDevice, ctx->stream));
+        if (nf > 0) KIWI_CUDA(ctx, cudaMemcpyAsync(d_nb, cells->face_nbr, b_nb, cudaMemcpyHostToDevice, ctx->stream));
+        KIWI_CUDA(ctx, cudaMemcpyAsync(d_vol, cells->volume, b_vol, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    DevParticles P{n, dpart, dpart + n, dpart + 2 * n, dpart + 3 * n, dpart + 4 * n, dpart + 5 * n, dpart + 6 * n,
+                   dpart + 7 * n};
+    KiwiVoronoiCells dc{nc, d_fo, d_vo, d_v, d_nb, d_vol};
+    CartOutputs out{dout, dout + nc, dout + 2 * nc, dout + 3 * nc, raw4 ? dout + 4 * nc : nullptr, nullptr};
+    KIWI_TRY(voronoi_map_dev(ctx, P, dhome, dc, kc, out, stats));
+    double* dst[4] = {density, vx, vy, vz};
+    for (int a = 0; a < 4 && nc > 0; ++a)
+        if (dst[a])
+            KIWI_CUDA(ctx, cudaMemcpyAsync(dst[a], dout + a * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    if (raw4 && nc > 0)
+        KIWI_CUDA(ctx, cudaMemcpyAsync(raw4, dout + 4 * nc, sizeof(double) * 4 * nc, cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        stats->total_ms = ms;
+    }
+    return KIWI_OK;
 }
 
 }  // extern "C"

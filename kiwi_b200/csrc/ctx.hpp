@@ -121,6 +121,12 @@ enum ScratchSlot {
     S_MISC1,
     S_MISC2,
     S_MISC3,
+    S_VOR_MARK,      // Voronoi walk: visited markers per work slot
+    S_VOR_QUEUE,     // Voronoi walk: queues per work slot
+    S_VOR_PAIRS,     // Voronoi walk: visited cells of every particle
+    S_VOR_NEXT,      // Voronoi walk: particle counter
+    S_VOR_CSR,       // staged cell geometry (host entry point)
+    S_VOR_HOME,      // staged home cells (host entry point)
 };
 
 }  // namespace kiwi_b200

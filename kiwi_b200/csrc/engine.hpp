@@ -45,6 +45,11 @@ bool particles_ok(KiwiCtx* ctx, const KiwiParticles* p, int* rc);
 int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
                     const CartOutputs& out, KiwiStats* stats);
 
+// voronoi.cu
+int voronoi_init_tables(KiwiCtx* ctx);
+int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, const KiwiVoronoiCells& cells,
+                    const KernelChoice& kc, const CartOutputs& out, KiwiStats* stats);
+
 // kiwi_fp64.cu
 int fp64_init_tables(KiwiCtx* ctx);
 int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,

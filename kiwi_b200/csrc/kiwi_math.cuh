@@ -19,10 +19,10 @@
 
 #ifdef __CUDACC__
 #define KIWI_HD __host__ __device__ __forceinline__
-#define KIWI_HD_NOINLINE __host__ __device__ __noinline__
+#define KIWI_HD_NOINLINE static __host__ __device__ __noinline__
 #else
 #define KIWI_HD inline
-#define KIWI_HD_NOINLINE inline
+#define KIWI_HD_NOINLINE static inline
 #endif
 
 namespace kiwi_b200 {
@@ -427,6 +427,60 @@ KIWI_HD double face_integral(double x0, double y0, double z0, double support_rad
         *out_vert = (face_dist >= support_radius) ? n : 0;
     }
     return face_Msum;
+}
+
+// The reachability half of the face walk alone (src/kernel_integral.cpp:533-645, no integrals): true iff
+// the face's closest point to the particle lies within the support radius, i.e. iff the reference's
+// out_vert != n, the condition under which its BFS enqueues the neighbour behind the face
+// (src/mapping.cpp:187-193).  Same operations as face_integral's geometry.
+template <class Verts>
+KIWI_HD bool face_reachable(double x0, double y0, double z0, double support_radius, const Verts& V, int n) {
+    if (n < 3) return true;  // out_vert = 0 != n
+    const double x1 = V.x(0), y1 = V.y(0), z1 = V.z(0);
+    const double x2s = V.x(1), y2s = V.y(1), z2s = V.z(1);
+    const double x3s = V.x(2), y3s = V.y(2), z3s = V.z(2);
+    const double A = (y2s - y1) * (z3s - z1) - (y3s - y1) * (z2s - z1);
+    const double B = (z2s - z1) * (x3s - x1) - (z3s - z1) * (x2s - x1);
+    const double C = (x2s - x1) * (y3s - y1) - (x3s - x1) * (y2s - y1);
+    const double D = -A * x1 - B * y1 - C * z1;
+    const double norm = sqrt(A * A + B * B + C * C);
+    const double r0 = (A * x0 + B * y0 + C * z0 + D) / norm;
+    const double ar0 = fabs(r0);
+    const double xp = x0 - r0 * A / norm;
+    const double yp = y0 - r0 * B / norm;
+    const double zp = z0 - r0 * C / norm;
+    bool inside_polygon = true, have_sign = false;
+    double sign_ref = 0.0;
+    double min_edge_dist = INFINITY;
+    for (int j = 0; j < n; ++j) {
+        const double x2 = V.x(j), y2 = V.y(j), z2 = V.z(j);
+        const int jn = (j == n - 1) ? 0 : j + 1;
+        const double x3 = V.x(jn), y3 = V.y(jn), z3 = V.z(jn);
+        const double r23 = sqrt((x3 - x2) * (x3 - x2) + (y3 - y2) * (y3 - y2) + (z3 - z2) * (z3 - z2));
+        const double r12 = sqrt((xp - x2) * (xp - x2) + (yp - y2) * (yp - y2) + (zp - z2) * (zp - z2));
+        const double r13 = sqrt((xp - x3) * (xp - x3) + (yp - y3) * (yp - y3) + (zp - z3) * (zp - z3));
+        const double cosa = ((x3 - x2) * (xp - x2) + (y3 - y2) * (yp - y2) + (z3 - z2) * (zp - z2)) / r12 / r23;
+        const double R_0 = (fabs(cosa) < 1.0) ? r12 * sqrt(1 - cosa * cosa) : 0.0;
+        const double phi1 = (R_0 < r12) ? acos(R_0 / r12) : 0.0;
+        const double phi2 = (R_0 < r13) ? acos(R_0 / r13) : 0.0;
+        const double ex = x3 - x2, ey = y3 - y2, ez = z3 - z2;
+        const double tpx = xp - x2, tpy = yp - y2, tpz = zp - z2;
+        const double side = (ey * tpz - ez * tpy) * A + (ez * tpx - ex * tpz) * B + (ex * tpy - ey * tpx) * C;
+        const double side_eps = 1e-9 * norm * r23 * dmax2(dmax2(fabs(tpx), fabs(tpy)), dmax2(fabs(tpz), 1.0));
+        if (fabs(side) > side_eps) {
+            if (!have_sign) {
+                sign_ref = side;
+                have_sign = true;
+            } else if ((side > 0) != (sign_ref > 0)) {
+                inside_polygon = false;
+            }
+        }
+        const bool foot_beyond_endpoint = (r12 * sin(phi1) >= r23) || (r13 * sin(phi2) >= r23);
+        const double in_plane_dist = foot_beyond_endpoint ? dmin2(r12, r13) : R_0;
+        min_edge_dist = dmin2(min_edge_dist, in_plane_dist);
+    }
+    const double face_dist = inside_polygon ? ar0 : sqrt(r0 * r0 + min_edge_dist * min_edge_dist);
+    return !(face_dist >= support_radius);
 }
 
 // Flattened xyz vertex array (a Voronoi face, or a face handed over by the scalar API).

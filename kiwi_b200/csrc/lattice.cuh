@@ -50,7 +50,7 @@ KIWI_HD_NOINLINE PhiSeries phi_series_sc(double phi, double sinp, double cosp, d
 
 // Vertex-pyramid mass of the right triangle with legs R_0 (projection -> edge line) and t (along the
 // edge) in a wall at distance r0: the vertex tier of src/kernel_integral.cpp:356-400 at phi = atan2(t, R_0).
-__device__ __noinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
+static __device__ __noinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
     if (r0 == 0.0 || R_0 == 0.0 || t == 0.0) return 0.0;
     const CubicWall w = cubic_wall(h, r0);
     const double a = R_0 / r0;

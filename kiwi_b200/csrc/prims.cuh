@@ -45,7 +45,7 @@ __global__ void k_scan_partials(const T* __restrict__ in, int64_t n, int64_t* __
 }
 
 // Single block: exclusive scan of the block partials in place, total to *total.
-__global__ void k_scan_partials_scan(int64_t* __restrict__ partial, int64_t nblocks, int64_t* __restrict__ total) {
+static __global__ void k_scan_partials_scan(int64_t* __restrict__ partial, int64_t nblocks, int64_t* __restrict__ total) {
     __shared__ int64_t sh[kScanThreads];
     __shared__ int64_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -127,7 +127,7 @@ constexpr int kSortThreads = 256;
 constexpr int kSortRounds = 8;
 constexpr int kSortSeg = kSortThreads * kSortRounds;  // elements per block segment
 
-__global__ void k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int shift, uint32_t* __restrict__ hist,
+static __global__ void k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int shift, uint32_t* __restrict__ hist,
                              int nblocks) {
     __shared__ uint32_t h[kRadix];
     for (int i = threadIdx.x; i < kRadix; i += kSortThreads) h[i] = 0;
@@ -144,7 +144,7 @@ __global__ void k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int s
 
 // Stable scatter: element order inside a block segment is round-major, then thread order, i.e. the
 // input order; ranks among equal digits follow that order.
-__global__ void k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, int64_t n,
+static __global__ void k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, int64_t n,
                                 int shift, const int64_t* __restrict__ offs, int nblocks, uint32_t* __restrict__ kout,
                                 uint32_t* __restrict__ vout) {
     __shared__ int64_t base_off[kRadix];

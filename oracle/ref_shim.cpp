@@ -309,7 +309,12 @@ void* ref_voronoi_build(long n, const double* x, const double* y, const double* 
             R->home.push_back((found && sid >= 0 && sid <= max_id) ? reverse[sid] : -1);
         }
         if (run_map) {
-            kiwi::MappingResult mr = kiwi::run_mapping_stage(c);
+            // A fresh run of the stage in its own work folder, as `kiwi map` on an empty folder runs it:
+            // it recomputes the point set and uses it in memory (reusing the cached point-set file above
+            // would give it the 15-digit rounded points instead).
+            kiwi::Config cm = c;
+            cm.work_folder = dir + "/runs_map";
+            kiwi::MappingResult mr = kiwi::run_mapping_stage(cm);
             const size_t nc = R->id.size();
             R->density.assign(nc, 0.0);
             R->vx.assign(nc, 0.0);

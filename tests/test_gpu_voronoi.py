@@ -1,0 +1,113 @@
+"""GPU parity of the Voronoi map (run_mapping_stage's particle loop, src/mapping.cpp:400-502) against the
+reference's own mapping.dat values on its own Voro++ geometry (fixtures tests/golden/vor_*.npz, made by
+the reference library) and the exact integral (__float128 oracle), plus the cell walk's visited pairs
+against the oracle, edge cases, and the reference's lattice identity (tools/test_lattice_grid.cpp): on a
+cubic lattice of cells the Voronoi map equals sph-to-grid."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from conftest import box_faces, random_particles
+from gpu_checks import assert_within_envelope, velocity_errors
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "vor_*.npz")))
+
+
+def _load(fn):
+    d = np.load(fn)
+    P = {k: d[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+    geo = {k[4:]: d[k] for k in d.files if k.startswith("geo_")}
+    return d, P, geo
+
+
+@pytest.mark.parametrize("fn", GOLDEN, ids=[os.path.basename(f)[4:-4] for f in GOLDEN])
+def test_matches_reference_mapping(kiwi, ctx, oracle, fn):
+    d, P, geo = _load(fn)
+    k = int(d["kernel_index"])
+    res = kiwi.map_voronoi(P, d["home"], geo, kernel=kiwi.KernelIntegrator(kernel=k), raw=True, ctx=ctx)
+    tr = d["truth_raw"]
+    truth_density = np.where(geo["volume"] > 0, tr[0] / geo["volume"], 0.0)
+    assert_within_envelope(res.density, d["out_density"], truth_density, label=os.path.basename(fn))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        for i, name in enumerate(("vx", "vy", "vz")):
+            tv = np.where(tr[0] > 0, tr[i + 1] / np.where(tr[0] > 0, tr[0], 1.0), 0.0)
+            assert velocity_errors(getattr(res, name), tv, tr[0]) <= \
+                4.0 * velocity_errors(d["out_" + name], tv, tr[0]) + 1e-13
+    # the walk visits exactly the reference's (cell, particle) pairs
+    _, _, _, _, _, visited = oracle.map_voronoi(P, d["home"], geo, kernel=k if k > 0 else -1,
+                                                support_in_h=float(d["support_in_h"]))
+    assert res.stats["visited_pairs"] == visited
+    # mass conservation as far as the supports stay inside the domain
+    mass = float((res.density * geo["volume"]).sum())
+    ref_mass = float((d["out_density"] * geo["volume"]).sum())
+    assert abs(mass - ref_mass) <= 1e-12 * ref_mass
+
+
+def test_deterministic_and_edge_cases(kiwi, ctx):
+    d, P, geo = _load(GOLDEN[0])
+    a = kiwi.map_voronoi(P, d["home"], geo, raw=True, ctx=ctx)
+    b = kiwi.map_voronoi(P, d["home"], geo, raw=True, ctx=ctx)
+    assert np.array_equal(a.raw, b.raw)
+    # unresolved particles (home -1) and h <= 0 contribute nothing but still count in the mean velocity
+    home = d["home"].copy()
+    home[:10] = -1
+    P2 = dict(P)
+    P2["h"] = P["h"].copy()
+    P2["h"][10:20] = 0.0
+    r = kiwi.map_voronoi(P2, home, geo, ctx=ctx)
+    assert r.stats["unresolved"] == 10
+    keep = np.ones(len(home), bool)
+    keep[:20] = False
+    sub = {k: v[keep] for k, v in P.items()}
+    rs = kiwi.map_voronoi(sub, d["home"][keep], geo, raw=True, ctx=ctx)
+    r2 = kiwi.map_voronoi(P2, home, geo, raw=True, ctx=ctx)
+    assert np.array_equal(rs.raw, r2.raw)
+    # no particles at all
+    P0 = {k: np.zeros(0) for k in P}
+    r0 = kiwi.map_voronoi(P0, np.zeros(0, np.int32), geo, ctx=ctx)
+    assert np.all(r0.density == 0)
+    # bad geometry is rejected
+    bad = dict(geo)
+    bad["face_nbr"] = geo["face_nbr"].copy()
+    bad["face_nbr"][0] = len(geo["volume"]) + 5
+    with pytest.raises(kiwi.KiwiError):
+        kiwi.map_voronoi(P, d["home"], bad, ctx=ctx)
+
+
+def lattice_cells(n, lo, hi):
+    """CSR geometry of an n^3 lattice of box cells over [lo, hi]^3, faces wound as the face walk needs."""
+    d = (hi - lo) / n
+    face_off, vert_off, vxyz, nbr, vol = [0], [0], [], [], []
+    idx = lambda i, j, k: (i * n + j) * n + k
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                c = np.array([lo + (i + 0.5) * d, lo + (j + 0.5) * d, lo + (k + 0.5) * d])
+                faces = box_faces(c - 0.5 * d, c + 0.5 * d)
+                nb = [idx(i + 1, j, k) if i + 1 < n else -1, idx(i - 1, j, k) if i > 0 else -1,
+                      idx(i, j + 1, k) if j + 1 < n else -1, idx(i, j - 1, k) if j > 0 else -1,
+                      idx(i, j, k + 1) if k + 1 < n else -1, idx(i, j, k - 1) if k > 0 else -1]
+                for f, b in zip(faces, nb):
+                    vxyz.extend(f)
+                    vert_off.append(vert_off[-1] + 4)
+                    nbr.append(b)
+                face_off.append(face_off[-1] + 6)
+                vol.append(d ** 3)
+    return {"face_off": np.array(face_off), "vert_off": np.array(vert_off), "vxyz": np.array(vxyz),
+            "face_nbr": np.array(nbr, np.int32), "volume": np.array(vol)}, d
+
+
+def test_lattice_voronoi_equals_sph_to_grid(kiwi, ctx):
+    n, lo, hi = 10, 0.0, 2.0
+    geo, d = lattice_cells(n, lo, hi)
+    P = random_particles(60, 17, box=(0.4, 1.6), hmin=0.05, hmax=0.25)
+    home = ((np.floor(P["x"] / d) * n + np.floor(P["y"] / d)) * n + np.floor(P["z"] / d)).astype(np.int32)
+    v = kiwi.map_voronoi(P, home, geo, raw=True, ctx=ctx)
+    g = kiwi.sph_to_grid(P, (lo, hi, lo, hi, lo, hi), (n, n, n), raw=True, ctx=ctx, precision="fp64_reference_order")
+    m = g.raw[0] > 1e-6 * g.raw[0].max()
+    assert np.max(np.abs(v.raw[0][m] - g.raw[0][m]) / g.raw[0][m]) < 1e-9
+    assert abs(v.raw[0].sum() - g.raw[0].sum()) <= 1e-12 * g.raw[0].sum()
