@@ -77,10 +77,8 @@ struct PhiSeries {
     double I0, I_2, I_4, I1, I_1, I_3, I_5, cosp;
 };
 
-KIWI_HD_NOINLINE PhiSeries phi_series(double phi, double a, double a2) {
+KIWI_HD_NOINLINE PhiSeries phi_series_sc(double phi, double sinp, double cosp, double a, double a2) {
     PhiSeries s;
-    double sinp, cosp;
-    sincos(phi, &sinp, &cosp);
     s.cosp = cosp;
     const double cosp2 = cosp * cosp;
     const double mu = cosp / a / sqrt(1. + cosp2 / a2);
@@ -95,6 +93,13 @@ KIWI_HD_NOINLINE PhiSeries phi_series(double phi, double a, double a2) {
     s.I_3 = s.I_1 + a * (1. + a2) / 4. * (2 * u / (1 - u * u) + logs);
     s.I_5 = s.I_3 + a * (1. + a2) * (1. + a2) / 16. * ((10 * u - 6 * u * u * u) / (1 - u * u) / (1 - u * u) + 3. * logs);
     return s;
+}
+
+// The series at phi, with the sincos of phi (the edge tier's h and 2h angles).
+KIWI_HD_NOINLINE PhiSeries phi_series(double phi, double a, double a2) {
+    double sinp, cosp;
+    sincos(phi, &sinp, &cosp);
+    return phi_series_sc(phi, sinp, cosp, a, a2);
 }
 
 KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) {
@@ -131,13 +136,28 @@ KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) {
     return e;
 }
 
+// I1 = atan(u/a) alone, by the same operations as the full series: beyond 2h the vertex tier needs only
+// I0 = phi and I1, so the logarithms, tan and I_2..I_5 (dead there) are not evaluated.
+KIWI_HD double phi_I1(double sinp, double cosp, double a, double a2) {
+    const double cosp2 = cosp * cosp;
+    const double mu = cosp / a / sqrt(1. + cosp2 / a2);
+    const double u = sinp * sqrt(1 - mu * mu);
+    return atan(u / a);
+}
+
 KIWI_HD double cubic_vertex(const CubicWall& w, const CubicEdge& e, double phi) {
     if (!w.valid || !e.valid) return 0.0;
     if (phi == 0.0) return 0.0;
     const double r0 = w.r0, h = w.h, r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    const PhiSeries s = phi_series(phi, e.a, e.a2);
-    const double R = e.R_0 / s.cosp;
+    double sinp, cosp;
+    sincos(phi, &sinp, &cosp);
+    const double R = e.R_0 / cosp;
     const double r2 = r0 * r0 + R * R;
+    if (!(r2 < 4.0 * w.h2)) {
+        const double I1 = phi_I1(sinp, cosp, e.a, e.a2);
+        return r0h3 / kPi * (-0.25 * r0h_3 * I1 + w.B3 / r03 * phi + e.D3);
+    }
+    const PhiSeries s = phi_series_sc(phi, sinp, cosp, e.a, e.a2);
     double full_int;
     if (r2 < w.h2) {
         full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);

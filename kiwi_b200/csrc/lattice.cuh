@@ -29,27 +29,9 @@ constexpr int kLatPMax = 32;     // particles per chunk
 constexpr int kLatECap = 1536;   // edge-tier entries per chunk (one full 8^3 particle box needs 486)
 constexpr int kLatSCap = 4096;   // corner values per chunk (one full 8^3 particle box needs 2187)
 
-// The I-series at an angle whose sine and cosine are given (no sincos); out of line for code size.
-KIWI_HD_NOINLINE PhiSeries phi_series_sc(double phi, double sinp, double cosp, double a, double a2) {
-    PhiSeries s;
-    s.cosp = cosp;
-    const double cosp2 = cosp * cosp;
-    const double mu = cosp / a / sqrt(1. + cosp2 / a2);
-    const double tanp = sinp / cosp;
-    s.I0 = phi;
-    s.I_2 = phi + a2 * tanp;
-    s.I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + 1. / cosp2);
-    const double u = sinp * sqrt(1 - mu * mu);
-    const double logs = log(1 + u) - log(1 - u);
-    s.I1 = atan(u / a);
-    s.I_1 = a / 2. * logs + s.I1;
-    s.I_3 = s.I_1 + a * (1. + a2) / 4. * (2 * u / (1 - u * u) + logs);
-    s.I_5 = s.I_3 + a * (1. + a2) * (1. + a2) / 16. * ((10 * u - 6 * u * u * u) / (1 - u * u) / (1 - u * u) + 3. * logs);
-    return s;
-}
-
 // Vertex-pyramid mass of the right triangle with legs R_0 (projection -> edge line) and t (along the
-// edge) in a wall at distance r0: the vertex tier of src/kernel_integral.cpp:356-400 at phi = atan2(t, R_0).
+// edge) in a wall at distance r0: the vertex tier of src/kernel_integral.cpp:356-400 at phi = atan2(t, R_0)
+// (beyond 2h only I0 and I1 are needed, as in cubic_vertex).
 static __device__ __noinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
     if (r0 == 0.0 || R_0 == 0.0 || t == 0.0) return 0.0;
     const CubicWall w = cubic_wall(h, r0);
@@ -58,9 +40,14 @@ static __device__ __noinline__ double lattice_vertex(double h, double r0, double
     const double s2 = R_0 * R_0 + t * t;
     const double rr = sqrt(s2);
     const double phi = atan2(t, R_0);
-    const PhiSeries s = phi_series_sc(phi, t / rr, R_0 / rr, a, a2);
+    const double sinp = t / rr, cosp = R_0 / rr;
     const double r2 = r0 * r0 + s2;
     const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+    if (!(r2 < 4.0 * w.h2)) {
+        const double I1 = phi_I1(sinp, cosp, a, a2);
+        return r0h3 / kPi * (-0.25 * r0h_3 * I1 + w.B3 / r03 * phi + D3);
+    }
+    const PhiSeries s = phi_series_sc(phi, sinp, cosp, a, a2);
     double full_int;
     if (r2 < w.h2) {
         full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);

@@ -1,0 +1,36 @@
+// Test-only: compiles the device maths header kiwi_b200/csrc/kiwi_math.cuh for the host (glibc libm,
+// -ffp-contract=off) so that tests/test_host_math.py can check its transcription of the reference's
+// formulas against the oracle bit for bit, without a GPU.  Never part of the product library.
+#include <cmath>
+#include <cstdint>
+
+#include "../kiwi_b200/csrc/kiwi_math.cuh"
+
+using namespace kiwi_b200;
+
+extern "C" {
+
+double hm_full_integral(int kernel, double arg0, double phi, double r0, double R0) {
+    return kernel < 0 ? cubic_full_integral(arg0, phi, r0, R0)
+                      : generic_full_integral(&kiwi_kernel_tables[kernel], arg0, phi, r0, R0);
+}
+
+double hm_face_integral(double x0, double y0, double z0, int kernel, double h, double support, const double* verts,
+                        int n, int* out_vert) {
+    FlatVerts V{verts};
+    if (kernel < 0) {
+        CubicEval ev;
+        ev.h = h;
+        return face_integral(x0, y0, z0, 2 * h, V, n, out_vert, ev);
+    }
+    static GenericEval ev;
+    ev.K = &kiwi_kernel_tables[kernel];
+    ev.H = support;
+    return face_integral(x0, y0, z0, support, V, n, out_vert, ev);
+}
+
+int hm_face_reachable(double x0, double y0, double z0, double support, const double* verts, int n) {
+    FlatVerts V{verts};
+    return face_reachable(x0, y0, z0, support, V, n) ? 1 : 0;
+}
+}
