@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kiwi", choices=["kiwi", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed", "fp64_reference_order"])
     ap.add_argument("--full-box", action="store_true",
                     help="evaluate every cell of each support bounding box, as the reference does")
     ap.add_argument("--n", type=int, default=2_000_000)

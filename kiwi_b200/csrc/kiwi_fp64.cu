@@ -281,6 +281,8 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
         s_vy[kLatPMax], s_vz[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
     __shared__ int s_np, s_etot, s_stot;
+    __shared__ int s_wexp[kThreads / 32], s_wcheap[kThreads / 32];
+    __shared__ unsigned short s_blist[kLatSCap];
     extern __shared__ double s_dyn[];
     double* s_D2 = s_dyn;
     double* s_D3 = s_dyn + kLatECap;
@@ -379,8 +381,64 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
         }
         __syncthreads();
 
+        // (B0) order the corner items so that the cheap ones (corner beyond 2h: only I0 and I1; or a zero
+        // corner) run in warps of their own: the others from the front of s_blist, the cheap ones from
+        // the back.  Results do not depend on this order.
+        {
+            unsigned cheap = 0;
+            int nitems = 0;
+#pragma unroll
+            for (int q = 0; q < kLatSCap / kThreads; ++q) {
+                const int it = threadIdx.x + q * kThreads;
+                if (it >= stot) break;
+                ++nitems;
+                const int jp = chunk_search(s_soff, np, it);
+                const int s = it - s_soff[jp];
+                const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                const int L = (s_dim[jp][0] + 1) * n1 * n2;
+                const int axis = s / L, rem = s % L;
+                const int i = rem / (n1 * n2), jj = (rem / n2) % n1, k = rem % n2;
+                const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
+                const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
+                const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+                const double ua = axis == 0 ? ux : (axis == 1 ? uy : uz);
+                const double u1 = axis == 0 ? uy : ux, u2 = axis == 2 ? uy : uz;
+                const double h = s_h[jp];
+                const bool zero = ua == 0.0 || u1 == 0.0 || u2 == 0.0;
+                if (zero || !(ua * ua + (u1 * u1 + u2 * u2) < 4.0 * (h * h))) cheap |= 1u << q;
+            }
+            const int ncheap = __popc(cheap), nexp = nitems - ncheap;
+            int ie = nexp, ic = ncheap;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vc = __shfl_up_sync(0xffffffffu, ic, o);
+                if (lane >= o) {
+                    ie += ve;
+                    ic += vc;
+                }
+            }
+            if (lane == 31) {
+                s_wexp[warp] = ie;
+                s_wcheap[warp] = ic;
+            }
+            __syncthreads();
+            int be = ie - nexp, bc = ic - ncheap;
+            for (int w = 0; w < warp; ++w) {
+                be += s_wexp[w];
+                bc += s_wcheap[w];
+            }
+#pragma unroll
+            for (int q = 0; q < kLatSCap / kThreads; ++q) {
+                const int it = threadIdx.x + q * kThreads;
+                if (it >= stot) break;
+                if (cheap & (1u << q)) s_blist[stot - 1 - bc++] = (unsigned short)it;
+                else s_blist[be++] = (unsigned short)it;
+            }
+            __syncthreads();
+        }
+
         // (B) corner values S_a(i, j, k) for the three plane orientations a
-        for (int it = threadIdx.x; it < stot; it += kThreads) {
+        for (int li = threadIdx.x; li < stot; li += kThreads) {
+            const int it = s_blist[li];
             const int jp = chunk_search(s_soff, np, it);
             const int s = it - s_soff[jp];
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;

@@ -137,7 +137,8 @@ KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) {
 }
 
 // I1 = atan(u/a) alone, by the same operations as the full series: beyond 2h the vertex tier needs only
-// I0 = phi and I1, so the logarithms, tan and I_2..I_5 (dead there) are not evaluated.
+// I0 = phi and I1, so the logarithms, tan and I_2..I_5 (dead there) can be skipped where whole warps are
+// in that region (the lattice kernel groups its corner items that way).
 KIWI_HD double phi_I1(double sinp, double cosp, double a, double a2) {
     const double cosp2 = cosp * cosp;
     const double mu = cosp / a / sqrt(1. + cosp2 / a2);
@@ -149,15 +150,10 @@ KIWI_HD double cubic_vertex(const CubicWall& w, const CubicEdge& e, double phi) 
     if (!w.valid || !e.valid) return 0.0;
     if (phi == 0.0) return 0.0;
     const double r0 = w.r0, h = w.h, r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    double sinp, cosp;
-    sincos(phi, &sinp, &cosp);
-    const double R = e.R_0 / cosp;
+    // (the full series in every region: a per-lane shortcut for the outer region only diverges warps here)
+    const PhiSeries s = phi_series(phi, e.a, e.a2);
+    const double R = e.R_0 / s.cosp;
     const double r2 = r0 * r0 + R * R;
-    if (!(r2 < 4.0 * w.h2)) {
-        const double I1 = phi_I1(sinp, cosp, e.a, e.a2);
-        return r0h3 / kPi * (-0.25 * r0h_3 * I1 + w.B3 / r03 * phi + e.D3);
-    }
-    const PhiSeries s = phi_series_sc(phi, sinp, cosp, e.a, e.a2);
     double full_int;
     if (r2 < w.h2) {
         full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
