@@ -138,6 +138,19 @@ int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const 
                             const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy,
                             double* vz, double* raw4, KiwiStats* stats);
 
+/* Adjoint of the sph-to-grid raw sums.  It has no counterpart in the reference (which has no gradients).
+ * With M_c = sum_p m_p K_pc and P_c = sum_p m_p K_pc v_p the raw sums of kiwi_sph_to_grid_device
+ * (K_pc the particle's kernel mass in cell c, clamped at 0), and raw4 the cotangents dL/dM, dL/dPx,
+ * dL/dPy, dL/dPz (4 * ncells doubles, the raw4 layout), it writes per particle dL/dx, dL/dy, dL/dz,
+ * dL/dh, dL/dm, dL/dvx, dL/dvy, dL/dvz (any output may be NULL).  The per-pair integrals are recomputed
+ * in FP64 with forward-mode derivatives, over the pairs of the default (support-culled) evaluation.
+ * Every pointer is in device memory; runs on the context's stream and returns when done.  Cubic spline
+ * with support 2h only (KIWI_ERR_UNSUPPORTED otherwise). */
+int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                                    const KiwiKernelSel* kernel, const double* raw4, double* dx, double* dy,
+                                    double* dz, double* dh, double* dm, double* dvx, double* dvy, double* dvz,
+                                    KiwiStats* stats);
+
 /* Allocation-free variant of kiwi_sph_to_grid_device.  It has no counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: codes that hand all device memory to their own pool

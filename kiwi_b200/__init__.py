@@ -107,6 +107,9 @@ def load_library(path: str = LIB_PATH):
            _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
     L.kiwi_sph_to_grid.argtypes = sig
     L.kiwi_sph_to_grid_device.argtypes = sig
+    L.kiwi_sph_to_grid_adjoint_device.argtypes = ([C.c_void_p, C.POINTER(KiwiParticles), C.POINTER(KiwiCartGrid),
+                                                   C.POINTER(KiwiKernelSel), _dp] + [_dp] * 8 +
+                                                  [C.POINTER(KiwiStats)])
     L.kiwi_map_voronoi.argtypes = [C.c_void_p, C.POINTER(KiwiParticles), _i32p, C.POINTER(KiwiVoronoiCells),
                                    C.POINTER(KiwiKernelSel), C.c_int, _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
     _lib = L
@@ -379,6 +382,27 @@ def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, p
                                              precision_code(precision, full_box), dp(out.get("density")),
                                              dp(out.get("vx")), dp(out.get("vy")), dp(out.get("vz")),
                                              dp(out.get("raw4")), C.byref(st)), "sph-to-grid")
+    return st.as_dict()
+
+
+def sph_to_grid_adjoint_device(particles: dict, bounds, shape, raw4_cot, grads: dict, kernel=None, ctx=None):
+    """Adjoint of the raw sums (no counterpart in the reference): `particles` holds CUDA float64 tensors,
+    `raw4_cot` the cotangents dL/dM, dL/dPx, dL/dPy, dL/dPz (4 * ncells, CUDA float64), `grads` maps any of
+    x y z h m vx vy vz to CUDA float64 tensors that receive dL/d(that input).  Returns the call's stats."""
+    ctx = ctx or default_context()
+    ki = kernel or KernelIntegrator()
+    Ps, _ = _particles_struct(particles, device=True)
+    nx, ny, nz = (int(s) for s in shape)
+    grid = KiwiCartGrid((C.c_double * 6)(*[float(b) for b in bounds]), nx, ny, nz)
+    st = KiwiStats()
+    sel = ki.sel()
+
+    def dp(t):
+        return C.cast(C.c_void_p(int(t.data_ptr())), _dp) if t is not None else None
+
+    outs = [dp(grads.get(k)) for k in ("x", "y", "z", "h", "m", "vx", "vy", "vz")]
+    ctx.check(ctx._L.kiwi_sph_to_grid_adjoint_device(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
+                                                     dp(raw4_cot), *outs, C.byref(st)), "sph-to-grid adjoint")
     return st.as_dict()
 
 

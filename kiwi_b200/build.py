@@ -28,6 +28,7 @@ UNITS = [
     ("kiwi_fp64.cu", ["--fmad=false"]),
     ("noalloc.cu", ["--fmad=false"]),
     ("voronoi.cu", ["--fmad=false"]),
+    ("adjoint.cu", ["--fmad=false"]),
 ]
 
 

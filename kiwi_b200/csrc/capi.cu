@@ -410,6 +410,37 @@ int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const 
     return KIWI_OK;
 }
 
+int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                                    const KiwiKernelSel* kernel, const double* d_raw4, double* d_x, double* d_y,
+                                    double* d_z, double* d_h, double* d_m, double* d_vx, double* d_vy, double* d_vz,
+                                    KiwiStats* stats) {
+    KIWI_TRY(check_ctx(ctx));
+    int rc = KIWI_OK;
+    if (!particles_ok(ctx, particles, &rc)) return rc;
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    CartGeom g;
+    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+    if (!d_raw4 && particles->n > 0) return set_err(ctx, KIWI_ERR_ARG, "adjoint: the cotangent array raw4 is null");
+    if (stats) *stats = KiwiStats{};
+    DevParticles P{particles->n, particles->x, particles->y, particles->z, particles->vx,
+                   particles->vy, particles->vz, particles->m, particles->h};
+    AdjointOutputs out{d_x, d_y, d_z, d_h, d_m, d_vx, d_vy, d_vz};
+    const int64_t launches0 = ctx->launches;
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    KIWI_TRY(cart_adjoint_dev(ctx, P, g, kc, d_raw4, out, stats));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        stats->total_ms = ms;
+        stats->gather_ms = ms;
+        stats->launches = ctx->launches - launches0;
+    }
+    return KIWI_OK;
+}
+
 int kiwi_sph_to_grid(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                      const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy, double* vz,
                      double* raw4, KiwiStats* stats) {

@@ -38,12 +38,21 @@ struct CartOutputs {
     const double* meanv;              // device, 3 doubles: mean particle velocity
 };
 
+// Gradient outputs of the adjoint (device, one double per particle each; any may be null).
+struct AdjointOutputs {
+    double *x, *y, *z, *h, *m, *vx, *vy, *vz;
+};
+
 // capi.cu: argument resolution and the device pipeline of one sph-to-grid call
 int resolve_kernel(KiwiCtx* ctx, const KiwiKernelSel* sel, KernelChoice* out);
 int make_geom(KiwiCtx* ctx, const KiwiCartGrid* grid, double support_in_h, CartGeom* g);
 bool particles_ok(KiwiCtx* ctx, const KiwiParticles* p, int* rc);
 int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
                     const CartOutputs& out, KiwiStats* stats);
+
+// adjoint.cu
+int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc,
+                     const double* d_cot, const AdjointOutputs& out, KiwiStats* stats);
 
 // voronoi.cu
 int voronoi_init_tables(KiwiCtx* ctx);

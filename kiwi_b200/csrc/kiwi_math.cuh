@@ -31,18 +31,26 @@ constexpr double kPi = 3.14159265358979323846;
 
 // ------------------------------------------------------------------ cubic spline closed form
 
-struct CubicWall {
+// Every function of the cubic closed form and of the face walk is written once over the real type T:
+// T = double is the FP64 evaluation (the reference's operations one by one), T = Dual4 (dual.cuh) carries
+// the derivatives with respect to the particle's position and smoothing length for the adjoint.
+template <class T>
+struct CubicWallT {
     bool valid;
-    double r0, h, h2, r03, r0h2, r0h3, r0h_2, r0h_3, B1, B2, B3;
+    T r0, h, h2, r03, r0h2, r0h3, r0h_2, r0h_3, B1, B2, B3;
 };
+using CubicWall = CubicWallT<double>;
 
-struct CubicEdge {
+template <class T>
+struct CubicEdgeT {
     bool valid;
-    double R_0, a, a2, D2, D3;
+    T R_0, a, a2, D2, D3;
 };
+using CubicEdge = CubicEdgeT<double>;
 
-KIWI_HD CubicWall cubic_wall(double h, double r0) {
-    CubicWall w;
+template <class T>
+KIWI_HD CubicWallT<T> cubic_wall_t(T h, T r0) {
+    CubicWallT<T> w;
     w.valid = false;
     w.h = h;
     w.r0 = r0;
@@ -68,26 +76,30 @@ KIWI_HD CubicWall cubic_wall(double h, double r0) {
     }
     return w;
 }
+KIWI_HD CubicWall cubic_wall(double h, double r0) { return cubic_wall_t<double>(h, r0); }
 
 // The I-series at one angle (src/kernel_integral.cpp:278-294 and 372-386), with the sincos of the angle
 // it starts from.  This is the bulk of the transcendental work of every tier; it is kept out of line so
 // that a single copy of it serves the edge tier's two angles and the vertex tier's two vertices (inlined
 // four times per edge it overflows the instruction cache).
-struct PhiSeries {
-    double I0, I_2, I_4, I1, I_1, I_3, I_5, cosp;
+template <class T>
+struct PhiSeriesT {
+    T I0, I_2, I_4, I1, I_1, I_3, I_5, cosp;
 };
+using PhiSeries = PhiSeriesT<double>;
 
-KIWI_HD_NOINLINE PhiSeries phi_series_sc(double phi, double sinp, double cosp, double a, double a2) {
-    PhiSeries s;
+template <class T>
+KIWI_HD_NOINLINE PhiSeriesT<T> phi_series_sc(T phi, T sinp, T cosp, T a, T a2) {
+    PhiSeriesT<T> s;
     s.cosp = cosp;
-    const double cosp2 = cosp * cosp;
-    const double mu = cosp / a / sqrt(1. + cosp2 / a2);
-    const double tanp = sinp / cosp;
+    const T cosp2 = cosp * cosp;
+    const T mu = cosp / a / sqrt(1. + cosp2 / a2);
+    const T tanp = sinp / cosp;
     s.I0 = phi;
     s.I_2 = phi + a2 * tanp;
     s.I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + 1. / cosp2);
-    const double u = sinp * sqrt(1 - mu * mu);
-    const double logs = log(1 + u) - log(1 - u);
+    const T u = sinp * sqrt(1 - mu * mu);
+    const T logs = log(1 + u) - log(1 - u);
     s.I1 = atan(u / a);
     s.I_1 = a / 2. * logs + s.I1;
     s.I_3 = s.I_1 + a * (1. + a2) / 4. * (2 * u / (1 - u * u) + logs);
@@ -96,35 +108,37 @@ KIWI_HD_NOINLINE PhiSeries phi_series_sc(double phi, double sinp, double cosp, d
 }
 
 // The series at phi, with the sincos of phi (the edge tier's h and 2h angles).
-KIWI_HD_NOINLINE PhiSeries phi_series(double phi, double a, double a2) {
-    double sinp, cosp;
+template <class T>
+KIWI_HD_NOINLINE PhiSeriesT<T> phi_series(T phi, T a, T a2) {
+    T sinp, cosp;
     sincos(phi, &sinp, &cosp);
-    return phi_series_sc(phi, sinp, cosp, a, a2);
+    return phi_series_sc<T>(phi, sinp, cosp, a, a2);
 }
 
-KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) {
-    CubicEdge e;
+template <class T>
+KIWI_HD CubicEdgeT<T> cubic_edge_t(const CubicWallT<T>& w, T R_0) {
+    CubicEdgeT<T> e;
     e.valid = false;
     e.R_0 = R_0;
     e.a = e.a2 = e.D2 = e.D3 = 0.0;
     if (!w.valid || R_0 == 0.0) return e;
     e.valid = true;
-    const double h = w.h, r0 = w.r0, h2 = w.h2;
-    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    double D2 = 0.0, D3 = 0.0;
-    const double a = R_0 / r0;
-    const double a2 = a * a;
+    const T h = w.h, r0 = w.r0, h2 = w.h2;
+    const T r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+    T D2 = 0.0, D3 = 0.0;
+    const T a = R_0 / r0;
+    const T a2 = a * a;
     e.a = a;
     e.a2 = a2;
-    const double linedist2 = r0 * r0 + R_0 * R_0;
+    const T linedist2 = r0 * r0 + R_0 * R_0;
     if (linedist2 <= 4.0 * h2) {
         // pass 0: the angle where the vertex radius reaches h (inner edges only) -> D2;
         // pass 1: the angle where it reaches 2h -> D3
 #pragma unroll 1
         for (int pass = (linedist2 <= h2) ? 0 : 1; pass < 2; ++pass) {
-            const double hh = (pass == 0) ? h * h : 4.0 * h * h;
-            const double phik = acos(R_0 / sqrt(hh - r0 * r0));
-            const PhiSeries s = phi_series(phik, a, a2);
+            const T hh = (pass == 0) ? h * h : 4.0 * h * h;
+            const T phik = acos(R_0 / sqrt(hh - r0 * r0));
+            const PhiSeriesT<T> s = phi_series<T>(phik, a, a2);
             if (pass == 0)
                 D2 = -1. / 6. * s.I_2 + 0.25 * (r0 / h) * s.I_3 - 0.15 * r0h2 * s.I_4 + 1. / 30. * r0h3 * s.I_5 - 1. / 60. * r0h_3 * s.I1 + (w.B1 - w.B2) / r03 * s.I0;
             else
@@ -135,6 +149,7 @@ KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) {
     e.D3 = D3;
     return e;
 }
+KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) { return cubic_edge_t<double>(w, R_0); }
 
 // I1 = atan(u/a) alone, by the same operations as the full series: beyond 2h the vertex tier needs only
 // I0 = phi and I1, so the logarithms, tan and I_2..I_5 (dead there) can be skipped where whole warps are
@@ -146,15 +161,16 @@ KIWI_HD double phi_I1(double sinp, double cosp, double a, double a2) {
     return atan(u / a);
 }
 
-KIWI_HD double cubic_vertex(const CubicWall& w, const CubicEdge& e, double phi) {
-    if (!w.valid || !e.valid) return 0.0;
-    if (phi == 0.0) return 0.0;
-    const double r0 = w.r0, h = w.h, r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+template <class T>
+KIWI_HD T cubic_vertex_t(const CubicWallT<T>& w, const CubicEdgeT<T>& e, T phi) {
+    if (!w.valid || !e.valid) return T(0.0);
+    if (phi == 0.0) return T(0.0);
+    const T r0 = w.r0, h = w.h, r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
     // (the full series in every region: a per-lane shortcut for the outer region only diverges warps here)
-    const PhiSeries s = phi_series(phi, e.a, e.a2);
-    const double R = e.R_0 / s.cosp;
-    const double r2 = r0 * r0 + R * R;
-    double full_int;
+    const PhiSeriesT<T> s = phi_series<T>(phi, e.a, e.a2);
+    const T R = e.R_0 / s.cosp;
+    const T r2 = r0 * r0 + R * R;
+    T full_int;
     if (r2 < w.h2) {
         full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
     } else if (r2 < 4.0 * w.h2) {
@@ -164,6 +180,7 @@ KIWI_HD double cubic_vertex(const CubicWall& w, const CubicEdge& e, double phi) 
     }
     return full_int;
 }
+KIWI_HD double cubic_vertex(const CubicWall& w, const CubicEdge& e, double phi) { return cubic_vertex_t<double>(w, e, phi); }
 
 // full_integral_new (src/kernel_integral.cpp:410-418)
 KIWI_HD double cubic_full_integral(double h, double phi, double r0, double R_0) {
@@ -340,14 +357,16 @@ KIWI_HD double generic_full_integral(const KiwiKernelTable* K, double H, double 
 // Evaluator hooks (the strategy of src/kernel_integral.cpp:433-467): set_wall once per face with the
 // unsigned wall distance, set_edge once per edge with the in-plane distance to the edge line, at(phi)
 // once per edge vertex.
-struct CubicEval {
-    double h;
-    CubicWall w;
-    CubicEdge e;
-    KIWI_HD void set_wall(double ar0) { w = cubic_wall(h, ar0); }
-    KIWI_HD void set_edge(double R_0) { e = cubic_edge(w, R_0); }
-    KIWI_HD double at(double phi) const { return cubic_vertex(w, e, phi); }
+template <class T>
+struct CubicEvalT {
+    T h;
+    CubicWallT<T> w;
+    CubicEdgeT<T> e;
+    KIWI_HD void set_wall(T ar0) { w = cubic_wall_t<T>(h, ar0); }
+    KIWI_HD void set_edge(T R_0) { e = cubic_edge_t<T>(w, R_0); }
+    KIWI_HD T at(T phi) const { return cubic_vertex_t<T>(w, e, phi); }
 };
+using CubicEval = CubicEvalT<double>;
 
 struct GenericEval {
     const KiwiKernelTable* K;
@@ -361,17 +380,22 @@ struct GenericEval {
 
 KIWI_HD double dmax2(double a, double b) { return a > b ? a : b; }
 KIWI_HD double dmin2(double a, double b) { return a < b ? a : b; }
+template <class T>
+KIWI_HD T vmax2(const T& a, const T& b) { return a > b ? a : b; }
+template <class T>
+KIWI_HD T vmin2(const T& a, const T& b) { return a < b ? a : b; }
 
 // Vertex source for the face walk: VX(i), VY(i), VZ(i) give vertex i of the face (n vertices, n >= 3).
 // face_integral_impl of src/kernel_integral.cpp:471-647, including the out_vert reachability rule.
-template <class Verts, class Eval>
-KIWI_HD double face_integral(double x0, double y0, double z0, double support_radius, const Verts& V, int n,
-                             int* out_vert, Eval& ev) {
+// T is the type of the particle's coordinates (the face's vertices are plain doubles): double, or Dual4
+// for the derivatives of the face integral with respect to the particle.
+template <class T, class Verts, class Eval>
+KIWI_HD T face_integral(T x0, T y0, T z0, T support_radius, const Verts& V, int n, int* out_vert, Eval& ev) {
     if (n < 3) {
         if (out_vert) *out_vert = 0;
-        return 0.0;
+        return T(0.0);
     }
-    double face_Msum = 0.0;
+    T face_Msum = 0.0;
     const double x1 = V.x(0), y1 = V.y(0), z1 = V.z(0);
     const double x2s = V.x(1), y2s = V.y(1), z2s = V.z(1);
     const double x3s = V.x(2), y3s = V.y(2), z3s = V.z(2);
@@ -380,38 +404,38 @@ KIWI_HD double face_integral(double x0, double y0, double z0, double support_rad
     const double C = (x2s - x1) * (y3s - y1) - (x3s - x1) * (y2s - y1);
     const double D = -A * x1 - B * y1 - C * z1;
     const double norm = sqrt(A * A + B * B + C * C);
-    const double r0 = (A * x0 + B * y0 + C * z0 + D) / norm;
-    const double ar0 = fabs(r0);
-    const double xp = x0 - r0 * A / norm;
-    const double yp = y0 - r0 * B / norm;
-    const double zp = z0 - r0 * C / norm;
-    const double x1r = x1 - x0, y1r = y1 - y0, z1r = z1 - z0;
-    const double x2sr = x2s - x0, y2sr = y2s - y0, z2sr = z2s - z0;
-    const double x3sr = x3s - x0, y3sr = y3s - y0, z3sr = z3s - z0;
-    const double s2 = x1r * (y2sr * z3sr - z2sr * y3sr) + y1r * (z2sr * x3sr - x2sr * z3sr) + z1r * (x2sr * y3sr - y2sr * x3sr);
+    const T r0 = (A * x0 + B * y0 + C * z0 + D) / norm;
+    const T ar0 = fabs(r0);
+    const T xp = x0 - r0 * A / norm;
+    const T yp = y0 - r0 * B / norm;
+    const T zp = z0 - r0 * C / norm;
+    const T x1r = x1 - x0, y1r = y1 - y0, z1r = z1 - z0;
+    const T x2sr = x2s - x0, y2sr = y2s - y0, z2sr = z2s - z0;
+    const T x3sr = x3s - x0, y3sr = y3s - y0, z3sr = z3s - z0;
+    const T s2 = x1r * (y2sr * z3sr - z2sr * y3sr) + y1r * (z2sr * x3sr - x2sr * z3sr) + z1r * (x2sr * y3sr - y2sr * x3sr);
     ev.set_wall(ar0);
     bool inside_polygon = true, have_sign = false;
-    double sign_ref = 0.0;
-    double min_edge_dist = INFINITY;
+    T sign_ref = 0.0;
+    T min_edge_dist = INFINITY;
     for (int j = 0; j < n; ++j) {
         const double x2 = V.x(j), y2 = V.y(j), z2 = V.z(j);
         const int jn = (j == n - 1) ? 0 : j + 1;
         const double x3 = V.x(jn), y3 = V.y(jn), z3 = V.z(jn);
         const double r23 = sqrt((x3 - x2) * (x3 - x2) + (y3 - y2) * (y3 - y2) + (z3 - z2) * (z3 - z2));
-        const double r12 = sqrt((xp - x2) * (xp - x2) + (yp - y2) * (yp - y2) + (zp - z2) * (zp - z2));
-        const double r13 = sqrt((xp - x3) * (xp - x3) + (yp - y3) * (yp - y3) + (zp - z3) * (zp - z3));
-        const double cosa = ((x3 - x2) * (xp - x2) + (y3 - y2) * (yp - y2) + (z3 - z2) * (zp - z2)) / r12 / r23;
-        const double R_0 = (fabs(cosa) < 1.0) ? r12 * sqrt(1 - cosa * cosa) : 0.0;
-        const double xpr = xp - x0, ypr = yp - y0, zpr = zp - z0;
-        const double x2r = x2 - x0, y2r = y2 - y0, z2r = z2 - z0;
-        const double x3r = x3 - x0, y3r = y3 - y0, z3r = z3 - z0;
-        const double s1 = xpr * (y2r * z3r - z2r * y3r) + ypr * (z2r * x3r - x2r * z3r) + zpr * (x2r * y3r - y2r * x3r);
-        const double phi1 = (R_0 < r12) ? acos(R_0 / r12) : 0.0;
-        const double phi2 = (R_0 < r13) ? acos(R_0 / r13) : 0.0;
+        const T r12 = sqrt((xp - x2) * (xp - x2) + (yp - y2) * (yp - y2) + (zp - z2) * (zp - z2));
+        const T r13 = sqrt((xp - x3) * (xp - x3) + (yp - y3) * (yp - y3) + (zp - z3) * (zp - z3));
+        const T cosa = ((x3 - x2) * (xp - x2) + (y3 - y2) * (yp - y2) + (z3 - z2) * (zp - z2)) / r12 / r23;
+        const T R_0 = (fabs(cosa) < 1.0) ? r12 * sqrt(1 - cosa * cosa) : T(0.0);
+        const T xpr = xp - x0, ypr = yp - y0, zpr = zp - z0;
+        const T x2r = x2 - x0, y2r = y2 - y0, z2r = z2 - z0;
+        const T x3r = x3 - x0, y3r = y3 - y0, z3r = z3 - z0;
+        const T s1 = xpr * (y2r * z3r - z2r * y3r) + ypr * (z2r * x3r - x2r * z3r) + zpr * (x2r * y3r - y2r * x3r);
+        const T phi1 = (R_0 < r12) ? acos(R_0 / r12) : T(0.0);
+        const T phi2 = (R_0 < r13) ? acos(R_0 / r13) : T(0.0);
         const double ex = x3 - x2, ey = y3 - y2, ez = z3 - z2;
-        const double tpx = xp - x2, tpy = yp - y2, tpz = zp - z2;
-        const double side = (ey * tpz - ez * tpy) * A + (ez * tpx - ex * tpz) * B + (ex * tpy - ey * tpx) * C;
-        const double side_eps = 1e-9 * norm * r23 * dmax2(dmax2(fabs(tpx), fabs(tpy)), dmax2(fabs(tpz), 1.0));
+        const T tpx = xp - x2, tpy = yp - y2, tpz = zp - z2;
+        const T side = (ey * tpz - ez * tpy) * A + (ez * tpx - ex * tpz) * B + (ex * tpy - ey * tpx) * C;
+        const T side_eps = 1e-9 * norm * r23 * vmax2(vmax2(fabs(tpx), fabs(tpy)), vmax2(fabs(tpz), T(1.0)));
         if (fabs(side) > side_eps) {
             if (!have_sign) {
                 sign_ref = side;
@@ -421,14 +445,14 @@ KIWI_HD double face_integral(double x0, double y0, double z0, double support_rad
             }
         }
         const bool foot_beyond_endpoint = (r12 * sin(phi1) >= r23) || (r13 * sin(phi2) >= r23);
-        const double in_plane_dist = foot_beyond_endpoint ? dmin2(r12, r13) : R_0;
-        min_edge_dist = dmin2(min_edge_dist, in_plane_dist);
-        double M = (s1 * s2 * r0 <= 0) ? -1.0 : 1.0;
+        const T in_plane_dist = foot_beyond_endpoint ? vmin2(r12, r13) : R_0;
+        min_edge_dist = vmin2(min_edge_dist, in_plane_dist);
+        T M = (s1 * s2 * r0 <= 0) ? T(-1.0) : T(1.0);
         ev.set_edge(R_0);
-        double I1v = 0.0, I2v = 0.0;
+        T I1v = 0.0, I2v = 0.0;
 #pragma unroll 1
         for (int v = 0; v < 2; ++v) {
-            const double t = ev.at(v == 0 ? phi1 : phi2);
+            const T t = ev.at(v == 0 ? phi1 : phi2);
             if (v == 0) I1v = t; else I2v = t;
         }
         if (foot_beyond_endpoint) {
@@ -439,7 +463,7 @@ KIWI_HD double face_integral(double x0, double y0, double z0, double support_rad
         face_Msum += M;
     }
     if (out_vert) {
-        const double face_dist = inside_polygon ? ar0 : sqrt(r0 * r0 + min_edge_dist * min_edge_dist);
+        const T face_dist = inside_polygon ? ar0 : sqrt(r0 * r0 + min_edge_dist * min_edge_dist);
         *out_vert = (face_dist >= support_radius) ? n : 0;
     }
     return face_Msum;
@@ -535,9 +559,9 @@ KIWI_HD unsigned box_face_pattern(int f) {
 
 // Msum of one box cell for one particle: the 6 faces summed in order, then the clamp of
 // src/cartesian_grid.cpp:256-269 (the caller counts the clamps).
-template <class Eval>
-KIWI_HD double box_cell_msum(double x0, double y0, double z0, double support, double cx, double cy, double cz,
-                             double hx, double hy, double hz, Eval& ev) {
+template <class T, class Eval>
+KIWI_HD T box_cell_msum(T x0, T y0, T z0, T support, double cx, double cy, double cz, double hx, double hy,
+                        double hz, Eval& ev) {
     BoxFace bf;
     bf.xm = cx - hx;
     bf.xp = cx + hx;
@@ -545,11 +569,11 @@ KIWI_HD double box_cell_msum(double x0, double y0, double z0, double support, do
     bf.yp = cy + hy;
     bf.zm = cz - hz;
     bf.zp = cz + hz;
-    double Msum = 0.0;
+    T Msum = 0.0;
 #pragma unroll 1
     for (int f = 0; f < 6; ++f) {
         bf.pat = box_face_pattern(f);
-        Msum += face_integral(x0, y0, z0, support, bf, 4, (int*)nullptr, ev);
+        Msum += face_integral<T>(x0, y0, z0, support, bf, 4, (int*)nullptr, ev);
     }
     return Msum;
 }

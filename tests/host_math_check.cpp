@@ -5,6 +5,7 @@
 #include <cstdint>
 
 #include "../kiwi_b200/csrc/kiwi_math.cuh"
+#include "../kiwi_b200/csrc/dual.cuh"
 
 using namespace kiwi_b200;
 
@@ -32,5 +33,21 @@ double hm_face_integral(double x0, double y0, double z0, int kernel, double h, d
 int hm_face_reachable(double x0, double y0, double z0, double support, const double* verts, int n) {
     FlatVerts V{verts};
     return face_reachable(x0, y0, z0, support, V, n) ? 1 : 0;
+}
+
+// One box cell's Msum for one particle (cubic spline, support 2h) by the double evaluation and by the
+// Dual4 evaluation of the adjoint: out[0] = double Msum, out[1] = Dual4 value, out[2..5] = d/dx0, d/dy0,
+// d/dz0, d/dh.
+void hm_cell_grad(double x0, double y0, double z0, double h, double cx, double cy, double cz, double hx, double hy,
+                  double hz, double* out) {
+    CubicEval ev;
+    ev.h = h;
+    out[0] = box_cell_msum(x0, y0, z0, 2 * h, cx, cy, cz, hx, hy, hz, ev);
+    CubicEvalT<Dual4> evd;
+    evd.h = Dual4::seed(h, 3);
+    const Dual4 X = Dual4::seed(x0, 0), Y = Dual4::seed(y0, 1), Z = Dual4::seed(z0, 2);
+    const Dual4 m = box_cell_msum<Dual4>(X, Y, Z, 2 * evd.h, cx, cy, cz, hx, hy, hz, evd);
+    out[1] = m.v;
+    for (int k = 0; k < 4; ++k) out[2 + k] = m.d[k];
 }
 }

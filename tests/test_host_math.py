@@ -27,6 +27,7 @@ def hm(tmp_path_factory):
     L.hm_face_integral.argtypes = [C.c_double] * 3 + [C.c_int, C.c_double, C.c_double, dp, C.c_int,
                                                       C.POINTER(C.c_int)]
     L.hm_face_reachable.argtypes = [C.c_double] * 4 + [dp, C.c_int]
+    L.hm_cell_grad.argtypes = [C.c_double] * 10 + [dp]
     return L
 
 
@@ -56,3 +57,42 @@ def test_face_walk_bit_identical(hm, oracle):
                 assert a == b and ov.value == ovo
                 reach = hm.hm_face_reachable(*p, 1.4 if k < 0 else 1.7, v.ctypes.data_as(C.POINTER(C.c_double)), 4)
                 assert reach == (ovo != 4)
+
+
+def test_dual_cell_gradient(hm, oracle):
+    """The adjoint's forward-mode evaluation of one cell's Msum (kiwi_b200/csrc/dual.cuh through the
+    templated face walk): its value equals the FP64 evaluation bit for bit, and its derivatives with
+    respect to x0, y0, z0, h agree with central differences of the exact (__float128) cell integral."""
+    from oracle.oracle import load_truth
+
+    truth = load_truth()
+    rng = np.random.default_rng(21)
+    bounds, n = [0.0, 1.0] * 3, 8
+    d = 1.0 / n
+    out = (C.c_double * 6)()
+    worst = 0.0
+    for _ in range(10):
+        h = 0.05 + 0.15 * rng.random()
+        th = np.array([*(0.2 + 0.6 * rng.random(3)), h])
+
+        def M(t):
+            P = dict(x=[t[0]], y=[t[1]], z=[t[2]], vx=[0.0], vy=[0.0], vz=[0.0], m=[1.0], h=[t[3]])
+            return truth.sph_to_grid(P, bounds, (n, n, n))[4][0]
+
+        fd = np.zeros((4, n ** 3))
+        for k in range(4):
+            step = 1e-6 * max(abs(th[k]), h)
+            a, b = th.copy(), th.copy()
+            a[k] += step
+            b[k] -= step
+            fd[k] = (M(a) - M(b)) / (2 * step)
+        g = np.zeros((4, n ** 3))
+        for c in np.nonzero(M(th))[0]:
+            ix, iy, iz = c // (n * n), (c // n) % n, c % n
+            hm.hm_cell_grad(*th, (ix + 0.5) * d, (iy + 0.5) * d, (iz + 0.5) * d, d / 2, d / 2, d / 2, out)
+            assert out[0] == out[1]
+            if out[1] > 0:
+                g[:, c] = out[2:]
+        worst = max(worst, (np.abs(g - fd) / np.abs(fd).max(axis=1, keepdims=True)).max())
+    assert worst < 1e-7, worst
+
