@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kiwi", choices=["kiwi", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_mixed", "fp64_reference_order"])
+    ap.add_argument("--precision", default="fp64",
+                    choices=["fp64", "fp32_mixed", "fp32_mixed_guaranteed", "fp64_reference_order"])
     ap.add_argument("--full-box", action="store_true",
                     help="evaluate every cell of each support bounding box, as the reference does")
     ap.add_argument("--n", type=int, default=2_000_000)
@@ -291,6 +292,22 @@ def main():
         job_ms, job_pairs, job_bbox = tot_ms, float(sph_pairs), float(bbox_pairs)
     value = job_pairs / (job_ms * 1e-3)
 
+    # accuracy of an FP32 form: against the FP64 form on the same input (untimed)
+    accuracy = None
+    if args.precision.startswith("fp32"):
+        ref = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
+        kiwi_b200.sph_to_grid_device(dP, bounds, shape, ref, kernel=ki, precision="fp64", ctx=ctx)
+        torch.cuda.synchronize()
+        r, g = ref["density"], out["density"]
+        msk = r >= 1e-6 * r.max()
+        rel = ((g[msk] - r[msk]).abs() / r[msk]).double()
+        accuracy = {"against": "the FP64 form (lattice), same input", "cells_above_1e-6_peak": int(msk.sum()),
+                    "max_rel_cell_err": float(rel.max()), "median_rel_cell_err": float(rel.median()),
+                    "q99_rel_cell_err": float(torch.quantile(rel[: 1 << 24].float(), 0.99)),
+                    "cells_over_1e-6": int((rel > 1e-6).sum()),
+                    "total_mass_rel_err": float(abs(g.sum() - r.sum()) / r.sum()),
+                    "cells_fp32_bound_over_1e-6": int(st["fp64_fallback"]), "fp64_tiles": int(st["fp64_tiles"])}
+
     # end to end through the public host API: pinned host arrays in, host arrays out
     e2e = None
     if args.e2e_steps > 0:
@@ -349,6 +366,8 @@ def main():
             "clocks": clk, "gpu_launches": int(launches), "wall_s_timed_region": wall,
             "e2e": e2e, "cpu_baseline": cpu,
         }
+        if accuracy is not None:
+            line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()

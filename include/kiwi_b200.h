@@ -38,7 +38,12 @@ extern "C" {
  * reference's per-cell evaluation order.
  * KIWI_FP64_REFERENCE_ORDER: all FP64 in the reference's per-cell evaluation order, operation by
  * operation (6 faces x 4 edges x 2 vertices per cell, src/kernel_integral.cpp:471-647).
- * KIWI_FP32_MIXED: FP32 bulk with FP64 islands and FP64 per-cell totals. */
+ * KIWI_FP32_MIXED (cubic spline with support 2h): the edge tiers and vertex pyramids of the lattice
+ * form in FP32, evaluated from FP64 plane offsets relative to the particle; the per-cell assembly and the
+ * per-cell totals in FP64.  Each cell also gets a bound on its rounding error (2 x 2^-24 x the summed
+ * magnitudes of the FP32 terms it was assembled from).  The closed form subtracts pyramid masses that
+ * can exceed the cell's mass by orders of magnitude, so the FP32 error grows with the support size in
+ * cells; fp64_fallback in KiwiStats counts the cells whose bound exceeds 1e-6 of their mass. */
 #define KIWI_FP64 0
 #define KIWI_FP32_MIXED 1
 #define KIWI_FP64_REFERENCE_ORDER 2
@@ -48,6 +53,10 @@ extern "C" {
  * radius are evaluated; the others hold no kernel mass and the reference's values for them are
  * rounding noise around zero (clamped at 0). */
 #define KIWI_FULL_BOX 0x100
+/* Flag for KIWI_FP32_MIXED: recompute in FP64 (lattice form) every 8x8x8 cell tile holding a cell whose
+ * mass is at least 1e-6 of the peak cell mass and whose FP32 rounding bound exceeds 1e-6 of its mass, so
+ * that those cells are within 1e-6 relative by construction.  KiwiStats.fp64_tiles counts the tiles. */
+#define KIWI_FP32_GUARANTEE 0x200
 
 typedef struct KiwiCtx KiwiCtx;
 
@@ -83,7 +92,7 @@ typedef struct KiwiStats {
     int64_t skipped_outside; /* particles whose support misses the grid (src/cartesian_grid.cpp:234-237) */
     int64_t neg_clamped;     /* pair integrals < 0 clamped to 0 (src/cartesian_grid.cpp:264-269) */
     int64_t neg_warned;      /* of those, <= -0.01 (the reference prints a warning for each) */
-    int64_t fp64_fallback;   /* FP32-mixed form: edges evaluated in FP64 */
+    int64_t fp64_fallback;   /* FP32-mixed form: cells whose FP32 rounding bound exceeds 1e-6 of their mass */
     int64_t tile_pairs;      /* (tile, particle) list entries built by the binning step */
     int64_t launches;        /* GPU kernels launched by this call */
     double gather_ms;        /* device time of the cell-integral kernel(s) of this call (CUDA events) */
@@ -91,6 +100,7 @@ typedef struct KiwiStats {
     /* work items of the lattice-factorised FP64 evaluation (0 for the other forms): edge tiers by the
      * distance of the edge line (beyond 2h, between h and 2h, within h) and vertex pyramids */
     int64_t edge_tiers_outer, edge_tiers_middle, edge_tiers_inner, vertex_pyramids;
+    int64_t fp64_tiles;      /* KIWI_FP32_GUARANTEE: cell tiles recomputed in FP64 */
 } KiwiStats;
 
 /* ---- context --------------------------------------------------------------------------------- */

@@ -28,7 +28,9 @@ LIB_PATH = os.environ.get("KIWI_B200_LIB") or os.path.join(HERE, "libkiwi_b200.s
 KIWI_FP64 = 0
 KIWI_FP32_MIXED = 1
 KIWI_FP64_REFERENCE_ORDER = 2
-PRECISIONS = {"fp64": KIWI_FP64, "fp32_mixed": KIWI_FP32_MIXED, "fp64_reference_order": KIWI_FP64_REFERENCE_ORDER}
+KIWI_FP32_GUARANTEE = 0x200
+PRECISIONS = {"fp64": KIWI_FP64, "fp32_mixed": KIWI_FP32_MIXED, "fp64_reference_order": KIWI_FP64_REFERENCE_ORDER,
+              "fp32_mixed_guaranteed": KIWI_FP32_MIXED | KIWI_FP32_GUARANTEE}
 
 KERNEL_KEYS = ["M4", "M5", "M6", "WC2", "WC4", "WC6"]
 KERNEL_NAMES = ["cubic_spline", "quartic_spline", "quintic_spline", "wendland_c2", "wendland_c4", "wendland_c6"]
@@ -68,7 +70,7 @@ class KiwiStats(C.Structure):
                 ("skipped_outside", C.c_int64), ("neg_clamped", C.c_int64), ("neg_warned", C.c_int64),
                 ("fp64_fallback", C.c_int64), ("tile_pairs", C.c_int64), ("launches", C.c_int64), ("gather_ms", C.c_double),
                 ("total_ms", C.c_double), ("edge_tiers_outer", C.c_int64), ("edge_tiers_middle", C.c_int64),
-                ("edge_tiers_inner", C.c_int64), ("vertex_pyramids", C.c_int64)]
+                ("edge_tiers_inner", C.c_int64), ("vertex_pyramids", C.c_int64), ("fp64_tiles", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -29,6 +29,7 @@ UNITS = [
     ("noalloc.cu", ["--fmad=false"]),
     ("voronoi.cu", ["--fmad=false"]),
     ("adjoint.cu", ["--fmad=false"]),
+    ("mixed.cu", []),
 ]
 
 

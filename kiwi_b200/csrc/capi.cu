@@ -196,8 +196,40 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     const int form = precision & KIWI_FORM_MASK;
     const bool full_box = (precision & KIWI_FULL_BOX) != 0;
+    int64_t fp64_tiles = 0;
+    if ((precision & KIWI_FP32_GUARANTEE) && form != KIWI_FP32_MIXED)
+        return set_err(ctx, KIWI_ERR_ARG, "KIWI_FP32_GUARANTEE applies to the FP32-mixed form only");
     if (form == KIWI_FP64 || form == KIWI_FP64_REFERENCE_ORDER) {
         KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl, out, d_stats, full_box, form == KIWI_FP64_REFERENCE_ORDER));
+    } else if (form == KIWI_FP32_MIXED) {
+        if (!kc.cubic)
+            return set_err(ctx, KIWI_ERR_UNSUPPORTED,
+                           "the FP32-mixed form is available for the cubic spline kernel with support 2h");
+        if (full_box) return set_err(ctx, KIWI_ERR_ARG, "KIWI_FULL_BOX is available with the FP64 forms only");
+        const bool guarantee = (precision & KIWI_FP32_GUARANTEE) != 0;
+        const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+        double *cerr = nullptr, *cmass = nullptr;
+        if (guarantee) {
+            KIWI_TRY(scratch_t(ctx, S_CELL_ERR, (size_t)ncell, &cerr));
+            KIWI_TRY(scratch_t(ctx, S_CELL_MASS, (size_t)ncell, &cmass));
+        }
+        KIWI_TRY(mixed_cart_gather(ctx, g, P, tl, out, cerr, cmass, d_stats));
+        if (guarantee) {
+            int32_t* map = nullptr;
+            int64_t* d_nmap = nullptr;
+            DevStats* d_st2 = nullptr;
+            KIWI_TRY(scratch_t(ctx, S_TILE_MAP, (size_t)ntiles, &map));
+            KIWI_TRY(scratch_t(ctx, S_MISC3, 1, &d_nmap));
+            KIWI_TRY(scratch_t(ctx, S_STATS2, 1, &d_st2));
+            KIWI_TRY(mixed_flag_tiles(ctx, g, cerr, cmass, 1e-6, 1e-6, map, d_nmap));
+            KIWI_CUDA(ctx, cudaMemcpyAsync(&fp64_tiles, d_nmap, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+            KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            KIWI_CUDA(ctx, cudaMemsetAsync(d_st2, 0, sizeof(DevStats), ctx->stream));
+            TileLists tl2 = tl;
+            tl2.map = map;
+            tl2.nmap = fp64_tiles;
+            KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl2, out, d_st2, false, false));
+        }
     } else {
         return set_err(ctx, KIWI_ERR_UNSUPPORTED, "precision %d is not available in this build", precision);
     }
@@ -223,6 +255,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         stats->edge_tiers_middle = (int64_t)hs.edge_middle;
         stats->edge_tiers_inner = (int64_t)hs.edge_inner;
         stats->vertex_pyramids = (int64_t)hs.vertex_pyramids;
+        stats->fp64_tiles = fp64_tiles;
     }
     return KIWI_OK;
 }

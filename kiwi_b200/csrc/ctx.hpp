@@ -16,7 +16,7 @@ struct KiwiCtx {
     std::string err;
     int64_t launches = 0;  // kernels launched on this context (for the stats of a call)
     // Scratch slots: each is grown on demand and reused by later calls on this context.
-    static constexpr int kSlots = 24;
+    static constexpr int kSlots = 32;
     void* slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Fixed arena mode (used only by the allocation-free entry point): when `arena` is set, scratch
@@ -127,6 +127,10 @@ enum ScratchSlot {
     S_VOR_NEXT,      // Voronoi walk: particle counter
     S_VOR_CSR,       // staged cell geometry (host entry point)
     S_VOR_HOME,      // staged home cells (host entry point)
+    S_CELL_ERR,      // FP32-mixed form: per-cell rounding bound
+    S_CELL_MASS,     // FP32-mixed form: per-cell raw mass
+    S_TILE_MAP,      // FP32-mixed form: tiles recomputed in FP64
+    S_STATS2,        // device counters of a second pass
 };
 
 }  // namespace kiwi_b200

@@ -30,6 +30,8 @@ struct TileLists {
     const uint32_t* list;
     const int64_t* range;
     int64_t ntiles;
+    const int32_t* map = nullptr;  // optional: run only tiles map[0 .. nmap) (device array)
+    int64_t nmap = 0;
 };
 
 struct CartOutputs {
@@ -53,6 +55,15 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
 // adjoint.cu
 int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc,
                      const double* d_cot, const AdjointOutputs& out, KiwiStats* stats);
+
+// mixed.cu: the FP32-mixed form (cubic spline).  cell_err (device, ncell doubles) receives each cell's
+// rounding-error bound and cell_mass (ncell doubles) its raw mass sum M.
+int mixed_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const TileLists& tl,
+                      const CartOutputs& out, double* cell_err, double* cell_mass, DevStats* d_stats);
+// Tiles holding a cell above floor_frac of the peak cell mass whose bound exceeds rel_tol of its mass:
+// writes their indices to map (ascending) and their count to *d_nmap (device).
+int mixed_flag_tiles(KiwiCtx* ctx, const CartGeom& g, const double* cell_err, const double* cell_mass,
+                     double rel_tol, double floor_frac, int32_t* map, int64_t* d_nmap);
 
 // voronoi.cu
 int voronoi_init_tables(KiwiCtx* ctx);

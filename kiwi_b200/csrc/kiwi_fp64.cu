@@ -257,15 +257,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
 constexpr int kLatMinBlocks = 2;
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 
-// Position of the smallest j with s_off[j] <= it among the chunk's np particles (s_off ascending).
-__device__ __forceinline__ int chunk_search(const int* s_off, int np, int it) {
-    int lo = 0, hi = np - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
 
 // One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
 // the edge and corner tables in shared memory.  Per chunk: (A) the edge tiers of every (plane, edge
@@ -276,6 +267,7 @@ template <bool CULL>
 __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGeom g, DevParticles P,
                                                                           const uint32_t* __restrict__ list,
                                                                           const int64_t* __restrict__ range,
+                                                                          const int32_t* __restrict__ tile_map,
                                                                           CartOutputs out, DevStats* __restrict__ st) {
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
         s_vy[kLatPMax], s_vz[kLatPMax];
@@ -288,7 +280,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
     double* s_D3 = s_dyn + kLatECap;
     double* s_S = s_dyn + 2 * kLatECap;
 
-    const int64_t t = blockIdx.x;
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -662,16 +654,21 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
                      bool reference_order) {
     if (tl.ntiles <= 0) return KIWI_OK;
     if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
-    const dim3 grid((unsigned)tl.ntiles);
+    if (tl.map && !(k.cubic && !reference_order))
+        return set_err(ctx, KIWI_ERR_ARG, "a tile subset is only supported by the lattice evaluation");
+    if (tl.map && tl.nmap <= 0) return KIWI_OK;
+    const dim3 grid((unsigned)(tl.map ? tl.nmap : tl.ntiles));
     if (k.cubic && !reference_order) {
         if (full_box) {
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
-            k_cart_lattice<false><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, out, d_stats);
+            k_cart_lattice<false><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
+                                                                                d_stats);
         } else {
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
-            k_cart_lattice<true><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, out, d_stats);
+            k_cart_lattice<true><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
+                                                                               d_stats);
         }
     } else if (k.cubic && !full_box)
         k_cart_gather<true, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);

@@ -59,6 +59,16 @@ static __device__ __noinline__ double lattice_vertex(double h, double r0, double
     return full_int;
 }
 
+// Position of the smallest j with s_off[j] <= it among the chunk's np particles (s_off ascending).
+static __device__ __forceinline__ int chunk_search(const int* s_off, int np, int it) {
+    int lo = 0, hi = np - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_off[mid] <= it) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 // Offset of lattice plane P (global plane index) from the particle coordinate x0 along one axis.
 __device__ __forceinline__ double lattice_offset(double mn, double d, int P, double x0) {
     return add_rn(mn, mul_rn((double)P, d)) - x0;
