@@ -40,8 +40,9 @@ extern "C" {
  * operation (6 faces x 4 edges x 2 vertices per cell, src/kernel_integral.cpp:471-647).
  * KIWI_FP32_MIXED (cubic spline with support 2h): the edge tiers and vertex pyramids of the lattice
  * form in FP32, evaluated from FP64 plane offsets relative to the particle; the per-cell assembly and the
- * per-cell totals in FP64.  Each cell also gets a bound on its rounding error (2 x 2^-24 x the summed
- * magnitudes of the FP32 terms it was assembled from).  The closed form subtracts pyramid masses that
+ * per-cell totals in FP64; planes within 1e-3 h of the particle in FP64 throughout.  Each cell also gets a
+ * bound on its rounding error (4 x 2^-24 x the summed magnitudes of the FP32 terms it was assembled
+ * from).  The closed form subtracts pyramid masses that
  * can exceed the cell's mass by orders of magnitude, so the FP32 error grows with the support size in
  * cells; fp64_fallback in KiwiStats counts the cells whose bound exceeds 1e-6 of their mass. */
 #define KIWI_FP64 0

@@ -34,10 +34,13 @@ constexpr int kMxPMax = 32;
 constexpr int kMxECap = 1536;  // edge entries per chunk (a full 8^3 particle box needs 486)
 constexpr int kMxSCap = 4096;  // corner entries per chunk (a full 8^3 particle box needs 2187)
 constexpr size_t kMxDynSmem = sizeof(float) * (4 * kMxECap + 2 * kMxSCap);
-// Rounding-error bound per unit of term magnitude: 2 x the FP32 unit roundoff (measured on the
-// lognormal-cube workload: |error| <= 0.5 x 2^-24 x magnitude for 99.9% of the pairs, and below
-// 2 x 2^-24 x magnitude for all of them).
-constexpr double kBoundScale = 2.0 * 5.9604644775390625e-08;
+// Rounding-error bound per unit of term magnitude: 4 x the FP32 unit roundoff 2^-24 (measured on 11M
+// pairs of the lognormal-cube workload: |error| <= 0.5 x 2^-24 x magnitude for 99.9% of the pairs and
+// <= 1.96 x 2^-24 x magnitude for all of them).
+constexpr double kBoundScale = 4.0 * 5.9604644775390625e-08;
+// FP64 islands: planes closer to the particle than this fraction of h are evaluated in FP64 (the wall
+// tier's (h/r0)^3 and the edge ratio a = R0/r0 grow without bound as r0 -> 0, beyond FP32's range).
+constexpr double kIslandFrac = 1e-3;
 
 __device__ __forceinline__ void add_stat(unsigned long long* dst, unsigned long long v) {
     if (v) atomicAdd(dst, v);
@@ -76,7 +79,7 @@ __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, 
     for (int c = 0; c < kMxCellsPerThread; ++c)
         acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = acc[c][4] = 0.0;
     unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0, n_vp = 0;
-    unsigned long long n_eo = 0, n_em = 0, n_ei = 0;
+    unsigned long long n_eo = 0, n_em = 0, n_ei = 0, n_island = 0;
     const int64_t beg = range[2 * t], end = range[2 * t + 1];
 
     for (int64_t pos = beg; pos < end;) {
@@ -151,7 +154,9 @@ __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, 
             const float h = s_h[j];
             MxEdge<float> ed;
             ed.D2 = ed.D3 = ed.A2 = ed.A3 = 0.0f;
-            if (r0 > 0.0f && R0 > 0.0f) ed = mixed::mx_edge(mixed::mx_wall(h, r0), R0);
+            // (an island plane's edge tiers are evaluated in FP64 by the corner pass itself)
+            if (r0 > 0.0f && R0 > 0.0f && !((double)r0 < kIslandFrac * s_hd[j]))
+                ed = mixed::mx_edge(mixed::mx_wall(h, r0), R0);
             s_D2[it] = ed.D2;
             s_D3[it] = ed.D3;
             s_A2[it] = ed.A2;
@@ -194,7 +199,18 @@ __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, 
             float f = 0.0f, fa = 0.0f;
             const float sg = fsgn(u1d) * fsgn(u2d);
             const float r0 = (float)fabs(r0d);
-            if (sg != 0.0f && r0 > 0.0f) {
+            if (sg != 0.0f && r0d != 0.0 && fabs(r0d) < kIslandFrac * s_hd[jp]) {
+                // FP64 island: the whole corner (its wall, both edge tiers and both vertex pyramids)
+                const double hd = s_hd[jp], a1 = fabs(u1d), a2 = fabs(u2d);
+                const MxWall<double> w = mixed::mx_wall(hd, fabs(r0d));
+                double ab1, ab2;
+                const double fd = mixed::mx_vertex(w, mixed::mx_edge(w, a1), a1, a2, &ab1) +
+                                  mixed::mx_vertex(w, mixed::mx_edge(w, a2), a2, a1, &ab2);
+                f = (float)fd;
+                // rounding scale: the FP32 storage of the value, plus the FP64 terms' own (2^-53, not 2^-24)
+                fa = 0.25f * fabsf(f) + (float)((ab1 + ab2) * 1e-9);
+                ++n_island;
+            } else if (sg != 0.0f && r0 > 0.0f) {
                 const float a1 = (float)fabs(u1d), a2 = (float)fabs(u2d);
                 const MxWall<float> w = mixed::mx_wall(s_h[jp], r0);
                 MxEdge<float> E1, E2;

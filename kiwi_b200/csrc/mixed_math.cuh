@@ -13,7 +13,7 @@
 //   u = a sin(phi) / sqrt(a^2 + cos^2 phi)       (= sin(phi) sqrt(1 - mu^2), mu = cos(phi) / sqrt(a^2 + cos^2))
 //   1 - u^2 = cos^2(phi) (1 + a^2) / (a^2 + cos^2)
 //   I1 = atan(u / a) = atan(sin(phi) / sqrt(a^2 + cos^2 phi))
-//   log((1 + u) / (1 - u)) = log1p(u) - log1p(-u)
+//   log((1 + u) / (1 - u)) = 2 log1p(u) - log(1 - u^2)
 //   B_k / r0^3 and the r0^3/h^3 prefactors taken as powers of q = r0 / h.
 // Every literal is converted to T, so T = float evaluates in FP32 throughout.
 #pragma once
@@ -37,6 +37,8 @@ template <class T>
 KIWI_MX T mx_atan(T x) { return atan(x); }
 template <class T>
 KIWI_MX T mx_log1p(T x) { return log1p(x); }
+template <class T>
+KIWI_MX T mx_log(T x) { return log(x); }
 template <>
 KIWI_MX float mx_sqrt<float>(float x) { return sqrtf(x); }
 template <>
@@ -45,6 +47,8 @@ template <>
 KIWI_MX float mx_atan<float>(float x) { return atanf(x); }
 template <>
 KIWI_MX float mx_log1p<float>(float x) { return log1pf(x); }
+template <>
+KIWI_MX float mx_log<float>(float x) { return logf(x); }
 
 // Wall tier of a plane at distance r0 > 0: q = r0/h and the B_k / r0^3 coefficients.
 template <class T>
@@ -95,7 +99,8 @@ KIWI_MX MxSeries<T> mx_series(T phi, T sinp, T cosp, T a) {
     const T u = a * sinp / rs;
     const T omu2 = cos2 * (T(1) + a2) / den;  // 1 - u^2
     const T tanp = sinp / cosp;
-    const T logs = mx_log1p(u) - mx_log1p(-u);
+    // log((1 + u) / (1 - u)) with 1 - u = (1 - u^2) / (1 + u): no cancellation as u -> 1
+    const T logs = T(2) * mx_log1p(u) - mx_log(omu2);
     s.I0 = phi;
     s.I_2 = phi + a2 * tanp;
     s.I_4 = phi + T(2) * a2 * tanp + T(1.0 / 3.0) * a2 * a2 * tanp * (T(2) + T(1) / cos2);

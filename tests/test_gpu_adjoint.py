@@ -70,7 +70,7 @@ def test_adjoint_matches_fd_of_gpu_forward(kiwi, ctx):
     assert st["evaluated_pairs"] > 0 and st["launches"] == 1
 
     def loss(P1):
-        r = kiwi.sph_to_grid(P1, bounds, shape, raw=True, ctx=ctx, precision="fp64_reference_order")
+        r = kiwi.sph_to_grid(P1, bounds, shape, raw=True, ctx=ctx, precision="fp64")
         return float(r.raw.reshape(-1) @ cot)
 
     worst = np.zeros(3)
