@@ -302,6 +302,7 @@ def main():
         msk = r >= 1e-6 * r.max()
         rel = ((g[msk] - r[msk]).abs() / r[msk]).double()
         accuracy = {"against": "the FP64 form (lattice), same input", "cells_above_1e-6_peak": int(msk.sum()),
+                    "nonfinite_cells": int((~torch.isfinite(g)).sum()),
                     "max_rel_cell_err": float(rel.max()), "median_rel_cell_err": float(rel.median()),
                     "q99_rel_cell_err": float(torch.quantile(rel[: 1 << 24].float(), 0.99)),
                     "cells_over_1e-6": int((rel > 1e-6).sum()),

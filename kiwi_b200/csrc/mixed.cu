@@ -149,14 +149,15 @@ __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, 
             const int p = e / n[bax], q = e % n[bax];
             const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
             const double pc[3] = {s_x[j], s_y[j], s_z[j]};
-            const float r0 = (float)fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
+            const double r0d = fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
+            const float r0 = (float)r0d;
             const float R0 = (float)fabs(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]));
             const float h = s_h[j];
             MxEdge<float> ed;
             ed.D2 = ed.D3 = ed.A2 = ed.A3 = 0.0f;
-            // (an island plane's edge tiers are evaluated in FP64 by the corner pass itself)
-            if (r0 > 0.0f && R0 > 0.0f && !((double)r0 < kIslandFrac * s_hd[j]))
-                ed = mixed::mx_edge(mixed::mx_wall(h, r0), R0);
+            // (an island plane's edge tiers are evaluated in FP64 by the corner pass itself; the island
+            // test is the corner pass's own, on the FP64 offset)
+            if (r0 > 0.0f && R0 > 0.0f && !(r0d < kIslandFrac * s_hd[j])) ed = mixed::mx_edge(mixed::mx_wall(h, r0), R0);
             s_D2[it] = ed.D2;
             s_D3[it] = ed.D3;
             s_A2[it] = ed.A2;

@@ -129,7 +129,8 @@ KIWI_MX MxEdge<T> mx_edge(const MxWall<T>& w, T R0) {
     const T a = R0 / r0;
     if (ld2 <= h * h) {
         const T rr = mx_sqrt(h * h - r0 * r0);
-        const T sq = mx_sqrt((rr - R0) * (rr + R0));
+        const T d = (rr - R0) * (rr + R0);  // >= 0 up to rounding (the line lies within h)
+        const T sq = mx_sqrt(d > T(0) ? d : T(0));
         const MxSeries<T> s = mx_series(mx_atan2(sq, R0), sq / rr, R0 / rr, a);
         const T t0 = T(-1.0 / 6.0) * s.I_2, t1 = T(0.25) * w.q * s.I_3, t2 = T(-0.15) * w.q2 * s.I_4,
                 t3 = T(1.0 / 30.0) * w.q3 * s.I_5, t4 = T(-1.0 / 60.0) * w.iq3 * s.I1, t5 = (w.b1 - w.b2) * s.I0;
@@ -137,7 +138,8 @@ KIWI_MX MxEdge<T> mx_edge(const MxWall<T>& w, T R0) {
         e.A2 = fabs(t0) + fabs(t1) + fabs(t2) + fabs(t3) + fabs(t4) + fabs(t5);
     }
     const T rr = mx_sqrt(T(4) * h * h - r0 * r0);
-    const T sq = mx_sqrt((rr - R0) * (rr + R0));
+    const T d = (rr - R0) * (rr + R0);  // >= 0 up to rounding (the line lies within 2h)
+    const T sq = mx_sqrt(d > T(0) ? d : T(0));
     const MxSeries<T> s = mx_series(mx_atan2(sq, R0), sq / rr, R0 / rr, a);
     const T t0 = T(1.0 / 3.0) * s.I_2, t1 = T(-0.25) * w.q * s.I_3, t2 = T(3.0 / 40.0) * w.q2 * s.I_4,
             t3 = T(-1.0 / 120.0) * w.q3 * s.I_5, t4 = T(4.0 / 15.0) * w.iq3 * s.I1, t5 = (w.b2 - w.b3) * s.I0;
