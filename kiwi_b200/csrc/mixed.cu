@@ -354,7 +354,7 @@ __global__ void k_max_mass(const double* __restrict__ M, int64_t n, unsigned lon
     if ((threadIdx.x & 31) == 0) atomicMax(peak_bits, (unsigned long long)__double_as_longlong(v));
 }
 
-// One thread per tile: 1 if a cell of the tile above floor_frac x peak has bound > rel_tol x mass.
+// One thread per tile: 1 if a cell of the tile that may lie above floor_frac x peak has bound > rel_tol x mass.
 __global__ void k_flag_tiles(CartGeom g, const double* __restrict__ E, const double* __restrict__ M,
                              const unsigned long long* __restrict__ peak_bits, double rel_tol, double floor_frac,
                              uint32_t* __restrict__ flags) {
@@ -370,8 +370,10 @@ __global__ void k_flag_tiles(CartGeom g, const double* __restrict__ E, const dou
                 const int ix = tx * kTileX + lx, iy = ty * kTileY + ly, iz = tz * kTileZ + lz;
                 if (ix >= g.nx || iy >= g.ny || iz >= g.nz) continue;
                 const int64_t i3 = ((int64_t)ix * g.ny + iy) * g.nz + iz;
-                const double m = M[i3];
-                if (m >= floor_m && m > 0.0 && E[i3] > rel_tol * m) {
+                // a cell counts if its mass can be at the floor or above (its FP32 mass plus the error
+                // bound), and fails if the bound exceeds rel_tol of its mass
+                const double m = M[i3], e = E[i3];
+                if (m + e >= floor_m && m + e > 0.0 && e > rel_tol * m) {
                     f = 1;
                     break;
                 }
