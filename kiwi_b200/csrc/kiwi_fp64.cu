@@ -397,10 +397,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
                 const double u1 = axis == 0 ? uy : ux, u2 = axis == 2 ? uy : uz;
                 const double h = s_h[jp];
                 const bool zero = ua == 0.0 || u1 == 0.0 || u2 == 0.0;
-                const bool needed = !CULL || lattice_needed(g, s_lo[jp], s_dim[jp], s_lo[jp][0] + i, s_lo[jp][1] + jj,
-                                                            s_lo[jp][2] + k, s_x[jp], s_y[jp], s_z[jp],
-                                                            mul_rn(g.support_in_h, h));
-                if (zero || !needed || !(ua * ua + (u1 * u1 + u2 * u2) < 4.0 * (h * h))) cheap |= 1u << q;
+                if (zero || !(ua * ua + (u1 * u1 + u2 * u2) < 4.0 * (h * h))) cheap |= 1u << q;
             }
             const int ncheap = __popc(cheap), nexp = nitems - ncheap;
             int ie = nexp, ic = ncheap;
@@ -462,11 +459,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
             }
             double f = 0.0;
             const double sg = sgn(u1) * sgn(u2);
-            // corners of no support cell are never read: left at 0
-            const bool needed = !CULL || lattice_needed(g, s_lo[jp], s_dim[jp], s_lo[jp][0] + i, s_lo[jp][1] + jj,
-                                                        s_lo[jp][2] + k, s_x[jp], s_y[jp], s_z[jp],
-                                                        mul_rn(g.support_in_h, s_h[jp]));
-            if (needed && sg != 0.0 && r0 != 0.0) {
+            if (sg != 0.0 && r0 != 0.0) {
                 const double a1 = fabs(u1), a2 = fabs(u2);
                 f = lattice_vertex(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1]) +
                     lattice_vertex(s_h[jp], r0, a2, a1, s_D2[e2], s_D3[e2]);

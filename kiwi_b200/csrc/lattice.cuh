@@ -74,21 +74,6 @@ __device__ __forceinline__ double lattice_offset(double mn, double d, int P, dou
     return add_rn(mn, mul_rn((double)P, d)) - x0;
 }
 
-// Whether lattice point (gi, gj, gk) (global plane indices) is a corner of some cell of the particle's
-// in-tile box [lo, lo + dim) whose closest point lies within the support radius -- the only cells whose
-// values are assembled.  The cells around the point form a box; its closest point to the particle is
-// tested against the radius with a relative margin, so rounding can only keep more points.
-static __device__ __forceinline__ bool lattice_needed(const CartGeom& g, const int* lo, const int* dim, int gi, int gj,
-                                                     int gk, double x0, double y0, double z0, double radius) {
-    const int ax0 = max(gi - 1, lo[0]), ax1 = min(gi, lo[0] + dim[0] - 1);
-    const int ay0 = max(gj - 1, lo[1]), ay1 = min(gj, lo[1] + dim[1] - 1);
-    const int az0 = max(gk - 1, lo[2]), az1 = min(gk, lo[2] + dim[2] - 1);
-    const double ex = fmax(fmax((g.x_min + ax0 * g.dpx) - x0, x0 - (g.x_min + (ax1 + 1) * g.dpx)), 0.0);
-    const double ey = fmax(fmax((g.y_min + ay0 * g.dpy) - y0, y0 - (g.y_min + (ay1 + 1) * g.dpy)), 0.0);
-    const double ez = fmax(fmax((g.z_min + az0 * g.dpz) - z0, z0 - (g.z_min + (az1 + 1) * g.dpz)), 0.0);
-    return ex * ex + ey * ey + ez * ez < radius * radius * (1.0 + 1e-9);
-}
-
 __device__ __forceinline__ double sgn(double v) { return (v > 0.0) ? 1.0 : ((v < 0.0) ? -1.0 : 0.0); }
 
 }  // namespace kiwi_b200

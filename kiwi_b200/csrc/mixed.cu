@@ -198,13 +198,8 @@ __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, 
                 e2 = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
             }
             float f = 0.0f, fa = 0.0f;
-            const float sg0 = fsgn(u1d) * fsgn(u2d);
+            const float sg = fsgn(u1d) * fsgn(u2d);
             const float r0 = (float)fabs(r0d);
-            // corners of no support cell are never read: left at 0
-            const bool needed = lattice_needed(g, s_lo[jp], s_dim[jp], s_lo[jp][0] + i, s_lo[jp][1] + jj,
-                                               s_lo[jp][2] + k, s_x[jp], s_y[jp], s_z[jp],
-                                               mul_rn(g.support_in_h, s_hd[jp]));
-            const float sg = needed ? sg0 : 0.0f;
             if (sg != 0.0f && r0d != 0.0 && fabs(r0d) < kIslandFrac * s_hd[jp]) {
                 // FP64 island: the whole corner (its wall, both edge tiers and both vertex pyramids)
                 const double hd = s_hd[jp], a1 = fabs(u1d), a2 = fabs(u2d);
