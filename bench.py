@@ -72,6 +72,16 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32-compare", action="store_true",
+                    help="with --precision fp64: skip timing the FP32-mixed form beside it")
+    ap.add_argument("--workload", default="lognormal", choices=["lognormal", "batch"],
+                    help="batch: many column snapshots of log-uniform sizes on grids of log-uniform resolution, "
+                         "kernels cycling M4 / M6 / WC4, in one persistent graph-recorded launch")
+    ap.add_argument("--batch-items", type=int, default=64)
+    ap.add_argument("--batch-nmin", type=int, default=10_000)
+    ap.add_argument("--batch-nmax", type=int, default=2_000_000)
+    ap.add_argument("--batch-resmin", type=int, default=64)
+    ap.add_argument("--batch-resmax", type=int, default=256)
     return ap.parse_args()
 
 
@@ -214,10 +224,91 @@ def run_reference(args):
     return 0
 
 
+def run_batch(args):
+    """Batched sph-to-grid: args.batch_items column snapshots (item i seeded 5000 + i), N log-uniform in
+    [nmin, nmax], grid res^3 with res log-uniform in [resmin, resmax], kernels cycling M4 / M6 / WC4; one
+    kiwi_batch_create, then timed graph replays.  Also times the same items as one sph-to-grid call each."""
+    import torch
+
+    import kiwi_b200
+    from kiwi_b200.workloads import column_snapshot
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5000)
+    kernels = ["cubic_spline", "quintic_spline", "wendland_c4"]
+    items, t_gen = [], time.perf_counter()
+    for i in range(args.batch_items):
+        n = int(round(np.exp(rng.uniform(np.log(args.batch_nmin), np.log(args.batch_nmax)))))
+        res = int(round(np.exp(rng.uniform(np.log(args.batch_resmin), np.log(args.batch_resmax)))))
+        kname = kernels[i % 3]
+        P, bounds = column_snapshot(n=n, seed=5000 + i, hfact=kiwi_b200.get_kernel(kname).hfact)
+        dP = {k: torch.from_numpy(v).to(dev) for k, v in P.items()}
+        nc = res ** 3
+        out = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
+        items.append({"particles": dP, "bounds": bounds, "shape": (res, res, res),
+                      "kernel": kiwi_b200.make_kernel_integrator(kname), "out": out, "n": n})
+    t_gen = time.perf_counter() - t_gen
+    ctx = kiwi_b200.Context(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch = kiwi_b200.Batch(items, precision=args.precision, ctx=ctx)
+    create_s = time.perf_counter() - t0
+    batch.run()
+    lpt, ctas = batch.tune()
+    for _ in range(max(args.warmup - 1, 0)):
+        batch.run()
+    peak_fp64 = kiwi_b200.measure_fp64_peak(ctx)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms, pairs, cells = [], 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        per, tot = batch.run()
+        ms.append(tot["gather_ms"])
+        pairs += tot["sphere_pairs"]
+    clk = clocks.stop()
+    ncells = sum(int(np.prod(it["shape"])) for it in items)
+    # the same items as one call each (the unbatched baseline)
+    torch.cuda.synchronize()
+    t_single, single_pairs = 0.0, 0
+    for it in items:
+        st = kiwi_b200.sph_to_grid_device(it["particles"], it["bounds"], it["shape"], it["out"], kernel=it["kernel"],
+                                          precision=args.precision, ctx=ctx)
+        t_single += st["total_ms"]
+        single_pairs += st["sphere_pairs"]
+    batch.close()
+    tot_ms = float(np.sum(ms))
+    line = {
+        "metric": "particle-cell integrals/s (support pairs), batched sph-to-grid", "value": pairs / (tot_ms * 1e-3),
+        "unit": "pair-integrals/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.batch_items} column snapshots (C1 recipe, seeds 5000+i), N log-uniform in "
+                               f"[{args.batch_nmin}, {args.batch_nmax}], grids res^3 with res log-uniform in "
+                               f"[{args.batch_resmin}, {args.batch_resmax}], kernels cycling M4/M6/WC4",
+                   "precision": args.precision, "particles": int(sum(it["n"] for it in items)), "cells": ncells,
+                   "l2": "flushed between timed steps (256 MB write)"},
+        "cells_per_s": ncells * args.steps / (tot_ms * 1e-3),
+        "pairs_per_step": pairs / args.steps,
+        "launch_shape": {"longest_first": lpt, "ctas_per_sm": ctas},
+        "plan_create_s": create_s, "generate_s": t_gen,
+        "unbatched": {"ms": t_single, "value": single_pairs / (t_single * 1e-3),
+                      "note": "the same items as one kiwi_sph_to_grid_device call each, binning included"},
+        "fp64_peak_tflops": peak_fp64, "clocks": clk, "gpu_launches": int(per[0]["launches"]) if per else 0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch":
+        return run_batch(args)
     ws, rank, local = dist_env()
     import torch
 
@@ -292,22 +383,52 @@ def main():
         job_ms, job_pairs, job_bbox = tot_ms, float(sph_pairs), float(bbox_pairs)
     value = job_pairs / (job_ms * 1e-3)
 
+    def fp32_accuracy(g, r, st_last):
+        """Per-cell and total-mass error of FP32-form densities g against FP64-form densities r."""
+        msk = r >= 1e-6 * r.max()
+        rel = ((g[msk] - r[msk]).abs() / r[msk]).double()
+        return {"against": "the FP64 form (lattice), same input", "cells_above_1e-6_peak": int(msk.sum()),
+                "nonfinite_cells": int((~torch.isfinite(g)).sum()),
+                "max_rel_cell_err": float(rel.max()), "median_rel_cell_err": float(rel.median()),
+                "q99_rel_cell_err": float(torch.quantile(rel[: 1 << 24].float(), 0.99)),
+                "cells_over_1e-6": int((rel > 1e-6).sum()),
+                "total_mass_rel_err": float(abs(g.sum() - r.sum()) / r.sum()),
+                "cells_fp32_bound_over_1e-6": int(st_last["fp64_fallback"]), "fp64_tiles": int(st_last["fp64_tiles"])}
+
     # accuracy of an FP32 form: against the FP64 form on the same input (untimed)
     accuracy = None
     if args.precision.startswith("fp32"):
         ref = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
         kiwi_b200.sph_to_grid_device(dP, bounds, shape, ref, kernel=ki, precision="fp64", ctx=ctx)
         torch.cuda.synchronize()
-        r, g = ref["density"], out["density"]
-        msk = r >= 1e-6 * r.max()
-        rel = ((g[msk] - r[msk]).abs() / r[msk]).double()
-        accuracy = {"against": "the FP64 form (lattice), same input", "cells_above_1e-6_peak": int(msk.sum()),
-                    "nonfinite_cells": int((~torch.isfinite(g)).sum()),
-                    "max_rel_cell_err": float(rel.max()), "median_rel_cell_err": float(rel.median()),
-                    "q99_rel_cell_err": float(torch.quantile(rel[: 1 << 24].float(), 0.99)),
-                    "cells_over_1e-6": int((rel > 1e-6).sum()),
-                    "total_mass_rel_err": float(abs(g.sum() - r.sum()) / r.sum()),
-                    "cells_fp32_bound_over_1e-6": int(st["fp64_fallback"]), "fp64_tiles": int(st["fp64_tiles"])}
+        accuracy = fp32_accuracy(out["density"], ref["density"], st)
+
+    # the FP32-mixed form timed beside the FP64 form (same input, same step protocol), with its error
+    # against this run's FP64 output: the FP32-mixed vs FP64 comparison of the metric
+    fp32_side = None
+    if args.precision == "fp64" and not args.no_fp32_compare and args.kernel == "cubic_spline" and not args.full_box:
+        o32 = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
+        for _ in range(min(args.warmup, 2)):
+            kiwi_b200.sph_to_grid_device(dP, bounds, shape, o32, kernel=ki, precision="fp32_mixed", ctx=ctx)
+        ms32, pairs32 = 0.0, 0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            st32 = kiwi_b200.sph_to_grid_device(dP, bounds, shape, o32, kernel=ki, precision="fp32_mixed", ctx=ctx)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ms32 += e0.elapsed_time(e1)
+            pairs32 += st32["sphere_pairs"]
+        acc32 = fp32_accuracy(o32["density"], out["density"], st32)
+        v32 = pairs32 / (ms32 * 1e-3)
+        fp32_side = {"precision": "fp32_mixed", "value": v32 * ws, "unit": "pair-integrals/s",
+                     "ms_per_step": ms32 / args.steps, "ratio_vs_fp64": v32 / (tot_ms and sph_pairs / (tot_ms * 1e-3)),
+                     "meets_1e-6_per_cell": acc32["max_rel_cell_err"] <= 1e-6, "accuracy": acc32}
+        del o32
 
     # end to end through the public host API: pinned host arrays in, host arrays out
     e2e = None
@@ -369,6 +490,8 @@ def main():
         }
         if accuracy is not None:
             line["accuracy"] = accuracy
+        if fp32_side is not None:
+            line["fp32_mixed"] = fp32_side
         print(json.dumps(line), flush=True)
     if ws > 1:
         dist.barrier()

@@ -184,6 +184,35 @@ int kiwi_sph_to_grid_device_noalloc(void* stream, const KiwiParticles* particles
                                     double* vy, double* vz, double* raw4, KiwiStats* stats, char* err,
                                     size_t err_len);
 
+/* ---- batches of sph-to-grid problems (no counterpart in the reference) ----------------------- */
+/* Many snapshots, each mapped onto its own grid with its own kernel, in one persistent launch recorded
+ * as a CUDA graph.  The reference maps one snapshot per run; a caller with many (a time series, a
+ * parameter sweep, a set of zoom regions) would otherwise pay one launch sequence per snapshot and leave
+ * the GPU idle on the small ones.  Every pointer of an item is in device memory. */
+typedef struct KiwiBatchItem {
+    KiwiParticles particles;
+    KiwiCartGrid grid;
+    KiwiKernelSel kernel;
+    double *density, *vx, *vy, *vz; /* outputs, ncells each (any may be NULL) */
+    double* raw4;                   /* optional raw sums, 4 * ncells */
+} KiwiBatchItem;
+typedef struct KiwiBatch KiwiBatch;
+
+/* Bins every item's particles into the cell tiles of its grid (one scan and one sort over all items),
+ * orders the tiles longest-first, and records the graph.  precision: KIWI_FP64 (lattice form for the
+ * cubic closed form, the reference's evaluation order for the generic kernels) or
+ * KIWI_FP64_REFERENCE_ORDER; no flags.  The plan holds the tile lists of the particles' positions and
+ * smoothing lengths at creation: masses and velocities may change between runs, positions and smoothing
+ * lengths may not.  Results equal kiwi_sph_to_grid_device's for each item, bit for bit. */
+int kiwi_batch_create(KiwiCtx* ctx, const KiwiBatchItem* items, int n_items, int precision, KiwiBatch** out);
+/* Replays the graph on the context's stream and waits for it.  item_stats (n_items entries) and total
+ * may be NULL; gather_ms / total_ms hold the device time of the whole batch. */
+int kiwi_batch_run(KiwiBatch* batch, KiwiStats* item_stats, KiwiStats* total);
+/* Times the launch shapes (longest-first or natural tile order x 1 or 2 resident CTAs per SM; one run
+ * each) and keeps the fastest; *chosen = 0x100 if longest-first, | CTAs per SM. */
+int kiwi_batch_tune(KiwiBatch* batch, int* chosen);
+void kiwi_batch_destroy(KiwiBatch* batch);
+
 /* ---- Voronoi map stage (run_mapping_stage's particle loop, src/mapping.cpp:105-206, 400-502) --- */
 /* Cell geometry in CSR form: the plain data of CellFaceGeometry (src/mapping.cpp:49-54) with vertex
  * coordinates made absolute as src/mapping.cpp:168-175 does and neighbour ids resolved to cell indices. */

@@ -76,6 +76,11 @@ class KiwiStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class KiwiBatchItem(C.Structure):
+    _fields_ = [("particles", KiwiParticles), ("grid", KiwiCartGrid), ("kernel", KiwiKernelSel),
+                ("density", _dp), ("vx", _dp), ("vy", _dp), ("vz", _dp), ("raw4", _dp)]
+
+
 class KiwiVoronoiCells(C.Structure):
     _fields_ = [("n_cells", C.c_int64), ("face_off", _i64p), ("vert_off", _i64p), ("vxyz", _dp),
                 ("face_nbr", _i32p), ("volume", _dp)]
@@ -112,6 +117,10 @@ def load_library(path: str = LIB_PATH):
     L.kiwi_sph_to_grid_adjoint_device.argtypes = ([C.c_void_p, C.POINTER(KiwiParticles), C.POINTER(KiwiCartGrid),
                                                    C.POINTER(KiwiKernelSel), _dp] + [_dp] * 8 +
                                                   [C.POINTER(KiwiStats)])
+    L.kiwi_batch_create.argtypes = [C.c_void_p, C.POINTER(KiwiBatchItem), C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+    L.kiwi_batch_run.argtypes = [C.c_void_p, C.POINTER(KiwiStats), C.POINTER(KiwiStats)]
+    L.kiwi_batch_tune.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    L.kiwi_batch_destroy.argtypes = [C.c_void_p]
     L.kiwi_map_voronoi.argtypes = [C.c_void_p, C.POINTER(KiwiParticles), _i32p, C.POINTER(KiwiVoronoiCells),
                                    C.POINTER(KiwiKernelSel), C.c_int, _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
     _lib = L
@@ -406,6 +415,61 @@ def sph_to_grid_adjoint_device(particles: dict, bounds, shape, raw4_cot, grads: 
     ctx.check(ctx._L.kiwi_sph_to_grid_adjoint_device(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
                                                      dp(raw4_cot), *outs, C.byref(st)), "sph-to-grid adjoint")
     return st.as_dict()
+
+
+class Batch:
+    """Many sph-to-grid problems in one persistent, graph-recorded launch (kiwi_batch_create / run /
+    tune / destroy; no counterpart in the reference).  `items` is a list of dicts with `particles` (CUDA
+    float64 tensors x y z vx vy vz m h), `bounds`, `shape`, optional `kernel` (KernelIntegrator) and `out`
+    (CUDA float64 tensors density vx vy vz [raw4]).  The tensors must stay alive while the batch is used;
+    positions and smoothing lengths must not change after creation."""
+
+    def __init__(self, items, precision="fp64", ctx=None):
+        self.ctx = ctx or default_context()
+        self._keep = []
+        arr = (KiwiBatchItem * len(items))()
+
+        def dp(t):
+            return C.cast(C.c_void_p(int(t.data_ptr())), _dp) if t is not None else None
+
+        for i, it in enumerate(items):
+            Ps, _ = _particles_struct(it["particles"], device=True)
+            nx, ny, nz = (int(v) for v in it["shape"])
+            grid = KiwiCartGrid((C.c_double * 6)(*[float(b) for b in it["bounds"]]), nx, ny, nz)
+            sel = (it.get("kernel") or KernelIntegrator()).sel()
+            out = it.get("out", {})
+            arr[i] = KiwiBatchItem(Ps, grid, sel, dp(out.get("density")), dp(out.get("vx")), dp(out.get("vy")),
+                                   dp(out.get("vz")), dp(out.get("raw4")))
+            self._keep.append((it["particles"], out))
+        self.n_items = len(items)
+        h = C.c_void_p()
+        self.ctx.check(self.ctx._L.kiwi_batch_create(self.ctx.handle, arr, len(items),
+                                                     precision_code(precision), C.byref(h)), "batch create")
+        self._h = h
+
+    def run(self):
+        """Runs the batch; returns (per-item stats, total stats)."""
+        st = (KiwiStats * self.n_items)()
+        tot = KiwiStats()
+        self.ctx.check(self.ctx._L.kiwi_batch_run(self._h, st, C.byref(tot)), "batch run")
+        return [s.as_dict() for s in st], tot.as_dict()
+
+    def tune(self):
+        """Times the launch shapes and keeps the fastest; returns (longest_first, ctas_per_sm)."""
+        c = C.c_int(0)
+        self.ctx.check(self.ctx._L.kiwi_batch_tune(self._h, C.byref(c)), "batch tune")
+        return bool(c.value & 0x100), c.value & 0xff
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.ctx._L.kiwi_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 @dataclass

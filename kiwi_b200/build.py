@@ -30,6 +30,7 @@ UNITS = [
     ("voronoi.cu", ["--fmad=false"]),
     ("adjoint.cu", ["--fmad=false"]),
     ("mixed.cu", []),
+    ("batch.cu", ["--fmad=false"]),
 ]
 
 

@@ -11,70 +11,12 @@
 #include "../../include/kiwi_b200.h"
 #include "engine.hpp"
 #include "kernel_tables.h"
+#include "binning.cuh"
 #include "prims.cuh"
 
 using namespace kiwi_b200;
 
 namespace {
-
-// ------------------------------------------------------------------ binning kernels
-
-struct TileBox {
-    int x0, x1, y0, y1, z0, z1;  // inclusive tile ranges
-};
-
-// Per particle: the number of cell tiles its clamped support box touches (0 if none).
-__global__ void k_tile_counts(CartGeom g, DevParticles P, uint32_t* __restrict__ counts, TileBox* __restrict__ boxes,
-                              DevStats* __restrict__ st) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long outside_count = 0;
-    if (i < P.n) {
-        CellBox b;
-        bool outside = false;
-        uint32_t c = 0;
-        TileBox tb{0, -1, 0, -1, 0, -1};
-        if (particle_cell_box(g, P.x[i], P.y[i], P.z[i], P.h[i], b, &outside)) {
-            tb.x0 = b.x0 / kTileX; tb.x1 = b.x1 / kTileX;
-            tb.y0 = b.y0 / kTileY; tb.y1 = b.y1 / kTileY;
-            tb.z0 = b.z0 / kTileZ; tb.z1 = b.z1 / kTileZ;
-            c = (uint32_t)((tb.x1 - tb.x0 + 1) * (tb.y1 - tb.y0 + 1) * (tb.z1 - tb.z0 + 1));
-        }
-        if (outside) outside_count = 1;
-        counts[i] = c;
-        boxes[i] = tb;
-    }
-    for (int o = 16; o > 0; o >>= 1) outside_count += __shfl_down_sync(0xffffffffu, outside_count, o);
-    if ((threadIdx.x & 31) == 0 && outside_count) atomicAdd(&st->skipped_outside, outside_count);
-}
-
-// One thread per (particle, tile) entry: key = tile id, value = particle index, written in particle
-// order (the offsets are the exclusive scan of the counts).
-__global__ void k_tile_emit(CartGeom g, int64_t n, const int64_t* __restrict__ offs, const TileBox* __restrict__ boxes,
-                            int64_t total, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= total) return;
-    // particle = last p with offs[p] <= k
-    int64_t lo = 0, hi = n - 1;
-    while (lo < hi) {
-        const int64_t mid = (lo + hi + 1) >> 1;
-        if (offs[mid] <= k) lo = mid; else hi = mid - 1;
-    }
-    const TileBox tb = boxes[lo];
-    const int64_t q = k - offs[lo];
-    const int dz = tb.z1 - tb.z0 + 1, dy = tb.y1 - tb.y0 + 1;
-    const int tz = tb.z0 + (int)(q % dz), ty = tb.y0 + (int)((q / dz) % dy), tx = tb.x0 + (int)(q / ((int64_t)dz * dy));
-    keys[k] = (uint32_t)(((int64_t)tx * g.nty + ty) * g.ntz + tz);
-    vals[k] = (uint32_t)lo;
-}
-
-// range[2t], range[2t+1] = [begin, end) of tile t in the sorted key array (zero-length if absent).
-__global__ void k_tile_ranges(const uint32_t* __restrict__ keys, int64_t total, int64_t* __restrict__ range) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= total) return;
-    const uint32_t k = keys[i];
-    if (i == 0 || keys[i - 1] != k) range[2 * (int64_t)k] = i;
-    if (i == total - 1 || keys[i + 1] != k) range[2 * (int64_t)k + 1] = i + 1;
-}
 
 }  // namespace
 
@@ -180,7 +122,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
     KIWI_TRY(scratch_t(ctx, S_VALS1, (size_t)std::max<int64_t>(total, 1), &v1));
     const uint32_t* sorted_vals = v0;
     if (total > 0) {
-        k_tile_emit<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(g, n, offs, boxes, total, k0, v0);
+        k_tile_emit<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(g, n, offs, boxes, 0, total, 0u, k0, v0);
         KIWI_LAUNCHED(ctx);
         int key_bits = 1;
         while ((1LL << key_bits) < ntiles) ++key_bits;

@@ -56,6 +56,26 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
 int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc,
                      const double* d_cot, const AdjointOutputs& out, KiwiStats* stats);
 
+// One grid of a batch (batch.cu): its geometry, particles and outputs, how its tiles are evaluated,
+// and where its tiles start in the batch's concatenated tile lists.
+enum BatchMode { kBatchLattice = 0, kBatchGatherCubic = 1, kBatchGatherGeneric = 2 };
+struct BatchItemDev {
+    CartGeom g;
+    DevParticles P;
+    CartOutputs out;
+    int kernel;
+    int mode;
+    int64_t tile_base;
+    DevStats* st;
+};
+
+// kiwi_fp64.cu: one persistent launch over the tiles of every item of a batch, taken in the order
+// order[0 .. ntiles) (null: ascending) from the work counter *next (zero before the launch).
+int fp64_batch_prepare(KiwiCtx* ctx);
+int fp64_batch_gather(KiwiCtx* ctx, const BatchItemDev* d_items, const int32_t* d_item_of_tile, const int32_t* d_order,
+                      int64_t ntiles, const uint32_t* list, const int64_t* range, unsigned long long* d_next,
+                      int blocks);
+
 // mixed.cu: the FP32-mixed form (cubic spline).  cell_err (device, ncell doubles) receives each cell's
 // rounding-error bound and cell_mass (ncell doubles) its raw mass sum M.
 int mixed_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const TileLists& tl,

@@ -74,11 +74,15 @@ __device__ __forceinline__ void decode_pair(int k, int np, const int* s_start, c
     iz = bz + s_lo[j][2] + qz;
 }
 
-template <bool CUBIC, bool CULL>
-__global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g, DevParticles P, int kernel,
-                                                          const uint32_t* __restrict__ list,
-                                                          const int64_t* __restrict__ range, CartOutputs out,
-                                                          DevStats* __restrict__ st) {
+// The work of one CTA on one cell tile: t is the tile's index in its grid (its cell coordinates), t_range
+// its entry in range[] (the same unless the tile lists of several grids are concatenated).  With
+// RUNTIME_CUBIC the closed form is chosen by cubic_rt instead of CUBIC (one instance serves both, so a
+// kernel that needs both keeps one copy of the tile's shared memory).
+template <bool CUBIC, bool CULL, bool RUNTIME_CUBIC = false>
+__device__ __forceinline__ void gather_tile(const CartGeom& g, const DevParticles& P, int kernel,
+                                            const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
+                                            int64_t t_range, int64_t t, const CartOutputs& out,
+                                            DevStats* __restrict__ st, bool cubic_rt = false) {
     static_assert(kChunkCap / kThreads <= 32, "per-thread keep mask is 32 bits");
     __shared__ double s_x[kPMax], s_y[kPMax], s_z[kPMax], s_h[kPMax], s_m[kPMax], s_vx[kPMax], s_vy[kPMax],
         s_vz[kPMax];
@@ -88,7 +92,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
     __shared__ unsigned short s_list[kChunkCap];
     __shared__ double s_R[kChunkCap];
 
-    const int64_t t = blockIdx.x;
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -98,7 +101,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
 
     unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
-    const int64_t beg = range[2 * t], end = range[2 * t + 1];
+    const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
     const double sup_in_h = g.support_in_h;
 
     for (int64_t pos = beg; pos < end;) {
@@ -192,8 +195,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
             const double cy = cell_centre(g.y_min, iy, g.dpy);
             const double cz = cell_centre(g.z_min, iz, g.dpz);
             ++n_eval;
-            double msum = pair_msum<CUBIC>(kernel, x0, y0, z0, h, CUBIC ? 2 * h : radius, cx, cy, cz, g.hpx, g.hpy,
-                                           g.hpz);
+            double msum;
+            if (RUNTIME_CUBIC ? cubic_rt : CUBIC)
+                msum = pair_msum<true>(kernel, x0, y0, z0, h, 2 * h, cx, cy, cz, g.hpx, g.hpy, g.hpz);
+            else
+                msum = pair_msum<false>(kernel, x0, y0, z0, h, radius, cx, cy, cz, g.hpx, g.hpy, g.hpz);
             if (msum < 0.0) {
                 ++n_neg;
                 if (msum <= -0.01) ++n_warn;
@@ -252,6 +258,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
     add_stat(&st->neg_warned, n_warn);
 }
 
+template <bool CUBIC, bool CULL>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g, DevParticles P, int kernel,
+                                                          const uint32_t* __restrict__ list,
+                                                          const int64_t* __restrict__ range, CartOutputs out,
+                                                          DevStats* __restrict__ st) {
+    gather_tile<CUBIC, CULL>(g, P, kernel, list, range, blockIdx.x, blockIdx.x, out, st);
+}
+
 // ------------------------------------------------------------------ lattice-factorised gather (cubic)
 
 constexpr int kLatMinBlocks = 2;
@@ -264,11 +278,10 @@ constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 // assembles the cells it owns from the corner values, particle by particle in list order, and adds them
 // to its accumulators -- the same fixed per-cell summation order as k_cart_gather, no atomics.
 template <bool CULL>
-__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGeom g, DevParticles P,
-                                                                          const uint32_t* __restrict__ list,
-                                                                          const int64_t* __restrict__ range,
-                                                                          const int32_t* __restrict__ tile_map,
-                                                                          CartOutputs out, DevStats* __restrict__ st) {
+__device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
+                                             const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
+                                             int64_t t_range, int64_t t, const CartOutputs& out,
+                                             DevStats* __restrict__ st) {
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
         s_vy[kLatPMax], s_vz[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
@@ -280,7 +293,6 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
     double* s_D3 = s_dyn + kLatECap;
     double* s_S = s_dyn + 2 * kLatECap;
 
-    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
     unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
     unsigned long long n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0;
-    const int64_t beg = range[2 * t], end = range[2 * t + 1];
+    const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
 
     for (int64_t pos = beg; pos < end;) {
         if (warp == 0) {
@@ -552,6 +564,43 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
     add_stat(&st->vertex_pyramids, n_vp);
 }
 
+template <bool CULL>
+__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGeom g, DevParticles P,
+                                                                          const uint32_t* __restrict__ list,
+                                                                          const int64_t* __restrict__ range,
+                                                                          const int32_t* __restrict__ tile_map,
+                                                                          CartOutputs out, DevStats* __restrict__ st) {
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    lattice_tile<CULL>(g, P, list, range, t, t, out, st);
+}
+
+// A batch of grids in one persistent launch: each CTA takes the next tile from the work counter and runs
+// the tile body its item asks for (the same bodies as the single-grid kernels, so every cell's value and
+// summation order are those of a single-grid call).
+__global__ void __launch_bounds__(kThreads, 2) k_batch_persistent(const BatchItemDev* __restrict__ items,
+                                                                 const int32_t* __restrict__ item_of_tile,
+                                                                 const int32_t* __restrict__ order, int64_t ntiles,
+                                                                 const uint32_t* __restrict__ list,
+                                                                 const int64_t* __restrict__ range,
+                                                                 unsigned long long* __restrict__ next) {
+    __shared__ long long s_w;
+    for (;;) {
+        if (threadIdx.x == 0) s_w = (long long)atomicAdd(next, 1ull);
+        __syncthreads();
+        const int64_t w = s_w;
+        if (w >= ntiles) break;
+        const int64_t tg = order ? (int64_t)order[w] : w;
+        const BatchItemDev& it = items[item_of_tile[tg]];
+        const int64_t tl = tg - it.tile_base;
+        if (it.mode == kBatchLattice)
+            lattice_tile<true>(it.g, it.P, list, range, tg, tl, it.out, it.st);
+        else
+            gather_tile<false, true, true>(it.g, it.P, it.kernel, list, range, tg, tl, it.out, it.st,
+                                           it.mode == kBatchGatherCubic);
+        __syncthreads();
+    }
+}
+
 __global__ void k_full_integral(int kernel, int64_t n, const double* __restrict__ arg0, const double* __restrict__ phi,
                                 const double* __restrict__ r0, const double* __restrict__ R0, double* __restrict__ out) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -678,6 +727,22 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
         k_cart_gather<false, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
     else
         k_cart_gather<false, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+    KIWI_LAUNCHED(ctx);
+    return KIWI_OK;
+}
+
+int fp64_batch_prepare(KiwiCtx* ctx) {
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kLatDynSmem));
+    return KIWI_OK;
+}
+
+int fp64_batch_gather(KiwiCtx* ctx, const BatchItemDev* d_items, const int32_t* d_item_of_tile, const int32_t* d_order,
+                      int64_t ntiles, const uint32_t* list, const int64_t* range, unsigned long long* d_next,
+                      int blocks) {
+    if (ntiles <= 0) return KIWI_OK;
+    k_batch_persistent<<<blocks, kThreads, kLatDynSmem, ctx->stream>>>(d_items, d_item_of_tile, d_order, ntiles, list,
+                                                                       range, d_next);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

@@ -1,0 +1,105 @@
+"""Batches (kiwi_batch_create / run / tune): many snapshots on their own grids with their own kernels in
+one persistent, graph-recorded launch.  Each item's output must equal a single-grid call of the same
+form bit for bit (the batch runs the same tile bodies with the same per-cell particle order)."""
+import numpy as np
+import pytest
+
+from conftest import random_particles
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+KEYS = ("x", "y", "z", "vx", "vy", "vz", "m", "h")
+
+
+def _items(kiwi):
+    rng = np.random.default_rng(77)
+    specs = [
+        (600, (16, 16, 16), "cubic_spline", 0.02, 0.25),
+        (50, (9, 20, 7), "quintic_spline", 0.05, 0.3),
+        (0, (8, 8, 8), "cubic_spline", 0.05, 0.2),          # empty snapshot
+        (300, (24, 12, 12), "wendland_c4", 0.03, 0.2),
+        (40, (5, 5, 5), "cubic_spline", 0.05, 0.1),         # every particle outside the grid (below)
+        (1500, (32, 32, 32), "cubic_spline", 0.01, 0.15),
+    ]
+    items = []
+    for i, (n, shape, kname, hmin, hmax) in enumerate(specs):
+        P = random_particles(n, seed=100 + i, hmin=hmin, hmax=hmax)
+        if i == 4:
+            P["x"] = P["x"] + 10.0
+        b = (0.0, 2.0, -0.1, 2.0, 0.05, 1.9)
+        dP = {k: torch.tensor(np.asarray(P[k], dtype=np.float64), device="cuda") for k in KEYS}
+        nc = int(np.prod(shape))
+        out = {k: torch.full((nc,), float(rng.normal()), dtype=torch.float64, device="cuda")
+               for k in ("density", "vx", "vy", "vz")}
+        out["raw4"] = torch.full((4 * nc,), -1.0, dtype=torch.float64, device="cuda")
+        items.append({"particles": dP, "bounds": b, "shape": shape, "kernel": kiwi.make_kernel_integrator(kname),
+                      "out": out})
+    return items
+
+
+def _single(kiwi, ctx, it, precision):
+    nc = int(np.prod(it["shape"]))
+    out = {k: torch.empty(nc, dtype=torch.float64, device="cuda") for k in ("density", "vx", "vy", "vz")}
+    out["raw4"] = torch.empty(4 * nc, dtype=torch.float64, device="cuda")
+    st = kiwi.sph_to_grid_device(it["particles"], it["bounds"], it["shape"], out, kernel=it["kernel"],
+                                 precision=precision, ctx=ctx)
+    return out, st
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reference_order"])
+def test_batch_equals_single_calls(kiwi, ctx, precision):
+    items = _items(kiwi)
+    batch = kiwi.Batch(items, precision=precision, ctx=ctx)
+    try:
+        for rep in range(2):
+            per, tot = batch.run()
+            torch.cuda.synchronize()
+            for i, it in enumerate(items):
+                ref, st = _single(kiwi, ctx, it, precision)
+                for k in ("density", "vx", "vy", "vz", "raw4"):
+                    assert torch.equal(it["out"][k], ref[k]), (rep, i, k)
+                for k in ("bbox_pairs", "sphere_pairs", "evaluated_pairs", "skipped_outside", "neg_clamped",
+                          "tile_pairs", "vertex_pyramids"):
+                    assert per[i][k] == st[k], (rep, i, k, per[i][k], st[k])
+            assert tot["sphere_pairs"] == sum(p["sphere_pairs"] for p in per)
+            assert per[4]["skipped_outside"] == 40 and per[2]["sphere_pairs"] == 0
+        # the launch-shape tuning keeps the results
+        lpt, ctas = batch.tune()
+        assert ctas in (1, 2)
+        for it in items:
+            for k in it["out"]:
+                it["out"][k].fill_(123.0)
+        batch.run()
+        torch.cuda.synchronize()
+        for i, it in enumerate(items):
+            ref, _ = _single(kiwi, ctx, it, precision)
+            assert torch.equal(it["out"]["density"], ref["density"]), i
+    finally:
+        batch.close()
+
+
+def test_batch_masses_may_change_between_runs(kiwi, ctx):
+    items = _items(kiwi)[:2]
+    batch = kiwi.Batch(items, ctx=ctx)
+    try:
+        batch.run()
+        items[0]["particles"]["m"].mul_(2.0)
+        batch.run()
+        torch.cuda.synchronize()
+        ref, _ = _single(kiwi, ctx, items[0], "fp64")
+        assert torch.equal(items[0]["out"]["density"], ref["density"])
+    finally:
+        batch.close()
+
+
+def test_batch_rejects_bad_arguments(kiwi, ctx):
+    items = _items(kiwi)[:1]
+    with pytest.raises(kiwi.KiwiError):
+        kiwi.Batch(items, precision="fp32_mixed", ctx=ctx)
+    bad = dict(items[0])
+    bad["bounds"] = (1.0, 0.0, 0.0, 1.0, 0.0, 1.0)
+    with pytest.raises(kiwi.KiwiError):
+        kiwi.Batch([bad], ctx=ctx)
+    with pytest.raises(kiwi.KiwiError):
+        kiwi.Batch([], ctx=ctx)
