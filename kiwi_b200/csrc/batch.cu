@@ -140,7 +140,8 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
         d.out = CartOutputs{it.density, it.vx, it.vy, it.vz, it.raw4, nullptr};
         d.kernel = kc.kernel;
         const int form = b->precision & KIWI_FORM_MASK;
-        d.mode = !kc.cubic ? kBatchGatherGeneric : (form == KIWI_FP64 ? kBatchLattice : kBatchGatherCubic);
+        if (form == KIWI_FP64) d.mode = kc.cubic ? kBatchLattice : kBatchLatticeGeneric;
+        else d.mode = kc.cubic ? kBatchGatherCubic : kBatchGatherGeneric;
         d.tile_base = b->tile_base[i];
         b->tile_base[i + 1] = b->tile_base[i] + (int64_t)d.g.ntx * d.g.nty * d.g.ntz;
         pbase[i + 1] = pbase[i] + it.particles.n;

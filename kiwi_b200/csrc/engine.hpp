@@ -58,7 +58,7 @@ int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, con
 
 // One grid of a batch (batch.cu): its geometry, particles and outputs, how its tiles are evaluated,
 // and where its tiles start in the batch's concatenated tile lists.
-enum BatchMode { kBatchLattice = 0, kBatchGatherCubic = 1, kBatchGatherGeneric = 2 };
+enum BatchMode { kBatchLattice = 0, kBatchGatherCubic = 1, kBatchGatherGeneric = 2, kBatchLatticeGeneric = 3 };
 struct BatchItemDev {
     CartGeom g;
     DevParticles P;

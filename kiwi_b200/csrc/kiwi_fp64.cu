@@ -270,6 +270,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
 
 constexpr int kLatMinBlocks = 2;
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
+constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatSCap);
+constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;
 
 
 // One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
@@ -277,11 +279,14 @@ constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 // line) of every particle's box, (B) the corner values of every (plane, lattice point), (C) each thread
 // assembles the cells it owns from the corner values, particle by particle in list order, and adds them
 // to its accumulators -- the same fixed per-cell summation order as k_cart_gather, no atomics.
-template <bool CULL>
+// GENERIC: the table-driven tiers of kernel `kernel` (support radius support_in_h x h) instead of the
+// cubic closed form; the edge tiers are then lattice_generic_edge records and the corner items run in
+// their natural order.
+template <bool CULL, bool GENERIC = false>
 __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
                                              const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
                                              int64_t t_range, int64_t t, const CartOutputs& out,
-                                             DevStats* __restrict__ st) {
+                                             DevStats* __restrict__ st, int kernel = 0) {
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
         s_vy[kLatPMax], s_vz[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
@@ -291,7 +296,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     extern __shared__ double s_dyn[];
     double* s_D2 = s_dyn;
     double* s_D3 = s_dyn + kLatECap;
-    double* s_S = s_dyn + 2 * kLatECap;
+    double* s_S = s_dyn + (GENERIC ? kLatGenERec * kLatGenECap : 2 * kLatECap);
+    double* s_E = s_dyn;  // generic edge records
+    constexpr int kECap = GENERIC ? kLatGenECap : kLatECap;
+    const KiwiKernelTable* K = &c_tables[kernel];
 
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
@@ -332,7 +340,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     is += vs;
                 }
             }
-            const bool take = (idx < end) && ie <= kLatECap && is <= kLatSCap;
+            const bool take = (idx < end) && ie <= kECap && is <= kLatSCap;
             const int np = __popc(__ballot_sync(0xffffffffu, take));
             if (take) {
                 s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph;
@@ -374,6 +382,11 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const double pc[3] = {s_x[j], s_y[j], s_z[j]};
             const double r0 = fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
             const double R0 = fabs(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]));
+            if (GENERIC) {
+                lattice_generic_edge(K, mul_rn(g.support_in_h, s_h[j]), r0, R0, s_E + kLatGenERec * it);
+                ++n_ei;
+                continue;
+            }
             const CubicWall w = cubic_wall(s_h[j], r0);
             const CubicEdge ed = cubic_edge(w, R0);
             s_D2[it] = ed.D2;
@@ -388,7 +401,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         // (B0) order the corner items so that the cheap ones (corner beyond 2h: only I0 and I1; or a zero
         // corner) run in warps of their own: the others from the front of s_blist, the cheap ones from
         // the back.  Results do not depend on this order.
-        {
+        if (!GENERIC) {
             unsigned cheap = 0;
             int nitems = 0;
 #pragma unroll
@@ -442,7 +455,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
 
         // (B) corner values S_a(i, j, k) for the three plane orientations a
         for (int li = threadIdx.x; li < stot; li += kThreads) {
-            const int it = s_blist[li];
+            const int it = GENERIC ? li : s_blist[li];
             const int jp = chunk_search(s_soff, np, it);
             const int s = it - s_soff[jp];
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
@@ -473,8 +486,14 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const double sg = sgn(u1) * sgn(u2);
             if (sg != 0.0 && r0 != 0.0) {
                 const double a1 = fabs(u1), a2 = fabs(u2);
-                f = lattice_vertex(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1]) +
-                    lattice_vertex(s_h[jp], r0, a2, a1, s_D2[e2], s_D3[e2]);
+                if (GENERIC) {
+                    const double H = mul_rn(g.support_in_h, s_h[jp]);
+                    f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
+                        lattice_generic_vertex(K, H, r0, a2, a1, s_E + kLatGenERec * e2);
+                } else {
+                    f = lattice_vertex(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1]) +
+                        lattice_vertex(s_h[jp], r0, a2, a1, s_D2[e2], s_D3[e2]);
+                }
                 n_vp += 2;
             }
             s_S[it] = sg * f;
@@ -574,6 +593,15 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
     lattice_tile<CULL>(g, P, list, range, t, t, out, st);
 }
 
+// The lattice form for the generic kernels (support cells only).
+__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_generic(CartGeom g, DevParticles P, int kernel,
+                                                                                  const uint32_t* __restrict__ list,
+                                                                                  const int64_t* __restrict__ range,
+                                                                                  CartOutputs out,
+                                                                                  DevStats* __restrict__ st) {
+    lattice_tile<true, true>(g, P, list, range, blockIdx.x, blockIdx.x, out, st, kernel);
+}
+
 // A batch of grids in one persistent launch: each CTA takes the next tile from the work counter and runs
 // the tile body its item asks for (the same bodies as the single-grid kernels, so every cell's value and
 // summation order are those of a single-grid call).
@@ -594,6 +622,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_persistent(const BatchIte
         const int64_t tl = tg - it.tile_base;
         if (it.mode == kBatchLattice)
             lattice_tile<true>(it.g, it.P, list, range, tg, tl, it.out, it.st);
+        else if (it.mode == kBatchLatticeGeneric)
+            lattice_tile<true, true>(it.g, it.P, list, range, tg, tl, it.out, it.st, it.kernel);
         else
             gather_tile<false, true, true>(it.g, it.P, it.kernel, list, range, tg, tl, it.out, it.st,
                                            it.mode == kBatchGatherCubic);
@@ -719,6 +749,11 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
             k_cart_lattice<true><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
                                                                                d_stats);
         }
+    } else if (!k.cubic && !reference_order && !full_box) {
+        KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_generic, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kLatGenDynSmem));
+        k_cart_lattice_generic<<<grid, kThreads, kLatGenDynSmem, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out,
+                                                                                d_stats);
     } else if (k.cubic && !full_box)
         k_cart_gather<true, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
     else if (k.cubic)
@@ -733,7 +768,7 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
 
 int fp64_batch_prepare(KiwiCtx* ctx) {
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kLatDynSmem));
+                                        (int)kLatMaxDynSmem));
     return KIWI_OK;
 }
 
@@ -741,7 +776,7 @@ int fp64_batch_gather(KiwiCtx* ctx, const BatchItemDev* d_items, const int32_t* 
                       int64_t ntiles, const uint32_t* list, const int64_t* range, unsigned long long* d_next,
                       int blocks) {
     if (ntiles <= 0) return KIWI_OK;
-    k_batch_persistent<<<blocks, kThreads, kLatDynSmem, ctx->stream>>>(d_items, d_item_of_tile, d_order, ntiles, list,
+    k_batch_persistent<<<blocks, kThreads, kLatMaxDynSmem, ctx->stream>>>(d_items, d_item_of_tile, d_order, ntiles, list,
                                                                        range, d_next);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;

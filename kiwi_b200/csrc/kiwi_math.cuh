@@ -212,8 +212,8 @@ struct GenericEdge {
 
 // I_i(phi) = int_0^phi mu^i dphi', i = 1, 0, -1, ..., imin, stored at out[1 - i]
 // (src/kernel_integral_generic.cpp:19-66).
-KIWI_HD void generic_basis(double a, double a2, double phi, int imin, double* out) {
-    const double sinp = sin(phi), cosp = cos(phi);
+// With sin(phi) and cos(phi) given (the lattice form knows them from the legs of its right triangles).
+KIWI_HD void generic_basis_sc(double a, double a2, double phi, double sinp, double cosp, int imin, double* out) {
     const double den = a2 + cosp * cosp;
     const double u = a * sinp / sqrt(den);
     const double one_minus_u2 = cosp * cosp * (1.0 + a2) / den;
@@ -254,6 +254,11 @@ KIWI_HD void generic_basis(double a, double a2, double phi, int imin, double* ou
             out[1 + 2 * k] = sum;
         }
     }
+}
+
+KIWI_HD void generic_basis(double a, double a2, double phi, int imin, double* out) {
+    const double sinp = sin(phi), cosp = cos(phi);
+    generic_basis_sc(a, a2, phi, sinp, cosp, imin, out);
 }
 
 KIWI_HD int generic_region(const KiwiKernelTable* K, double q) {

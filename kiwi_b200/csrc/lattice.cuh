@@ -69,6 +69,68 @@ static __device__ __forceinline__ int chunk_search(const int* s_off, int np, int
     return lo;
 }
 
+// ---- generic kernels (table-driven tiers, src/kernel_integral_generic.cpp) in the lattice form
+//
+// The edge tier of a generic kernel is the list of the kernel's regions crossed along the edge line, with
+// the angles where it leaves each region and the continuity offsets (generic_edge, :119-148).  Its lattice
+// record packs that as 7 doubles: [0] = nseg + 8 x first region, [1..3] = phi_end of segments 0..2,
+// [4..6] = offset of segments 1..3 (segment 0's is 0; the last segment ends at pi/2).
+constexpr int kLatGenERec = 7;
+constexpr int kLatGenECap = 640;  // edge records per chunk (a full 8^3 particle box needs 486)
+
+static __device__ __forceinline__ void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0, double R0,
+                                                           double* rec) {
+    for (int i = 0; i < kLatGenERec; ++i) rec[i] = 0.0;
+    if (r0 == 0.0 || R0 == 0.0) return;
+    GenericWall w;
+    GenericEdge e;
+    generic_wall(w, K, H, r0);
+    generic_edge(e, w, R0);
+    rec[0] = (double)(e.nseg + 8 * e.region[0]);
+    for (int s = 0; s + 1 < e.nseg && s < 3; ++s) rec[1 + s] = e.phi_end[s];
+    for (int s = 1; s < e.nseg && s < 4; ++s) rec[3 + s] = e.offset[s];
+}
+
+// Vertex tier of a generic kernel for the right triangle with legs R0 (projection -> edge line) and t
+// (along the edge) in a wall at distance r0 (generic_vertex, :150-156, at phi = atan2(t, R0)): the region
+// segment holding phi, its offset, and G_k(phi) = bphi_k phi + sum_i coef_k,i I_i(phi) with the wall
+// coefficients A3 a_k,i (r0/H)^i formed on the fly (powers by running product).
+static __device__ __noinline__ double lattice_generic_vertex(const KiwiKernelTable* K, double H, double r0, double R0,
+                                                            double t, const double* rec) {
+    const int packed = (int)rec[0];
+    const int nseg = packed & 7, k0 = packed >> 3;
+    if (nseg == 0 || t == 0.0) return 0.0;
+    const double a = R0 / r0, a2 = a * a;
+    const double rr = sqrt(R0 * R0 + t * t);
+    const double phi = atan2(t, R0);
+    const double sinp = t / rr, cosp = R0 / rr;
+    int s = 0;
+    while (s + 1 < nseg && phi > rec[1 + s]) ++s;
+    const int k = k0 + s;
+    const double q0 = r0 / H;
+    const int j = generic_region(K, q0);
+    int imin = 1;
+    for (int idx = KIWI_NI - 1; idx >= 0; --idx)
+        if (K->a[k - 1][idx] != 0.0) {
+            imin = 1 - idx;
+            break;
+        }
+    double I[KIWI_NI];
+    generic_basis_sc(a, a2, phi, sinp, cosp, imin, I);
+    const double A3 = K->A3_pi / kPi;
+    double b = 0.0;
+    if (k >= j)
+        for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
+    double sum = (A3 * b) * phi;
+    double qp = 1.0;
+    for (int idx = 0; idx < KIWI_NI; ++idx) {
+        const double c = K->a[k - 1][idx];
+        if (c != 0.0) sum += (A3 * c * qp) * I[idx];
+        qp *= q0;
+    }
+    return (s > 0 ? rec[3 + s] : 0.0) + sum;
+}
+
 // Offset of lattice plane P (global plane index) from the particle coordinate x0 along one axis.
 __device__ __forceinline__ double lattice_offset(double mn, double d, int P, double x0) {
     return add_rn(mn, mul_rn((double)P, d)) - x0;
