@@ -94,7 +94,7 @@ static __device__ __forceinline__ void lattice_generic_edge(const KiwiKernelTabl
 // Vertex tier of a generic kernel for the right triangle with legs R0 (projection -> edge line) and t
 // (along the edge) in a wall at distance r0 (generic_vertex, :150-156, at phi = atan2(t, R0)): the region
 // segment holding phi, its offset, and G_k(phi) = bphi_k phi + sum_i coef_k,i I_i(phi) with the wall
-// coefficients A3 a_k,i (r0/H)^i formed on the fly (powers by running product).
+// coefficients A3 a_k,i (r0/H)^i formed on the fly.
 static __device__ __noinline__ double lattice_generic_vertex(const KiwiKernelTable* K, double H, double r0, double R0,
                                                             double t, const double* rec) {
     const int packed = (int)rec[0];
@@ -122,11 +122,17 @@ static __device__ __noinline__ double lattice_generic_vertex(const KiwiKernelTab
     if (k >= j)
         for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
     double sum = (A3 * b) * phi;
-    double qp = 1.0;
+    // q0^idx as a compensated running product (hi + lo, the product's rounding error carried exactly by
+    // fma): the terms can cancel heavily, and a plain running product's rounding (up to ~idx ulp)
+    // measurably raised the error of low-density cells; this is within an ulp, like pow, at a fraction
+    // of its cost
+    double ph = 1.0, pl = 0.0;
     for (int idx = 0; idx < KIWI_NI; ++idx) {
         const double c = K->a[k - 1][idx];
-        if (c != 0.0) sum += (A3 * c * qp) * I[idx];
-        qp *= q0;
+        if (c != 0.0) sum += (A3 * c * (ph + pl)) * I[idx];
+        const double nh = ph * q0;
+        pl = fma(pl, q0, fma(ph, q0, -nh));
+        ph = nh;
     }
     return (s > 0 ? rec[3 + s] : 0.0) + sum;
 }
