@@ -185,8 +185,8 @@ int kiwi_sph_to_grid_device_noalloc(void* stream, const KiwiParticles* particles
                                     size_t err_len);
 
 /* ---- batches of sph-to-grid problems (no counterpart in the reference) ----------------------- */
-/* Many snapshots, each mapped onto its own grid with its own kernel, in one persistent launch recorded
- * as a CUDA graph.  The reference maps one snapshot per run; a caller with many (a time series, a
+/* Many snapshots, each mapped onto its own grid with its own kernel, in one persistent launch per
+ * evaluation family (cubic lattice, generic lattice, per-cell gather) recorded as one CUDA graph.  The reference maps one snapshot per run; a caller with many (a time series, a
  * parameter sweep, a set of zoom regions) would otherwise pay one launch sequence per snapshot and leave
  * the GPU idle on the small ones.  Every pointer of an item is in device memory. */
 typedef struct KiwiBatchItem {

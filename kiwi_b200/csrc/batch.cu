@@ -1,11 +1,13 @@
 // Batches of independent sph-to-grid problems (many snapshots, each on its own grid, with any kernel) in
-// one persistent launch, replayed as a CUDA graph.
+// one persistent launch per tile-body family, replayed as a CUDA graph.
 //
 // kiwi_batch_create bins every item's particles into its own grid's cell tiles with one shared key space
 // (item i's tiles follow item i-1's), so a single scan and a single stable sort build every tile list at
-// once; it then orders the tiles longest-first (by their (tile, particle) entry count, ties by tile index)
-// and records one CUDA graph: per-item counter resets and mean velocities, then k_batch_persistent, whose
-// CTAs pull tiles from a work counter and run the same tile bodies as the single-grid kernels.  Every cell
+// once; it groups the tiles by the tile body their item needs (cubic lattice, generic lattice, per-cell
+// gather), orders each group longest-first (by (tile, particle) entry count, ties by tile index) and
+// records one CUDA graph: counter resets and per-item mean velocities, then one k_batch_persistent launch
+// per group, whose CTAs pull tiles from a work counter and run the same tile bodies as the single-grid
+// kernels.  Every cell
 // is therefore summed in the same particle order with the same arithmetic as a single-grid call of the
 // same form: the batch's outputs equal the per-item outputs bit for bit.  kiwi_batch_run replays the graph.
 // kiwi_batch_tune times the launch shapes (tile order x resident CTAs per SM) and keeps the fastest.
@@ -30,10 +32,13 @@ struct KiwiBatch {
     std::vector<void*> allocs;
     BatchItemDev* d_items = nullptr;
     int32_t* d_item_of_tile = nullptr;
-    int32_t* d_order = nullptr;  // longest-first tile order
+    // per tile-body family: its tiles in natural (item, tile) order and longest-first, and its counter
+    int32_t* d_natural[kBatchFamilies] = {};
+    int32_t* d_lpt[kBatchFamilies] = {};
+    int64_t fam_tiles[kBatchFamilies] = {};
     const uint32_t* d_list = nullptr;
     int64_t* d_range = nullptr;
-    unsigned long long* d_next = nullptr;
+    unsigned long long* d_next = nullptr;  // kBatchFamilies counters
     DevStats* d_stats = nullptr;  // per item
     double* d_meanv = nullptr;    // 4 per item
     std::vector<BatchItemDev> items;
@@ -57,14 +62,16 @@ __global__ void k_gather_i64(const int64_t* __restrict__ src, const int64_t* __r
     if (i < n) dst[i] = src[idx[i]];
 }
 
-// Longest-first sort keys: ~entries (ascending key = descending entry count), value = tile index.
-__global__ void k_tile_weights(const int64_t* __restrict__ range, int64_t n, uint32_t* __restrict__ keys,
-                               uint32_t* __restrict__ vals) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+// Longest-first sort keys for the tiles tiles[0 .. n): ~entries (ascending key = descending entry count),
+// value = tile index.
+__global__ void k_tile_weights(const int64_t* __restrict__ range, const int32_t* __restrict__ tiles, int64_t n,
+                               uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n) return;
+    const int64_t t = tiles[w];
     const int64_t e = range[2 * t + 1] - range[2 * t];
-    keys[t] = 0xffffffffu - (uint32_t)(e < 0xffffffffLL ? e : 0xffffffffLL);
-    vals[t] = (uint32_t)t;
+    keys[w] = 0xffffffffu - (uint32_t)(e < 0xffffffffLL ? e : 0xffffffffLL);
+    vals[w] = (uint32_t)t;
 }
 
 template <class T>
@@ -89,14 +96,16 @@ void batch_free(KiwiBatch* b) {
     b->allocs.clear();
 }
 
-// The replayed work: reset the counters, the mean velocities, the persistent gather.
+// The replayed work: reset the counters, the mean velocities, one persistent launch per family present.
 int batch_enqueue(KiwiBatch* b) {
     KiwiCtx* ctx = b->ctx;
-    KIWI_CUDA(ctx, cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long), ctx->stream));
+    KIWI_CUDA(ctx, cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long) * kBatchFamilies, ctx->stream));
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_stats, 0, sizeof(DevStats) * b->n_items, ctx->stream));
     for (int i = 0; i < b->n_items; ++i) KIWI_TRY(fp64_mean_velocity(ctx, b->items[i].P, b->d_meanv + 4 * i));
-    return fp64_batch_gather(ctx, b->d_items, b->d_item_of_tile, b->lpt ? b->d_order : nullptr, b->n_tiles, b->d_list,
-                             b->d_range, b->d_next, b->sms * b->ctas_per_sm);
+    for (int f = 0; f < kBatchFamilies; ++f)
+        KIWI_TRY(fp64_batch_gather(ctx, f, b->d_items, b->d_item_of_tile, b->lpt ? b->d_lpt[f] : b->d_natural[f],
+                                   b->fam_tiles[f], b->d_list, b->d_range, b->d_next + f, b->sms * b->ctas_per_sm));
+    return KIWI_OK;
 }
 
 int batch_record(KiwiBatch* b) {
@@ -154,11 +163,24 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
 
     KIWI_TRY(balloc(b, (size_t)n, &b->d_stats));
     KIWI_TRY(balloc(b, (size_t)4 * n, &b->d_meanv));
-    KIWI_TRY(balloc(b, 1, &b->d_next));
+    KIWI_TRY(balloc(b, kBatchFamilies, &b->d_next));
     KIWI_TRY(balloc(b, (size_t)n, &b->d_items));
     KIWI_TRY(balloc(b, (size_t)b->n_tiles, &b->d_item_of_tile));
-    KIWI_TRY(balloc(b, (size_t)b->n_tiles, &b->d_order));
     KIWI_TRY(balloc(b, (size_t)2 * b->n_tiles, &b->d_range));
+    // each family's tiles in natural order (the tile ranges of its items, in item order)
+    std::vector<int32_t> nat[kBatchFamilies];
+    for (int i = 0; i < n; ++i) {
+        std::vector<int32_t>& v = nat[batch_family(b->items[i].mode)];
+        for (int64_t t = b->tile_base[i]; t < b->tile_base[i + 1]; ++t) v.push_back((int32_t)t);
+    }
+    for (int f = 0; f < kBatchFamilies; ++f) {
+        b->fam_tiles[f] = (int64_t)nat[f].size();
+        KIWI_TRY(balloc(b, nat[f].size(), &b->d_natural[f]));
+        KIWI_TRY(balloc(b, nat[f].size(), &b->d_lpt[f]));
+        if (!nat[f].empty())
+            KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_natural[f], nat[f].data(), sizeof(int32_t) * nat[f].size(),
+                                           cudaMemcpyHostToDevice, ctx->stream));
+    }
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_stats, 0, sizeof(DevStats) * n, ctx->stream));
     for (int i = 0; i < n; ++i) {
         b->items[i].st = b->d_stats + i;
@@ -243,12 +265,16 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
         k_fill_i32<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(b->d_item_of_tile + b->tile_base[i], nt, i);
         KIWI_LAUNCHED(ctx);
     }
-    k_tile_weights<<<(unsigned)((b->n_tiles + 255) / 256), 256, 0, ctx->stream>>>(b->d_range, b->n_tiles, k0, v0);
-    KIWI_LAUNCHED(ctx);
-    bool second = false;
-    KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, b->n_tiles, 32, &second));
-    KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_order, second ? v1 : v0, sizeof(int32_t) * b->n_tiles,
-                                   cudaMemcpyDeviceToDevice, ctx->stream));
+    for (int f = 0; f < kBatchFamilies; ++f) {
+        const int64_t nf = b->fam_tiles[f];
+        if (nf <= 0) continue;
+        k_tile_weights<<<(unsigned)((nf + 255) / 256), 256, 0, ctx->stream>>>(b->d_range, b->d_natural[f], nf, k0, v0);
+        KIWI_LAUNCHED(ctx);
+        bool second = false;
+        KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, nf, 32, &second));
+        KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_lpt[f], second ? v1 : v0, sizeof(int32_t) * nf, cudaMemcpyDeviceToDevice,
+                                       ctx->stream));
+    }
     KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_items, b->items.data(), sizeof(BatchItemDev) * n, cudaMemcpyHostToDevice,
                                    ctx->stream));
     DevStats* hs = nullptr;
@@ -311,7 +337,8 @@ int kiwi_batch_run(KiwiBatch* b, KiwiStats* item_stats, KiwiStats* total) {
     KIWI_TRY(batch_time_once(b, &ms));
     std::vector<DevStats> h(b->n_items);
     KIWI_CUDA(ctx, cudaMemcpy(h.data(), b->d_stats, sizeof(DevStats) * b->n_items, cudaMemcpyDeviceToHost));
-    const int64_t kernels = (int64_t)b->n_items + (b->n_tiles > 0 ? 1 : 0);  // mean velocities + the gather
+    int64_t kernels = b->n_items;  // mean velocities, then one gather launch per family present
+    for (int f = 0; f < kBatchFamilies; ++f) kernels += b->fam_tiles[f] > 0 ? 1 : 0;
     (void)launches0;
     KiwiStats sum{};
     for (int i = 0; i < b->n_items; ++i) {

@@ -59,6 +59,12 @@ int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, con
 // One grid of a batch (batch.cu): its geometry, particles and outputs, how its tiles are evaluated,
 // and where its tiles start in the batch's concatenated tile lists.
 enum BatchMode { kBatchLattice = 0, kBatchGatherCubic = 1, kBatchGatherGeneric = 2, kBatchLatticeGeneric = 3 };
+// tile-body families, one persistent launch each
+enum BatchFamily { kBatchFamilyLattice = 0, kBatchFamilyLatticeGeneric = 1, kBatchFamilyGather = 2, kBatchFamilies = 3 };
+inline int batch_family(int mode) {
+    return mode == kBatchLattice ? kBatchFamilyLattice
+                                 : (mode == kBatchLatticeGeneric ? kBatchFamilyLatticeGeneric : kBatchFamilyGather);
+}
 struct BatchItemDev {
     CartGeom g;
     DevParticles P;
@@ -69,12 +75,12 @@ struct BatchItemDev {
     DevStats* st;
 };
 
-// kiwi_fp64.cu: one persistent launch over the tiles of every item of a batch, taken in the order
-// order[0 .. ntiles) (null: ascending) from the work counter *next (zero before the launch).
+// kiwi_fp64.cu: one persistent launch over the tiles order[0 .. ntiles) (global tile indices) of the items
+// of one family, taken from the work counter *next (zero before the launch).
 int fp64_batch_prepare(KiwiCtx* ctx);
-int fp64_batch_gather(KiwiCtx* ctx, const BatchItemDev* d_items, const int32_t* d_item_of_tile, const int32_t* d_order,
-                      int64_t ntiles, const uint32_t* list, const int64_t* range, unsigned long long* d_next,
-                      int blocks);
+int fp64_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
+                      const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
+                      unsigned long long* d_next, int blocks);
 
 // mixed.cu: the FP32-mixed form (cubic spline).  cell_err (device, ncell doubles) receives each cell's
 // rounding-error bound and cell_mass (ncell doubles) its raw mass sum M.

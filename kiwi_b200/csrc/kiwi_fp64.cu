@@ -602,9 +602,11 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_generi
     lattice_tile<true, true>(g, P, list, range, blockIdx.x, blockIdx.x, out, st, kernel);
 }
 
-// A batch of grids in one persistent launch: each CTA takes the next tile from the work counter and runs
-// the tile body its item asks for (the same bodies as the single-grid kernels, so every cell's value and
-// summation order are those of a single-grid call).
+// The tiles of a batch of grids, one persistent launch per tile-body family (cubic lattice, generic
+// lattice, per-cell gather): each CTA takes the next of the family's tiles (order[w]) from the work
+// counter and runs the same tile body as the single-grid kernel, so every cell's value and summation
+// order are those of a single-grid call.  One instance per family keeps each body's register budget.
+template <int FAMILY>
 __global__ void __launch_bounds__(kThreads, 2) k_batch_persistent(const BatchItemDev* __restrict__ items,
                                                                  const int32_t* __restrict__ item_of_tile,
                                                                  const int32_t* __restrict__ order, int64_t ntiles,
@@ -617,12 +619,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_persistent(const BatchIte
         __syncthreads();
         const int64_t w = s_w;
         if (w >= ntiles) break;
-        const int64_t tg = order ? (int64_t)order[w] : w;
+        const int64_t tg = (int64_t)order[w];
         const BatchItemDev& it = items[item_of_tile[tg]];
         const int64_t tl = tg - it.tile_base;
-        if (it.mode == kBatchLattice)
+        if (FAMILY == kBatchFamilyLattice)
             lattice_tile<true>(it.g, it.P, list, range, tg, tl, it.out, it.st);
-        else if (it.mode == kBatchLatticeGeneric)
+        else if (FAMILY == kBatchFamilyLatticeGeneric)
             lattice_tile<true, true>(it.g, it.P, list, range, tg, tl, it.out, it.st, it.kernel);
         else
             gather_tile<false, true, true>(it.g, it.P, it.kernel, list, range, tg, tl, it.out, it.st,
@@ -767,17 +769,26 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
 }
 
 int fp64_batch_prepare(KiwiCtx* ctx) {
-    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kLatMaxDynSmem));
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_persistent<kBatchFamilyLattice>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatDynSmem));
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_persistent<kBatchFamilyLatticeGeneric>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatGenDynSmem));
     return KIWI_OK;
 }
 
-int fp64_batch_gather(KiwiCtx* ctx, const BatchItemDev* d_items, const int32_t* d_item_of_tile, const int32_t* d_order,
-                      int64_t ntiles, const uint32_t* list, const int64_t* range, unsigned long long* d_next,
-                      int blocks) {
+int fp64_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
+                      const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
+                      unsigned long long* d_next, int blocks) {
     if (ntiles <= 0) return KIWI_OK;
-    k_batch_persistent<<<blocks, kThreads, kLatMaxDynSmem, ctx->stream>>>(d_items, d_item_of_tile, d_order, ntiles, list,
-                                                                       range, d_next);
+    if (family == kBatchFamilyLattice)
+        k_batch_persistent<kBatchFamilyLattice><<<blocks, kThreads, kLatDynSmem, ctx->stream>>>(
+            d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
+    else if (family == kBatchFamilyLatticeGeneric)
+        k_batch_persistent<kBatchFamilyLatticeGeneric><<<blocks, kThreads, kLatGenDynSmem, ctx->stream>>>(
+            d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
+    else
+        k_batch_persistent<kBatchFamilyGather><<<blocks, kThreads, 0, ctx->stream>>>(d_items, d_item_of_tile, d_order,
+                                                                                     ntiles, list, range, d_next);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }
