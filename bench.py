@@ -51,6 +51,9 @@ EDGE_MIDDLE = 127.0 + TRANS_FLOPS * 6
 EDGE_INNER = 209.0 + TRANS_FLOPS * 12
 VERTEX_PYRAMID = 121.0 + TRANS_FLOPS * 4
 CELL_ASSEMBLY = 60.0
+# DRAM bytes (read + write) of one k_cart_lattice launch on the default workload (2M particles, 256^3),
+# ncu dram__bytes_read.sum + dram__bytes_write.sum (profiles/k_cart_lattice_fp64_lognormal.md).
+LATTICE_DRAM_BYTES_FULL = 274.63e6 + 598.75e6
 
 L2_BYTES = 126 * 1024 * 1024
 
@@ -452,9 +455,11 @@ def main():
     if rank == 0:
         g_ms = float(np.mean(gather_ms))
         evaluated_per_launch = evaluated / args.steps
+        is32 = args.precision.startswith("fp32")
         if items.get("vertex_pyramids", 0) > 0:
             # lattice-factorised kernel: its own work items x their measured costs
-            kname = "k_cart_lattice (FP64 lattice-factorised cell-integral gather)"
+            kname = ("k_cart_lattice_f32 (FP32 lattice tiers, FP64 assembly)" if is32 else
+                     "k_cart_lattice (FP64 lattice-factorised cell-integral gather)")
             work = (items["edge_tiers_outer"] * EDGE_OUTER + items["edge_tiers_middle"] * EDGE_MIDDLE +
                     items["edge_tiers_inner"] * EDGE_INNER + items["vertex_pyramids"] * VERTEX_PYRAMID +
                     evaluated * CELL_ASSEMBLY) / args.steps
@@ -464,6 +469,19 @@ def main():
             work_per_pair = WORK_PER_BBOX_PAIR if args.full_box else WORK_PER_SUPPORT_PAIR
             work = evaluated_per_launch * work_per_pair
         achieved = work / (g_ms * 1e-3) / 1e12
+        peak = kiwi_b200.measure_fp32_peak(ctx) if is32 else peak_fp64
+        # DRAM traffic of the kernel per launch, from the ncu capture of this exact workload
+        # (profiles/k_cart_lattice_fp64_lognormal.md); None for other workloads
+        traffic = None
+        if (not is32 and args.n == 2_000_000 and args.res == 256 and args.kernel == "cubic_spline" and
+                not args.full_box and args.precision == "fp64"):
+            traffic = LATTICE_DRAM_BYTES_FULL
+        hbm_peak = None
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                hbm_peak = float(json.load(f)["hbm_gbs"])
+        except (OSError, ValueError, KeyError):
+            pass
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -478,12 +496,17 @@ def main():
             "pairs": {"support_pairs_per_step": job_pairs / args.steps / ws,
                       "bbox_pairs_per_step": job_bbox / args.steps / ws,
                       "bbox_pairs_per_s": job_bbox / (job_ms * 1e-3)},
-            "roofline": {"bound": "fp64", "kernel": kname, "work_items_per_launch":
+            "roofline": {"bound": "fp32" if is32 else "fp64", "kernel": kname, "work_items_per_launch":
                          {k: v / args.steps for k, v in items.items()},
-                         "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
-                         "frac": achieved / peak_fp64 if peak_fp64 else None, "traffic": None,
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "hbm": ({"achieved_gbs": traffic / (g_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
+                                  "frac": traffic / (g_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": "MEASURED_PEAKS.json"}
+                                 if traffic and hbm_peak else None),
                          "work_per_pair_flops": work_per_pair, "evaluated_pairs_per_launch": evaluated_per_launch,
-                         "peak_source": "measured FP64 FMA probe (kiwi_measure_fp64_peak) in this run",
+                         "peak_source": ("measured FP32 FMA probe (kiwi_measure_fp32_peak)" if is32 else
+                                         "measured FP64 FMA probe (kiwi_measure_fp64_peak)") +
+                                        " in this run; MEASURED_PEAKS.json has no FP64/FP32 figure",
                          "gather_ms_per_launch": g_ms},
             "clocks": clk, "gpu_launches": int(launches), "wall_s_timed_region": wall,
             "e2e": e2e, "cpu_baseline": cpu,
@@ -491,6 +514,12 @@ def main():
         if accuracy is not None:
             line["accuracy"] = accuracy
         if fp32_side is not None:
+            # the FP32 kernel evaluates the same lattice work items as the FP64 one
+            peak32 = kiwi_b200.measure_fp32_peak(ctx)
+            a32 = work_per_pair * fp32_side["value"] / ws / 1e12
+            fp32_side["roofline"] = {"bound": "fp32", "kernel": "k_cart_lattice_f32", "achieved": a32, "peak": peak32,
+                                     "unit": "TFLOP/s", "frac": a32 / peak32 if peak32 else None,
+                                     "peak_source": "measured FP32 FMA probe (kiwi_measure_fp32_peak) in this run"}
             line["fp32_mixed"] = fp32_side
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -114,6 +114,8 @@ const char* kiwi_version(void);
 /* Measured FP64 FMA throughput of the context's GPU in TFLOP/s (a short probe kernel).  No counterpart in
  * the reference: it provides the roofline denominator of the FP64 cell-integral kernels. */
 int kiwi_measure_fp64_peak(KiwiCtx* ctx, double* tflops);
+/* The same for FP32 FMA throughput (the roofline denominator of the FP32-mixed form's kernel). */
+int kiwi_measure_fp32_peak(KiwiCtx* ctx, double* tflops);
 
 /* ---- kernel tables (include/kiwi/kernel_spec.hpp:18-44, src/kernel_spec_data.cpp:175-187) ----- */
 /* get_kernel(name): index 0..5 for a key or alias ("M4", "cubic_spline", "wendland_c4", ...), -1 if

@@ -526,3 +526,12 @@ def measure_fp64_peak(ctx=None) -> float:
     ctx._L.kiwi_measure_fp64_peak.argtypes = [C.c_void_p, _dp]
     ctx.check(ctx._L.kiwi_measure_fp64_peak(ctx.handle, C.byref(v)), "fp64 peak")
     return v.value
+
+
+def measure_fp32_peak(ctx=None) -> float:
+    """Measured FP32 FMA throughput (TFLOP/s) of the context's GPU."""
+    ctx = ctx or default_context()
+    v = C.c_double(0.0)
+    ctx._L.kiwi_measure_fp32_peak.argtypes = [C.c_void_p, _dp]
+    ctx.check(ctx._L.kiwi_measure_fp32_peak(ctx.handle, C.byref(v)), "fp32 peak")
+    return v.value

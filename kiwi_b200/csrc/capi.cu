@@ -279,6 +279,12 @@ int kiwi_measure_fp64_peak(KiwiCtx* ctx, double* tflops) {
     return fp64_measure_peak(ctx, tflops);
 }
 
+int kiwi_measure_fp32_peak(KiwiCtx* ctx, double* tflops) {
+    KIWI_TRY(check_ctx(ctx));
+    if (!tflops) return set_err(ctx, KIWI_ERR_ARG, "tflops is null");
+    return fp32_measure_peak(ctx, tflops);
+}
+
 int kiwi_kernel_index(const char* name) {
     if (!name) return -1;
     std::string n(name);

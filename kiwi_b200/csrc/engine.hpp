@@ -90,6 +90,7 @@ int mixed_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, co
 // writes their indices to map (ascending) and their count to *d_nmap (device).
 int mixed_flag_tiles(KiwiCtx* ctx, const CartGeom& g, const double* cell_err, const double* cell_mass,
                      double rel_tol, double floor_frac, int32_t* map, int64_t* d_nmap);
+int fp32_measure_peak(KiwiCtx* ctx, double* tflops);
 
 // voronoi.cu
 int voronoi_init_tables(KiwiCtx* ctx);

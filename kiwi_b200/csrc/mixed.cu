@@ -387,7 +387,39 @@ __global__ void k_compact_tiles(const uint32_t* __restrict__ flags, const int64_
     if (t < n && flags[t]) map[offs[t]] = (int32_t)t;
 }
 
+// FP32 FMA throughput probe: 8 independent fma chains per thread.
+__global__ void __launch_bounds__(256) k_ffma_peak(int iters, float seed, float* __restrict__ sink) {
+    float a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+          a7 = a0 + 7;
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; ++i) {
+        a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+        a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+    }
+    const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 12345.678f) sink[threadIdx.x] = s;  // keeps the chains live
+}
+
 }  // namespace
+
+int fp32_measure_peak(KiwiCtx* ctx, double* tflops) {
+    int sms = 0;
+    KIWI_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    float* sink = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_MISC0, 256, &sink));
+    const int blocks = sms * 8, iters = 1 << 15;
+    k_ffma_peak<<<blocks, 256, 0, ctx->stream>>>(256, 1.0f, sink);  // warm-up
+    KIWI_LAUNCHED(ctx);
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
+    k_ffma_peak<<<blocks, 256, 0, ctx->stream>>>(iters, 1.0f, sink);
+    KIWI_LAUNCHED(ctx);
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0.f;
+    KIWI_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    *tflops = 2.0 * 8.0 * iters * (double)blocks * 256.0 / (ms * 1e-3) / 1e12;
+    return KIWI_OK;
+}
 
 int mixed_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const TileLists& tl,
                       const CartOutputs& out, double* cell_err, double* cell_mass, DevStats* d_stats) {
