@@ -7,8 +7,10 @@ pair count the reference evaluates is reported beside it.
 
 Workload (one GPU): the 2,000,000-particle log-normal cube (sigma_ln rho = 1.5, P(k) ~ k^-4, 10 pc,
 domain padded by max 2h) on a 256^3 grid, cubic spline (M4) -- seeded synthetic input.  With N GPUs
-(torchrun, one process per GPU) each rank maps its own independently seeded snapshot of the same size
-(weak scaling, replicas: no data-path collective).
+(torchrun, one process per GPU) the ranks split that one grid (--multi tiles, the default: each rank
+computes the cell tiles of its part, kiwi_sph_to_grid_device_part, a weight-balanced run of x rows; strong
+scaling, no data-path collective) or each maps its own independently seeded snapshot of the same size
+(--multi replicas: weak scaling).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32_mixed] [--impl reference]
 
@@ -77,6 +79,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="with --precision fp64: skip timing the FP32-mixed form beside it")
+    ap.add_argument("--multi", default="tiles", choices=["tiles", "replicas"],
+                    help="with N > 1 GPUs: split one grid by cell tiles (strong scaling) or map one snapshot per "
+                         "rank (weak scaling)")
     ap.add_argument("--workload", default="lognormal", choices=["lognormal", "batch"],
                     help="batch: many column snapshots of log-uniform sizes on grids of log-uniform resolution, "
                          "kernels cycling M4 / M6 / WC4, in one persistent graph-recorded launch")
@@ -329,8 +334,10 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
 
-    P, bounds, shape = make_workload(args.n, args.res, args.seed + 1000 * rank, args.kernel)
+    split = ws > 1 and args.multi == "tiles"
+    P, bounds, shape = make_workload(args.n, args.res, args.seed + (0 if split else 1000 * rank), args.kernel)
     ki = kiwi_b200.make_kernel_integrator(args.kernel)
+    part, n_parts = (rank, ws) if split else (0, 1)
     ctx = kiwi_b200.Context(dev.index)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     dP = {k: torch.from_numpy(v).to(dev) for k, v in P.items()}
@@ -340,7 +347,8 @@ def main():
     torch.cuda.synchronize()
 
     for _ in range(args.warmup):
-        kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx)
+        kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, full_box=args.full_box,
+                                     ctx=ctx, part=part, n_parts=n_parts)
     peak_fp64 = kiwi_b200.measure_fp64_peak(ctx)
 
     clocks = ClockSampler(dev.index)
@@ -357,7 +365,8 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-        st = kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx)
+        st = kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision,
+                                          full_box=args.full_box, ctx=ctx, part=part, n_parts=n_parts)
         with torch.cuda.stream(stream):
             e1.record(stream)
         e1.synchronize()
@@ -400,7 +409,7 @@ def main():
 
     # accuracy of an FP32 form: against the FP64 form on the same input (untimed)
     accuracy = None
-    if args.precision.startswith("fp32"):
+    if args.precision.startswith("fp32") and not split:
         ref = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
         kiwi_b200.sph_to_grid_device(dP, bounds, shape, ref, kernel=ki, precision="fp64", ctx=ctx)
         torch.cuda.synchronize()
@@ -409,7 +418,8 @@ def main():
     # the FP32-mixed form timed beside the FP64 form (same input, same step protocol), with its error
     # against this run's FP64 output: the FP32-mixed vs FP64 comparison of the metric
     fp32_side = None
-    if args.precision == "fp64" and not args.no_fp32_compare and args.kernel == "cubic_spline" and not args.full_box:
+    if (args.precision == "fp64" and not args.no_fp32_compare and args.kernel == "cubic_spline" and not args.full_box
+            and not split):
         o32 = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
         for _ in range(min(args.warmup, 2)):
             kiwi_b200.sph_to_grid_device(dP, bounds, shape, o32, kernel=ki, precision="fp32_mixed", ctx=ctx)
@@ -435,7 +445,40 @@ def main():
 
     # end to end through the public host API: pinned host arrays in, host arrays out
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and split:
+        # each rank: the whole snapshot host -> device, its part, its x rows device -> host; max over ranks
+        from kiwi_b200 import shard
+
+        sup = ki.support_in_h or kiwi_b200.get_kernel(args.kernel).radkern
+        own = shard.tile_owners(shard.tile_entry_counts(P, bounds, shape, sup), ws)
+        ix0, ix1 = shard.part_rows(own, rank, shape)
+        c0, c1 = ix0 * shape[1] * shape[2], ix1 * shape[1] * shape[2]
+        hP = {k: torch.from_numpy(v).pin_memory() for k, v in P.items()}
+        hout = {k: torch.empty(c1 - c0, dtype=torch.float64).pin_memory() for k in out}
+        e_ms, e_pairs = 0.0, 0
+        for i in range(args.e2e_steps + 1):
+            dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for k in dP:
+                dP[k].copy_(hP[k], non_blocking=True)
+            torch.cuda.synchronize()
+            st = kiwi_b200.sph_to_grid_device(dP, bounds, shape, out, kernel=ki, precision=args.precision,
+                                              full_box=args.full_box, ctx=ctx, part=part, n_parts=n_parts)
+            for k in out:
+                hout[k].copy_(out[k][c0:c1], non_blocking=True)
+            torch.cuda.synchronize()
+            if i > 0:  # the first pass is a warm-up
+                e_ms += (time.perf_counter() - t0) * 1e3
+                e_pairs += st["sphere_pairs"]
+        from kiwi_b200.shard import reduce_step
+
+        e_max, e_all = reduce_step(e_ms, float(e_pairs), device=dev)
+        e2e = {"value": e_all / (e_max * 1e-3), "unit": "pair-integrals/s",
+               "h2d_bytes_per_step": int(8 * 8 * len(P["x"])) * ws, "d2h_bytes_per_step": int(4 * 8 * nc),
+               "ms_per_step": e_max / args.e2e_steps,
+               "note": "max over ranks of the wall time of each rank's copies in, part, and its rows out"}
+    elif args.e2e_steps > 0:
         hP = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in P.items()}
         hout = [torch.empty(nc, dtype=torch.float64).pin_memory().numpy() for _ in range(4)]
         kiwi_b200.sph_to_grid(hP, bounds, shape, kernel=ki, precision=args.precision, full_box=args.full_box, ctx=ctx, out=hout)
@@ -474,7 +517,7 @@ def main():
         # (profiles/k_cart_lattice_fp64_lognormal.md); None for other workloads
         traffic = None
         if (not is32 and args.n == 2_000_000 and args.res == 256 and args.kernel == "cubic_spline" and
-                not args.full_box and args.precision == "fp64"):
+                not args.full_box and args.precision == "fp64" and ws == 1):
             traffic = LATTICE_DRAM_BYTES_FULL
         hbm_peak = None
         try:
@@ -485,14 +528,15 @@ def main():
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": job_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": job_ms / args.steps, "higher_is_better": True, "scaling": "strong" if split else "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": f"lognormal_cube n={args.n} sigma_ln=1.5 P(k)~k^-4 10pc padded, "
                                    f"grid {args.res}^3, kernel {args.kernel}",
                        "precision": args.precision, "particles_per_gpu": args.n, "cells": nc,
                        "l2": "flushed between timed steps (256 MB write) and inputs+outputs > L2",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+                       "parallelism": (f"cell-tile parts x{ws} of one grid" if split else f"replicas x{ws}")
+                       if ws > 1 else "single GPU"},
             "pairs": {"support_pairs_per_step": job_pairs / args.steps / ws,
                       "bbox_pairs_per_step": job_bbox / args.steps / ws,
                       "bbox_pairs_per_s": job_bbox / (job_ms * 1e-3)},

@@ -151,6 +151,17 @@ int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const 
                             const KiwiKernelSel* kernel, int precision, double* density, double* vx, double* vy,
                             double* vz, double* raw4, KiwiStats* stats);
 
+/* One part of kiwi_sph_to_grid_device, for splitting one grid over several GPUs (one process or context
+ * per GPU, each with every particle; no counterpart in the reference, whose OpenMP loop splits
+ * particles inside one process).  The 8x8x8-cell tiles are split into n_parts contiguous runs of the
+ * tile order (tile (tx, ty, tz) at index (tx * nty + ty) * ntz + tz, so each run covers a slab of x rows)
+ * holding near-equal numbers of (tile, particle) entries; part `part` computes and writes only the cells
+ * of its own tiles, each equal bit for bit to the whole call's.  The other cells of the outputs are left
+ * as they were.  KIWI_FP32_GUARANTEE needs n_parts = 1.  1 <= n_parts <= 65536. */
+int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                                 const KiwiKernelSel* kernel, int precision, int part, int n_parts, double* density,
+                                 double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
+
 /* Adjoint of the sph-to-grid raw sums.  It has no counterpart in the reference (which has no gradients).
  * With M_c = sum_p m_p K_pc and P_c = sum_p m_p K_pc v_p the raw sums of kiwi_sph_to_grid_device
  * (K_pc the particle's kernel mass in cell c, clamped at 0), and raw4 the cotangents dL/dM, dL/dPx,

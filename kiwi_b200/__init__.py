@@ -114,6 +114,7 @@ def load_library(path: str = LIB_PATH):
            _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
     L.kiwi_sph_to_grid.argtypes = sig
     L.kiwi_sph_to_grid_device.argtypes = sig
+    L.kiwi_sph_to_grid_device_part.argtypes = sig[:5] + [C.c_int, C.c_int] + sig[5:]
     L.kiwi_sph_to_grid_adjoint_device.argtypes = ([C.c_void_p, C.POINTER(KiwiParticles), C.POINTER(KiwiCartGrid),
                                                    C.POINTER(KiwiKernelSel), _dp] + [_dp] * 8 +
                                                   [C.POINTER(KiwiStats)])
@@ -375,9 +376,11 @@ def sph_to_grid(particles: dict, bounds, shape, kernel=None, precision="fp64", r
 
 
 def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, precision="fp64", ctx=None,
-                       full_box=False):
+                       full_box=False, part=0, n_parts=1):
     """Device variant: `particles` and `out` (density, vx, vy, vz[, raw4]) hold CUDA tensors (float64,
-    contiguous).  Runs on the context's stream and returns the call's stats."""
+    contiguous).  Runs on the context's stream and returns the call's stats.  With n_parts > 1 only the
+    cells of the tiles owned by `part` are computed and written (kiwi_sph_to_grid_device_part): one part
+    per GPU splits one grid over several GPUs."""
     ctx = ctx or default_context()
     ki = kernel or KernelIntegrator()
     Ps, _ = _particles_struct(particles, device=True)
@@ -389,10 +392,15 @@ def sph_to_grid_device(particles: dict, bounds, shape, out: dict, kernel=None, p
     def dp(t):
         return C.cast(C.c_void_p(int(t.data_ptr())), _dp) if t is not None else None
 
-    ctx.check(ctx._L.kiwi_sph_to_grid_device(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
-                                             precision_code(precision, full_box), dp(out.get("density")),
-                                             dp(out.get("vx")), dp(out.get("vy")), dp(out.get("vz")),
-                                             dp(out.get("raw4")), C.byref(st)), "sph-to-grid")
+    outs = [dp(out.get(k)) for k in ("density", "vx", "vy", "vz", "raw4")]
+    if n_parts == 1:
+        ctx.check(ctx._L.kiwi_sph_to_grid_device(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
+                                                 precision_code(precision, full_box), *outs, C.byref(st)),
+                  "sph-to-grid")
+    else:
+        ctx.check(ctx._L.kiwi_sph_to_grid_device_part(ctx.handle, C.byref(Ps), C.byref(grid), C.byref(sel),
+                                                      precision_code(precision, full_box), int(part), int(n_parts),
+                                                      *outs, C.byref(st)), "sph-to-grid part")
     return st.as_dict()
 
 

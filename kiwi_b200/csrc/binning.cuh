@@ -70,4 +70,32 @@ static __global__ void k_tile_ranges(const uint32_t* __restrict__ keys, int64_t 
 }
 
 
+// Per tile: its (tile, particle) entry count, the weight by which the tiles are split between parts.
+static __global__ void k_tile_entry_counts(const int64_t* __restrict__ range, int64_t ntiles, uint32_t* __restrict__ w) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const int64_t e = range[2 * t + 1] - range[2 * t];
+    w[t] = (uint32_t)(e < 0xffffffffLL ? e : 0xffffffffLL);
+}
+
+// 1 if tile t belongs to part `part` of n: part floor(prefix(t) n / W), prefix(t) the entries of the tiles
+// before t and W the total (capped at n - 1), so the parts are contiguous runs of the tile order with
+// near-equal entry counts; with W = 0 the tiles are split evenly by number.
+static __global__ void k_tile_part_flags(const int64_t* __restrict__ prefix, const int64_t* __restrict__ total,
+                                         int64_t ntiles, int part, int n, uint32_t* __restrict__ flags) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const int64_t W = *total;
+    int64_t owner = W > 0 ? (prefix[t] * n) / W : (t * n) / ntiles;
+    if (owner > n - 1) owner = n - 1;
+    flags[t] = owner == part ? 1u : 0u;
+}
+
+// map[offs[t]] = t for the flagged tiles (offs: the exclusive scan of the flags).
+static __global__ void k_compact_map(const uint32_t* __restrict__ flags, const int64_t* __restrict__ offs, int64_t n,
+                                     int32_t* __restrict__ map) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n && flags[t]) map[offs[t]] = (int32_t)t;
+}
+
 }  // namespace kiwi_b200

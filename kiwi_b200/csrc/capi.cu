@@ -82,7 +82,11 @@ int check_ctx(KiwiCtx* ctx) {
 
 // The full device pipeline of one sph-to-grid call: mean velocity, binning, gather.
 int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
-                    const CartOutputs& out_in, KiwiStats* stats) {
+                    const CartOutputs& out_in, KiwiStats* stats, int part, int n_parts) {
+    if (n_parts < 1 || n_parts > 65536 || part < 0 || part >= n_parts)
+        return set_err(ctx, KIWI_ERR_ARG, "part %d of %d parts is out of range (1 <= parts <= 65536)", part, n_parts);
+    if (n_parts > 1 && (precision & KIWI_FP32_GUARANTEE))
+        return set_err(ctx, KIWI_ERR_ARG, "KIWI_FP32_GUARANTEE needs the whole grid (n_parts = 1)");
     const int64_t launches0 = ctx->launches;
     DevStats* d_stats = nullptr;
     double* d_meanv = nullptr;
@@ -134,6 +138,32 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         KIWI_LAUNCHED(ctx);
     }
     TileLists tl{sorted_vals, range, ntiles};
+    if (n_parts > 1) {
+        // this part's tiles: a contiguous run of the tile order holding ~1/n_parts of the entries
+        uint32_t *w = nullptr, *flags = nullptr;
+        int64_t* prefix = nullptr;
+        int32_t* map = nullptr;
+        KIWI_TRY(scratch_t(ctx, S_MISC0, (size_t)ntiles, &w));
+        KIWI_TRY(scratch_t(ctx, S_MISC1, (size_t)ntiles + 1, &prefix));
+        KIWI_TRY(scratch_t(ctx, S_MISC2, (size_t)ntiles, &flags));
+        KIWI_TRY(scratch_t(ctx, S_TILE_MAP, (size_t)ntiles, &map));
+        const unsigned nb = (unsigned)((ntiles + 255) / 256);
+        k_tile_entry_counts<<<nb, 256, 0, ctx->stream>>>(range, ntiles, w);
+        KIWI_LAUNCHED(ctx);
+        KIWI_TRY(exclusive_scan<uint32_t>(ctx, w, ntiles, prefix, prefix + ntiles));
+        k_tile_part_flags<<<nb, 256, 0, ctx->stream>>>(prefix, prefix + ntiles, ntiles, part, n_parts, flags);
+        KIWI_LAUNCHED(ctx);
+        int64_t* moffs = nullptr;
+        KIWI_TRY(scratch_t(ctx, S_OFFS, (size_t)ntiles + 1, &moffs));
+        KIWI_TRY(exclusive_scan<uint32_t>(ctx, flags, ntiles, moffs, moffs + ntiles));
+        k_compact_map<<<nb, 256, 0, ctx->stream>>>(flags, moffs, ntiles, map);
+        KIWI_LAUNCHED(ctx);
+        int64_t nmap = 0;
+        KIWI_CUDA(ctx, cudaMemcpyAsync(&nmap, moffs + ntiles, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+        KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        tl.map = map;
+        tl.nmap = nmap;
+    }
 
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     const int form = precision & KIWI_FORM_MASK;
@@ -381,6 +411,31 @@ int kiwi_sph_to_grid_device(KiwiCtx* ctx, const KiwiParticles* particles, const 
     CartOutputs out{density, vx, vy, vz, raw4, nullptr};
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     KIWI_TRY(sph_to_grid_dev(ctx, P, g, kc, precision, out, stats));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        stats->total_ms = ms;
+    }
+    return KIWI_OK;
+}
+
+int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                                 const KiwiKernelSel* kernel, int precision, int part, int n_parts, double* density,
+                                 double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats) {
+    KIWI_TRY(check_ctx(ctx));
+    int rc = KIWI_OK;
+    if (!particles_ok(ctx, particles, &rc)) return rc;
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    CartGeom g;
+    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+    DevParticles P{particles->n, particles->x, particles->y, particles->z, particles->vx,
+                   particles->vy, particles->vz, particles->m, particles->h};
+    CartOutputs out{density, vx, vy, vz, raw4, nullptr};
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    KIWI_TRY(sph_to_grid_dev(ctx, P, g, kc, precision, out, stats, part, n_parts));
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
     KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
     if (stats) {

@@ -49,8 +49,10 @@ struct AdjointOutputs {
 int resolve_kernel(KiwiCtx* ctx, const KiwiKernelSel* sel, KernelChoice* out);
 int make_geom(KiwiCtx* ctx, const KiwiCartGrid* grid, double support_in_h, CartGeom* g);
 bool particles_ok(KiwiCtx* ctx, const KiwiParticles* p, int* rc);
+// part / n_parts: evaluate only the cell tiles owned by part `part` of `n_parts` (contiguous runs of the
+// tile order with near-equal (tile, particle) entry counts); n_parts = 1 evaluates every tile.
 int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
-                    const CartOutputs& out, KiwiStats* stats);
+                    const CartOutputs& out, KiwiStats* stats, int part = 0, int n_parts = 1);
 
 // adjoint.cu
 int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc,

@@ -261,9 +261,11 @@ __device__ __forceinline__ void gather_tile(const CartGeom& g, const DevParticle
 template <bool CUBIC, bool CULL>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g, DevParticles P, int kernel,
                                                           const uint32_t* __restrict__ list,
-                                                          const int64_t* __restrict__ range, CartOutputs out,
+                                                          const int64_t* __restrict__ range,
+                                                          const int32_t* __restrict__ tile_map, CartOutputs out,
                                                           DevStats* __restrict__ st) {
-    gather_tile<CUBIC, CULL>(g, P, kernel, list, range, blockIdx.x, blockIdx.x, out, st);
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    gather_tile<CUBIC, CULL>(g, P, kernel, list, range, t, t, out, st);
 }
 
 // ------------------------------------------------------------------ lattice-factorised gather (cubic)
@@ -597,9 +599,11 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
 __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_generic(CartGeom g, DevParticles P, int kernel,
                                                                                   const uint32_t* __restrict__ list,
                                                                                   const int64_t* __restrict__ range,
+                                                                                  const int32_t* __restrict__ tile_map,
                                                                                   CartOutputs out,
                                                                                   DevStats* __restrict__ st) {
-    lattice_tile<true, true>(g, P, list, range, blockIdx.x, blockIdx.x, out, st, kernel);
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    lattice_tile<true, true>(g, P, list, range, t, t, out, st, kernel);
 }
 
 // The tiles of a batch of grids, one persistent launch per tile-body family (cubic lattice, generic
@@ -735,8 +739,6 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
                      bool reference_order) {
     if (tl.ntiles <= 0) return KIWI_OK;
     if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
-    if (tl.map && !(k.cubic && !reference_order))
-        return set_err(ctx, KIWI_ERR_ARG, "a tile subset is only supported by the lattice evaluation");
     if (tl.map && tl.nmap <= 0) return KIWI_OK;
     const dim3 grid((unsigned)(tl.map ? tl.nmap : tl.ntiles));
     if (k.cubic && !reference_order) {
@@ -754,16 +756,20 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
     } else if (!k.cubic && !reference_order && !full_box) {
         KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_generic, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)kLatGenDynSmem));
-        k_cart_lattice_generic<<<grid, kThreads, kLatGenDynSmem, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out,
-                                                                                d_stats);
+        k_cart_lattice_generic<<<grid, kThreads, kLatGenDynSmem, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range,
+                                                                                tl.map, out, d_stats);
     } else if (k.cubic && !full_box)
-        k_cart_gather<true, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+        k_cart_gather<true, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, tl.map, out,
+                                                                      d_stats);
     else if (k.cubic)
-        k_cart_gather<true, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+        k_cart_gather<true, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, tl.map, out,
+                                                                       d_stats);
     else if (!full_box)
-        k_cart_gather<false, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+        k_cart_gather<false, true><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, tl.map, out,
+                                                                       d_stats);
     else
-        k_cart_gather<false, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, out, d_stats);
+        k_cart_gather<false, false><<<grid, kThreads, 0, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range, tl.map, out,
+                                                                        d_stats);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

@@ -51,6 +51,7 @@ __device__ __forceinline__ float fsgn(double v) { return (v > 0.0) ? 1.0f : ((v 
 __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, DevParticles P,
                                                                     const uint32_t* __restrict__ list,
                                                                     const int64_t* __restrict__ range,
+                                                                    const int32_t* __restrict__ tile_map,
                                                                     CartOutputs out, double* __restrict__ cell_err,
                                                                     double* __restrict__ cell_mass,
                                                                     DevStats* __restrict__ st) {
@@ -68,7 +69,7 @@ __global__ void __launch_bounds__(kMxThreads, 2) k_cart_lattice_f32(CartGeom g, 
     float* s_S = s_dynf + 4 * kMxECap;
     float* s_Sa = s_S + kMxSCap;
 
-    const int64_t t = blockIdx.x;
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -427,8 +428,10 @@ int mixed_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, co
     if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_f32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kMxDynSmem));
-    k_cart_lattice_f32<<<(unsigned)tl.ntiles, kMxThreads, kMxDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, out,
-                                                                                   cell_err, cell_mass, d_stats);
+    if (tl.map && tl.nmap <= 0) return KIWI_OK;
+    const unsigned grid = (unsigned)(tl.map ? tl.nmap : tl.ntiles);
+    k_cart_lattice_f32<<<grid, kMxThreads, kMxDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out, cell_err,
+                                                                      cell_mass, d_stats);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

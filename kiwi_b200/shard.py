@@ -1,0 +1,99 @@
+"""Splitting one grid over several GPUs: the host side of kiwi_sph_to_grid_device_part.
+
+The library splits a grid's 8x8x8-cell tiles into n parts, each a contiguous run of the tile order
+(tile (tx, ty, tz) at index (tx * nty + ty) * ntz + tz) with a near-equal number of (tile, particle)
+entries: tile t belongs to part floor(prefix(t) * n / W) (capped at n - 1), prefix(t) being the entries of
+the tiles before t and W their total; with W = 0 the tiles split evenly by number.  This module restates
+that rule on the host -- the entry counts from the particles' clamped support boxes, exactly as the
+binning computes them -- so that a rank knows which x rows of the grid it owns (to copy back only those)
+before the GPU has run, and every rank agrees on the split without talking to the others.  It also
+holds the max-over-ranks reduction of a step's timing.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+TILE = 8
+
+
+def tile_grid(shape):
+    nx, ny, nz = (int(s) for s in shape)
+    return (nx + TILE - 1) // TILE, (ny + TILE - 1) // TILE, (nz + TILE - 1) // TILE
+
+
+def tile_entry_counts(particles: dict, bounds, shape, support_in_h: float) -> np.ndarray:
+    """(tile, particle) entries per tile, in tile order: the number of particles whose clamped support
+    box (src/cartesian_grid.cpp:211-237) touches the tile."""
+    nx, ny, nz = (int(s) for s in shape)
+    ntx, nty, ntz = tile_grid(shape)
+    x, y, z, h = (np.asarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "h"))
+    b = [float(v) for v in bounds]
+    d = [(b[1] - b[0]) / nx, (b[3] - b[2]) / ny, (b[5] - b[4]) / nz]
+    ok = h > 0
+    radius = support_in_h * h
+    lo, hi = [], []
+    for c, mn, dd, n in ((x, b[0], d[0], nx), (y, b[2], d[1], ny), (z, b[4], d[2], nz)):
+        with np.errstate(invalid="ignore", over="ignore"):
+            a0 = np.clip(np.floor((c - radius - mn) / dd), -2e9, 2e9)
+            a1 = np.clip(np.floor((c + radius - mn) / dd), -2e9, 2e9)
+        a0 = np.maximum(a0, 0)
+        a1 = np.minimum(a1, n - 1)
+        ok &= a0 <= a1
+        lo.append(a0)
+        hi.append(a1)
+    cnt = np.zeros((ntx + 1, nty + 1, ntz + 1), dtype=np.int64)
+    t0 = [(lo[i][ok] // TILE).astype(np.int64) for i in range(3)]
+    t1 = [(hi[i][ok] // TILE).astype(np.int64) + 1 for i in range(3)]
+    # 3-D difference array: +1 on the box's corners with inclusion-exclusion signs
+    for sx, ix in ((1, t0[0]), (-1, t1[0])):
+        for sy, iy in ((1, t0[1]), (-1, t1[1])):
+            for sz, iz in ((1, t0[2]), (-1, t1[2])):
+                np.add.at(cnt, (ix, iy, iz), sx * sy * sz)
+    cnt = cnt.cumsum(0).cumsum(1).cumsum(2)[:ntx, :nty, :ntz]
+    return cnt.reshape(-1)
+
+
+def tile_owners(weights: np.ndarray, n_parts: int) -> np.ndarray:
+    """The part of every tile (the library's rule, integer arithmetic as on the device)."""
+    w = np.minimum(np.asarray(weights, dtype=np.int64), 0xFFFFFFFF)
+    n = len(w)
+    prefix = np.concatenate([[0], np.cumsum(w)[:-1]]) if n else np.zeros(0, dtype=np.int64)
+    W = int(w.sum())
+    if W > 0:
+        owner = (prefix * n_parts) // W
+    else:
+        owner = (np.arange(n, dtype=np.int64) * n_parts) // max(n, 1)
+    return np.minimum(owner, n_parts - 1)
+
+
+def part_rows(owner: np.ndarray, part: int, shape) -> tuple[int, int]:
+    """The x rows [ix0, ix1) of cells that cover every tile of `part` (empty if it owns none).  The cells
+    of rows ix0 .. ix1 - 1 are contiguous in the (ix * ny + iy) * nz + iz layout."""
+    nx = int(shape[0])
+    ntx, nty, ntz = tile_grid(shape)
+    mine = np.nonzero(owner == part)[0]
+    if len(mine) == 0:
+        return 0, 0
+    tx0, tx1 = int(mine[0]) // (nty * ntz), int(mine[-1]) // (nty * ntz)
+    return tx0 * TILE, min(nx, (tx1 + 1) * TILE)
+
+
+def cells_of_part(owner: np.ndarray, part: int, shape) -> np.ndarray:
+    """Boolean mask over the cells (x-major) of the tiles owned by `part`."""
+    nx, ny, nz = (int(s) for s in shape)
+    ntx, nty, ntz = tile_grid(shape)
+    t = (owner == part).reshape(ntx, nty, ntz)
+    m = np.repeat(np.repeat(np.repeat(t, TILE, 0), TILE, 1), TILE, 2)[:nx, :ny, :nz]
+    return m.reshape(-1)
+
+
+def reduce_step(ms: float, pairs: float, device=None):
+    """(max over ranks of ms, sum over ranks of pairs) through torch.distributed (NCCL or gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms, pairs], dtype=torch.float64, device=device)
+    mx = t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(mx[0]), float(t[1])
