@@ -226,6 +226,23 @@ int kiwi_batch_run(KiwiBatch* batch, KiwiStats* item_stats, KiwiStats* total);
 int kiwi_batch_tune(KiwiBatch* batch, int* chosen);
 void kiwi_batch_destroy(KiwiBatch* batch);
 
+/* ---- stage output files (host only; no GPU needed) ------------------------------------------- */
+/* save_cartesian_grid (src/cartesian_grid.cpp:323-347): the VGTCGRD2 binary file -- "VGTCGRD2", int32 nx,
+ * ny, nz, 6 doubles of bounds, then density, vx, vy, vz (nx*ny*nz doubles each, x-major).  Errors:
+ * KIWI_ERR_ARG with the reference's message in err (if err_len > 0). */
+int kiwi_save_cartesian_grid(const char* path, int32_t nx, int32_t ny, int32_t nz, const double* bounds6,
+                             const double* density, const double* vx, const double* vy, const double* vz, char* err,
+                             size_t err_len);
+/* load_cartesian_grid (src/cartesian_grid.cpp:349-394).  With all four arrays NULL only the header is read
+ * (nxyz[3], bounds6 may be NULL), so the caller can size the arrays; otherwise all four are filled. */
+int kiwi_load_cartesian_grid(const char* path, int32_t* nxyz, double* bounds6, double* density, double* vx,
+                             double* vy, double* vz, char* err, size_t err_len);
+/* save_mapping (src/mapping.cpp:307-315): mapping.dat, "id x y z volume density vx vy vz" per cell with
+ * 15 significant digits. */
+int kiwi_save_mapping(const char* path, int64_t n_cells, const int64_t* id, const double* x, const double* y,
+                      const double* z, const double* volume, const double* density, const double* vx, const double* vy,
+                      const double* vz, char* err, size_t err_len);
+
 /* ---- Voronoi map stage (run_mapping_stage's particle loop, src/mapping.cpp:105-206, 400-502) --- */
 /* Cell geometry in CSR form: the plain data of CellFaceGeometry (src/mapping.cpp:49-54) with vertex
  * coordinates made absolute as src/mapping.cpp:168-175 does and neighbour ids resolved to cell indices. */

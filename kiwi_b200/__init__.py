@@ -492,6 +492,56 @@ class MappingResult:
     stats: dict = field(default_factory=dict)
 
 
+def _io_lib():
+    L = load_library()
+    L.kiwi_save_cartesian_grid.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32] + [_dp] * 5 + [C.c_char_p,
+                                                                                                   C.c_size_t]
+    L.kiwi_load_cartesian_grid.argtypes = [C.c_char_p, C.POINTER(C.c_int32)] + [_dp] * 5 + [C.c_char_p, C.c_size_t]
+    L.kiwi_save_mapping.argtypes = ([C.c_char_p, C.c_int64, _i64p] + [_dp] * 8 + [C.c_char_p, C.c_size_t])
+    return L
+
+
+def _io_check(rc, err):
+    if rc != 0:
+        raise KiwiError(rc, err.value.decode() or "file error")
+
+
+def save_cartesian_grid(result: CartesianGridResult, path: str):
+    """save_cartesian_grid (src/cartesian_grid.cpp:323-347): the VGTCGRD2 file of a CartesianGridResult."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    arrs = [_f64(a) for a in (result.density, result.vx, result.vy, result.vz)]
+    b = _f64(result.bounds)
+    _io_check(L.kiwi_save_cartesian_grid(path.encode(), result.nx, result.ny, result.nz, _p(b), *[_p(a) for a in arrs],
+                                         err, len(err)), err)
+
+
+def load_cartesian_grid(path: str) -> CartesianGridResult:
+    """load_cartesian_grid (src/cartesian_grid.cpp:349-394)."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    n = (C.c_int32 * 3)()
+    b = np.zeros(6)
+    _io_check(L.kiwi_load_cartesian_grid(path.encode(), n, _p(b), None, None, None, None, err, len(err)), err)
+    nc = n[0] * n[1] * n[2]
+    arrs = [np.empty(nc) for _ in range(4)]
+    _io_check(L.kiwi_load_cartesian_grid(path.encode(), n, _p(b), *[_p(a) for a in arrs], err, len(err)), err)
+    return CartesianGridResult(n[0], n[1], n[2], tuple(b), *arrs)
+
+
+def save_mapping(path: str, ids, sites, volume, result):
+    """save_mapping (src/mapping.cpp:307-315): mapping.dat rows "id x y z volume density vx vy vz" for the
+    cells of a MappingResult (ids and site coordinates from the caller's tessellation)."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    ids = np.ascontiguousarray(ids, dtype=np.int64)
+    sites = np.asarray(sites, dtype=np.float64)
+    arrs = [_f64(sites[:, 0]), _f64(sites[:, 1]), _f64(sites[:, 2]), _f64(volume), _f64(result.density),
+            _f64(result.vx), _f64(result.vy), _f64(result.vz)]
+    _io_check(L.kiwi_save_mapping(path.encode(), len(ids), ids.ctypes.data_as(_i64p), *[_p(a) for a in arrs], err,
+                                  len(err)), err)
+
+
 def map_voronoi(particles: dict, home_cell, cells: dict, kernel=None, precision="fp64", raw=False, ctx=None):
     """Density and mass-weighted velocity of an SPH snapshot on Voronoi cells -- the particle loop of
     run_mapping_stage (src/mapping.cpp:400-502).  `cells` holds the CSR geometry: face_off (n_cells+1),

@@ -31,6 +31,7 @@ UNITS = [
     ("adjoint.cu", ["--fmad=false"]),
     ("mixed.cu", []),
     ("batch.cu", ["--fmad=false"]),
+    ("io.cu", []),
 ]
 
 

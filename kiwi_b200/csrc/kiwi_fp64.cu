@@ -270,7 +270,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
 
 // ------------------------------------------------------------------ lattice-factorised gather (cubic)
 
-constexpr int kLatMinBlocks = 2;
+#ifndef KIWI_LATTICE_MIN_BLOCKS
+#define KIWI_LATTICE_MIN_BLOCKS 2
+#endif
+constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatSCap);
 constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;

@@ -167,6 +167,20 @@ class RefLib:
                                                               C.c_int, C.c_int, C.c_long, C.c_long,
                                                               C.POINTER(C.c_long), C.POINTER(C.c_long), _dp])
         L.ref_max_threads.restype = C.c_int
+        L.ref_save_cartesian_grid.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int] + [_dp] * 5
+        L.ref_save_mapping.argtypes = [C.c_char_p, C.c_long, C.POINTER(C.c_long)] + [_dp] * 8
+
+    def save_cartesian_grid(self, path, shape, bounds, density, vx, vy, vz):
+        arrs = [_f64(a) for a in (bounds, density, vx, vy, vz)]
+        if self.lib.ref_save_cartesian_grid(path.encode(), *[int(s) for s in shape], *[_d(a) for a in arrs]) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def save_mapping(self, path, ids, x, y, z, volume, density, vx, vy, vz):
+        ids = np.ascontiguousarray(ids, dtype=np.int64)
+        arrs = [_f64(a) for a in (x, y, z, volume, density, vx, vy, vz)]
+        if self.lib.ref_save_mapping(path.encode(), len(ids), ids.ctypes.data_as(C.POINTER(C.c_long)),
+                                     *[_d(a) for a in arrs]) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
 
     def max_threads(self):
         return self.lib.ref_max_threads()

@@ -370,4 +370,57 @@ void ref_voronoi_copy(void* h, int* id, double* site, double* volume, long* face
 
 void ref_voronoi_free(void* h) { delete static_cast<RefVoronoi*>(h); }
 
+// The reference's own stage-file writers (src/cartesian_grid.cpp:323-347, src/mapping.cpp:307-315).
+int ref_save_cartesian_grid(const char* path, int nx, int ny, int nz, const double* b, const double* density,
+                            const double* vx, const double* vy, const double* vz) {
+    try {
+        kiwi::CartesianGridResult g;
+        g.nx = nx;
+        g.ny = ny;
+        g.nz = nz;
+        g.domain.x_min = b[0];
+        g.domain.x_max = b[1];
+        g.domain.y_min = b[2];
+        g.domain.y_max = b[3];
+        g.domain.z_min = b[4];
+        g.domain.z_max = b[5];
+        const size_t n = (size_t)nx * ny * nz;
+        g.density.assign(density, density + n);
+        g.vx.assign(vx, vx + n);
+        g.vy.assign(vy, vy + n);
+        g.vz.assign(vz, vz + n);
+        kiwi::save_cartesian_grid(g, path);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+int ref_save_mapping(const char* path, long n, const long* id, const double* x, const double* y, const double* z,
+                     const double* volume, const double* density, const double* vx, const double* vy,
+                     const double* vz) {
+    try {
+        kiwi::MappingResult m;
+        for (long i = 0; i < n; ++i) {
+            kiwi::CellMapping c;
+            c.id = (int)id[i];
+            c.x = x[i];
+            c.y = y[i];
+            c.z = z[i];
+            c.volume = volume[i];
+            c.density = density[i];
+            c.vx = vx[i];
+            c.vy = vy[i];
+            c.vz = vz[i];
+            m.cells.push_back(c);
+        }
+        kiwi::save_mapping(m, path);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 }  // extern "C"
