@@ -83,7 +83,8 @@ def parse():
                     help="with N > 1 GPUs: split one grid by cell tiles (strong scaling) or map one snapshot per "
                          "rank (weak scaling)")
     ap.add_argument("--fd-particles", type=int, default=40, help="adjoint workload: particles checked by FD")
-    ap.add_argument("--workload", default="lognormal", choices=["lognormal", "batch", "adjoint"],
+    ap.add_argument("--vor-n", type=int, default=200_000, help="voronoi workload: particles")
+    ap.add_argument("--workload", default="lognormal", choices=["lognormal", "batch", "adjoint", "voronoi"],
                     help="batch: many column snapshots of log-uniform sizes on grids of log-uniform resolution, "
                          "kernels cycling M4 / M6 / WC4, in one persistent graph-recorded launch")
     ap.add_argument("--batch-items", type=int, default=64)
@@ -331,6 +332,65 @@ def run_adjoint(args):
     return 0
 
 
+def run_voronoi(args):
+    """Voronoi-cell map: --vor-n column-recipe particles on a 5 pc cube (filament through the centre, seed
+    1003), coverage_grid buffer points (spacing 0.05 x 5 pc) and one Lloyd iteration; the tessellation is
+    built on the host by the reference's own point-set stage and Voro++ (oracle/_ref, as the reference
+    keeps it on the host), which also runs the reference's OpenMP mapping loop as the CPU baseline.  The
+    GPU map is timed through kiwi_map_voronoi (geometry and particles staged from host arrays)."""
+    import torch
+
+    import kiwi_b200
+    from kiwi_b200.workloads import column_snapshot
+    from oracle.oracle import load_ref
+
+    ref = load_ref()
+    if ref is None:
+        print(json.dumps({"workload": "voronoi", "unavailable": "oracle/_ref (the reference library) is not built"}))
+        return 0
+    torch.cuda.set_device(0)
+    P, bounds = column_snapshot(n=args.vor_n, seed=1003, box=(5.0, 5.0, 5.0))
+    threads = ref.max_threads()
+    t0 = time.perf_counter()
+    geo, _ = ref.voronoi(P, bounds, buffer=True, spacing_fraction=0.05, lloyd=1, threads=threads, run_map=False)
+    t_geo = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    geo2, ref_res = ref.voronoi(P, bounds, buffer=True, spacing_fraction=0.05, lloyd=1, threads=threads, run_map=True)
+    t_ref_total = time.perf_counter() - t0
+    t_ref_map = max(t_ref_total - t_geo, 1e-9)
+    cells = {k: geo2[k] for k in ("face_off", "vert_off", "vxyz", "face_nbr", "volume")}
+    ctx = kiwi_b200.Context(0)
+    r = kiwi_b200.map_voronoi(P, geo2["home"], cells, ctx=ctx)  # warm-up
+    g_ms, t_ms = [], []
+    for _ in range(args.steps):
+        r = kiwi_b200.map_voronoi(P, geo2["home"], cells, ctx=ctx)
+        g_ms.append(r.stats["gather_ms"])
+        t_ms.append(r.stats["total_ms"])
+    pairs = r.stats["evaluated_pairs"]
+    d_ref = ref_res[0]
+    m = d_ref > 1e-2 * d_ref.max()
+    line = {
+        "metric": "particle-cell integrals/s (BFS-visited pairs), Voronoi map", "value": pairs / (np.mean(g_ms) * 1e-3),
+        "unit": "pair-integrals/s", "n_gpus": 1, "steps": args.steps, "warmup": 1,
+        "ms_per_step": float(np.mean(g_ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.vor_n} column-recipe particles, 5 pc cube, coverage_grid buffer 0.05, "
+                               "1 Lloyd iteration, cubic spline", "cells": int(len(geo2["volume"])),
+                   "faces": int(len(geo2["vert_off"]) - 1)},
+        "visited_pairs": int(pairs),
+        "e2e": {"value": pairs / (np.mean(t_ms) * 1e-3), "unit": "pair-integrals/s",
+                "ms_per_step": float(np.mean(t_ms)), "note": "host arrays in and out (kiwi_map_voronoi)"},
+        "cpu_baseline": {"value": pairs / t_ref_map, "unit": "pair-integrals/s", "cores": threads, "kind": "reference",
+                         "sample": f"the whole map: run_mapping_stage's loop, {t_ref_map:.1f} s (geometry build "
+                                   f"{t_geo:.1f} s excluded)"},
+        "agreement_with_reference": {"max_rel_density_diff_top_band": float(np.max(np.abs(r.density[m] - d_ref[m]) /
+                                                                                   d_ref[m])),
+                                     "cells_compared": int(m.sum())},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """Batched sph-to-grid: args.batch_items column snapshots (item i seeded 5000 + i), N log-uniform in
     [nmin, nmax], grid res^3 with res log-uniform in [resmin, resmax], kernels cycling M4 / M6 / WC4; one
@@ -418,6 +478,8 @@ def main():
         return run_batch(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "voronoi":
+        return run_voronoi(args)
     ws, rank, local = dist_env()
     import torch
 
