@@ -131,6 +131,7 @@ enum ScratchSlot {
     S_CELL_MASS,     // FP32-mixed form: per-cell raw mass
     S_TILE_MAP,      // FP32-mixed form: tiles recomputed in FP64
     S_STATS2,        // device counters of a second pass
+    S_VOR_MASK,      // Voronoi walk: per pair, the faces whose neighbour was processed earlier
 };
 
 }  // namespace kiwi_b200

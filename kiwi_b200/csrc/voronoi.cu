@@ -1,20 +1,23 @@
 // Voronoi-cell mapping: the particle loop of run_mapping_stage (src/mapping.cpp:400-502) on the GPU.
 //
 //  (1) k_vor_bfs, one warp per particle (persistent, particles pulled from a counter): the breadth-first
-//      walk of src/mapping.cpp:441-460 over the cell-neighbour graph from the particle's home cell,
-//      entering a neighbour when the shared face's closest point lies within the support radius
-//      (face_reachable: the out_vert rule of src/kernel_integral.cpp:636-645 and
+//      walk of src/mapping.cpp:441-460 over the cell-neighbour graph from the particle's home cell, in
+//      the reference's queue order, entering a neighbour when the shared face's closest point lies within
+//      the support radius (face_reachable: the out_vert rule of src/kernel_integral.cpp:636-645 and
 //      src/mapping.cpp:187-193).  It needs no integrals.  Run twice: first it counts each particle's
-//      visited cells, then it writes them at the particle's offset, so the (cell, particle) pairs come
-//      out grouped by particle in ascending particle order.
-//  (2) a stable radix sort by cell index: every cell's particles stay in ascending order.
+//      visited cells, then it writes them (in walk order) at the particle's offset with, per visited
+//      cell, which of its faces lead to a cell the walk processed earlier.
+//  (2) a stable radix sort of the pairs by cell index: every cell's particles stay in ascending order.
 //  (3) k_vor_gather, one CTA per cell: the cell's faces are staged in shared memory, each thread takes
 //      one particle of the cell's list and evaluates compute_cell_integral (src/mapping.cpp:105-206): the
 //      sum over the cell's faces of the face walk, clamped at 0; the values are then added in particle
 //      order -- the reference's single-threaded summation order, no atomics -- and finalised as
 //      src/mapping.cpp:482-502 does.
-// The reference evaluates a face shared by two visited cells once per particle and reuses its negation
-// on the other side (src/mapping.cpp:56-93); here each side evaluates it: the two agree to rounding.
+// The reference keeps a per-particle cache of face values keyed by the pair of cells (src/mapping.cpp:
+// 56-93): a face towards a cell the walk processed earlier takes that cell's value of their shared face,
+// negated.  Voro++ computes each cell separately, so the two sides' vertices of a shared face can differ
+// (by ~1e-8 in near-degenerate spots), and the side the cache picks shows in the result; the gather
+// therefore takes the same side.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -57,20 +60,28 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 // marker value of particle p in pass `pass`: distinct for every (particle, pass), never -1
 __device__ __forceinline__ int marker(int64_t p, int pass) { return (int)(2 * p + pass); }
 
+// One warp per particle: the particle's BFS over the cell graph in the reference's order
+// (src/mapping.cpp:441-460): cells are processed first in, first out; a processed cell's faces are taken
+// in order, and each unvisited neighbour whose face the kernel reaches is appended -- the lanes test 32
+// faces at a time and append in face order (ballot + prefix count), so the queue is the reference's
+// sequential queue.  A face whose neighbour already appeared on an earlier face of the same cell is a
+// face-cache hit in the reference and discovers nothing.  mark[cell] = (marker << 32) | queue position.
+// Pass 1 also records per (particle, cell) the faces whose neighbour the walk processed earlier (bit i:
+// face i of the cell, first 64 faces): the reference reuses that neighbour's cached, negated face value.
 __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, DevParticles P,
                                                                     const int32_t* __restrict__ home,
                                                                     double support_in_h, int pass,
                                                                     unsigned long long* __restrict__ next,
-                                                                    int* __restrict__ mark_base,
+                                                                    long long* __restrict__ mark_base,
                                                                     int32_t* __restrict__ queue_base,
                                                                     int64_t* __restrict__ counts,
                                                                     const int64_t* __restrict__ offs,
                                                                     int32_t* __restrict__ pair_cells,
+                                                                    unsigned long long* __restrict__ pair_mask,
                                                                     DevStats* __restrict__ st) {
-    __shared__ int s_tail[kBfsWarpsPerBlock];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * kBfsWarpsPerBlock + warp;
-    int* mark = mark_base + slot * C.n_cells;
+    long long* mark = mark_base + slot * C.n_cells;
     int32_t* queue = queue_base + slot * C.n_cells;
     unsigned long long n_unresolved = 0, n_unmapped = 0, n_limit = 0;
     for (;;) {
@@ -89,49 +100,67 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
         }
         const double x0 = P.x[p], y0 = P.y[p], z0 = P.z[p];
         const double radius = mul_rn(support_in_h, h);
-        const int mk = marker((int64_t)p, pass);
+        const long long mk = marker((int64_t)p, pass);
+        const int64_t o = (pass == 1) ? offs[p] : 0;
         if (lane == 0) {
             queue[0] = k0;
-            mark[k0] = mk;
-            s_tail[warp] = 1;
+            mark[k0] = mk << 32;
         }
         __syncwarp();
         int head = 0, tail = 1;
-        int64_t guard = 0;
         while (head < tail) {
-            if (++guard > C.n_cells + 1) {  // cannot happen: each cell enters the queue once
+            if (head > C.n_cells) {  // cannot happen: each cell enters the queue once
                 n_limit += (lane == 0);
                 break;
             }
-            const int batch = min(32, tail - head);
-            if (lane < batch) {
-                const int32_t cell = queue[head + lane];
-                for (int64_t f = C.face_off[cell]; f < C.face_off[cell + 1]; ++f) {
-                    const int32_t nb = C.face_nbr[f];
-                    if (nb < 0 || nb >= C.n_cells) continue;
-                    if (mark[nb] == mk) continue;
-                    const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
-                    const int nv = (int)(C.vert_off[f + 1] - C.vert_off[f]);
-                    if (!face_reachable(x0, y0, z0, radius, V, nv)) continue;
-                    if (atomicExch(&mark[nb], mk) != mk) {
-                        const int pos = atomicAdd(&s_tail[warp], 1);
-                        queue[pos] = nb;
+            const int32_t cell = queue[head];
+            const int64_t fa = C.face_off[cell], fz = C.face_off[cell + 1];
+            unsigned long long earlier = 0;
+            for (int64_t fb = fa; fb < fz; fb += 32) {
+                const int64_t f = fb + lane;
+                bool add = false, before = false;
+                int32_t nb = -1;
+                if (f < fz) {
+                    nb = C.face_nbr[f];
+                    if (nb >= 0 && nb < C.n_cells) {
+                        const long long mv = mark[nb];
+                        const bool seen = (mv >> 32) == mk;
+                        before = seen && (int)(mv & 0xffffffffLL) < head;
+                        if (!seen) {
+                            bool dup = false;
+                            for (int64_t e = fa; e < f; ++e)
+                                if (C.face_nbr[e] == nb) {
+                                    dup = true;
+                                    break;
+                                }
+                            if (!dup) {
+                                const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
+                                add = face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]));
+                            }
+                        }
                     }
                 }
+                const unsigned bb = __ballot_sync(0xffffffffu, before);
+                const int64_t lf = fb - fa;
+                if (lf < 64) earlier |= (unsigned long long)bb << lf;
+                const unsigned ba = __ballot_sync(0xffffffffu, add);
+                if (add) {
+                    const int pos = tail + __popc(ba & ((1u << lane) - 1u));
+                    queue[pos] = nb;
+                    mark[nb] = (mk << 32) | (long long)pos;
+                }
+                tail += __popc(ba);
+                __syncwarp();
             }
-            __syncwarp();
-            head += batch;
-            tail = s_tail[warp];
-            __syncwarp();
+            if (pass == 1 && lane == 0) {
+                pair_cells[o + head] = cell;
+                pair_mask[o + head] = earlier;
+            }
+            ++head;
         }
-        if (pass == 0) {
-            if (lane == 0) {
-                counts[p] = tail;
-                if (tail == 1) ++n_unmapped;
-            }
-        } else {
-            const int64_t o = offs[p];
-            for (int i = lane; i < tail; i += 32) pair_cells[o + i] = queue[i];
+        if (pass == 0 && lane == 0) {
+            counts[p] = tail;
+            if (tail == 1) ++n_unmapped;
         }
         __syncwarp();
     }
@@ -145,18 +174,39 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
     if (lane == 0 && n_limit) atomicAdd(&st->limit_hit, n_limit);
 }
 
-// pair index of particle p's k-th visited cell -> (key = cell, value = particle)
-__global__ void k_vor_pairs(const int32_t* __restrict__ pair_cells, int64_t total, const int64_t* __restrict__ offs,
-                            int64_t n, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+// pair k (particle p's visited cells in BFS order, at offs[p]) -> (key = cell, value = k)
+__global__ void k_vor_pairs(const int32_t* __restrict__ pair_cells, int64_t total, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ vals) {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= total) return;
+    keys[k] = (uint32_t)pair_cells[k];
+    vals[k] = (uint32_t)k;
+}
+
+// The particle of pair k: the last p with offs[p] <= k.
+__device__ __forceinline__ int64_t pair_particle(const int64_t* __restrict__ offs, int64_t n, int64_t k) {
     int64_t lo = 0, hi = n - 1;
     while (lo < hi) {
         const int64_t mid = (lo + hi + 1) >> 1;
         if (offs[mid] <= k) lo = mid; else hi = mid - 1;
     }
-    keys[k] = (uint32_t)pair_cells[k];
-    vals[k] = (uint32_t)lo;
+    return lo;
+}
+
+// One face's integral for one particle (the face walk with the kernel's evaluator).
+template <bool CUBIC>
+static __device__ __noinline__ double vor_face(const double* verts, int nv, double x0, double y0, double z0, double h,
+                                               double radius, int kernel) {
+    const FlatVerts V{verts};
+    if (CUBIC) {
+        CubicEval ev;
+        ev.h = h;
+        return face_integral(x0, y0, z0, 2 * h, V, nv, (int*)nullptr, ev);
+    }
+    GenericEval ev;
+    ev.K = &c_vor_tables[kernel];
+    ev.H = radius;
+    return face_integral(x0, y0, z0, radius, V, nv, (int*)nullptr, ev);
 }
 
 __global__ void k_cell_ranges(const uint32_t* __restrict__ keys, int64_t total, int64_t* __restrict__ range) {
@@ -172,6 +222,9 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
                                                                 double support_in_h,
                                                                 const uint32_t* __restrict__ plist,
                                                                 const int64_t* __restrict__ range,
+                                                                const int64_t* __restrict__ offs,
+                                                                const int32_t* __restrict__ pair_cells,
+                                                                const unsigned long long* __restrict__ pair_mask,
                                                                 CartOutputs out, DevStats* __restrict__ st) {
     __shared__ double s_v[3 * kGatherVertCap];
     __shared__ double s_val[kGatherThreads], s_m[kGatherThreads], s_vx[kGatherThreads], s_vy[kGatherThreads],
@@ -190,26 +243,57 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
         const int64_t k = base + threadIdx.x;
         double msum = 0.0;
         if (k < end) {
-            const uint32_t p = plist[k];
+            const int64_t pk = plist[k];
+            const int64_t p = pair_particle(offs, P.n, pk);
+            const int64_t seg = offs[p], rank = pk - seg;
+            const unsigned long long mask = pair_mask[pk];
             const double x0 = P.x[p], y0 = P.y[p], z0 = P.z[p], h = P.h[p];
             const double radius = mul_rn(support_in_h, h);
-            if (CUBIC) {
-                CubicEval ev;
-                ev.h = h;
+            // compute_cell_integral (src/mapping.cpp:105-206) with its per-particle face cache: a face whose
+            // neighbour this particle's walk processed earlier takes the neighbour's value of their shared
+            // face, negated; a second face towards the same neighbour takes the first one's value; every
+            // other face is evaluated here.  (The two sides' copies of a face can differ in their vertices,
+            // so the choice shows in the result.)
 #pragma unroll 1
-                for (int64_t f = f0; f < f1; ++f) {
-                    const FlatVerts V{staged ? s_v + 3 * (C.vert_off[f] - v0) : C.vxyz + 3 * C.vert_off[f]};
-                    msum += face_integral(x0, y0, z0, 2 * h, V, (int)(C.vert_off[f + 1] - C.vert_off[f]), (int*)nullptr, ev);
+            for (int64_t f = f0; f < f1; ++f) {
+                const int32_t nb = C.face_nbr[f];
+                int64_t src = f;  // the face whose value this face contributes
+                double sign = 1.0;
+                if (nb >= 0 && nb < C.n_cells) {
+                    bool before;
+                    if (f - f0 < 64) {
+                        before = (mask >> (f - f0)) & 1ull;
+                    } else {
+                        before = false;
+                        for (int64_t q = 0; q < rank; ++q)
+                            if (pair_cells[seg + q] == nb) {
+                                before = true;
+                                break;
+                            }
+                    }
+                    int64_t g = -1;
+                    if (before)
+                        for (int64_t e = C.face_off[nb]; e < C.face_off[nb + 1]; ++e)
+                            if (C.face_nbr[e] == (int32_t)cell) {
+                                g = e;
+                                break;
+                            }
+                    if (g >= 0) {
+                        src = g;
+                        sign = -1.0;
+                    } else {
+                        for (int64_t e = f0; e < f; ++e)
+                            if (C.face_nbr[e] == nb) {
+                                src = e;
+                                break;
+                            }
+                    }
                 }
-            } else {
-                GenericEval ev;
-                ev.K = &c_vor_tables[kernel];
-                ev.H = radius;
-#pragma unroll 1
-                for (int64_t f = f0; f < f1; ++f) {
-                    const FlatVerts V{staged ? s_v + 3 * (C.vert_off[f] - v0) : C.vxyz + 3 * C.vert_off[f]};
-                    msum += face_integral(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]), (int*)nullptr, ev);
-                }
+                const int nv = (int)(C.vert_off[src + 1] - C.vert_off[src]);
+                const double* verts = (src >= f0 && src < f1 && staged) ? s_v + 3 * (C.vert_off[src] - v0)
+                                                                         : C.vxyz + 3 * C.vert_off[src];
+                const double val = vor_face<CUBIC>(verts, nv, x0, y0, z0, h, radius, kernel);
+                if (sign < 0.0) msum -= val; else msum += val;
             }
             if (msum < 0.0) {
                 ++n_neg;
@@ -281,10 +365,10 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     int64_t slots = (int64_t)sms * 8;
     const int64_t budget = (int64_t)16 << 30;  // bytes of BFS scratch at most
-    while (slots > kBfsWarpsPerBlock && slots * nc * 8 > budget) slots /= 2;
+    while (slots > kBfsWarpsPerBlock && slots * nc * 12 > budget) slots /= 2;
     slots = std::max<int64_t>(kBfsWarpsPerBlock, (slots / kBfsWarpsPerBlock) * kBfsWarpsPerBlock);
     const int blocks = (int)(slots / kBfsWarpsPerBlock);
-    int* mark = nullptr;
+    long long* mark = nullptr;
     int32_t* queue = nullptr;
     int64_t *counts = nullptr, *offs = nullptr, *range = nullptr;
     KIWI_TRY(scratch_t(ctx, S_VOR_MARK, (size_t)(slots * nc), &mark));
@@ -293,7 +377,7 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_TRY(scratch_t(ctx, S_OFFS, (size_t)std::max<int64_t>(n, 1) + 1, &offs));
     KIWI_TRY(scratch_t(ctx, S_TILE_RANGE, (size_t)(2 * nc), &range));
     int64_t* d_total = offs + std::max<int64_t>(n, 1);
-    KIWI_CUDA(ctx, cudaMemsetAsync(mark, 0xff, sizeof(int) * slots * nc, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemsetAsync(mark, 0xff, sizeof(long long) * slots * nc, ctx->stream));
     KIWI_CUDA(ctx, cudaMemsetAsync(range, 0, sizeof(int64_t) * 2 * nc, ctx->stream));
 
     const double sup = kc.support_in_h;
@@ -301,7 +385,7 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
     if (n > 0) {
         k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 0, d_next, mark, queue,
-                                                                     counts, nullptr, nullptr, d_stats);
+                                                                     counts, nullptr, nullptr, nullptr, d_stats);
         KIWI_LAUNCHED(ctx);
     }
     KIWI_TRY(exclusive_scan<int64_t>(ctx, counts, n, offs, d_total));
@@ -310,8 +394,10 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (total >= (1LL << 32)) return set_err(ctx, KIWI_ERR_LIMIT, "too many (cell, particle) pairs: %lld", (long long)total);
     int32_t* pair_cells = nullptr;
+    unsigned long long* pair_mask = nullptr;
     uint32_t *k0, *v0, *k1, *v1;
     KIWI_TRY(scratch_t(ctx, S_VOR_PAIRS, (size_t)std::max<int64_t>(total, 1), &pair_cells));
+    KIWI_TRY(scratch_t(ctx, S_VOR_MASK, (size_t)std::max<int64_t>(total, 1), &pair_mask));
     KIWI_TRY(scratch_t(ctx, S_KEYS0, (size_t)std::max<int64_t>(total, 1), &k0));
     KIWI_TRY(scratch_t(ctx, S_VALS0, (size_t)std::max<int64_t>(total, 1), &v0));
     KIWI_TRY(scratch_t(ctx, S_KEYS1, (size_t)std::max<int64_t>(total, 1), &k1));
@@ -321,9 +407,9 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
         // pass 1: write each particle's visited cells at its offset
         KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
         k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 1, d_next, mark, queue,
-                                                                     counts, offs, pair_cells, d_stats);
+                                                                     counts, offs, pair_cells, pair_mask, d_stats);
         KIWI_LAUNCHED(ctx);
-        k_vor_pairs<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(pair_cells, total, offs, n, k0, v0);
+        k_vor_pairs<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(pair_cells, total, k0, v0);
         KIWI_LAUNCHED(ctx);
         int key_bits = 1;
         while ((1LL << key_bits) < nc) ++key_bits;
@@ -337,9 +423,11 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     if (nc > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cells (%lld)", (long long)nc);
     if (kc.cubic)
-        k_vor_gather<true><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, kc.kernel, sup, plist, range, out, d_stats);
+        k_vor_gather<true><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, kc.kernel, sup, plist, range, offs,
+                                                                            pair_cells, pair_mask, out, d_stats);
     else
-        k_vor_gather<false><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, kc.kernel, sup, plist, range, out, d_stats);
+        k_vor_gather<false><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, kc.kernel, sup, plist, range, offs,
+                                                                             pair_cells, pair_mask, out, d_stats);
     KIWI_LAUNCHED(ctx);
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     DevStats hs;

@@ -101,13 +101,78 @@ def lattice_cells(n, lo, hi):
             "face_nbr": np.array(nbr, np.int32), "volume": np.array(vol)}, d
 
 
-def test_lattice_voronoi_equals_sph_to_grid(kiwi, ctx):
+def test_lattice_voronoi_equals_sph_to_grid(kiwi, ctx, oracle):
+    """Box cells given as a Voronoi geometry: the map agrees with the oracle's map (the reference's
+    compute_cell_integral, face cache included) to rounding, and with sph-to-grid up to the face cache's
+    effect: a shared face's value taken, negated, from the neighbour's side (the same face with another
+    vertex order) cancels differently in low-density cells (the oracle shows the same 3e-8 there)."""
     n, lo, hi = 10, 0.0, 2.0
     geo, d = lattice_cells(n, lo, hi)
     P = random_particles(60, 17, box=(0.4, 1.6), hmin=0.05, hmax=0.25)
     home = ((np.floor(P["x"] / d) * n + np.floor(P["y"] / d)) * n + np.floor(P["z"] / d)).astype(np.int32)
     v = kiwi.map_voronoi(P, home, geo, raw=True, ctx=ctx)
+    o = oracle.map_voronoi(P, home, geo)[4][0]
     g = kiwi.sph_to_grid(P, (lo, hi, lo, hi, lo, hi), (n, n, n), raw=True, ctx=ctx, precision="fp64_reference_order")
-    m = g.raw[0] > 1e-6 * g.raw[0].max()
-    assert np.max(np.abs(v.raw[0][m] - g.raw[0][m]) / g.raw[0][m]) < 1e-9
+    peak = g.raw[0].max()
+    for band, tol_oracle, tol_grid in ((1e-2, 1e-13, 1e-11), (1e-4, 1e-11, 1e-9), (1e-6, 1e-9, 1e-7)):
+        m = g.raw[0] > band * peak
+        assert np.max(np.abs(v.raw[0][m] - o[m]) / o[m]) < tol_oracle, band
+        assert np.max(np.abs(v.raw[0][m] - g.raw[0][m]) / g.raw[0][m]) < tol_grid, band
     assert abs(v.raw[0].sum() - g.raw[0].sum()) <= 1e-12 * g.raw[0].sum()
+
+
+def _cells_as_lists(geo):
+    fo, vo, vx, nb = geo["face_off"], geo["vert_off"], geo["vxyz"].reshape(-1, 3), geo["face_nbr"]
+    cells = []
+    for c in range(len(geo["volume"])):
+        cells.append([(vx[vo[f]:vo[f + 1]].copy(), int(nb[f])) for f in range(fo[c], fo[c + 1])])
+    return cells
+
+
+def _lists_as_cells(cells, vol):
+    face_off, vert_off, vxyz, nbr = [0], [0], [], []
+    for faces in cells:
+        for v, b in faces:
+            vxyz.extend(v.reshape(-1))
+            vert_off.append(vert_off[-1] + len(v))
+            nbr.append(b)
+        face_off.append(face_off[-1] + len(faces))
+    return {"face_off": np.array(face_off), "vert_off": np.array(vert_off), "vxyz": np.array(vxyz),
+            "face_nbr": np.array(nbr, np.int32), "volume": np.asarray(vol)}
+
+
+def test_face_cache_semantics(kiwi, ctx, oracle):
+    """The reference reuses, negated, the value a neighbouring cell computed for their shared face
+    (src/mapping.cpp:56-206), and a second face towards the same neighbour reuses the first one's value.
+    Here one shared face's two copies differ by 1e-5 in a vertex (Voro++ computes each cell on its own, so
+    copies can differ) and one face is split into two triangles towards the same neighbour: the map must
+    follow the reference's choice of side (the oracle restates it), not evaluate each side itself."""
+    n, lo, hi = 6, 0.0, 1.2
+    geo, d = lattice_cells(n, lo, hi)
+    cells = _cells_as_lists(geo)
+    idx = lambda i, j, k: (i * n + j) * n + k
+    # (a) cell (3,2,2)'s copy of its face towards (2,2,2): one vertex moved by 1e-5 in the face plane
+    c, nb = idx(3, 2, 2), idx(2, 2, 2)
+    for fi, (v, b) in enumerate(cells[c]):
+        if b == nb:
+            v[0, 1] += 1e-5
+    # (b) cell (2,3,2)'s face towards (2,3,3), a quad, split into two triangles with the same neighbour
+    c2, nb2 = idx(2, 3, 2), idx(2, 3, 3)
+    faces = []
+    for v, b in cells[c2]:
+        if b == nb2:
+            faces.append((v[[0, 1, 2]].copy(), b))
+            faces.append((v[[0, 2, 3]].copy(), b))
+        else:
+            faces.append((v, b))
+    cells[c2] = faces
+    g2 = _lists_as_cells(cells, geo["volume"])
+    P = random_particles(80, 29, box=(0.35, 0.85), hmin=0.08, hmax=0.3)
+    home = ((np.floor(P["x"] / d) * n + np.floor(P["y"] / d)) * n + np.floor(P["z"] / d)).astype(np.int32)
+    v = kiwi.map_voronoi(P, home, g2, raw=True, ctx=ctx)
+    o = oracle.map_voronoi(P, home, g2)
+    assert v.stats["visited_pairs"] == o[5]
+    ref = o[4][0]
+    for band, tol in ((1e-2, 1e-12), (1e-4, 1e-11), (1e-6, 1e-9)):
+        m = ref > band * ref.max()
+        assert np.max(np.abs(v.raw[0][m] - ref[m]) / ref[m]) < tol, band
