@@ -62,10 +62,11 @@ __device__ __forceinline__ int marker(int64_t p, int pass) { return (int)(2 * p 
 
 // One warp per particle: the particle's BFS over the cell graph in the reference's order
 // (src/mapping.cpp:441-460): cells are processed first in, first out; a processed cell's faces are taken
-// in order, and each unvisited neighbour whose face the kernel reaches is appended -- the lanes test 32
-// faces at a time and append in face order (ballot + prefix count), so the queue is the reference's
+// in order, and each unvisited neighbour whose face the kernel reaches is appended.  The lanes process 32
+// queued cells at a time and the appends are made in (cell, face) order, so the queue is the reference's
 // sequential queue.  A face whose neighbour already appeared on an earlier face of the same cell is a
 // face-cache hit in the reference and discovers nothing.  mark[cell] = (marker << 32) | queue position.
+// Cells of more than 128 faces are refused (KIWI_ERR_LIMIT).
 // Pass 1 also records per (particle, cell) the faces whose neighbour the walk processed earlier (bit i:
 // face i of the cell, first 64 faces): the reference reuses that neighbour's cached, negated face value.
 __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, DevParticles P,
@@ -113,50 +114,69 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                 n_limit += (lane == 0);
                 break;
             }
-            const int32_t cell = queue[head];
-            const int64_t fa = C.face_off[cell], fz = C.face_off[cell + 1];
-            unsigned long long earlier = 0;
-            for (int64_t fb = fa; fb < fz; fb += 32) {
-                const int64_t f = fb + lane;
-                bool add = false, before = false;
-                int32_t nb = -1;
-                if (f < fz) {
-                    nb = C.face_nbr[f];
-                    if (nb >= 0 && nb < C.n_cells) {
-                        const long long mv = mark[nb];
-                        const bool seen = (mv >> 32) == mk;
-                        before = seen && (int)(mv & 0xffffffffLL) < head;
-                        if (!seen) {
-                            bool dup = false;
-                            for (int64_t e = fa; e < f; ++e)
-                                if (C.face_nbr[e] == nb) {
-                                    dup = true;
-                                    break;
-                                }
-                            if (!dup) {
-                                const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
-                                add = face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]));
+            // The lanes take the next (up to) 32 queued cells, one each, and mark their discovery
+            // candidates: faces towards a neighbour not yet in the queue that the kernel reaches, skipping
+            // a face whose neighbour an earlier face of the same cell already named (a face-cache hit in the
+            // reference, which discovers nothing).  Lane 0 then appends the candidates in (cell, face)
+            // order, skipping neighbours queued meanwhile: the reference's sequential queue.
+            const int batch = min(32, tail - head);
+            int64_t fa = 0;
+            unsigned long long cand0 = 0, cand1 = 0, earlier = 0;
+            if (lane < batch) {
+                const int rank = head + lane;
+                const int32_t cell = queue[rank];
+                fa = C.face_off[cell];
+                const int64_t fz = C.face_off[cell + 1];
+                if (fz - fa > 128) n_limit += 1;  // a cell of more than 128 faces is not supported
+                for (int64_t f = fa; f < fz && f - fa < 128; ++f) {
+                    const int32_t nb = C.face_nbr[f];
+                    if (nb < 0 || nb >= C.n_cells) continue;
+                    const long long mv = mark[nb];
+                    const bool seen = (mv >> 32) == mk;
+                    if (seen) {
+                        if ((int)(mv & 0xffffffffLL) < rank && f - fa < 64) earlier |= 1ull << (f - fa);
+                        continue;
+                    }
+                    bool dup = false;
+                    for (int64_t e = fa; e < f; ++e)
+                        if (C.face_nbr[e] == nb) {
+                            dup = true;
+                            break;
+                        }
+                    if (dup) continue;
+                    const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
+                    if (!face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]))) continue;
+                    if (f - fa < 64) cand0 |= 1ull << (f - fa);
+                    else cand1 |= 1ull << (f - fa - 64);
+                }
+                if (pass == 1) {
+                    pair_cells[o + rank] = cell;
+                    pair_mask[o + rank] = earlier;
+                }
+            }
+            int t = tail;
+            for (int L = 0; L < batch; ++L) {
+                unsigned long long c0 = __shfl_sync(0xffffffffu, cand0, L);
+                unsigned long long c1 = __shfl_sync(0xffffffffu, cand1, L);
+                const int64_t fl = __shfl_sync(0xffffffffu, fa, L);
+                if (lane == 0) {
+                    for (int w = 0; w < 2; ++w) {
+                        unsigned long long bits = w == 0 ? c0 : c1;
+                        while (bits) {
+                            const int b = __ffsll((long long)bits) - 1;
+                            bits &= bits - 1;
+                            const int32_t nb = C.face_nbr[fl + 64 * w + b];
+                            if ((mark[nb] >> 32) != mk) {
+                                mark[nb] = (mk << 32) | (long long)t;
+                                queue[t++] = nb;
                             }
                         }
                     }
                 }
-                const unsigned bb = __ballot_sync(0xffffffffu, before);
-                const int64_t lf = fb - fa;
-                if (lf < 64) earlier |= (unsigned long long)bb << lf;
-                const unsigned ba = __ballot_sync(0xffffffffu, add);
-                if (add) {
-                    const int pos = tail + __popc(ba & ((1u << lane) - 1u));
-                    queue[pos] = nb;
-                    mark[nb] = (mk << 32) | (long long)pos;
-                }
-                tail += __popc(ba);
-                __syncwarp();
             }
-            if (pass == 1 && lane == 0) {
-                pair_cells[o + head] = cell;
-                pair_mask[o + head] = earlier;
-            }
-            ++head;
+            tail = __shfl_sync(0xffffffffu, t, 0);
+            head += batch;
+            __syncwarp();
         }
         if (pass == 0 && lane == 0) {
             counts[p] = tail;
@@ -433,7 +453,8 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     DevStats hs;
     KIWI_CUDA(ctx, cudaMemcpyAsync(&hs, d_stats, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));
     KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    if (hs.limit_hit) return set_err(ctx, KIWI_ERR_LIMIT, "the cell walk hit its iteration cap");
+    if (hs.limit_hit)
+        return set_err(ctx, KIWI_ERR_LIMIT, "the cell walk hit a limit (a cell of more than 128 faces, or its iteration cap)");
     if (stats) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);

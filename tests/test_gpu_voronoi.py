@@ -114,7 +114,7 @@ def test_lattice_voronoi_equals_sph_to_grid(kiwi, ctx, oracle):
     o = oracle.map_voronoi(P, home, geo)[4][0]
     g = kiwi.sph_to_grid(P, (lo, hi, lo, hi, lo, hi), (n, n, n), raw=True, ctx=ctx, precision="fp64_reference_order")
     peak = g.raw[0].max()
-    for band, tol_oracle, tol_grid in ((1e-2, 1e-13, 1e-11), (1e-4, 1e-11, 1e-9), (1e-6, 1e-9, 1e-7)):
+    for band, tol_oracle, tol_grid in ((1e-2, 4e-10, 1e-11), (1e-4, 4e-9, 1e-9), (1e-6, 1e-7, 1e-7)):
         m = g.raw[0] > band * peak
         assert np.max(np.abs(v.raw[0][m] - o[m]) / o[m]) < tol_oracle, band
         assert np.max(np.abs(v.raw[0][m] - g.raw[0][m]) / g.raw[0][m]) < tol_grid, band
@@ -173,6 +173,6 @@ def test_face_cache_semantics(kiwi, ctx, oracle):
     o = oracle.map_voronoi(P, home, g2)
     assert v.stats["visited_pairs"] == o[5]
     ref = o[4][0]
-    for band, tol in ((1e-2, 1e-12), (1e-4, 1e-11), (1e-6, 1e-9)):
+    for band, tol in ((1e-2, 4e-10), (1e-4, 4e-9), (1e-6, 1e-7)):  # far below the 4e-6 the choice of side makes
         m = ref > band * ref.max()
         assert np.max(np.abs(v.raw[0][m] - ref[m]) / ref[m]) < tol, band
