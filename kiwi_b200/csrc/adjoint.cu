@@ -13,98 +13,325 @@
 // gradient.  The pairs are those of the forward's default evaluation: the cells of the particle's
 // support bounding box whose closest point lies within the support radius.
 //
-// One warp per particle: the lanes stride over the particle's support cells and the eight per-lane sums
-// are combined by a fixed xor-shuffle tree, so the result is deterministic and no atomics touch the
-// gradients.
+// The evaluation is the lattice form of the forward pass (lattice.cuh) in Dual4: one CTA per 8^3-cell
+// tile walks the tile's particles in chunks; (A) the edge tiers of every (plane, edge line) and (B) the
+// corner values of every (plane, lattice point) are computed once per particle with their derivatives;
+// (C) for each particle, each thread assembles the cells it owns from the 24 corner values (value and
+// derivatives alike), weighs them with the cells' cotangents, and a fixed-order block reduction writes the
+// particle's partial gradient for this tile to its (tile, particle) entry.  (D) Each particle's entries
+// are then added in tile order.  Deterministic, no atomics on the gradients.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
+#include "binning.cuh"
 #include "cart_common.cuh"
 #include "ctx.hpp"
 #include "dual.cuh"
 #include "engine.hpp"
 #include "kiwi_math.cuh"
+#include "lattice.cuh"
+#include "prims.cuh"
 
 namespace kiwi_b200 {
 
 namespace {
 
-constexpr int kAdjThreads = 128;
-constexpr int kAdjWarps = kAdjThreads / 32;
+constexpr int kAdjLatThreads = 256;
+constexpr int kAdjCellsPerThread = kTileCells / kAdjLatThreads;
+constexpr int kAdjPMax = 32;
+constexpr int kAdjECap = 512;   // edge entries per chunk (a full 8^3 particle box needs 486)
+constexpr int kAdjSCap = 2304;  // corner entries per chunk (a full 8^3 particle box needs 2187)
+constexpr int kAdjERec = 10;    // D2, D3 as Dual4
+constexpr int kAdjSRec = 5;     // S as Dual4
+constexpr size_t kAdjDynSmem = sizeof(double) * (kAdjERec * kAdjECap + kAdjSRec * kAdjSCap);
 
 struct AdjGrads {
     double *x, *y, *z, *h, *m, *vx, *vy, *vz;
 };
 
-__global__ void __launch_bounds__(kAdjThreads) k_cart_adjoint(DevParticles P, CartGeom g,
-                                                             const double* __restrict__ cot, AdjGrads G,
-                                                             DevStats* __restrict__ st) {
-    const int lane = threadIdx.x & 31;
-    const int64_t nwarps = (int64_t)gridDim.x * kAdjWarps;
+__device__ __forceinline__ Dual4 dual_abs_offset(double off, int axis) {
+    // |plane - x_axis| and its derivative with respect to the particle's coordinate on that axis
+    Dual4 r(fabs(off));
+    r.d[axis] = off > 0.0 ? -1.0 : (off < 0.0 ? 1.0 : 0.0);
+    return r;
+}
+
+__device__ __forceinline__ Dual4 load_dual(const double* p) {
+    Dual4 r(p[0]);
+    r.d[0] = p[1];
+    r.d[1] = p[2];
+    r.d[2] = p[3];
+    r.d[3] = p[4];
+    return r;
+}
+
+__device__ __forceinline__ void store_dual(double* p, const Dual4& v) {
+    p[0] = v.v;
+    p[1] = v.d[0];
+    p[2] = v.d[1];
+    p[3] = v.d[2];
+    p[4] = v.d[3];
+}
+
+__device__ __forceinline__ unsigned long long block_count(unsigned long long v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// (A)-(C) for one tile: list holds (tile, particle) entry indices (the entries of particle p are
+// offs[p] .. offs[p+1]-1); part receives 8 doubles per entry: dL/dm, dL/d(x, y, z, h), dL/d(vx, vy, vz)
+// over this tile's cells.
+__global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(CartGeom g, DevParticles P,
+                                                                          const uint32_t* __restrict__ list,
+                                                                          const int64_t* __restrict__ range,
+                                                                          const int64_t* __restrict__ offs,
+                                                                          const double* __restrict__ cot,
+                                                                          double* __restrict__ part,
+                                                                          DevStats* __restrict__ st) {
+    __shared__ double s_x[kAdjPMax], s_y[kAdjPMax], s_z[kAdjPMax], s_h[kAdjPMax], s_m[kAdjPMax], s_vx[kAdjPMax],
+        s_vy[kAdjPMax], s_vz[kAdjPMax];
+    __shared__ int s_lo[kAdjPMax][3], s_dim[kAdjPMax][3], s_eoff[kAdjPMax], s_soff[kAdjPMax];
+    __shared__ uint32_t s_entry[kAdjPMax];
+    __shared__ int s_np, s_etot, s_stot;
+    __shared__ double s_red[kAdjLatThreads / 32][8];
+    extern __shared__ double s_adj[];
+    double* s_E = s_adj;
+    double* s_S = s_adj + kAdjERec * kAdjECap;
+
+    const int64_t t = blockIdx.x;
+    const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
+    const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
     unsigned long long n_eval = 0, n_neg = 0;
-    for (int64_t p = (int64_t)blockIdx.x * kAdjWarps + threadIdx.x / 32; p < P.n; p += nwarps) {
-        const double x0 = P.x[p], y0 = P.y[p], z0 = P.z[p], h = P.h[p];
-        const double pvx = P.vx[p], pvy = P.vy[p], pvz = P.vz[p], pm = P.m[p];
-        // 0: sum K gs; 1-4: sum dK/d(x,y,z,h) gs; 5-7: sum K gP   (gs = gM + v . gP)
-        double acc[8];
+    const int64_t beg = range[2 * t], end = range[2 * t + 1];
+
+    for (int64_t pos = beg; pos < end;) {
+        if (warp == 0) {
+            const int64_t idx = pos + lane;
+            int ne = 0, ns = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+            double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
+            uint32_t e = 0;
+            if (idx < end) {
+                e = list[idx];
+                int64_t lo = 0, hi = P.n - 1;  // the entry's particle: the last p with offs[p] <= e
+                while (lo < hi) {
+                    const int64_t mid = (lo + hi + 1) >> 1;
+                    if (offs[mid] <= (int64_t)e) lo = mid; else hi = mid - 1;
+                }
+                const int64_t p = lo;
+                px = P.x[p]; py = P.y[p]; pz = P.z[p]; ph = P.h[p];
+                pm = P.m[p]; pvx = P.vx[p]; pvy = P.vy[p]; pvz = P.vz[p];
+                CellBox b;
+                bool outside;
+                particle_cell_box(g, px, py, pz, ph, b, &outside);
+                lo0 = max(b.x0, bx); lo1 = max(b.y0, by); lo2 = max(b.z0, bz);
+                d0 = min(b.x1, bx + kTileX - 1) - lo0 + 1;
+                d1 = min(b.y1, by + kTileY - 1) - lo1 + 1;
+                d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
+                const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
+                ne = 2 * (n0 * n1 + n0 * n2 + n1 * n2);
+                ns = 3 * n0 * n1 * n2;
+            }
+            int ie = ne, is = ns;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vs = __shfl_up_sync(0xffffffffu, is, o);
+                if (lane >= o) {
+                    ie += ve;
+                    is += vs;
+                }
+            }
+            const bool take = (idx < end) && ie <= kAdjECap && is <= kAdjSCap;
+            const int np = __popc(__ballot_sync(0xffffffffu, take));
+            if (take) {
+                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph;
+                s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
+                s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
+                s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
+                s_eoff[lane] = ie - ne;
+                s_soff[lane] = is - ns;
+                s_entry[lane] = e;
+            }
+            if (lane == np - 1) {
+                s_np = np;
+                s_etot = ie;
+                s_stot = is;
+            }
+        }
+        __syncthreads();
+        const int np = s_np, etot = s_etot, stot = s_stot;
+
+        // (A) edge tiers with derivatives
+        for (int it = threadIdx.x; it < etot; it += kAdjLatThreads) {
+            const int j = chunk_search(s_eoff, np, it);
+            int e = it - s_eoff[j];
+            const int n[3] = {s_dim[j][0] + 1, s_dim[j][1] + 1, s_dim[j][2] + 1};
+            int a = 0, bax = 1;
+            {
+                const int sz[6] = {n[0] * n[1], n[0] * n[2], n[1] * n[0], n[1] * n[2], n[2] * n[0], n[2] * n[1]};
+                const int aa[6] = {0, 0, 1, 1, 2, 2}, bb[6] = {1, 2, 0, 2, 0, 1};
+                int blk = 0;
+                while (e >= sz[blk]) {
+                    e -= sz[blk];
+                    ++blk;
+                }
+                a = aa[blk];
+                bax = bb[blk];
+            }
+            const int p = e / n[bax], q = e % n[bax];
+            const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
+            const double pc[3] = {s_x[j], s_y[j], s_z[j]};
+            const Dual4 r0 = dual_abs_offset(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]), a);
+            const Dual4 R0 = dual_abs_offset(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]), bax);
+            const Dual4 hD = Dual4::seed(s_h[j], 3);
+            const CubicWallT<Dual4> w = cubic_wall_t<Dual4>(hD, r0);
+            const CubicEdgeT<Dual4> ed = cubic_edge_t<Dual4>(w, R0);
+            store_dual(s_E + kAdjERec * it, ed.D2);
+            store_dual(s_E + kAdjERec * it + 5, ed.D3);
+        }
+        __syncthreads();
+
+        // (B) corner values with derivatives
+        for (int it = threadIdx.x; it < stot; it += kAdjLatThreads) {
+            const int jp = chunk_search(s_soff, np, it);
+            const int s = it - s_soff[jp];
+            const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+            const int L = n0 * n1 * n2;
+            const int axis = s / L, rem = s % L;
+            const int i = rem / (n1 * n2), jj = (rem / n2) % n1, k = rem % n2;
+            const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
+            const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
+            const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+            const int eb = s_eoff[jp];
+            const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
+            double ua, u1, u2;
+            int ax1, ax2, e1, e2;
+            if (axis == 0) {
+                ua = ux; u1 = uy; u2 = uz; ax1 = 1; ax2 = 2;
+                e1 = eb + i * n1 + jj;
+                e2 = eb + nxy + i * n2 + k;
+            } else if (axis == 1) {
+                ua = uy; u1 = ux; u2 = uz; ax1 = 0; ax2 = 2;
+                e1 = eb + nxy + nxz + jj * n0 + i;
+                e2 = eb + 2 * nxy + nxz + jj * n2 + k;
+            } else {
+                ua = uz; u1 = ux; u2 = uy; ax1 = 0; ax2 = 1;
+                e1 = eb + 2 * nxy + nxz + nyz + k * n0 + i;
+                e2 = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
+            }
+            Dual4 f(0.0);
+            const double sg = sgn(u1) * sgn(u2);
+            if (sg != 0.0 && ua != 0.0) {
+                const Dual4 r0 = dual_abs_offset(ua, axis);
+                const Dual4 a1 = dual_abs_offset(u1, ax1), a2 = dual_abs_offset(u2, ax2);
+                const Dual4 hD = Dual4::seed(s_h[jp], 3);
+                f = lattice_vertex_t<Dual4>(hD, r0, a1, a2, load_dual(s_E + kAdjERec * e1), load_dual(s_E + kAdjERec * e1 + 5)) +
+                    lattice_vertex_t<Dual4>(hD, r0, a2, a1, load_dual(s_E + kAdjERec * e2), load_dual(s_E + kAdjERec * e2 + 5));
+            }
+            store_dual(s_S + kAdjSRec * it, sg * f);
+        }
+        __syncthreads();
+
+        // (C) per particle: the cells' values and derivatives from the corners, weighed by the cotangents
+        for (int j = 0; j < np; ++j) {
+            double acc[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] = 0.0;
-        CellBox b;
-        bool outside;
-        if (particle_cell_box(g, x0, y0, z0, h, b, &outside)) {
-            const int dy = b.y1 - b.y0 + 1, dz = b.z1 - b.z0 + 1;
-            const int64_t nb = (int64_t)(b.x1 - b.x0 + 1) * dy * dz;
-            const double radius = mul_rn(g.support_in_h, h);
-            for (int64_t k = lane; k < nb; k += 32) {
-                const int iz = b.z0 + (int)(k % dz);
-                const int iy = b.y0 + (int)((k / dz) % dy);
-                const int ix = b.x0 + (int)(k / ((int64_t)dz * dy));
-                const double cx = cell_centre(g.x_min, ix, g.dpx);
-                const double cy = cell_centre(g.y_min, iy, g.dpy);
-                const double cz = cell_centre(g.z_min, iz, g.dpz);
-                const double ex = fmax(fabs(x0 - cx) - g.hpx, 0.0);
-                const double ey = fmax(fabs(y0 - cy) - g.hpy, 0.0);
-                const double ez = fmax(fabs(z0 - cz) - g.hpz, 0.0);
+            for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+            const double x0 = s_x[j], y0 = s_y[j], z0 = s_z[j];
+            const double radius = mul_rn(g.support_in_h, s_h[j]);
+            const int n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
+            const int L = (s_dim[j][0] + 1) * n1 * n2;
+            const double* Sx = s_S + kAdjSRec * s_soff[j];
+            const double* Sy = Sx + kAdjSRec * L;
+            const double* Sz = Sy + kAdjSRec * L;
+#pragma unroll
+            for (int c = 0; c < kAdjCellsPerThread; ++c) {
+                const int li = threadIdx.x + c * kAdjLatThreads;
+                const int gz = bz + li % kTileZ, gy = by + (li / kTileZ) % kTileY, gx = bx + li / (kTileZ * kTileY);
+                const int i = gx - s_lo[j][0], jj = gy - s_lo[j][1], k = gz - s_lo[j][2];
+                if (i < 0 || jj < 0 || k < 0 || i >= s_dim[j][0] || jj >= s_dim[j][1] || k >= s_dim[j][2]) continue;
+                const double ex = fmax(fabs(x0 - cell_centre(g.x_min, gx, g.dpx)) - g.hpx, 0.0);
+                const double ey = fmax(fabs(y0 - cell_centre(g.y_min, gy, g.dpy)) - g.hpy, 0.0);
+                const double ez = fmax(fabs(z0 - cell_centre(g.z_min, gz, g.dpz)) - g.hpz, 0.0);
                 if (!(ex * ex + ey * ey + ez * ez < radius * radius)) continue;
-                CubicEvalT<Dual4> ev;
-                ev.h = Dual4::seed(h, 3);
-                const Dual4 msum = box_cell_msum<Dual4>(Dual4::seed(x0, 0), Dual4::seed(y0, 1), Dual4::seed(z0, 2),
-                                                        2 * ev.h, cx, cy, cz, g.hpx, g.hpy, g.hpz, ev);
                 ++n_eval;
-                if (msum.v < 0.0) {
+                const double sx1 = sgn(lattice_offset(g.x_min, g.dpx, gx + 1, x0)), sx0 = sgn(lattice_offset(g.x_min, g.dpx, gx, x0));
+                const double sy1 = sgn(lattice_offset(g.y_min, g.dpy, gy + 1, y0)), sy0 = sgn(lattice_offset(g.y_min, g.dpy, gy, y0));
+                const double sz1 = sgn(lattice_offset(g.z_min, g.dpz, gz + 1, z0)), sz0 = sgn(lattice_offset(g.z_min, g.dpz, gz, z0));
+                // component comp of the cell's Msum: 0 the value (the forward's sum, same order), 1..4 d/d(x, y, z, h)
+                auto cell_sum = [&](int comp) {
+                    auto at = [&](const double* S, int a, int b, int cc) { return S[kAdjSRec * ((a * n1 + b) * n2 + cc) + comp]; };
+                    double m = 0.0;
+                    m += sx1 * (at(Sx, i + 1, jj + 1, k + 1) - at(Sx, i + 1, jj, k + 1) - at(Sx, i + 1, jj + 1, k) + at(Sx, i + 1, jj, k));
+                    m -= sx0 * (at(Sx, i, jj + 1, k + 1) - at(Sx, i, jj, k + 1) - at(Sx, i, jj + 1, k) + at(Sx, i, jj, k));
+                    m += sy1 * (at(Sy, i + 1, jj + 1, k + 1) - at(Sy, i, jj + 1, k + 1) - at(Sy, i + 1, jj + 1, k) + at(Sy, i, jj + 1, k));
+                    m -= sy0 * (at(Sy, i + 1, jj, k + 1) - at(Sy, i, jj, k + 1) - at(Sy, i + 1, jj, k) + at(Sy, i, jj, k));
+                    m += sz1 * (at(Sz, i + 1, jj + 1, k + 1) - at(Sz, i, jj + 1, k + 1) - at(Sz, i + 1, jj, k + 1) + at(Sz, i, jj, k + 1));
+                    m -= sz0 * (at(Sz, i + 1, jj + 1, k) - at(Sz, i, jj + 1, k) - at(Sz, i + 1, jj, k) + at(Sz, i, jj, k));
+                    return m;
+                };
+                const double msum = cell_sum(0);
+                if (msum < 0.0) {
                     ++n_neg;
                     continue;
                 }
-                if (msum.v == 0.0) continue;
-                const int64_t i3 = ((int64_t)ix * g.ny + iy) * g.nz + iz;
-                const double gM = cot[i3], gx = cot[ncell + i3], gy = cot[2 * ncell + i3], gz = cot[3 * ncell + i3];
-                const double gs = gM + pvx * gx + pvy * gy + pvz * gz;
-                acc[0] += msum.v * gs;
-                acc[1] += msum.d[0] * gs;
-                acc[2] += msum.d[1] * gs;
-                acc[3] += msum.d[2] * gs;
-                acc[4] += msum.d[3] * gs;
-                acc[5] += msum.v * gx;
-                acc[6] += msum.v * gy;
-                acc[7] += msum.v * gz;
+                if (msum == 0.0) continue;
+                const int64_t i3 = ((int64_t)gx * g.ny + gy) * g.nz + gz;
+                const double gM = cot[i3], gx_ = cot[ncell + i3], gy_ = cot[2 * ncell + i3], gz_ = cot[3 * ncell + i3];
+                const double gs = gM + s_vx[j] * gx_ + s_vy[j] * gy_ + s_vz[j] * gz_;
+                acc[0] += msum * gs;
+#pragma unroll 1
+                for (int comp = 1; comp <= 4; ++comp) acc[comp] += cell_sum(comp) * gs;
+                acc[5] += msum * gx_;
+                acc[6] += msum * gy_;
+                acc[7] += msum * gz_;
             }
-        }
+            // fixed-order block reduction: xor tree within each warp, then the warps in order
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-            for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
-        if (lane == 0) {
-            if (G.m) G.m[p] = acc[0];
-            if (G.x) G.x[p] = pm * acc[1];
-            if (G.y) G.y[p] = pm * acc[2];
-            if (G.z) G.z[p] = pm * acc[3];
-            if (G.h) G.h[p] = pm * acc[4];
-            if (G.vx) G.vx[p] = pm * acc[5];
-            if (G.vy) G.vy[p] = pm * acc[6];
-            if (G.vz) G.vz[p] = pm * acc[7];
+            for (int c = 0; c < 8; ++c)
+                for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+            if (lane == 0)
+#pragma unroll
+                for (int c = 0; c < 8; ++c) s_red[warp][c] = acc[c];
+            __syncthreads();
+            if (threadIdx.x < 8) {
+                double v = 0.0;
+                for (int w = 0; w < kAdjLatThreads / 32; ++w) v += s_red[w][threadIdx.x];
+                const double pm = s_m[j];
+                part[8 * (int64_t)s_entry[j] + threadIdx.x] = (threadIdx.x == 0) ? v : pm * v;
+            }
+            __syncthreads();
         }
+        pos += np;
     }
-    if (n_eval) atomicAdd(&st->evaluated_pairs, n_eval);
-    if (n_neg) atomicAdd(&st->neg_clamped, n_neg);
+    n_eval = block_count(n_eval);
+    n_neg = block_count(n_neg);
+    if (lane == 0) {
+        if (n_eval) atomicAdd(&st->evaluated_pairs, n_eval);
+        if (n_neg) atomicAdd(&st->neg_clamped, n_neg);
+    }
+}
+
+// (D) each particle's gradient: its entries' partial sums in tile order.
+__global__ void k_adjoint_reduce(int64_t n, const int64_t* __restrict__ offs, const double* __restrict__ part,
+                                 AdjGrads G) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    double acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = 0.0;
+    for (int64_t e = offs[p]; e < offs[p + 1]; ++e)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] += part[8 * e + c];
+    if (G.m) G.m[p] = acc[0];
+    if (G.x) G.x[p] = acc[1];
+    if (G.y) G.y[p] = acc[2];
+    if (G.z) G.z[p] = acc[3];
+    if (G.h) G.h[p] = acc[4];
+    if (G.vx) G.vx[p] = acc[5];
+    if (G.vy) G.vy[p] = acc[6];
+    if (G.vz) G.vz[p] = acc[7];
 }
 
 }  // namespace
@@ -115,16 +342,55 @@ int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, con
         return set_err(ctx, KIWI_ERR_UNSUPPORTED,
                        "the adjoint is available for the cubic spline kernel with support 2h (generic_path unset)");
     DevStats* d_st = nullptr;
-    KIWI_TRY(scratch(ctx, S_MISC3, sizeof(DevStats), (void**)&d_st));
+    KIWI_TRY(scratch_t(ctx, S_STATS, 1, &d_st));
     KIWI_CUDA(ctx, cudaMemsetAsync(d_st, 0, sizeof(DevStats), ctx->stream));
-    if (P.n > 0) {
-        int dev_sms = 148;
-        cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        const int64_t want = (P.n + kAdjWarps - 1) / kAdjWarps;
-        const int64_t cap = (int64_t)dev_sms * 16;
-        const int blocks = (int)(want < cap ? want : cap);
+    const int64_t n = P.n;
+    const int64_t ntiles = (int64_t)g.ntx * g.nty * g.ntz;
+    // binning as the forward pass, with the sort carrying each (tile, particle) entry's index
+    uint32_t* counts = nullptr;
+    TileBox* boxes = nullptr;
+    int64_t *offs = nullptr, *range = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_COUNT, (size_t)std::max<int64_t>(n, 1), &counts));
+    KIWI_TRY(scratch_t(ctx, S_BOX, (size_t)std::max<int64_t>(n, 1), &boxes));
+    KIWI_TRY(scratch_t(ctx, S_OFFS, (size_t)std::max<int64_t>(n, 1) + 1, &offs));
+    KIWI_TRY(scratch_t(ctx, S_TILE_RANGE, (size_t)(2 * ntiles), &range));
+    int64_t* d_total = offs + std::max<int64_t>(n, 1);
+    KIWI_CUDA(ctx, cudaMemsetAsync(range, 0, sizeof(int64_t) * 2 * ntiles, ctx->stream));
+    if (n > 0) {
+        k_tile_counts<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(g, P, counts, boxes, d_st);
+        KIWI_LAUNCHED(ctx);
+    }
+    KIWI_TRY(exclusive_scan<uint32_t>(ctx, counts, n, offs, d_total));
+    int64_t total = 0;
+    KIWI_CUDA(ctx, cudaMemcpyAsync(&total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (total >= (1LL << 32)) return set_err(ctx, KIWI_ERR_LIMIT, "too many (tile, particle) entries: %lld", (long long)total);
+    uint32_t *k0, *v0, *k1, *v1;
+    double* part = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_KEYS0, (size_t)std::max<int64_t>(total, 1), &k0));
+    KIWI_TRY(scratch_t(ctx, S_VALS0, (size_t)std::max<int64_t>(total, 1), &v0));
+    KIWI_TRY(scratch_t(ctx, S_KEYS1, (size_t)std::max<int64_t>(total, 1), &k1));
+    KIWI_TRY(scratch_t(ctx, S_VALS1, (size_t)std::max<int64_t>(total, 1), &v1));
+    KIWI_TRY(scratch_t(ctx, S_ADJ_PART, (size_t)8 * std::max<int64_t>(total, 1), &part));
+    if (total > 0) {
+        k_tile_emit<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(g, n, offs, boxes, 0, total, 0u, k0, v0,
+                                                                              true);
+        KIWI_LAUNCHED(ctx);
+        int key_bits = 1;
+        while ((1LL << key_bits) < ntiles) ++key_bits;
+        bool second = false;
+        KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, total, key_bits, &second));
+        k_tile_ranges<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(second ? k1 : k0, total, range);
+        KIWI_LAUNCHED(ctx);
+        KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_adjoint_lattice, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kAdjDynSmem));
+        k_cart_adjoint_lattice<<<(unsigned)ntiles, kAdjLatThreads, kAdjDynSmem, ctx->stream>>>(
+            g, P, second ? v1 : v0, range, offs, d_cot, part, d_st);
+        KIWI_LAUNCHED(ctx);
+    }
+    if (n > 0) {
         AdjGrads G{out.x, out.y, out.z, out.h, out.m, out.vx, out.vy, out.vz};
-        k_cart_adjoint<<<blocks, kAdjThreads, 0, ctx->stream>>>(P, g, d_cot, G, d_st);
+        k_adjoint_reduce<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, offs, part, G);
         KIWI_LAUNCHED(ctx);
     }
     if (stats) {
@@ -133,6 +399,8 @@ int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, con
         KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         stats->evaluated_pairs = (int64_t)h.evaluated_pairs;
         stats->neg_clamped = (int64_t)h.neg_clamped;
+        stats->skipped_outside = (int64_t)h.skipped_outside;
+        stats->tile_pairs = total;
     }
     return KIWI_OK;
 }

@@ -38,11 +38,12 @@ static __global__ void k_tile_counts(CartGeom g, DevParticles P, uint32_t* __res
 }
 
 // One thread per (particle, tile) entry k in [k0, k0 + count): key = key_base + tile id, value = particle
-// index, written in particle order (offs: the exclusive scan of the counts of these n particles, whose
-// first entry is k0 -- entries of several grids can share one key space and one sort).
+// index (or, with value_is_entry, the entry index k itself), written in particle order (offs: the
+// exclusive scan of the counts of these n particles, whose first entry is k0 -- entries of several grids
+// can share one key space and one sort).
 static __global__ void k_tile_emit(CartGeom g, int64_t n, const int64_t* __restrict__ offs, const TileBox* __restrict__ boxes,
                             int64_t k0, int64_t count, uint32_t key_base, uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ vals) {
+                            uint32_t* __restrict__ vals, bool value_is_entry = false) {
     const int64_t kk = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (kk >= count) return;
     const int64_t k = k0 + kk;
@@ -57,7 +58,7 @@ static __global__ void k_tile_emit(CartGeom g, int64_t n, const int64_t* __restr
     const int dz = tb.z1 - tb.z0 + 1, dy = tb.y1 - tb.y0 + 1;
     const int tz = tb.z0 + (int)(q % dz), ty = tb.y0 + (int)((q / dz) % dy), tx = tb.x0 + (int)(q / ((int64_t)dz * dy));
     keys[k] = key_base + (uint32_t)(((int64_t)tx * g.nty + ty) * g.ntz + tz);
-    vals[k] = (uint32_t)lo;
+    vals[k] = value_is_entry ? (uint32_t)k : (uint32_t)lo;
 }
 
 // range[2t], range[2t+1] = [begin, end) of tile t in the sorted key array (zero-length if absent).

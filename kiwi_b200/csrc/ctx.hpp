@@ -132,6 +132,7 @@ enum ScratchSlot {
     S_TILE_MAP,      // FP32-mixed form: tiles recomputed in FP64
     S_STATS2,        // device counters of a second pass
     S_VOR_MASK,      // Voronoi walk: per pair, the faces whose neighbour was processed earlier
+    S_ADJ_PART,      // adjoint: partial gradients per (tile, particle) entry
 };
 
 }  // namespace kiwi_b200

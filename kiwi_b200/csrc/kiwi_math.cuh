@@ -154,10 +154,11 @@ KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) { return cubic_edge
 // I1 = atan(u/a) alone, by the same operations as the full series: beyond 2h the vertex tier needs only
 // I0 = phi and I1, so the logarithms, tan and I_2..I_5 (dead there) can be skipped where whole warps are
 // in that region (the lattice kernel groups its corner items that way).
-KIWI_HD double phi_I1(double sinp, double cosp, double a, double a2) {
-    const double cosp2 = cosp * cosp;
-    const double mu = cosp / a / sqrt(1. + cosp2 / a2);
-    const double u = sinp * sqrt(1 - mu * mu);
+template <class T>
+KIWI_HD T phi_I1(T sinp, T cosp, T a, T a2) {
+    const T cosp2 = cosp * cosp;
+    const T mu = cosp / a / sqrt(1. + cosp2 / a2);
+    const T u = sinp * sqrt(1 - mu * mu);
     return atan(u / a);
 }
 

@@ -32,23 +32,25 @@ constexpr int kLatSCap = 4096;   // corner values per chunk (one full 8^3 partic
 // Vertex-pyramid mass of the right triangle with legs R_0 (projection -> edge line) and t (along the
 // edge) in a wall at distance r0: the vertex tier of src/kernel_integral.cpp:356-400 at phi = atan2(t, R_0)
 // (beyond 2h only I0 and I1 are needed, as in cubic_vertex).
-static __device__ __noinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
-    if (r0 == 0.0 || R_0 == 0.0 || t == 0.0) return 0.0;
-    const CubicWall w = cubic_wall(h, r0);
-    const double a = R_0 / r0;
-    const double a2 = a * a;
-    const double s2 = R_0 * R_0 + t * t;
-    const double rr = sqrt(s2);
-    const double phi = atan2(t, R_0);
-    const double sinp = t / rr, cosp = R_0 / rr;
-    const double r2 = r0 * r0 + s2;
-    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+// Written over the real type T: double here, Dual4 (dual.cuh) for the adjoint.
+template <class T>
+static __device__ __noinline__ T lattice_vertex_t(T h, T r0, T R_0, T t, T D2, T D3) {
+    if (r0 == 0.0 || R_0 == 0.0 || t == 0.0) return T(0.0);
+    const CubicWallT<T> w = cubic_wall_t<T>(h, r0);
+    const T a = R_0 / r0;
+    const T a2 = a * a;
+    const T s2 = R_0 * R_0 + t * t;
+    const T rr = sqrt(s2);
+    const T phi = atan2(t, R_0);
+    const T sinp = t / rr, cosp = R_0 / rr;
+    const T r2 = r0 * r0 + s2;
+    const T r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
     if (!(r2 < 4.0 * w.h2)) {
-        const double I1 = phi_I1(sinp, cosp, a, a2);
+        const T I1 = phi_I1<T>(sinp, cosp, a, a2);
         return r0h3 / kPi * (-0.25 * r0h_3 * I1 + w.B3 / r03 * phi + D3);
     }
-    const PhiSeries s = phi_series_sc(phi, sinp, cosp, a, a2);
-    double full_int;
+    const PhiSeriesT<T> s = phi_series_sc<T>(phi, sinp, cosp, a, a2);
+    T full_int;
     if (r2 < w.h2) {
         full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
     } else if (r2 < 4.0 * w.h2) {
@@ -57,6 +59,9 @@ static __device__ __noinline__ double lattice_vertex(double h, double r0, double
         full_int = r0h3 / kPi * (-0.25 * r0h_3 * s.I1 + w.B3 / r03 * s.I0 + D3);
     }
     return full_int;
+}
+static __device__ __forceinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
+    return lattice_vertex_t<double>(h, r0, R_0, t, D2, D3);
 }
 
 // Position of the smallest j with s_off[j] <= it among the chunk's np particles (s_off ascending).
