@@ -67,7 +67,7 @@ def test_adjoint_matches_fd_of_gpu_forward(kiwi, ctx):
     rng = np.random.default_rng(7)
     cot = rng.standard_normal(4 * int(np.prod(shape)))
     ad, st = _adjoint(kiwi, ctx, P, bounds, shape, cot)
-    assert st["evaluated_pairs"] > 0 and st["launches"] == 1
+    assert st["evaluated_pairs"] > 0 and st["launches"] >= 1
 
     def loss(P1):
         r = kiwi.sph_to_grid(P1, bounds, shape, raw=True, ctx=ctx, precision="fp64")
