@@ -83,6 +83,8 @@ def parse():
                     help="with N > 1 GPUs: split one grid by cell tiles (strong scaling) or map one snapshot per "
                          "rank (weak scaling)")
     ap.add_argument("--fd-particles", type=int, default=40, help="adjoint workload: particles checked by FD")
+    ap.add_argument("--adj-n", type=int, default=500_000, help="adjoint workload: particles")
+    ap.add_argument("--adj-res", type=int, default=128, help="adjoint workload: grid cells per axis")
     ap.add_argument("--vor-n", type=int, default=200_000, help="voronoi workload: particles")
     ap.add_argument("--workload", default="lognormal", choices=["lognormal", "batch", "adjoint", "voronoi"],
                     help="batch: many column snapshots of log-uniform sizes on grids of log-uniform resolution, "
@@ -248,7 +250,7 @@ def run_adjoint(args):
 
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    n, res, box = 500_000, 128, (4.0, 4.0, 4.0)
+    n, res, box = args.adj_n, args.adj_res, (4.0, 4.0, 4.0)
     P, bounds = column_snapshot(n=n, seed=1004, box=box)
     Tp, _ = column_snapshot(n=n, seed=2004, box=box)
     shape = (res, res, res)
@@ -321,7 +323,7 @@ def run_adjoint(args):
         "value": adj_pairs / (ms_adj * 1e-3), "unit": "pair-integrals/s", "n_gpus": 1, "steps": args.steps,
         "warmup": 1, "ms_per_step": ms_adj, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (forward-mode derivatives)", "data": "synthetic",
-        "config": {"workload": "500000 column-recipe particles in a 4 pc cube (seed 1004), grid 128^3, "
+        "config": {"workload": f"{n} column-recipe particles in a 4 pc cube (seed 1004), grid {res}^3, "
                                "L = sum_xy (sum_z rho dz - T_xy)^2, T from the seed-2004 realisation"},
         "forward_ms": {k: v[0] for k, v in times.items()},
         "forward_pairs_per_s": {k: v[1] / (v[0] * 1e-3) for k, v in times.items()},
