@@ -83,25 +83,109 @@ static __device__ __forceinline__ int chunk_search(const int* s_off, int np, int
 constexpr int kLatGenERec = 7;
 constexpr int kLatGenECap = 640;  // edge records per chunk (a full 8^3 particle box needs 486)
 
+// G_k(phi) = bphi_k phi + sum_i coef_k,i I_i(phi) for a wall at q0 = r0 / H in region j of the kernel
+// (generic_G, src/kernel_integral_generic.cpp:82-92), a = R0 / r0, with sin(phi) and cos(phi) given.
+// The wall coefficients A3 a_k,i q0^i are formed on the fly and each basis integral I_i (the recurrences
+// of :19-66) is added as soon as it is formed, in ascending index order: every loop is unrolled over the
+// table's fixed width and predicated on the region's lowest index, so the basis values, the sec-power
+// integrals J_2l and the powers of q0 stay in registers.  q0^i is a compensated running product (hi + lo,
+// the product's rounding error carried exactly by fma): the terms can cancel heavily, and a plain running
+// product's rounding (up to ~i ulp) measurably raised the error of low-density cells; this is within an
+// ulp, like pow, at a fraction of its cost.
+static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K, double q0, int j, int k, double a,
+                                                        double a2, double phi, double sinp, double cosp) {
+    const double* ak = K->a[k - 1];
+    int imin = 1;
+    for (int idx = KIWI_NI - 1; idx >= 0; --idx)
+        if (ak[idx] != 0.0) {
+            imin = 1 - idx;
+            break;
+        }
+    const double A3 = K->A3_pi / kPi;
+    double b = 0.0;
+    if (k >= j)
+        for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
+    double sum = (A3 * b) * phi;
+    const double den = a2 + cosp * cosp;
+    const double u = a * sinp / sqrt(den);
+    const double one_minus_u2 = cosp * cosp * (1.0 + a2) / den;
+    const double tn = imin <= -2 ? sinp / cosp : 0.0, sc = imin <= -2 ? 1.0 / cosp : 0.0;
+    double ph = 1.0, pl = 0.0;  // q0^idx
+    double Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
+    double J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
+#pragma unroll
+    for (int idx = 0; idx < KIWI_NI; ++idx) {
+        if (1 - idx < imin) break;
+        double Iv;
+        if (idx == 0) {  // I_1 = atan(u / a)
+            Iv = atan(u / a);
+            Iodd = Iv;
+            Kc = atanh(u);
+        } else if (idx == 1) {  // I_0 = phi
+            Iv = phi;
+        } else if ((idx & 1) == 0) {  // I_-(2m+1), m = idx / 2 - 1
+            const int m = idx / 2 - 1;
+            if (m > 0) {
+                Kc = u / (2.0 * m * pow(one_minus_u2, (double)m)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
+                pow1a2 *= (1.0 + a2);
+            }
+            Iodd += a * pow1a2 * Kc;
+            Iv = Iodd;
+        } else {  // I_-2kk = sum_l C(kk, l) a^2l J_2l, kk = (idx - 1) / 2
+            const int kk = (idx - 1) / 2;
+            if (kk == 1) {
+                J[0] = phi;
+                J[1] = tn;
+            } else {
+                spow *= sc * sc;
+                J[kk] = spow * tn / (2 * kk - 1.0) + (2 * kk - 2.0) / (2 * kk - 1.0) * J[kk - 1];
+            }
+            double s = J[0], apow = 1.0, bc = 1.0;
+#pragma unroll
+            for (int l = 1; l <= kk; ++l) {
+                bc = bc * (kk - l + 1) / l;
+                apow *= a2;
+                s += bc * apow * J[l];
+            }
+            Iv = s;
+        }
+        const double c = ak[idx];
+        if (c != 0.0) sum += (A3 * c * (ph + pl)) * Iv;
+        const double nh = ph * q0;
+        pl = fma(pl, q0, fma(ph, q0, -nh));
+        ph = nh;
+    }
+    return sum;
+}
+
 static __device__ __forceinline__ void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0, double R0,
                                                            double* rec) {
     for (int i = 0; i < kLatGenERec; ++i) rec[i] = 0.0;
     if (r0 == 0.0 || R0 == 0.0) return;
-    GenericWall w;
-    GenericEdge e;
-    generic_wall(w, K, H, r0);
-    generic_edge(e, w, R0);
-    rec[0] = (double)(e.nseg + 8 * e.region[0]);
-    for (int s = 0; s + 1 < e.nseg && s < 3; ++s) rec[1 + s] = e.phi_end[s];
-    for (int s = 1; s < e.nseg && s < 4; ++s) rec[3 + s] = e.offset[s];
+    // the regions crossed along the edge line and the angles where it leaves them (generic_edge, :119-148)
+    const double q0 = r0 / H, qR = R0 / H;
+    const double a = R0 / r0, a2 = a * a;
+    const int j = generic_region(K, q0);
+    const int k0 = generic_region(K, sqrt(q0 * q0 + qR * qR));
+    const int nseg = K->nreg - k0 + 1;
+    rec[0] = (double)(nseg + 8 * k0);
+    double off = 0.0;
+    for (int s = 0; s + 1 < nseg; ++s) {
+        const int k = k0 + s;
+        const double c = K->c[k - 1];
+        const double pb = acos(fmin(1.0, qR / sqrt(c * c - q0 * q0)));
+        if (s < 3) rec[1 + s] = pb;
+        const double sp = sin(pb), cp = cos(pb);
+        off = off + lattice_generic_G(K, q0, j, k, a, a2, pb, sp, cp) - lattice_generic_G(K, q0, j, k + 1, a, a2, pb, sp, cp);
+        if (s < 3) rec[4 + s] = off;
+    }
 }
 
 // Vertex tier of a generic kernel for the right triangle with legs R0 (projection -> edge line) and t
 // (along the edge) in a wall at distance r0 (generic_vertex, :150-156, at phi = atan2(t, R0)): the region
-// segment holding phi, its offset, and G_k(phi) = bphi_k phi + sum_i coef_k,i I_i(phi) with the wall
-// coefficients A3 a_k,i (r0/H)^i formed on the fly.
-static __device__ __noinline__ double lattice_generic_vertex(const KiwiKernelTable* K, double H, double r0, double R0,
-                                                            double t, const double* rec) {
+// segment holding phi, its offset, and G_k(phi).
+static __device__ __forceinline__ double lattice_generic_vertex(const KiwiKernelTable* K, double H, double r0,
+                                                               double R0, double t, const double* rec) {
     const int packed = (int)rec[0];
     const int nseg = packed & 7, k0 = packed >> 3;
     if (nseg == 0 || t == 0.0) return 0.0;
@@ -111,35 +195,9 @@ static __device__ __noinline__ double lattice_generic_vertex(const KiwiKernelTab
     const double sinp = t / rr, cosp = R0 / rr;
     int s = 0;
     while (s + 1 < nseg && phi > rec[1 + s]) ++s;
-    const int k = k0 + s;
     const double q0 = r0 / H;
-    const int j = generic_region(K, q0);
-    int imin = 1;
-    for (int idx = KIWI_NI - 1; idx >= 0; --idx)
-        if (K->a[k - 1][idx] != 0.0) {
-            imin = 1 - idx;
-            break;
-        }
-    double I[KIWI_NI];
-    generic_basis_sc(a, a2, phi, sinp, cosp, imin, I);
-    const double A3 = K->A3_pi / kPi;
-    double b = 0.0;
-    if (k >= j)
-        for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
-    double sum = (A3 * b) * phi;
-    // q0^idx as a compensated running product (hi + lo, the product's rounding error carried exactly by
-    // fma): the terms can cancel heavily, and a plain running product's rounding (up to ~idx ulp)
-    // measurably raised the error of low-density cells; this is within an ulp, like pow, at a fraction
-    // of its cost
-    double ph = 1.0, pl = 0.0;
-    for (int idx = 0; idx < KIWI_NI; ++idx) {
-        const double c = K->a[k - 1][idx];
-        if (c != 0.0) sum += (A3 * c * (ph + pl)) * I[idx];
-        const double nh = ph * q0;
-        pl = fma(pl, q0, fma(ph, q0, -nh));
-        ph = nh;
-    }
-    return (s > 0 ? rec[3 + s] : 0.0) + sum;
+    const double G = lattice_generic_G(K, q0, generic_region(K, q0), k0 + s, a, a2, phi, sinp, cosp);
+    return (s > 0 ? rec[3 + s] : 0.0) + G;
 }
 
 // Offset of lattice plane P (global plane index) from the particle coordinate x0 along one axis.
