@@ -58,6 +58,8 @@ CELL_ASSEMBLY = 60.0
 LATTICE_DRAM_BYTES_FULL = 274.63e6 + 598.75e6
 
 L2_BYTES = 126 * 1024 * 1024
+# the tabulated integral: one trilinear lookup reads 8 table entries
+TAB_BYTES_PER_LOOKUP = 64.0
 
 
 def parse():
@@ -73,6 +75,9 @@ def parse():
     ap.add_argument("--n", type=int, default=2_000_000)
     ap.add_argument("--res", type=int, default=256)
     ap.add_argument("--kernel", default="cubic_spline")
+    ap.add_argument("--tabulated", action="store_true",
+                    help="the cubic spline's tabulated integral (lookups in the GPU-generated canonical table) "
+                         "instead of its closed form; every cell of each support bounding box, as the reference")
     ap.add_argument("--seed", type=int, default=1002)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU-baseline sample")
@@ -501,7 +506,7 @@ def main():
 
     split = ws > 1 and args.multi == "tiles"
     P, bounds, shape = make_workload(args.n, args.res, args.seed + (0 if split else 1000 * rank), args.kernel)
-    ki = kiwi_b200.make_kernel_integrator(args.kernel)
+    ki = kiwi_b200.make_kernel_integrator(args.kernel, use_tabulated_integral=args.tabulated)
     part, n_parts = (rank, ws) if split else (0, 1)
     ctx = kiwi_b200.Context(dev.index)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -584,7 +589,7 @@ def main():
     # against this run's FP64 output: the FP32-mixed vs FP64 comparison of the metric
     fp32_side = None
     if (args.precision == "fp64" and not args.no_fp32_compare and args.kernel == "cubic_spline" and not args.full_box
-            and not split):
+            and not split and not args.tabulated):
         o32 = {k: torch.empty(nc, dtype=torch.float64, device=dev) for k in ("density", "vx", "vy", "vz")}
         for _ in range(min(args.warmup, 2)):
             kiwi_b200.sph_to_grid_device(dP, bounds, shape, o32, kernel=ki, precision="fp32_mixed", ctx=ctx)
@@ -657,7 +662,7 @@ def main():
                "ms_per_step": e_ms / args.e2e_steps}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.tabulated:
         cpu = cpu_baseline(P, bounds, shape, args.kernel, args.cpu_seconds)
 
     if rank == 0:
@@ -667,7 +672,9 @@ def main():
         if items.get("vertex_pyramids", 0) > 0:
             # lattice-factorised kernel: its own work items x their measured costs
             kname = ("k_cart_lattice_f32 (FP32 lattice tiers, FP64 assembly)" if is32 else
-                     "k_cart_lattice (FP64 lattice-factorised cell-integral gather)")
+                     "k_cart_lattice (FP64 lattice-factorised cell-integral gather)" if args.kernel == "cubic_spline"
+                     else "k_cart_lattice_generic (FP64 lattice form, table-driven tiers; work items costed at the "
+                          "cubic tiers' rates)")
             work = (items["edge_tiers_outer"] * EDGE_OUTER + items["edge_tiers_middle"] * EDGE_MIDDLE +
                     items["edge_tiers_inner"] * EDGE_INNER + items["vertex_pyramids"] * VERTEX_PYRAMID +
                     evaluated * CELL_ASSEMBLY) / args.steps
@@ -690,6 +697,17 @@ def main():
                 hbm_peak = float(json.load(f)["hbm_gbs"])
         except (OSError, ValueError, KeyError):
             pass
+        tab_roofline = None
+        if args.tabulated:
+            # each vertex pyramid is one trilinear lookup: 8 table entries (64 bytes) from a 182 MB table
+            lookups = items.get("vertex_pyramids", 0) / args.steps
+            ach = lookups * TAB_BYTES_PER_LOOKUP / (g_ms * 1e-3) / 1e9
+            tab_roofline = {"bound": "hbm", "kernel": "k_cart_lattice_tab (FP64 lattice form, tabulated integral)",
+                            "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                            "frac": ach / hbm_peak if hbm_peak else None, "traffic": None,
+                            "algorithmic_bytes": "64 bytes (8 table entries) per lookup x lookups per launch",
+                            "lookups_per_launch": lookups, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                            "gather_ms_per_launch": g_ms}
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -697,7 +715,8 @@ def main():
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"workload": f"lognormal_cube n={args.n} sigma_ln=1.5 P(k)~k^-4 10pc padded, "
-                                   f"grid {args.res}^3, kernel {args.kernel}",
+                                   f"grid {args.res}^3, kernel {args.kernel}" +
+                                   (", tabulated integral" if args.tabulated else ""),
                        "precision": args.precision, "particles_per_gpu": args.n, "cells": nc,
                        "l2": "flushed between timed steps (256 MB write) and inputs+outputs > L2",
                        "parallelism": (f"cell-tile parts x{ws} of one grid" if split else f"replicas x{ws}")
@@ -720,6 +739,8 @@ def main():
             "clocks": clk, "gpu_launches": int(launches), "wall_s_timed_region": wall,
             "e2e": e2e, "cpu_baseline": cpu,
         }
+        if tab_roofline is not None:
+            line["roofline"] = tab_roofline
         if accuracy is not None:
             line["accuracy"] = accuracy
         if fp32_side is not None:

@@ -83,7 +83,8 @@ typedef struct KiwiKernelSel {
     int32_t kernel;       /* kiwi_kernel_index(): 0 M4, 1 M5, 2 M6, 3 WC2, 4 WC4, 5 WC6 */
     double support_in_h;  /* kernel support radius in units of h; 0 = the kernel's default radkern */
     int32_t generic_path; /* force the generic integral for M4 */
-    int32_t tabulated;    /* cubic path only: trilinear lookup table instead of the closed form */
+    int32_t tabulated;    /* cubic path only: trilinear lookup in the context's density table instead of the
+                           * closed form (the canonical table is generated on first use if none is loaded) */
 } KiwiKernelSel;
 
 typedef struct KiwiStats {
@@ -102,6 +103,8 @@ typedef struct KiwiStats {
      * distance of the edge line (beyond 2h, between h and 2h, within h) and vertex pyramids */
     int64_t edge_tiers_outer, edge_tiers_middle, edge_tiers_inner, vertex_pyramids;
     int64_t fp64_tiles;      /* KIWI_FP32_GUARANTEE: cell tiles recomputed in FP64 */
+    int64_t table_clamps;    /* tabulated integral: lookup indices clamped into the table (the reference
+                              * prints a warning for each, src/kernel_integral.cpp:125-133) */
 } KiwiStats;
 
 /* ---- context --------------------------------------------------------------------------------- */
@@ -137,6 +140,31 @@ int kiwi_full_integral_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* 
  * (may be NULL) receives the reference's out_vert per item. */
 int kiwi_face_integral_batch(KiwiCtx* ctx, const KiwiKernelSel* kernel, int64_t n_faces, const double* particle,
                              const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert);
+
+/* ---- tabulated cubic integral (DensityLookupTable, include/kiwi/kernel_integral.hpp:21-72) ------ */
+/* The shape of a density lookup table: three axes (r0/h, mu0, cos phi), each two uniform sub-grids split
+ * at rl, mul, cphil (the header of the reference's table file). */
+typedef struct KiwiDensityTableInfo {
+    int32_t nr01, nR_01, nphi1, nr02, nR_02, nphi2;
+    double rl, mul, cphil;
+    int64_t n_values; /* (nr01 + nr02 + 2) (nR_01 + nR_02 + 1) (nphi1 + nphi2 + 1) */
+} KiwiDensityTableInfo;
+/* generate_density_table (src/kernel_integral.cpp:57-119): the canonical 251 x 301 x 301 table, computed on
+ * the GPU into the context (replacing any table it holds). */
+int kiwi_density_table_generate(KiwiCtx* ctx);
+/* load_density_table (src/kernel_integral.cpp:20-55): the reference's text format, into the context.
+ * Errors (KIWI_ERR_ARG) carry the reference's messages; shapes the reference would divide by zero on or
+ * that exceed 2^31 values are rejected too. */
+int kiwi_density_table_load(KiwiCtx* ctx, const char* path);
+/* Shape of the context's table (KIWI_ERR_ARG if it holds none). */
+int kiwi_density_table_info(KiwiCtx* ctx, KiwiDensityTableInfo* info);
+/* Copy the table's n_values values to host memory, laid out as the reference's DensityLookupTable::at. */
+int kiwi_density_table_read(KiwiCtx* ctx, double* values, int64_t n);
+void kiwi_density_table_release(KiwiCtx* ctx);
+/* gridded_integral(table, h, phi, r0, R_0) (src/kernel_integral.cpp:136-190) for n items (host arrays);
+ * clamps (may be NULL) receives the number of lookup indices clamped into the table. */
+int kiwi_gridded_integral_batch(KiwiCtx* ctx, int64_t n, const double* h, const double* phi, const double* r0,
+                                const double* R_0, double* out, int64_t* clamps);
 
 /* ---- sph-to-grid stage (run_sph_to_grid_stage, src/cartesian_grid.cpp:76-321) ---------------- */
 /* Host arrays in, host arrays out (density, vx, vy, vz as CartesianGridResult holds them,

@@ -70,10 +70,16 @@ class KiwiStats(C.Structure):
                 ("skipped_outside", C.c_int64), ("neg_clamped", C.c_int64), ("neg_warned", C.c_int64),
                 ("fp64_fallback", C.c_int64), ("tile_pairs", C.c_int64), ("launches", C.c_int64), ("gather_ms", C.c_double),
                 ("total_ms", C.c_double), ("edge_tiers_outer", C.c_int64), ("edge_tiers_middle", C.c_int64),
-                ("edge_tiers_inner", C.c_int64), ("vertex_pyramids", C.c_int64), ("fp64_tiles", C.c_int64)]
+                ("edge_tiers_inner", C.c_int64), ("vertex_pyramids", C.c_int64), ("fp64_tiles", C.c_int64),
+                ("table_clamps", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KiwiDensityTableInfo(C.Structure):
+    _fields_ = [(k, C.c_int32) for k in ("nr01", "nR_01", "nphi1", "nr02", "nR_02", "nphi2")] + \
+               [(k, C.c_double) for k in ("rl", "mul", "cphil")] + [("n_values", C.c_int64)]
 
 
 class KiwiBatchItem(C.Structure):
@@ -124,6 +130,13 @@ def load_library(path: str = LIB_PATH):
     L.kiwi_batch_destroy.argtypes = [C.c_void_p]
     L.kiwi_map_voronoi.argtypes = [C.c_void_p, C.POINTER(KiwiParticles), _i32p, C.POINTER(KiwiVoronoiCells),
                                    C.POINTER(KiwiKernelSel), C.c_int, _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
+    L.kiwi_density_table_generate.argtypes = [C.c_void_p]
+    L.kiwi_density_table_load.argtypes = [C.c_void_p, C.c_char_p]
+    L.kiwi_density_table_info.argtypes = [C.c_void_p, C.POINTER(KiwiDensityTableInfo)]
+    L.kiwi_density_table_read.argtypes = [C.c_void_p, _dp, C.c_int64]
+    L.kiwi_density_table_release.argtypes = [C.c_void_p]
+    L.kiwi_density_table_release.restype = None
+    L.kiwi_gridded_integral_batch.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -242,9 +255,10 @@ def _sel(kernel=0, support_in_h=0.0, generic_path=False, tabulated=False) -> Kiw
     return KiwiKernelSel(k, float(support_in_h), int(bool(generic_path)), int(bool(tabulated)))
 
 
-def face_integrals(particles, faces, kernel=0, support_in_h=0.0, generic_path=False, ctx=None):
+def face_integrals(particles, faces, kernel=0, support_in_h=0.0, generic_path=False, ctx=None, tabulated=False):
     """Batched face integrals: particles (n, 4) = (x0, y0, z0, h); faces: list of (nv, 3) vertex arrays in
-    the face's winding.  Returns (values, out_vert)."""
+    the face's winding.  Returns (values, out_vert).  tabulated: the cubic spline's lookup table (the
+    context's density table) instead of its closed form."""
     ctx = ctx or default_context()
     part = _f64(particles).reshape(-1, 4)
     n = part.shape[0]
@@ -256,15 +270,16 @@ def face_integrals(particles, faces, kernel=0, support_in_h=0.0, generic_path=Fa
     verts = _f64(np.concatenate([_f64(f).reshape(-1) for f in faces]) if n else np.zeros(0))
     out = np.empty(n)
     ov = np.empty(n, dtype=np.int32)
-    sel = _sel(kernel, support_in_h, generic_path)
+    sel = _sel(kernel, support_in_h, generic_path, tabulated)
     ctx.check(ctx._L.kiwi_face_integral_batch(ctx.handle, C.byref(sel), n, _p(part), off.ctypes.data_as(_i64p),
                                               _p(verts), _p(out), ov.ctypes.data_as(_i32p)), "face_integral")
     return out, ov
 
 
-def compute_face_integral(x0, y0, z0, h, vertices, out_vert=False, ctx=None):
-    """compute_face_integral(x0, y0, z0, h, false, nullptr, vertices, &out_vert): cubic spline, support 2h."""
-    v, ov = face_integrals([[x0, y0, z0, h]], [vertices], kernel=0, support_in_h=2.0, ctx=ctx)
+def compute_face_integral(x0, y0, z0, h, vertices, out_vert=False, ctx=None, tabulated=False):
+    """compute_face_integral(x0, y0, z0, h, tabulated, table, vertices, &out_vert): cubic spline, support 2h;
+    with tabulated, the lookups go to the context's density table."""
+    v, ov = face_integrals([[x0, y0, z0, h]], [vertices], kernel=0, support_in_h=2.0, ctx=ctx, tabulated=tabulated)
     return (float(v[0]), int(ov[0])) if out_vert else float(v[0])
 
 
@@ -274,6 +289,63 @@ def compute_face_integral_generic(x0, y0, z0, K, H, vertices, out_vert=False, ct
     # H is passed as h = H / support_in_h with support_in_h = 1 on the generic path
     v, ov = face_integrals([[x0, y0, z0, H]], [vertices], kernel=k.index, support_in_h=1.0, generic_path=True, ctx=ctx)
     return (float(v[0]), int(ov[0])) if out_vert else float(v[0])
+
+
+# ---- tabulated cubic integral (DensityLookupTable, include/kiwi/kernel_integral.hpp:21-72)
+
+def generate_density_table(ctx=None):
+    """generate_density_table (src/kernel_integral.cpp:57-119): the canonical table, computed on the GPU into
+    the context.  Returns its shape (density_table_info)."""
+    ctx = ctx or default_context()
+    ctx.check(ctx._L.kiwi_density_table_generate(ctx.handle), "generate_density_table")
+    return density_table_info(ctx)
+
+
+def load_density_table(path, ctx=None):
+    """load_density_table (src/kernel_integral.cpp:20-55): the reference's text format, into the context
+    (KiwiError with the reference's messages on a missing, malformed or truncated file)."""
+    ctx = ctx or default_context()
+    ctx.check(ctx._L.kiwi_density_table_load(ctx.handle, os.fsencode(path)), "load_density_table")
+    return density_table_info(ctx)
+
+
+def density_table_info(ctx=None) -> dict:
+    ctx = ctx or default_context()
+    info = KiwiDensityTableInfo()
+    ctx.check(ctx._L.kiwi_density_table_info(ctx.handle, C.byref(info)), "density_table_info")
+    return {k: getattr(info, k) for k, _ in info._fields_}
+
+
+def density_table_values(ctx=None) -> np.ndarray:
+    """The context's table values, shape (nr0 + 2, nR_0 + 1, nphi + 1), indexed as DensityLookupTable::at."""
+    ctx = ctx or default_context()
+    d = density_table_info(ctx)
+    out = np.empty(d["n_values"])
+    ctx.check(ctx._L.kiwi_density_table_read(ctx.handle, _p(out), out.size), "density_table_read")
+    return out.reshape(d["nr01"] + d["nr02"] + 2, d["nR_01"] + d["nR_02"] + 1, d["nphi1"] + d["nphi2"] + 1)
+
+
+def release_density_table(ctx=None):
+    ctx = ctx or default_context()
+    ctx._L.kiwi_density_table_release(ctx.handle)
+
+
+def gridded_integral(h, phi, r0, R_0, ctx=None, return_clamps=False):
+    """gridded_integral(table, h, phi, r0, R_0) (src/kernel_integral.cpp:136-190), batched over broadcast
+    arrays, with the context's density table (the canonical one is generated if none is loaded).  With
+    return_clamps, also the number of lookup indices clamped into the table (the reference prints a
+    warning for each)."""
+    ctx = ctx or default_context()
+    a = np.broadcast_arrays(*[np.asarray(v, dtype=np.float64) for v in (h, phi, r0, R_0)])
+    shape = a[0].shape
+    a = [_f64(v.reshape(-1)) for v in a]
+    n = a[0].size
+    out = np.empty(n)
+    cl = C.c_int64(0)
+    ctx.check(ctx._L.kiwi_gridded_integral_batch(ctx.handle, n, *[_p(v) for v in a], _p(out), C.byref(cl)),
+              "gridded_integral")
+    res = out.reshape(shape) if shape else float(out[0])
+    return (res, cl.value) if return_clamps else res
 
 
 @dataclass

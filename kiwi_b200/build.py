@@ -32,6 +32,7 @@ UNITS = [
     ("mixed.cu", []),
     ("batch.cu", ["--fmad=false"]),
     ("io.cu", []),
+    ("tabulated.cu", ["--fmad=false"]),
 ]
 
 

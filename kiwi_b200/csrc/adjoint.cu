@@ -338,9 +338,10 @@ __global__ void k_adjoint_reduce(int64_t n, const int64_t* __restrict__ offs, co
 
 int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc,
                      const double* d_cot, const AdjointOutputs& out, KiwiStats* stats) {
-    if (!kc.cubic)
+    if (!kc.cubic || kc.tabulated)
         return set_err(ctx, KIWI_ERR_UNSUPPORTED,
-                       "the adjoint is available for the cubic spline kernel with support 2h (generic_path unset)");
+                       "the adjoint is available for the analytic cubic spline integral with support 2h (generic_path "
+                       "and tabulated unset)");
     DevStats* d_st = nullptr;
     KIWI_TRY(scratch_t(ctx, S_STATS, 1, &d_st));
     KIWI_CUDA(ctx, cudaMemsetAsync(d_st, 0, sizeof(DevStats), ctx->stream));

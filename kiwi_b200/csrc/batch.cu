@@ -142,6 +142,7 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
         if (!particles_ok(ctx, &it.particles, &rc)) return rc;
         KernelChoice kc;
         KIWI_TRY(resolve_kernel(ctx, &it.kernel, &kc));
+        if (kc.tabulated) return set_err(ctx, KIWI_ERR_UNSUPPORTED, "batch: the tabulated integral is not available");
         BatchItemDev& d = b->items[i];
         KIWI_TRY(make_geom(ctx, &it.grid, kc.support_in_h, &d.g));
         d.P = DevParticles{it.particles.n, it.particles.x, it.particles.y, it.particles.z, it.particles.vx,

@@ -36,7 +36,6 @@ int resolve_kernel(KiwiCtx* ctx, const KiwiKernelSel* sel, KernelChoice* out) {
         return set_err(ctx, KIWI_ERR_ARG,
                        "use_tabulated_integral is only available for the cubic spline kernel with its default support "
                        "radius (and kernel.generic_path unset)");
-    if (tab) return set_err(ctx, KIWI_ERR_UNSUPPORTED, "the tabulated integral is not available in this build");
     out->cubic = !generic;
     out->tabulated = tab;
     out->kernel = k;
@@ -81,12 +80,21 @@ int check_ctx(KiwiCtx* ctx) {
 }
 
 // The full device pipeline of one sph-to-grid call: mean velocity, binning, gather.
-int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc, int precision,
+int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc_in, int precision,
                     const CartOutputs& out_in, KiwiStats* stats, int part, int n_parts) {
     if (n_parts < 1 || n_parts > 65536 || part < 0 || part >= n_parts)
         return set_err(ctx, KIWI_ERR_ARG, "part %d of %d parts is out of range (1 <= parts <= 65536)", part, n_parts);
     if (n_parts > 1 && (precision & KIWI_FP32_GUARANTEE))
         return set_err(ctx, KIWI_ERR_ARG, "KIWI_FP32_GUARANTEE needs the whole grid (n_parts = 1)");
+    KernelChoice kc = kc_in;
+    if (kc.tabulated) {
+        if (ctx->arena)
+            return set_err(ctx, KIWI_ERR_UNSUPPORTED,
+                           "the tabulated integral needs a context holding its table (not the allocation-free call)");
+        if ((precision & KIWI_FORM_MASK) == KIWI_FP32_MIXED)
+            return set_err(ctx, KIWI_ERR_UNSUPPORTED, "the FP32-mixed form is available for the analytic integral only");
+        KIWI_TRY(table_ensure(ctx, &kc.tab));
+    }
     const int64_t launches0 = ctx->launches;
     DevStats* d_stats = nullptr;
     double* d_meanv = nullptr;
@@ -228,6 +236,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         stats->edge_tiers_inner = (int64_t)hs.edge_inner;
         stats->vertex_pyramids = (int64_t)hs.vertex_pyramids;
         stats->fp64_tiles = fp64_tiles;
+        stats->table_clamps = (int64_t)hs.table_clamps;
     }
     return KIWI_OK;
 }
@@ -285,6 +294,7 @@ void kiwi_ctx_destroy(KiwiCtx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    table_free(ctx);
     for (int i = 0; i < KiwiCtx::kSlots; ++i)
         if (ctx->slot_ptr[i]) cudaFree(ctx->slot_ptr[i]);
     for (auto& ev : ctx->ev)
@@ -372,6 +382,7 @@ int kiwi_face_integral_batch(KiwiCtx* ctx, const KiwiKernelSel* kernel, int64_t 
     if (n_faces < 0 || (n_faces > 0 && (!particle || !vert_off || !verts || !out)))
         return set_err(ctx, KIWI_ERR_ARG, "bad arrays");
     if (n_faces == 0) return KIWI_OK;
+    if (kc.tabulated) KIWI_TRY(table_ensure(ctx, &kc.tab));
     const int64_t nv = vert_off[n_faces];
     if (nv < 0 || vert_off[0] != 0) return set_err(ctx, KIWI_ERR_ARG, "vert_off must start at 0 and be non-decreasing");
     for (int64_t i = 0; i < n_faces; ++i)
@@ -530,6 +541,7 @@ int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t
     KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
     if ((precision & KIWI_FORM_MASK) != KIWI_FP64 && (precision & KIWI_FORM_MASK) != KIWI_FP64_REFERENCE_ORDER)
         return set_err(ctx, KIWI_ERR_UNSUPPORTED, "the Voronoi map is available in the FP64 form only");
+    if (kc.tabulated) KIWI_TRY(table_ensure(ctx, &kc.tab));
     if (!cells || cells->n_cells < 0 || (cells->n_cells > 0 && (!cells->face_off || !cells->vert_off ||
                                                                  !cells->vxyz || !cells->face_nbr || !cells->volume)))
         return set_err(ctx, KIWI_ERR_ARG, "cell geometry is incomplete");

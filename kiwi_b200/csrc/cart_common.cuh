@@ -88,6 +88,7 @@ struct DevStats {
     // work items of the lattice-factorised evaluation: edge tiers whose edge line lies outside 2h,
     // between h and 2h, within h of the particle; vertex pyramids evaluated
     unsigned long long edge_outer, edge_middle, edge_inner, vertex_pyramids;
+    unsigned long long table_clamps;  // tabulated integral: lookup indices clamped into the table
 };
 
 }  // namespace kiwi_b200

@@ -9,6 +9,16 @@
 
 #include "../../include/kiwi_b200.h"
 
+namespace kiwi_b200 {
+// A density lookup table in device memory (DensityLookupTable, include/kiwi/kernel_integral.hpp:21-72):
+// the sub-grid sizes and split points of its three axes and the values, laid out as the reference does.
+struct TabDev {
+    const double* v = nullptr;
+    int nr01 = 0, nR_01 = 0, nphi1 = 0, nr02 = 0, nR_02 = 0, nphi2 = 0, nr0 = 0, nR_0 = 0, nphi = 0;
+    double rl = 0.0, mul = 0.0, cphil = 0.0;
+};
+}  // namespace kiwi_b200
+
 struct KiwiCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
@@ -23,6 +33,10 @@ struct KiwiCtx {
     // slots are carved from it instead of allocated, and a request that does not fit is an error.
     unsigned char* arena = nullptr;
     size_t arena_bytes = 0, arena_used = 0;
+    // The density lookup table of the tabulated integral (generated or loaded on demand; tab.v owns
+    // tab_bytes of device memory).
+    kiwi_b200::TabDev tab;
+    size_t tab_bytes = 0;
 };
 
 namespace kiwi_b200 {

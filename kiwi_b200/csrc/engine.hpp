@@ -22,7 +22,12 @@ struct KernelChoice {
     bool tabulated;
     int kernel;
     double support_in_h;
+    TabDev tab;  // the context's density table when tabulated (set by table_ensure)
 };
+
+// tabulated.cu: the context's density table, generating the canonical one if it holds none.
+int table_ensure(KiwiCtx* ctx, TabDev* out);
+void table_free(KiwiCtx* ctx);
 
 // Tile lists built by the binning step: tile t owns list[range[2t] .. range[2t+1]) (particle indices in
 // ascending order).

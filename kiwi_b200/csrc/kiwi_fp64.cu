@@ -6,6 +6,7 @@
 #include "engine.hpp"
 #include "kiwi_math.cuh"
 #include "lattice.cuh"
+#include "tabulated.cuh"
 
 namespace kiwi_b200 {
 
@@ -75,14 +76,17 @@ __device__ __forceinline__ void decode_pair(int k, int np, const int* s_start, c
 }
 
 // The work of one CTA on one cell tile: t is the tile's index in its grid (its cell coordinates), t_range
-// its entry in range[] (the same unless the tile lists of several grids are concatenated).  With
-// RUNTIME_CUBIC the closed form is chosen by cubic_rt instead of CUBIC (one instance serves both, so a
-// kernel that needs both keeps one copy of the tile's shared memory).
-template <bool CUBIC, bool CULL, bool RUNTIME_CUBIC = false>
+// its entry in range[] (the same unless the tile lists of several grids are concatenated).  EV selects the
+// pair integral: kEvGeneric, kEvCubic (closed form) or kEvTab (lookups in `tab`).  With RUNTIME_CUBIC the
+// closed form is chosen by cubic_rt instead of EV (one instance serves both, so a kernel that needs both
+// keeps one copy of the tile's shared memory).
+constexpr int kEvGeneric = 0, kEvCubic = 1, kEvTab = 2;
+template <int EV, bool CULL, bool RUNTIME_CUBIC = false>
 __device__ __forceinline__ void gather_tile(const CartGeom& g, const DevParticles& P, int kernel,
                                             const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
                                             int64_t t_range, int64_t t, const CartOutputs& out,
-                                            DevStats* __restrict__ st, bool cubic_rt = false) {
+                                            DevStats* __restrict__ st, bool cubic_rt = false,
+                                            const TabDev tab = TabDev{}) {
     static_assert(kChunkCap / kThreads <= 32, "per-thread keep mask is 32 bits");
     __shared__ double s_x[kPMax], s_y[kPMax], s_z[kPMax], s_h[kPMax], s_m[kPMax], s_vx[kPMax], s_vy[kPMax],
         s_vz[kPMax];
@@ -101,6 +105,7 @@ __device__ __forceinline__ void gather_tile(const CartGeom& g, const DevParticle
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
 
     unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
+    unsigned n_clamp = 0;
     const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
     const double sup_in_h = g.support_in_h;
 
@@ -196,7 +201,10 @@ __device__ __forceinline__ void gather_tile(const CartGeom& g, const DevParticle
             const double cz = cell_centre(g.z_min, iz, g.dpz);
             ++n_eval;
             double msum;
-            if (RUNTIME_CUBIC ? cubic_rt : CUBIC)
+            if (EV == kEvTab) {
+                TabEval ev{tab, h, 0.0, 0.0, &n_clamp};
+                msum = box_cell_msum(x0, y0, z0, 2 * h, cx, cy, cz, g.hpx, g.hpy, g.hpz, ev);
+            } else if (RUNTIME_CUBIC ? cubic_rt : EV == kEvCubic)
                 msum = pair_msum<true>(kernel, x0, y0, z0, h, 2 * h, cx, cy, cz, g.hpx, g.hpy, g.hpz);
             else
                 msum = pair_msum<false>(kernel, x0, y0, z0, h, radius, cx, cy, cz, g.hpx, g.hpy, g.hpz);
@@ -256,6 +264,7 @@ __device__ __forceinline__ void gather_tile(const CartGeom& g, const DevParticle
     add_stat(&st->evaluated_pairs, n_eval);
     add_stat(&st->neg_clamped, n_neg);
     add_stat(&st->neg_warned, n_warn);
+    if (EV == kEvTab) add_stat(&st->table_clamps, n_clamp);
 }
 
 template <bool CUBIC, bool CULL>
@@ -265,7 +274,18 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather(CartGeom g
                                                           const int32_t* __restrict__ tile_map, CartOutputs out,
                                                           DevStats* __restrict__ st) {
     const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
-    gather_tile<CUBIC, CULL>(g, P, kernel, list, range, t, t, out, st);
+    gather_tile<CUBIC ? kEvCubic : kEvGeneric, CULL>(g, P, kernel, list, range, t, t, out, st);
+}
+
+// The per-cell gather with the tabulated integral, every cell of the particles' bounding boxes (outside the
+// support the lookups do not cancel exactly, and the reference keeps what they leave).
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGeom g, DevParticles P, const TabDev tab,
+                                                                         const uint32_t* __restrict__ list,
+                                                                         const int64_t* __restrict__ range,
+                                                                         const int32_t* __restrict__ tile_map,
+                                                                         CartOutputs out, DevStats* __restrict__ st) {
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    gather_tile<kEvTab, false>(g, P, 0, list, range, t, t, out, st, false, tab);
 }
 
 // ------------------------------------------------------------------ lattice-factorised gather (cubic)
@@ -277,6 +297,7 @@ constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;  // resident CTAs per SM 
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatSCap);
 constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;
+constexpr size_t kLatTabDynSmem = sizeof(double) * kLatSCap;
 
 
 // One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
@@ -286,12 +307,13 @@ constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : k
 // to its accumulators -- the same fixed per-cell summation order as k_cart_gather, no atomics.
 // GENERIC: the table-driven tiers of kernel `kernel` (support radius support_in_h x h) instead of the
 // cubic closed form; the edge tiers are then lattice_generic_edge records and the corner items run in
-// their natural order.
-template <bool CULL, bool GENERIC = false>
+// their natural order.  TAB: the tabulated cubic integral (lookups in `tab`): no edge tiers, and a corner
+// value is two lookups.
+template <bool CULL, bool GENERIC = false, bool TAB = false>
 __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
                                              const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
                                              int64_t t_range, int64_t t, const CartOutputs& out,
-                                             DevStats* __restrict__ st, int kernel = 0) {
+                                             DevStats* __restrict__ st, int kernel = 0, const TabDev tab = TabDev{}) {
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
         s_vy[kLatPMax], s_vz[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
@@ -301,7 +323,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     extern __shared__ double s_dyn[];
     double* s_D2 = s_dyn;
     double* s_D3 = s_dyn + kLatECap;
-    double* s_S = s_dyn + (GENERIC ? kLatGenERec * kLatGenECap : 2 * kLatECap);
+    double* s_S = s_dyn + (GENERIC ? kLatGenERec * kLatGenECap : (TAB ? 0 : 2 * kLatECap));
     double* s_E = s_dyn;  // generic edge records
     constexpr int kECap = GENERIC ? kLatGenECap : kLatECap;
     const KiwiKernelTable* K = &c_tables[kernel];
@@ -315,6 +337,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
     unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
     unsigned long long n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0;
+    unsigned n_clamp = 0;
     const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
 
     for (int64_t pos = beg; pos < end;) {
@@ -334,7 +357,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 d1 = min(b.y1, by + kTileY - 1) - lo1 + 1;
                 d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
                 const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
-                ne = 2 * (n0 * n1 + n0 * n2 + n1 * n2);
+                ne = TAB ? 0 : 2 * (n0 * n1 + n0 * n2 + n1 * n2);
                 ns = 3 * n0 * n1 * n2;
             }
             int ie = ne, is = ns;
@@ -406,7 +429,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         // (B0) order the corner items so that the cheap ones (corner beyond 2h: only I0 and I1; or a zero
         // corner) run in warps of their own: the others from the front of s_blist, the cheap ones from
         // the back.  Results do not depend on this order.
-        if (!GENERIC) {
+        if (!GENERIC && !TAB) {
             unsigned cheap = 0;
             int nitems = 0;
 #pragma unroll
@@ -460,7 +483,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
 
         // (B) corner values S_a(i, j, k) for the three plane orientations a
         for (int li = threadIdx.x; li < stot; li += kThreads) {
-            const int it = GENERIC ? li : s_blist[li];
+            const int it = (GENERIC || TAB) ? li : s_blist[li];
             const int jp = chunk_search(s_soff, np, it);
             const int s = it - s_soff[jp];
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
@@ -491,7 +514,11 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const double sg = sgn(u1) * sgn(u2);
             if (sg != 0.0 && r0 != 0.0) {
                 const double a1 = fabs(u1), a2 = fabs(u2);
-                if (GENERIC) {
+                if (TAB) {
+                    // two right-triangle vertex pyramids; cos(phi) from the legs
+                    const double h = s_h[jp], rr = sqrt(a1 * a1 + a2 * a2);
+                    f = tab_gridded_c(tab, h, a1 / rr, r0, a1, n_clamp) + tab_gridded_c(tab, h, a2 / rr, r0, a2, n_clamp);
+                } else if (GENERIC) {
                     const double H = mul_rn(g.support_in_h, s_h[jp]);
                     f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
                         lattice_generic_vertex(K, H, r0, a2, a1, s_E + kLatGenERec * e2);
@@ -586,6 +613,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     add_stat(&st->edge_middle, n_em);
     add_stat(&st->edge_inner, n_ei);
     add_stat(&st->vertex_pyramids, n_vp);
+    if (TAB) add_stat(&st->table_clamps, n_clamp);
 }
 
 template <bool CULL>
@@ -607,6 +635,18 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_generi
                                                                                   DevStats* __restrict__ st) {
     const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
     lattice_tile<true, true>(g, P, list, range, t, t, out, st, kernel);
+}
+
+// The lattice form with the tabulated integral, every cell of the particles' bounding boxes (outside the
+// support the lookups do not cancel exactly, and the reference keeps what they leave).
+__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_tab(CartGeom g, DevParticles P, const TabDev tab,
+                                                                              const uint32_t* __restrict__ list,
+                                                                              const int64_t* __restrict__ range,
+                                                                              const int32_t* __restrict__ tile_map,
+                                                                              CartOutputs out,
+                                                                              DevStats* __restrict__ st) {
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    lattice_tile<false, false, true>(g, P, list, range, t, t, out, st, 0, tab);
 }
 
 // The tiles of a batch of grids, one persistent launch per tile-body family (cubic lattice, generic
@@ -634,8 +674,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_batch_persistent(const BatchIte
         else if (FAMILY == kBatchFamilyLatticeGeneric)
             lattice_tile<true, true>(it.g, it.P, list, range, tg, tl, it.out, it.st, it.kernel);
         else
-            gather_tile<false, true, true>(it.g, it.P, it.kernel, list, range, tg, tl, it.out, it.st,
-                                           it.mode == kBatchGatherCubic);
+            gather_tile<kEvGeneric, true, true>(it.g, it.P, it.kernel, list, range, tg, tl, it.out, it.st,
+                                                it.mode == kBatchGatherCubic);
         __syncthreads();
     }
 }
@@ -648,8 +688,8 @@ __global__ void k_full_integral(int kernel, int64_t n, const double* __restrict_
                           : generic_full_integral(&c_tables[kernel], arg0[i], phi[i], r0[i], R0[i]);
 }
 
-__global__ void k_face_integral(bool cubic, int kernel, double support_in_h, int64_t n,
-                                const double* __restrict__ particle, const int64_t* __restrict__ vert_off,
+__global__ void k_face_integral(bool cubic, int kernel, double support_in_h, const TabDev tab, bool tabulated,
+                                int64_t n, const double* __restrict__ particle, const int64_t* __restrict__ vert_off,
                                 const double* __restrict__ verts, double* __restrict__ out,
                                 int32_t* __restrict__ out_vert) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -659,7 +699,11 @@ __global__ void k_face_integral(bool cubic, int kernel, double support_in_h, int
     const int nv = (int)(vert_off[i + 1] - vert_off[i]);
     int ov = 0;
     double r;
-    if (cubic) {
+    if (tabulated) {
+        unsigned nc = 0;
+        TabEval ev{tab, h, 0.0, 0.0, &nc};
+        r = face_integral(x0, y0, z0, 2 * h, V, nv, &ov, ev);
+    } else if (cubic) {
         CubicEval ev;
         ev.h = h;
         r = face_integral(x0, y0, z0, 2 * h, V, nv, &ov, ev);
@@ -744,7 +788,14 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
     if (tl.ntiles > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cell tiles (%lld)", (long long)tl.ntiles);
     if (tl.map && tl.nmap <= 0) return KIWI_OK;
     const dim3 grid((unsigned)(tl.map ? tl.nmap : tl.ntiles));
-    if (k.cubic && !reference_order) {
+    if (k.tabulated && !reference_order) {
+        KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_tab, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kLatTabDynSmem));
+        k_cart_lattice_tab<<<grid, kThreads, kLatTabDynSmem, ctx->stream>>>(g, P, k.tab, tl.list, tl.range, tl.map,
+                                                                            out, d_stats);
+    } else if (k.tabulated) {
+        k_cart_gather_tab<<<grid, kThreads, 0, ctx->stream>>>(g, P, k.tab, tl.list, tl.range, tl.map, out, d_stats);
+    } else if (k.cubic && !reference_order) {
         if (full_box) {
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
@@ -813,8 +864,8 @@ int fp64_full_integral(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, 
 int fp64_face_integral(KiwiCtx* ctx, const KernelChoice& k, int64_t n, const double* particle,
                        const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert) {
     if (n <= 0) return KIWI_OK;
-    k_face_integral<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(k.cubic, k.kernel, k.support_in_h, n,
-                                                                          particle, vert_off, verts, out, out_vert);
+    k_face_integral<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+        k.cubic, k.kernel, k.support_in_h, k.tab, k.tabulated, n, particle, vert_off, verts, out, out_vert);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

@@ -26,6 +26,7 @@
 #include "engine.hpp"
 #include "kiwi_math.cuh"
 #include "prims.cuh"
+#include "tabulated.cuh"
 
 namespace kiwi_b200 {
 
@@ -213,12 +214,18 @@ __device__ __forceinline__ int64_t pair_particle(const int64_t* __restrict__ off
     return lo;
 }
 
-// One face's integral for one particle (the face walk with the kernel's evaluator).
-template <bool CUBIC>
+// One face's integral for one particle (the face walk with the kernel's evaluator).  MODE: kVorGeneric,
+// kVorCubic (closed form) or kVorTab (lookups in tab; clamped indices counted in *nclamp).
+constexpr int kVorGeneric = 0, kVorCubic = 1, kVorTab = 2;
+template <int MODE>
 static __device__ __noinline__ double vor_face(const double* verts, int nv, double x0, double y0, double z0, double h,
-                                               double radius, int kernel) {
+                                               double radius, int kernel, const TabDev& tab, unsigned* nclamp) {
     const FlatVerts V{verts};
-    if (CUBIC) {
+    if (MODE == kVorTab) {
+        TabEval ev{tab, h, 0.0, 0.0, nclamp};
+        return face_integral(x0, y0, z0, 2 * h, V, nv, (int*)nullptr, ev);
+    }
+    if (MODE == kVorCubic) {
         CubicEval ev;
         ev.h = h;
         return face_integral(x0, y0, z0, 2 * h, V, nv, (int*)nullptr, ev);
@@ -237,9 +244,9 @@ __global__ void k_cell_ranges(const uint32_t* __restrict__ keys, int64_t total, 
     if (i == total - 1 || keys[i + 1] != k) range[2 * (int64_t)k + 1] = i + 1;
 }
 
-template <bool CUBIC>
+template <int MODE>
 __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevParticles P, int kernel,
-                                                                double support_in_h,
+                                                                double support_in_h, const TabDev tab,
                                                                 const uint32_t* __restrict__ plist,
                                                                 const int64_t* __restrict__ range,
                                                                 const int64_t* __restrict__ offs,
@@ -259,6 +266,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
     const int64_t beg = range[2 * cell], end = range[2 * cell + 1];
     double M = 0.0, Px = 0.0, Py = 0.0, Pz = 0.0;
     unsigned long long n_neg = 0, n_warn = 0;
+    unsigned n_clamp = 0;
     for (int64_t base = beg; base < end; base += kGatherThreads) {
         const int64_t k = base + threadIdx.x;
         double msum = 0.0;
@@ -312,7 +320,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
                 const int nv = (int)(C.vert_off[src + 1] - C.vert_off[src]);
                 const double* verts = (src >= f0 && src < f1 && staged) ? s_v + 3 * (C.vert_off[src] - v0)
                                                                          : C.vxyz + 3 * C.vert_off[src];
-                const double val = vor_face<CUBIC>(verts, nv, x0, y0, z0, h, radius, kernel);
+                const double val = vor_face<MODE>(verts, nv, x0, y0, z0, h, radius, kernel, tab, &n_clamp);
                 if (sign < 0.0) msum -= val; else msum += val;
             }
             if (msum < 0.0) {
@@ -341,9 +349,11 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
     }
     n_neg = warp_sum_u64(n_neg);
     n_warn = warp_sum_u64(n_warn);
+    const unsigned long long n_cl = warp_sum_u64(n_clamp);
     if ((threadIdx.x & 31) == 0) {
         if (n_neg) atomicAdd(&st->neg_clamped, n_neg);
         if (n_warn) atomicAdd(&st->neg_warned, n_warn);
+        if (n_cl) atomicAdd(&st->table_clamps, n_cl);
     }
     if (threadIdx.x == 0) {
         const double vol = C.volume[cell];
@@ -442,12 +452,15 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     }
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     if (nc > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cells (%lld)", (long long)nc);
-    if (kc.cubic)
-        k_vor_gather<true><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, kc.kernel, sup, plist, range, offs,
-                                                                            pair_cells, pair_mask, out, d_stats);
+    if (kc.tabulated)
+        k_vor_gather<kVorTab><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats);
+    else if (kc.cubic)
+        k_vor_gather<kVorCubic><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats);
     else
-        k_vor_gather<false><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, kc.kernel, sup, plist, range, offs,
-                                                                             pair_cells, pair_mask, out, d_stats);
+        k_vor_gather<kVorGeneric><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats);
     KIWI_LAUNCHED(ctx);
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     DevStats hs;
@@ -464,6 +477,7 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
         stats->skipped_outside = (int64_t)hs.skipped_outside;  // particles whose home cell is unresolved
         stats->neg_clamped = (int64_t)hs.neg_clamped;
         stats->neg_warned = (int64_t)hs.neg_warned;
+        stats->table_clamps = (int64_t)hs.table_clamps;
         stats->tile_pairs = (int64_t)hs.tile_pairs;  // particles whose walk never left the home cell
         stats->gather_ms = ms;
         stats->launches = ctx->launches - launches0;

@@ -10,6 +10,7 @@
 #include "kiwi_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 

@@ -6,6 +6,7 @@
 // pairs gives the algorithmic work per pair, F_pair (flops) and T_pair (transcendentals), of the
 // reference's evaluation order -- the numerator of the cell-integral kernel's roofline.
 #include <math.h>
+#include <stdio.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>

@@ -9,6 +9,7 @@
  */
 #define _GNU_SOURCE
 #include <math.h>
+#include <stdio.h>
 #include <quadmath.h>
 #include <stdint.h>
 #include <stdlib.h>

@@ -65,6 +65,14 @@ class Oracle:
         L.or_sph_to_grid.argtypes = ([C.c_int64] + [_dp] * 8 + [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                                                 C.c_int, C.c_int64, C.c_int64] + [_dp] * 5 +
                                      [C.POINTER(OrStats)])
+        for name in ("table_load", "table_reset", "table_values"):
+            setattr(L, "or_" + name, getattr(L, pfx + name))
+        L.or_table_load.restype = C.c_int
+        L.or_table_load.argtypes = [C.c_char_p]
+        L.or_table_reset.restype = None
+        L.or_table_reset.argtypes = []
+        L.or_table_values.restype = C.c_int64
+        L.or_table_values.argtypes = [_dp]
         L.or_map_voronoi.restype = C.c_int
         L.or_map_voronoi.argtypes = ([C.c_int64, _i32p] + [_dp] * 8 + [C.c_int64, _i64p, _i64p, _dp, _i32p, _dp,
                                                                       C.c_int, C.c_double, C.c_int] + [_dp] * 5 +
@@ -78,6 +86,21 @@ class Oracle:
 
     def gridded_integral(self, h, phi, r0, R0):
         return self.lib.or_gridded_integral(h, phi, r0, R0)
+
+    def table_load(self, path) -> int:
+        """load_density_table restated: 0, or -1 / -2 / -3 (cannot open / header malformed / truncated)."""
+        return self.lib.or_table_load(os.fsencode(path))
+
+    def table_reset(self):
+        """Back to the canonical (generated) table."""
+        self.lib.or_table_reset()
+
+    def table_values(self) -> np.ndarray:
+        """The values of the table in use, flat, laid out as DensityLookupTable::at."""
+        n = self.lib.or_table_values(None)
+        out = np.empty(n)
+        self.lib.or_table_values(_d(out))
+        return out
 
     def face_integral(self, x0, y0, z0, verts, kernel=-1, h=1.0, support=None, tabulated=False):
         v = _f64(verts).reshape(-1)
@@ -169,6 +192,26 @@ class RefLib:
         L.ref_max_threads.restype = C.c_int
         L.ref_save_cartesian_grid.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int] + [_dp] * 5
         L.ref_save_mapping.argtypes = [C.c_char_p, C.c_long, C.POINTER(C.c_long)] + [_dp] * 8
+        L.ref_table_load_gridded.restype = C.c_int
+        L.ref_table_load_gridded.argtypes = [C.c_char_p, C.c_int64] + [_dp] * 5
+        L.ref_table_values.restype = C.c_int64
+        L.ref_table_values.argtypes = [_dp]
+
+    def table_load_gridded(self, path, h, phi, r0, R0):
+        """load_density_table(path), then gridded_integral with that table over the arrays (RuntimeError
+        with the reference's message when loading fails)."""
+        a = [_f64(np.atleast_1d(v)) for v in (h, phi, r0, R0)]
+        out = np.empty(a[0].size)
+        if self.lib.ref_table_load_gridded(os.fsencode(path), out.size, *[_d(v) for v in a], _d(out)) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return out
+
+    def table_values(self) -> np.ndarray:
+        """generate_density_table()'s values, flat, laid out as DensityLookupTable::at."""
+        n = self.lib.ref_table_values(None)
+        out = np.empty(n)
+        self.lib.ref_table_values(_d(out))
+        return out
 
     def save_cartesian_grid(self, path, shape, bounds, density, vx, vy, vz):
         arrs = [_f64(a) for a in (bounds, density, vx, vy, vz)]

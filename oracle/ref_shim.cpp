@@ -92,6 +92,30 @@ double ref_gridded_integral(double h, double phi, double r0, double R_0) {
     return kiwi::gridded_integral(table, h, phi, r0, R_0);
 }
 
+// load_density_table(path), then gridded_integral with it on n items.  0, or -1 with the reference's
+// exception message in ref_last_error().
+int ref_table_load_gridded(const char* path, int64_t n, const double* h, const double* phi, const double* r0,
+                           const double* R_0, double* out) {
+    try {
+        const kiwi::DensityLookupTable t = kiwi::load_density_table(path);
+        for (int64_t i = 0; i < n; ++i) out[i] = kiwi::gridded_integral(t, h[i], phi[i], r0[i], R_0[i]);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// The values of generate_density_table(), laid out as DensityLookupTable::at (out may be NULL to ask for
+// their count).
+int64_t ref_table_values(double* out) {
+    static kiwi::DensityLookupTable table = kiwi::generate_density_table();
+    const int64_t n = (int64_t)table.values.size();
+    if (out)
+        for (int64_t i = 0; i < n; ++i) out[i] = table.values[i];
+    return n;
+}
+
 // kernel < 0: compute_face_integral (support 2h); else compute_face_integral_generic with H = support.
 double ref_face_integral(double x0, double y0, double z0, int kernel, double h, double support, int tabulated,
                          const double* verts, int n, int* out_vert) {
