@@ -271,6 +271,17 @@ int kiwi_save_mapping(const char* path, int64_t n_cells, const int64_t* id, cons
                       const double* z, const double* volume, const double* density, const double* vx, const double* vy,
                       const double* vz, char* err, size_t err_len);
 
+/* save_inverse_mapping_test (src/mapping.cpp:505-513): inverse-mapping-test.dat, a '#' header, the totals
+ * (original, grid, recovered mass) and "id m_original m_recovered coverage_fraction" per particle, with 15
+ * significant digits. */
+int kiwi_save_inverse_mapping_test(const char* path, int64_t n, const int64_t* id, const double* m_original,
+                                   const double* m_recovered, const double* coverage, const double* totals3, char* err,
+                                   size_t err_len);
+/* load_inverse_mapping_test (src/mapping.cpp:519-538): *n receives the row count; rows are stored while
+ * they fit in `capacity` (id may be NULL to count only); the reference's messages on a bad file. */
+int kiwi_load_inverse_mapping_test(const char* path, int64_t* n, double* totals3, int64_t* id, double* m_original,
+                                   double* m_recovered, double* coverage, int64_t capacity, char* err, size_t err_len);
+
 /* ---- Voronoi map stage (run_mapping_stage's particle loop, src/mapping.cpp:105-206, 400-502) --- */
 /* Cell geometry in CSR form: the plain data of CellFaceGeometry (src/mapping.cpp:49-54) with vertex
  * coordinates made absolute as src/mapping.cpp:168-175 does and neighbour ids resolved to cell indices. */
@@ -289,6 +300,19 @@ typedef struct KiwiVoronoiCells {
 int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
                      const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
                      double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
+
+/* The inverse-mapping check (run_inverse_mapping_test_stage's particle loop, src/mapping.cpp:540-701): the
+ * same cell walk and cell integrals as kiwi_map_voronoi, summed per particle instead of per cell, in the
+ * walk's order: m_recovered[i] = sum over the cells i reaches of (integral m_i' / M_c) M_c over cells with
+ * M_c > 0, coverage[i] = m_recovered[i] / m_i (0 if m_i <= 0); particles with h <= 0 or an unresolved home
+ * cell recover 0.  cell_mass (may be NULL): M_c per cell, density x volume of the forward mapping (the
+ * reference takes mapping.dat's rows); NULL uses this call's own forward map.  totals3 (may be NULL):
+ * total original mass, total grid mass (sum of M_c), total recovered mass, summed in order.  density (may
+ * be NULL) receives the forward map's densities.  Host arrays. */
+int kiwi_inverse_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                             const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision,
+                             const double* cell_mass, double* m_recovered, double* coverage, double* totals3,
+                             double* density, KiwiStats* stats);
 
 #ifdef __cplusplus
 }

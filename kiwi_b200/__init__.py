@@ -570,6 +570,10 @@ def _io_lib():
                                                                                                    C.c_size_t]
     L.kiwi_load_cartesian_grid.argtypes = [C.c_char_p, C.POINTER(C.c_int32)] + [_dp] * 5 + [C.c_char_p, C.c_size_t]
     L.kiwi_save_mapping.argtypes = ([C.c_char_p, C.c_int64, _i64p] + [_dp] * 8 + [C.c_char_p, C.c_size_t])
+    L.kiwi_save_inverse_mapping_test.argtypes = ([C.c_char_p, C.c_int64, _i64p] + [_dp] * 4 +
+                                                 [C.c_char_p, C.c_size_t])
+    L.kiwi_load_inverse_mapping_test.argtypes = ([C.c_char_p, C.POINTER(C.c_int64), _dp, _i64p] + [_dp] * 3 +
+                                                 [C.c_int64, C.c_char_p, C.c_size_t])
     return L
 
 
@@ -643,6 +647,83 @@ def map_voronoi(particles: dict, home_cell, cells: dict, kernel=None, precision=
     d["unmapped"] = d["tile_pairs"]
     d["visited_pairs"] = d["evaluated_pairs"]
     return MappingResult(*outs, raw=rawa.reshape(4, nc) if raw else None, stats=d)
+
+
+@dataclass
+class InverseMappingResult:
+    """run_inverse_mapping_test_stage's results (include/kiwi/mapping.hpp:88-106): per particle, in snapshot
+    order, the mass recovered from the cells its kernel reaches and its coverage fraction; the totals of the
+    original masses, the grid's cell masses and the recovered masses."""
+    m_original: np.ndarray
+    m_recovered: np.ndarray
+    coverage: np.ndarray
+    total_original_mass: float
+    total_grid_mass: float
+    total_recovered_mass: float
+    density: np.ndarray | None = None
+    stats: dict = field(default_factory=dict)
+
+
+def inverse_map_voronoi(particles: dict, home_cell, cells: dict, kernel=None, cell_mass=None, precision="fp64",
+                        ctx=None) -> InverseMappingResult:
+    """The inverse-mapping check (run_inverse_mapping_test_stage's particle loop, src/mapping.cpp:540-701):
+    the cell walk and cell integrals of map_voronoi, summed per particle.  `cell_mass`: M_c per cell
+    (density x volume of the forward mapping's rows, as the stage reads them from mapping.dat); None uses
+    this call's own forward map."""
+    ctx = ctx or default_context()
+    ki = kernel or KernelIntegrator()
+    Ps, keep = _particles_struct(particles)
+    n = int(Ps.n)
+    home = np.ascontiguousarray(home_cell, dtype=np.int32)
+    fo = np.ascontiguousarray(cells["face_off"], dtype=np.int64)
+    vo = np.ascontiguousarray(cells["vert_off"], dtype=np.int64)
+    vx_ = _f64(cells["vxyz"]).reshape(-1)
+    nb = np.ascontiguousarray(cells["face_nbr"], dtype=np.int32)
+    vol = _f64(cells["volume"])
+    nc = len(vol)
+    cs = KiwiVoronoiCells(nc, fo.ctypes.data_as(_i64p), vo.ctypes.data_as(_i64p), _p(vx_), nb.ctypes.data_as(_i32p),
+                          _p(vol))
+    cm = _f64(cell_mass) if cell_mass is not None else None
+    rec, cov, tot, dens = np.zeros(n), np.zeros(n), np.zeros(3), np.empty(nc)
+    st = KiwiStats()
+    sel = ki.sel()
+    ctx._L.kiwi_inverse_map_voronoi.argtypes = [C.c_void_p, C.POINTER(KiwiParticles), _i32p,
+                                                C.POINTER(KiwiVoronoiCells), C.POINTER(KiwiKernelSel), C.c_int,
+                                                _dp, _dp, _dp, _dp, _dp, C.POINTER(KiwiStats)]
+    ctx.check(ctx._L.kiwi_inverse_map_voronoi(ctx.handle, C.byref(Ps), home.ctypes.data_as(_i32p), C.byref(cs),
+                                              C.byref(sel), precision_code(precision), _p(cm), _p(rec), _p(cov),
+                                              _p(tot), _p(dens), C.byref(st)), "inverse map")
+    d = st.as_dict()
+    d["unresolved"] = d["skipped_outside"]
+    d["visited_pairs"] = d["evaluated_pairs"]
+    return InverseMappingResult(_f64(particles["m"]).copy(), rec, cov, float(tot[0]), float(tot[1]), float(tot[2]),
+                                density=dens, stats=d)
+
+
+def save_inverse_mapping_test(path: str, ids, result: InverseMappingResult):
+    """save_inverse_mapping_test (src/mapping.cpp:505-513): inverse-mapping-test.dat."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    ids = np.ascontiguousarray(ids, dtype=np.int64)
+    arrs = [_f64(result.m_original), _f64(result.m_recovered), _f64(result.coverage)]
+    tot = np.array([result.total_original_mass, result.total_grid_mass, result.total_recovered_mass])
+    _io_check(L.kiwi_save_inverse_mapping_test(path.encode(), len(ids), ids.ctypes.data_as(_i64p),
+                                               *[_p(a) for a in arrs], _p(tot), err, len(err)), err)
+
+
+def load_inverse_mapping_test(path: str):
+    """load_inverse_mapping_test (src/mapping.cpp:519-538): (ids, InverseMappingResult)."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    n = C.c_int64(0)
+    tot = np.zeros(3)
+    _io_check(L.kiwi_load_inverse_mapping_test(path.encode(), C.byref(n), _p(tot), None, None, None, None, 0, err,
+                                               len(err)), err)
+    ids = np.zeros(n.value, dtype=np.int64)
+    arrs = [np.zeros(n.value) for _ in range(3)]
+    _io_check(L.kiwi_load_inverse_mapping_test(path.encode(), C.byref(n), _p(tot), ids.ctypes.data_as(_i64p),
+                                               *[_p(a) for a in arrs], n.value, err, len(err)), err)
+    return ids, InverseMappingResult(*arrs, float(tot[0]), float(tot[1]), float(tot[2]))
 
 
 def version() -> str:

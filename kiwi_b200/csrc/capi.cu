@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/kiwi_b200.h"
 #include "engine.hpp"
@@ -531,9 +532,22 @@ int kiwi_sph_to_grid(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCar
     return KIWI_OK;
 }
 
-int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+}  // extern "C"
+
+namespace {
+
+// Host outputs of the inverse-mapping check (kiwi_inverse_map_voronoi).
+struct InverseHost {
+    const double* cell_mass;
+    double* m_recovered;
+    double* coverage;
+    double* totals3;
+};
+
+// kiwi_map_voronoi on host arrays: stage, map (and with inv, the inverse check), copy back.
+int map_voronoi_host(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
                      const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
-                     double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats) {
+                     double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats, const InverseHost* inv) {
     KIWI_TRY(check_ctx(ctx));
     int rc = KIWI_OK;
     if (!particles_ok(ctx, particles, &rc)) return rc;
@@ -573,6 +587,8 @@ int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t
     KIWI_TRY(scratch_t(ctx, S_VOR_HOME, (size_t)std::max<int64_t>(n, 1), &dhome));
     KIWI_TRY(scratch_t(ctx, S_VOR_CSR, geo_bytes, &dgeo));
     KIWI_TRY(scratch_t(ctx, S_OUT, (size_t)(raw4 ? 8 : 4) * std::max<int64_t>(nc, 1), &dout));
+    double* dinv = nullptr;  // inverse check: cell masses (given), recovered masses, coverage
+    if (inv) KIWI_TRY(scratch_t(ctx, S_INV_OUT, (size_t)(std::max<int64_t>(nc, 1) + 2 * std::max<int64_t>(n, 1)), &dinv));
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
     const double* src[8] = {particles->x, particles->y, particles->z, particles->vx,
                             particles->vy, particles->vz, particles->m, particles->h};
@@ -596,7 +612,28 @@ int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t
                    dpart + 7 * n};
     KiwiVoronoiCells dc{nc, d_fo, d_vo, d_v, d_nb, d_vol};
     CartOutputs out{dout, dout + nc, dout + 2 * nc, dout + 3 * nc, raw4 ? dout + 4 * nc : nullptr, nullptr};
-    KIWI_TRY(voronoi_map_dev(ctx, P, dhome, dc, kc, out, stats));
+    VorInverse dinv_v{nullptr, nullptr, nullptr};
+    if (inv) {
+        double* d_cm = dinv;
+        dinv_v.m_recovered = dinv + std::max<int64_t>(nc, 1);
+        dinv_v.coverage = dinv_v.m_recovered + std::max<int64_t>(n, 1);
+        if (n > 0) {
+            KIWI_CUDA(ctx, cudaMemsetAsync(dinv_v.m_recovered, 0, sizeof(double) * n, ctx->stream));
+            KIWI_CUDA(ctx, cudaMemsetAsync(dinv_v.coverage, 0, sizeof(double) * n, ctx->stream));
+        }
+        if (inv->cell_mass && nc > 0) {
+            KIWI_CUDA(ctx, cudaMemcpyAsync(d_cm, inv->cell_mass, sizeof(double) * nc, cudaMemcpyHostToDevice, ctx->stream));
+            dinv_v.cell_mass = d_cm;
+        }
+    }
+    KIWI_TRY(voronoi_map_dev(ctx, P, dhome, dc, kc, out, stats, inv ? &dinv_v : nullptr));
+    if (inv && n > 0) {
+        KIWI_CUDA(ctx, cudaMemcpyAsync(inv->m_recovered, dinv_v.m_recovered, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+        if (inv->coverage)
+            KIWI_CUDA(ctx, cudaMemcpyAsync(inv->coverage, dinv_v.coverage, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                           ctx->stream));
+    }
     double* dst[4] = {density, vx, vy, vz};
     for (int a = 0; a < 4 && nc > 0; ++a)
         if (dst[a])
@@ -610,7 +647,52 @@ int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t
         cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
         stats->total_ms = ms;
     }
+    if (inv && inv->totals3) {
+        // the totals of src/mapping.cpp:675-682, summed in particle and cell order on the host: the
+        // original masses (every particle), the grid mass sum of m_i, the recovered masses
+        double t_orig = 0.0, t_grid = 0.0, t_rec = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+            t_orig += particles->m[i];
+            t_rec += inv->m_recovered[i];
+        }
+        if (inv->cell_mass) {
+            for (int64_t c = 0; c < nc; ++c) t_grid += inv->cell_mass[c];
+        } else if (density) {
+            for (int64_t c = 0; c < nc; ++c) t_grid += density[c] * cells->volume[c];
+        }
+        inv->totals3[0] = t_orig;
+        inv->totals3[1] = t_grid;
+        inv->totals3[2] = t_rec;
+    }
     return KIWI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                     const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
+                     double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats) {
+    return map_voronoi_host(ctx, particles, home_cell, cells, kernel, precision, density, vx, vy, vz, raw4, stats,
+                            nullptr);
+}
+
+int kiwi_inverse_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                             const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision,
+                             const double* cell_mass, double* m_recovered, double* coverage, double* totals3,
+                             double* density, KiwiStats* stats) {
+    if (ctx && particles && particles->n > 0 && !m_recovered)
+        return set_err(ctx, KIWI_ERR_ARG, "inverse map: m_recovered is null");
+    // the grid-mass total without given cell masses needs the forward densities on the host
+    std::vector<double> dens_tmp;
+    if (!cell_mass && totals3 && !density && cells && cells->n_cells > 0) {
+        dens_tmp.resize((size_t)cells->n_cells);
+        density = dens_tmp.data();
+    }
+    const InverseHost inv{cell_mass, m_recovered, coverage, totals3};
+    return map_voronoi_host(ctx, particles, home_cell, cells, kernel, precision, density, nullptr, nullptr, nullptr,
+                            nullptr, stats, &inv);
 }
 
 }  // extern "C"

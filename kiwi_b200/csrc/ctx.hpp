@@ -26,7 +26,7 @@ struct KiwiCtx {
     std::string err;
     int64_t launches = 0;  // kernels launched on this context (for the stats of a call)
     // Scratch slots: each is grown on demand and reused by later calls on this context.
-    static constexpr int kSlots = 32;
+    static constexpr int kSlots = 40;
     void* slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Fixed arena mode (used only by the allocation-free entry point): when `arena` is set, scratch
@@ -54,9 +54,11 @@ inline int set_err(KiwiCtx* ctx, int code, const char* fmt, ...) {
 #define KIWI_CUDA(ctx, call)                                                                              \
     do {                                                                                                  \
         cudaError_t e_ = (call);                                                                          \
-        if (e_ != cudaSuccess)                                                                            \
+        if (e_ != cudaSuccess) {                                                                          \
+            cudaGetLastError(); /* a non-sticky error must not resurface at the next launch check */      \
             return ::kiwi_b200::set_err((ctx), KIWI_ERR_CUDA, "%s failed: %s (%s:%d)", #call,              \
                                         cudaGetErrorString(e_), __FILE__, __LINE__);                      \
+        }                                                                                                 \
     } while (0)
 
 #define KIWI_LAUNCHED(ctx)                                                                                \
@@ -147,6 +149,10 @@ enum ScratchSlot {
     S_STATS2,        // device counters of a second pass
     S_VOR_MASK,      // Voronoi walk: per pair, the faces whose neighbour was processed earlier
     S_ADJ_PART,      // adjoint: partial gradients per (tile, particle) entry
+    S_VOR_PVAL,      // inverse map: each visited pair's cell integral
+    S_VOR_CMASS,     // inverse map: per-cell mass m_i
+    S_INV_OUT,       // inverse map: given cell masses, recovered masses and coverage (host entry point)
 };
+static_assert(S_INV_OUT < KiwiCtx::kSlots, "scratch slots");
 
 }  // namespace kiwi_b200

@@ -101,8 +101,17 @@ int fp32_measure_peak(KiwiCtx* ctx, double* tflops);
 
 // voronoi.cu
 int voronoi_init_tables(KiwiCtx* ctx);
+// The inverse-mapping check's outputs (run_inverse_mapping_test_stage, src/mapping.cpp:540-701): per
+// particle the mass recovered from the cells it reaches and its coverage fraction (device arrays of n);
+// cell_mass: m_i per cell (device), or null for density x volume of the same call's forward map.
+struct VorInverse {
+    const double* cell_mass;
+    double* m_recovered;
+    double* coverage;
+};
 int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, const KiwiVoronoiCells& cells,
-                    const KernelChoice& kc, const CartOutputs& out, KiwiStats* stats);
+                    const KernelChoice& kc, const CartOutputs& out, KiwiStats* stats,
+                    const VorInverse* inv = nullptr);
 
 // kiwi_fp64.cu
 int fp64_init_tables(KiwiCtx* ctx);

@@ -6,6 +6,8 @@
 //   doubles each in the x-major cell order, all in the machine's (little-endian) byte order.
 //   mapping.dat (src/mapping.cpp:307-315): one line per cell, "id x y z volume density vx vy vz", the
 //   numbers printed by an ostream with precision 15.
+//   inverse-mapping-test.dat (src/mapping.cpp:505-538): a '#' header line, the three totals, then one line
+//   per particle, "id m_original m_recovered coverage_fraction", precision 15.
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -91,6 +93,59 @@ int kiwi_save_mapping(const char* path, int64_t n_cells, const int64_t* id, cons
         f << id[c] << " " << x[c] << " " << y[c] << " " << z[c] << " " << volume[c] << " " << density[c] << " "
           << vx[c] << " " << vy[c] << " " << vz[c] << "\n";
     if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("failed writing mapping file: ") + path);
+    return KIWI_OK;
+}
+
+int kiwi_save_inverse_mapping_test(const char* path, int64_t n, const int64_t* id, const double* m_original,
+                                   const double* m_recovered, const double* coverage, const double* totals3, char* err,
+                                   size_t err_len) {
+    if (!path || !totals3 || n < 0 || (n > 0 && (!id || !m_original || !m_recovered || !coverage)))
+        return io_err(err, err_len, KIWI_ERR_ARG, "save_inverse_mapping_test: a null argument");
+    std::ofstream f(path);
+    if (!f)
+        return io_err(err, err_len, KIWI_ERR_ARG,
+                      std::string("could not open inverse-mapping-test file for writing: ") + path);
+    f << std::setprecision(15);
+    f << "# total_original_mass total_grid_mass total_recovered_mass\n";
+    f << totals3[0] << " " << totals3[1] << " " << totals3[2] << "\n";
+    for (int64_t i = 0; i < n; ++i)
+        f << id[i] << " " << m_original[i] << " " << m_recovered[i] << " " << coverage[i] << "\n";
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("failed writing inverse-mapping-test file: ") + path);
+    return KIWI_OK;
+}
+
+int kiwi_load_inverse_mapping_test(const char* path, int64_t* n, double* totals3, int64_t* id, double* m_original,
+                                   double* m_recovered, double* coverage, int64_t capacity, char* err, size_t err_len) {
+    if (!path || !n) return io_err(err, err_len, KIWI_ERR_ARG, "load_inverse_mapping_test: a null argument");
+    std::ifstream f(path);
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("could not open inverse-mapping-test file: ") + path);
+    std::string header;
+    if (!std::getline(f, header) || header.empty() || header[0] != '#')
+        return io_err(err, err_len, KIWI_ERR_ARG,
+                      std::string("inverse-mapping-test file missing expected '#' totals header: ") + path);
+    double t[3];
+    if (!(f >> t[0] >> t[1] >> t[2]))
+        return io_err(err, err_len, KIWI_ERR_ARG,
+                      std::string("could not read totals line from inverse-mapping-test file: ") + path);
+    if (totals3) std::memcpy(totals3, t, sizeof(t));
+    int64_t rows = 0;
+    long long rid;
+    double a, b, c;
+    while (f >> rid >> a >> b >> c) {
+        if (id && rows < capacity) {
+            id[rows] = (int64_t)rid;
+            if (m_original) m_original[rows] = a;
+            if (m_recovered) m_recovered[rows] = b;
+            if (coverage) coverage[rows] = c;
+        }
+        ++rows;
+    }
+    if (rows == 0)
+        return io_err(err, err_len, KIWI_ERR_ARG,
+                      std::string("inverse-mapping-test file contained no particle rows (wrong format?): ") + path);
+    *n = rows;
+    if (id && rows > capacity)
+        return io_err(err, err_len, KIWI_ERR_ARG, "load_inverse_mapping_test: more rows than the arrays hold");
     return KIWI_OK;
 }
 

@@ -252,7 +252,8 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
                                                                 const int64_t* __restrict__ offs,
                                                                 const int32_t* __restrict__ pair_cells,
                                                                 const unsigned long long* __restrict__ pair_mask,
-                                                                CartOutputs out, DevStats* __restrict__ st) {
+                                                                CartOutputs out, DevStats* __restrict__ st,
+                                                                double* __restrict__ pair_val) {
     __shared__ double s_v[3 * kGatherVertCap];
     __shared__ double s_val[kGatherThreads], s_m[kGatherThreads], s_vx[kGatherThreads], s_vy[kGatherThreads],
         s_vz[kGatherThreads];
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
                 if (msum <= -0.01) ++n_warn;
                 msum = 0.0;
             }
+            if (pair_val) pair_val[pk] = msum;
             s_m[threadIdx.x] = P.m[p];
             s_vx[threadIdx.x] = P.vx[p];
             s_vy[threadIdx.x] = P.vy[p];
@@ -371,10 +373,36 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
     }
 }
 
+// m_i = density * volume per cell (the forward map's cell mass, as run_inverse_mapping_test_stage forms
+// it from the mapping's rows, src/mapping.cpp:554-561).
+__global__ void k_vor_cell_mass(int64_t nc, const double* __restrict__ density, const double* __restrict__ volume,
+                                double* __restrict__ cmass) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) cmass[c] = density[c] * volume[c];
+}
+
+// Per particle, the inverse-mapping sum over its visited cells in the walk's order
+// (src/mapping.cpp:635-661): recovered += (integral m / m_i) m_i for cells with m_i > 0; coverage =
+// recovered / m (0 for m <= 0).  Particles without pairs (h <= 0, unresolved home cell) recover 0.
+__global__ void k_vor_recover(DevParticles P, const int64_t* __restrict__ offs, const int32_t* __restrict__ pair_cells,
+                              const double* __restrict__ pair_val, const double* __restrict__ cmass,
+                              double* __restrict__ recovered, double* __restrict__ coverage) {
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.n) return;
+    const double m = P.m[p];
+    double r = 0.0;
+    for (int64_t k = offs[p]; k < offs[p + 1]; ++k) {
+        const double mi = cmass[pair_cells[k]];
+        if (mi > 0.0) r += (pair_val[k] * m / mi) * mi;
+    }
+    recovered[p] = r;
+    coverage[p] = (m > 0.0) ? r / m : 0.0;
+}
+
 }  // namespace
 
 int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, const KiwiVoronoiCells& cells,
-                    const KernelChoice& kc, const CartOutputs& out_in, KiwiStats* stats) {
+                    const KernelChoice& kc, const CartOutputs& out_in, KiwiStats* stats, const VorInverse* inv) {
     const int64_t launches0 = ctx->launches;
     const int64_t n = P.n, nc = cells.n_cells;
     VorCells C{nc, cells.face_off, cells.vert_off, cells.vxyz, cells.face_nbr, cells.volume};
@@ -452,16 +480,32 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     }
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
     if (nc > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cells (%lld)", (long long)nc);
+    double* pair_val = nullptr;
+    if (inv) KIWI_TRY(scratch_t(ctx, S_VOR_PVAL, (size_t)std::max<int64_t>(total, 1), &pair_val));
     if (kc.tabulated)
         k_vor_gather<kVorTab><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
-            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats);
+            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
     else if (kc.cubic)
         k_vor_gather<kVorCubic><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
-            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats);
+            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
     else
         k_vor_gather<kVorGeneric><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
-            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats);
+            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
     KIWI_LAUNCHED(ctx);
+    if (inv && n > 0) {
+        const double* cmass = inv->cell_mass;
+        if (!cmass) {
+            if (!out.density) return set_err(ctx, KIWI_ERR_ARG, "inverse map: no cell masses and no density output");
+            double* cm = nullptr;
+            KIWI_TRY(scratch_t(ctx, S_VOR_CMASS, (size_t)nc, &cm));
+            k_vor_cell_mass<<<(unsigned)((nc + 255) / 256), 256, 0, ctx->stream>>>(nc, out.density, cells.volume, cm);
+            KIWI_LAUNCHED(ctx);
+            cmass = cm;
+        }
+        k_vor_recover<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(P, offs, pair_cells, pair_val, cmass,
+                                                                            inv->m_recovered, inv->coverage);
+        KIWI_LAUNCHED(ctx);
+    }
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
     DevStats hs;
     KIWI_CUDA(ctx, cudaMemcpyAsync(&hs, d_stats, sizeof hs, cudaMemcpyDeviceToHost, ctx->stream));

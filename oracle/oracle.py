@@ -65,6 +65,10 @@ class Oracle:
         L.or_sph_to_grid.argtypes = ([C.c_int64] + [_dp] * 8 + [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                                                 C.c_int, C.c_int64, C.c_int64] + [_dp] * 5 +
                                      [C.POINTER(OrStats)])
+        L.or_inverse_map = getattr(L, pfx + "inverse_map")
+        L.or_inverse_map.restype = C.c_int
+        L.or_inverse_map.argtypes = ([C.c_int64, _i32p] + [_dp] * 8 + [C.c_int64, _i64p, _i64p, _dp, _i32p, _dp,
+                                                                       C.c_int, C.c_double, C.c_int] + [_dp] * 3)
         for name in ("table_load", "table_reset", "table_values"):
             setattr(L, "or_" + name, getattr(L, pfx + name))
         L.or_table_load.restype = C.c_int
@@ -86,6 +90,24 @@ class Oracle:
 
     def gridded_integral(self, h, phi, r0, R0):
         return self.lib.or_gridded_integral(h, phi, r0, R0)
+
+    def inverse_map(self, P, home, geo, kernel=-1, support_in_h=2.0, tabulated=False, cell_mass=None):
+        """run_inverse_mapping_test_stage's particle loop: (m_recovered, coverage) per particle."""
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+        n = len(arrs[0])
+        home = np.ascontiguousarray(home, dtype=np.int32)
+        fo = np.ascontiguousarray(geo["face_off"], dtype=np.int64)
+        vo = np.ascontiguousarray(geo["vert_off"], dtype=np.int64)
+        vx_ = _f64(geo["vxyz"]).reshape(-1)
+        fn = np.ascontiguousarray(geo["face_nbr"], dtype=np.int32)
+        vol = _f64(geo["volume"])
+        cm = _f64(cell_mass) if cell_mass is not None else None
+        rec, cov = np.zeros(n), np.zeros(n)
+        self.lib.or_inverse_map(n, home.ctypes.data_as(_i32p), *[_d(a) for a in arrs], len(vol),
+                                fo.ctypes.data_as(_i64p), vo.ctypes.data_as(_i64p), _d(vx_),
+                                fn.ctypes.data_as(_i32p), _d(vol), kernel, support_in_h, int(tabulated), _d(cm),
+                                _d(rec), _d(cov))
+        return rec, cov
 
     def table_load(self, path) -> int:
         """load_density_table restated: 0, or -1 / -2 / -3 (cannot open / header malformed / truncated)."""
@@ -192,6 +214,8 @@ class RefLib:
         L.ref_max_threads.restype = C.c_int
         L.ref_save_cartesian_grid.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int] + [_dp] * 5
         L.ref_save_mapping.argtypes = [C.c_char_p, C.c_long, C.POINTER(C.c_long)] + [_dp] * 8
+        L.ref_voronoi_inverse_copy.argtypes = [C.c_void_p] + [_dp] * 4
+        L.ref_voronoi_inverse_copy.restype = None
         L.ref_table_load_gridded.restype = C.c_int
         L.ref_table_load_gridded.argtypes = [C.c_char_p, C.c_int64] + [_dp] * 5
         L.ref_table_values.restype = C.c_int64
@@ -216,6 +240,14 @@ class RefLib:
     def save_cartesian_grid(self, path, shape, bounds, density, vx, vy, vz):
         arrs = [_f64(a) for a in (bounds, density, vx, vy, vz)]
         if self.lib.ref_save_cartesian_grid(path.encode(), *[int(s) for s in shape], *[_d(a) for a in arrs]) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def save_inverse_mapping_test(self, path, ids, m_original, m_recovered, coverage, totals):
+        ids = np.ascontiguousarray(ids, dtype=np.int64)
+        arrs = [_f64(a) for a in (m_original, m_recovered, coverage, totals)]
+        f = self.lib.ref_save_inverse_mapping_test
+        f.argtypes = [C.c_char_p, C.c_long, C.POINTER(C.c_long)] + [_dp] * 4
+        if f(path.encode(), len(ids), ids.ctypes.data_as(C.POINTER(C.c_long)), *[_d(a) for a in arrs]) != 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
 
     def save_mapping(self, path, ids, x, y, z, volume, density, vx, vy, vz):
@@ -277,7 +309,8 @@ class RefLib:
     def voronoi(self, P, bounds, buffer=False, spacing_fraction=0.0, lloyd=0, kernel="cubic_spline",
                 support_in_h=0.0, generic_path=False, threads=0, run_map=True):
         """Cell geometry (CSR, as src/mapping.cpp builds it), home cells and, if run_map, the reference's
-        own mapping.dat values per cell."""
+        own mapping.dat values per cell; with run_map=2 also the inverse-mapping check's results
+        (run_inverse_mapping_test_stage: per-particle recovered mass and coverage, totals, cell masses)."""
         arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
         n = len(arrs[0])
         b = _f64(bounds)
@@ -299,6 +332,13 @@ class RefLib:
                                   g["face_off"].ctypes.data_as(lp), g["vert_off"].ctypes.data_as(lp), _d(g["vxyz"]),
                                   g["face_nbr"].ctypes.data_as(_ip), g["home"].ctypes.data_as(_ip),
                                   *[_d(r) for r in res])
+        if run_map == 2:
+            inv = {"m_recovered": np.zeros(npart), "coverage": np.zeros(npart), "totals": np.zeros(3),
+                   "cell_mass": np.zeros(nc)}
+            self.lib.ref_voronoi_inverse_copy(hnd, _d(inv["m_recovered"]), _d(inv["coverage"]), _d(inv["totals"]),
+                                              _d(inv["cell_mass"]))
+            self.lib.ref_voronoi_free(hnd)
+            return g, res, inv
         self.lib.ref_voronoi_free(hnd)
         return g, (res if run_map else None)
 

@@ -243,13 +243,92 @@ struct RefVoronoi {
     std::vector<int> face_nbr;              // resolved cell index or -1
     std::vector<int> home;                  // per particle: cell index or -1
     std::vector<double> density, vx, vy, vz;
+    // run_map == 2: run_inverse_mapping_test_stage's rows (per particle, snapshot order), its totals and
+    // the cell masses it used (density x volume of the cached mapping rows, geometry order)
+    std::vector<double> inv_recovered, inv_coverage, inv_cell_mass;
+    double inv_totals[3] = {0.0, 0.0, 0.0};
 };
 
-// Builds the cell geometry the way src/mapping.cpp:222-269 does (same container and block setup), in
-// CSR form with vertices made absolute as src/mapping.cpp:168-175 does, plus each particle's home cell
-// as src/mapping.cpp:434-439 finds it.  Points: the final point set (after buffer/Lloyd) -- taken from
-// run_point_set_stage on the same snapshot, as run_mapping_stage does.  Then runs run_mapping_stage
-// itself and keeps its per-cell rows (matched by site id to the geometry order).
+// Tessellates the point set the way src/mapping.cpp:222-269 does (same container and block setup) into R's
+// CSR geometry, vertices made absolute as src/mapping.cpp:168-175 does, plus each particle's home cell as
+// src/mapping.cpp:434-439 finds it; returns the largest site id.
+static int tessellate(const kiwi::Config& c, const kiwi::PointSet& pts, long n, const double* x, const double* y,
+                      const double* z, RefVoronoi* R, std::vector<int>& reverse) {
+    const kiwi::Domain& d = c.domain;
+    voro::pre_container pcon(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, false, false, false);
+    for (size_t i = 0; i < pts.size(); ++i) pcon.put(pts.id[i], pts.x[i], pts.y[i], pts.z[i]);
+    int bx, by, bz;
+    kiwi::guess_scaled_blocks(pcon, c.grid_blocks.block_scale_factor, bx, by, bz);
+    voro::container con(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, bx, by, bz, false, false, false, 8);
+    pcon.setup(con);
+    int max_id = 0;
+    for (int pid : pts.id) max_id = std::max(max_id, pid);
+    reverse.assign(max_id + 1, -1);
+    std::vector<std::vector<int>> fvert_all, nlist_all;
+    std::vector<std::vector<double>> fcoord_all;
+    voro::voronoicell_neighbor cell;
+    voro::c_loop_all clo(con);
+    double px, py, pz;
+    if (clo.start()) do {
+        if (con.compute_cell(cell, clo)) {
+            int idx = static_cast<int>(R->id.size());
+            R->id.push_back(clo.pid());
+            reverse[clo.pid()] = idx;
+            clo.pos(px, py, pz);
+            R->site.push_back(px);
+            R->site.push_back(py);
+            R->site.push_back(pz);
+            std::vector<int> fv, nl;
+            std::vector<double> fc;
+            cell.face_vertices(fv);
+            cell.vertices(fc);
+            cell.neighbors(nl);
+            R->volume.push_back(cell.volume());
+            fvert_all.push_back(std::move(fv));
+            fcoord_all.push_back(std::move(fc));
+            nlist_all.push_back(std::move(nl));
+        }
+    } while (clo.inc());
+    R->face_off.push_back(0);
+    R->vert_off.push_back(0);
+    for (size_t ci = 0; ci < R->id.size(); ++ci) {
+        const std::vector<int>& fv = fvert_all[ci];
+        const std::vector<double>& fc = fcoord_all[ci];
+        const std::vector<int>& nl = nlist_all[ci];
+        const double sx = R->site[3 * ci], sy = R->site[3 * ci + 1], sz = R->site[3 * ci + 2];
+        size_t it = 0;
+        int fi = 0;
+        while (it < fv.size()) {
+            int cnt = fv[it];
+            for (int k = 0; k < cnt; ++k) {
+                int ci2 = fv[it + 1 + k];
+                R->vxyz.push_back(fc[3 * ci2] + sx);
+                R->vxyz.push_back(fc[3 * ci2 + 1] + sy);
+                R->vxyz.push_back(fc[3 * ci2 + 2] + sz);
+            }
+            R->vert_off.push_back(R->vert_off.back() + cnt);
+            int nb = nl[fi];
+            R->face_nbr.push_back(nb >= 0 && nb <= max_id ? reverse[nb] : -1);
+            it += cnt + 1;
+            ++fi;
+        }
+        R->face_off.push_back(R->face_off.back() + fi);
+    }
+    for (long i = 0; i < n; ++i) {
+        double fx, fy, fz;
+        int sid;
+        bool found = con.find_voronoi_cell(x[i], y[i], z[i], fx, fy, fz, sid);
+        R->home.push_back((found && sid >= 0 && sid <= max_id) ? reverse[sid] : -1);
+    }
+    return max_id;
+}
+
+// Builds the cell geometry (tessellate) of the final point set (after buffer/Lloyd) -- taken from
+// run_point_set_stage on the same snapshot, as run_mapping_stage does.  With run_map, then runs
+// run_mapping_stage itself and keeps its per-cell rows (matched by site id to the geometry order).  With
+// run_map == 2, runs run_inverse_mapping_test_stage after it in the same work folder, as
+// `kiwi inverse-mapping-test` does, and returns instead the geometry that stage tessellated (from the point
+// set cached by the forward stage), with the cell masses it used and its per-particle results.
 void* ref_voronoi_build(long n, const double* x, const double* y, const double* z, const double* vx,
                         const double* vy, const double* vz, const double* m, const double* h,
                         const double bounds[6], int buffer_enabled, double spacing_fraction, int lloyd_iterations,
@@ -265,73 +344,8 @@ void* ref_voronoi_build(long n, const double* x, const double* y, const double* 
         c.lloyd.iterations = lloyd_iterations;
         if (threads > 0) omp_set_num_threads(threads);
         kiwi::PointSet pts = kiwi::run_point_set_stage(c);
-
-        const kiwi::Domain& d = c.domain;
-        voro::pre_container pcon(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, false, false, false);
-        for (size_t i = 0; i < pts.size(); ++i) pcon.put(pts.id[i], pts.x[i], pts.y[i], pts.z[i]);
-        int bx, by, bz;
-        kiwi::guess_scaled_blocks(pcon, c.grid_blocks.block_scale_factor, bx, by, bz);
-        voro::container con(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, bx, by, bz, false, false, false, 8);
-        pcon.setup(con);
-        int max_id = 0;
-        for (int pid : pts.id) max_id = std::max(max_id, pid);
-        std::vector<int> reverse(max_id + 1, -1);
-        std::vector<std::vector<int>> fvert_all, nlist_all;
-        std::vector<std::vector<double>> fcoord_all;
-        voro::voronoicell_neighbor cell;
-        voro::c_loop_all clo(con);
-        double px, py, pz;
-        if (clo.start()) do {
-            if (con.compute_cell(cell, clo)) {
-                int idx = static_cast<int>(R->id.size());
-                R->id.push_back(clo.pid());
-                reverse[clo.pid()] = idx;
-                clo.pos(px, py, pz);
-                R->site.push_back(px);
-                R->site.push_back(py);
-                R->site.push_back(pz);
-                std::vector<int> fv, nl;
-                std::vector<double> fc;
-                cell.face_vertices(fv);
-                cell.vertices(fc);
-                cell.neighbors(nl);
-                R->volume.push_back(cell.volume());
-                fvert_all.push_back(std::move(fv));
-                fcoord_all.push_back(std::move(fc));
-                nlist_all.push_back(std::move(nl));
-            }
-        } while (clo.inc());
-        R->face_off.push_back(0);
-        R->vert_off.push_back(0);
-        for (size_t ci = 0; ci < R->id.size(); ++ci) {
-            const std::vector<int>& fv = fvert_all[ci];
-            const std::vector<double>& fc = fcoord_all[ci];
-            const std::vector<int>& nl = nlist_all[ci];
-            const double sx = R->site[3 * ci], sy = R->site[3 * ci + 1], sz = R->site[3 * ci + 2];
-            size_t it = 0;
-            int fi = 0;
-            while (it < fv.size()) {
-                int cnt = fv[it];
-                for (int k = 0; k < cnt; ++k) {
-                    int ci2 = fv[it + 1 + k];
-                    R->vxyz.push_back(fc[3 * ci2] + sx);
-                    R->vxyz.push_back(fc[3 * ci2 + 1] + sy);
-                    R->vxyz.push_back(fc[3 * ci2 + 2] + sz);
-                }
-                R->vert_off.push_back(R->vert_off.back() + cnt);
-                int nb = nl[fi];
-                R->face_nbr.push_back(nb >= 0 && nb <= max_id ? reverse[nb] : -1);
-                it += cnt + 1;
-                ++fi;
-            }
-            R->face_off.push_back(R->face_off.back() + fi);
-        }
-        for (long i = 0; i < n; ++i) {
-            double fx, fy, fz;
-            int sid;
-            bool found = con.find_voronoi_cell(x[i], y[i], z[i], fx, fy, fz, sid);
-            R->home.push_back((found && sid >= 0 && sid <= max_id) ? reverse[sid] : -1);
-        }
+        std::vector<int> reverse;
+        int max_id = tessellate(c, pts, n, x, y, z, R, reverse);
         if (run_map) {
             // A fresh run of the stage in its own work folder, as `kiwi map` on an empty folder runs it:
             // it recomputes the point set and uses it in memory (reusing the cached point-set file above
@@ -351,6 +365,27 @@ void* ref_voronoi_build(long n, const double* x, const double* y, const double* 
                 R->vx[ci] = row.vx;
                 R->vy[ci] = row.vy;
                 R->vz[ci] = row.vz;
+            }
+            if (run_map == 2) {
+                kiwi::InverseMappingTestResult ir = kiwi::run_inverse_mapping_test_stage(cm);
+                kiwi::MappingResult cached = kiwi::run_mapping_stage(cm);       // the rows the stage read
+                kiwi::PointSet cached_pts = kiwi::run_point_set_stage(cm);      // the points it tessellated
+                auto* G = new RefVoronoi();
+                max_id = tessellate(cm, cached_pts, n, x, y, z, G, reverse);
+                G->inv_cell_mass.assign(G->id.size(), 0.0);
+                for (const auto& row : cached.cells) {
+                    if (row.id < 0 || row.id > max_id || reverse[row.id] < 0) continue;
+                    G->inv_cell_mass[reverse[row.id]] = row.density * row.volume;
+                }
+                for (const auto& p : ir.particles) {
+                    G->inv_recovered.push_back(p.m_recovered);
+                    G->inv_coverage.push_back(p.coverage_fraction);
+                }
+                G->inv_totals[0] = ir.total_original_mass;
+                G->inv_totals[1] = ir.total_grid_mass;
+                G->inv_totals[2] = ir.total_recovered_mass;
+                delete R;
+                R = G;
             }
         }
     } catch (const std::exception& e) {
@@ -392,6 +427,19 @@ void ref_voronoi_copy(void* h, int* id, double* site, double* volume, long* face
     cp(vz, R->vz);
 }
 
+// The inverse-mapping results of a run_map == 2 build: per particle recovered mass and coverage, the three
+// totals, and per cell the mass the stage used.
+void ref_voronoi_inverse_copy(void* h, double* recovered, double* coverage, double* totals3, double* cell_mass) {
+    auto* R = static_cast<RefVoronoi*>(h);
+    auto cp = [](double* dst, const std::vector<double>& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    cp(recovered, R->inv_recovered);
+    cp(coverage, R->inv_coverage);
+    cp(cell_mass, R->inv_cell_mass);
+    if (totals3) std::memcpy(totals3, R->inv_totals, sizeof(R->inv_totals));
+}
+
 void ref_voronoi_free(void* h) { delete static_cast<RefVoronoi*>(h); }
 
 // The reference's own stage-file writers (src/cartesian_grid.cpp:323-347, src/mapping.cpp:307-315).
@@ -414,6 +462,30 @@ int ref_save_cartesian_grid(const char* path, int nx, int ny, int nz, const doub
         g.vy.assign(vy, vy + n);
         g.vz.assign(vz, vz + n);
         kiwi::save_cartesian_grid(g, path);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// save_inverse_mapping_test (src/mapping.cpp:505-513).
+int ref_save_inverse_mapping_test(const char* path, long n, const long* id, const double* m_original,
+                                  const double* m_recovered, const double* coverage, const double* totals3) {
+    try {
+        kiwi::InverseMappingTestResult r;
+        r.total_original_mass = totals3[0];
+        r.total_grid_mass = totals3[1];
+        r.total_recovered_mass = totals3[2];
+        for (long i = 0; i < n; ++i) {
+            kiwi::InverseMappingTestRow row;
+            row.id = (int)id[i];
+            row.m_original = m_original[i];
+            row.m_recovered = m_recovered[i];
+            row.coverage_fraction = coverage[i];
+            r.particles.push_back(row);
+        }
+        kiwi::save_inverse_mapping_test(r, path);
         return 0;
     } catch (const std::exception& e) {
         g_err = e.what();

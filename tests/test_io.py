@@ -65,3 +65,44 @@ def test_grid_reader_errors(kiwi, tmp_path):
         kiwi.load_cartesian_grid(str(p))
     with pytest.raises(kiwi.KiwiError, match="could not open"):
         kiwi.load_cartesian_grid(str(tmp_path / "missing.bin"))
+
+
+def _inverse(kiwi, n=57, seed=3):
+    rng = np.random.default_rng(seed)
+    m = rng.uniform(0.001, 0.05, n)
+    rec = m * rng.uniform(0.0, 1.0 + 1e-9, n)
+    rec[::7] = 0.0
+    cov = np.where(m > 0, rec / m, 0.0)
+    r = kiwi.InverseMappingResult(m, rec, cov, float(m.sum()), float(rec.sum()) * (1 + 1e-12), float(rec.sum()))
+    return np.arange(1, n + 1, dtype=np.int64) * 3, r
+
+
+def test_inverse_mapping_file_equals_reference_writer(kiwi, reflib, tmp_path):
+    ids, r = _inverse(kiwi)
+    a, b = str(tmp_path / "a.dat"), str(tmp_path / "b.dat")
+    kiwi.save_inverse_mapping_test(a, ids, r)
+    reflib.save_inverse_mapping_test(b, ids, r.m_original, r.m_recovered, r.coverage,
+                                     [r.total_original_mass, r.total_grid_mass, r.total_recovered_mass])
+    assert open(a, "rb").read() == open(b, "rb").read()
+
+
+def test_inverse_mapping_file_round_trip_and_errors(kiwi, tmp_path):
+    ids, r = _inverse(kiwi)
+    p = str(tmp_path / "inv.dat")
+    kiwi.save_inverse_mapping_test(p, ids, r)
+    ids2, r2 = kiwi.load_inverse_mapping_test(p)
+    assert np.array_equal(ids2, ids)
+    for k in ("m_original", "m_recovered", "coverage"):
+        assert np.allclose(getattr(r2, k), getattr(r, k), rtol=1e-14, atol=0)  # 15 significant digits
+    with pytest.raises(kiwi.KiwiError, match="could not open inverse-mapping-test file"):
+        kiwi.load_inverse_mapping_test(str(tmp_path / "missing.dat"))
+    bad = tmp_path / "bad.dat"
+    bad.write_text("1 2 3\n")
+    with pytest.raises(kiwi.KiwiError, match="missing expected '#' totals header"):
+        kiwi.load_inverse_mapping_test(str(bad))
+    bad.write_text("# totals\nx y z\n")
+    with pytest.raises(kiwi.KiwiError, match="could not read totals line"):
+        kiwi.load_inverse_mapping_test(str(bad))
+    bad.write_text("# totals\n1 2 3\n")
+    with pytest.raises(kiwi.KiwiError, match="contained no particle rows"):
+        kiwi.load_inverse_mapping_test(str(bad))
