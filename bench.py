@@ -91,7 +91,10 @@ def parse():
     ap.add_argument("--adj-n", type=int, default=500_000, help="adjoint workload: particles")
     ap.add_argument("--adj-res", type=int, default=128, help="adjoint workload: grid cells per axis")
     ap.add_argument("--vor-n", type=int, default=200_000, help="voronoi workload: particles")
-    ap.add_argument("--workload", default="lognormal", choices=["lognormal", "batch", "adjoint", "voronoi"],
+    ap.add_argument("--cmap-n", type=int, default=1_000_000, help="cartesian_map workload: sites")
+    ap.add_argument("--cmap-res", type=int, default=256, help="cartesian_map workload: grid cells per axis")
+    ap.add_argument("--workload", default="lognormal",
+                    choices=["lognormal", "batch", "adjoint", "voronoi", "cartesian_map"],
                     help="batch: many column snapshots of log-uniform sizes on grids of log-uniform resolution, "
                          "kernels cycling M4 / M6 / WC4, in one persistent graph-recorded launch")
     ap.add_argument("--batch-items", type=int, default=64)
@@ -398,6 +401,70 @@ def run_voronoi(args):
     return 0
 
 
+def run_cartesian_map(args):
+    """Cartesian-map point location: --cmap-n column-recipe particle positions on a 5 pc cube as the sites
+    (seed 1003), a --cmap-res^3 grid; each cell centre takes its nearest site's values and id
+    (kiwi_cartesian_map: host arrays in and out).  `value` is cells located per second over the device time
+    of the binning and location kernels; the CPU baseline is the reference stage's own loop (one Voro++
+    container per OpenMP thread, find_voronoi_cell per cell) over a bounded sample of x-slabs, container
+    builds included, and the GPU's owners are checked against it there."""
+    import torch
+
+    import kiwi_b200
+    from kiwi_b200.workloads import column_snapshot
+    from oracle.oracle import load_ref
+
+    torch.cuda.set_device(0)
+    P, bounds = column_snapshot(n=args.cmap_n, seed=1003, box=(5.0, 5.0, 5.0))
+    xyz = np.stack([P["x"], P["y"], P["z"]], axis=1)
+    n = len(P["x"])
+    ids = np.arange(n, dtype=np.int32)
+    rng = np.random.default_rng(1)
+    vals = [rng.random(n) for _ in range(4)]
+    res = args.cmap_res
+    ctx = kiwi_b200.Context(0)
+    for _ in range(max(args.warmup, 1)):
+        m = kiwi_b200.cartesian_map(xyz, bounds, res, *vals, site_id=ids, ctx=ctx)
+    g_ms, t_ms, launches = [], [], 0
+    clocks = ClockSampler(0)
+    clocks.start()
+    for _ in range(args.steps):
+        m = kiwi_b200.cartesian_map(xyz, bounds, res, *vals, site_id=ids, ctx=ctx)
+        g_ms.append(m.stats["gather_ms"])
+        t_ms.append(m.stats["total_ms"])
+        launches += m.stats["launches"]
+    clk = clocks.stop()
+    nq = res ** 3
+    cpu, agree = None, None
+    ref = load_ref()
+    if ref is not None and not args.no_cpu_baseline:
+        threads = ref.max_threads()
+        slabs = max(1, res // 32)
+        i0 = res // 2 - slabs // 2
+        sec, rid, build = ref.locate_sample(xyz, ids, bounds, res, i0, i0 + slabs, threads=threads)
+        q = sec - build
+        whole = build + q * res / slabs  # the stage over the whole grid: one set of builds, every slab's queries
+        cpu = {"value": nq / whole, "unit": "cells/s", "cores": threads, "kind": "reference",
+               "sample": f"x-slabs {i0}..{i0 + slabs - 1} of {res} ({slabs * res * res} cells, through the filament): "
+                         f"{q:.2f} s of queries, scaled to the whole grid, plus {build:.2f} s of per-thread container "
+                         f"builds; sample rate {slabs * res * res / q:.4g} cells/s without the builds"}
+        gpu_ids = m.voronoi_cell_id.reshape(res, res, res)[i0:i0 + slabs].reshape(-1)
+        agree = {"cells_compared": int(rid.size), "owners_equal": int(np.sum(gpu_ids == rid))}
+    line = {
+        "metric": "cartesian-map cells located/s (nearest-site point location)", "value": nq / (np.mean(g_ms) * 1e-3),
+        "unit": "cells/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1),
+        "ms_per_step": float(np.mean(g_ms)), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{n} column-recipe sites, 5 pc cube, grid {res}^3", "sites": n, "cells": nq},
+        "gpu_launches": int(launches), "clocks": clk,
+        "e2e": {"value": nq / (np.mean(t_ms) * 1e-3), "unit": "cells/s", "ms_per_step": float(np.mean(t_ms)),
+                "h2d_bytes_per_step": int(n * (7 * 8 + 4)), "d2h_bytes_per_step": int(nq * (4 * 8 + 4))},
+        "cpu_baseline": cpu, "agreement_with_reference": agree,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """Batched sph-to-grid: args.batch_items column snapshots (item i seeded 5000 + i), N log-uniform in
     [nmin, nmax], grid res^3 with res log-uniform in [resmin, resmax], kernels cycling M4 / M6 / WC4; one
@@ -487,6 +554,8 @@ def main():
         return run_adjoint(args)
     if args.workload == "voronoi":
         return run_voronoi(args)
+    if args.workload == "cartesian_map":
+        return run_cartesian_map(args)
     ws, rank, local = dist_env()
     import torch
 

@@ -271,6 +271,13 @@ int kiwi_save_mapping(const char* path, int64_t n_cells, const int64_t* id, cons
                       const double* z, const double* volume, const double* density, const double* vx, const double* vy,
                       const double* vz, char* err, size_t err_len);
 
+/* save_cartesian_map / load_cartesian_map (src/cartesian_map.cpp:202-279): the VGTCMAP1 file of a cartesian
+ * map; the loader reads the header only when all five arrays are NULL. */
+int kiwi_save_cartesian_map(const char* path, int32_t res, const double* bounds6, const double* density,
+                            const double* vx, const double* vy, const double* vz, const int32_t* voronoi_cell_id,
+                            char* err, size_t err_len);
+int kiwi_load_cartesian_map(const char* path, int32_t* res, double* bounds6, double* density, double* vx, double* vy,
+                            double* vz, int32_t* voronoi_cell_id, char* err, size_t err_len);
 /* save_inverse_mapping_test (src/mapping.cpp:505-513): inverse-mapping-test.dat, a '#' header, the totals
  * (original, grid, recovered mass) and "id m_original m_recovered coverage_fraction" per particle, with 15
  * significant digits. */
@@ -313,6 +320,22 @@ int kiwi_inverse_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const
                              const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision,
                              const double* cell_mass, double* m_recovered, double* coverage, double* totals3,
                              double* density, KiwiStats* stats);
+
+/* ---- cartesian-map stage (run_cartesian_map_stage's point location, src/cartesian_map.cpp:84-200) ---- */
+/* Every cell centre of a resolution^3 grid over bounds6 takes the values of its nearest site (the Voronoi
+ * cell it lies in: container::find_voronoi_cell) and that site's id.  Sites (3 doubles each, host arrays)
+ * outside bounds6 are ignored, as the container drops them; site_id (may be NULL: the site index) gives the
+ * ids written to voronoi_cell_id; cell_density / cell_vx / cell_vy / cell_vz hold each site's mapping row and
+ * mapped (may be NULL: all) marks the sites that have one.  Outputs are host arrays of resolution^3 in the
+ * x-major order (ix*res + iy)*res + iz; cells with no site (no sites at all) keep 0 and id 0, cells whose
+ * site has no mapping row keep 0 with the site's id.  counts2 (may be NULL) receives those two counts (the
+ * reference's "unresolved" and "unmapped" warnings).  Exactly equidistant sites resolve to the smallest
+ * site index. */
+int kiwi_cartesian_map(KiwiCtx* ctx, int64_t n_sites, const double* site_xyz, const int32_t* site_id,
+                       const double* cell_density, const double* cell_vx, const double* cell_vy,
+                       const double* cell_vz, const uint8_t* mapped, const double* bounds6, int32_t resolution,
+                       double* density, double* vx, double* vy, double* vz, int32_t* voronoi_cell_id,
+                       int64_t* counts2, KiwiStats* stats);
 
 #ifdef __cplusplus
 }

@@ -570,6 +570,10 @@ def _io_lib():
                                                                                                    C.c_size_t]
     L.kiwi_load_cartesian_grid.argtypes = [C.c_char_p, C.POINTER(C.c_int32)] + [_dp] * 5 + [C.c_char_p, C.c_size_t]
     L.kiwi_save_mapping.argtypes = ([C.c_char_p, C.c_int64, _i64p] + [_dp] * 8 + [C.c_char_p, C.c_size_t])
+    L.kiwi_save_cartesian_map.argtypes = [C.c_char_p, C.c_int32, _dp, _dp, _dp, _dp, _dp, _i32p, C.c_char_p,
+                                          C.c_size_t]
+    L.kiwi_load_cartesian_map.argtypes = [C.c_char_p, C.POINTER(C.c_int32), _dp, _dp, _dp, _dp, _dp, _i32p,
+                                          C.c_char_p, C.c_size_t]
     L.kiwi_save_inverse_mapping_test.argtypes = ([C.c_char_p, C.c_int64, _i64p] + [_dp] * 4 +
                                                  [C.c_char_p, C.c_size_t])
     L.kiwi_load_inverse_mapping_test.argtypes = ([C.c_char_p, C.POINTER(C.c_int64), _dp, _i64p] + [_dp] * 3 +
@@ -724,6 +728,77 @@ def load_inverse_mapping_test(path: str):
     _io_check(L.kiwi_load_inverse_mapping_test(path.encode(), C.byref(n), _p(tot), ids.ctypes.data_as(_i64p),
                                                *[_p(a) for a in arrs], n.value, err, len(err)), err)
     return ids, InverseMappingResult(*arrs, float(tot[0]), float(tot[1]), float(tot[2]))
+
+
+@dataclass
+class CartesianMap:
+    """CartesianMap (include/kiwi/cartesian_map.hpp): a resolution^3 grid over the domain, each cell holding
+    the mapping values of the Voronoi cell its centre lies in and that cell's site id."""
+    resolution: int
+    bounds: tuple
+    density: np.ndarray
+    vx: np.ndarray
+    vy: np.ndarray
+    vz: np.ndarray
+    voronoi_cell_id: np.ndarray
+    stats: dict = field(default_factory=dict)
+
+
+def cartesian_map(sites, bounds, resolution, cell_density, cell_vx, cell_vy, cell_vz, site_id=None, mapped=None,
+                  ctx=None) -> CartesianMap:
+    """run_cartesian_map_stage's point location (src/cartesian_map.cpp:84-200) on the GPU: `sites` (n, 3)
+    the point set, `cell_*` each site's mapping row, `site_id` the ids written to voronoi_cell_id (default:
+    the site index), `mapped` which sites have a mapping row (default: all)."""
+    ctx = ctx or default_context()
+    xyz = _f64(np.asarray(sites, dtype=np.float64).reshape(-1, 3))
+    n = xyz.shape[0]
+    vals = [_f64(v) for v in (cell_density, cell_vx, cell_vy, cell_vz)]
+    sid = np.ascontiguousarray(site_id, dtype=np.int32) if site_id is not None else None
+    mp = np.ascontiguousarray(mapped, dtype=np.uint8) if mapped is not None else None
+    b = _f64(bounds)
+    res = int(resolution)
+    nq = res ** 3 if res > 0 else 0
+    outs = [np.empty(nq) for _ in range(4)]
+    cid = np.empty(nq, dtype=np.int32)
+    counts = np.zeros(2, dtype=np.int64)
+    st = KiwiStats()
+    f = ctx._L.kiwi_cartesian_map
+    f.argtypes = [C.c_void_p, C.c_int64, _dp, _i32p, _dp, _dp, _dp, _dp, C.POINTER(C.c_uint8), _dp, C.c_int32,
+                  _dp, _dp, _dp, _dp, _i32p, _i64p, C.POINTER(KiwiStats)]
+    ctx.check(f(ctx.handle, n, _p(xyz), sid.ctypes.data_as(_i32p) if sid is not None else None, *[_p(v) for v in vals],
+                mp.ctypes.data_as(C.POINTER(C.c_uint8)) if mp is not None else None, _p(b), res,
+                *[_p(o) for o in outs], cid.ctypes.data_as(_i32p), counts.ctypes.data_as(_i64p), C.byref(st)),
+              "cartesian_map")
+    d = st.as_dict()
+    d["unresolved"], d["unmapped"] = int(counts[0]), int(counts[1])
+    return CartesianMap(res, tuple(float(v) for v in b), *outs, cid, stats=d)
+
+
+def save_cartesian_map(m: CartesianMap, path: str):
+    """save_cartesian_map (src/cartesian_map.cpp:202-229): the VGTCMAP1 file."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    b = _f64(m.bounds)
+    arrs = [_f64(a) for a in (m.density, m.vx, m.vy, m.vz)]
+    cid = np.ascontiguousarray(m.voronoi_cell_id, dtype=np.int32)
+    _io_check(L.kiwi_save_cartesian_map(path.encode(), m.resolution, _p(b), *[_p(a) for a in arrs],
+                                        cid.ctypes.data_as(_i32p), err, len(err)), err)
+
+
+def load_cartesian_map(path: str) -> CartesianMap:
+    """load_cartesian_map (src/cartesian_map.cpp:231-277)."""
+    L = _io_lib()
+    err = C.create_string_buffer(512)
+    r = C.c_int32(0)
+    b = np.zeros(6)
+    _io_check(L.kiwi_load_cartesian_map(path.encode(), C.byref(r), _p(b), None, None, None, None, None, err, len(err)),
+              err)
+    nq = r.value ** 3
+    arrs = [np.empty(nq) for _ in range(4)]
+    cid = np.empty(nq, dtype=np.int32)
+    _io_check(L.kiwi_load_cartesian_map(path.encode(), C.byref(r), _p(b), *[_p(a) for a in arrs],
+                                        cid.ctypes.data_as(_i32p), err, len(err)), err)
+    return CartesianMap(r.value, tuple(b), *arrs, cid)
 
 
 def version() -> str:

@@ -33,6 +33,7 @@ UNITS = [
     ("batch.cu", ["--fmad=false"]),
     ("io.cu", []),
     ("tabulated.cu", ["--fmad=false"]),
+    ("cartmap.cu", ["--fmad=false"]),
 ]
 
 

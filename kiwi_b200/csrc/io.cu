@@ -6,6 +6,8 @@
 //   doubles each in the x-major cell order, all in the machine's (little-endian) byte order.
 //   mapping.dat (src/mapping.cpp:307-315): one line per cell, "id x y z volume density vx vy vz", the
 //   numbers printed by an ostream with precision 15.
+//   cartesian_map.dat (src/cartesian_map.cpp:202-279): the 8 bytes "VGTCMAP1", int32 resolution, six doubles
+//   of domain bounds, density, vx, vy, vz as res^3 doubles each and the Voronoi cell ids as res^3 int32.
 //   inverse-mapping-test.dat (src/mapping.cpp:505-538): a '#' header line, the three totals, then one line
 //   per particle, "id m_original m_recovered coverage_fraction", precision 15.
 #include <cstdint>
@@ -20,6 +22,7 @@
 namespace {
 
 const char kGridMagic[8] = {'V', 'G', 'T', 'C', 'G', 'R', 'D', '2'};
+const char kMapMagic[8] = {'V', 'G', 'T', 'C', 'M', 'A', 'P', '1'};
 
 int io_err(char* err, size_t len, int code, const std::string& what) {
     if (err && len > 0) std::snprintf(err, len, "%s", what.c_str());
@@ -93,6 +96,52 @@ int kiwi_save_mapping(const char* path, int64_t n_cells, const int64_t* id, cons
         f << id[c] << " " << x[c] << " " << y[c] << " " << z[c] << " " << volume[c] << " " << density[c] << " "
           << vx[c] << " " << vy[c] << " " << vz[c] << "\n";
     if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("failed writing mapping file: ") + path);
+    return KIWI_OK;
+}
+
+int kiwi_save_cartesian_map(const char* path, int32_t res, const double* bounds6, const double* density,
+                            const double* vx, const double* vy, const double* vz, const int32_t* voronoi_cell_id,
+                            char* err, size_t err_len) {
+    if (!path || res <= 0 || !bounds6 || !density || !vx || !vy || !vz || !voronoi_cell_id)
+        return io_err(err, err_len, KIWI_ERR_ARG, "save_cartesian_map: a null argument");
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("could not open output file: ") + path);
+    f.write(kMapMagic, sizeof(kMapMagic));
+    f.write(reinterpret_cast<const char*>(&res), sizeof(res));
+    f.write(reinterpret_cast<const char*>(bounds6), 6 * sizeof(double));
+    const std::streamsize n = (std::streamsize)((size_t)res * res * res);
+    for (const double* a : {density, vx, vy, vz}) f.write(reinterpret_cast<const char*>(a), n * (std::streamsize)sizeof(double));
+    f.write(reinterpret_cast<const char*>(voronoi_cell_id), n * (std::streamsize)sizeof(int32_t));
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("failed writing output file (disk full?): ") + path);
+    return KIWI_OK;
+}
+
+int kiwi_load_cartesian_map(const char* path, int32_t* res, double* bounds6, double* density, double* vx, double* vy,
+                            double* vz, int32_t* voronoi_cell_id, char* err, size_t err_len) {
+    if (!path || !res) return io_err(err, err_len, KIWI_ERR_ARG, "load_cartesian_map: a null argument");
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("could not open cartesian map file: ") + path);
+    char magic[8];
+    f.read(magic, sizeof(magic));
+    if (!f || std::memcmp(magic, kMapMagic, sizeof(magic)) != 0)
+        return io_err(err, err_len, KIWI_ERR_ARG,
+                      std::string("cartesian map file has an unrecognized header (wrong format or corrupt): ") + path);
+    int32_t r = 0;
+    f.read(reinterpret_cast<char*>(&r), sizeof(r));
+    if (!f || r <= 0)
+        return io_err(err, err_len, KIWI_ERR_ARG, std::string("cartesian map file has an invalid resolution: ") + path);
+    double b[6];
+    f.read(reinterpret_cast<char*>(b), sizeof(b));
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("cartesian map file is truncated (domain bounds): ") + path);
+    *res = r;
+    if (bounds6) std::memcpy(bounds6, b, sizeof(b));
+    if (!density && !vx && !vy && !vz && !voronoi_cell_id) return KIWI_OK;  // header only
+    if (!density || !vx || !vy || !vz || !voronoi_cell_id)
+        return io_err(err, err_len, KIWI_ERR_ARG, "load_cartesian_map: give all five arrays or none");
+    const std::streamsize n = (std::streamsize)((size_t)r * r * r);
+    for (double* a : {density, vx, vy, vz}) f.read(reinterpret_cast<char*>(a), n * (std::streamsize)sizeof(double));
+    f.read(reinterpret_cast<char*>(voronoi_cell_id), n * (std::streamsize)sizeof(int32_t));
+    if (!f) return io_err(err, err_len, KIWI_ERR_ARG, std::string("cartesian map file is truncated/corrupt: ") + path);
     return KIWI_OK;
 }
 

@@ -69,6 +69,9 @@ class Oracle:
         L.or_inverse_map.restype = C.c_int
         L.or_inverse_map.argtypes = ([C.c_int64, _i32p] + [_dp] * 8 + [C.c_int64, _i64p, _i64p, _dp, _i32p, _dp,
                                                                        C.c_int, C.c_double, C.c_int] + [_dp] * 3)
+        L.or_cartesian_map_nearest = getattr(L, pfx + "cartesian_map_nearest")
+        L.or_cartesian_map_nearest.restype = C.c_int
+        L.or_cartesian_map_nearest.argtypes = [C.c_int64, _dp, _dp, C.c_int, _i32p]
         for name in ("table_load", "table_reset", "table_values"):
             setattr(L, "or_" + name, getattr(L, pfx + name))
         L.or_table_load.restype = C.c_int
@@ -108,6 +111,13 @@ class Oracle:
                                 fn.ctypes.data_as(_i32p), _d(vol), kernel, support_in_h, int(tabulated), _d(cm),
                                 _d(rec), _d(cov))
         return rec, cov
+
+    def cartesian_map_nearest(self, sites, bounds, res):
+        """Nearest site index of every cell centre of the res^3 grid (-1 without sites), brute force."""
+        xyz = _f64(np.asarray(sites, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros(res ** 3, dtype=np.int32)
+        self.lib.or_cartesian_map_nearest(xyz.shape[0], _d(xyz), _d(_f64(bounds)), res, out.ctypes.data_as(_i32p))
+        return out
 
     def table_load(self, path) -> int:
         """load_density_table restated: 0, or -1 / -2 / -3 (cannot open / header malformed / truncated)."""
@@ -220,6 +230,53 @@ class RefLib:
         L.ref_table_load_gridded.argtypes = [C.c_char_p, C.c_int64] + [_dp] * 5
         L.ref_table_values.restype = C.c_int64
         L.ref_table_values.argtypes = [_dp]
+
+    def cartesian_map(self, P, bounds, resolution, threads=1):
+        """run_cartesian_map_stage on a fresh work folder: (points {id, xyz}, mapping rows {id, density, vx,
+        vy, vz}, map {density, vx, vy, vz, cell_id})."""
+        L = self.lib
+        L.ref_cartesian_map.restype = C.c_void_p
+        L.ref_cartesian_map.argtypes = [C.c_long] + [_dp] * 8 + [_dp, C.c_int, C.c_int]
+        L.ref_cartesian_map_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_long)]
+        L.ref_cartesian_map_copy.argtypes = [C.c_void_p, _ip, _dp, _ip] + [_dp] * 8 + [_ip]
+        L.ref_cartesian_map_free.argtypes = [C.c_void_p]
+        arrs = [_f64(P[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")]
+        hnd = L.ref_cartesian_map(len(arrs[0]), *[_d(a) for a in arrs], _d(_f64(bounds)), int(resolution), threads)
+        if not hnd:
+            raise RuntimeError("reference cartesian map failed: " + L.ref_last_error().decode())
+        sz = (C.c_long * 3)()
+        L.ref_cartesian_map_sizes(hnd, sz)
+        npt, nrow, nq = sz[0], sz[1], sz[2]
+        pts = {"id": np.zeros(npt, np.int32), "xyz": np.zeros(3 * npt)}
+        rows = {"id": np.zeros(nrow, np.int32), **{k: np.zeros(nrow) for k in ("density", "vx", "vy", "vz")}}
+        mp = {**{k: np.zeros(nq) for k in ("density", "vx", "vy", "vz")}, "cell_id": np.zeros(nq, np.int32)}
+        L.ref_cartesian_map_copy(hnd, pts["id"].ctypes.data_as(_ip), _d(pts["xyz"]), rows["id"].ctypes.data_as(_ip),
+                                 *[_d(rows[k]) for k in ("density", "vx", "vy", "vz")],
+                                 *[_d(mp[k]) for k in ("density", "vx", "vy", "vz")], mp["cell_id"].ctypes.data_as(_ip))
+        L.ref_cartesian_map_free(hnd)
+        return pts, rows, mp
+
+    def locate_sample(self, xyz, ids, bounds, res, ix_begin, ix_end, threads=0):
+        """The stage's point location over x-slabs [ix_begin, ix_end): (seconds, owning site id per cell,
+        seconds of it spent building the per-thread containers)."""
+        f = self.lib.ref_locate_sample
+        f.restype = C.c_double
+        f.argtypes = [C.c_long, _ip, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _ip, _dp]
+        xyz = _f64(np.asarray(xyz, dtype=np.float64).reshape(-1))
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        out = np.zeros((ix_end - ix_begin) * res * res, dtype=np.int32)
+        build = C.c_double(0.0)
+        sec = f(len(ids), ids.ctypes.data_as(_ip), _d(xyz), _d(_f64(bounds)), int(res), int(ix_begin), int(ix_end),
+                int(threads), out.ctypes.data_as(_ip), C.byref(build))
+        return sec, out, build.value
+
+    def save_cartesian_map(self, path, res, bounds, density, vx, vy, vz, cell_id):
+        f = self.lib.ref_save_cartesian_map
+        f.argtypes = [C.c_char_p, C.c_int] + [_dp] * 5 + [_ip]
+        cid = np.ascontiguousarray(cell_id, dtype=np.int32)
+        if f(path.encode(), int(res), *[_d(_f64(a)) for a in (bounds, density, vx, vy, vz)],
+             cid.ctypes.data_as(_ip)) != 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
 
     def table_load_gridded(self, path, h, phi, r0, R0):
         """load_density_table(path), then gridded_integral with that table over the arrays (RuntimeError

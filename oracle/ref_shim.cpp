@@ -25,6 +25,7 @@
 #include "kiwi/kernel_integral_generic.hpp"
 #include "kiwi/kernel_integrator.hpp"
 #include "kiwi/kernel_spec.hpp"
+#include "kiwi/cartesian_map.hpp"
 #include "kiwi/mapping.hpp"
 #include "kiwi/point_set.hpp"
 #include "kiwi/voro_grid.hpp"
@@ -396,6 +397,170 @@ void* ref_voronoi_build(long n, const double* x, const double* y, const double* 
     }
     rm_rf(dir);
     return R;
+}
+
+// run_cartesian_map_stage (src/cartesian_map.cpp:84-200) on a fresh work folder, plus the point set and the
+// mapping rows it used, each recomputed the same way in a fresh folder of its own (they are deterministic;
+// reading them back from the stage's cache files would give their 15-digit rounded copies).  The stage
+// locates against the point set it computed in memory, and its mapping stage tessellates the point set
+// as cached by then.
+struct RefCartMap {
+    std::vector<int> pt_id;
+    std::vector<double> pt_xyz;
+    std::vector<int> row_id;
+    std::vector<double> row_density, row_vx, row_vy, row_vz;
+    std::vector<double> density, vx, vy, vz;
+    std::vector<int> cell_id;
+};
+
+void* ref_cartesian_map(long n, const double* x, const double* y, const double* z, const double* vx,
+                        const double* vy, const double* vz, const double* m, const double* h,
+                        const double bounds[6], int resolution, int threads) {
+    std::string dir = make_tmpdir();
+    auto* R = new RefCartMap();
+    try {
+        write_snapshot(dir + "/snap.txt", n, x, y, z, vx, vy, vz, m, h);
+        kiwi::Config c = base_config(dir, bounds, "cubic_spline", 0.0, 0);
+        c.buffer.enabled = false;
+        c.lloyd.iterations = 0;
+        c.cartesian_map.resolution = resolution;
+        if (threads > 0) omp_set_num_threads(threads);
+        kiwi::Config c1 = c, c2 = c, c3 = c;
+        c1.work_folder = dir + "/runs_points";
+        c2.work_folder = dir + "/runs_mapping";
+        c3.work_folder = dir + "/runs_cmap";
+        kiwi::PointSet pts = kiwi::run_point_set_stage(c1);
+        for (size_t i = 0; i < pts.size(); ++i) {
+            R->pt_id.push_back(pts.id[i]);
+            R->pt_xyz.push_back(pts.x[i]);
+            R->pt_xyz.push_back(pts.y[i]);
+            R->pt_xyz.push_back(pts.z[i]);
+        }
+        // as inside the stage: the point-set stage runs (and caches its points) first, so the mapping stage
+        // tessellates the cached points
+        kiwi::run_point_set_stage(c2);
+        kiwi::MappingResult mr = kiwi::run_mapping_stage(c2);
+        for (const auto& row : mr.cells) {
+            R->row_id.push_back(row.id);
+            R->row_density.push_back(row.density);
+            R->row_vx.push_back(row.vx);
+            R->row_vy.push_back(row.vy);
+            R->row_vz.push_back(row.vz);
+        }
+        kiwi::CartesianMap cm = kiwi::run_cartesian_map_stage(c3);
+        R->density = cm.density;
+        R->vx = cm.vx;
+        R->vy = cm.vy;
+        R->vz = cm.vz;
+        R->cell_id.assign(cm.voronoi_cell_id.begin(), cm.voronoi_cell_id.end());
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        rm_rf(dir);
+        delete R;
+        return nullptr;
+    }
+    rm_rf(dir);
+    return R;
+}
+
+// Sizes: [points, mapping rows, grid cells]
+void ref_cartesian_map_sizes(void* h, long* out3) {
+    auto* R = static_cast<RefCartMap*>(h);
+    out3[0] = (long)R->pt_id.size();
+    out3[1] = (long)R->row_id.size();
+    out3[2] = (long)R->cell_id.size();
+}
+
+void ref_cartesian_map_copy(void* h, int* pt_id, double* pt_xyz, int* row_id, double* row_density, double* row_vx,
+                            double* row_vy, double* row_vz, double* density, double* vx, double* vy, double* vz,
+                            int* cell_id) {
+    auto* R = static_cast<RefCartMap*>(h);
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(pt_id, R->pt_id);
+    cp(pt_xyz, R->pt_xyz);
+    cp(row_id, R->row_id);
+    cp(row_density, R->row_density);
+    cp(row_vx, R->row_vx);
+    cp(row_vy, R->row_vy);
+    cp(row_vz, R->row_vz);
+    cp(density, R->density);
+    cp(vx, R->vx);
+    cp(vy, R->vy);
+    cp(vz, R->vz);
+    cp(cell_id, R->cell_id);
+}
+
+void ref_cartesian_map_free(void* h) { delete static_cast<RefCartMap*>(h); }
+
+// The cartesian-map stage's point location over the x-slabs [ix_begin, ix_end) of a res^3 grid, as the
+// stage runs it (src/cartesian_map.cpp:146-184: one Voro++ container per OpenMP thread, collapse(2) over
+// ix, iy): the owning site id per cell into out_ids, and the wall time in seconds, container builds
+// included (*build_s, if given, receives the container builds' share).  The CPU baseline of the GPU point
+// location.
+double ref_locate_sample(long n_sites, const int* ids, const double* xyz, const double b[6], int res, int ix_begin,
+                         int ix_end, int threads, int* out_ids, double* build_s) {
+    kiwi::Config c;
+    c.domain.x_min = b[0]; c.domain.x_max = b[1];
+    c.domain.y_min = b[2]; c.domain.y_max = b[3];
+    c.domain.z_min = b[4]; c.domain.z_max = b[5];
+    if (threads > 0) omp_set_num_threads(threads);
+    const double t0 = omp_get_wtime();
+    const int nt = omp_get_max_threads();
+    std::vector<std::unique_ptr<voro::container>> cons(nt);
+    const kiwi::Domain& d = c.domain;
+#pragma omp parallel for
+    for (int t = 0; t < nt; ++t) {
+        voro::pre_container pcon(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, false, false, false);
+        for (long i = 0; i < n_sites; ++i) pcon.put(ids[i], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        int bx, by, bz;
+        kiwi::guess_scaled_blocks(pcon, c.grid_blocks.block_scale_factor, bx, by, bz);
+        cons[t] = std::make_unique<voro::container>(d.x_min, d.x_max, d.y_min, d.y_max, d.z_min, d.z_max, bx, by, bz,
+                                                    false, false, false, 8);
+        pcon.setup(*cons[t]);
+    }
+    if (build_s) *build_s = omp_get_wtime() - t0;
+    const double dpx = (d.x_max - d.x_min) / res, dpy = (d.y_max - d.y_min) / res, dpz = (d.z_max - d.z_min) / res;
+#pragma omp parallel for collapse(2) schedule(dynamic)
+    for (int ix = ix_begin; ix < ix_end; ++ix) {
+        for (int iy = 0; iy < res; ++iy) {
+            voro::container& con = *cons[omp_get_thread_num()];
+            const double x = d.x_min + (ix + 0.5) * dpx;
+            const double y = d.y_min + (iy + 0.5) * dpy;
+            for (int iz = 0; iz < res; ++iz) {
+                const double z = d.z_min + (iz + 0.5) * dpz;
+                double rx, ry, rz;
+                int pid = 0;
+                if (!con.find_voronoi_cell(x, y, z, rx, ry, rz, pid)) pid = 0;
+                out_ids[((size_t)(ix - ix_begin) * res + iy) * res + iz] = pid;
+            }
+        }
+    }
+    return omp_get_wtime() - t0;
+}
+
+// save_cartesian_map (src/cartesian_map.cpp:202-229).
+int ref_save_cartesian_map(const char* path, int res, const double* b, const double* density, const double* vx,
+                           const double* vy, const double* vz, const int* cell_id) {
+    try {
+        kiwi::CartesianMap cm;
+        cm.resolution = res;
+        cm.domain.x_min = b[0]; cm.domain.x_max = b[1];
+        cm.domain.y_min = b[2]; cm.domain.y_max = b[3];
+        cm.domain.z_min = b[4]; cm.domain.z_max = b[5];
+        const size_t nq = (size_t)res * res * res;
+        cm.density.assign(density, density + nq);
+        cm.vx.assign(vx, vx + nq);
+        cm.vy.assign(vy, vy + nq);
+        cm.vz.assign(vz, vz + nq);
+        cm.voronoi_cell_id.assign(cell_id, cell_id + nq);
+        kiwi::save_cartesian_map(cm, path);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
 }
 
 // Sizes: [n_cells, n_faces, n_vertices, n_particles]

@@ -106,3 +106,41 @@ def test_inverse_mapping_file_round_trip_and_errors(kiwi, tmp_path):
     bad.write_text("# totals\n1 2 3\n")
     with pytest.raises(kiwi.KiwiError, match="contained no particle rows"):
         kiwi.load_inverse_mapping_test(str(bad))
+
+
+def _cmap(kiwi, res=5, seed=4):
+    rng = np.random.default_rng(seed)
+    nq = res ** 3
+    return kiwi.CartesianMap(res, (-1.0, 2.0, 0.5, 3.5, 1.0, 4.0), rng.random(nq), rng.normal(size=nq),
+                             rng.normal(size=nq), rng.normal(size=nq), rng.integers(0, 1000, nq).astype(np.int32))
+
+
+def test_cartesian_map_file_equals_reference_writer(kiwi, reflib, tmp_path):
+    m = _cmap(kiwi)
+    a, b = str(tmp_path / "a.dat"), str(tmp_path / "b.dat")
+    kiwi.save_cartesian_map(m, a)
+    reflib.save_cartesian_map(b, m.resolution, m.bounds, m.density, m.vx, m.vy, m.vz, m.voronoi_cell_id)
+    assert open(a, "rb").read() == open(b, "rb").read()
+
+
+def test_cartesian_map_file_round_trip_and_errors(kiwi, tmp_path):
+    m = _cmap(kiwi)
+    p = str(tmp_path / "m.dat")
+    kiwi.save_cartesian_map(m, p)
+    r = kiwi.load_cartesian_map(p)
+    assert r.resolution == m.resolution and r.bounds == m.bounds
+    for k in ("density", "vx", "vy", "vz", "voronoi_cell_id"):
+        assert np.array_equal(getattr(r, k), getattr(m, k)), k
+    with pytest.raises(kiwi.KiwiError, match="could not open cartesian map file"):
+        kiwi.load_cartesian_map(str(tmp_path / "missing.dat"))
+    bad = tmp_path / "bad.dat"
+    bad.write_bytes(b"VGTCGRD2" + struct.pack("<i", 5))
+    with pytest.raises(kiwi.KiwiError, match="unrecognized header"):
+        kiwi.load_cartesian_map(str(bad))
+    bad.write_bytes(b"VGTCMAP1" + struct.pack("<i", 0))
+    with pytest.raises(kiwi.KiwiError, match="invalid resolution"):
+        kiwi.load_cartesian_map(str(bad))
+    raw = open(p, "rb").read()
+    bad.write_bytes(raw[:-9])
+    with pytest.raises(kiwi.KiwiError, match="truncated"):
+        kiwi.load_cartesian_map(str(bad))
