@@ -321,6 +321,22 @@ int kiwi_inverse_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const
                              const double* cell_mass, double* m_recovered, double* coverage, double* totals3,
                              double* density, KiwiStats* stats);
 
+/* ---- point-set stage (src/point_set.cpp) ------------------------------------------------------ */
+/* The candidate lattice of the coverage-grid buffer (generate_cartesian_lattice, src/point_set.cpp:166-195):
+ * spacing = spacing_fraction x the smallest extent, round(extent / spacing) (at least 1) cell-centred
+ * candidates per axis; returns their count (-1 on bad arguments), dims3 (may be NULL) the per-axis counts.
+ * Host only. */
+int64_t kiwi_coverage_grid_candidates(const double* bounds6, double spacing_fraction, int32_t* dims3);
+/* add_coverage_grid_buffer (src/point_set.cpp:198-262): the lattice candidates that no particle covers
+ * (squared distance <= (coverage_radius_factor x h_i)^2), in lattice order, with ids n + 1, n + 2, ...
+ * (host arrays).  *n_added receives their count; with all four outputs NULL only the count is computed,
+ * else they must hold capacity >= *n_added points.  KIWI_ERR_ARG with the reference's message if every
+ * h <= 0. */
+int kiwi_coverage_grid_buffer(KiwiCtx* ctx, int64_t n, const double* x, const double* y, const double* z,
+                              const double* h, const double* bounds6, double spacing_fraction,
+                              double coverage_radius_factor, int64_t capacity, double* out_x, double* out_y,
+                              double* out_z, int32_t* out_id, int64_t* n_added);
+
 /* ---- cartesian-map stage (run_cartesian_map_stage's point location, src/cartesian_map.cpp:84-200) ---- */
 /* Every cell centre of a resolution^3 grid over bounds6 takes the values of its nearest site (the Voronoi
  * cell it lies in: container::find_voronoi_cell) and that site's id.  Sites (3 doubles each, host arrays)

@@ -801,6 +801,32 @@ def load_cartesian_map(path: str) -> CartesianMap:
     return CartesianMap(r.value, tuple(b), *arrs, cid)
 
 
+def coverage_grid_buffer(particles: dict, bounds, spacing_fraction=0.05, coverage_radius_factor=2.0, ctx=None):
+    """add_coverage_grid_buffer (src/point_set.cpp:198-262) on the GPU: the cell-centred lattice candidates
+    no particle's sphere of radius coverage_radius_factor x h reaches, in lattice order, ids from n + 1.
+    `particles` holds x y z h.  Returns (xyz (k, 3), ids (k,))."""
+    ctx = ctx or default_context()
+    L = ctx._L
+    L.kiwi_coverage_grid_candidates.restype = C.c_int64
+    L.kiwi_coverage_grid_candidates.argtypes = [_dp, C.c_double, _i32p]
+    L.kiwi_coverage_grid_buffer.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                                            C.c_int64, _dp, _dp, _dp, _i32p, _i64p]
+    b = _f64(bounds)
+    cap = L.kiwi_coverage_grid_candidates(_p(b), float(spacing_fraction), None)
+    if cap < 0:
+        raise KiwiError(-1, "coverage buffer: bad domain or spacing_fraction")
+    a = [_f64(particles[k]) for k in ("x", "y", "z", "h")]
+    n = len(a[0])
+    out = [np.empty(max(cap, 1)) for _ in range(3)]
+    ids = np.empty(max(cap, 1), dtype=np.int32)
+    na = C.c_int64(0)
+    ctx.check(L.kiwi_coverage_grid_buffer(ctx.handle, n, *[_p(v) for v in a], _p(b), float(spacing_fraction),
+                                          float(coverage_radius_factor), cap, *[_p(o) for o in out],
+                                          ids.ctypes.data_as(_i32p), C.byref(na)), "coverage buffer")
+    k = na.value
+    return np.stack([o[:k] for o in out], axis=1), ids[:k].copy()
+
+
 def version() -> str:
     return load_library().kiwi_version().decode()
 

@@ -34,6 +34,7 @@ UNITS = [
     ("io.cu", []),
     ("tabulated.cu", ["--fmad=false"]),
     ("cartmap.cu", ["--fmad=false"]),
+    ("pointset.cu", ["--fmad=false"]),
 ]
 
 

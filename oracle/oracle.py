@@ -69,6 +69,9 @@ class Oracle:
         L.or_inverse_map.restype = C.c_int
         L.or_inverse_map.argtypes = ([C.c_int64, _i32p] + [_dp] * 8 + [C.c_int64, _i64p, _i64p, _dp, _i32p, _dp,
                                                                        C.c_int, C.c_double, C.c_int] + [_dp] * 3)
+        L.or_coverage_grid_buffer = getattr(L, pfx + "coverage_grid_buffer")
+        L.or_coverage_grid_buffer.restype = C.c_int64
+        L.or_coverage_grid_buffer.argtypes = [C.c_int64] + [_dp] * 5 + [C.c_double, C.c_double, _dp, _i32p]
         L.or_cartesian_map_nearest = getattr(L, pfx + "cartesian_map_nearest")
         L.or_cartesian_map_nearest.restype = C.c_int
         L.or_cartesian_map_nearest.argtypes = [C.c_int64, _dp, _dp, C.c_int, _i32p]
@@ -111,6 +114,21 @@ class Oracle:
                                 fn.ctypes.data_as(_i32p), _d(vol), kernel, support_in_h, int(tabulated), _d(cm),
                                 _d(rec), _d(cov))
         return rec, cov
+
+    def coverage_grid_buffer(self, P, bounds, spacing_fraction=0.05, factor=2.0):
+        """add_coverage_grid_buffer by brute force: (xyz (k, 3), ids (k,)), or None if every h <= 0."""
+        a = [_f64(P[k]) for k in ("x", "y", "z", "h")]
+        b = _f64(bounds)
+        ex, ey, ez = b[1] - b[0], b[3] - b[2], b[5] - b[4]
+        sp = spacing_fraction * min(ex, ey, ez)
+        cap = max(1, int(round(ex / sp))) * max(1, int(round(ey / sp))) * max(1, int(round(ez / sp)))
+        xyz = np.zeros(3 * cap)
+        ids = np.zeros(cap, dtype=np.int32)
+        k = self.lib.or_coverage_grid_buffer(len(a[0]), *[_d(v) for v in a], _d(b), spacing_fraction, factor, _d(xyz),
+                                             ids.ctypes.data_as(_i32p))
+        if k < 0:
+            return None
+        return xyz[:3 * k].reshape(-1, 3), ids[:k]
 
     def cartesian_map_nearest(self, sites, bounds, res):
         """Nearest site index of every cell centre of the res^3 grid (-1 without sites), brute force."""
@@ -255,6 +273,22 @@ class RefLib:
                                  *[_d(mp[k]) for k in ("density", "vx", "vy", "vz")], mp["cell_id"].ctypes.data_as(_ip))
         L.ref_cartesian_map_free(hnd)
         return pts, rows, mp
+
+    def coverage_grid_buffer(self, P, bounds, spacing_fraction=0.05, factor=2.0):
+        """The reference's add_coverage_grid_buffer on the particles as the point set: the appended points,
+        (xyz (k, 3), ids (k,)) (RuntimeError with its message when it throws)."""
+        f = self.lib.ref_coverage_grid_buffer
+        f.restype = C.c_long
+        f.argtypes = [C.c_long] + [_dp] * 5 + [C.c_double, C.c_double, _dp, _ip, C.c_long]
+        a = [_f64(P[k]) for k in ("x", "y", "z", "h")]
+        cap = 1 << 22
+        xyz = np.zeros(3 * cap)
+        ids = np.zeros(cap, dtype=np.int32)
+        k = f(len(a[0]), *[_d(v) for v in a], _d(_f64(bounds)), spacing_fraction, factor, _d(xyz),
+              ids.ctypes.data_as(_ip), cap)
+        if k < 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return xyz[:3 * k].reshape(-1, 3).copy(), ids[:k].copy()
 
     def locate_sample(self, xyz, ids, bounds, res, ix_begin, ix_end, threads=0):
         """The stage's point location over x-slabs [ix_begin, ix_end): (seconds, owning site id per cell,

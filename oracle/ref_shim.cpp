@@ -540,6 +540,37 @@ double ref_locate_sample(long n_sites, const int* ids, const double* xyz, const 
     return omp_get_wtime() - t0;
 }
 
+// add_coverage_grid_buffer (src/point_set.cpp:198-262) on the particles as the point set (ids 1..n): the
+// appended points and their ids; the count, or -1 with the reference's message.
+long ref_coverage_grid_buffer(long n, const double* x, const double* y, const double* z, const double* h,
+                              const double b[6], double spacing_fraction, double factor, double* out_xyz, int* out_id,
+                              long capacity) {
+    try {
+        kiwi::PointSet pts;
+        for (long i = 0; i < n; ++i) pts.append((int)(i + 1), x[i], y[i], z[i]);
+        std::vector<double> hv(h, h + n);
+        kiwi::Domain d;
+        d.x_min = b[0]; d.x_max = b[1];
+        d.y_min = b[2]; d.y_max = b[3];
+        d.z_min = b[4]; d.z_max = b[5];
+        kiwi::CoverageGridBufferParams params;
+        params.spacing_fraction = spacing_fraction;
+        params.coverage_radius_factor = factor;
+        kiwi::PointSet out = kiwi::add_coverage_grid_buffer(pts, hv, d, params);
+        long k = 0;
+        for (size_t i = (size_t)n; i < out.size() && k < capacity; ++i, ++k) {
+            out_xyz[3 * k] = out.x[i];
+            out_xyz[3 * k + 1] = out.y[i];
+            out_xyz[3 * k + 2] = out.z[i];
+            out_id[k] = out.id[i];
+        }
+        return k;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
 // save_cartesian_map (src/cartesian_map.cpp:202-229).
 int ref_save_cartesian_map(const char* path, int res, const double* b, const double* density, const double* vx,
                            const double* vy, const double* vz, const int* cell_id) {
