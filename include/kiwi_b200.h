@@ -340,7 +340,9 @@ int kiwi_coverage_grid_buffer(KiwiCtx* ctx, int64_t n, const double* x, const do
 /* ---- cartesian-map stage (run_cartesian_map_stage's point location, src/cartesian_map.cpp:84-200) ---- */
 /* Every cell centre of a resolution^3 grid over bounds6 takes the values of its nearest site (the Voronoi
  * cell it lies in: container::find_voronoi_cell) and that site's id.  Sites (3 doubles each, host arrays)
- * outside bounds6 are ignored, as the container drops them; site_id (may be NULL: the site index) gives the
+ * the reference's container drops are ignored: outside bounds6, or in a block index past the last (a site
+ * on an upper wall can be; block_scale_factor is grid_blocks.block_scale_factor, 0 = its default 3, which
+ * sets the container's block grid); site_id (may be NULL: the site index) gives the
  * ids written to voronoi_cell_id; cell_density / cell_vx / cell_vy / cell_vz hold each site's mapping row and
  * mapped (may be NULL: all) marks the sites that have one.  Outputs are host arrays of resolution^3 in the
  * x-major order (ix*res + iy)*res + iz; cells with no site (no sites at all) keep 0 and id 0, cells whose
@@ -350,8 +352,8 @@ int kiwi_coverage_grid_buffer(KiwiCtx* ctx, int64_t n, const double* x, const do
 int kiwi_cartesian_map(KiwiCtx* ctx, int64_t n_sites, const double* site_xyz, const int32_t* site_id,
                        const double* cell_density, const double* cell_vx, const double* cell_vy,
                        const double* cell_vz, const uint8_t* mapped, const double* bounds6, int32_t resolution,
-                       double* density, double* vx, double* vy, double* vz, int32_t* voronoi_cell_id,
-                       int64_t* counts2, KiwiStats* stats);
+                       double block_scale_factor, double* density, double* vx, double* vy, double* vz,
+                       int32_t* voronoi_cell_id, int64_t* counts2, KiwiStats* stats);
 
 #ifdef __cplusplus
 }

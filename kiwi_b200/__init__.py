@@ -745,10 +745,11 @@ class CartesianMap:
 
 
 def cartesian_map(sites, bounds, resolution, cell_density, cell_vx, cell_vy, cell_vz, site_id=None, mapped=None,
-                  ctx=None) -> CartesianMap:
+                  block_scale_factor=3.0, ctx=None) -> CartesianMap:
     """run_cartesian_map_stage's point location (src/cartesian_map.cpp:84-200) on the GPU: `sites` (n, 3)
     the point set, `cell_*` each site's mapping row, `site_id` the ids written to voronoi_cell_id (default:
-    the site index), `mapped` which sites have a mapping row (default: all)."""
+    the site index), `mapped` which sites have a mapping row (default: all); sites the reference's
+    container drops (outside the domain, or past its last block) own no cell."""
     ctx = ctx or default_context()
     xyz = _f64(np.asarray(sites, dtype=np.float64).reshape(-1, 3))
     n = xyz.shape[0]
@@ -764,9 +765,10 @@ def cartesian_map(sites, bounds, resolution, cell_density, cell_vx, cell_vy, cel
     st = KiwiStats()
     f = ctx._L.kiwi_cartesian_map
     f.argtypes = [C.c_void_p, C.c_int64, _dp, _i32p, _dp, _dp, _dp, _dp, C.POINTER(C.c_uint8), _dp, C.c_int32,
-                  _dp, _dp, _dp, _dp, _i32p, _i64p, C.POINTER(KiwiStats)]
+                  C.c_double, _dp, _dp, _dp, _dp, _i32p, _i64p, C.POINTER(KiwiStats)]
     ctx.check(f(ctx.handle, n, _p(xyz), sid.ctypes.data_as(_i32p) if sid is not None else None, *[_p(v) for v in vals],
                 mp.ctypes.data_as(C.POINTER(C.c_uint8)) if mp is not None else None, _p(b), res,
+                float(block_scale_factor),
                 *[_p(o) for o in outs], cid.ctypes.data_as(_i32p), counts.ctypes.data_as(_i64p), C.byref(st)),
               "cartesian_map")
     d = st.as_dict()

@@ -3,11 +3,12 @@
 // i.e. of its nearest site (container::find_voronoi_cell, an exact nearest-site search), and that site's
 // id.
 //
-// GPU form: the sites are binned into a uniform grid of about one site per bin (a stable radix sort by
-// bin, so a bin lists its sites in ascending site order), and one thread per cell centre searches shells
-// of bins around its own bin, nearest first, until no unsearched bin can hold a closer site.  Distances
-// are (site - centre)^2 summed x, y, z, as the reference's search computes them.  Exact ties (equidistant
-// sites) go to the smallest site index.  Built with --fmad=false, like the other FP64 units.
+// GPU form: the sites the reference's container keeps (sitebins.cuh) are binned into a uniform grid of
+// about one site per bin (a stable radix sort by bin, so a bin lists its sites in ascending site order),
+// and one thread per cell centre searches shells of bins around its own bin, nearest first, until no
+// unsearched bin can hold a closer site.  Distances are (site - centre)^2 summed x, y, z, as the
+// reference's search computes them.  Exact ties (equidistant sites) go to the smallest site index.  Built
+// with --fmad=false, like the other FP64 units.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,64 +17,11 @@
 
 #include "engine.hpp"
 #include "prims.cuh"
+#include "sitebins.cuh"
 
 using namespace kiwi_b200;
 
 namespace {
-
-struct SiteBins {
-    double x0, y0, z0;     // domain minimum
-    double wx, wy, wz;     // bin widths
-    int nbx, nby, nbz;
-    const int64_t* range;  // per bin [begin, end) in the sorted site arrays
-    const double *sx, *sy, *sz;
-    const int32_t* sidx;   // original site index
-    double margin;         // safety margin of the search's stopping distance
-};
-
-__device__ __forceinline__ int bin_of(double v, double v0, double w, int nb) {
-    int b = (int)((v - v0) / w);
-    return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
-}
-
-// Bin key of each site inside the domain (inclusive bounds, as the container keeps them); sites outside
-// get the key nbins, which sorts them past every bin.
-__global__ void k_site_keys(int64_t n, const double* __restrict__ xyz, double xmin, double xmax, double ymin,
-                            double ymax, double zmin, double zmax, SiteBins B, uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ vals) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
-    const bool in = x >= xmin && x <= xmax && y >= ymin && y <= ymax && z >= zmin && z <= zmax;
-    uint32_t key = (uint32_t)B.nbx * B.nby * B.nbz;
-    if (in) {
-        const int bx = bin_of(x, B.x0, B.wx, B.nbx), by = bin_of(y, B.y0, B.wy, B.nby), bz = bin_of(z, B.z0, B.wz, B.nbz);
-        key = (uint32_t)(((int64_t)bx * B.nby + by) * B.nbz + bz);
-    }
-    keys[i] = key;
-    vals[i] = (uint32_t)i;
-}
-
-__global__ void k_bin_ranges(const uint32_t* __restrict__ keys, int64_t n, uint32_t nbins, int64_t* __restrict__ range) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t k = keys[i];
-    if (k >= nbins) return;
-    if (i == 0 || keys[i - 1] != k) range[2 * (int64_t)k] = i;
-    if (i == n - 1 || keys[i + 1] != k) range[2 * (int64_t)k + 1] = i + 1;
-}
-
-__global__ void k_sorted_sites(int64_t n, const uint32_t* __restrict__ vals, const double* __restrict__ xyz,
-                               double* __restrict__ sx, double* __restrict__ sy, double* __restrict__ sz,
-                               int32_t* __restrict__ sidx) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t s = vals[i];
-    sx[i] = xyz[3 * (int64_t)s];
-    sy[i] = xyz[3 * (int64_t)s + 1];
-    sz[i] = xyz[3 * (int64_t)s + 2];
-    sidx[i] = (int32_t)s;
-}
 
 __device__ __forceinline__ void scan_bin(const SiteBins& B, int64_t b, double x, double y, double z, double& best,
                                          int32_t& bi) {
@@ -171,8 +119,9 @@ __global__ void k_locate(int res, double xmin, double ymin, double zmin, double 
 extern "C" int kiwi_cartesian_map(KiwiCtx* ctx, int64_t n_sites, const double* site_xyz, const int32_t* site_id,
                                   const double* cell_density, const double* cell_vx, const double* cell_vy,
                                   const double* cell_vz, const uint8_t* mapped, const double* bounds6,
-                                  int32_t resolution, double* density, double* vx, double* vy, double* vz,
-                                  int32_t* voronoi_cell_id, int64_t* counts2, KiwiStats* stats) {
+                                  int32_t resolution, double block_scale_factor, double* density, double* vx,
+                                  double* vy, double* vz, int32_t* voronoi_cell_id, int64_t* counts2,
+                                  KiwiStats* stats) {
     if (!ctx) return KIWI_ERR_ARG;
     KIWI_CUDA(ctx, cudaSetDevice(ctx->device));
     if (resolution <= 0) return set_err(ctx, KIWI_ERR_ARG, "cartesian_map.resolution must be > 0");
@@ -181,42 +130,26 @@ extern "C" int kiwi_cartesian_map(KiwiCtx* ctx, int64_t n_sites, const double* s
     if (n_sites < 0 || (n_sites > 0 && (!site_xyz || !cell_density || !cell_vx || !cell_vy || !cell_vz)))
         return set_err(ctx, KIWI_ERR_ARG, "bad site arrays");
     if (n_sites >= (1LL << 31)) return set_err(ctx, KIWI_ERR_ARG, "too many sites");
+    if (block_scale_factor == 0.0) block_scale_factor = 3.0;  // GridBlocks' default
+    if (!(block_scale_factor > 0.0)) return set_err(ctx, KIWI_ERR_ARG, "grid_blocks.block_scale_factor must be > 0");
     const int64_t nq = (int64_t)resolution * resolution * resolution;
     if (!density || !vx || !vy || !vz || !voronoi_cell_id) return set_err(ctx, KIWI_ERR_ARG, "null output");
     const int64_t launches0 = ctx->launches;
     const double xmin = bounds6[0], ymin = bounds6[2], zmin = bounds6[4];
     const double ex = bounds6[1] - xmin, ey = bounds6[3] - ymin, ez = bounds6[5] - zmin;
-    // about one site per bin, bins as close to cubes as the domain allows
-    const double vol = ex * ey * ez;
-    const double target = std::max<double>((double)n_sites, 1.0);
-    const double w = std::cbrt(vol / target);
-    auto nb = [&](double e) { return (int)std::min<double>(std::max<double>(std::floor(e / w), 1.0), 1024.0); };
+    const VoroBlocks V = voro_blocks_for(bounds6, n_sites, site_xyz, block_scale_factor);
     SiteBins B;
-    B.nbx = nb(ex);
-    B.nby = nb(ey);
-    B.nbz = nb(ez);
-    B.x0 = xmin;
-    B.y0 = ymin;
-    B.z0 = zmin;
-    B.wx = ex / B.nbx;
-    B.wy = ey / B.nby;
-    B.wz = ez / B.nbz;
+    site_bins_shape(bounds6, n_sites, B);
     const int64_t nbins = (int64_t)B.nbx * B.nby * B.nbz;
-    B.margin = 1e-9 * std::max(B.wx, std::max(B.wy, B.wz));
 
     // stage the sites and their values
     const int64_t ns = std::max<int64_t>(n_sites, 1);
-    double* d = nullptr;  // xyz (3), values (4), sorted xyz (3)
+    double* d = nullptr;    // xyz (3), values (4), sorted xyz (3)
     int32_t* di = nullptr;  // site ids, sorted index
     uint8_t* dm = nullptr;
     KIWI_TRY(scratch_t(ctx, S_PART, (size_t)(10 * ns), &d));
     KIWI_TRY(scratch_t(ctx, S_VOR_HOME, (size_t)(2 * ns), &di));
     KIWI_TRY(scratch_t(ctx, S_MISC2, (size_t)ns, &dm));
-    uint32_t *k0, *v0, *k1, *v1;
-    KIWI_TRY(scratch_t(ctx, S_KEYS0, (size_t)ns, &k0));
-    KIWI_TRY(scratch_t(ctx, S_VALS0, (size_t)ns, &v0));
-    KIWI_TRY(scratch_t(ctx, S_KEYS1, (size_t)ns, &k1));
-    KIWI_TRY(scratch_t(ctx, S_VALS1, (size_t)ns, &v1));
     int64_t* range = nullptr;
     KIWI_TRY(scratch_t(ctx, S_TILE_RANGE, (size_t)(2 * nbins), &range));
     double* dout = nullptr;
@@ -237,30 +170,9 @@ extern "C" int kiwi_cartesian_map(KiwiCtx* ctx, int64_t n_sites, const double* s
             KIWI_CUDA(ctx, cudaMemcpyAsync(di, site_id, sizeof(int32_t) * n_sites, cudaMemcpyHostToDevice, ctx->stream));
         if (mapped) KIWI_CUDA(ctx, cudaMemcpyAsync(dm, mapped, (size_t)n_sites, cudaMemcpyHostToDevice, ctx->stream));
     }
-    KIWI_CUDA(ctx, cudaMemsetAsync(range, 0, sizeof(int64_t) * 2 * nbins, ctx->stream));
     KIWI_CUDA(ctx, cudaMemsetAsync(dcount, 0, 2 * sizeof(unsigned long long), ctx->stream));
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
-    if (n_sites > 0) {
-        const unsigned g = (unsigned)((n_sites + 255) / 256);
-        k_site_keys<<<g, 256, 0, ctx->stream>>>(n_sites, d, bounds6[0], bounds6[1], bounds6[2], bounds6[3], bounds6[4],
-                                                bounds6[5], B, k0, v0);
-        KIWI_LAUNCHED(ctx);
-        int key_bits = 1;
-        while ((1LL << key_bits) <= nbins) ++key_bits;
-        bool second = false;
-        KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, n_sites, key_bits, &second));
-        const uint32_t* sk = second ? k1 : k0;
-        const uint32_t* sv = second ? v1 : v0;
-        k_bin_ranges<<<g, 256, 0, ctx->stream>>>(sk, n_sites, (uint32_t)nbins, range);
-        KIWI_LAUNCHED(ctx);
-        k_sorted_sites<<<g, 256, 0, ctx->stream>>>(n_sites, sv, d, d + 7 * ns, d + 8 * ns, d + 9 * ns, di + ns);
-        KIWI_LAUNCHED(ctx);
-    }
-    B.range = range;
-    B.sx = d + 7 * ns;
-    B.sy = d + 8 * ns;
-    B.sz = d + 9 * ns;
-    B.sidx = di + ns;
+    KIWI_TRY(build_site_bins(ctx, n_sites, d, V, B, d + 7 * ns, di + ns, range));
     const double dpx = ex / resolution, dpy = ey / resolution, dpz = ez / resolution;
     k_locate<<<(unsigned)((nq + 255) / 256), 256, 0, ctx->stream>>>(
         resolution, xmin, ymin, zmin, dpx, dpy, dpz, B, site_id ? di : nullptr, d + 3 * ns, d + 4 * ns, d + 5 * ns,

@@ -72,6 +72,9 @@ class Oracle:
         L.or_coverage_grid_buffer = getattr(L, pfx + "coverage_grid_buffer")
         L.or_coverage_grid_buffer.restype = C.c_int64
         L.or_coverage_grid_buffer.argtypes = [C.c_int64] + [_dp] * 5 + [C.c_double, C.c_double, _dp, _i32p]
+        L.or_container_order = getattr(L, pfx + "container_order")
+        L.or_container_order.restype = C.c_int64
+        L.or_container_order.argtypes = [C.c_int64, _dp, _dp, C.c_double, _i64p]
         L.or_cartesian_map_nearest = getattr(L, pfx + "cartesian_map_nearest")
         L.or_cartesian_map_nearest.restype = C.c_int
         L.or_cartesian_map_nearest.argtypes = [C.c_int64, _dp, _dp, C.c_int, _i32p]
@@ -129,6 +132,13 @@ class Oracle:
         if k < 0:
             return None
         return xyz[:3 * k].reshape(-1, 3), ids[:k]
+
+    def container_order(self, sites, bounds, scale=3.0):
+        """The site indices the reference's Voro++ container keeps, in its walk order."""
+        xyz = _f64(np.asarray(sites, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros(max(len(xyz), 1), dtype=np.int64)
+        k = self.lib.or_container_order(len(xyz), _d(xyz), _d(_f64(bounds)), scale, out.ctypes.data_as(_i64p))
+        return out[:k]
 
     def cartesian_map_nearest(self, sites, bounds, res):
         """Nearest site index of every cell centre of the res^3 grid (-1 without sites), brute force."""
@@ -289,6 +299,32 @@ class RefLib:
         if k < 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
         return xyz[:3 * k].reshape(-1, 3).copy(), ids[:k].copy()
+
+    def container_order(self, sites, bounds, scale=3.0):
+        """The site indices a container built as the reference builds it keeps, in c_loop_all order."""
+        f = self.lib.ref_container_order
+        f.restype = C.c_long
+        f.argtypes = [C.c_long, _dp, _dp, C.c_double, C.POINTER(C.c_long)]
+        xyz = _f64(np.asarray(sites, dtype=np.float64).reshape(-1))
+        n = len(xyz) // 3
+        out = np.zeros(max(n, 1), dtype=np.int64)
+        k = f(n, _d(xyz), _d(_f64(bounds)), scale, out.ctypes.data_as(C.POINTER(C.c_long)))
+        return out[:k]
+
+    def lloyd_step(self, xyz, ids, bounds, scale=3.0):
+        """The reference's lloyd_step: (ids, xyz (k, 3)) in the container's walk order."""
+        f = self.lib.ref_lloyd_step
+        f.restype = C.c_long
+        f.argtypes = [C.c_long, _ip, _dp, _dp, C.c_double, _ip, _dp, C.c_long]
+        xyz = _f64(np.asarray(xyz, dtype=np.float64).reshape(-1))
+        ids = np.ascontiguousarray(ids, dtype=np.int32)
+        n = len(ids)
+        oid = np.zeros(max(n, 1), dtype=np.int32)
+        oxyz = np.zeros(3 * max(n, 1))
+        k = f(n, ids.ctypes.data_as(_ip), _d(xyz), _d(_f64(bounds)), scale, oid.ctypes.data_as(_ip), _d(oxyz), n)
+        if k < 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return oid[:k].copy(), oxyz[:3 * k].reshape(-1, 3).copy()
 
     def locate_sample(self, xyz, ids, bounds, res, ix_begin, ix_end, threads=0):
         """The stage's point location over x-slabs [ix_begin, ix_end): (seconds, owning site id per cell,

@@ -571,6 +571,51 @@ long ref_coverage_grid_buffer(long n, const double* x, const double* y, const do
     }
 }
 
+// lloyd_step (src/point_set.cpp:265-293) on the given point set: the moved points in the container's walk
+// order (ids and positions, out_xyz 3 per point); returns their count, or -1 with the reference's message.
+long ref_lloyd_step(long n, const int* ids, const double* xyz, const double b[6], double scale, int* out_id,
+                    double* out_xyz, long capacity) {
+    try {
+        kiwi::PointSet pts;
+        for (long i = 0; i < n; ++i) pts.append(ids[i], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        kiwi::Domain d;
+        d.x_min = b[0]; d.x_max = b[1];
+        d.y_min = b[2]; d.y_max = b[3];
+        d.z_min = b[4]; d.z_max = b[5];
+        kiwi::GridBlocks blocks;
+        blocks.block_scale_factor = scale;
+        kiwi::PointSet out = kiwi::lloyd_step(pts, d, blocks);
+        long k = 0;
+        for (size_t i = 0; i < out.size() && k < capacity; ++i, ++k) {
+            out_id[k] = out.id[i];
+            out_xyz[3 * k] = out.x[i];
+            out_xyz[3 * k + 1] = out.y[i];
+            out_xyz[3 * k + 2] = out.z[i];
+        }
+        return k;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// A container built as the reference builds it (pre_container -> guess_scaled_blocks -> setup, ids = site
+// indices): the site indices it keeps, in its c_loop_all walk order; returns their count.
+long ref_container_order(long n, const double* xyz, const double b[6], double scale, long* out) {
+    voro::pre_container pcon(b[0], b[1], b[2], b[3], b[4], b[5], false, false, false);
+    for (long i = 0; i < n; ++i) pcon.put((int)i, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    int bx, by, bz;
+    kiwi::guess_scaled_blocks(pcon, scale, bx, by, bz);
+    voro::container con(b[0], b[1], b[2], b[3], b[4], b[5], bx, by, bz, false, false, false, 8);
+    pcon.setup(con);
+    voro::c_loop_all clo(con);
+    long k = 0;
+    if (clo.start()) do {
+        out[k++] = clo.pid();
+    } while (clo.inc());
+    return k;
+}
+
 // save_cartesian_map (src/cartesian_map.cpp:202-229).
 int ref_save_cartesian_map(const char* path, int res, const double* b, const double* density, const double* vx,
                            const double* vy, const double* vz, const int* cell_id) {

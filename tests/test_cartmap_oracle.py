@@ -37,3 +37,18 @@ def test_oracle_matches_reference_stage(oracle, fn):
     outside = ~((xyz[:, 0] >= b[0]) & (xyz[:, 0] <= b[1]) & (xyz[:, 1] >= b[2]) & (xyz[:, 1] <= b[3]) &
                 (xyz[:, 2] >= b[4]) & (xyz[:, 2] <= b[5]))
     assert not np.isin(np.nonzero(outside)[0], near).any()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_container_filter_and_order_match_reference(oracle, reflib, seed):
+    """Which sites the reference's Voro++ container keeps (a site on an upper wall falls out) and the order
+    it walks them in, restated by the oracle, against a container built as the reference builds it."""
+    rng = np.random.default_rng(seed)
+    xyz = rng.uniform(-0.1, 1.1, (400, 3))
+    xyz[:20, 0] = 1.0
+    xyz[20:40, 1] = 0.0
+    xyz[40:45] = [1.0, 1.0, 1.0]
+    xyz[45:50] = [0.0, 0.0, 0.0]
+    for b in ((0.0, 1.0, 0.0, 1.0, 0.0, 1.0), (0.0, 1.0, -0.3, 1.0, 0.0, 0.7)):
+        for scale in (3.0, 1.0):
+            assert np.array_equal(oracle.container_order(xyz, b, scale), reflib.container_order(xyz, b, scale))

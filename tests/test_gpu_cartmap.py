@@ -49,6 +49,8 @@ def test_random_sites_vs_oracle(kiwi, ctx, oracle, case):
     else:
         bounds, res = (-36.0, -34.0, -60.0, -57.5, 1.4, 2.0), 15
         xyz = rng.uniform([-36.2, -60.1, 1.3], [-33.9, -57.4, 2.1], (300, 3))
+        xyz[:15, 0] = -34.0  # on the upper x wall: the container drops some or all of them
+        xyz[15:30, 2] = 1.4  # on the lower z wall: kept
     n = len(xyz)
     vals = [rng.random(n) for _ in range(4)]
     m = kiwi.cartesian_map(xyz, bounds, res, *vals, ctx=ctx)
@@ -98,8 +100,10 @@ def test_edge_cases(kiwi, ctx):
     # sites outside the domain only: the same
     m = kiwi.cartesian_map(np.array([[2.0, 0.5, 0.5], [-0.1, 0.5, 0.5]]), bounds, 3, *[np.ones(2)] * 4, ctx=ctx)
     assert m.stats["unresolved"] == 27
-    # a site on the domain's upper corner is kept; one cell
+    # the reference's container drops a site on the domain's upper corner and keeps one on the lower corner
     m = kiwi.cartesian_map(np.array([[1.0, 1.0, 1.0]]), bounds, 1, *[np.array([7.0])] * 4, site_id=[42], ctx=ctx)
+    assert m.stats["unresolved"] == 1 and m.voronoi_cell_id[0] == 0
+    m = kiwi.cartesian_map(np.array([[0.0, 0.0, 0.0]]), bounds, 1, *[np.array([7.0])] * 4, site_id=[42], ctx=ctx)
     assert m.voronoi_cell_id[0] == 42 and m.density[0] == 7.0
     # unmapped sites: their cells keep 0 and carry the id
     xyz = np.array([[0.25, 0.5, 0.5], [0.75, 0.5, 0.5]])
