@@ -337,6 +337,17 @@ int kiwi_coverage_grid_buffer(KiwiCtx* ctx, int64_t n, const double* x, const do
                               double coverage_radius_factor, int64_t capacity, double* out_x, double* out_y,
                               double* out_z, int32_t* out_id, int64_t* n_added);
 
+/* lloyd_step (src/point_set.cpp:265-293): every site the reference's Voro++ container keeps (see
+ * kiwi_cartesian_map) moves to the centroid of its Voronoi cell clipped to the domain; the moved sites come
+ * out in the container's walk order (blocks in index order, each block's sites in input order), ids carried
+ * along (ids may be NULL: the input index).  out_id / out_xyz (3 per site) / out_volume (the cell volumes,
+ * may be NULL) must hold n entries; *n_out receives the count, *n_failed (may be NULL) the kept sites whose
+ * cell could not be built (dropped, as Voro++ drops a cell it cannot compute).  block_scale_factor: as for
+ * kiwi_cartesian_map.  Host arrays. */
+int kiwi_lloyd_step(KiwiCtx* ctx, int64_t n, const int32_t* ids, const double* xyz, const double* bounds6,
+                    double block_scale_factor, int32_t* out_id, double* out_xyz, double* out_volume, int64_t* n_out,
+                    int64_t* n_failed, KiwiStats* stats);
+
 /* ---- cartesian-map stage (run_cartesian_map_stage's point location, src/cartesian_map.cpp:84-200) ---- */
 /* Every cell centre of a resolution^3 grid over bounds6 takes the values of its nearest site (the Voronoi
  * cell it lies in: container::find_voronoi_cell) and that site's id.  Sites (3 doubles each, host arrays)

@@ -829,6 +829,32 @@ def coverage_grid_buffer(particles: dict, bounds, spacing_fraction=0.05, coverag
     return np.stack([o[:k] for o in out], axis=1), ids[:k].copy()
 
 
+def lloyd_step(sites, bounds, ids=None, block_scale_factor=3.0, ctx=None):
+    """lloyd_step (src/point_set.cpp:265-293) on the GPU: the sites the reference's container keeps, each
+    moved to its Voronoi cell's centroid, in the container's walk order.  Returns (ids, xyz (k, 3), cell
+    volumes (k,), stats)."""
+    ctx = ctx or default_context()
+    xyz = _f64(np.asarray(sites, dtype=np.float64).reshape(-1, 3))
+    n = xyz.shape[0]
+    sid = np.ascontiguousarray(ids, dtype=np.int32) if ids is not None else None
+    oid = np.empty(max(n, 1), dtype=np.int32)
+    oxyz = np.empty((max(n, 1), 3))
+    ovol = np.empty(max(n, 1))
+    k, failed = C.c_int64(0), C.c_int64(0)
+    st = KiwiStats()
+    f = ctx._L.kiwi_lloyd_step
+    f.argtypes = [C.c_void_p, C.c_int64, _i32p, _dp, _dp, C.c_double, _i32p, _dp, _dp, _i64p, _i64p,
+                  C.POINTER(KiwiStats)]
+    ctx.check(f(ctx.handle, n, sid.ctypes.data_as(_i32p) if sid is not None else None, _p(xyz), _p(_f64(bounds)),
+                float(block_scale_factor), oid.ctypes.data_as(_i32p), _p(oxyz), _p(ovol), C.byref(k), C.byref(failed),
+                C.byref(st)), "lloyd step")
+    d = st.as_dict()
+    d["failed"] = failed.value
+    d["dropped"] = d["skipped_outside"]
+    m = k.value
+    return oid[:m].copy(), oxyz[:m].copy(), ovol[:m].copy(), d
+
+
 def version() -> str:
     return load_library().kiwi_version().decode()
 

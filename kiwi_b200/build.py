@@ -35,6 +35,7 @@ UNITS = [
     ("tabulated.cu", ["--fmad=false"]),
     ("cartmap.cu", ["--fmad=false"]),
     ("pointset.cu", ["--fmad=false"]),
+    ("lloyd.cu", ["--fmad=false"]),
 ]
 
 

@@ -86,7 +86,7 @@ struct SiteBins {
     double margin;         // safety margin of a search's stopping distance
 };
 
-__device__ __forceinline__ int bin_of(double v, double v0, double w, int nb) {
+__host__ __device__ inline int bin_of(double v, double v0, double w, int nb) {
     int b = (int)((v - v0) / w);
     return b < 0 ? 0 : (b >= nb ? nb - 1 : b);
 }
