@@ -93,8 +93,9 @@ def parse():
     ap.add_argument("--vor-n", type=int, default=200_000, help="voronoi workload: particles")
     ap.add_argument("--cmap-n", type=int, default=1_000_000, help="cartesian_map workload: sites")
     ap.add_argument("--cmap-res", type=int, default=256, help="cartesian_map workload: grid cells per axis")
+    ap.add_argument("--lloyd-n", type=int, default=1_000_000, help="lloyd workload: particles")
     ap.add_argument("--workload", default="lognormal",
-                    choices=["lognormal", "batch", "adjoint", "voronoi", "cartesian_map"],
+                    choices=["lognormal", "batch", "adjoint", "voronoi", "cartesian_map", "lloyd"],
                     help="batch: many column snapshots of log-uniform sizes on grids of log-uniform resolution, "
                          "kernels cycling M4 / M6 / WC4, in one persistent graph-recorded launch")
     ap.add_argument("--batch-items", type=int, default=64)
@@ -465,6 +466,72 @@ def run_cartesian_map(args):
     return 0
 
 
+def run_lloyd(args):
+    """Point-set stage on the GPU: --lloyd-n column-recipe particles on a 5 pc cube (seed 1003), their
+    coverage-grid buffer (spacing 0.05 x 5 pc, kiwi_coverage_grid_buffer) and one Lloyd step
+    (kiwi_lloyd_step: every kept site's Voronoi cell built and its centroid taken).  `value` is Voronoi cells
+    built per second over the Lloyd step's device time; the CPU baseline is the reference's own lloyd_step
+    (single-threaded Voro++, as the reference runs it) on the sites of a sub-box holding a bounded sample."""
+    import torch
+
+    import kiwi_b200
+    from kiwi_b200.workloads import column_snapshot
+    from oracle.oracle import load_ref
+
+    torch.cuda.set_device(0)
+    P, bounds = column_snapshot(n=args.lloyd_n, seed=1003, box=(5.0, 5.0, 5.0))
+    ctx = kiwi_b200.Context(0)
+    t0 = time.perf_counter()
+    bxyz, bids = kiwi_b200.coverage_grid_buffer(P, bounds, 0.05, 2.0, ctx=ctx)
+    t_buf = time.perf_counter() - t0
+    xyz = np.concatenate([np.stack([P["x"], P["y"], P["z"]], axis=1), bxyz])
+    ids = np.arange(1, len(xyz) + 1, dtype=np.int32)
+    for _ in range(max(args.warmup, 1)):
+        r = kiwi_b200.lloyd_step(xyz, bounds, ids=ids, ctx=ctx)
+    g_ms, t_ms, launches = [], [], 0
+    clocks = ClockSampler(0)
+    clocks.start()
+    for _ in range(args.steps):
+        r = kiwi_b200.lloyd_step(xyz, bounds, ids=ids, ctx=ctx)
+        g_ms.append(r[3]["gather_ms"])
+        t_ms.append(r[3]["total_ms"])
+        launches += r[3]["launches"]
+    clk = clocks.stop()
+    cells = len(r[0])
+    vol_err = abs(r[2].sum() - np.prod([bounds[2 * a + 1] - bounds[2 * a] for a in range(3)]))
+    cpu, agree = None, None
+    ref = load_ref()
+    if ref is not None and not args.no_cpu_baseline:
+        # the sites of a centred sub-box (its own domain), about 20 k of them
+        frac = min(1.0, (20_000 / len(xyz)) ** (1 / 3))
+        c = [(bounds[2 * a] + bounds[2 * a + 1]) / 2 for a in range(3)]
+        half = [(bounds[2 * a + 1] - bounds[2 * a]) * frac / 2 for a in range(3)]
+        sb = tuple(v for a in range(3) for v in (c[a] - half[a], c[a] + half[a]))
+        m = np.all((xyz >= [sb[0], sb[2], sb[4]]) & (xyz <= [sb[1], sb[3], sb[5]]), axis=1)
+        t0 = time.perf_counter()
+        rid, rxyz = ref.lloyd_step(xyz[m], ids[m], sb)
+        sec = time.perf_counter() - t0
+        cpu = {"value": len(rid) / sec, "unit": "cells/s", "cores": 1, "kind": "reference",
+               "sample": f"lloyd_step on the {int(m.sum())} sites of a centred sub-box (its own domain), {sec:.2f} s"}
+        gid, gxyz, _, _ = kiwi_b200.lloyd_step(xyz[m], sb, ids=ids[m], ctx=ctx)
+        agree = {"sites": int(len(rid)), "order_equal": bool(np.array_equal(gid, rid)),
+                 "max_abs_position_diff": float(np.abs(gxyz - rxyz).max()) if np.array_equal(gid, rid) else None}
+    line = {
+        "metric": "Voronoi cells built/s (Lloyd step)", "value": cells / (np.mean(g_ms) * 1e-3), "unit": "cells/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": float(np.mean(g_ms)),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.lloyd_n} column-recipe particles + {len(bids)} coverage-grid buffer points, "
+                               "5 pc cube, one Lloyd step", "sites": int(len(xyz)), "cells": int(cells)},
+        "failed_cells": int(r[3]["failed"]), "cell_volume_sum_minus_domain": float(vol_err),
+        "coverage_buffer_s_end_to_end": t_buf, "gpu_launches": int(launches), "clocks": clk,
+        "e2e": {"value": cells / (np.mean(t_ms) * 1e-3), "unit": "cells/s", "ms_per_step": float(np.mean(t_ms)),
+                "h2d_bytes_per_step": int(len(xyz) * 28), "d2h_bytes_per_step": int(cells * 36)},
+        "cpu_baseline": cpu, "agreement_with_reference": agree,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch(args):
     """Batched sph-to-grid: args.batch_items column snapshots (item i seeded 5000 + i), N log-uniform in
     [nmin, nmax], grid res^3 with res log-uniform in [resmin, resmax], kernels cycling M4 / M6 / WC4; one
@@ -556,6 +623,8 @@ def main():
         return run_voronoi(args)
     if args.workload == "cartesian_map":
         return run_cartesian_map(args)
+    if args.workload == "lloyd":
+        return run_lloyd(args)
     ws, rank, local = dist_env()
     import torch
 
