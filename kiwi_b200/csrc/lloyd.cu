@@ -6,7 +6,8 @@
 // convex polyhedron -- its planes, and its vertices as triangles of three plane indices ordered
 // counter-clockwise seen from outside -- and is clipped by the bisector plane of each neighbouring site,
 // taken shell by shell from a uniform bin grid around the site, each shell's sites nearest first (so the
-// cell shrinks fast and few planes are spent on sites that later clips make irrelevant): a clip removes the
+// cell shrinks fast and few planes are spent on sites that later clips make irrelevant; dense bins are
+// scanned in several passes of at most 128 candidates): a clip removes the
 // vertices beyond the plane and closes the hole with one new vertex per crossing edge (the removed vertices' edges whose
 // twin edge belongs to a kept vertex).  The search stops once no unsearched site can be nearer than twice
 // the cell's radius (any farther site's bisector misses the cell).  Volume and centroid come from a fan of
@@ -205,36 +206,16 @@ __host__ __device__ int cell_moments(const Cell& c, double* vol, double* cen) {
     return kCellOk;
 }
 
-constexpr int kCandMax = 128;  // neighbour candidates sorted and clipped together
+constexpr int kCandMax = 128;  // neighbour candidates held (sorted) at a time
 
-// Clips the cell by the candidates cand[0 .. n) (squared distance, sorted index) nearest first.
-__host__ __device__ int clip_candidates(Cell& c, const SiteBins& B, double sx, double sy, double sz, double* cd,
-                                        int64_t* ci, int n, double eps, double* r2) {
-    for (int i = 1; i < n; ++i) {  // insertion sort by distance, then by index (a fixed order)
-        const double d = cd[i];
-        const int64_t x = ci[i];
-        int j = i - 1;
-        while (j >= 0 && (cd[j] > d || (cd[j] == d && ci[j] > x))) {
-            cd[j + 1] = cd[j];
-            ci[j + 1] = ci[j];
-            --j;
-        }
-        cd[j + 1] = d;
-        ci[j + 1] = x;
-    }
-    for (int i = 0; i < n; ++i) {
-        const double dd = cd[i];
-        if (dd >= 4.0 * *r2) break;  // sorted: the rest are beyond reach too
-        const int64_t s = ci[i];
-        const int st = cell_clip(c, B.sx[s] - sx, B.sy[s] - sy, B.sz[s] - sz, 0.5 * dd, eps * sqrt(dd), r2);
-        if (st != kCellOk) return st;
-    }
-    return kCellOk;
-}
+// (d, i) < (e, j) in the order candidates are clipped: by squared distance, then by sorted index.
+__host__ __device__ inline bool cand_less(double d, int64_t i, double e, int64_t j) { return d < e || (d == e && i < j); }
 
-// The Voronoi cell in the box of the q-th kept site of B: neighbours gathered shell by shell of search
-// bins, each shell's candidates clipped nearest first; stops once every unsearched site is at least twice
-// the cell's radius away.  Returns a CellStatus; the centroid (absolute) and volume on success.
+// The Voronoi cell in the box of the q-th kept site of B.  Neighbours come shell by shell of search bins;
+// within a shell they are clipped nearest first: a pass keeps the kCandMax nearest not yet clipped, clips
+// them, and scans the shell again while it had to leave some out (dense bins).  Stops once every unsearched
+// site is at least twice the cell's radius away.  Returns a CellStatus; the centroid (absolute) and volume
+// on success.
 __host__ __device__ int build_cell(Cell& c, const SiteBins& B, const VoroBlocks& V, int64_t q, double eps,
                                    double* cen, double* vol) {
     const double sx = B.sx[q], sy = B.sy[q], sz = B.sz[q];
@@ -246,37 +227,56 @@ __host__ __device__ int build_cell(Cell& c, const SiteBins& B, const VoroBlocks&
     const int rmax = max(max(B.nbx, B.nby), B.nbz);
     double cd[kCandMax];
     int64_t ci[kCandMax];
-    int st = kCellOk;
     for (int r = 0; r <= rmax; ++r) {
         const int i0 = max(bx - r, 0), i1 = min(bx + r, B.nbx - 1);
         const int j0 = max(by - r, 0), j1 = min(by + r, B.nby - 1);
         const int k0 = max(bz - r, 0), k1 = min(bz + r, B.nbz - 1);
-        int nc = 0;
-        for (int i = i0; i <= i1; ++i)
-            for (int j = j0; j <= j1; ++j) {
-                const bool face = (i == bx - r || i == bx + r || j == by - r || j == by + r);
-                const int64_t row = ((int64_t)i * B.nby + j) * B.nbz;
-                for (int k = k0; k <= k1; ++k) {
-                    if (!face && k != bz - r && k != bz + r) continue;
-                    const int64_t bin = row + k;
-                    const int64_t e = B.range[2 * bin + 1];
-                    for (int64_t s = B.range[2 * bin]; s < e; ++s) {
-                        if (B.sidx[s] == self) continue;
-                        const double dx = B.sx[s] - sx, dy = B.sy[s] - sy, dz = B.sz[s] - sz;
-                        const double dd = dx * dx + dy * dy + dz * dz;
-                        if (dd == 0.0 || dd >= 4.0 * r2) continue;  // a coincident site, or one beyond reach
-                        cd[nc] = dd;
-                        ci[nc] = s;
-                        if (++nc == kCandMax) {
-                            st = clip_candidates(c, B, sx, sy, sz, cd, ci, nc, eps, &r2);
-                            if (st != kCellOk) return st;
-                            nc = 0;
+        double done_d = -1.0;  // candidates up to (done_d, done_i) are clipped already
+        int64_t done_i = -1;
+        for (int pass = 0;; ++pass) {
+            int nc = 0;
+            bool left_out = false;
+            for (int i = i0; i <= i1; ++i)
+                for (int j = j0; j <= j1; ++j) {
+                    const bool face = (i == bx - r || i == bx + r || j == by - r || j == by + r);
+                    const int64_t row = ((int64_t)i * B.nby + j) * B.nbz;
+                    for (int k = k0; k <= k1; ++k) {
+                        if (!face && k != bz - r && k != bz + r) continue;
+                        const int64_t bin = row + k;
+                        const int64_t e = B.range[2 * bin + 1];
+                        for (int64_t s = B.range[2 * bin]; s < e; ++s) {
+                            if (B.sidx[s] == self) continue;
+                            const double dx = B.sx[s] - sx, dy = B.sy[s] - sy, dz = B.sz[s] - sz;
+                            const double dd = dx * dx + dy * dy + dz * dz;
+                            if (dd == 0.0 || dd >= 4.0 * r2) continue;  // a coincident site, or beyond reach
+                            if (!cand_less(done_d, done_i, dd, s)) continue;  // clipped in an earlier pass
+                            // insert into the sorted buffer, keeping the kCandMax nearest
+                            if (nc == kCandMax) {
+                                left_out = true;
+                                if (!cand_less(dd, s, cd[nc - 1], ci[nc - 1])) continue;
+                                --nc;
+                            }
+                            int m = nc++;
+                            while (m > 0 && cand_less(dd, s, cd[m - 1], ci[m - 1])) {
+                                cd[m] = cd[m - 1];
+                                ci[m] = ci[m - 1];
+                                --m;
+                            }
+                            cd[m] = dd;
+                            ci[m] = s;
                         }
                     }
                 }
+            for (int m = 0; m < nc; ++m) {
+                if (cd[m] >= 4.0 * r2) break;  // sorted: the rest are beyond reach too
+                const int64_t s = ci[m];
+                const int st = cell_clip(c, B.sx[s] - sx, B.sy[s] - sy, B.sz[s] - sz, 0.5 * cd[m], eps * sqrt(cd[m]), &r2);
+                if (st != kCellOk) return st;
             }
-        st = clip_candidates(c, B, sx, sy, sz, cd, ci, nc, eps, &r2);
-        if (st != kCellOk) return st;
+            if (!left_out || pass > 1000000) break;
+            done_d = cd[nc - 1];
+            done_i = ci[nc - 1];
+        }
         if (i0 == 0 && j0 == 0 && k0 == 0 && i1 == B.nbx - 1 && j1 == B.nby - 1 && k1 == B.nbz - 1) break;
         double dmin = INFINITY;
         if (i0 > 0) dmin = fmin(dmin, sx - (B.x0 + i0 * B.wx));
@@ -289,7 +289,7 @@ __host__ __device__ int build_cell(Cell& c, const SiteBins& B, const VoroBlocks&
         if (dmin * dmin >= 4.0 * r2) break;  // every unsearched site is at least 2R away
     }
     double cc[3] = {0.0, 0.0, 0.0};
-    st = cell_moments(c, vol, cc);
+    const int st = cell_moments(c, vol, cc);
     cen[0] = sx + cc[0];
     cen[1] = sy + cc[1];
     cen[2] = sz + cc[2];

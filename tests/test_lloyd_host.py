@@ -61,3 +61,37 @@ def test_clustered_cells_tile_the_domain(cells, oracle):
     cen, vol, st = cells(xyz, b)
     assert np.all(st[order] == 0)
     assert abs(vol[order].sum() - 1000.0) <= 1e-10 * 1000.0
+
+
+def test_dense_cells_match_an_independent_construction(cells, reflib):
+    """Dense clustered sites (a filament, as in the column recipe): interior cells against qhull's
+    Voronoi regions (scipy), an independent construction.  Here the reference's Voro++ centroids can sit
+    ~1e-8 from both (its vertex tolerance), so the reference is compared with that looser bound."""
+    from scipy.spatial import ConvexHull, Voronoi
+
+    rng = np.random.default_rng(12)
+    n = 4000
+    xyz = np.column_stack([1.0 + 0.05 * rng.standard_normal(n), 1.0 + 0.05 * rng.standard_normal(n), rng.random(n) * 2])
+    xyz = np.concatenate([xyz, rng.random((500, 3)) * 2])
+    b = (0.0, 2.0, 0.0, 2.0, 0.0, 2.0)
+    cen, vol, st = cells(xyz, b)
+    vor = Voronoi(xyz)
+    inner = np.nonzero((np.abs(xyz[:, 0] - 1) < 0.03) & (np.abs(xyz[:, 1] - 1) < 0.03) &
+                       (xyz[:, 2] > 0.3) & (xyz[:, 2] < 1.7))[0][:200]
+    worst = 0.0
+    for s in inner:
+        reg = vor.regions[vor.point_region[s]]
+        assert -1 not in reg
+        V = vor.vertices[reg]
+        hull = ConvexHull(V)
+        acc, tot = np.zeros(3), 0.0
+        for simp in hull.simplices:
+            a, p, q = V[simp]
+            v = abs(np.dot(a - xyz[s], np.cross(p - xyz[s], q - xyz[s]))) / 6
+            tot += v
+            acc += v * (xyz[s] + a + p + q) / 4
+        worst = max(worst, np.abs(cen[s] - acc / tot).max() / np.cbrt(tot))
+        assert abs(vol[s] - hull.volume) <= 1e-10 * hull.volume
+    assert worst <= 1e-11, worst
+    rid, rxyz = reflib.lloyd_step(xyz, np.arange(len(xyz), dtype=np.int32), b)
+    assert np.abs(cen[rid] - rxyz).max() <= 1e-6
