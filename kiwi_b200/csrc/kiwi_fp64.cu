@@ -523,8 +523,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
                         lattice_generic_vertex(K, H, r0, a2, a1, s_E + kLatGenERec * e2);
                 } else {
-                    f = lattice_vertex(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1]) +
-                        lattice_vertex(s_h[jp], r0, a2, a1, s_D2[e2], s_D3[e2]);
+                    f = lattice_corner(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1], s_D2[e2], s_D3[e2]);
                 }
                 n_vp += 2;
             }

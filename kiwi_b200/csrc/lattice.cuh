@@ -64,6 +64,45 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
     return lattice_vertex_t<double>(h, r0, R_0, t, D2, D3);
 }
 
+// The pyramid pair of one corner value, F(r0, a1, a2) + F(r0, a2, a1): the two right triangles of the
+// rectangle spanned by the particle's projection and the corner (legs a1 along the first edge line and a2
+// along the second, and the reverse), in the wall at distance r0.  The pair shares the wall constants and
+// the hypotenuse, computed once.  Beyond 2h a vertex tier needs I0 = phi and I1 only, and the two angles
+// atan2(a2, a1) + atan2(a1, a2) sum to pi/2 exactly, so the pair needs no arc tangent of an angle there.
+// r0, a1, a2 > 0 (the callers skip zero corners); (D2a, D3a) and (D2b, D3b) are the two edge tiers.
+static __device__ __noinline__ double lattice_corner(double h, double r0, double a1, double a2, double D2a,
+                                                     double D3a, double D2b, double D3b) {
+    const CubicWall w = cubic_wall(h, r0);
+    const double s2 = a1 * a1 + a2 * a2;
+    const double rr = sqrt(s2);
+    const double r2 = r0 * r0 + s2;
+    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+    const double aa = a1 / r0, ab = a2 / r0;
+    const double sa = a2 / rr, ca = a1 / rr;  // pyramid a: R_0 = a1, t = a2; pyramid b: the legs swapped
+    if (!(r2 < 4.0 * w.h2)) {
+        const double I1a = phi_I1<double>(sa, ca, aa, aa * aa);
+        const double I1b = phi_I1<double>(ca, sa, ab, ab * ab);
+        return r0h3 / kPi * (-0.25 * r0h_3 * (I1a + I1b) + w.B3 / r03 * (0.5 * kPi) + D3a + D3b);
+    }
+    double sum = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        const double a = k ? ab : aa, sinp = k ? ca : sa, cosp = k ? sa : ca;
+        const double phi = k ? atan2(a1, a2) : atan2(a2, a1);
+        const PhiSeries s = phi_series_sc<double>(phi, sinp, cosp, a, a * a);
+        double f;
+        if (r2 < w.h2) {
+            f = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
+        } else {
+            f = r0h3 / kPi * (0.25 * (4. / 3. * s.I_2 - (r0 / h) * s.I_3 + 0.3 * r0h2 * s.I_4 - 1. / 30. * r0h3 * s.I_5 +
+                                      1. / 15. * r0h_3 * s.I1) +
+                              w.B2 / r03 * s.I0 + (k ? D2b : D2a));
+        }
+        sum += f;
+    }
+    return sum;
+}
+
 // Position of the smallest j with s_off[j] <= it among the chunk's np particles (s_off ascending).
 static __device__ __forceinline__ int chunk_search(const int* s_off, int np, int it) {
     int lo = 0, hi = np - 1;
