@@ -66,37 +66,57 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
 
 // The pyramid pair of one corner value, F(r0, a1, a2) + F(r0, a2, a1): the two right triangles of the
 // rectangle spanned by the particle's projection and the corner (legs a1 along the first edge line and a2
-// along the second, and the reverse), in the wall at distance r0.  The pair shares the wall constants and
-// the hypotenuse, computed once.  Beyond 2h a vertex tier needs I0 = phi and I1 only, and the two angles
-// atan2(a2, a1) + atan2(a1, a2) sum to pi/2 exactly, so the pair needs no arc tangent of an angle there.
+// along the second, and the reverse), in the wall at distance r0.  The vertex tier's series
+// (src/kernel_integral.cpp:356-400) is written here in the triangle's own lengths, which the pair shares:
+// with r the distance to the corner, the series variable u = sin(phi) sqrt(1 - mu^2) is a2 / r for the
+// first pyramid and a1 / r for the second, tan(phi) = a2 / a1 (a1 / a2), 1 / cos^2(phi) = (a1^2 + a2^2) / a1^2
+// (/ a2^2), and the two angles sum to pi/2 (the smaller one is taken by atan2, the larger as its complement,
+// both to an ulp).  log(1 + u) - log(1 - u) is 2 atanh(u).  Beyond 2h a tier needs I0 = phi and I1 only,
+// so the pair there needs no angle at all.  The wall constants are computed once for the pair.
 // r0, a1, a2 > 0 (the callers skip zero corners); (D2a, D3a) and (D2b, D3b) are the two edge tiers.
 static __device__ __noinline__ double lattice_corner(double h, double r0, double a1, double a2, double D2a,
                                                      double D3a, double D2b, double D3b) {
     const CubicWall w = cubic_wall(h, r0);
     const double s2 = a1 * a1 + a2 * a2;
-    const double rr = sqrt(s2);
     const double r2 = r0 * r0 + s2;
+    const double r = sqrt(r2);
     const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
     const double aa = a1 / r0, ab = a2 / r0;
-    const double sa = a2 / rr, ca = a1 / rr;  // pyramid a: R_0 = a1, t = a2; pyramid b: the legs swapped
+    const double ua = a2 / r, ub = a1 / r;
     if (!(r2 < 4.0 * w.h2)) {
-        const double I1a = phi_I1<double>(sa, ca, aa, aa * aa);
-        const double I1b = phi_I1<double>(ca, sa, ab, ab * ab);
+        const double I1a = atan(ua / aa), I1b = atan(ub / ab);
         return r0h3 / kPi * (-0.25 * r0h_3 * (I1a + I1b) + w.B3 / r03 * (0.5 * kPi) + D3a + D3b);
     }
+    double pa, pb;
+    if (a2 <= a1) {
+        pa = atan2(a2, a1);
+        pb = 0.5 * kPi - pa;
+    } else {
+        pb = atan2(a1, a2);
+        pa = 0.5 * kPi - pb;
+    }
+    const bool inner = r2 < w.h2;
     double sum = 0.0;
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
-        const double a = k ? ab : aa, sinp = k ? ca : sa, cosp = k ? sa : ca;
-        const double phi = k ? atan2(a1, a2) : atan2(a2, a1);
-        const PhiSeries s = phi_series_sc<double>(phi, sinp, cosp, a, a * a);
+        const double a = k ? ab : aa, u = k ? ub : ua, phi = k ? pb : pa;
+        const double tanp = k ? a1 / a2 : a2 / a1, sec2 = k ? s2 / (a2 * a2) : s2 / (a1 * a1);
+        const double a2k = a * a;
+        const double I0 = phi;
+        const double I_2 = phi + a2k * tanp;
+        const double I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
+        const double logs = 2.0 * atanh(u);
+        const double I1 = atan(u / a);
+        const double I_1 = a / 2. * logs + I1;
+        const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u / (1 - u * u) + logs);
+        const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) / (1 - u * u) / (1 - u * u) + 3. * logs);
         double f;
-        if (r2 < w.h2) {
-            f = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
+        if (inner) {
+            f = r0h3 / kPi * (1. / 6. * I_2 - 3. / 40. * r0h2 * I_4 + 1. / 40. * r0h3 * I_5 + w.B1 / r03 * I0);
         } else {
-            f = r0h3 / kPi * (0.25 * (4. / 3. * s.I_2 - (r0 / h) * s.I_3 + 0.3 * r0h2 * s.I_4 - 1. / 30. * r0h3 * s.I_5 +
-                                      1. / 15. * r0h_3 * s.I1) +
-                              w.B2 / r03 * s.I0 + (k ? D2b : D2a));
+            f = r0h3 / kPi * (0.25 * (4. / 3. * I_2 - (r0 / h) * I_3 + 0.3 * r0h2 * I_4 - 1. / 30. * r0h3 * I_5 +
+                                      1. / 15. * r0h_3 * I1) +
+                              w.B2 / r03 * I0 + (k ? D2b : D2a));
         }
         sum += f;
     }
