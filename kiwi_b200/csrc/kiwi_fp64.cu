@@ -294,6 +294,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGe
 #define KIWI_LATTICE_MIN_BLOCKS 2
 #endif
 constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
+constexpr double kNeedPad = 1.0 + 1e-6;
+constexpr int kLatPtsPerThread = (kLatSCap / 3 + kThreads - 1) / kThreads;  // lattice points per thread in B0
+static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");  // half-width factor of the cells around a lattice point
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatSCap);
 constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;
@@ -319,7 +322,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
     __shared__ int s_np, s_etot, s_stot;
     __shared__ int s_wexp[kThreads / 32], s_wcheap[kThreads / 32];
-    __shared__ unsigned short s_blist[kLatSCap];
+    __shared__ uint32_t s_blist[kLatSCap];
     extern __shared__ double s_dyn[];
     double* s_D2 = s_dyn;
     double* s_D3 = s_dyn + kLatECap;
@@ -426,33 +429,46 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         }
         __syncthreads();
 
-        // (B0) order the corner items so that the cheap ones (corner beyond 2h: only I0 and I1; or a zero
-        // corner) run in warps of their own: the others from the front of s_blist, the cheap ones from
-        // the back.  Results do not depend on this order.
+        // (B0) list the corner items lattice point by lattice point (the three plane orientations of a
+        // point share its offsets and its class), so that the cheap ones (corner beyond 2h: only I0 and
+        // I1; or a zero corner) run in warps of their own: the others from the front of s_blist, the
+        // cheap ones after them.  Results do not depend on this order.  With CULL, a lattice point none
+        // of whose eight cells meets the support sphere is read by no evaluated cell: its items are left
+        // out.  The test bounds the distance to the 2 x 2 x 2 cells around the point, their half-widths
+        // padded by 1e-6 of a cell so that rounding never drops a point an evaluated cell reads.  A list
+        // entry packs (particle, orientation, i, j, k): 5 + 2 + 3 x 4 bits.
+        int nblist = stot;
         if (!GENERIC && !TAB) {
-            unsigned cheap = 0;
-            int nitems = 0;
+            unsigned cheap = 0, skip = 0;
+            int npts = 0;
+            const int ptot = stot / 3;
 #pragma unroll
-            for (int q = 0; q < kLatSCap / kThreads; ++q) {
-                const int it = threadIdx.x + q * kThreads;
-                if (it >= stot) break;
-                ++nitems;
-                const int jp = chunk_search(s_soff, np, it);
-                const int s = it - s_soff[jp];
+            for (int q = 0; q < kLatPtsPerThread; ++q) {
+                const int pt = threadIdx.x + q * kThreads;
+                if (pt >= ptot) break;
+                ++npts;
+                const int jp = chunk_search(s_soff, np, 3 * pt);
+                const int lp = pt - s_soff[jp] / 3;
                 const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-                const int L = (s_dim[jp][0] + 1) * n1 * n2;
-                const int axis = s / L, rem = s % L;
-                const int i = rem / (n1 * n2), jj = (rem / n2) % n1, k = rem % n2;
+                const int i = lp / (n1 * n2), jj = (lp / n2) % n1, k = lp % n2;
                 const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
                 const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
                 const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
-                const double ua = axis == 0 ? ux : (axis == 1 ? uy : uz);
-                const double u1 = axis == 0 ? uy : ux, u2 = axis == 2 ? uy : uz;
                 const double h = s_h[jp];
-                const bool zero = ua == 0.0 || u1 == 0.0 || u2 == 0.0;
-                if (zero || !(ua * ua + (u1 * u1 + u2 * u2) < 4.0 * (h * h))) cheap |= 1u << q;
+                if (CULL) {
+                    const double radius = mul_rn(g.support_in_h, h);
+                    const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
+                    const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
+                    const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
+                    if (!(ex * ex + ey * ey + ez * ez < radius * radius)) {
+                        skip |= 1u << q;
+                        continue;
+                    }
+                }
+                const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
+                if (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) cheap |= 1u << q;
             }
-            const int ncheap = __popc(cheap), nexp = nitems - ncheap;
+            const int ncheap = 3 * __popc(cheap), nexp = 3 * (npts - __popc(cheap) - __popc(skip));
             int ie = nexp, ic = ncheap;
             for (int o = 1; o < 32; o <<= 1) {
                 const int ve = __shfl_up_sync(0xffffffffu, ie, o), vc = __shfl_up_sync(0xffffffffu, ic, o);
@@ -466,30 +482,63 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 s_wcheap[warp] = ic;
             }
             __syncthreads();
-            int be = ie - nexp, bc = ic - ncheap;
-            for (int w = 0; w < warp; ++w) {
-                be += s_wexp[w];
-                bc += s_wcheap[w];
+            int be = ie - nexp, bc = ic - ncheap, texp = 0;
+            nblist = 0;
+            for (int w = 0; w < kThreads / 32; ++w) {
+                if (w < warp) {
+                    be += s_wexp[w];
+                    bc += s_wcheap[w];
+                }
+                texp += s_wexp[w];
+                nblist += s_wexp[w] + s_wcheap[w];
             }
+            bc += texp;
 #pragma unroll
-            for (int q = 0; q < kLatSCap / kThreads; ++q) {
-                const int it = threadIdx.x + q * kThreads;
-                if (it >= stot) break;
-                if (cheap & (1u << q)) s_blist[stot - 1 - bc++] = (unsigned short)it;
-                else s_blist[be++] = (unsigned short)it;
+            for (int q = 0; q < kLatPtsPerThread; ++q) {
+                const int pt = threadIdx.x + q * kThreads;
+                if (pt >= ptot) break;
+                if (skip & (1u << q)) continue;
+                const int jp = chunk_search(s_soff, np, 3 * pt);
+                const int lp = pt - s_soff[jp] / 3;
+                const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                const uint32_t rec = (uint32_t)jp | (uint32_t)(lp / (n1 * n2)) << 7 | (uint32_t)((lp / n2) % n1) << 11 |
+                                     (uint32_t)(lp % n2) << 15;
+                const bool ch = (cheap & (1u << q)) != 0;
+                const int b = ch ? bc : be;
+                s_blist[b] = rec;
+                s_blist[b + 1] = rec | 1u << 5;
+                s_blist[b + 2] = rec | 2u << 5;
+                if (ch) bc += 3;
+                else be += 3;
             }
             __syncthreads();
         }
 
         // (B) corner values S_a(i, j, k) for the three plane orientations a
-        for (int li = threadIdx.x; li < stot; li += kThreads) {
-            const int it = (GENERIC || TAB) ? li : s_blist[li];
-            const int jp = chunk_search(s_soff, np, it);
-            const int s = it - s_soff[jp];
+        for (int li = threadIdx.x; li < nblist; li += kThreads) {
+            int it, jp, axis, i, jj, k;
+            if (GENERIC || TAB) {
+                it = li;
+                jp = chunk_search(s_soff, np, it);
+                const int s = it - s_soff[jp];
+                const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                const int L = (s_dim[jp][0] + 1) * n1 * n2;
+                axis = s / L;
+                const int rem = s % L;
+                i = rem / (n1 * n2);
+                jj = (rem / n2) % n1;
+                k = rem % n2;
+            } else {
+                const uint32_t rec = s_blist[li];
+                jp = (int)(rec & 31u);
+                axis = (int)((rec >> 5) & 3u);
+                i = (int)((rec >> 7) & 15u);
+                jj = (int)((rec >> 11) & 15u);
+                k = (int)((rec >> 15) & 15u);
+                const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                it = s_soff[jp] + axis * ((s_dim[jp][0] + 1) * n1 * n2) + (i * n1 + jj) * n2 + k;
+            }
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-            const int L = n0 * n1 * n2;
-            const int axis = s / L, rem = s % L;
-            const int i = rem / (n1 * n2), jj = (rem / n2) % n1, k = rem % n2;
             const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
             const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
             const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
