@@ -418,14 +418,20 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 ++n_ei;
                 continue;
             }
-            const CubicWall w = cubic_wall(s_h[j], r0);
-            const CubicEdge ed = cubic_edge(w, R0);
-            s_D2[it] = ed.D2;
-            s_D3[it] = ed.D3;
+            const double h = s_h[j], h2 = h * h;
             const double ld2 = r0 * r0 + R0 * R0;
-            if (!ed.valid || ld2 > 4.0 * w.h2) ++n_eo;
-            else if (ld2 > w.h2) ++n_em;
-            else ++n_ei;
+            double D2 = 0.0, D3 = 0.0;
+            if (r0 != 0.0 && R0 != 0.0 && ld2 <= 4.0 * h2) {
+                const LatticeEdge ed = lattice_edge(h, r0, R0);
+                D2 = ed.D2;
+                D3 = ed.D3;
+                if (ld2 > h2) ++n_em;
+                else ++n_ei;
+            } else {
+                ++n_eo;
+            }
+            s_D2[it] = D2;
+            s_D3[it] = D3;
         }
         __syncthreads();
 

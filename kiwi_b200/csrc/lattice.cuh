@@ -64,6 +64,50 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
     return lattice_vertex_t<double>(h, r0, R_0, t, D2, D3);
 }
 
+// The edge tier of one (wall, edge line) pair: D2 (inner edges, line within h) and D3 (line within 2h),
+// src/kernel_integral.cpp:253-350.  The tier evaluates the I-series at the angles phi_H where the distance
+// to the particle along the edge line reaches H = h and 2h (the reference: acos(R_0 / sqrt(H^2 - r0^2)),
+// its sincos, then the series).  Written in the edge's own lengths, with c2 = H^2 - r0^2 and
+// t = sqrt(c2 - R_0^2) (the half-chord of the H-sphere on the line): phi_H = atan2(t, R_0),
+// tan(phi_H) = t / R_0, 1 / cos^2(phi_H) = c2 / R_0^2, and the series variable u = sin(phi) sqrt(1 - mu^2)
+// with mu = r0 / H is t / H, so 1 - u^2 = (r0^2 + R_0^2) / H^2 exactly and
+// log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  No cosine, sine or arccosine is needed.
+// r0, R_0 > 0 and r0^2 + R_0^2 <= 4 h^2 (the caller gives D2 = D3 = 0 otherwise).
+struct LatticeEdge {
+    double D2, D3;
+};
+static __device__ __noinline__ LatticeEdge lattice_edge(double h, double r0, double R_0) {
+    const CubicWall w = cubic_wall(h, r0);
+    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
+    const double a = R_0 / r0, a2 = a * a;
+    const double ld2 = r0 * r0 + R_0 * R_0;
+    double D2 = 0.0, D3 = 0.0;
+#pragma unroll 1
+    for (int pass = (ld2 <= w.h2) ? 0 : 1; pass < 2; ++pass) {
+        const double H = pass == 0 ? h : 2.0 * h;
+        const double c2 = H * H - r0 * r0;
+        const double t = sqrt(fmax(c2 - R_0 * R_0, 0.0));
+        const double phi = atan2(t, R_0);
+        const double tanp = t / R_0, sec2 = c2 / (R_0 * R_0);
+        const double u = t / H, omu2 = ld2 / (H * H);
+        const double logs = log1p(2.0 * u * (1.0 + u) / omu2);
+        const double I0 = phi;
+        const double I_2 = phi + a2 * tanp;
+        const double I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + sec2);
+        const double I1 = atan(u / a);
+        const double I_1 = a / 2. * logs + I1;
+        const double I_3 = I_1 + a * (1. + a2) / 4. * (2 * u / omu2 + logs);
+        const double I_5 = I_3 + a * (1. + a2) * (1. + a2) / 16. * ((10 * u - 6 * u * u * u) / omu2 / omu2 + 3. * logs);
+        if (pass == 0)
+            D2 = -1. / 6. * I_2 + 0.25 * (r0 / h) * I_3 - 0.15 * r0h2 * I_4 + 1. / 30. * r0h3 * I_5 - 1. / 60. * r0h_3 * I1 +
+                 (w.B1 - w.B2) / r03 * I0;
+        else
+            D3 = 1. / 3. * I_2 - 0.25 * (r0 / h) * I_3 + 3. / 40. * r0h2 * I_4 - 1. / 120. * r0h3 * I_5 + 4. / 15. * r0h_3 * I1 +
+                 (w.B2 - w.B3) / r03 * I0 + D2;
+    }
+    return {D2, D3};
+}
+
 // The pyramid pair of one corner value, F(r0, a1, a2) + F(r0, a2, a1): the two right triangles of the
 // rectangle spanned by the particle's projection and the corner (legs a1 along the first edge line and a2
 // along the second, and the reverse), in the wall at distance r0.  The vertex tier's series
