@@ -422,7 +422,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const double ld2 = r0 * r0 + R0 * R0;
             double D2 = 0.0, D3 = 0.0;
             if (r0 != 0.0 && R0 != 0.0 && ld2 <= 4.0 * h2) {
-                const LatticeEdge ed = lattice_edge(h, r0, R0);
+                const LatticeEdge ed = lattice_edge(h, 1.0 / h, r0, R0);
                 D2 = ed.D2;
                 D3 = ed.D3;
                 if (ld2 > h2) ++n_em;
@@ -578,7 +578,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
                         lattice_generic_vertex(K, H, r0, a2, a1, s_E + kLatGenERec * e2);
                 } else {
-                    f = lattice_corner(s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1], s_D2[e2], s_D3[e2]);
+                    f = lattice_corner(s_h[jp], 1.0 / s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1], s_D2[e2], s_D3[e2]);
                 }
                 n_vp += 2;
             }

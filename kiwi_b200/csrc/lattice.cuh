@@ -64,6 +64,33 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
     return lattice_vertex_t<double>(h, r0, R_0, t, D2, D3);
 }
 
+// The wall constants of the cubic spline (src/kernel_integral.cpp:222-247) divided by r0^3, as
+// polynomials in r0 / h and h / r0 (the reference forms B_k = r0^3 / 4 (...) and divides by r0^3 at each
+// use).  Powers from one reciprocal of h and one of r0.
+struct LatticeWall {
+    double r0h, r0h2, r0h3, r0h_2, r0h_3;  // (r0/h)^k and (h/r0)^k
+};
+static __device__ __forceinline__ LatticeWall lattice_wall(double ih, double h, double ir0, double r0) {
+    LatticeWall w;
+    w.r0h = r0 * ih;
+    w.r0h2 = w.r0h * w.r0h;
+    w.r0h3 = w.r0h2 * w.r0h;
+    const double hr0 = h * ir0;
+    w.r0h_2 = hr0 * hr0;
+    w.r0h_3 = w.r0h_2 * hr0;
+    return w;
+}
+// B2 / r0^3 for h < r0 < 2h (its B1 is 0) and for r0 <= h; B1 / r0^3 for r0 <= h; B3 / r0^3 in each range.
+static __device__ __forceinline__ double wall_b2_mid(const LatticeWall& w) {
+    return 0.25 * (-4. / 3. + w.r0h - 0.3 * w.r0h2 + 1. / 30. * w.r0h3 - 1. / 15. * w.r0h_3);
+}
+static __device__ __forceinline__ double wall_b2_in(const LatticeWall& w) {
+    return 0.25 * (-2. / 3. + 0.3 * w.r0h2 - 0.1 * w.r0h3 - 0.2 * w.r0h_2);
+}
+static __device__ __forceinline__ double wall_b1_in(const LatticeWall& w) {
+    return 0.25 * (-2. / 3. + 0.3 * w.r0h2 - 0.1 * w.r0h3);
+}
+
 // The edge tier of one (wall, edge line) pair: D2 (inner edges, line within h) and D3 (line within 2h),
 // src/kernel_integral.cpp:253-350.  The tier evaluates the I-series at the angles phi_H where the distance
 // to the particle along the edge line reaches H = h and 2h (the reference: acos(R_0 / sqrt(H^2 - r0^2)),
@@ -71,39 +98,45 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
 // t = sqrt(c2 - R_0^2) (the half-chord of the H-sphere on the line): phi_H = atan2(t, R_0),
 // tan(phi_H) = t / R_0, 1 / cos^2(phi_H) = c2 / R_0^2, and the series variable u = sin(phi) sqrt(1 - mu^2)
 // with mu = r0 / H is t / H, so 1 - u^2 = (r0^2 + R_0^2) / H^2 exactly and
-// log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  No cosine, sine or arccosine is needed.
-// r0, R_0 > 0 and r0^2 + R_0^2 <= 4 h^2 (the caller gives D2 = D3 = 0 otherwise).
+// log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  No cosine, sine or arccosine is needed, and
+// the ratios come from the reciprocals of h, r0, R_0 and r0^2 + R_0^2.  The wall differences
+// (B1 - B2) / r0^3 and (B2 - B3) / r0^3 are 0.05 (h/r0)^2 and -0.4 (h/r0)^2 within h; -B2 / r0^3 and
+// -0.4 (h/r0)^2 between h and 2h.
+// ih = 1 / h; r0, R_0 > 0 and r0^2 + R_0^2 <= 4 h^2 (the caller gives D2 = D3 = 0 otherwise).
 struct LatticeEdge {
     double D2, D3;
 };
-static __device__ __noinline__ LatticeEdge lattice_edge(double h, double r0, double R_0) {
-    const CubicWall w = cubic_wall(h, r0);
-    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    const double a = R_0 / r0, a2 = a * a;
-    const double ld2 = r0 * r0 + R_0 * R_0;
+static __device__ __noinline__ LatticeEdge lattice_edge(double h, double ih, double r0, double R_0) {
+    const double ir0 = 1.0 / r0, iR0 = 1.0 / R_0;
+    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
+    const double a = R_0 * ir0, a2 = a * a;
+    const double ld2 = r0 * r0 + R_0 * R_0, ild2 = 1.0 / ld2;
+    const double b12 = r0 > h ? -wall_b2_mid(w) : 0.05 * w.r0h_2;
+    const double b23 = -0.4 * w.r0h_2;
+    const double c3 = a * (1. + a2) / 4., c5 = a * (1. + a2) * (1. + a2) / 16.;
     double D2 = 0.0, D3 = 0.0;
 #pragma unroll 1
-    for (int pass = (ld2 <= w.h2) ? 0 : 1; pass < 2; ++pass) {
-        const double H = pass == 0 ? h : 2.0 * h;
+    for (int pass = (ld2 <= h * h) ? 0 : 1; pass < 2; ++pass) {
+        const double H = pass == 0 ? h : 2.0 * h, iH = pass == 0 ? ih : 0.5 * ih;
         const double c2 = H * H - r0 * r0;
         const double t = sqrt(fmax(c2 - R_0 * R_0, 0.0));
         const double phi = atan2(t, R_0);
-        const double tanp = t / R_0, sec2 = c2 / (R_0 * R_0);
-        const double u = t / H, omu2 = ld2 / (H * H);
-        const double logs = log1p(2.0 * u * (1.0 + u) / omu2);
+        const double tanp = t * iR0, sec2 = c2 * iR0 * iR0;
+        const double u = t * iH, iomu2 = H * H * ild2;
+        const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
         const double I0 = phi;
         const double I_2 = phi + a2 * tanp;
         const double I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + sec2);
-        const double I1 = atan(u / a);
+        const double I1 = atan(u * r0 * iR0);
         const double I_1 = a / 2. * logs + I1;
-        const double I_3 = I_1 + a * (1. + a2) / 4. * (2 * u / omu2 + logs);
-        const double I_5 = I_3 + a * (1. + a2) * (1. + a2) / 16. * ((10 * u - 6 * u * u * u) / omu2 / omu2 + 3. * logs);
+        const double I_3 = I_1 + c3 * (2 * u * iomu2 + logs);
+        const double I_5 = I_3 + c5 * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
         if (pass == 0)
-            D2 = -1. / 6. * I_2 + 0.25 * (r0 / h) * I_3 - 0.15 * r0h2 * I_4 + 1. / 30. * r0h3 * I_5 - 1. / 60. * r0h_3 * I1 +
-                 (w.B1 - w.B2) / r03 * I0;
+            D2 = -1. / 6. * I_2 + 0.25 * w.r0h * I_3 - 0.15 * w.r0h2 * I_4 + 1. / 30. * w.r0h3 * I_5 -
+                 1. / 60. * w.r0h_3 * I1 + b12 * I0;
         else
-            D3 = 1. / 3. * I_2 - 0.25 * (r0 / h) * I_3 + 3. / 40. * r0h2 * I_4 - 1. / 120. * r0h3 * I_5 + 4. / 15. * r0h_3 * I1 +
-                 (w.B2 - w.B3) / r03 * I0 + D2;
+            D3 = 1. / 3. * I_2 - 0.25 * w.r0h * I_3 + 3. / 40. * w.r0h2 * I_4 - 1. / 120. * w.r0h3 * I_5 +
+                 4. / 15. * w.r0h_3 * I1 + b23 * I0 + D2;
     }
     return {D2, D3};
 }
@@ -113,23 +146,29 @@ static __device__ __noinline__ LatticeEdge lattice_edge(double h, double r0, dou
 // along the second, and the reverse), in the wall at distance r0.  The vertex tier's series
 // (src/kernel_integral.cpp:356-400) is written here in the triangle's own lengths, which the pair shares:
 // with r the distance to the corner, the series variable u = sin(phi) sqrt(1 - mu^2) is a2 / r for the
-// first pyramid and a1 / r for the second, tan(phi) = a2 / a1 (a1 / a2), 1 / cos^2(phi) = (a1^2 + a2^2) / a1^2
-// (/ a2^2), and the two angles sum to pi/2 (the smaller one is taken by atan2, the larger as its complement,
-// both to an ulp).  log(1 + u) - log(1 - u) is 2 atanh(u).  Beyond 2h a tier needs I0 = phi and I1 only,
-// so the pair there needs no angle at all.  The wall constants are computed once for the pair.
-// r0, a1, a2 > 0 (the callers skip zero corners); (D2a, D3a) and (D2b, D3b) are the two edge tiers.
-static __device__ __noinline__ double lattice_corner(double h, double r0, double a1, double a2, double D2a,
+// first pyramid and a1 / r for the second (so 1 - u^2 = (r0^2 + a1^2) / r^2, (r0^2 + a2^2) / r^2 exactly),
+// tan(phi) = a2 / a1 (a1 / a2), 1 / cos^2(phi) = (a1^2 + a2^2) / a1^2 (/ a2^2), u / a = a2 r0 / (a1 r)
+// (a1 r0 / (a2 r)), and the two angles sum to pi/2 (the smaller one is taken by atan2, the larger as its
+// complement, both to an ulp).  log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  The ratios
+// come from the reciprocals of h, r0, r, a1, a2 and the two 1 - u^2.  Beyond 2h a tier needs I0 = phi
+// and I1 only: the angles sum to pi/2 and I1a + I1b = atan(r0 r / (a1 a2)) (tan of the sum of the two
+// arctangents), so the pair is one arctangent; for r0 >= 2h, where B3 / r0^3 = (h/r0)^3 / 4, the pair is
+// (h/r0)^3 / 4 atan(a1 a2 / (r0 r)).  ih = 1 / h; r0, a1, a2 > 0 (the callers skip zero corners);
+// (D2a, D3a) and (D2b, D3b) are the two edge tiers.
+static __device__ __noinline__ double lattice_corner(double h, double ih, double r0, double a1, double a2, double D2a,
                                                      double D3a, double D2b, double D3b) {
-    const CubicWall w = cubic_wall(h, r0);
+    const double ir0 = 1.0 / r0;
+    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
     const double s2 = a1 * a1 + a2 * a2;
     const double r2 = r0 * r0 + s2;
     const double r = sqrt(r2);
-    const double r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    const double aa = a1 / r0, ab = a2 / r0;
-    const double ua = a2 / r, ub = a1 / r;
-    if (!(r2 < 4.0 * w.h2)) {
-        const double I1a = atan(ua / aa), I1b = atan(ub / ab);
-        return r0h3 / kPi * (-0.25 * r0h_3 * (I1a + I1b) + w.B3 / r03 * (0.5 * kPi) + D3a + D3b);
+    const double K = w.r0h3 * (1.0 / kPi);
+    if (!(r2 < 4.0 * (h * h))) {
+        if (r0 >= 2.0 * h) return K * (0.25 * w.r0h_3 * atan(a1 * a2 / (r0 * r)) + D3a + D3b);
+        const double b3 = r0 > h ? 0.25 * (-4. / 3. + w.r0h - 0.3 * w.r0h2 + 1. / 30. * w.r0h3 - 1. / 15. * w.r0h_3 +
+                                           8. / 5. * w.r0h_2)
+                                 : 0.25 * (-2. / 3. + 0.3 * w.r0h2 - 0.1 * w.r0h3 + 7. / 5. * w.r0h_2);
+        return K * (-0.25 * w.r0h_3 * atan(r0 * r / (a1 * a2)) + b3 * (0.5 * kPi) + D3a + D3b);
     }
     double pa, pb;
     if (a2 <= a1) {
@@ -139,28 +178,34 @@ static __device__ __noinline__ double lattice_corner(double h, double r0, double
         pb = atan2(a1, a2);
         pa = 0.5 * kPi - pb;
     }
-    const bool inner = r2 < w.h2;
+    const bool inner = r2 < h * h;
+    const double b1 = inner ? wall_b1_in(w) : 0.0;
+    const double b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
+    const double ir = 1.0 / r, ia1 = 1.0 / a1, ia2 = 1.0 / a2;
+    const double r0r = r0 * ir;
     double sum = 0.0;
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
-        const double a = k ? ab : aa, u = k ? ub : ua, phi = k ? pb : pa;
-        const double tanp = k ? a1 / a2 : a2 / a1, sec2 = k ? s2 / (a2 * a2) : s2 / (a1 * a1);
+        const double leg = k ? a2 : a1, opp = k ? a1 : a2, ileg = k ? ia2 : ia1, phi = k ? pb : pa;
+        const double a = leg * ir0, u = opp * ir;
+        const double tanp = opp * ileg, sec2 = s2 * ileg * ileg;
+        const double iomu2 = r2 / (r0 * r0 + leg * leg);
         const double a2k = a * a;
         const double I0 = phi;
         const double I_2 = phi + a2k * tanp;
         const double I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
-        const double logs = 2.0 * atanh(u);
-        const double I1 = atan(u / a);
+        const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
+        const double I1 = atan(tanp * r0r);
         const double I_1 = a / 2. * logs + I1;
-        const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u / (1 - u * u) + logs);
-        const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) / (1 - u * u) / (1 - u * u) + 3. * logs);
+        const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
+        const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
         double f;
         if (inner) {
-            f = r0h3 / kPi * (1. / 6. * I_2 - 3. / 40. * r0h2 * I_4 + 1. / 40. * r0h3 * I_5 + w.B1 / r03 * I0);
+            f = K * (1. / 6. * I_2 - 3. / 40. * w.r0h2 * I_4 + 1. / 40. * w.r0h3 * I_5 + b1 * I0);
         } else {
-            f = r0h3 / kPi * (0.25 * (4. / 3. * I_2 - (r0 / h) * I_3 + 0.3 * r0h2 * I_4 - 1. / 30. * r0h3 * I_5 +
-                                      1. / 15. * r0h_3 * I1) +
-                              w.B2 / r03 * I0 + (k ? D2b : D2a));
+            f = K * (0.25 * (4. / 3. * I_2 - w.r0h * I_3 + 0.3 * w.r0h2 * I_4 - 1. / 30. * w.r0h3 * I_5 +
+                             1. / 15. * w.r0h_3 * I1) +
+                     b2 * I0 + (k ? D2b : D2a));
         }
         sum += f;
     }
