@@ -318,7 +318,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                                              int64_t t_range, int64_t t, const CartOutputs& out,
                                              DevStats* __restrict__ st, int kernel = 0, const TabDev tab = TabDev{}) {
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
-        s_vy[kLatPMax], s_vz[kLatPMax];
+        s_vy[kLatPMax], s_vz[kLatPMax], s_ih[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
     __shared__ int s_np, s_etot, s_stot;
     __shared__ int s_wexp[kThreads / 32], s_wcheap[kThreads / 32];
@@ -374,7 +374,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const bool take = (idx < end) && ie <= kECap && is <= kLatSCap;
             const int np = __popc(__ballot_sync(0xffffffffu, take));
             if (take) {
-                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph;
+                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph; s_ih[lane] = 1.0 / ph;
                 s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
                 s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
                 s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
@@ -422,7 +422,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const double ld2 = r0 * r0 + R0 * R0;
             double D2 = 0.0, D3 = 0.0;
             if (r0 != 0.0 && R0 != 0.0 && ld2 <= 4.0 * h2) {
-                const LatticeEdge ed = lattice_edge(h, 1.0 / h, r0, R0);
+                const LatticeEdge ed = lattice_edge(h, s_ih[j], r0, R0);
                 D2 = ed.D2;
                 D3 = ed.D3;
                 if (ld2 > h2) ++n_em;
@@ -578,7 +578,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
                         lattice_generic_vertex(K, H, r0, a2, a1, s_E + kLatGenERec * e2);
                 } else {
-                    f = lattice_corner(s_h[jp], 1.0 / s_h[jp], r0, a1, a2, s_D2[e1], s_D3[e1], s_D2[e2], s_D3[e2]);
+                    f = lattice_corner(s_h[jp], s_ih[jp], r0, a1, a2, s_D2[e1], s_D3[e1], s_D2[e2], s_D3[e2]);
                 }
                 n_vp += 2;
             }

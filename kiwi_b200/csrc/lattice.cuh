@@ -99,7 +99,7 @@ static __device__ __forceinline__ double wall_b1_in(const LatticeWall& w) {
 // tan(phi_H) = t / R_0, 1 / cos^2(phi_H) = c2 / R_0^2, and the series variable u = sin(phi) sqrt(1 - mu^2)
 // with mu = r0 / H is t / H, so 1 - u^2 = (r0^2 + R_0^2) / H^2 exactly and
 // log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  No cosine, sine or arccosine is needed, and
-// the ratios come from the reciprocals of h, r0, R_0 and r0^2 + R_0^2.  The wall differences
+// the ratios come from the reciprocal of h and one of r0 R_0 (r0^2 + R_0^2).  The wall differences
 // (B1 - B2) / r0^3 and (B2 - B3) / r0^3 are 0.05 (h/r0)^2 and -0.4 (h/r0)^2 within h; -B2 / r0^3 and
 // -0.4 (h/r0)^2 between h and 2h.
 // ih = 1 / h; r0, R_0 > 0 and r0^2 + R_0^2 <= 4 h^2 (the caller gives D2 = D3 = 0 otherwise).
@@ -107,10 +107,11 @@ struct LatticeEdge {
     double D2, D3;
 };
 static __device__ __noinline__ LatticeEdge lattice_edge(double h, double ih, double r0, double R_0) {
-    const double ir0 = 1.0 / r0, iR0 = 1.0 / R_0;
+    const double ld2 = r0 * r0 + R_0 * R_0;
+    const double inv = 1.0 / (r0 * R_0 * ld2);
+    const double ir0 = R_0 * ld2 * inv, iR0 = r0 * ld2 * inv, ild2 = r0 * R_0 * inv;
     const LatticeWall w = lattice_wall(ih, h, ir0, r0);
     const double a = R_0 * ir0, a2 = a * a;
-    const double ld2 = r0 * r0 + R_0 * R_0, ild2 = 1.0 / ld2;
     const double b12 = r0 > h ? -wall_b2_mid(w) : 0.05 * w.r0h_2;
     const double b23 = -0.4 * w.r0h_2;
     const double c3 = a * (1. + a2) / 4., c5 = a * (1. + a2) * (1. + a2) / 16.;
@@ -148,40 +149,46 @@ static __device__ __noinline__ LatticeEdge lattice_edge(double h, double ih, dou
 // with r the distance to the corner, the series variable u = sin(phi) sqrt(1 - mu^2) is a2 / r for the
 // first pyramid and a1 / r for the second (so 1 - u^2 = (r0^2 + a1^2) / r^2, (r0^2 + a2^2) / r^2 exactly),
 // tan(phi) = a2 / a1 (a1 / a2), 1 / cos^2(phi) = (a1^2 + a2^2) / a1^2 (/ a2^2), u / a = a2 r0 / (a1 r)
-// (a1 r0 / (a2 r)), and the two angles sum to pi/2 (the smaller one is taken by atan2, the larger as its
-// complement, both to an ulp).  log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  The ratios
-// come from the reciprocals of h, r0, r, a1, a2 and the two 1 - u^2.  Beyond 2h a tier needs I0 = phi
-// and I1 only: the angles sum to pi/2 and I1a + I1b = atan(r0 r / (a1 a2)) (tan of the sum of the two
-// arctangents), so the pair is one arctangent; for r0 >= 2h, where B3 / r0^3 = (h/r0)^3 / 4, the pair is
-// (h/r0)^3 / 4 atan(a1 a2 / (r0 r)).  ih = 1 / h; r0, a1, a2 > 0 (the callers skip zero corners);
-// (D2a, D3a) and (D2b, D3b) are the two edge tiers.
+// (a1 r0 / (a2 r)), and the two angles sum to pi/2 (the smaller one is the arctangent of its tangent, the
+// larger its complement, both to an ulp).  log(1 + u) - log(1 - u) = log1p(2 u (1 + u) / (1 - u^2)).  The
+// ratios come from two reciprocals: of r0 r a1 a2 and of (r0^2 + a1^2)(r0^2 + a2^2).  Beyond 2h a tier
+// needs I0 = phi and I1 only: the angles sum to pi/2 and I1a + I1b = atan(r0 r / (a1 a2)) (tan of the sum
+// of the two arctangents), so the pair is one arctangent, and with the prefactor (r0/h)^3 / pi multiplied
+// in, the wall term B3 / r0^3 x pi/2 is a polynomial in r0 / h: the pair needs no reciprocal of r0.  For
+// r0 >= 2h (B3 / r0^3 = (h/r0)^3 / 4) it is atan(a1 a2 / (r0 r)) / (4 pi).  ih = 1 / h; r0, a1, a2 > 0 (the
+// callers skip zero corners); (D2a, D3a) and (D2b, D3b) are the two edge tiers.
 static __device__ __noinline__ double lattice_corner(double h, double ih, double r0, double a1, double a2, double D2a,
                                                      double D3a, double D2b, double D3b) {
-    const double ir0 = 1.0 / r0;
-    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
     const double s2 = a1 * a1 + a2 * a2;
     const double r2 = r0 * r0 + s2;
     const double r = sqrt(r2);
-    const double K = w.r0h3 * (1.0 / kPi);
     if (!(r2 < 4.0 * (h * h))) {
-        if (r0 >= 2.0 * h) return K * (0.25 * w.r0h_3 * atan(a1 * a2 / (r0 * r)) + D3a + D3b);
-        const double b3 = r0 > h ? 0.25 * (-4. / 3. + w.r0h - 0.3 * w.r0h2 + 1. / 30. * w.r0h3 - 1. / 15. * w.r0h_3 +
-                                           8. / 5. * w.r0h_2)
-                                 : 0.25 * (-2. / 3. + 0.3 * w.r0h2 - 0.1 * w.r0h3 + 7. / 5. * w.r0h_2);
-        return K * (-0.25 * w.r0h_3 * atan(r0 * r / (a1 * a2)) + b3 * (0.5 * kPi) + D3a + D3b);
+        const double x = r0 * ih, x2 = x * x, x3 = x2 * x;
+        const double K = x3 * (1.0 / kPi);
+        if (r0 >= 2.0 * h) return 0.25 / kPi * atan(a1 * a2 / (r0 * r)) + K * (D3a + D3b);
+        const double x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
+        const double p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
+                                : -2. / 3. * x3 + 0.3 * x5 - 0.1 * x6 + 7. / 5. * x;
+        return -0.25 / kPi * atan(r0 * r / (a1 * a2)) + 0.125 * p + K * (D3a + D3b);
     }
+    const double inv1 = 1.0 / (r0 * r * (a1 * a2));
+    const double ir0 = r * (a1 * a2) * inv1, ir = r0 * (a1 * a2) * inv1;
+    const double ia1 = r0 * r * a2 * inv1, ia2 = r0 * r * a1 * inv1;
+    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
+    const double K = w.r0h3 * (1.0 / kPi);
     double pa, pb;
     if (a2 <= a1) {
-        pa = atan2(a2, a1);
+        pa = atan(a2 * ia1);
         pb = 0.5 * kPi - pa;
     } else {
-        pb = atan2(a1, a2);
+        pb = atan(a1 * ia2);
         pa = 0.5 * kPi - pb;
     }
     const bool inner = r2 < h * h;
     const double b1 = inner ? wall_b1_in(w) : 0.0;
     const double b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
-    const double ir = 1.0 / r, ia1 = 1.0 / a1, ia2 = 1.0 / a2;
+    const double q1 = r0 * r0 + a1 * a1, q2 = r0 * r0 + a2 * a2;
+    const double inv2 = 1.0 / (q1 * q2);
     const double r0r = r0 * ir;
     double sum = 0.0;
 #pragma unroll 1
@@ -189,7 +196,7 @@ static __device__ __noinline__ double lattice_corner(double h, double ih, double
         const double leg = k ? a2 : a1, opp = k ? a1 : a2, ileg = k ? ia2 : ia1, phi = k ? pb : pa;
         const double a = leg * ir0, u = opp * ir;
         const double tanp = opp * ileg, sec2 = s2 * ileg * ileg;
-        const double iomu2 = r2 / (r0 * r0 + leg * leg);
+        const double iomu2 = r2 * (k ? q1 : q2) * inv2;
         const double a2k = a * a;
         const double I0 = phi;
         const double I_2 = phi + a2k * tanp;
