@@ -295,8 +295,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGe
 #endif
 constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 constexpr double kNeedPad = 1.0 + 1e-6;
-constexpr int kLatPtsPerThread = (kLatSCap / 3 + kThreads - 1) / kThreads;  // lattice points per thread in B0
-static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");  // half-width factor of the cells around a lattice point
+static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");
+static_assert(kLatECap <= 2048, "packed edge-list entries");  // half-width factor of the cells around a lattice point
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatSCap);
 constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;
@@ -320,9 +320,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
         s_vy[kLatPMax], s_vz[kLatPMax], s_ih[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
-    __shared__ int s_np, s_etot, s_stot;
-    __shared__ int s_wexp[kThreads / 32], s_wcheap[kThreads / 32];
+    __shared__ int s_np, s_etot, s_stot, s_nexp, s_ncheap, s_nheavy;
     __shared__ uint32_t s_blist[kLatSCap];
+    __shared__ uint16_t s_hlist[kLatECap];
     extern __shared__ double s_dyn[];
     double* s_D2 = s_dyn;
     double* s_D3 = s_dyn + kLatECap;
@@ -385,140 +385,140 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 s_np = np;
                 s_etot = ie;
                 s_stot = is;
+                s_nexp = s_ncheap = s_nheavy = 0;
             }
         }
         __syncthreads();
         const int np = s_np, etot = s_etot, stot = s_stot;
 
-        // (A) edge tiers: block (a, b) holds r0 along axis a, R_0 along axis b
-        for (int it = threadIdx.x; it < etot; it += kThreads) {
-            const int j = chunk_search(s_eoff, np, it);
-            int e = it - s_eoff[j];
-            const int n[3] = {s_dim[j][0] + 1, s_dim[j][1] + 1, s_dim[j][2] + 1};
-            // blocks in order xy, xz, yx, yz, zx, zy
-            int a = 0, bax = 1;
-            {
-                const int sz[6] = {n[0] * n[1], n[0] * n[2], n[1] * n[0], n[1] * n[2], n[2] * n[0], n[2] * n[1]};
-                const int aa[6] = {0, 0, 1, 1, 2, 2}, bb[6] = {1, 2, 0, 2, 0, 1};
-                int blk = 0;
-                while (e >= sz[blk]) {
-                    e -= sz[blk];
-                    ++blk;
+        // (A) edge tiers: block (a, b) holds r0 along axis a, R_0 along axis b.  Cubic: edges beyond 2h
+        // (and zero ones) get D2 = D3 = 0 here; the others are appended to s_hlist (edge slot | particle
+        // << 11) with r0, R_0 parked in their slots, and evaluated in (A2) by full warps.  Appends are
+        // warp-aggregated; the list order does not affect the results.
+        for (int base = warp * 32; base < etot; base += kThreads) {
+            const int it = base + lane;
+            bool heavy = false;
+            int j = 0;
+            if (it < etot) {
+                j = chunk_search(s_eoff, np, it);
+                int e = it - s_eoff[j];
+                const int n[3] = {s_dim[j][0] + 1, s_dim[j][1] + 1, s_dim[j][2] + 1};
+                // blocks in order xy, xz, yx, yz, zx, zy
+                int a = 0, bax = 1;
+                {
+                    const int sz[6] = {n[0] * n[1], n[0] * n[2], n[1] * n[0], n[1] * n[2], n[2] * n[0], n[2] * n[1]};
+                    const int aa[6] = {0, 0, 1, 1, 2, 2}, bb[6] = {1, 2, 0, 2, 0, 1};
+                    int blk = 0;
+                    while (e >= sz[blk]) {
+                        e -= sz[blk];
+                        ++blk;
+                    }
+                    a = aa[blk];
+                    bax = bb[blk];
                 }
-                a = aa[blk];
-                bax = bb[blk];
+                const int p = e / n[bax], q = e % n[bax];
+                const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
+                const double pc[3] = {s_x[j], s_y[j], s_z[j]};
+                const double r0 = fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
+                const double R0 = fabs(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]));
+                if (GENERIC) {
+                    lattice_generic_edge(K, mul_rn(g.support_in_h, s_h[j]), r0, R0, s_E + kLatGenERec * it);
+                    ++n_ei;
+                } else {
+                    const double h2 = s_h[j] * s_h[j];
+                    const double ld2 = r0 * r0 + R0 * R0;
+                    heavy = r0 != 0.0 && R0 != 0.0 && ld2 <= 4.0 * h2;
+                    if (heavy) {
+                        if (ld2 > h2) ++n_em;
+                        else ++n_ei;
+                        s_D2[it] = r0;
+                        s_D3[it] = R0;
+                    } else {
+                        ++n_eo;
+                        s_D2[it] = 0.0;
+                        s_D3[it] = 0.0;
+                    }
+                }
             }
-            const int p = e / n[bax], q = e % n[bax];
-            const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
-            const double pc[3] = {s_x[j], s_y[j], s_z[j]};
-            const double r0 = fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
-            const double R0 = fabs(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]));
-            if (GENERIC) {
-                lattice_generic_edge(K, mul_rn(g.support_in_h, s_h[j]), r0, R0, s_E + kLatGenERec * it);
-                ++n_ei;
-                continue;
+            if (!GENERIC) {
+                const unsigned m = __ballot_sync(0xffffffffu, heavy);
+                int pos = 0;
+                if (lane == 0 && m) pos = atomicAdd(&s_nheavy, __popc(m));
+                pos = __shfl_sync(0xffffffffu, pos, 0);
+                if (heavy) s_hlist[pos + __popc(m & ((1u << lane) - 1))] = (uint16_t)(it | j << 11);
             }
-            const double h = s_h[j], h2 = h * h;
-            const double ld2 = r0 * r0 + R0 * R0;
-            double D2 = 0.0, D3 = 0.0;
-            if (r0 != 0.0 && R0 != 0.0 && ld2 <= 4.0 * h2) {
-                const LatticeEdge ed = lattice_edge(h, s_ih[j], r0, R0);
-                D2 = ed.D2;
-                D3 = ed.D3;
-                if (ld2 > h2) ++n_em;
-                else ++n_ei;
-            } else {
-                ++n_eo;
-            }
-            s_D2[it] = D2;
-            s_D3[it] = D3;
         }
-        __syncthreads();
 
         // (B0) list the corner items lattice point by lattice point (the three plane orientations of a
         // point share its offsets and its class), so that the cheap ones (corner beyond 2h: only I0 and
         // I1; or a zero corner) run in warps of their own: the others from the front of s_blist, the
-        // cheap ones after them.  Results do not depend on this order.  With CULL, a lattice point none
-        // of whose eight cells meets the support sphere is read by no evaluated cell: its items are left
-        // out.  The test bounds the distance to the 2 x 2 x 2 cells around the point, their half-widths
-        // padded by 1e-6 of a cell so that rounding never drops a point an evaluated cell reads.  A list
-        // entry packs (particle, orientation, i, j, k): 5 + 2 + 3 x 4 bits.
-        int nblist = stot;
+        // cheap ones from its end.  Appends are warp-aggregated; results do not depend on the order.
+        // With CULL, a lattice point none of whose eight cells meets the support sphere is read by no
+        // evaluated cell: its items are left out.  The test bounds the distance to the 2 x 2 x 2 cells
+        // around the point, their half-widths padded by 1e-6 of a cell so that rounding never drops a point
+        // an evaluated cell reads.  A list entry packs (particle, orientation, i, j, k): 5 + 2 + 3 x 4 bits.
         if (!GENERIC && !TAB) {
-            unsigned cheap = 0, skip = 0;
-            int npts = 0;
             const int ptot = stot / 3;
-#pragma unroll
-            for (int q = 0; q < kLatPtsPerThread; ++q) {
-                const int pt = threadIdx.x + q * kThreads;
-                if (pt >= ptot) break;
-                ++npts;
-                const int jp = chunk_search(s_soff, np, 3 * pt);
-                const int lp = pt - s_soff[jp] / 3;
-                const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-                const int i = lp / (n1 * n2), jj = (lp / n2) % n1, k = lp % n2;
-                const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
-                const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
-                const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
-                const double h = s_h[jp];
-                if (CULL) {
-                    const double radius = mul_rn(g.support_in_h, h);
-                    const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
-                    const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
-                    const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
-                    if (!(ex * ex + ey * ey + ez * ez < radius * radius)) {
-                        skip |= 1u << q;
-                        continue;
+            for (int base = warp * 32; base < ptot; base += kThreads) {
+                const int pt = base + lane;
+                int cls = -1;  // -1 none, 0 general, 1 cheap
+                uint32_t rec = 0;
+                if (pt < ptot) {
+                    const int jp = chunk_search(s_soff, np, 3 * pt);
+                    const int lp = pt - s_soff[jp] / 3;
+                    const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                    const int i = lp / (n1 * n2), jj = (lp / n2) % n1, k = lp % n2;
+                    const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
+                    const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
+                    const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+                    const double h = s_h[jp];
+                    bool keep = true;
+                    if (CULL) {
+                        const double radius = mul_rn(g.support_in_h, h);
+                        const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
+                        const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
+                        const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
+                        keep = ex * ex + ey * ey + ez * ez < radius * radius;
+                    }
+                    if (keep) {
+                        const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
+                        cls = (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) ? 1 : 0;
+                        rec = (uint32_t)jp | (uint32_t)i << 7 | (uint32_t)jj << 11 | (uint32_t)k << 15;
                     }
                 }
-                const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
-                if (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) cheap |= 1u << q;
-            }
-            const int ncheap = 3 * __popc(cheap), nexp = 3 * (npts - __popc(cheap) - __popc(skip));
-            int ie = nexp, ic = ncheap;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vc = __shfl_up_sync(0xffffffffu, ic, o);
-                if (lane >= o) {
-                    ie += ve;
-                    ic += vc;
+                const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
+                int pe = 0, pcb = 0;
+                if (lane == 0) {
+                    if (me) pe = atomicAdd(&s_nexp, 3 * __popc(me));
+                    if (mc) pcb = atomicAdd(&s_ncheap, 3 * __popc(mc));
+                }
+                pe = __shfl_sync(0xffffffffu, pe, 0);
+                pcb = __shfl_sync(0xffffffffu, pcb, 0);
+                const unsigned below = (1u << lane) - 1;
+                if (cls >= 0) {
+                    const int b = cls == 0 ? pe + 3 * __popc(me & below) : kLatSCap - 3 - pcb - 3 * __popc(mc & below);
+                    s_blist[b] = rec;
+                    s_blist[b + 1] = rec | 1u << 5;
+                    s_blist[b + 2] = rec | 2u << 5;
                 }
             }
-            if (lane == 31) {
-                s_wexp[warp] = ie;
-                s_wcheap[warp] = ic;
-            }
-            __syncthreads();
-            int be = ie - nexp, bc = ic - ncheap, texp = 0;
-            nblist = 0;
-            for (int w = 0; w < kThreads / 32; ++w) {
-                if (w < warp) {
-                    be += s_wexp[w];
-                    bc += s_wcheap[w];
-                }
-                texp += s_wexp[w];
-                nblist += s_wexp[w] + s_wcheap[w];
-            }
-            bc += texp;
-#pragma unroll
-            for (int q = 0; q < kLatPtsPerThread; ++q) {
-                const int pt = threadIdx.x + q * kThreads;
-                if (pt >= ptot) break;
-                if (skip & (1u << q)) continue;
-                const int jp = chunk_search(s_soff, np, 3 * pt);
-                const int lp = pt - s_soff[jp] / 3;
-                const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-                const uint32_t rec = (uint32_t)jp | (uint32_t)(lp / (n1 * n2)) << 7 | (uint32_t)((lp / n2) % n1) << 11 |
-                                     (uint32_t)(lp % n2) << 15;
-                const bool ch = (cheap & (1u << q)) != 0;
-                const int b = ch ? bc : be;
-                s_blist[b] = rec;
-                s_blist[b + 1] = rec | 1u << 5;
-                s_blist[b + 2] = rec | 2u << 5;
-                if (ch) bc += 3;
-                else be += 3;
+        }
+        __syncthreads();
+
+        // (A2) the listed edges (cubic)
+        if (!GENERIC) {
+            const int nheavy = s_nheavy;
+            for (int li = threadIdx.x; li < nheavy; li += kThreads) {
+                const int rec = s_hlist[li];
+                const int it = rec & 2047, j = rec >> 11;
+                const LatticeEdge ed = lattice_edge(s_h[j], s_ih[j], s_D2[it], s_D3[it]);
+                s_D2[it] = ed.D2;
+                s_D3[it] = ed.D3;
             }
             __syncthreads();
         }
+        const int nexp = s_nexp, ncheap = s_ncheap;
+        const int nblist = (GENERIC || TAB) ? stot : nexp + ncheap;
 
         // (B) corner values S_a(i, j, k) for the three plane orientations a
         for (int li = threadIdx.x; li < nblist; li += kThreads) {
@@ -535,7 +535,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 jj = (rem / n2) % n1;
                 k = rem % n2;
             } else {
-                const uint32_t rec = s_blist[li];
+                const uint32_t rec = s_blist[li < nexp ? li : kLatSCap - ncheap + (li - nexp)];
                 jp = (int)(rec & 31u);
                 axis = (int)((rec >> 5) & 3u);
                 i = (int)((rec >> 7) & 15u);
