@@ -189,7 +189,6 @@ static __device__ __noinline__ double lattice_corner(double h, double ih, double
     const double b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
     const double q1 = r0 * r0 + a1 * a1, q2 = r0 * r0 + a2 * a2;
     const double inv2 = 1.0 / (q1 * q2);
-    const double r0r = r0 * ir;
     double sum = 0.0;
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
@@ -202,21 +201,20 @@ static __device__ __noinline__ double lattice_corner(double h, double ih, double
         const double I_2 = phi + a2k * tanp;
         const double I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
         const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
-        const double I1 = atan(tanp * r0r);
-        const double I_1 = a / 2. * logs + I1;
+        // I_1, I_3, I_5 without their common I1 term (added below for the pair)
+        const double I_1 = a / 2. * logs;
         const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
         const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
-        double f;
-        if (inner) {
-            f = K * (1. / 6. * I_2 - 3. / 40. * w.r0h2 * I_4 + 1. / 40. * w.r0h3 * I_5 + b1 * I0);
-        } else {
-            f = K * (0.25 * (4. / 3. * I_2 - w.r0h * I_3 + 0.3 * w.r0h2 * I_4 - 1. / 30. * w.r0h3 * I_5 +
-                             1. / 15. * w.r0h_3 * I1) +
-                     b2 * I0 + (k ? D2b : D2a));
-        }
-        sum += f;
+        if (inner) sum += 1. / 6. * I_2 - 3. / 40. * w.r0h2 * I_4 + 1. / 40. * w.r0h3 * I_5 + b1 * I0;
+        else
+            sum += 0.25 * (4. / 3. * I_2 - w.r0h * I_3 + 0.3 * w.r0h2 * I_4 - 1. / 30. * w.r0h3 * I_5) + b2 * I0 +
+                   (k ? D2b : D2a);
     }
-    return sum;
+    // I1 enters both pyramids with one coefficient (through I_1, I_3, I_5 and, between h and 2h, on its own):
+    // the pair needs I1a + I1b = atan(r0 r / (a1 a2)) only.
+    const double I1s = atan((r0 * r) * (r0 * r) * inv1);
+    const double c1 = inner ? 1. / 40. * w.r0h3 : 0.25 * (-w.r0h - 1. / 30. * w.r0h3 + 1. / 15. * w.r0h_3);
+    return K * (sum + c1 * I1s);
 }
 
 // Position of the smallest j with s_off[j] <= it among the chunk's np particles (s_off ascending).
