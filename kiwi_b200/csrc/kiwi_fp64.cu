@@ -3,6 +3,8 @@
 // rounds exactly as in the reference's x86-64 build (see kiwi_math.cuh).
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include "engine.hpp"
 #include "kiwi_math.cuh"
 #include "lattice.cuh"
@@ -312,6 +314,20 @@ constexpr size_t kLatTabDynSmem = sizeof(double) * kLatSCap;
 // cubic closed form; the edge tiers are then lattice_generic_edge records and the corner items run in
 // their natural order.  TAB: the tabulated cubic integral (lookups in `tab`): no edge tiers, and a corner
 // value is two lookups.
+// The chunk particle that owns item base + lane, for a warp whose 32 items start at base (a multiple of
+// 32): off is this lane's particle's first item (lane < np; INT_MAX beyond).  Every particle owns at least
+// one item, so the particles starting inside the window are distinct bits of one mask.  All 32 lanes call.
+__device__ __forceinline__ int warp_owner(int base, int off, int lane) {
+    const unsigned before = __ballot_sync(0xffffffffu, off <= base);
+    const int d = off - base;
+    const unsigned starts = __reduce_or_sync(0xffffffffu, (d > 0 && d < 32) ? 1u << d : 0u);
+    return __popc(before) - 1 + __popc(starts & (0xffffffffu >> (31 - lane)));
+}
+
+// x / n for 0 <= x < 1400 and 1 <= n <= 81 as (x * magic(n)) >> 20 (exact over that range).
+__host__ __device__ __forceinline__ uint32_t div_magic(int n) { return ((1u << 20) + (uint32_t)n - 1) / (uint32_t)n; }
+__device__ __forceinline__ int div_by(int x, uint32_t m) { return (int)(((uint32_t)x * m) >> 20); }
+
 template <bool CULL, bool GENERIC = false, bool TAB = false>
 __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
                                              const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
@@ -320,6 +336,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
         s_vy[kLatPMax], s_vz[kLatPMax], s_ih[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
+    __shared__ uint32_t s_mag[kLatPMax][4];  // div_magic of n0, n1, n2 and n1 n2
     __shared__ int s_np, s_etot, s_stot, s_nexp, s_ncheap, s_nheavy;
     __shared__ uint32_t s_blist[kLatSCap];
     __shared__ uint16_t s_hlist[kLatECap];
@@ -380,6 +397,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
                 s_eoff[lane] = ie - ne;
                 s_soff[lane] = is - ns;
+                s_mag[lane][0] = div_magic(d0 + 1);
+                s_mag[lane][1] = div_magic(d1 + 1);
+                s_mag[lane][2] = div_magic(d2 + 1);
+                s_mag[lane][3] = div_magic((d1 + 1) * (d2 + 1));
             }
             if (lane == np - 1) {
                 s_np = np;
@@ -395,32 +416,30 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         // (and zero ones) get D2 = D3 = 0 here; the others are appended to s_hlist (edge slot | particle
         // << 11) with r0, R_0 parked in their slots, and evaluated in (A2) by full warps.  Appends are
         // warp-aggregated; the list order does not affect the results.
+        const int eoff_l = lane < np ? s_eoff[lane] : INT_MAX;
         for (int base = warp * 32; base < etot; base += kThreads) {
             const int it = base + lane;
             bool heavy = false;
-            int j = 0;
+            const int j = warp_owner(base, eoff_l, lane);
+            const int eoff = __shfl_sync(0xffffffffu, eoff_l, j & 31);
             if (it < etot) {
-                j = chunk_search(s_eoff, np, it);
-                int e = it - s_eoff[j];
-                const int n[3] = {s_dim[j][0] + 1, s_dim[j][1] + 1, s_dim[j][2] + 1};
-                // blocks in order xy, xz, yx, yz, zx, zy
-                int a = 0, bax = 1;
-                {
-                    const int sz[6] = {n[0] * n[1], n[0] * n[2], n[1] * n[0], n[1] * n[2], n[2] * n[0], n[2] * n[1]};
-                    const int aa[6] = {0, 0, 1, 1, 2, 2}, bb[6] = {1, 2, 0, 2, 0, 1};
-                    int blk = 0;
-                    while (e >= sz[blk]) {
-                        e -= sz[blk];
-                        ++blk;
-                    }
-                    a = aa[blk];
-                    bax = bb[blk];
-                }
-                const int p = e / n[bax], q = e % n[bax];
-                const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
-                const double pc[3] = {s_x[j], s_y[j], s_z[j]};
-                const double r0 = fabs(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]));
-                const double R0 = fabs(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]));
+                int e = it - eoff;
+                const int n0 = s_dim[j][0] + 1, n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
+                // blocks in order xy, xz, yx, yz, zx, zy (plane axis a = blk / 2, line axis from 0x102021)
+                const int c1 = n0 * n1, c2 = c1 + n0 * n2, c3 = c2 + n1 * n0, c4 = c3 + n1 * n2, c5 = c4 + n2 * n0;
+                const int blk = (e >= c1) + (e >= c2) + (e >= c3) + (e >= c4) + (e >= c5);
+                e -= blk == 0 ? 0 : blk == 1 ? c1 : blk == 2 ? c2 : blk == 3 ? c3 : blk == 4 ? c4 : c5;
+                const int a = blk >> 1, bax = (0x102021 >> (4 * blk)) & 15;
+                const int nb = bax == 0 ? n0 : (bax == 1 ? n1 : n2);
+                const int p = div_by(e, s_mag[j][bax]), q = e - p * nb;
+                const double mna = a == 0 ? g.x_min : (a == 1 ? g.y_min : g.z_min);
+                const double dda = a == 0 ? g.dpx : (a == 1 ? g.dpy : g.dpz);
+                const double pca = a == 0 ? s_x[j] : (a == 1 ? s_y[j] : s_z[j]);
+                const double mnb = bax == 0 ? g.x_min : (bax == 1 ? g.y_min : g.z_min);
+                const double ddb = bax == 0 ? g.dpx : (bax == 1 ? g.dpy : g.dpz);
+                const double pcb = bax == 0 ? s_x[j] : (bax == 1 ? s_y[j] : s_z[j]);
+                const double r0 = fabs(lattice_offset(mna, dda, s_lo[j][a] + p, pca));
+                const double R0 = fabs(lattice_offset(mnb, ddb, s_lo[j][bax] + q, pcb));
                 if (GENERIC) {
                     lattice_generic_edge(K, mul_rn(g.support_in_h, s_h[j]), r0, R0, s_E + kLatGenERec * it);
                     ++n_ei;
@@ -459,15 +478,18 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         // an evaluated cell reads.  A list entry packs (particle, orientation, i, j, k): 5 + 2 + 3 x 4 bits.
         if (!GENERIC && !TAB) {
             const int ptot = stot / 3;
+            const int poff_l = lane < np ? s_soff[lane] / 3 : INT_MAX;
             for (int base = warp * 32; base < ptot; base += kThreads) {
                 const int pt = base + lane;
                 int cls = -1;  // -1 none, 0 general, 1 cheap
                 uint32_t rec = 0;
+                const int jp = warp_owner(base, poff_l, lane);
+                const int poff = __shfl_sync(0xffffffffu, poff_l, jp & 31);
                 if (pt < ptot) {
-                    const int jp = chunk_search(s_soff, np, 3 * pt);
-                    const int lp = pt - s_soff[jp] / 3;
-                    const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-                    const int i = lp / (n1 * n2), jj = (lp / n2) % n1, k = lp % n2;
+                    const int lp = pt - poff;
+                    const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
+                    const int i = div_by(lp, s_mag[jp][3]), rem = lp - i * n12;
+                    const int jj = div_by(rem, s_mag[jp][2]), k = rem - jj * n2;
                     const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
                     const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
                     const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
