@@ -292,11 +292,18 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGe
 
 // ------------------------------------------------------------------ lattice-factorised gather (cubic)
 
+// Resident CTAs per SM the register budget is sized for: three for the cubic kernel (80 registers; its
+// 70 KB of shared memory fits three times), two for the generic and tabulated ones.
 #ifndef KIWI_LATTICE_MIN_BLOCKS
-#define KIWI_LATTICE_MIN_BLOCKS 2
+#define KIWI_LATTICE_MIN_BLOCKS 3
 #endif
-constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
+#ifndef KIWI_LATTICE_GEN_MIN_BLOCKS
+#define KIWI_LATTICE_GEN_MIN_BLOCKS 2
+#endif
+constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;
+constexpr int kLatGenMinBlocks = KIWI_LATTICE_GEN_MIN_BLOCKS;
 constexpr double kNeedPad = 1.0 + 1e-6;
+constexpr int kLatPtCap = kLatSCap / 3;  // lattice points per chunk (three corner items each)
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");
 static_assert(kLatECap <= 2048, "packed edge-list entries");  // half-width factor of the cells around a lattice point
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
@@ -338,7 +345,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
     __shared__ uint32_t s_mag[kLatPMax][4];  // div_magic of n0, n1, n2 and n1 n2
     __shared__ int s_np, s_etot, s_stot, s_nexp, s_ncheap, s_nheavy;
-    __shared__ uint32_t s_blist[kLatSCap];
+    __shared__ uint32_t s_blist[kLatPtCap];
     __shared__ uint16_t s_hlist[kLatECap];
     extern __shared__ double s_dyn[];
     double* s_D2 = s_dyn;
@@ -355,9 +362,23 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     double acc[kCellsPerThread][4];
 #pragma unroll
     for (int c = 0; c < kCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
-    unsigned long long n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
-    unsigned long long n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0;
-    unsigned n_clamp = 0;
+    // work counters: 32-bit per thread (a chunk adds at most 64 to any of them), flushed to the 64-bit
+    // totals every 2^20 chunks and at the end
+    unsigned n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
+    unsigned n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0, n_clamp = 0, n_chunks = 0;
+    auto flush = [&]() {
+        add_stat(&st->bbox_pairs, n_bbox);
+        add_stat(&st->sphere_pairs, n_sphere);
+        add_stat(&st->evaluated_pairs, n_eval);
+        add_stat(&st->neg_clamped, n_neg);
+        add_stat(&st->neg_warned, n_warn);
+        add_stat(&st->edge_outer, n_eo);
+        add_stat(&st->edge_middle, n_em);
+        add_stat(&st->edge_inner, n_ei);
+        add_stat(&st->vertex_pyramids, n_vp);
+        if (TAB) add_stat(&st->table_clamps, n_clamp);
+        n_bbox = n_sphere = n_eval = n_neg = n_warn = n_eo = n_em = n_ei = n_vp = n_clamp = 0;
+    };
     const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
 
     for (int64_t pos = beg; pos < end;) {
@@ -471,11 +492,12 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         // (B0) list the corner items lattice point by lattice point (the three plane orientations of a
         // point share its offsets and its class), so that the cheap ones (corner beyond 2h: only I0 and
         // I1; or a zero corner) run in warps of their own: the others from the front of s_blist, the
-        // cheap ones from its end.  Appends are warp-aggregated; results do not depend on the order.
+        // cheap ones from its end; a point's three items follow one another in (B).  Appends are
+        // warp-aggregated; results do not depend on the order.
         // With CULL, a lattice point none of whose eight cells meets the support sphere is read by no
         // evaluated cell: its items are left out.  The test bounds the distance to the 2 x 2 x 2 cells
         // around the point, their half-widths padded by 1e-6 of a cell so that rounding never drops a point
-        // an evaluated cell reads.  A list entry packs (particle, orientation, i, j, k): 5 + 2 + 3 x 4 bits.
+        // an evaluated cell reads.  A list entry packs (particle, i, j, k): 5 + 3 x 4 bits.
         if (!GENERIC && !TAB) {
             const int ptot = stot / 3;
             const int poff_l = lane < np ? s_soff[lane] / 3 : INT_MAX;
@@ -505,24 +527,19 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     if (keep) {
                         const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
                         cls = (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) ? 1 : 0;
-                        rec = (uint32_t)jp | (uint32_t)i << 7 | (uint32_t)jj << 11 | (uint32_t)k << 15;
+                        rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
                     }
                 }
                 const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
                 int pe = 0, pcb = 0;
                 if (lane == 0) {
-                    if (me) pe = atomicAdd(&s_nexp, 3 * __popc(me));
-                    if (mc) pcb = atomicAdd(&s_ncheap, 3 * __popc(mc));
+                    if (me) pe = atomicAdd(&s_nexp, __popc(me));
+                    if (mc) pcb = atomicAdd(&s_ncheap, __popc(mc));
                 }
                 pe = __shfl_sync(0xffffffffu, pe, 0);
                 pcb = __shfl_sync(0xffffffffu, pcb, 0);
                 const unsigned below = (1u << lane) - 1;
-                if (cls >= 0) {
-                    const int b = cls == 0 ? pe + 3 * __popc(me & below) : kLatSCap - 3 - pcb - 3 * __popc(mc & below);
-                    s_blist[b] = rec;
-                    s_blist[b + 1] = rec | 1u << 5;
-                    s_blist[b + 2] = rec | 2u << 5;
-                }
+                if (cls >= 0) s_blist[cls == 0 ? pe + __popc(me & below) : kLatPtCap - 1 - pcb - __popc(mc & below)] = rec;
             }
         }
         __syncthreads();
@@ -539,8 +556,8 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             }
             __syncthreads();
         }
-        const int nexp = s_nexp, ncheap = s_ncheap;
-        const int nblist = (GENERIC || TAB) ? stot : nexp + ncheap;
+        const int nexp = s_nexp, ncheap = s_ncheap;  // lattice points
+        const int nblist = (GENERIC || TAB) ? stot : 3 * (nexp + ncheap);
 
         // (B) corner values S_a(i, j, k) for the three plane orientations a
         for (int li = threadIdx.x; li < nblist; li += kThreads) {
@@ -557,12 +574,13 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 jj = (rem / n2) % n1;
                 k = rem % n2;
             } else {
-                const uint32_t rec = s_blist[li < nexp ? li : kLatSCap - ncheap + (li - nexp)];
+                const int pli = li / 3;
+                axis = li - 3 * pli;
+                const uint32_t rec = s_blist[pli < nexp ? pli : kLatPtCap - ncheap + (pli - nexp)];
                 jp = (int)(rec & 31u);
-                axis = (int)((rec >> 5) & 3u);
-                i = (int)((rec >> 7) & 15u);
-                jj = (int)((rec >> 11) & 15u);
-                k = (int)((rec >> 15) & 15u);
+                i = (int)((rec >> 5) & 15u);
+                jj = (int)((rec >> 9) & 15u);
+                k = (int)((rec >> 13) & 15u);
                 const int n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
                 it = s_soff[jp] + axis * ((s_dim[jp][0] + 1) * n1 * n2) + (i * n1 + jj) * n2 + k;
             }
@@ -657,6 +675,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         }
         __syncthreads();
         pos += np;
+        if (++n_chunks == (1u << 20)) {
+            flush();
+            n_chunks = 0;
+        }
     }
 
     const double mvx = out.meanv[0], mvy = out.meanv[1], mvz = out.meanv[2];
@@ -680,16 +702,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             out.raw4[3 * ncell + i3] = acc[c][3];
         }
     }
-    add_stat(&st->bbox_pairs, n_bbox);
-    add_stat(&st->sphere_pairs, n_sphere);
-    add_stat(&st->evaluated_pairs, n_eval);
-    add_stat(&st->neg_clamped, n_neg);
-    add_stat(&st->neg_warned, n_warn);
-    add_stat(&st->edge_outer, n_eo);
-    add_stat(&st->edge_middle, n_em);
-    add_stat(&st->edge_inner, n_ei);
-    add_stat(&st->vertex_pyramids, n_vp);
-    if (TAB) add_stat(&st->table_clamps, n_clamp);
+    flush();
 }
 
 template <bool CULL>
@@ -703,7 +716,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice(CartGe
 }
 
 // The lattice form for the generic kernels (support cells only).
-__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_generic(CartGeom g, DevParticles P, int kernel,
+__global__ void __launch_bounds__(kThreads, kLatGenMinBlocks) k_cart_lattice_generic(CartGeom g, DevParticles P, int kernel,
                                                                                   const uint32_t* __restrict__ list,
                                                                                   const int64_t* __restrict__ range,
                                                                                   const int32_t* __restrict__ tile_map,
@@ -715,7 +728,7 @@ __global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_generi
 
 // The lattice form with the tabulated integral, every cell of the particles' bounding boxes (outside the
 // support the lookups do not cancel exactly, and the reference keeps what they leave).
-__global__ void __launch_bounds__(kThreads, kLatMinBlocks) k_cart_lattice_tab(CartGeom g, DevParticles P, const TabDev tab,
+__global__ void __launch_bounds__(kThreads, kLatGenMinBlocks) k_cart_lattice_tab(CartGeom g, DevParticles P, const TabDev tab,
                                                                               const uint32_t* __restrict__ list,
                                                                               const int64_t* __restrict__ range,
                                                                               const int32_t* __restrict__ tile_map,
@@ -875,11 +888,15 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
         if (full_box) {
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
+            KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                (int)cudaSharedmemCarveoutMaxShared));
             k_cart_lattice<false><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
                                                                                 d_stats);
         } else {
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
+            KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                                (int)cudaSharedmemCarveoutMaxShared));
             k_cart_lattice<true><<<grid, kThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
                                                                                d_stats);
         }
