@@ -64,6 +64,16 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
     return lattice_vertex_t<double>(h, r0, R_0, t, D2, D3);
 }
 
+// The edge and corner tiers are inlined into the lattice kernels by default (at 80 registers a call
+// costs more in saved registers than the larger code does); define either as __noinline__ to keep it out
+// of line.
+#ifndef KIWI_EDGE_INLINE
+#define KIWI_EDGE_INLINE __forceinline__
+#endif
+#ifndef KIWI_CORNER_INLINE
+#define KIWI_CORNER_INLINE __forceinline__
+#endif
+
 // The wall constants of the cubic spline (src/kernel_integral.cpp:222-247) divided by r0^3, as
 // polynomials in r0 / h and h / r0 (the reference forms B_k = r0^3 / 4 (...) and divides by r0^3 at each
 // use).  Powers from one reciprocal of h and one of r0.
@@ -106,7 +116,7 @@ static __device__ __forceinline__ double wall_b1_in(const LatticeWall& w) {
 struct LatticeEdge {
     double D2, D3;
 };
-static __device__ __noinline__ LatticeEdge lattice_edge(double h, double ih, double r0, double R_0) {
+static __device__ KIWI_EDGE_INLINE LatticeEdge lattice_edge(double h, double ih, double r0, double R_0) {
     const double ld2 = r0 * r0 + R_0 * R_0;
     const double inv = 1.0 / (r0 * R_0 * ld2);
     const double ir0 = R_0 * ld2 * inv, iR0 = r0 * ld2 * inv, ild2 = r0 * R_0 * inv;
@@ -157,7 +167,7 @@ static __device__ __noinline__ LatticeEdge lattice_edge(double h, double ih, dou
 // in, the wall term B3 / r0^3 x pi/2 is a polynomial in r0 / h: the pair needs no reciprocal of r0.  For
 // r0 >= 2h (B3 / r0^3 = (h/r0)^3 / 4) it is atan(a1 a2 / (r0 r)) / (4 pi).  ih = 1 / h; r0, a1, a2 > 0 (the
 // callers skip zero corners); (D2a, D3a) and (D2b, D3b) are the two edge tiers.
-static __device__ __noinline__ double lattice_corner(double h, double ih, double r0, double a1, double a2, double D2a,
+static __device__ KIWI_CORNER_INLINE double lattice_corner(double h, double ih, double r0, double a1, double a2, double D2a,
                                                      double D3a, double D2b, double D3b) {
     const double s2 = a1 * a1 + a2 * a2;
     const double r2 = r0 * r0 + s2;
