@@ -302,25 +302,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGe
 #endif
 constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;
 constexpr int kLatGenMinBlocks = KIWI_LATTICE_GEN_MIN_BLOCKS;
-constexpr double kNeedPad = 1.0 + 1e-6;
+constexpr double kNeedPad = 1.0 + 1e-6;  // half-width factor of the cells around a lattice point
 constexpr int kLatPtCap = kLatSCap / 3;  // lattice points per chunk (three corner items each)
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");
-static_assert(kLatECap <= 2048, "packed edge-list entries");  // half-width factor of the cells around a lattice point
+static_assert(kLatECap <= 2048, "packed edge-list entries");
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap + kLatSCap);
 constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatSCap);
 constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;
 constexpr size_t kLatTabDynSmem = sizeof(double) * kLatSCap;
 
 
-// One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
-// the edge and corner tables in shared memory.  Per chunk: (A) the edge tiers of every (plane, edge
-// line) of every particle's box, (B) the corner values of every (plane, lattice point), (C) each thread
-// assembles the cells it owns from the corner values, particle by particle in list order, and adds them
-// to its accumulators -- the same fixed per-cell summation order as k_cart_gather, no atomics.
-// GENERIC: the table-driven tiers of kernel `kernel` (support radius support_in_h x h) instead of the
-// cubic closed form; the edge tiers are then lattice_generic_edge records and the corner items run in
-// their natural order.  TAB: the tabulated cubic integral (lookups in `tab`): no edge tiers, and a corner
-// value is two lookups.
 // The chunk particle that owns item base + lane, for a warp whose 32 items start at base (a multiple of
 // 32): off is this lane's particle's first item (lane < np; INT_MAX beyond).  Every particle owns at least
 // one item, so the particles starting inside the window are distinct bits of one mask.  All 32 lanes call.
@@ -335,6 +326,15 @@ __device__ __forceinline__ int warp_owner(int base, int off, int lane) {
 __host__ __device__ __forceinline__ uint32_t div_magic(int n) { return ((1u << 20) + (uint32_t)n - 1) / (uint32_t)n; }
 __device__ __forceinline__ int div_by(int x, uint32_t m) { return (int)(((uint32_t)x * m) >> 20); }
 
+// One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
+// the edge and corner tables in shared memory.  Per chunk: (A) the edge tiers of every (plane, edge
+// line) of every particle's box, (B) the corner values of every (plane, lattice point), (C) each thread
+// assembles the cells it owns from the corner values, particle by particle in list order, and adds them
+// to its accumulators -- the same fixed per-cell summation order as k_cart_gather, no atomics.
+// GENERIC: the table-driven tiers of kernel `kernel` (support radius support_in_h x h) instead of the
+// cubic closed form; the edge tiers are then lattice_generic_edge records.  TAB: the tabulated cubic
+// integral (lookups in `tab`): no edge tiers, a corner value is two lookups, and the corner items run in
+// their natural order.
 template <bool CULL, bool GENERIC = false, bool TAB = false>
 __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
                                              const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
@@ -490,15 +490,17 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         }
 
         // (B0) list the corner items lattice point by lattice point (the three plane orientations of a
-        // point share its offsets and its class), so that the cheap ones (corner beyond 2h: only I0 and
-        // I1; or a zero corner) run in warps of their own: the others from the front of s_blist, the
+        // point share its offsets and its class), so that the cheap ones (corner beyond the support -- for
+        // the cubic spline beyond 2h: only I0 and I1 -- or a zero corner) run in warps of their own (cubic
+        // and generic kernels; the tabulated one runs the items in natural order): the others from the
+        // front of s_blist, the
         // cheap ones from its end; a point's three items follow one another in (B).  Appends are
         // warp-aggregated; results do not depend on the order.
         // With CULL, a lattice point none of whose eight cells meets the support sphere is read by no
         // evaluated cell: its items are left out.  The test bounds the distance to the 2 x 2 x 2 cells
         // around the point, their half-widths padded by 1e-6 of a cell so that rounding never drops a point
         // an evaluated cell reads.  A list entry packs (particle, i, j, k): 5 + 3 x 4 bits.
-        if (!GENERIC && !TAB) {
+        if (!TAB) {
             const int ptot = stot / 3;
             const int poff_l = lane < np ? s_soff[lane] / 3 : INT_MAX;
             for (int base = warp * 32; base < ptot; base += kThreads) {
@@ -525,8 +527,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                         keep = ex * ex + ey * ey + ez * ez < radius * radius;
                     }
                     if (keep) {
+                        // beyond the support (2h for the cubic spline)
+                        const double H = GENERIC ? mul_rn(g.support_in_h, h) : 2.0 * h;
                         const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
-                        cls = (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) ? 1 : 0;
+                        cls = (zero || !(ux * ux + uy * uy + uz * uz < H * H)) ? 1 : 0;
                         rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
                     }
                 }
@@ -557,12 +561,12 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             __syncthreads();
         }
         const int nexp = s_nexp, ncheap = s_ncheap;  // lattice points
-        const int nblist = (GENERIC || TAB) ? stot : 3 * (nexp + ncheap);
+        const int nblist = TAB ? stot : 3 * (nexp + ncheap);
 
         // (B) corner values S_a(i, j, k) for the three plane orientations a
         for (int li = threadIdx.x; li < nblist; li += kThreads) {
             int it, jp, axis, i, jj, k;
-            if (GENERIC || TAB) {
+            if (TAB) {
                 it = li;
                 jp = chunk_search(s_soff, np, it);
                 const int s = it - s_soff[jp];
