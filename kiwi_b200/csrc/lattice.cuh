@@ -254,7 +254,7 @@ constexpr int kLatGenECap = 640;  // edge records per chunk (a full 8^3 particle
 // integrals J_2l and the powers of q0 stay in registers.  q0^i is a compensated running product (hi + lo,
 // the product's rounding error carried exactly by fma): the terms can cancel heavily, and a plain running
 // product's rounding (up to ~i ulp) measurably raised the error of low-density cells; this is within an
-// ulp, like pow, at a fraction of its cost.
+// ulp, like pow, at a fraction of its cost; (1 - u^2)^m in the K recurrence is formed the same way.
 static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K, double q0, int j, int k, double a,
                                                         double a2, double phi, double sinp, double cosp) {
     const double* ak = K->a[k - 1];
@@ -274,6 +274,7 @@ static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K
     const double one_minus_u2 = cosp * cosp * (1.0 + a2) / den;
     const double tn = imin <= -2 ? sinp / cosp : 0.0, sc = imin <= -2 ? 1.0 / cosp : 0.0;
     double ph = 1.0, pl = 0.0;  // q0^idx
+    double wh = 1.0, wl = 0.0;  // (1 - u^2)^m, compensated like q0^idx
     double Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
     double J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
 #pragma unroll
@@ -289,7 +290,10 @@ static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K
         } else if ((idx & 1) == 0) {  // I_-(2m+1), m = idx / 2 - 1
             const int m = idx / 2 - 1;
             if (m > 0) {
-                Kc = u / (2.0 * m * pow(one_minus_u2, (double)m)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
+                const double nw = wh * one_minus_u2;
+                wl = fma(wl, one_minus_u2, fma(wh, one_minus_u2, -nw));
+                wh = nw;
+                Kc = u / (2.0 * m * (wh + wl)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
                 pow1a2 *= (1.0 + a2);
             }
             Iodd += a * pow1a2 * Kc;
