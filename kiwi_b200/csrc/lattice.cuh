@@ -254,7 +254,7 @@ constexpr int kLatGenECap = 640;  // edge records per chunk (a full 8^3 particle
 // integrals J_2l and the powers of q0 stay in registers.  q0^i is a compensated running product (hi + lo,
 // the product's rounding error carried exactly by fma): the terms can cancel heavily, and a plain running
 // product's rounding (up to ~i ulp) measurably raised the error of low-density cells; this is within an
-// ulp, like pow, at a fraction of its cost; (1 - u^2)^m in the K recurrence is formed the same way.
+// ulp, like pow, at a fraction of its cost; (1 - u^2)^-m in the K recurrence is formed the same way.
 static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K, double q0, int j, int k, double a,
                                                         double a2, double phi, double sinp, double cosp) {
     const double* ak = K->a[k - 1];
@@ -269,12 +269,14 @@ static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K
     if (k >= j)
         for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
     double sum = (A3 * b) * phi;
-    const double den = a2 + cosp * cosp;
-    const double u = a * sinp / sqrt(den);
-    const double one_minus_u2 = cosp * cosp * (1.0 + a2) / den;
-    const double tn = imin <= -2 ? sinp / cosp : 0.0, sc = imin <= -2 ? 1.0 / cosp : 0.0;
+    // u = a sin(phi) / sqrt(a^2 + cos^2(phi)), so u / a = sin(phi) / sqrt(...) and
+    // 1 / (1 - u^2) = (a^2 + cos^2(phi)) / (cos^2(phi) (1 + a^2)): three reciprocals in all
+    const double den = a2 + cosp * cosp, iden = 1.0 / den;
+    const double ua = sinp * sqrt(iden), u = a * ua;
+    const double iomu2 = den / (cosp * cosp * (1.0 + a2));
+    const double sc = imin <= -2 ? 1.0 / cosp : 0.0, tn = sinp * sc;
     double ph = 1.0, pl = 0.0;  // q0^idx
-    double wh = 1.0, wl = 0.0;  // (1 - u^2)^m, compensated like q0^idx
+    double wh = 1.0, wl = 0.0;  // (1 - u^2)^-m, compensated like q0^idx
     double Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
     double J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
 #pragma unroll
@@ -282,7 +284,7 @@ static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K
         if (1 - idx < imin) break;
         double Iv;
         if (idx == 0) {  // I_1 = atan(u / a)
-            Iv = atan(u / a);
+            Iv = atan(ua);
             Iodd = Iv;
             Kc = atanh(u);
         } else if (idx == 1) {  // I_0 = phi
@@ -290,10 +292,10 @@ static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K
         } else if ((idx & 1) == 0) {  // I_-(2m+1), m = idx / 2 - 1
             const int m = idx / 2 - 1;
             if (m > 0) {
-                const double nw = wh * one_minus_u2;
-                wl = fma(wl, one_minus_u2, fma(wh, one_minus_u2, -nw));
+                const double nw = wh * iomu2;
+                wl = fma(wl, iomu2, fma(wh, iomu2, -nw));
                 wh = nw;
-                Kc = u / (2.0 * m * (wh + wl)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
+                Kc = u * (wh + wl) * (1.0 / (2.0 * m)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
                 pow1a2 *= (1.0 + a2);
             }
             Iodd += a * pow1a2 * Kc;
@@ -305,7 +307,7 @@ static __device__ __noinline__ double lattice_generic_G(const KiwiKernelTable* K
                 J[1] = tn;
             } else {
                 spow *= sc * sc;
-                J[kk] = spow * tn / (2 * kk - 1.0) + (2 * kk - 2.0) / (2 * kk - 1.0) * J[kk - 1];
+                J[kk] = spow * tn * (1.0 / (2 * kk - 1.0)) + (2 * kk - 2.0) / (2 * kk - 1.0) * J[kk - 1];
             }
             double s = J[0], apow = 1.0, bc = 1.0;
 #pragma unroll
