@@ -55,7 +55,7 @@ VERTEX_PYRAMID = 121.0 + TRANS_FLOPS * 4
 CELL_ASSEMBLY = 60.0
 # DRAM bytes (read + write) of one k_cart_lattice launch on the default workload (2M particles, 256^3),
 # ncu dram__bytes_read.sum + dram__bytes_write.sum (profiles/k_cart_lattice_fp64_lognormal.md).
-LATTICE_DRAM_BYTES_FULL = 285.03e6 + 702.90e6
+LATTICE_DRAM_BYTES_FULL = 212.32e6 + 520.65e6
 
 L2_BYTES = 126 * 1024 * 1024
 # the tabulated integral: one trilinear lookup reads 8 table entries
