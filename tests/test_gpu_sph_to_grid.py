@@ -108,6 +108,73 @@ def test_matches_oracle_random_cases(kiwi, ctx, oracle, form):
         assert res.stats["skipped_outside"] == st.skipped_outside
 
 
+ALIGNED_BOUNDS = (-0.5, 2.5, -0.5, 2.5, -0.5, 2.5)  # 24^3 cells of 0.125 (exact); supports stay inside
+ALIGNED_SHAPE = (24, 24, 24)
+ALIGNED_DP = 0.125
+
+
+def _tangent_particles(n, seed, x_min=-0.5, dp=ALIGNED_DP):
+    """Particles anywhere in [0.4, 1.6]^3 whose support (2h) ends exactly on a lattice plane (kind 0) or
+    exactly at a lattice corner (kind 1), 1-3 cells away: the boundary of the lattice kernel's test for
+    corners that no evaluated cell reads.  Plane positions are formed as the kernel forms them."""
+    rng = np.random.default_rng(seed)
+    P = {ax: rng.uniform(0.4, 1.6, n) for ax in ("x", "y", "z")}
+    for ax in ("vx", "vy", "vz"):
+        P[ax] = rng.standard_normal(n)
+    P["m"] = rng.uniform(0.5, 1.5, n)
+    pos = np.stack([P["x"], P["y"], P["z"]], 1)
+    cell = np.floor((pos - x_min) / dp)
+    planes = x_min + (cell - rng.integers(1, 4, (n, 3)) + 1) * dp
+    d = np.abs(planes - pos)
+    face = d[np.arange(n), rng.integers(0, 3, n)]
+    corner = np.sqrt((d ** 2).sum(axis=1))
+    P["h"] = np.where(rng.integers(0, 2, n) == 0, face, corner) / 2.0
+    return P
+
+
+@pytest.mark.parametrize("k", [-1, 4])
+def test_lattice_tangent_supports(kiwi, ctx, oracle, k):
+    """Supports ending exactly on lattice planes and corners: the lattice form (which leaves out corners
+    that no evaluated cell reads) equals the per-cell gather and the oracle, over the same pairs."""
+    P = _tangent_particles(150, 17)
+    ki = kiwi.KernelIntegrator(kernel=max(k, 0))
+    lat = kiwi.sph_to_grid(P, ALIGNED_BOUNDS, ALIGNED_SHAPE, kernel=ki, ctx=ctx, precision="fp64")
+    gat = kiwi.sph_to_grid(P, ALIGNED_BOUNDS, ALIGNED_SHAPE, kernel=ki, ctx=ctx, precision="fp64_reference_order")
+    dens, vx, vy, vz, _, st = oracle.sph_to_grid(P, ALIGNED_BOUNDS, ALIGNED_SHAPE, kernel=k, support_in_h=2.0)
+    assert_band_tolerance(lat.density, gat.density, RANDOM_TOLS, label="lattice vs gather")
+    assert_band_tolerance(lat.density, dens, RANDOM_TOLS, label="lattice vs oracle")
+    assert lat.stats["sphere_pairs"] == gat.stats["sphere_pairs"] == st.sphere_pairs
+    assert lat.stats["bbox_pairs"] == st.bbox_pairs
+
+
+@pytest.mark.parametrize("x_min,x_max,step", [(-0.5, 2.5, 0.125), (-0.4, 2.0, 0.1)],
+                         ids=["exact_planes", "ulp_off_planes"])
+def test_lattice_particles_on_planes(kiwi, ctx, x_min, x_max, step):
+    """Particles on lattice planes, edges and corners (some with supports ending on planes): at
+    x_min + k step, step the cell size.  With (-0.5, 2.5) / 24 = 0.125 they lie exactly on the planes;
+    with (-0.4, 2.0) / 24 = 0.09999999999999999 the positions -0.4 + k x 0.1 miss the kernel's planes by
+    an ulp, so some wall distances are ~1e-17 -- where the reference's operations give NaN and negative
+    cell masses (its edge tier takes acos of a ratio that rounds above 1).  There is no reference value
+    to match there; the lattice form must give finite, non-negative cells that conserve the particles'
+    mass on the padded domain."""
+    b = (x_min, x_max, x_min, x_max, x_min, x_max)
+    dp = (x_max - x_min) / 24
+    rng = np.random.default_rng(23)
+    n = 120
+    P = {ax: x_min + rng.integers(8, 16, n) * step for ax in ("x", "y", "z")}
+    off = rng.integers(0, 2, (n, 3)) * (step / 2)  # half of them off the plane along some axes
+    for i, ax in enumerate(("x", "y", "z")):
+        P[ax] = P[ax] + off[:, i]
+    for ax in ("vx", "vy", "vz"):
+        P[ax] = rng.standard_normal(n)
+    P["m"] = rng.uniform(0.5, 1.5, n)
+    P["h"] = np.where(rng.integers(0, 2, n) == 0, rng.integers(1, 5, n) * (step / 2), rng.uniform(0.05, 0.3, n))
+    res = kiwi.sph_to_grid(P, b, ALIGNED_SHAPE, raw=True, ctx=ctx, precision="fp64")
+    assert np.all(np.isfinite(res.density)) and np.all(res.density >= 0.0)
+    mass = res.density.sum() * dp ** 3
+    assert abs(mass / P["m"].sum() - 1.0) < 1e-10
+
+
 def test_deterministic_bitwise(kiwi, ctx):
     P = random_particles(300, 9, hmin=0.02, hmax=0.5)
     b = (0, 2, 0, 2, 0, 2)
