@@ -15,6 +15,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "kernel_tables.h"
 
 #ifdef __CUDACC__
@@ -392,6 +394,13 @@ template <class T>
 KIWI_HD T vmin2(const T& a, const T& b) { return a < b ? a : b; }
 
 // Vertex source for the face walk: VX(i), VY(i), VZ(i) give vertex i of the face (n vertices, n >= 3).
+// Whether a face-walk evaluator takes the vertex pyramid's leg along the edge (at_len(t)) instead of its
+// angle (at(phi)).
+template <class E, class = void>
+struct EvalUsesLengths : std::false_type {};
+template <class E>
+struct EvalUsesLengths<E, std::void_t<decltype(E::kLengths)>> : std::integral_constant<bool, E::kLengths> {};
+
 // face_integral_impl of src/kernel_integral.cpp:471-647, including the out_vert reachability rule.
 // T is the type of the particle's coordinates (the face's vertices are plain doubles): double, or Dual4
 // for the derivatives of the face integral with respect to the particle.
@@ -436,8 +445,6 @@ KIWI_HD T face_integral(T x0, T y0, T z0, T support_radius, const Verts& V, int 
         const T x2r = x2 - x0, y2r = y2 - y0, z2r = z2 - z0;
         const T x3r = x3 - x0, y3r = y3 - y0, z3r = z3 - z0;
         const T s1 = xpr * (y2r * z3r - z2r * y3r) + ypr * (z2r * x3r - x2r * z3r) + zpr * (x2r * y3r - y2r * x3r);
-        const T phi1 = (R_0 < r12) ? acos(R_0 / r12) : T(0.0);
-        const T phi2 = (R_0 < r13) ? acos(R_0 / r13) : T(0.0);
         const double ex = x3 - x2, ey = y3 - y2, ez = z3 - z2;
         const T tpx = xp - x2, tpy = yp - y2, tpz = zp - z2;
         const T side = (ey * tpz - ez * tpy) * A + (ez * tpx - ex * tpz) * B + (ex * tpy - ey * tpx) * C;
@@ -450,19 +457,34 @@ KIWI_HD T face_integral(T x0, T y0, T z0, T support_radius, const Verts& V, int 
                 inside_polygon = false;
             }
         }
-        const bool foot_beyond_endpoint = (r12 * sin(phi1) >= r23) || (r13 * sin(phi2) >= r23);
+        bool foot_beyond_endpoint, first_wider;
+        T I1v = 0.0, I2v = 0.0;
+        if constexpr (EvalUsesLengths<Eval>::value) {
+            // the legs along the edge line from each vertex to the foot: r12 |cos a| and |r23 - r12 cos a|
+            // (the reference's r12 sin(phi1) and r13 sin(phi2)); phi1 >= phi2 iff t1 >= t2
+            const T t1 = r12 * fabs(cosa), t2 = fabs(r23 - r12 * cosa);
+            foot_beyond_endpoint = (t1 >= r23) || (t2 >= r23);
+            first_wider = t1 >= t2;
+            ev.set_edge(R_0);
+            I1v = ev.at_len(t1);
+            I2v = ev.at_len(t2);
+        } else {
+            const T phi1 = (R_0 < r12) ? acos(R_0 / r12) : T(0.0);
+            const T phi2 = (R_0 < r13) ? acos(R_0 / r13) : T(0.0);
+            foot_beyond_endpoint = (r12 * sin(phi1) >= r23) || (r13 * sin(phi2) >= r23);
+            first_wider = phi1 >= phi2;
+            ev.set_edge(R_0);
+#pragma unroll 1
+            for (int v = 0; v < 2; ++v) {
+                const T t = ev.at(v == 0 ? phi1 : phi2);
+                if (v == 0) I1v = t; else I2v = t;
+            }
+        }
         const T in_plane_dist = foot_beyond_endpoint ? vmin2(r12, r13) : R_0;
         min_edge_dist = vmin2(min_edge_dist, in_plane_dist);
         T M = (s1 * s2 * r0 <= 0) ? T(-1.0) : T(1.0);
-        ev.set_edge(R_0);
-        T I1v = 0.0, I2v = 0.0;
-#pragma unroll 1
-        for (int v = 0; v < 2; ++v) {
-            const T t = ev.at(v == 0 ? phi1 : phi2);
-            if (v == 0) I1v = t; else I2v = t;
-        }
         if (foot_beyond_endpoint) {
-            M = (phi1 >= phi2) ? M * (I1v - I2v) : M * (I2v - I1v);
+            M = first_wider ? M * (I1v - I2v) : M * (I2v - I1v);
         } else {
             M = M * (I1v + I2v);
         }

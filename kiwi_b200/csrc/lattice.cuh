@@ -152,6 +152,73 @@ static __device__ KIWI_EDGE_INLINE LatticeEdge lattice_edge(double h, double ih,
     return {D2, D3};
 }
 
+// One vertex pyramid of the face walk (src/kernel_integral.cpp:356-400) from its right triangle's
+// lengths: legs R_0 (projection -> edge line) and t (along the edge line) in a wall at distance r0,
+// r the distance to the vertex.  The series is lattice_corner's for one pyramid: phi = atan2(t, R_0),
+// tan(phi) = t / R_0, 1 / cos^2(phi) = (R_0^2 + t^2) / R_0^2, u = t / r, 1 - u^2 = (r0^2 + R_0^2) / r^2,
+// u / a = t r0 / (R_0 r).  Beyond 2h the tier is K (-(h/r0)^3 / 4 I1 + B3 / r0^3 phi + D3) with
+// K = (r0/h)^3 / pi, i.e. (-I1 + 4 x^3 b3 phi) / (4 pi) + K D3 with x = r0 / h and x^3 b3 a polynomial in
+// x; for r0 >= 2h (B3 / r0^3 = (h/r0)^3 / 4) it is (phi - I1) / (4 pi) + K D3, the difference of the two
+// arctangents taken as atan(t s^2 R_0 / ((r + r0) (R_0^2 r + t^2 r0))), s^2 = R_0^2 + t^2, which does not
+// cancel.  The ratios come from one reciprocal of r0 r R_0 t and one of r0^2 + R_0^2.
+// ih = 1 / h; r0, R_0, t > 0; (D2, D3) the edge tier of the triangle's edge line.
+static __device__ __forceinline__ double lattice_pyramid(double h, double ih, double r0, double R_0, double t,
+                                                         double D2, double D3) {
+    const double s2 = R_0 * R_0 + t * t;
+    const double r2 = r0 * r0 + s2;
+    const double r = sqrt(r2);
+    const double phi = atan2(t, R_0);
+    if (!(r2 < 4.0 * (h * h))) {
+        const double x = r0 * ih, x2 = x * x, x3 = x2 * x;
+        const double K = x3 * (1.0 / kPi);
+        if (r0 >= 2.0 * h)
+            return 0.25 / kPi * atan(t * s2 * R_0 / ((r + r0) * (R_0 * R_0 * r + t * t * r0))) + K * D3;
+        const double x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
+        const double p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
+                                : -2. / 3. * x3 + 0.3 * x5 - 0.1 * x6 + 7. / 5. * x;
+        return 0.25 / kPi * (p * phi - atan(t * r0 / (R_0 * r))) + K * D3;
+    }
+    const double inv = 1.0 / (r0 * r * (R_0 * t));
+    const double ir0 = r * (R_0 * t) * inv, ir = r0 * (R_0 * t) * inv, iR0 = r0 * r * t * inv;
+    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
+    const double K = w.r0h3 * (1.0 / kPi);
+    const double a = R_0 * ir0, a2k = a * a, u = t * ir;
+    const double tanp = t * iR0, sec2 = s2 * iR0 * iR0;
+    const double iomu2 = r2 / (r0 * r0 + R_0 * R_0);
+    const double I0 = phi;
+    const double I_2 = phi + a2k * tanp;
+    const double I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
+    const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
+    const double I1 = atan(tanp * r0 * ir);
+    const double I_1 = a / 2. * logs + I1;
+    const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
+    const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
+    if (r2 < h * h) return K * (1. / 6. * I_2 - 3. / 40. * w.r0h2 * I_4 + 1. / 40. * w.r0h3 * I_5 + wall_b1_in(w) * I0);
+    return K * (0.25 * (4. / 3. * I_2 - w.r0h * I_3 + 0.3 * w.r0h2 * I_4 - 1. / 30. * w.r0h3 * I_5 + 1. / 15. * w.r0h_3 * I1) +
+                (r0 > h ? wall_b2_mid(w) : wall_b2_in(w)) * I0 + D2);
+}
+
+// Face-walk evaluator of the plain FP64 Voronoi map (CubicEval's role): the edge tier in the edge's own
+// lengths (lattice_edge) and each vertex pyramid from its triangle's lengths (lattice_pyramid); the face
+// walk hands it the leg t along the edge instead of the angle (kLengths).
+struct LenCubicEval {
+    static constexpr bool kLengths = true;
+    double h = 0.0, ih = 0.0, r0 = 0.0, R_0 = 0.0, D2 = 0.0, D3 = 0.0;
+    __device__ void set_wall(double ar0) { r0 = ar0; }
+    __device__ void set_edge(double R) {
+        R_0 = R;
+        D2 = D3 = 0.0;
+        if (r0 != 0.0 && R != 0.0 && r0 * r0 + R * R <= 4.0 * (h * h)) {
+            const LatticeEdge e = lattice_edge(h, ih, r0, R);
+            D2 = e.D2;
+            D3 = e.D3;
+        }
+    }
+    __device__ double at_len(double t) const {
+        return (r0 == 0.0 || R_0 == 0.0 || t == 0.0) ? 0.0 : lattice_pyramid(h, ih, r0, R_0, t, D2, D3);
+    }
+};
+
 // The pyramid pair of one corner value, F(r0, a1, a2) + F(r0, a2, a1): the two right triangles of the
 // rectangle spanned by the particle's projection and the corner (legs a1 along the first edge line and a2
 // along the second, and the reverse), in the wall at distance r0.  The vertex tier's series

@@ -25,6 +25,7 @@
 #include "../../include/kiwi_b200.h"
 #include "engine.hpp"
 #include "kiwi_math.cuh"
+#include "lattice.cuh"
 #include "prims.cuh"
 #include "tabulated.cuh"
 
@@ -226,8 +227,9 @@ static __device__ __noinline__ double vor_face(const double* verts, int nv, doub
         return face_integral(x0, y0, z0, 2 * h, V, nv, (int*)nullptr, ev);
     }
     if (MODE == kVorCubic) {
-        CubicEval ev;
+        LenCubicEval ev;
         ev.h = h;
+        ev.ih = 1.0 / h;
         return face_integral(x0, y0, z0, 2 * h, V, nv, (int*)nullptr, ev);
     }
     GenericEval ev;
