@@ -6,8 +6,9 @@
 //   dL/dm_p     = sum_c K_pc (gM_c + v_p . gP_c)
 //   dL/dv_p     = m_p sum_c K_pc gP_c
 //   dL/dtheta_p = m_p sum_c dK_pc/dtheta (gM_c + v_p . gP_c),   theta = x, y, z, h.
-// The per-pair cell integrals are recomputed, not stored: the face walk is instantiated with the Dual4
-// type, which carries d/dx, d/dy, d/dz, d/dh of every intermediate through the same operations, so the
+// The per-pair cell integrals are recomputed, not stored: the forward kernel's lattice tiers (lattice_edge,
+// lattice_corner) are instantiated with the Dual4 type, which carries d/dx, d/dy, d/dz, d/dh of every
+// intermediate through the same operations, so the
 // value part equals the forward's Msum bit for bit and the derivative part is the exact derivative of the
 // evaluated formula (branch choices are taken on values).  A clamped pair (Msum < 0) has K = 0 and no
 // gradient.  The pairs are those of the forward's default evaluation: the cells of the particle's
@@ -185,10 +186,15 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
             const Dual4 r0 = dual_abs_offset(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]), a);
             const Dual4 R0 = dual_abs_offset(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]), bax);
             const Dual4 hD = Dual4::seed(s_h[j], 3);
-            const CubicWallT<Dual4> w = cubic_wall_t<Dual4>(hD, r0);
-            const CubicEdgeT<Dual4> ed = cubic_edge_t<Dual4>(w, R0);
-            store_dual(s_E + kAdjERec * it, ed.D2);
-            store_dual(s_E + kAdjERec * it + 5, ed.D3);
+            // the forward kernel's edge tier (lattice_edge) in Dual4; zero beyond 2h and for zero offsets
+            Dual4 D2(0.0), D3(0.0);
+            if (r0 != 0.0 && R0 != 0.0 && r0.v * r0.v + R0.v * R0.v <= 4.0 * (s_h[j] * s_h[j])) {
+                const LatticeEdgeT<Dual4> ed = lattice_edge(hD, 1.0 / hD, r0, R0);
+                D2 = ed.D2;
+                D3 = ed.D3;
+            }
+            store_dual(s_E + kAdjERec * it, D2);
+            store_dual(s_E + kAdjERec * it + 5, D3);
         }
         __syncthreads();
 
@@ -226,8 +232,9 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 const Dual4 r0 = dual_abs_offset(ua, axis);
                 const Dual4 a1 = dual_abs_offset(u1, ax1), a2 = dual_abs_offset(u2, ax2);
                 const Dual4 hD = Dual4::seed(s_h[jp], 3);
-                f = lattice_vertex_t<Dual4>(hD, r0, a1, a2, load_dual(s_E + kAdjERec * e1), load_dual(s_E + kAdjERec * e1 + 5)) +
-                    lattice_vertex_t<Dual4>(hD, r0, a2, a1, load_dual(s_E + kAdjERec * e2), load_dual(s_E + kAdjERec * e2 + 5));
+                // the forward kernel's corner pair (lattice_corner) in Dual4
+                f = lattice_corner(hD, 1.0 / hD, r0, a1, a2, load_dual(s_E + kAdjERec * e1), load_dual(s_E + kAdjERec * e1 + 5),
+                                   load_dual(s_E + kAdjERec * e2), load_dual(s_E + kAdjERec * e2 + 5));
             }
             store_dual(s_S + kAdjSRec * it, sg * f);
         }

@@ -122,6 +122,9 @@ KIWI_DD Dual4 fabs(const Dual4& x) { return x.v < 0.0 ? -x : x; }
 KIWI_DD Dual4 acos(const Dual4& x) { return chain(x, ::acos(x.v), -1.0 / ::sqrt(1.0 - x.v * x.v)); }
 KIWI_DD Dual4 atan(const Dual4& x) { return chain(x, ::atan(x.v), 1.0 / (1.0 + x.v * x.v)); }
 KIWI_DD Dual4 log(const Dual4& x) { return chain(x, ::log(x.v), 1.0 / x.v); }
+KIWI_DD Dual4 log1p(const Dual4& x) { return chain(x, ::log1p(x.v), 1.0 / (1.0 + x.v)); }
+// max with a constant: the constant (no derivative) where it wins
+KIWI_DD Dual4 fmax(const Dual4& x, double c) { return x.v >= c ? x : Dual4(c); }
 KIWI_DD Dual4 sin(const Dual4& x) { return chain(x, ::sin(x.v), ::cos(x.v)); }
 KIWI_DD Dual4 cos(const Dual4& x) { return chain(x, ::cos(x.v), -::sin(x.v)); }
 KIWI_DD void sincos(const Dual4& x, Dual4* s, Dual4* c) {

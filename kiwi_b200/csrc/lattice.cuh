@@ -76,28 +76,35 @@ static __device__ __forceinline__ double lattice_vertex(double h, double r0, dou
 
 // The wall constants of the cubic spline (src/kernel_integral.cpp:222-247) divided by r0^3, as
 // polynomials in r0 / h and h / r0 (the reference forms B_k = r0^3 / 4 (...) and divides by r0^3 at each
-// use).  Powers from one reciprocal of h and one of r0.
+// use).  Powers from one reciprocal of h and one of r0.  The functions below are written over the real
+// type T: double for the forward kernels, Dual4 (dual.cuh) for the adjoint, whose value part is then the
+// forward's bit for bit.
+template <class T>
 struct LatticeWall {
-    double r0h, r0h2, r0h3, r0h_2, r0h_3;  // (r0/h)^k and (h/r0)^k
+    T r0h, r0h2, r0h3, r0h_2, r0h_3;  // (r0/h)^k and (h/r0)^k
 };
-static __device__ __forceinline__ LatticeWall lattice_wall(double ih, double h, double ir0, double r0) {
-    LatticeWall w;
+template <class T>
+static __device__ __forceinline__ LatticeWall<T> lattice_wall(T ih, T h, T ir0, T r0) {
+    LatticeWall<T> w;
     w.r0h = r0 * ih;
     w.r0h2 = w.r0h * w.r0h;
     w.r0h3 = w.r0h2 * w.r0h;
-    const double hr0 = h * ir0;
+    const T hr0 = h * ir0;
     w.r0h_2 = hr0 * hr0;
     w.r0h_3 = w.r0h_2 * hr0;
     return w;
 }
 // B2 / r0^3 for h < r0 < 2h (its B1 is 0) and for r0 <= h; B1 / r0^3 for r0 <= h; B3 / r0^3 in each range.
-static __device__ __forceinline__ double wall_b2_mid(const LatticeWall& w) {
+template <class T>
+static __device__ __forceinline__ T wall_b2_mid(const LatticeWall<T>& w) {
     return 0.25 * (-4. / 3. + w.r0h - 0.3 * w.r0h2 + 1. / 30. * w.r0h3 - 1. / 15. * w.r0h_3);
 }
-static __device__ __forceinline__ double wall_b2_in(const LatticeWall& w) {
+template <class T>
+static __device__ __forceinline__ T wall_b2_in(const LatticeWall<T>& w) {
     return 0.25 * (-2. / 3. + 0.3 * w.r0h2 - 0.1 * w.r0h3 - 0.2 * w.r0h_2);
 }
-static __device__ __forceinline__ double wall_b1_in(const LatticeWall& w) {
+template <class T>
+static __device__ __forceinline__ T wall_b1_in(const LatticeWall<T>& w) {
     return 0.25 * (-2. / 3. + 0.3 * w.r0h2 - 0.1 * w.r0h3);
 }
 
@@ -113,35 +120,38 @@ static __device__ __forceinline__ double wall_b1_in(const LatticeWall& w) {
 // (B1 - B2) / r0^3 and (B2 - B3) / r0^3 are 0.05 (h/r0)^2 and -0.4 (h/r0)^2 within h; -B2 / r0^3 and
 // -0.4 (h/r0)^2 between h and 2h.
 // ih = 1 / h; r0, R_0 > 0 and r0^2 + R_0^2 <= 4 h^2 (the caller gives D2 = D3 = 0 otherwise).
-struct LatticeEdge {
-    double D2, D3;
+template <class T>
+struct LatticeEdgeT {
+    T D2, D3;
 };
-static __device__ KIWI_EDGE_INLINE LatticeEdge lattice_edge(double h, double ih, double r0, double R_0) {
-    const double ld2 = r0 * r0 + R_0 * R_0;
-    const double inv = 1.0 / (r0 * R_0 * ld2);
-    const double ir0 = R_0 * ld2 * inv, iR0 = r0 * ld2 * inv, ild2 = r0 * R_0 * inv;
-    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
-    const double a = R_0 * ir0, a2 = a * a;
-    const double b12 = r0 > h ? -wall_b2_mid(w) : 0.05 * w.r0h_2;
-    const double b23 = -0.4 * w.r0h_2;
-    const double c3 = a * (1. + a2) / 4., c5 = a * (1. + a2) * (1. + a2) / 16.;
-    double D2 = 0.0, D3 = 0.0;
+using LatticeEdge = LatticeEdgeT<double>;
+template <class T>
+static __device__ KIWI_EDGE_INLINE LatticeEdgeT<T> lattice_edge(T h, T ih, T r0, T R_0) {
+    const T ld2 = r0 * r0 + R_0 * R_0;
+    const T inv = 1.0 / (r0 * R_0 * ld2);
+    const T ir0 = R_0 * ld2 * inv, iR0 = r0 * ld2 * inv, ild2 = r0 * R_0 * inv;
+    const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
+    const T a = R_0 * ir0, a2 = a * a;
+    const T b12 = r0 > h ? -wall_b2_mid(w) : 0.05 * w.r0h_2;
+    const T b23 = -0.4 * w.r0h_2;
+    const T c3 = a * (1. + a2) / 4., c5 = a * (1. + a2) * (1. + a2) / 16.;
+    T D2 = 0.0, D3 = 0.0;
 #pragma unroll 1
     for (int pass = (ld2 <= h * h) ? 0 : 1; pass < 2; ++pass) {
-        const double H = pass == 0 ? h : 2.0 * h, iH = pass == 0 ? ih : 0.5 * ih;
-        const double c2 = H * H - r0 * r0;
-        const double t = sqrt(fmax(c2 - R_0 * R_0, 0.0));
-        const double phi = atan2(t, R_0);
-        const double tanp = t * iR0, sec2 = c2 * iR0 * iR0;
-        const double u = t * iH, iomu2 = H * H * ild2;
-        const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
-        const double I0 = phi;
-        const double I_2 = phi + a2 * tanp;
-        const double I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + sec2);
-        const double I1 = atan(u * r0 * iR0);
-        const double I_1 = a / 2. * logs + I1;
-        const double I_3 = I_1 + c3 * (2 * u * iomu2 + logs);
-        const double I_5 = I_3 + c5 * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
+        const T H = pass == 0 ? h : 2.0 * h, iH = pass == 0 ? ih : 0.5 * ih;
+        const T c2 = H * H - r0 * r0;
+        const T t = sqrt(fmax(c2 - R_0 * R_0, 0.0));
+        const T phi = atan2(t, R_0);
+        const T tanp = t * iR0, sec2 = c2 * iR0 * iR0;
+        const T u = t * iH, iomu2 = H * H * ild2;
+        const T logs = log1p(2.0 * u * (1.0 + u) * iomu2);
+        const T I0 = phi;
+        const T I_2 = phi + a2 * tanp;
+        const T I_4 = phi + 2 * a2 * tanp + 1. / 3. * a2 * a2 * tanp * (2. + sec2);
+        const T I1 = atan(u * r0 * iR0);
+        const T I_1 = a / 2. * logs + I1;
+        const T I_3 = I_1 + c3 * (2 * u * iomu2 + logs);
+        const T I_5 = I_3 + c5 * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
         if (pass == 0)
             D2 = -1. / 6. * I_2 + 0.25 * w.r0h * I_3 - 0.15 * w.r0h2 * I_4 + 1. / 30. * w.r0h3 * I_5 -
                  1. / 60. * w.r0h_3 * I1 + b12 * I0;
@@ -162,37 +172,37 @@ static __device__ KIWI_EDGE_INLINE LatticeEdge lattice_edge(double h, double ih,
 // arctangents taken as atan(t s^2 R_0 / ((r + r0) (R_0^2 r + t^2 r0))), s^2 = R_0^2 + t^2, which does not
 // cancel.  The ratios come from one reciprocal of r0 r R_0 t and one of r0^2 + R_0^2.
 // ih = 1 / h; r0, R_0, t > 0; (D2, D3) the edge tier of the triangle's edge line.
-static __device__ __forceinline__ double lattice_pyramid(double h, double ih, double r0, double R_0, double t,
-                                                         double D2, double D3) {
-    const double s2 = R_0 * R_0 + t * t;
-    const double r2 = r0 * r0 + s2;
-    const double r = sqrt(r2);
-    const double phi = atan2(t, R_0);
+template <class T>
+static __device__ __forceinline__ T lattice_pyramid(T h, T ih, T r0, T R_0, T t, T D2, T D3) {
+    const T s2 = R_0 * R_0 + t * t;
+    const T r2 = r0 * r0 + s2;
+    const T r = sqrt(r2);
+    const T phi = atan2(t, R_0);
     if (!(r2 < 4.0 * (h * h))) {
-        const double x = r0 * ih, x2 = x * x, x3 = x2 * x;
-        const double K = x3 * (1.0 / kPi);
+        const T x = r0 * ih, x2 = x * x, x3 = x2 * x;
+        const T K = x3 * (1.0 / kPi);
         if (r0 >= 2.0 * h)
             return 0.25 / kPi * atan(t * s2 * R_0 / ((r + r0) * (R_0 * R_0 * r + t * t * r0))) + K * D3;
-        const double x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
-        const double p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
+        const T x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
+        const T p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
                                 : -2. / 3. * x3 + 0.3 * x5 - 0.1 * x6 + 7. / 5. * x;
         return 0.25 / kPi * (p * phi - atan(t * r0 / (R_0 * r))) + K * D3;
     }
-    const double inv = 1.0 / (r0 * r * (R_0 * t));
-    const double ir0 = r * (R_0 * t) * inv, ir = r0 * (R_0 * t) * inv, iR0 = r0 * r * t * inv;
-    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
-    const double K = w.r0h3 * (1.0 / kPi);
-    const double a = R_0 * ir0, a2k = a * a, u = t * ir;
-    const double tanp = t * iR0, sec2 = s2 * iR0 * iR0;
-    const double iomu2 = r2 / (r0 * r0 + R_0 * R_0);
-    const double I0 = phi;
-    const double I_2 = phi + a2k * tanp;
-    const double I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
-    const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
-    const double I1 = atan(tanp * r0 * ir);
-    const double I_1 = a / 2. * logs + I1;
-    const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
-    const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
+    const T inv = 1.0 / (r0 * r * (R_0 * t));
+    const T ir0 = r * (R_0 * t) * inv, ir = r0 * (R_0 * t) * inv, iR0 = r0 * r * t * inv;
+    const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
+    const T K = w.r0h3 * (1.0 / kPi);
+    const T a = R_0 * ir0, a2k = a * a, u = t * ir;
+    const T tanp = t * iR0, sec2 = s2 * iR0 * iR0;
+    const T iomu2 = r2 / (r0 * r0 + R_0 * R_0);
+    const T I0 = phi;
+    const T I_2 = phi + a2k * tanp;
+    const T I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
+    const T logs = log1p(2.0 * u * (1.0 + u) * iomu2);
+    const T I1 = atan(tanp * r0 * ir);
+    const T I_1 = a / 2. * logs + I1;
+    const T I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
+    const T I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
     if (r2 < h * h) return K * (1. / 6. * I_2 - 3. / 40. * w.r0h2 * I_4 + 1. / 40. * w.r0h3 * I_5 + wall_b1_in(w) * I0);
     return K * (0.25 * (4. / 3. * I_2 - w.r0h * I_3 + 0.3 * w.r0h2 * I_4 - 1. / 30. * w.r0h3 * I_5 + 1. / 15. * w.r0h_3 * I1) +
                 (r0 > h ? wall_b2_mid(w) : wall_b2_in(w)) * I0 + D2);
@@ -234,26 +244,26 @@ struct LenCubicEval {
 // in, the wall term B3 / r0^3 x pi/2 is a polynomial in r0 / h: the pair needs no reciprocal of r0.  For
 // r0 >= 2h (B3 / r0^3 = (h/r0)^3 / 4) it is atan(a1 a2 / (r0 r)) / (4 pi).  ih = 1 / h; r0, a1, a2 > 0 (the
 // callers skip zero corners); (D2a, D3a) and (D2b, D3b) are the two edge tiers.
-static __device__ KIWI_CORNER_INLINE double lattice_corner(double h, double ih, double r0, double a1, double a2, double D2a,
-                                                     double D3a, double D2b, double D3b) {
-    const double s2 = a1 * a1 + a2 * a2;
-    const double r2 = r0 * r0 + s2;
-    const double r = sqrt(r2);
+template <class T>
+static __device__ KIWI_CORNER_INLINE T lattice_corner(T h, T ih, T r0, T a1, T a2, T D2a, T D3a, T D2b, T D3b) {
+    const T s2 = a1 * a1 + a2 * a2;
+    const T r2 = r0 * r0 + s2;
+    const T r = sqrt(r2);
     if (!(r2 < 4.0 * (h * h))) {
-        const double x = r0 * ih, x2 = x * x, x3 = x2 * x;
-        const double K = x3 * (1.0 / kPi);
+        const T x = r0 * ih, x2 = x * x, x3 = x2 * x;
+        const T K = x3 * (1.0 / kPi);
         if (r0 >= 2.0 * h) return 0.25 / kPi * atan(a1 * a2 / (r0 * r)) + K * (D3a + D3b);
-        const double x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
-        const double p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
+        const T x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
+        const T p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
                                 : -2. / 3. * x3 + 0.3 * x5 - 0.1 * x6 + 7. / 5. * x;
         return -0.25 / kPi * atan(r0 * r / (a1 * a2)) + 0.125 * p + K * (D3a + D3b);
     }
-    const double inv1 = 1.0 / (r0 * r * (a1 * a2));
-    const double ir0 = r * (a1 * a2) * inv1, ir = r0 * (a1 * a2) * inv1;
-    const double ia1 = r0 * r * a2 * inv1, ia2 = r0 * r * a1 * inv1;
-    const LatticeWall w = lattice_wall(ih, h, ir0, r0);
-    const double K = w.r0h3 * (1.0 / kPi);
-    double pa, pb;
+    const T inv1 = 1.0 / (r0 * r * (a1 * a2));
+    const T ir0 = r * (a1 * a2) * inv1, ir = r0 * (a1 * a2) * inv1;
+    const T ia1 = r0 * r * a2 * inv1, ia2 = r0 * r * a1 * inv1;
+    const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
+    const T K = w.r0h3 * (1.0 / kPi);
+    T pa, pb;
     if (a2 <= a1) {
         pa = atan(a2 * ia1);
         pb = 0.5 * kPi - pa;
@@ -262,26 +272,26 @@ static __device__ KIWI_CORNER_INLINE double lattice_corner(double h, double ih, 
         pa = 0.5 * kPi - pb;
     }
     const bool inner = r2 < h * h;
-    const double b1 = inner ? wall_b1_in(w) : 0.0;
-    const double b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
-    const double q1 = r0 * r0 + a1 * a1, q2 = r0 * r0 + a2 * a2;
-    const double inv2 = 1.0 / (q1 * q2);
-    double sum = 0.0;
+    const T b1 = inner ? wall_b1_in(w) : 0.0;
+    const T b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
+    const T q1 = r0 * r0 + a1 * a1, q2 = r0 * r0 + a2 * a2;
+    const T inv2 = 1.0 / (q1 * q2);
+    T sum = 0.0;
 #pragma unroll 1
     for (int k = 0; k < 2; ++k) {
-        const double leg = k ? a2 : a1, opp = k ? a1 : a2, ileg = k ? ia2 : ia1, phi = k ? pb : pa;
-        const double a = leg * ir0, u = opp * ir;
-        const double tanp = opp * ileg, sec2 = s2 * ileg * ileg;
-        const double iomu2 = r2 * (k ? q1 : q2) * inv2;
-        const double a2k = a * a;
-        const double I0 = phi;
-        const double I_2 = phi + a2k * tanp;
-        const double I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
-        const double logs = log1p(2.0 * u * (1.0 + u) * iomu2);
+        const T leg = k ? a2 : a1, opp = k ? a1 : a2, ileg = k ? ia2 : ia1, phi = k ? pb : pa;
+        const T a = leg * ir0, u = opp * ir;
+        const T tanp = opp * ileg, sec2 = s2 * ileg * ileg;
+        const T iomu2 = r2 * (k ? q1 : q2) * inv2;
+        const T a2k = a * a;
+        const T I0 = phi;
+        const T I_2 = phi + a2k * tanp;
+        const T I_4 = phi + 2 * a2k * tanp + 1. / 3. * a2k * a2k * tanp * (2. + sec2);
+        const T logs = log1p(2.0 * u * (1.0 + u) * iomu2);
         // I_1, I_3, I_5 without their common I1 term (added below for the pair)
-        const double I_1 = a / 2. * logs;
-        const double I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
-        const double I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
+        const T I_1 = a / 2. * logs;
+        const T I_3 = I_1 + a * (1. + a2k) / 4. * (2 * u * iomu2 + logs);
+        const T I_5 = I_3 + a * (1. + a2k) * (1. + a2k) / 16. * ((10 * u - 6 * u * u * u) * iomu2 * iomu2 + 3. * logs);
         if (inner) sum += 1. / 6. * I_2 - 3. / 40. * w.r0h2 * I_4 + 1. / 40. * w.r0h3 * I_5 + b1 * I0;
         else
             sum += 0.25 * (4. / 3. * I_2 - w.r0h * I_3 + 0.3 * w.r0h2 * I_4 - 1. / 30. * w.r0h3 * I_5) + b2 * I0 +
@@ -289,8 +299,8 @@ static __device__ KIWI_CORNER_INLINE double lattice_corner(double h, double ih, 
     }
     // I1 enters both pyramids with one coefficient (through I_1, I_3, I_5 and, between h and 2h, on its own):
     // the pair needs I1a + I1b = atan(r0 r / (a1 a2)) only.
-    const double I1s = atan((r0 * r) * (r0 * r) * inv1);
-    const double c1 = inner ? 1. / 40. * w.r0h3 : 0.25 * (-w.r0h - 1. / 30. * w.r0h3 + 1. / 15. * w.r0h_3);
+    const T I1s = atan((r0 * r) * (r0 * r) * inv1);
+    const T c1 = inner ? 1. / 40. * w.r0h3 : 0.25 * (-w.r0h - 1. / 30. * w.r0h3 + 1. / 15. * w.r0h_3);
     return K * (sum + c1 * I1s);
 }
 
