@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 
 #include "binning.cuh"
 #include "cart_common.cuh"
@@ -46,6 +47,7 @@ constexpr int kAdjSCap = 2304;  // corner entries per chunk (a full 8^3 particle
 constexpr int kAdjERec = 10;    // D2, D3 as Dual4
 constexpr int kAdjSRec = 5;     // S as Dual4
 constexpr size_t kAdjDynSmem = sizeof(double) * (kAdjERec * kAdjECap + kAdjSRec * kAdjSCap);
+constexpr int kAdjPtCap = kAdjSCap / 3;  // lattice points per chunk (three corner items each)
 
 struct AdjGrads {
     double *x, *y, *z, *h, *m, *vx, *vy, *vz;
@@ -94,7 +96,9 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
         s_vy[kAdjPMax], s_vz[kAdjPMax];
     __shared__ int s_lo[kAdjPMax][3], s_dim[kAdjPMax][3], s_eoff[kAdjPMax], s_soff[kAdjPMax];
     __shared__ uint32_t s_entry[kAdjPMax];
-    __shared__ int s_np, s_etot, s_stot;
+    __shared__ uint32_t s_mag[kAdjPMax][4];  // div_magic of n0, n1, n2 and n1 n2
+    __shared__ uint32_t s_blist[kAdjPtCap];
+    __shared__ int s_np, s_etot, s_stot, s_nexp, s_ncheap;
     __shared__ double s_red[kAdjLatThreads / 32][8];
     extern __shared__ double s_adj[];
     double* s_E = s_adj;
@@ -153,11 +157,16 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 s_eoff[lane] = ie - ne;
                 s_soff[lane] = is - ns;
                 s_entry[lane] = e;
+                s_mag[lane][0] = div_magic(d0 + 1);
+                s_mag[lane][1] = div_magic(d1 + 1);
+                s_mag[lane][2] = div_magic(d2 + 1);
+                s_mag[lane][3] = div_magic((d1 + 1) * (d2 + 1));
             }
             if (lane == np - 1) {
                 s_np = np;
                 s_etot = ie;
                 s_stot = is;
+                s_nexp = s_ncheap = 0;
             }
         }
         __syncthreads();
@@ -196,16 +205,60 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
             store_dual(s_E + kAdjERec * it, D2);
             store_dual(s_E + kAdjERec * it + 5, D3);
         }
+
+        // (B0) the corner items, listed lattice point by lattice point as in the forward kernel: corners
+        // that no evaluated cell reads left out (the same padded test), corners beyond 2h (or zero) from
+        // the end of s_blist so that they run in warps of their own; a list entry packs (particle, i, j, k).
+        {
+            const int ptot = stot / 3;
+            const int poff_l = lane < np ? s_soff[lane] / 3 : INT_MAX;
+            for (int base = warp * 32; base < ptot; base += kAdjLatThreads) {
+                const int pt = base + lane;
+                int cls = -1;  // -1 none, 0 general, 1 cheap
+                uint32_t rec = 0;
+                const int jp = warp_owner(base, poff_l, lane);
+                const int poff = __shfl_sync(0xffffffffu, poff_l, jp & 31);
+                if (pt < ptot) {
+                    const int lp = pt - poff;
+                    const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
+                    const int i = div_by(lp, s_mag[jp][3]), rem = lp - i * n12;
+                    const int jj = div_by(rem, s_mag[jp][2]), k = rem - jj * n2;
+                    const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
+                    const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
+                    const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+                    const double h = s_h[jp], radius = mul_rn(g.support_in_h, h);
+                    const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
+                    const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
+                    const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
+                    if (ex * ex + ey * ey + ez * ez < radius * radius) {
+                        const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
+                        cls = (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) ? 1 : 0;
+                        rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
+                    }
+                }
+                const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
+                int pe = 0, pcb = 0;
+                if (lane == 0) {
+                    if (me) pe = atomicAdd(&s_nexp, __popc(me));
+                    if (mc) pcb = atomicAdd(&s_ncheap, __popc(mc));
+                }
+                pe = __shfl_sync(0xffffffffu, pe, 0);
+                pcb = __shfl_sync(0xffffffffu, pcb, 0);
+                const unsigned below = (1u << lane) - 1;
+                if (cls >= 0) s_blist[cls == 0 ? pe + __popc(me & below) : kAdjPtCap - 1 - pcb - __popc(mc & below)] = rec;
+            }
+        }
         __syncthreads();
 
         // (B) corner values with derivatives
-        for (int it = threadIdx.x; it < stot; it += kAdjLatThreads) {
-            const int jp = chunk_search(s_soff, np, it);
-            const int s = it - s_soff[jp];
+        const int nexp = s_nexp, ncheap = s_ncheap;
+        for (int li = threadIdx.x; li < 3 * (nexp + ncheap); li += kAdjLatThreads) {
+            const int pli = li / 3, axis = li - 3 * pli;
+            const uint32_t rec = s_blist[pli < nexp ? pli : kAdjPtCap - ncheap + (pli - nexp)];
+            const int jp = (int)(rec & 31u), i = (int)((rec >> 5) & 15u), jj = (int)((rec >> 9) & 15u),
+                      k = (int)((rec >> 13) & 15u);
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-            const int L = n0 * n1 * n2;
-            const int axis = s / L, rem = s % L;
-            const int i = rem / (n1 * n2), jj = (rem / n2) % n1, k = rem % n2;
+            const int it = s_soff[jp] + axis * (n0 * n1 * n2) + (i * n1 + jj) * n2 + k;
             const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
             const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
             const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);

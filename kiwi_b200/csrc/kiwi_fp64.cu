@@ -302,7 +302,6 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGe
 #endif
 constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;
 constexpr int kLatGenMinBlocks = KIWI_LATTICE_GEN_MIN_BLOCKS;
-constexpr double kNeedPad = 1.0 + 1e-6;  // half-width factor of the cells around a lattice point
 constexpr int kLatPtCap = kLatSCap / 3;  // lattice points per chunk (three corner items each)
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");
 static_assert(kLatECap <= 2048, "packed edge-list entries");
@@ -312,19 +311,6 @@ constexpr size_t kLatMaxDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : k
 constexpr size_t kLatTabDynSmem = sizeof(double) * kLatSCap;
 
 
-// The chunk particle that owns item base + lane, for a warp whose 32 items start at base (a multiple of
-// 32): off is this lane's particle's first item (lane < np; INT_MAX beyond).  Every particle owns at least
-// one item, so the particles starting inside the window are distinct bits of one mask.  All 32 lanes call.
-__device__ __forceinline__ int warp_owner(int base, int off, int lane) {
-    const unsigned before = __ballot_sync(0xffffffffu, off <= base);
-    const int d = off - base;
-    const unsigned starts = __reduce_or_sync(0xffffffffu, (d > 0 && d < 32) ? 1u << d : 0u);
-    return __popc(before) - 1 + __popc(starts & (0xffffffffu >> (31 - lane)));
-}
-
-// x / n for 0 <= x < 1400 and 1 <= n <= 81 as (x * magic(n)) >> 20 (exact over that range).
-__host__ __device__ __forceinline__ uint32_t div_magic(int n) { return ((1u << 20) + (uint32_t)n - 1) / (uint32_t)n; }
-__device__ __forceinline__ int div_by(int x, uint32_t m) { return (int)(((uint32_t)x * m) >> 20); }
 
 // One CTA = one tile.  The tile's particle list (ascending particle index) is walked in chunks that fit
 // the edge and corner tables in shared memory.  Per chunk: (A) the edge tiers of every (plane, edge

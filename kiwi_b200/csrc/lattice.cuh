@@ -446,6 +446,25 @@ static __device__ __forceinline__ double lattice_generic_vertex(const KiwiKernel
     return (s > 0 ? rec[3 + s] : 0.0) + G;
 }
 
+// Bookkeeping shared by the lattice kernels (forward and adjoint).
+// Half-width factor of the cells around a lattice point in the test for corners that no evaluated cell
+// reads: the cells are padded by 1e-6 of a cell so that rounding never drops a corner a cell reads.
+constexpr double kNeedPad = 1.0 + 1e-6;
+
+// The chunk particle that owns item base + lane, for a warp whose 32 items start at base (a multiple of
+// 32): off is this lane's particle's first item (lane < np; INT_MAX beyond).  Every particle owns at least
+// one item, so the particles starting inside the window are distinct bits of one mask.  All 32 lanes call.
+__device__ __forceinline__ int warp_owner(int base, int off, int lane) {
+    const unsigned before = __ballot_sync(0xffffffffu, off <= base);
+    const int d = off - base;
+    const unsigned starts = __reduce_or_sync(0xffffffffu, (d > 0 && d < 32) ? 1u << d : 0u);
+    return __popc(before) - 1 + __popc(starts & (0xffffffffu >> (31 - lane)));
+}
+
+// x / n for 0 <= x < 1400 and 1 <= n <= 81 as (x * magic(n)) >> 20 (exact over that range).
+__host__ __device__ __forceinline__ uint32_t div_magic(int n) { return ((1u << 20) + (uint32_t)n - 1) / (uint32_t)n; }
+__device__ __forceinline__ int div_by(int x, uint32_t m) { return (int)(((uint32_t)x * m) >> 20); }
+
 // Offset of lattice plane P (global plane index) from the particle coordinate x0 along one axis.
 __device__ __forceinline__ double lattice_offset(double mn, double d, int P, double x0) {
     return add_rn(mn, mul_rn((double)P, d)) - x0;
