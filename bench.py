@@ -165,6 +165,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def hbm_peak_gbs():
+    """HBM copy bandwidth for the roofline: MEASURED_PEAKS.json's hbm_gbs (measured on this pool's B200s),
+    else the pool's earlier measurement of 6.65 TB/s, marked as the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent; of fallback)"
+
+
 def make_workload(n, res, seed, kernel_name):
     from kiwi_b200.workloads import lognormal_cube
     import kiwi_b200
@@ -829,12 +839,7 @@ def main():
         if (not is32 and args.n == 2_000_000 and args.res == 256 and args.kernel == "cubic_spline" and
                 not args.full_box and args.precision == "fp64" and ws == 1):
             traffic = LATTICE_DRAM_BYTES_FULL
-        hbm_peak = None
-        try:
-            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-                hbm_peak = float(json.load(f)["hbm_gbs"])
-        except (OSError, ValueError, KeyError):
-            pass
+        hbm_peak, hbm_src = hbm_peak_gbs()
         tab_roofline = None
         if args.tabulated:
             # each vertex pyramid is one trilinear lookup: 8 table entries (64 bytes) from a 182 MB table
@@ -844,7 +849,7 @@ def main():
                             "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
                             "frac": ach / hbm_peak if hbm_peak else None, "traffic": None,
                             "algorithmic_bytes": "64 bytes (8 table entries) per lookup x lookups per launch",
-                            "lookups_per_launch": lookups, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                            "lookups_per_launch": lookups, "peak_source": hbm_src,
                             "gather_ms_per_launch": g_ms}
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
@@ -867,7 +872,7 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "hbm": ({"achieved_gbs": traffic / (g_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
-                                  "frac": traffic / (g_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": "MEASURED_PEAKS.json"}
+                                  "frac": traffic / (g_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src}
                                  if traffic and hbm_peak else None),
                          "work_per_pair_flops": work_per_pair, "evaluated_pairs_per_launch": evaluated_per_launch,
                          "peak_source": ("measured FP32 FMA probe (kiwi_measure_fp32_peak)" if is32 else

@@ -330,6 +330,8 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         s_vy[kLatPMax], s_vz[kLatPMax], s_ih[kLatPMax];
     __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_soff[kLatPMax];
     __shared__ uint32_t s_mag[kLatPMax][4];  // div_magic of n0, n1, n2 and n1 n2
+    __shared__ TabWidths s_tw;               // TAB: the table's bin widths and their reciprocals
+    if (TAB && threadIdx.x == 0) s_tw = tab_widths(tab);  // read after the chunk load's barrier
     __shared__ int s_np, s_etot, s_stot, s_nexp, s_ncheap, s_nheavy;
     __shared__ uint32_t s_blist[kLatPtCap];
     __shared__ uint16_t s_hlist[kLatECap];
@@ -601,8 +603,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 const double a1 = fabs(u1), a2 = fabs(u2);
                 if (TAB) {
                     // two right-triangle vertex pyramids; cos(phi) from the legs
-                    const double h = s_h[jp], rr = sqrt(a1 * a1 + a2 * a2);
-                    f = tab_gridded_c(tab, h, a1 / rr, r0, a1, n_clamp) + tab_gridded_c(tab, h, a2 / rr, r0, a2, n_clamp);
+                    f = tab_pair(tab, s_tw, s_ih[jp], r0, a1, a2, n_clamp);
                 } else if (GENERIC) {
                     const double H = mul_rn(g.support_in_h, s_h[jp]);
                     f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
