@@ -606,8 +606,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     f = tab_pair(tab, s_tw, s_ih[jp], r0, a1, a2, n_clamp);
                 } else if (GENERIC) {
                     const double H = mul_rn(g.support_in_h, s_h[jp]);
-                    f = lattice_generic_vertex(K, H, r0, a1, a2, s_E + kLatGenERec * e1) +
-                        lattice_generic_vertex(K, H, r0, a2, a1, s_E + kLatGenERec * e2);
+                    f = lattice_generic_corner(K, H, r0, a1, a2, s_E + kLatGenERec * e1, s_E + kLatGenERec * e2);
                 } else {
                     f = lattice_corner(s_h[jp], s_ih[jp], r0, a1, a2, s_D2[e1], s_D3[e1], s_D2[e2], s_D3[e2]);
                 }

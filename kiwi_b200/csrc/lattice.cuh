@@ -427,23 +427,44 @@ static __device__ __forceinline__ void lattice_generic_edge(const KiwiKernelTabl
     }
 }
 
+
 // Vertex tier of a generic kernel for the right triangle with legs R0 (projection -> edge line) and t
 // (along the edge) in a wall at distance r0 (generic_vertex, :150-156, at phi = atan2(t, R0)): the region
 // segment holding phi, its offset, and G_k(phi).
-static __device__ __forceinline__ double lattice_generic_vertex(const KiwiKernelTable* K, double H, double r0,
-                                                               double R0, double t, const double* rec) {
-    const int packed = (int)rec[0];
-    const int nseg = packed & 7, k0 = packed >> 3;
-    if (nseg == 0 || t == 0.0) return 0.0;
-    const double a = R0 / r0, a2 = a * a;
-    const double rr = sqrt(R0 * R0 + t * t);
-    const double phi = atan2(t, R0);
-    const double sinp = t / rr, cosp = R0 / rr;
-    int s = 0;
-    while (s + 1 < nseg && phi > rec[1 + s]) ++s;
+// The two vertex tiers of a lattice corner (legs a1, a2 in the wall at r0; the edge records rec1 of the
+// a1 line and rec2 of the a2 line: vertex 1 has R0 = a1, t = a2 and vertex 2 the reverse) share what the
+// pair has in common: the distance sqrt(a1^2 + a2^2) and its reciprocal, 1 / r0, q0 = r0 / H and its
+// kernel region, and the angle pair (the smaller one from atan2, the larger its complement, as in
+// lattice_corner).  r0, a1, a2 > 0.
+static __device__ __forceinline__ double lattice_generic_corner(const KiwiKernelTable* K, double H, double r0,
+                                                               double a1, double a2, const double* rec1,
+                                                               const double* rec2) {
+    const double ir0 = 1.0 / r0, irr = 1.0 / sqrt(a1 * a1 + a2 * a2);
     const double q0 = r0 / H;
-    const double G = lattice_generic_G(K, q0, generic_region(K, q0), k0 + s, a, a2, phi, sinp, cosp);
-    return (s > 0 ? rec[3 + s] : 0.0) + G;
+    const int j = generic_region(K, q0);
+    double pa, pb;
+    if (a2 <= a1) {
+        pa = atan2(a2, a1);
+        pb = 0.5 * kPi - pa;
+    } else {
+        pb = atan2(a1, a2);
+        pa = 0.5 * kPi - pb;
+    }
+    double sum = 0.0;
+#pragma unroll 1
+    for (int v = 0; v < 2; ++v) {
+        const double* rec = v ? rec2 : rec1;
+        const int packed = (int)rec[0];
+        const int nseg = packed & 7, k0 = packed >> 3;
+        if (nseg == 0) continue;
+        const double R0 = v ? a2 : a1, t = v ? a1 : a2, phi = v ? pb : pa;
+        const double a = R0 * ir0;
+        int s = 0;
+        while (s + 1 < nseg && phi > rec[1 + s]) ++s;
+        const double G = lattice_generic_G(K, q0, j, k0 + s, a, a * a, phi, t * irr, R0 * irr);
+        sum += (s > 0 ? rec[3 + s] : 0.0) + G;
+    }
+    return sum;
 }
 
 // Bookkeeping shared by the lattice kernels (forward and adjoint).
