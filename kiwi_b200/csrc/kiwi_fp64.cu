@@ -346,6 +346,17 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the tile's lattice planes (every particle box is clipped to the tile, so its planes are these) and
+    // cell centres, formed once as lattice_offset and cell_centre form them; read after the first barrier
+    __shared__ double s_pl[3][kTileX + 1], s_cc[3][kTileX];
+    static_assert(kTileX == kTileY && kTileX == kTileZ, "cubic tiles");
+    if (threadIdx.x < 3 * (kTileX + 1)) {
+        const int a = threadIdx.x / (kTileX + 1), l = threadIdx.x % (kTileX + 1);
+        const double mn = a == 0 ? g.x_min : (a == 1 ? g.y_min : g.z_min), d = a == 0 ? g.dpx : (a == 1 ? g.dpy : g.dpz);
+        const int b0 = a == 0 ? bx : (a == 1 ? by : bz);
+        s_pl[a][l] = add_rn(mn, mul_rn((double)(b0 + l), d));
+        if (l < kTileX) s_cc[a][l] = cell_centre(mn, b0 + l, d);
+    }
 
     double acc[kCellsPerThread][4];
 #pragma unroll
@@ -502,9 +513,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
                     const int i = div_by(lp, s_mag[jp][3]), rem = lp - i * n12;
                     const int jj = div_by(rem, s_mag[jp][2]), k = rem - jj * n2;
-                    const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
-                    const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
-                    const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+                    const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
+                    const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
+                    const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
                     const double h = s_h[jp];
                     bool keep = true;
                     if (CULL) {
@@ -577,9 +588,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 it = s_soff[jp] + axis * ((s_dim[jp][0] + 1) * n1 * n2) + (i * n1 + jj) * n2 + k;
             }
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-            const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
-            const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
-            const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+            const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
+            const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
+            const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
             const int eb = s_eoff[jp];
             const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
             double r0, u1, u2;
@@ -627,9 +638,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 ++n_bbox;
                 const double x0 = s_x[j], y0 = s_y[j], z0 = s_z[j];
                 const double radius = mul_rn(g.support_in_h, s_h[j]);
-                const double ex = fmax(fabs(x0 - cell_centre(g.x_min, gx, g.dpx)) - g.hpx, 0.0);
-                const double ey = fmax(fabs(y0 - cell_centre(g.y_min, gy, g.dpy)) - g.hpy, 0.0);
-                const double ez = fmax(fabs(z0 - cell_centre(g.z_min, gz, g.dpz)) - g.hpz, 0.0);
+                const double ex = fmax(fabs(x0 - s_cc[0][gx - bx]) - g.hpx, 0.0);
+                const double ey = fmax(fabs(y0 - s_cc[1][gy - by]) - g.hpy, 0.0);
+                const double ez = fmax(fabs(z0 - s_cc[2][gz - bz]) - g.hpz, 0.0);
                 const bool in = ex * ex + ey * ey + ez * ez < radius * radius;
                 n_sphere += in;
                 if (CULL && !in) continue;
@@ -640,9 +651,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 const double* Sy = Sx + L;
                 const double* Sz = Sy + L;
                 auto at = [&](const double* S, int a, int b, int cc) { return S[(a * n1 + b) * n2 + cc]; };
-                const double sx1 = sgn(lattice_offset(g.x_min, g.dpx, gx + 1, x0)), sx0 = sgn(lattice_offset(g.x_min, g.dpx, gx, x0));
-                const double sy1 = sgn(lattice_offset(g.y_min, g.dpy, gy + 1, y0)), sy0 = sgn(lattice_offset(g.y_min, g.dpy, gy, y0));
-                const double sz1 = sgn(lattice_offset(g.z_min, g.dpz, gz + 1, z0)), sz0 = sgn(lattice_offset(g.z_min, g.dpz, gz, z0));
+                const int lx = gx - bx, ly = gy - by, lz = gz - bz;
+                const double sx1 = sgn(s_pl[0][lx + 1] - x0), sx0 = sgn(s_pl[0][lx] - x0);
+                const double sy1 = sgn(s_pl[1][ly + 1] - y0), sy0 = sgn(s_pl[1][ly] - y0);
+                const double sz1 = sgn(s_pl[2][lz + 1] - z0), sz0 = sgn(s_pl[2][lz] - z0);
                 double msum = 0.0;
                 msum += sx1 * (at(Sx, i + 1, jj + 1, k + 1) - at(Sx, i + 1, jj, k + 1) - at(Sx, i + 1, jj + 1, k) + at(Sx, i + 1, jj, k));
                 msum -= sx0 * (at(Sx, i, jj + 1, k + 1) - at(Sx, i, jj, k + 1) - at(Sx, i, jj + 1, k) + at(Sx, i, jj, k));
