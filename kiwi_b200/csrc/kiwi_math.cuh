@@ -153,17 +153,6 @@ KIWI_HD CubicEdgeT<T> cubic_edge_t(const CubicWallT<T>& w, T R_0) {
 }
 KIWI_HD CubicEdge cubic_edge(const CubicWall& w, double R_0) { return cubic_edge_t<double>(w, R_0); }
 
-// I1 = atan(u/a) alone, by the same operations as the full series: beyond 2h the vertex tier needs only
-// I0 = phi and I1, so the logarithms, tan and I_2..I_5 (dead there) can be skipped where whole warps are
-// in that region (the lattice kernel groups its corner items that way).
-template <class T>
-KIWI_HD T phi_I1(T sinp, T cosp, T a, T a2) {
-    const T cosp2 = cosp * cosp;
-    const T mu = cosp / a / sqrt(1. + cosp2 / a2);
-    const T u = sinp * sqrt(1 - mu * mu);
-    return atan(u / a);
-}
-
 template <class T>
 KIWI_HD T cubic_vertex_t(const CubicWallT<T>& w, const CubicEdgeT<T>& e, T phi) {
     if (!w.valid || !e.valid) return T(0.0);

@@ -16,8 +16,8 @@
 // x (inclusion-exclusion of S over the face's 4 corners).  This is algebraically the reference's sum --
 // the same 48 vertex-pyramid terms with the same signs (a face's edge/foot-beyond rule of
 // src/kernel_integral.cpp:613-631 is the 2-D inclusion-exclusion of a cumulative function) -- with
-// the vertex angle taken from the right triangle directly (phi = atan2(t, R_0), sin and cos from t, R_0
-// and their hypotenuse) instead of acos(R_0/r12) followed by sincos.
+// every series written in its triangle's or edge's own lengths from a few reciprocals (lattice_edge,
+// lattice_corner, lattice_pyramid) instead of acos(R_0/r12) followed by sincos and a division per ratio.
 #pragma once
 
 #include "cart_common.cuh"
@@ -28,41 +28,6 @@ namespace kiwi_b200 {
 constexpr int kLatPMax = 32;     // particles per chunk
 constexpr int kLatECap = 1536;   // edge-tier entries per chunk (one full 8^3 particle box needs 486)
 constexpr int kLatSCap = 4096;   // corner values per chunk (one full 8^3 particle box needs 2187)
-
-// Vertex-pyramid mass of the right triangle with legs R_0 (projection -> edge line) and t (along the
-// edge) in a wall at distance r0: the vertex tier of src/kernel_integral.cpp:356-400 at phi = atan2(t, R_0)
-// (beyond 2h only I0 and I1 are needed, as in cubic_vertex).
-// Written over the real type T: double here, Dual4 (dual.cuh) for the adjoint.
-template <class T>
-static __device__ __noinline__ T lattice_vertex_t(T h, T r0, T R_0, T t, T D2, T D3) {
-    if (r0 == 0.0 || R_0 == 0.0 || t == 0.0) return T(0.0);
-    const CubicWallT<T> w = cubic_wall_t<T>(h, r0);
-    const T a = R_0 / r0;
-    const T a2 = a * a;
-    const T s2 = R_0 * R_0 + t * t;
-    const T rr = sqrt(s2);
-    const T phi = atan2(t, R_0);
-    const T sinp = t / rr, cosp = R_0 / rr;
-    const T r2 = r0 * r0 + s2;
-    const T r03 = w.r03, r0h2 = w.r0h2, r0h3 = w.r0h3, r0h_3 = w.r0h_3;
-    if (!(r2 < 4.0 * w.h2)) {
-        const T I1 = phi_I1<T>(sinp, cosp, a, a2);
-        return r0h3 / kPi * (-0.25 * r0h_3 * I1 + w.B3 / r03 * phi + D3);
-    }
-    const PhiSeriesT<T> s = phi_series_sc<T>(phi, sinp, cosp, a, a2);
-    T full_int;
-    if (r2 < w.h2) {
-        full_int = r0h3 / kPi * (1. / 6. * s.I_2 - 3. / 40. * r0h2 * s.I_4 + 1. / 40. * r0h3 * s.I_5 + w.B1 / r03 * s.I0);
-    } else if (r2 < 4.0 * w.h2) {
-        full_int = r0h3 / kPi * (0.25 * (4. / 3. * s.I_2 - (r0 / h) * s.I_3 + 0.3 * r0h2 * s.I_4 - 1. / 30. * r0h3 * s.I_5 + 1. / 15. * r0h_3 * s.I1) + w.B2 / r03 * s.I0 + D2);
-    } else {
-        full_int = r0h3 / kPi * (-0.25 * r0h_3 * s.I1 + w.B3 / r03 * s.I0 + D3);
-    }
-    return full_int;
-}
-static __device__ __forceinline__ double lattice_vertex(double h, double r0, double R_0, double t, double D2, double D3) {
-    return lattice_vertex_t<double>(h, r0, R_0, t, D2, D3);
-}
 
 // The edge and corner tiers are inlined into the lattice kernels by default (at 80 registers a call
 // costs more in saved registers than the larger code does); define either as __noinline__ to keep it out
