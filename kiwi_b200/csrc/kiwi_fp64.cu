@@ -293,15 +293,20 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_cart_gather_tab(CartGe
 // ------------------------------------------------------------------ lattice-factorised gather (cubic)
 
 // Resident CTAs per SM the register budget is sized for: three for the cubic kernel (80 registers; its
-// 70 KB of shared memory fits three times), two for the generic and tabulated ones.
+// 70 KB of shared memory fits three times) and for the tabulated one (39 KB; four was slower), two for the
+// generic one (78 KB of shared memory).
 #ifndef KIWI_LATTICE_MIN_BLOCKS
 #define KIWI_LATTICE_MIN_BLOCKS 3
 #endif
 #ifndef KIWI_LATTICE_GEN_MIN_BLOCKS
 #define KIWI_LATTICE_GEN_MIN_BLOCKS 2
 #endif
+#ifndef KIWI_LATTICE_TAB_MIN_BLOCKS
+#define KIWI_LATTICE_TAB_MIN_BLOCKS 3
+#endif
 constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;
 constexpr int kLatGenMinBlocks = KIWI_LATTICE_GEN_MIN_BLOCKS;
+constexpr int kLatTabMinBlocks = KIWI_LATTICE_TAB_MIN_BLOCKS;
 constexpr int kLatPtCap = kLatSCap / 3;  // lattice points per chunk (three corner items each)
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed corner-list entries");
 static_assert(kLatECap <= 2048, "packed edge-list entries");
@@ -730,7 +735,7 @@ __global__ void __launch_bounds__(kThreads, kLatGenMinBlocks) k_cart_lattice_gen
 
 // The lattice form with the tabulated integral, every cell of the particles' bounding boxes (outside the
 // support the lookups do not cancel exactly, and the reference keeps what they leave).
-__global__ void __launch_bounds__(kThreads, kLatGenMinBlocks) k_cart_lattice_tab(CartGeom g, DevParticles P, const TabDev tab,
+__global__ void __launch_bounds__(kThreads, kLatTabMinBlocks) k_cart_lattice_tab(CartGeom g, DevParticles P, const TabDev tab,
                                                                               const uint32_t* __restrict__ list,
                                                                               const int64_t* __restrict__ range,
                                                                               const int32_t* __restrict__ tile_map,
