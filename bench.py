@@ -53,9 +53,10 @@ EDGE_MIDDLE = 127.0 + TRANS_FLOPS * 6
 EDGE_INNER = 209.0 + TRANS_FLOPS * 12
 VERTEX_PYRAMID = 121.0 + TRANS_FLOPS * 4
 CELL_ASSEMBLY = 60.0
-# DRAM bytes (read + write) of one k_cart_lattice launch on the default workload (2M particles, 256^3),
-# ncu dram__bytes_read.sum + dram__bytes_write.sum (profiles/k_cart_lattice_fp64_lognormal.md).
-LATTICE_DRAM_BYTES_FULL = 212.32e6 + 520.65e6
+
+# DRAM bytes (read + write) of one k_cart_lattice launch on the default workload (2 M particles, 256^3) from
+# a one-pass ncu capture, and the commit whose kernel was captured.
+LATTICE_TRAFFIC = {"bytes": 212.32e6 + 520.65e6, "commit": "e7ab734", "kernel": "k_cart_lattice"}
 
 L2_BYTES = 126 * 1024 * 1024
 # the tabulated integral: one trilinear lookup reads 8 table entries
@@ -80,7 +81,6 @@ def parse():
                          "instead of its closed form; every cell of each support bounding box, as the reference")
     ap.add_argument("--seed", type=int, default=1002)
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="with --precision fp64: skip timing the FP32-mixed form beside it")
@@ -175,81 +175,119 @@ def hbm_peak_gbs():
         return 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent; of fallback)"
 
 
-def make_workload(n, res, seed, kernel_name):
-    from kiwi_b200.workloads import lognormal_cube
-    import kiwi_b200
+def _standalone(name, relpath):
+    """Loads one pure-Python file of the package by path, without importing the package itself (so that the
+    reference arm maps no kiwi_b200 shared library into its process)."""
+    import importlib.util
 
-    hfact = kiwi_b200.get_kernel(kernel_name).hfact
-    P, bounds = lognormal_cube(n=n, seed=seed, mesh=min(res, 256), hfact=hfact)
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, relpath))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def kernel_hfact(kernel_name):
+    """hfact of a kernel, from the kernel-table generator's definitions (pure Python)."""
+    gen = _standalone("kiwi_kernel_table_gen", "kiwi_b200/tables/gen_kernel_tables.py")
+    for K in gen.KERNELS:
+        if kernel_name in (K.key, K.key.lower(), K.name.lower().replace(" ", "_")):
+            return K.hfact
+    raise ValueError(f"unknown kernel {kernel_name!r}")
+
+
+def make_workload(n, res, seed, kernel_name):
+    wl = _standalone("kiwi_workloads", "kiwi_b200/workloads.py")
+    P, bounds = wl.lognormal_cube(n=n, seed=seed, mesh=min(res, 256), hfact=kernel_hfact(kernel_name))
     return P, bounds, (res, res, res)
 
 
-def cpu_baseline(P, bounds, shape, kernel_name, target_s):
-    """The reference's own OpenMP pair loop (oracle/_ref) on a seeded particle sample sized to ~target_s."""
+def workload_config(args, nc=None, ws=1, split=False):
+    """The `config` object of the sph-to-grid line, shared by both arms."""
+    cfg = {"workload": f"lognormal_cube n={args.n} sigma_ln=1.5 P(k)~k^-4 10pc padded, grid {args.res}^3, "
+                       f"kernel {args.kernel}" + (", tabulated integral" if args.tabulated else ""),
+           "precision": args.precision, "particles_per_gpu": args.n, "cells": nc or args.res ** 3,
+           "l2": "flushed between timed steps (256 MB write) and inputs+outputs > L2",
+           "parallelism": (f"cell-tile parts x{ws} of one grid" if split else f"replicas x{ws}")
+           if ws > 1 else "single GPU"}
+    return cfg
+
+
+# The reference's pair loop runs OpenMP schedule(dynamic, 256) over particles; a sample step gives every
+# thread this many 256-particle chunks, so that the idle tail of the last chunks stays a small part of it.
+REF_CHUNKS_PER_THREAD = 6
+
+
+def ref_sample(P, bounds, shape, kernel_name, ref, threads, steps, warmup):
+    """The reference's own OpenMP pair loop (oracle/_ref: its KernelIntegrator::face over the six box faces
+    of every bounding-box cell, schedule(dynamic, 256), per-cell sums into a scalar instead of the grid) on
+    consecutive ranges of a seeded permutation of the workload's particles: `warmup` untimed ranges of one
+    chunk per thread, then `steps` timed ranges of REF_CHUNKS_PER_THREAD chunks per thread.
+    Returns (seconds, bbox pairs, support pairs, particles per step) summed over the timed ranges."""
+    n = len(P["x"])
+    perm = np.random.default_rng(99).permutation(n)
+    Ps = {k: np.ascontiguousarray(v[perm]) for k, v in P.items()}
+    pos = 0
+    for _ in range(warmup):
+        m = min(256 * threads, n - pos)
+        ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads, p_range=(pos, pos + m))
+        pos = (pos + m) % n
+    per_step = min(n, REF_CHUNKS_PER_THREAD * 256 * threads)
+    tt, bb, ss = 0.0, 0, 0
+    for _ in range(steps):
+        if pos + per_step > n:
+            pos = 0
+        t, b, s, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads,
+                                     p_range=(pos, pos + per_step))
+        pos += per_step
+        tt, bb, ss = tt + t, bb + b, ss + s
+    return tt, bb, ss, per_step
+
+
+def cpu_baseline(P, bounds, shape, kernel_name):
+    """One step of the reference arm (below) timed on this machine's host cores: the reported CPU baseline."""
     from oracle.oracle import load_ref
 
     ref = load_ref()
     if ref is None:
         return None
     threads = ref.max_threads()
-    n = len(P["x"])
-    rng = np.random.default_rng(99)
-    perm = rng.permutation(n)
-    Ps = {k: np.ascontiguousarray(v[perm]) for k, v in P.items()}
-    warm = min(n, 16 * threads)
-    ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads, p_range=(0, warm))  # thread start-up
-    probe_end = min(n, warm + 128 * threads)
-    t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads,
-                                       p_range=(warm, probe_end))
-    rate = (probe_end - warm) / max(t, 1e-3)  # particles / s
-    probe = probe_end
-    m = int(min(n - probe, max(threads * 4, rate * target_s)))
-    t, pairs, sph, _ = ref.pair_sample(Ps, bounds, shape, kernel=kernel_name, threads=threads,
-                                       p_range=(probe, probe + m))
-    return {"value": sph / t, "unit": "pair-integrals/s", "cores": threads, "kind": "reference",
-            "sample": f"{m} of {n} particles (seeded permutation), {pairs} bounding-box / {sph} support pairs, "
-                      f"{t:.1f} s wall on {threads} OpenMP threads",
-            "bbox_pairs_per_s": pairs / t}
+    t, b, s, per = ref_sample(P, bounds, shape, kernel_name, ref, threads, steps=1, warmup=1)
+    return {"value": s / t, "unit": "pair-integrals/s", "cores": threads, "kind": "reference",
+            "sample": f"{per} of {len(P['x'])} particles (seeded permutation; {REF_CHUNKS_PER_THREAD} chunks of 256 "
+                      f"per thread), {b} bounding-box / {s} support pairs, {t:.1f} s wall on {threads} OpenMP "
+                      f"threads; the reference's KernelIntegrator::face over each cell's six box faces",
+            "bbox_pairs_per_s": b / t}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU implementation of the path (oracle/_ref, built from its
+    sources) on the host cores, for the same workload, metric and unit as the GPU arm.  Imports nothing of
+    the kiwi_b200 package: the workload generator and the kernel's hfact are loaded as plain files."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    P, bounds, shape = make_workload(args.n, args.res, args.seed, args.kernel)
     from oracle.oracle import load_ref
 
     ref = load_ref()
     if ref is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkiwi_ref.so was not built"}))
         return 0
+    P, bounds, shape = make_workload(args.n, args.res, args.seed, args.kernel)
     threads = ref.max_threads()
-    n = len(P["x"])
-    perm = np.random.default_rng(99).permutation(n)
-    Ps = {k: np.ascontiguousarray(v[perm]) for k, v in P.items()}
-    t, _, _, _ = ref.pair_sample(Ps, bounds, shape, kernel=args.kernel, threads=threads, p_range=(0, 16 * threads))
-    per_step = int(max(threads * 4, 16 * threads / max(t, 1e-3) * 8.0))  # ~8 s of CPU work per step
-    pos = 16 * threads
-    for _ in range(args.warmup):
-        ref.pair_sample(Ps, bounds, shape, kernel=args.kernel, threads=threads, p_range=(pos, pos + per_step // 4))
-        pos += per_step // 4
-    tt, bb, ss = 0.0, 0, 0
-    for _ in range(args.steps):
-        t, b, s, _ = ref.pair_sample(Ps, bounds, shape, kernel=args.kernel, threads=threads,
-                                     p_range=(pos % n, min(n, pos % n + per_step)))
-        pos += per_step
-        tt += t
-        bb += b
-        ss += s
+    tt, bb, ss, per_step = ref_sample(P, bounds, shape, args.kernel, ref, threads, args.steps, args.warmup)
     value = ss / tt
+    sample = (f"{per_step} of {args.n} particles per step (consecutive ranges of a seeded permutation, "
+              f"{REF_CHUNKS_PER_THREAD} chunks of 256 per thread); {bb} bounding-box / {ss} support pairs over "
+              f"{args.steps} steps; the reference's KernelIntegrator::face over each cell's six box faces in its "
+              f"OpenMP schedule(dynamic, 256) particle loop, per-cell sums into a scalar instead of the grid")
     line = {"metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "impl": "reference", "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"lognormal_cube n={args.n} grid={args.res}^3 kernel={args.kernel}",
-                       "sample_particles_per_step": per_step},
+            "config": workload_config(args),
             "cpu_baseline": {"value": value, "unit": "pair-integrals/s", "cores": threads, "kind": "reference",
-                             "sample": f"{per_step} particles per step of {n}; {bb} bbox / {ss} support pairs"},
+                             "sample": sample},
+            "pairs": {"bbox_pairs_per_s": bb / tt, "sample_particles_per_step": per_step},
             "e2e": {"value": value, "unit": "pair-integrals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -811,7 +849,7 @@ def main():
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.tabulated:
-        cpu = cpu_baseline(P, bounds, shape, args.kernel, args.cpu_seconds)
+        cpu = cpu_baseline(P, bounds, shape, args.kernel)
 
     if rank == 0:
         g_ms = float(np.mean(gather_ms))
@@ -833,12 +871,15 @@ def main():
             work = evaluated_per_launch * work_per_pair
         achieved = work / (g_ms * 1e-3) / 1e12
         peak = kiwi_b200.measure_fp32_peak(ctx) if is32 else peak_fp64
-        # DRAM traffic of the kernel per launch, from the ncu capture of this exact workload
-        # (profiles/k_cart_lattice_fp64_lognormal.md); None for other workloads
-        traffic = None
+        # DRAM traffic of the kernel per launch: an ncu capture of this exact workload (one pass,
+        # dram__bytes_read.sum + dram__bytes_write.sum), stated with the commit it was captured at; the
+        # bench cannot count DRAM bytes itself, so other workloads report None
+        traffic, traffic_src = None, None
         if (not is32 and args.n == 2_000_000 and args.res == 256 and args.kernel == "cubic_spline" and
-                not args.full_box and args.precision == "fp64" and ws == 1):
-            traffic = LATTICE_DRAM_BYTES_FULL
+                not args.full_box and args.precision == "fp64" and ws == 1 and not args.tabulated):
+            traffic = LATTICE_TRAFFIC["bytes"]
+            traffic_src = (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one {LATTICE_TRAFFIC['kernel']} "
+                           f"launch of this workload, captured at commit {LATTICE_TRAFFIC['commit']}")
         hbm_peak, hbm_src = hbm_peak_gbs()
         tab_roofline = None
         if args.tabulated:
@@ -857,13 +898,7 @@ def main():
             "ms_per_step": job_ms / args.steps, "higher_is_better": True, "scaling": "strong" if split else "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": f"lognormal_cube n={args.n} sigma_ln=1.5 P(k)~k^-4 10pc padded, "
-                                   f"grid {args.res}^3, kernel {args.kernel}" +
-                                   (", tabulated integral" if args.tabulated else ""),
-                       "precision": args.precision, "particles_per_gpu": args.n, "cells": nc,
-                       "l2": "flushed between timed steps (256 MB write) and inputs+outputs > L2",
-                       "parallelism": (f"cell-tile parts x{ws} of one grid" if split else f"replicas x{ws}")
-                       if ws > 1 else "single GPU"},
+            "config": workload_config(args, nc, ws, split),
             "pairs": {"support_pairs_per_step": job_pairs / args.steps / ws,
                       "bbox_pairs_per_step": job_bbox / args.steps / ws,
                       "bbox_pairs_per_s": job_bbox / (job_ms * 1e-3)},
@@ -871,6 +906,7 @@ def main():
                          {k: v / args.steps for k, v in items.items()},
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "traffic_source": traffic_src,
                          "hbm": ({"achieved_gbs": traffic / (g_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
                                   "frac": traffic / (g_ms * 1e-3) / 1e9 / hbm_peak, "peak_source": hbm_src}
                                  if traffic and hbm_peak else None),
