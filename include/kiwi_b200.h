@@ -134,6 +134,21 @@ int kiwi_kernel_info(int kernel, double* out7);
 int kiwi_full_integral_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi,
                              const double* r0, const double* R_0, double* out);
 
+/* The tier constants of n (r0, R_0) pairs, as the reference's structs hold them (host arrays).  kernel < 0:
+ * the cubic spline with arg0 = h -- compute_wall_constants (src/kernel_integral.cpp:222-247) into
+ * KIWI_CUBIC_WALL_DOUBLES per item {valid, r0, h, h2, r03, r0h2, r0h3, r0h_2, r0h_3, B1, B2, B3} and
+ * compute_edge_constants (:253-350) into KIWI_CUBIC_EDGE_DOUBLES {valid, R_0, a, a2, D2, D3}
+ * (include/kiwi/kernel_integral.hpp:108-127).  kernel >= 0: arg0 = H -- generic_wall_constants
+ * (src/kernel_integral_generic.cpp:96-117) into KIWI_GENERIC_WALL_DOUBLES {valid, H, r0, q0, j,
+ * coef[4][15], bphi[4]} and generic_edge_constants (:119-148) into KIWI_GENERIC_EDGE_DOUBLES {valid, R_0, a,
+ * a2, nseg, region[4], phi_end[4], offset[4]} (include/kiwi/kernel_integral_generic.hpp:27-48). */
+#define KIWI_CUBIC_WALL_DOUBLES 12
+#define KIWI_CUBIC_EDGE_DOUBLES 6
+#define KIWI_GENERIC_WALL_DOUBLES 69
+#define KIWI_GENERIC_EDGE_DOUBLES 17
+int kiwi_tier_constants_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* r0,
+                              const double* R_0, double* wall_out, double* edge_out);
+
 /* compute_face_integral / compute_face_integral_generic (include/kiwi/kernel_integral.hpp:182-193) for
  * n_faces independent (particle, face) items.  particle: 4 doubles per item (x0, y0, z0, h); face i has
  * vertices vert_off[i]..vert_off[i+1]-1 of verts (xyz each, absolute, in the face's winding).  out_vert
@@ -156,6 +171,10 @@ int kiwi_density_table_generate(KiwiCtx* ctx);
  * Errors (KIWI_ERR_ARG) carry the reference's messages; shapes the reference would divide by zero on or
  * that exceed 2^31 values are rejected too. */
 int kiwi_density_table_load(KiwiCtx* ctx, const char* path);
+/* A caller's table (DensityLookupTable's header fields and its values, laid out as
+ * DensityLookupTable::at, include/kiwi/kernel_integral.hpp:27-40) copied into the context, replacing any table
+ * it holds; the shape is checked as the loader checks it. */
+int kiwi_density_table_set(KiwiCtx* ctx, const KiwiDensityTableInfo* info, const double* values);
 /* Shape of the context's table (KIWI_ERR_ARG if it holds none). */
 int kiwi_density_table_info(KiwiCtx* ctx, KiwiDensityTableInfo* info);
 /* Copy the table's n_values values to host memory, laid out as the reference's DensityLookupTable::at. */
@@ -218,7 +237,8 @@ int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles
  * entry plus 16 bytes per 8x8x8-cell tile) are rejected with KIWI_ERR_LIMIT and a message in err (if
  * err_len > 0).  Every call reuses the same array and leaves the last call's contents in it, so calls
  * whose GPU work overlaps -- on different streams or from different host threads -- race and must be
- * serialised by the caller.  Results equal kiwi_sph_to_grid_device's. */
+ * serialised by the caller.  A call that fails waits for the work it had queued on the stream before it
+ * returns, so nothing of it still writes the array afterwards.  Results equal kiwi_sph_to_grid_device's. */
 #define KIWI_NOALLOC_SCRATCH_BYTES (32u << 20)
 int kiwi_sph_to_grid_device_noalloc(void* stream, const KiwiParticles* particles, const KiwiCartGrid* grid,
                                     const KiwiKernelSel* kernel, int precision, double* density, double* vx,

@@ -26,6 +26,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 UNITS = [
     ("capi.cu", ["--fmad=false"]),
     ("kiwi_fp64.cu", ["--fmad=false"]),
+    ("lattice.cu", []),
     ("noalloc.cu", ["--fmad=false"]),
     ("voronoi.cu", ["--fmad=false"]),
     ("adjoint.cu", ["--fmad=false"]),
@@ -36,6 +37,8 @@ UNITS = [
     ("cartmap.cu", ["--fmad=false"]),
     ("pointset.cu", ["--fmad=false"]),
     ("lloyd.cu", ["--fmad=false"]),
+    # the C++ drop-in of the reference's kernel-integral layer (host code over the C ABI)
+    ("kernel_layer.cpp", ["-I" + os.path.join(HERE, "..", "include")]),
 ]
 
 
@@ -64,10 +67,12 @@ def build(verbose: bool = False, force: bool = False, defines: tuple = (), out: 
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
     headers.append(os.path.join(HERE, "..", "include", "kiwi_b200.h"))
+    inc_kiwi = os.path.join(HERE, "..", "include", "kiwi")
+    headers += [os.path.join(inc_kiwi, f) for f in os.listdir(inc_kiwi) if f.endswith(".hpp")]
     objs = []
     for src, extra in UNITS:
         s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
+        o = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
         objs.append(o)
         if force or _stale(o, [s, __file__] + headers):
             cmd = ([nvcc()] + ARCH + COMMON + extra + extra_defs + (["-Xptxas", "-v"] if verbose else []) +

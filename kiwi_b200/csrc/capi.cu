@@ -152,9 +152,9 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         uint32_t *w = nullptr, *flags = nullptr;
         int64_t* prefix = nullptr;
         int32_t* map = nullptr;
-        KIWI_TRY(scratch_t(ctx, S_MISC0, (size_t)ntiles, &w));
-        KIWI_TRY(scratch_t(ctx, S_MISC1, (size_t)ntiles + 1, &prefix));
-        KIWI_TRY(scratch_t(ctx, S_MISC2, (size_t)ntiles, &flags));
+        KIWI_TRY(scratch_t(ctx, S_PART_W, (size_t)ntiles, &w));
+        KIWI_TRY(scratch_t(ctx, S_PART_PREFIX, (size_t)ntiles + 1, &prefix));
+        KIWI_TRY(scratch_t(ctx, S_PART_FLAGS, (size_t)ntiles, &flags));
         KIWI_TRY(scratch_t(ctx, S_TILE_MAP, (size_t)ntiles, &map));
         const unsigned nb = (unsigned)((ntiles + 255) / 256);
         k_tile_entry_counts<<<nb, 256, 0, ctx->stream>>>(range, ntiles, w);
@@ -163,7 +163,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         k_tile_part_flags<<<nb, 256, 0, ctx->stream>>>(prefix, prefix + ntiles, ntiles, part, n_parts, flags);
         KIWI_LAUNCHED(ctx);
         int64_t* moffs = nullptr;
-        KIWI_TRY(scratch_t(ctx, S_OFFS, (size_t)ntiles + 1, &moffs));
+        KIWI_TRY(scratch_t(ctx, S_PART_OFFS, (size_t)ntiles + 1, &moffs));
         KIWI_TRY(exclusive_scan<uint32_t>(ctx, flags, ntiles, moffs, moffs + ntiles));
         k_compact_map<<<nb, 256, 0, ctx->stream>>>(flags, moffs, ntiles, map);
         KIWI_LAUNCHED(ctx);
@@ -200,7 +200,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
             int64_t* d_nmap = nullptr;
             DevStats* d_st2 = nullptr;
             KIWI_TRY(scratch_t(ctx, S_TILE_MAP, (size_t)ntiles, &map));
-            KIWI_TRY(scratch_t(ctx, S_MISC3, 1, &d_nmap));
+            KIWI_TRY(scratch_t(ctx, S_NMAP, 1, &d_nmap));
             KIWI_TRY(scratch_t(ctx, S_STATS2, 1, &d_st2));
             KIWI_TRY(mixed_flag_tiles(ctx, g, cerr, cmass, 1e-6, 1e-6, map, d_nmap));
             KIWI_CUDA(ctx, cudaMemcpyAsync(&fp64_tiles, d_nmap, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -371,6 +371,30 @@ int kiwi_full_integral_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* 
     KIWI_CUDA(ctx, cudaMemcpyAsync(d + 3 * n, R_0, b, cudaMemcpyHostToDevice, ctx->stream));
     KIWI_TRY(fp64_full_integral(ctx, kernel < 0 ? -1 : kernel, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n));
     KIWI_CUDA(ctx, cudaMemcpyAsync(out, d + 4 * n, b, cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return KIWI_OK;
+}
+
+int kiwi_tier_constants_batch(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* r0,
+                              const double* R_0, double* wall_out, double* edge_out) {
+    KIWI_TRY(check_ctx(ctx));
+    if (kernel >= KIWI_NUM_KERNELS) return set_err(ctx, KIWI_ERR_ARG, "unknown kernel index %d", kernel);
+    if (n < 0 || (n > 0 && (!arg0 || !r0 || !R_0 || !wall_out || !edge_out)))
+        return set_err(ctx, KIWI_ERR_ARG, "bad arrays");
+    if (n == 0) return KIWI_OK;
+    const int nw = kernel < 0 ? KIWI_CUBIC_WALL_DOUBLES : KIWI_GENERIC_WALL_DOUBLES;
+    const int ne = kernel < 0 ? KIWI_CUBIC_EDGE_DOUBLES : KIWI_GENERIC_EDGE_DOUBLES;
+    double* d = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_MISC0, (size_t)((3 + nw + ne) * n), &d));
+    const size_t b = sizeof(double) * n;
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d, arg0, b, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d + n, r0, b, cudaMemcpyHostToDevice, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(d + 2 * n, R_0, b, cudaMemcpyHostToDevice, ctx->stream));
+    double* dw = d + 3 * n;
+    double* de = dw + (size_t)nw * n;
+    KIWI_TRY(fp64_tier_constants(ctx, kernel < 0 ? -1 : kernel, n, d, d + n, d + 2 * n, dw, de));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(wall_out, dw, b * nw, cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(edge_out, de, b * ne, cudaMemcpyDeviceToHost, ctx->stream));
     KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return KIWI_OK;
 }

@@ -26,7 +26,7 @@ struct KiwiCtx {
     std::string err;
     int64_t launches = 0;  // kernels launched on this context (for the stats of a call)
     // Scratch slots: each is grown on demand and reused by later calls on this context.
-    static constexpr int kSlots = 40;
+    static constexpr int kSlots = 48;
     void* slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Fixed arena mode (used only by the allocation-free entry point): when `arena` is set, scratch
@@ -152,7 +152,15 @@ enum ScratchSlot {
     S_VOR_PVAL,      // inverse map: each visited pair's cell integral
     S_VOR_CMASS,     // inverse map: per-cell mass m_i
     S_INV_OUT,       // inverse map: given cell masses, recovered masses and coverage (host entry point)
+    S_PART_W,        // part split: per-tile entry counts
+    S_PART_PREFIX,   // part split: their prefix sums
+    S_PART_FLAGS,    // part split: tiles of this part
+    S_PART_OFFS,     // part split: compaction offsets
+    S_FLAG_PEAK,     // FP32-mixed guarantee: peak cell mass
+    S_FLAG_FLAGS,    // FP32-mixed guarantee: tiles to recompute
+    S_FLAG_OFFS,     // FP32-mixed guarantee: compaction offsets
+    S_NMAP,          // FP32-mixed guarantee: number of tiles to recompute
 };
-static_assert(S_INV_OUT < KiwiCtx::kSlots, "scratch slots");
+static_assert(S_NMAP < KiwiCtx::kSlots, "scratch slots");
 
 }  // namespace kiwi_b200

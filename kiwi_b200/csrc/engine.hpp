@@ -120,9 +120,22 @@ int fp64_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, con
                      bool reference_order);
 int fp64_full_integral(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* phi, const double* r0,
                        const double* R0, double* out);
+int fp64_tier_constants(KiwiCtx* ctx, int kernel, int64_t n, const double* arg0, const double* r0, const double* R0,
+                        double* wall, double* edge);
 int fp64_face_integral(KiwiCtx* ctx, const KernelChoice& k, int64_t n, const double* particle,
                        const int64_t* vert_off, const double* verts, double* out, int32_t* out_vert);
 int fp64_mean_velocity(KiwiCtx* ctx, const DevParticles& P, double* d_meanv);
 int fp64_measure_peak(KiwiCtx* ctx, double* tflops);
+
+// lattice.cu: the lattice-factorised gather of the plain FP64 form for the cubic spline (every cell of the
+// support boxes with full_box, else the cells the supports reach) and the generic kernels (the cells the
+// supports reach), and the batch's persistent launches of those two families.
+int lattice_init_tables(KiwiCtx* ctx);
+int lattice_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
+                        const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box);
+int lattice_batch_prepare(KiwiCtx* ctx);
+int lattice_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
+                         const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
+                         unsigned long long* d_next, int blocks);
 
 }  // namespace kiwi_b200

@@ -1,0 +1,423 @@
+// The tile body of the lattice-factorised gather (one CTA = one 8 x 8 x 8 cell tile), shared by the
+// single-grid kernels and the batch's persistent kernel.  A translation unit that includes this defines
+// `c_tables` (its __constant__ copy of the kernel tables) first.
+//
+// Per particle of the tile's list, the box of its support clipped to the tile (n0 x n1 x n2 cells) has
+// (n0 + 1)(n1 + 1)(n2 + 1) lattice points and 2 (n0' n1' + n0' n2' + n1' n2') edge lines (n' = n + 1):
+// every edge line of a plane, in the six orientation blocks xy, xz, yx, yz, zx, zy (block "ab": the wall
+// at distance |u_a| along axis a, the line at in-plane distance |u_b| along axis b).  The two edges of a
+// block pair (xy[i][j] and yx[j][i], ...) are the two orientations of one (|u_a|, |u_b|) pair and are
+// evaluated together (lattice_edge_pair).  A lattice point's octant value (the kernel mass of the box
+// spanned by the particle and the point, lattice_point) is sgn(ux) sgn(uy) sgn(uz) times the sum of its
+// three corner values; a cell's mass is the alternating sum of its eight corners' octant values, which is
+// the reference's sum over the cell's 6 faces x 4 edges x 2 vertex pyramids regrouped by corner
+// (src/cartesian_grid.cpp:246-259, src/kernel_integral.cpp:471-647).
+#pragma once
+
+#include <climits>
+
+#include "engine.hpp"
+#include "lattice.cuh"
+#include "tabulated.cuh"
+
+namespace kiwi_b200 {
+
+constexpr int kLatThreads = 256;
+constexpr int kLatCellsPerThread = kTileCells / kLatThreads;
+static_assert(kTileCells % kLatThreads == 0, "tile cells must split evenly over the threads");
+constexpr int kLatPtCap = 2304;   // lattice points per chunk (a full 8^3 particle box has 729)
+constexpr int kLatECap2 = 2048;   // cubic edge tiers per chunk (a full 8^3 particle box has 486)
+static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed point-list entries");
+static_assert(kLatECap2 <= 2048 && kLatGenECap <= 2048, "packed edge-pair entries (11-bit slots)");
+constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap2 + kLatPtCap);
+constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatPtCap);
+constexpr size_t kLatTabDynSmem = sizeof(double) * kLatPtCap;
+
+__device__ __forceinline__ void lat_add_stat(unsigned long long* dst, unsigned long long v) {
+    // warp-aggregate, then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// The chunk of a tile's particle list (ascending particle index) is walked in four phases separated by
+// barriers: (A) classify every edge pair, listing those within the support; (B0) list the lattice points
+// that some evaluated cell reads (the cheap ones -- beyond the support -- from the end of the list) and set
+// the octant value of the points on a particle plane to 0; (A2) the listed edge pairs; (B) the listed
+// points' octant values; (C) each thread adds, for the cells it owns, the chunk's particles in list order
+// -- every cell's sum runs over its particles in ascending index order with no atomics.
+// GENERIC: the table-driven tiers of kernel K (support radius support_in_h x h) instead of the cubic closed
+// form; edge tiers are lattice_generic_edge records.  TAB: the tabulated cubic integral (lookups in `tab`):
+// no edge tiers, and the points run in their natural order.  List order never affects the results.
+template <bool CULL, bool GENERIC = false, bool TAB = false>
+__device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
+                                             const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
+                                             int64_t t_range, int64_t t, const CartOutputs& out,
+                                             DevStats* __restrict__ st, const KiwiKernelTable* K = nullptr,
+                                             const TabDev tab = TabDev{}) {
+    __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
+        s_vy[kLatPMax], s_vz[kLatPMax], s_ih[kLatPMax];
+    __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_poff[kLatPMax];
+    __shared__ uint32_t s_mag[kLatPMax][4];  // div_magic of n0', n1', n2' and n1' n2'
+    __shared__ TabWidths s_tw;               // TAB: the table's bin widths and their reciprocals
+    if (TAB && threadIdx.x == 0) s_tw = tab_widths(tab);  // read after the chunk load's barrier
+    __shared__ int s_np, s_etot, s_ptot, s_nexp, s_ncheap, s_nheavy;
+    __shared__ uint32_t s_plist[TAB ? 1 : kLatPtCap];
+    __shared__ uint32_t s_hlist[(GENERIC || TAB) ? 1 : kLatECap2 / 2];
+    extern __shared__ double s_dyn[];
+    constexpr int kECap = GENERIC ? kLatGenECap : (TAB ? 0 : kLatECap2);
+    double* s_D2 = s_dyn;
+    double* s_D3 = s_dyn + kLatECap2;
+    double* s_E = s_dyn;  // generic edge records
+    double* s_T = s_dyn + (GENERIC ? kLatGenERec * kLatGenECap : (TAB ? 0 : 2 * kLatECap2));
+
+    const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
+    const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the tile's lattice planes (every particle box is clipped to the tile, so its planes are these) and
+    // cell centres, formed as the reference forms them; read after the first barrier
+    __shared__ double s_pl[3][kTileX + 1], s_cc[3][kTileX];
+    static_assert(kTileX == kTileY && kTileX == kTileZ, "cubic tiles");
+    if (threadIdx.x < 3 * (kTileX + 1)) {
+        const int a = threadIdx.x / (kTileX + 1), l = threadIdx.x % (kTileX + 1);
+        const double mn = a == 0 ? g.x_min : (a == 1 ? g.y_min : g.z_min), d = a == 0 ? g.dpx : (a == 1 ? g.dpy : g.dpz);
+        const int b0 = a == 0 ? bx : (a == 1 ? by : bz);
+        s_pl[a][l] = add_rn(mn, mul_rn((double)(b0 + l), d));
+        if (l < kTileX) s_cc[a][l] = cell_centre(mn, b0 + l, d);
+    }
+
+    double acc[kLatCellsPerThread][4];
+#pragma unroll
+    for (int c = 0; c < kLatCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
+    // work counters: 32-bit per thread (a chunk adds at most a few hundred to any of them), flushed to the
+    // 64-bit totals every 2^16 chunks and at the end
+    unsigned n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
+    unsigned n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0, n_clamp = 0, n_chunks = 0;
+    auto flush = [&]() {
+        lat_add_stat(&st->bbox_pairs, n_bbox);
+        lat_add_stat(&st->sphere_pairs, n_sphere);
+        lat_add_stat(&st->evaluated_pairs, n_eval);
+        lat_add_stat(&st->neg_clamped, n_neg);
+        lat_add_stat(&st->neg_warned, n_warn);
+        lat_add_stat(&st->edge_outer, n_eo);
+        lat_add_stat(&st->edge_middle, n_em);
+        lat_add_stat(&st->edge_inner, n_ei);
+        lat_add_stat(&st->vertex_pyramids, n_vp);
+        if (TAB) lat_add_stat(&st->table_clamps, n_clamp);
+        n_bbox = n_sphere = n_eval = n_neg = n_warn = n_eo = n_em = n_ei = n_vp = n_clamp = 0;
+    };
+    const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
+    const double sup_in_h = g.support_in_h;
+
+    for (int64_t pos = beg; pos < end;) {
+        if (warp == 0) {
+            const int64_t idx = pos + lane;
+            int ne = 0, npt = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+            double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
+            if (idx < end) {
+                const uint32_t p = list[idx];
+                px = P.x[p]; py = P.y[p]; pz = P.z[p]; ph = P.h[p];
+                pm = P.m[p]; pvx = P.vx[p]; pvy = P.vy[p]; pvz = P.vz[p];
+                CellBox b;
+                bool outside;
+                particle_cell_box(g, px, py, pz, ph, b, &outside);
+                lo0 = max(b.x0, bx); lo1 = max(b.y0, by); lo2 = max(b.z0, bz);
+                d0 = min(b.x1, bx + kTileX - 1) - lo0 + 1;
+                d1 = min(b.y1, by + kTileY - 1) - lo1 + 1;
+                d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
+                const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
+                ne = TAB ? 0 : 2 * (n0 * n1 + n0 * n2 + n1 * n2);
+                npt = n0 * n1 * n2;
+            }
+            int ie = ne, ip = npt;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vp = __shfl_up_sync(0xffffffffu, ip, o);
+                if (lane >= o) {
+                    ie += ve;
+                    ip += vp;
+                }
+            }
+            const bool take = (idx < end) && ie <= kECap && ip <= kLatPtCap;
+            const int np = __popc(__ballot_sync(0xffffffffu, take));
+            if (take) {
+                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph; s_ih[lane] = 1.0 / ph;
+                s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
+                s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
+                s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
+                s_eoff[lane] = ie - ne;
+                s_poff[lane] = ip - npt;
+                s_mag[lane][0] = div_magic(d0 + 1);
+                s_mag[lane][1] = div_magic(d1 + 1);
+                s_mag[lane][2] = div_magic(d2 + 1);
+                s_mag[lane][3] = div_magic((d1 + 1) * (d2 + 1));
+            }
+            if (lane == np - 1) {
+                s_np = np;
+                s_etot = ie;
+                s_ptot = ip;
+                s_nexp = s_ncheap = s_nheavy = 0;
+            }
+        }
+        __syncthreads();
+        const int np = s_np, etot = s_etot, ptot = s_ptot;
+
+        // (A) edge pairs: pair block 0 = (x, y) over n0' x n1', 1 = (x, z) over n0' x n2', 2 = (y, z) over
+        // n1' x n2'; pair (p, q) of block (a, b) is edge ab[p][q] and edge ba[q][p].  Cubic: pairs beyond 2h
+        // (and zero ones) get D2 = D3 = 0 here; the others are listed (slot ab | slot ba << 11 | particle <<
+        // 22) with |u_a|, |u_b| parked in slot ab, and evaluated in (A2).  Generic: both records here.
+        if (!TAB) {
+            const int qtot = etot >> 1;
+            const int qoff_l = lane < np ? (s_eoff[lane] >> 1) : INT_MAX;
+            for (int base = warp * 32; base < qtot; base += kLatThreads) {
+                const int it = base + lane;
+                bool heavy = false;
+                uint32_t hrec = 0;
+                const int j = warp_owner(base, qoff_l, lane);
+                const int qoff = __shfl_sync(0xffffffffu, qoff_l, j & 31);
+                if (it < qtot) {
+                    int e = it - qoff;
+                    const int n0 = s_dim[j][0] + 1, n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
+                    const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
+                    const int blk = (e >= nxy) + (e >= nxy + nxz);
+                    e -= blk == 0 ? 0 : (blk == 1 ? nxy : nxy + nxz);
+                    const int a = blk == 2 ? 1 : 0, b = blk == 0 ? 1 : 2;
+                    const int nb = b == 1 ? n1 : n2, na = a == 0 ? n0 : n1;
+                    const int pi = div_by(e, s_mag[j][b]), qi = e - pi * nb;
+                    const int eb = s_eoff[j];
+                    const int sab = eb + (blk == 0 ? 0 : (blk == 1 ? nxy : 2 * nxy + nxz)) + pi * nb + qi;
+                    const int sba = eb + (blk == 0 ? nxy + nxz : (blk == 1 ? 2 * nxy + nxz + nyz : 2 * nxy + 2 * nxz + nyz)) +
+                                    qi * na + pi;
+                    const int la = s_lo[j][a] - (a == 0 ? bx : by), lb = s_lo[j][b] - (b == 1 ? by : bz);
+                    const double pa = a == 0 ? s_x[j] : s_y[j], pb = b == 1 ? s_y[j] : s_z[j];
+                    const double vp = fabs(s_pl[a][la + pi] - pa), vq = fabs(s_pl[b][lb + qi] - pb);
+                    if (GENERIC) {
+                        const double H = mul_rn(sup_in_h, s_h[j]);
+                        lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
+                        lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+                        n_ei += 2;
+                    } else {
+                        const double h2 = s_h[j] * s_h[j];
+                        const double ld2 = add_rn(mul_rn(vp, vp), mul_rn(vq, vq));
+                        heavy = vp != 0.0 && vq != 0.0 && ld2 <= 4.0 * h2;
+                        if (heavy) {
+                            if (ld2 > h2) n_em += 2;
+                            else n_ei += 2;
+                            s_D2[sab] = vp;
+                            s_D3[sab] = vq;
+                            hrec = (uint32_t)sab | (uint32_t)sba << 11 | (uint32_t)j << 22;
+                        } else {
+                            n_eo += 2;
+                            s_D2[sab] = s_D3[sab] = 0.0;
+                            s_D2[sba] = s_D3[sba] = 0.0;
+                        }
+                    }
+                }
+                if (!GENERIC) {
+                    const unsigned m = __ballot_sync(0xffffffffu, heavy);
+                    int hp = 0;
+                    if (lane == 0 && m) hp = atomicAdd(&s_nheavy, __popc(m));
+                    hp = __shfl_sync(0xffffffffu, hp, 0);
+                    if (heavy) s_hlist[hp + __popc(m & ((1u << lane) - 1))] = hrec;
+                }
+            }
+        }
+
+        // (B0) the lattice points some evaluated cell reads: with CULL, a point none of whose eight cells
+        // meets the support sphere is left out (the test bounds the distance to the 2 x 2 x 2 cells around
+        // the point, their half-widths padded by 1e-6 of a cell so that rounding never drops a point an
+        // evaluated cell reads).  A point on a particle plane (an offset of 0) has octant value 0, written
+        // here; the others are listed, those within the support from the front of s_plist, those beyond it
+        // from the end, so that each kind runs in warps of its own.  An entry packs (particle, i, j, k):
+        // 5 + 3 x 4 bits.
+        if (!TAB) {
+            const int poff_l = lane < np ? s_poff[lane] : INT_MAX;
+            for (int base = warp * 32; base < ptot; base += kLatThreads) {
+                const int pt = base + lane;
+                int cls = -1;  // -1 none, 0 within the support, 1 beyond
+                uint32_t rec = 0;
+                const int jp = warp_owner(base, poff_l, lane);
+                const int poff = __shfl_sync(0xffffffffu, poff_l, jp & 31);
+                if (pt < ptot) {
+                    const int lp = pt - poff;
+                    const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
+                    const int i = div_by(lp, s_mag[jp][3]), rem = lp - i * n12;
+                    const int jj = div_by(rem, s_mag[jp][2]), k = rem - jj * n2;
+                    const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
+                    const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
+                    const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
+                    const double h = s_h[jp];
+                    bool keep = true;
+                    if (CULL) {
+                        const double radius = mul_rn(sup_in_h, h);
+                        const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
+                        const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
+                        const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
+                        keep = ex * ex + ey * ey + ez * ez < radius * radius;
+                    }
+                    if (keep) {
+                        if (ux == 0.0 || uy == 0.0 || uz == 0.0) {
+                            s_T[pt] = 0.0;
+                        } else {
+                            const double H = GENERIC ? mul_rn(sup_in_h, h) : 2.0 * h;
+                            cls = (ux * ux + uy * uy + uz * uz < H * H) ? 0 : 1;
+                            rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
+                        }
+                    }
+                }
+                const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
+                int pe = 0, pcb = 0;
+                if (lane == 0) {
+                    if (me) pe = atomicAdd(&s_nexp, __popc(me));
+                    if (mc) pcb = atomicAdd(&s_ncheap, __popc(mc));
+                }
+                pe = __shfl_sync(0xffffffffu, pe, 0);
+                pcb = __shfl_sync(0xffffffffu, pcb, 0);
+                const unsigned below = (1u << lane) - 1;
+                if (cls >= 0) s_plist[cls == 0 ? pe + __popc(me & below) : kLatPtCap - 1 - pcb - __popc(mc & below)] = rec;
+            }
+        }
+        __syncthreads();
+
+        // (A2) the listed edge pairs (cubic)
+        if (!GENERIC && !TAB) {
+            const int nheavy = s_nheavy;
+            for (int li = threadIdx.x; li < nheavy; li += kLatThreads) {
+                const uint32_t rec = s_hlist[li];
+                const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)(rec >> 22);
+                LatticeEdge e_pq, e_qp;
+                lattice_edge_pair(s_h[j], s_ih[j], s_D2[sab], s_D3[sab], e_pq, e_qp);
+                s_D2[sab] = e_pq.D2;
+                s_D3[sab] = e_pq.D3;
+                s_D2[sba] = e_qp.D2;
+                s_D3[sba] = e_qp.D3;
+            }
+            __syncthreads();
+        }
+        const int nexp = s_nexp, ncheap = s_ncheap;
+        const int nplist = TAB ? ptot : nexp + ncheap;
+
+        // (B) octant values of the listed points
+        for (int li = threadIdx.x; li < nplist; li += kLatThreads) {
+            int jp, i, jj, k, it;
+            if (TAB) {
+                it = li;
+                jp = chunk_search(s_poff, np, it);
+                const int lp = it - s_poff[jp];
+                const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
+                i = div_by(lp, s_mag[jp][3]);
+                const int rem = lp - i * n12;
+                jj = div_by(rem, s_mag[jp][2]);
+                k = rem - jj * n2;
+            } else {
+                const uint32_t rec = s_plist[li < nexp ? li : kLatPtCap - ncheap + (li - nexp)];
+                jp = (int)(rec & 31u);
+                i = (int)((rec >> 5) & 15u);
+                jj = (int)((rec >> 9) & 15u);
+                k = (int)((rec >> 13) & 15u);
+                it = s_poff[jp] + (i * (s_dim[jp][1] + 1) + jj) * (s_dim[jp][2] + 1) + k;
+            }
+            const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
+            const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
+            const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
+            const double sg = sgn(ux) * sgn(uy) * sgn(uz);
+            double f = 0.0;
+            if (sg != 0.0) {
+                const double ax = fabs(ux), ay = fabs(uy), az = fabs(uz);
+                if (TAB) {
+                    // two right-triangle vertex pyramids per wall; cos(phi) from the legs
+                    const double ih = s_ih[jp];
+                    f = tab_pair(tab, s_tw, ih, ax, ay, az, n_clamp) + tab_pair(tab, s_tw, ih, ay, ax, az, n_clamp) +
+                        tab_pair(tab, s_tw, ih, az, ax, ay, n_clamp);
+                } else {
+                    const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                    const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
+                    const int eb = s_eoff[jp];
+                    const int exy = eb + i * n1 + jj, exz = eb + nxy + i * n2 + k;
+                    const int eyx = eb + nxy + nxz + jj * n0 + i, eyz = eb + 2 * nxy + nxz + jj * n2 + k;
+                    const int ezx = eb + 2 * nxy + nxz + nyz + k * n0 + i, ezy = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
+                    if (GENERIC) {
+                        const double H = mul_rn(sup_in_h, s_h[jp]);
+                        f = lattice_generic_corner(K, H, ax, ay, az, s_E + kLatGenERec * exy, s_E + kLatGenERec * exz) +
+                            lattice_generic_corner(K, H, ay, ax, az, s_E + kLatGenERec * eyx, s_E + kLatGenERec * eyz) +
+                            lattice_generic_corner(K, H, az, ax, ay, s_E + kLatGenERec * ezx, s_E + kLatGenERec * ezy);
+                    } else {
+                        const PointEdges<double> E{s_D2[exy], s_D3[exy], s_D2[exz], s_D3[exz], s_D2[eyx], s_D3[eyx],
+                                                   s_D2[eyz], s_D3[eyz], s_D2[ezx], s_D3[ezx], s_D2[ezy], s_D3[ezy]};
+                        f = lattice_point(s_h[jp], s_ih[jp], ax, ay, az, E);
+                    }
+                }
+                n_vp += 6;
+            }
+            s_T[it] = sg * f;
+        }
+        __syncthreads();
+
+        // (C) cells: the alternating sum of the 8 corners' octant values, in particle order
+#pragma unroll
+        for (int c = 0; c < kLatCellsPerThread; ++c) {
+            const int li = threadIdx.x + c * kLatThreads;
+            const int lx = li / (kTileZ * kTileY), ly = (li / kTileZ) % kTileY, lz = li % kTileZ;
+            const int gx = bx + lx, gy = by + ly, gz = bz + lz;
+            for (int j = 0; j < np; ++j) {
+                const int i = gx - s_lo[j][0], jj = gy - s_lo[j][1], k = gz - s_lo[j][2];
+                if (i < 0 || jj < 0 || k < 0 || i >= s_dim[j][0] || jj >= s_dim[j][1] || k >= s_dim[j][2]) continue;
+                ++n_bbox;
+                const double radius = mul_rn(sup_in_h, s_h[j]);
+                const double ex = fmax(fabs(s_x[j] - s_cc[0][lx]) - g.hpx, 0.0);
+                const double ey = fmax(fabs(s_y[j] - s_cc[1][ly]) - g.hpy, 0.0);
+                const double ez = fmax(fabs(s_z[j] - s_cc[2][lz]) - g.hpz, 0.0);
+                // the support test of the pair counters, rounded as the host restatement rounds it
+                const bool in = add_rn(add_rn(mul_rn(ex, ex), mul_rn(ey, ey)), mul_rn(ez, ez)) < mul_rn(radius, radius);
+                n_sphere += in;
+                if (CULL && !in) continue;
+                ++n_eval;
+                const int n2 = s_dim[j][2] + 1, n12 = (s_dim[j][1] + 1) * n2;
+                const double* Tp = s_T + s_poff[j] + (i * (s_dim[j][1] + 1) + jj) * n2 + k;
+                const double m1 = (Tp[n12 + n2 + 1] - Tp[n12 + n2]) - (Tp[n12 + 1] - Tp[n12]);
+                const double m0 = (Tp[n2 + 1] - Tp[n2]) - (Tp[1] - Tp[0]);
+                double msum = m1 - m0;
+                if (msum < 0.0) {
+                    ++n_neg;
+                    if (msum <= -0.01) ++n_warn;
+                    msum = 0.0;
+                }
+                if (msum == 0.0) continue;
+                const double mm = msum * s_m[j];
+                acc[c][0] += mm;
+                acc[c][1] += mm * s_vx[j];
+                acc[c][2] += mm * s_vy[j];
+                acc[c][3] += mm * s_vz[j];
+            }
+        }
+        __syncthreads();
+        pos += np;
+        if (++n_chunks == (1u << 16)) {
+            flush();
+            n_chunks = 0;
+        }
+    }
+
+    const double mvx = out.meanv[0], mvy = out.meanv[1], mvz = out.meanv[2];
+    const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+#pragma unroll
+    for (int c = 0; c < kLatCellsPerThread; ++c) {
+        const int li = threadIdx.x + c * kLatThreads;
+        const int ix = bx + li / (kTileZ * kTileY), iy = by + (li / kTileZ) % kTileY, iz = bz + li % kTileZ;
+        if (ix >= g.nx || iy >= g.ny || iz >= g.nz) continue;
+        const int64_t i3 = ((int64_t)ix * g.ny + iy) * g.nz + iz;
+        const double M = acc[c][0];
+        if (out.density) out.density[i3] = M / g.cell_volume;
+        const bool has = M > 0.0;
+        if (out.vx) out.vx[i3] = has ? acc[c][1] / M : mvx;
+        if (out.vy) out.vy[i3] = has ? acc[c][2] / M : mvy;
+        if (out.vz) out.vz[i3] = has ? acc[c][3] / M : mvz;
+        if (out.raw4) {
+            out.raw4[i3] = M;
+            out.raw4[ncell + i3] = acc[c][1];
+            out.raw4[2 * ncell + i3] = acc[c][2];
+            out.raw4[3 * ncell + i3] = acc[c][3];
+        }
+    }
+    flush();
+}
+
+}  // namespace kiwi_b200

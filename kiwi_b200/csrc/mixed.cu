@@ -443,9 +443,9 @@ int mixed_flag_tiles(KiwiCtx* ctx, const CartGeom& g, const double* cell_err, co
     unsigned long long* peak = nullptr;
     uint32_t* flags = nullptr;
     int64_t* offs = nullptr;
-    KIWI_TRY(scratch_t(ctx, S_MISC1, 1, &peak));
-    KIWI_TRY(scratch_t(ctx, S_MISC2, (size_t)ntiles, &flags));
-    KIWI_TRY(scratch_t(ctx, S_OFFS, (size_t)ntiles + 1, &offs));
+    KIWI_TRY(scratch_t(ctx, S_FLAG_PEAK, 1, &peak));
+    KIWI_TRY(scratch_t(ctx, S_FLAG_FLAGS, (size_t)ntiles, &flags));
+    KIWI_TRY(scratch_t(ctx, S_FLAG_OFFS, (size_t)ntiles + 1, &offs));
     KIWI_CUDA(ctx, cudaMemsetAsync(peak, 0, sizeof(unsigned long long), ctx->stream));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);

@@ -12,6 +12,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/kiwi_b200.h"
 #include "engine.hpp"
@@ -27,6 +28,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 
 struct DeviceState {
+    std::mutex setup_mutex;  // first calls from several host threads set the device up once
     bool ready = false;
     KiwiCtx ctx;  // stream set per call; scratch slots carved from the device's scratch area
 };
@@ -41,8 +43,10 @@ void put_err(char* err, size_t err_len, const char* msg) {
 
 // Set-up for the current device, once: the device address of the scratch area, the kernel tables in
 // constant memory and two timing events.  Must run before any stream capture on that device.
+// A set-up that failed leaves nothing behind that a later attempt would duplicate.
 int setup(int dev, char* err, size_t err_len) {
     DeviceState& s = g_state[dev];
+    std::lock_guard<std::mutex> lock(s.setup_mutex);
     if (s.ready) return KIWI_OK;
     void* ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
@@ -58,7 +62,8 @@ int setup(int dev, char* err, size_t err_len) {
     s.ctx.arena = static_cast<unsigned char*>(ptr);
     s.ctx.arena_bytes = kScratchBytes;
     for (int i = 0; i < 2; ++i) {
-        if (cudaEventCreate(&s.ctx.ev[i]) != cudaSuccess) {
+        if (s.ctx.ev[i] == nullptr && cudaEventCreate(&s.ctx.ev[i]) != cudaSuccess) {
+            s.ctx.ev[i] = nullptr;
             put_err(err, err_len, "cudaEventCreate failed during set-up");
             cudaGetLastError();
             return KIWI_ERR_CUDA;
@@ -108,7 +113,13 @@ extern "C" int kiwi_sph_to_grid_device_noalloc(void* stream, const KiwiParticles
         CartOutputs out{density, vx, vy, vz, raw4, nullptr};
         rc = sph_to_grid_dev(ctx, P, g, kc, precision, out, stats);
     }
-    if (rc != KIWI_OK) put_err(err, err_len, ctx->err.c_str());
+    if (rc != KIWI_OK) {
+        put_err(err, err_len, ctx->err.c_str());
+        // a failed call may have queued kernels that still write the shared array: let them finish, so
+        // that the caller may reuse its buffers or call again on another stream at once
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();
+    }
     ctx->stream = nullptr;
     return rc;
 }

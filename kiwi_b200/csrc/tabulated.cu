@@ -209,6 +209,25 @@ int kiwi_density_table_load(KiwiCtx* ctx, const char* path) {
     return table_load(ctx, path);
 }
 
+int kiwi_density_table_set(KiwiCtx* ctx, const KiwiDensityTableInfo* info, const double* values) {
+    if (!ctx || !info || !values) return KIWI_ERR_ARG;
+    KIWI_CUDA(ctx, cudaSetDevice(ctx->device));
+    TabDev t;
+    t.nr01 = info->nr01; t.nR_01 = info->nR_01; t.nphi1 = info->nphi1;
+    t.nr02 = info->nr02; t.nR_02 = info->nR_02; t.nphi2 = info->nphi2;
+    t.rl = info->rl; t.mul = info->mul; t.cphil = info->cphil;
+    KIWI_TRY(table_shape(ctx, t));
+    if (info->n_values != table_values(t))
+        return set_err(ctx, KIWI_ERR_ARG, "n_values %lld does not match the table's shape (%lld)",
+                       (long long)info->n_values, (long long)table_values(t));
+    table_release(ctx);
+    KIWI_TRY(table_alloc(ctx, t));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(const_cast<double*>(ctx->tab.v), values, ctx->tab_bytes, cudaMemcpyHostToDevice,
+                                   ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return KIWI_OK;
+}
+
 int kiwi_density_table_info(KiwiCtx* ctx, KiwiDensityTableInfo* info) {
     if (!ctx || !info) return KIWI_ERR_ARG;
     if (!ctx->tab.v) return set_err(ctx, KIWI_ERR_ARG, "the context holds no density lookup table");

@@ -387,6 +387,20 @@ class RefLib:
     def max_threads(self):
         return self.lib.ref_max_threads()
 
+    def load_snapshot(self, path, hfact=1.2):
+        """The reference's own snapshot reader (load_sph_snapshot, format detected): dict of x y z vx vy vz m h."""
+        self.lib.ref_load_snapshot.restype = C.c_long
+        self.lib.ref_load_snapshot.argtypes = [C.c_char_p, C.c_double, C.c_void_p]
+        n = self.lib.ref_load_snapshot(path.encode(), hfact, None)
+        if n < 0:
+            raise RuntimeError("reference snapshot reader failed: " + self.lib.ref_last_error().decode())
+        keys = ("x", "y", "z", "vx", "vy", "vz", "m", "h")
+        cols = [np.zeros(n) for _ in keys]
+        ptrs = (C.POINTER(C.c_double) * 8)(*[_d(c) for c in cols])
+        if self.lib.ref_load_snapshot(path.encode(), hfact, C.cast(ptrs, C.c_void_p)) != n:
+            raise RuntimeError("reference snapshot reader failed: " + self.lib.ref_last_error().decode())
+        return dict(zip(keys, cols))
+
     def pair_sample(self, P, bounds, shape, kernel="cubic_spline", support_in_h=0.0, generic_path=False, threads=0,
                     p_range=None):
         """The reference's pair-integral loop over a particle range, OpenMP: (seconds, bbox pairs, sphere

@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "kiwi/cartesian_grid.hpp"
+#include "kiwi/snapshot.hpp"
 #include "kiwi/config.hpp"
 #include "kiwi/kernel_integral.hpp"
 #include "kiwi/kernel_integral_generic.hpp"
@@ -232,6 +233,24 @@ double ref_pair_sample(long n, const double* x, const double* y, const double* z
 }
 
 int ref_max_threads() { return omp_get_max_threads(); }
+
+// load_sph_snapshot (src/snapshot.cpp:511) on a snapshot file, format detected as the reference detects it.
+// With out == nullptr returns the particle count; else fills out[8][n] (x y z vx vy vz m h) and returns n.
+// Returns -1 on error (ref_last_error()).
+long ref_load_snapshot(const char* path, double hfact, double* const* out) {
+    try {
+        kiwi::SPHSnapshot s = kiwi::load_sph_snapshot(path, "auto", hfact);
+        const long n = static_cast<long>(s.size());
+        if (out) {
+            const std::vector<double>* cols[8] = {&s.x, &s.y, &s.z, &s.vx, &s.vy, &s.vz, &s.m, &s.h};
+            for (int k = 0; k < 8; ++k) std::memcpy(out[k], cols[k]->data(), n * sizeof(double));
+        }
+        return n;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
 
 // ---- Voronoi --------------------------------------------------------------------------------------
 

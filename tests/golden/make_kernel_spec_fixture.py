@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Extract the reference's kernel coefficient tables into ``kernel_spec_ref.json`` (a test fixture).
 
-Reads ``src/kernel_spec_data.cpp`` of a KIWI checkout (default: /root/reference) as text and collects
+Reads ``src/kernel_spec_data.cpp`` of a KIWI checkout (first argument, or KIWI_REF) as text and collects
 the numbers of each KernelSpec initializer in declaration order: key, name, nreg, c[4], A2_pi, A3_pi,
 radkern, hfact, a[4][15], B[4][4][16].  Run once where the reference is present; the JSON it writes
 is committed so that the tests never need the reference itself.
@@ -11,7 +11,9 @@ import os
 import re
 import sys
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KIWI_REF")
+if not ROOT:
+    sys.exit("usage: make_kernel_spec_fixture.py <KIWI checkout>  (or set KIWI_REF)")
 src = open(os.path.join(ROOT, "src", "kernel_spec_data.cpp")).read()
 body = src[src.index("kKernels[] = {"):src.index("} // namespace")]
 body = re.sub(r"//[^\n]*", "", body)

@@ -6,6 +6,7 @@
 
 #include "../kiwi_b200/csrc/kiwi_math.cuh"
 #include "../kiwi_b200/csrc/dual.cuh"
+#include "../kiwi_b200/csrc/lattice_math.cuh"
 
 using namespace kiwi_b200;
 
@@ -49,5 +50,32 @@ void hm_cell_grad(double x0, double y0, double z0, double h, double cx, double c
     const Dual4 m = box_cell_msum<Dual4>(X, Y, Z, 2 * evd.h, cx, cy, cz, hx, hy, hz, evd);
     out[1] = m.v;
     for (int k = 0; k < 4; ++k) out[2 + k] = m.d[k];
+}
+
+// The lattice kernels' tiers: one edge tier, both orientations of an edge pair, one wall's corner value,
+// and a lattice point's three corner values together.
+void hm_lattice_edge(double h, double r0, double R0, double* out2) {
+    const LatticeEdge e = lattice_edge(h, 1.0 / h, r0, R0);
+    out2[0] = e.D2;
+    out2[1] = e.D3;
+}
+
+void hm_lattice_edge_pair(double h, double p, double q, double* out4) {
+    LatticeEdge a, b;
+    lattice_edge_pair(h, 1.0 / h, p, q, a, b);
+    out4[0] = a.D2;
+    out4[1] = a.D3;
+    out4[2] = b.D2;
+    out4[3] = b.D3;
+}
+
+double hm_lattice_corner(double h, double r0, double a1, double a2, const double* d4) {
+    return lattice_corner(h, 1.0 / h, r0, a1, a2, d4[0], d4[1], d4[2], d4[3]);
+}
+
+// edges: D2, D3 of xy, xz, yx, yz, zx, zy
+double hm_lattice_point(double h, double ax, double ay, double az, const double* e) {
+    PointEdges<double> E{e[0], e[1], e[2], e[3], e[4], e[5], e[6], e[7], e[8], e[9], e[10], e[11]};
+    return lattice_point(h, 1.0 / h, ax, ay, az, E);
 }
 }

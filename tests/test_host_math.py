@@ -28,6 +28,12 @@ def hm(tmp_path_factory):
                                                       C.POINTER(C.c_int)]
     L.hm_face_reachable.argtypes = [C.c_double] * 4 + [dp, C.c_int]
     L.hm_cell_grad.argtypes = [C.c_double] * 10 + [dp]
+    L.hm_lattice_edge.argtypes = [C.c_double] * 3 + [dp]
+    L.hm_lattice_edge_pair.argtypes = [C.c_double] * 3 + [dp]
+    L.hm_lattice_corner.restype = C.c_double
+    L.hm_lattice_corner.argtypes = [C.c_double] * 4 + [dp]
+    L.hm_lattice_point.restype = C.c_double
+    L.hm_lattice_point.argtypes = [C.c_double] * 4 + [dp]
     return L
 
 
@@ -96,3 +102,58 @@ def test_dual_cell_gradient(hm, oracle):
         worst = max(worst, (np.abs(g - fd) / np.abs(fd).max(axis=1, keepdims=True)).max())
     assert worst < 1e-7, worst
 
+
+
+def _lattice_cases(n, seed):
+    """Random lattice-point offsets within and beyond the support of a particle with h = 0.8, a part of
+    them with one offset shrunk towards the particle's planes."""
+    rng = np.random.default_rng(seed)
+    h = 0.8
+    for it in range(n):
+        a = 2.4 * h * rng.random(3)
+        if it % 7 == 0:
+            a[0] *= 1e-3
+        if it % 11 == 0:
+            a[1] *= 1e-6
+        yield h, a
+
+
+def test_lattice_edge_pair(hm):
+    """The edge tiers of a (p, q) pair evaluated together (lattice_edge_pair: shared half-chord, log term and
+    reciprocal) equal the two single tiers (lattice_edge) to rounding.  The tiers enter a corner value
+    multiplied by (r0/h)^3 / pi, so the differences are compared at that scale."""
+    dp = C.POINTER(C.c_double)
+    worst = 0.0
+    for h, a in _lattice_cases(20000, 31):
+        p, q = a[0], a[1]
+        if not (p * p + q * q <= 4 * h * h):
+            continue
+        pair, one, two = np.zeros(4), np.zeros(2), np.zeros(2)
+        hm.hm_lattice_edge_pair(h, p, q, pair.ctypes.data_as(dp))
+        hm.hm_lattice_edge(h, p, q, one.ctypes.data_as(dp))
+        hm.hm_lattice_edge(h, q, p, two.ctypes.data_as(dp))
+        K = np.array([p, p, q, q]) ** 3 / h ** 3 / np.pi
+        worst = max(worst, float(np.abs(K * (pair - np.concatenate([one, two]))).max()))
+    assert worst < 4e-15, worst
+
+
+def test_lattice_point(hm):
+    """A lattice point's three corner values evaluated together (lattice_point: one root, two reciprocals,
+    three log terms for the six pyramids) equal the sum of the three single corner values (lattice_corner)
+    to rounding, inside the support, beyond it, and next to the particle's planes."""
+    dp = C.POINTER(C.c_double)
+    worst = 0.0
+    for h, a in _lattice_cases(20000, 32):
+        ax, ay, az = a
+        E = {}
+        for nm, (r0, R0) in dict(xy=(ax, ay), xz=(ax, az), yx=(ay, ax), yz=(ay, az), zx=(az, ax), zy=(az, ay)).items():
+            E[nm] = np.zeros(2)
+            if r0 * r0 + R0 * R0 <= 4 * h * h:
+                hm.hm_lattice_edge(h, r0, R0, E[nm].ctypes.data_as(dp))
+        e = np.concatenate([E[k] for k in ("xy", "xz", "yx", "yz", "zx", "zy")])
+        point = hm.hm_lattice_point(h, ax, ay, az, e.ctypes.data_as(dp))
+        corners = sum(hm.hm_lattice_corner(h, r0, a1, a2, np.concatenate([E[e1], E[e2]]).ctypes.data_as(dp))
+                      for r0, a1, a2, e1, e2 in ((ax, ay, az, "xy", "xz"), (ay, ax, az, "yx", "yz"),
+                                                 (az, ax, ay, "zx", "zy")))
+        worst = max(worst, abs(point - corners))
+    assert worst < 4e-15, worst

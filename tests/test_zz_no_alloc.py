@@ -45,13 +45,14 @@ def _device_particles(torch, n, seed):
     return {k: torch.from_numpy(v).cuda() for k, v in P.items()}
 
 
-def _call_noalloc(kiwi_b200, f, dP, bounds, shape, out):
+def _call_noalloc(kiwi_b200, f, dP, bounds, shape, out, precision=None):
     Ps, _ = kiwi_b200._particles_struct(dP, device=True)
     grid = kiwi_b200.KiwiCartGrid((C.c_double * 6)(*bounds), *shape)
     sel = kiwi_b200.KernelIntegrator().sel()
     st = kiwi_b200.KiwiStats()
     err = C.create_string_buffer(512)
-    rc = f(None, C.byref(Ps), C.byref(grid), C.byref(sel), kiwi_b200.KIWI_FP64, _dptr(out["density"]),
+    prec = kiwi_b200.KIWI_FP64 if precision is None else precision
+    rc = f(None, C.byref(Ps), C.byref(grid), C.byref(sel), prec, _dptr(out["density"]),
            _dptr(out["vx"]), _dptr(out["vy"]), _dptr(out["vz"]), _dptr(out["raw4"]), C.byref(st), err, 512)
     return rc, st, err.value.decode()
 
@@ -78,6 +79,36 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls():
         for k in ref:
             assert torch.equal(out[k], ref[k]), (call, k)
         assert st.bbox_pairs == st_ref["bbox_pairs"] and st.sphere_pairs == st_ref["sphere_pairs"]
+
+
+def test_noalloc_allocates_no_device_memory():
+    """After a first (set-up) call, further calls -- plain FP64 and FP32-mixed, whose mixed kernel takes its
+    own scratch -- leave the device's free memory unchanged, and the FP32-mixed call equals the allocating
+    entry point's FP32-mixed result bit for bit."""
+    import torch
+
+    import kiwi_b200
+
+    f = _noalloc_fn()
+    ctx = kiwi_b200.Context(0)
+    bounds, shape = (0.0, 2.0, 0.0, 2.0, 0.0, 2.0), (32, 32, 32)
+    nc = shape[0] * shape[1] * shape[2]
+    dP = _device_particles(torch, 2500, 3)
+    out = {k: torch.zeros(nc, dtype=torch.float64, device="cuda") for k in ("density", "vx", "vy", "vz")}
+    out["raw4"] = torch.zeros(4 * nc, dtype=torch.float64, device="cuda")
+    ref = {k: torch.zeros_like(v) for k, v in out.items()}
+    kiwi_b200.sph_to_grid_device(dP, bounds, shape, ref, precision="fp32_mixed", ctx=ctx)
+    rc, _, msg = _call_noalloc(kiwi_b200, f, dP, bounds, shape, out)
+    assert rc == 0, msg
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for prec in (kiwi_b200.KIWI_FP64, kiwi_b200.KIWI_FP32_MIXED, kiwi_b200.KIWI_FP32_MIXED):
+        rc, _, msg = _call_noalloc(kiwi_b200, f, dP, bounds, shape, out, precision=prec)
+        assert rc == 0, msg
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] >= free0
+    for k in ref:
+        assert torch.equal(out[k], ref[k]), k
 
 
 def test_noalloc_rejects_input_beyond_the_scratch_limit():
