@@ -82,6 +82,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=1002)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip parity_c1: config 1 on the GPU and through the reference's stage (~3 min of host CPU)")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="with --precision fp64: skip timing the FP32-mixed form beside it")
     ap.add_argument("--multi", default="tiles", choices=["tiles", "replicas"],
@@ -257,6 +259,42 @@ def cpu_baseline(P, bounds, shape, kernel_name):
                       f"per thread), {b} bounding-box / {s} support pairs, {t:.1f} s wall on {threads} OpenMP "
                       f"threads; the reference's KernelIntegrator::face over each cell's six box faces",
             "bbox_pairs_per_s": b / t}
+
+
+def cpu_baseline_c1(kiwi_b200, ctx):
+    """Config 1 (the 7,300-particle column on its 100 x 100 x 410 grid of 0.02 pc cells, the CPU-runnable
+    configuration) mapped twice: on the GPU through the public host API (host arrays in and out), and by the
+    reference's own run_sph_to_grid_stage (oracle/_ref) on all host cores -- its stage wall time is the CPU
+    baseline of this configuration, and its grid is the checker of the GPU's, cell by cell per density band
+    (parity_c1)."""
+    from oracle.compare import band_stats
+    from oracle.oracle import load_ref
+
+    ref = load_ref()
+    if ref is None:
+        return None
+    wl = _standalone("kiwi_workloads", "kiwi_b200/workloads.py")
+    P, b = wl.column_snapshot()
+    shape = (100, 100, 410)
+    kiwi_b200.sph_to_grid(P, b, shape, ctx=ctx)  # warm-up
+    t0 = time.perf_counter()
+    r = kiwi_b200.sph_to_grid(P, b, shape, ctx=ctx)
+    gpu_s = time.perf_counter() - t0
+    threads = ref.max_threads()
+    t0 = time.perf_counter()
+    rd = ref.sph_to_grid(P, b, shape, threads=threads)
+    ref_s = time.perf_counter() - t0
+    sig = rd[0] > 1e-6 * rd[0].max()
+    dv = max(float(np.max(np.abs(getattr(r, k)[sig] - v[sig]))) for k, v in zip(("vx", "vy", "vz"), rd[1:]))
+    pairs, bbox = r.stats["sphere_pairs"], r.stats["bbox_pairs"]
+    return {"workload": "column n=7300 (60% uniform + 40% filament, h from 57-NN), grid 100x100x410 of 0.02 pc",
+            "support_pairs": int(pairs), "bbox_pairs": int(bbox),
+            "gpu_e2e_s": gpu_s, "gpu_e2e_pairs_per_s": pairs / gpu_s,
+            "reference_stage_s": ref_s, "reference_stage_pairs_per_s": pairs / ref_s, "reference_cores": threads,
+            "against": "the reference's run_sph_to_grid_stage (oracle/_ref) on the same particles, every cell",
+            "density_bands": band_stats(r.density, rd[0]),
+            "max_abs_velocity_diff_above_1e-6_peak_km_s": dv,
+            "total_mass_rel_diff": float(abs(r.density.sum() - rd[0].sum()) / rd[0].sum())}
 
 
 def run_reference(args):
@@ -848,8 +886,11 @@ def main():
                "ms_per_step": e_ms / args.e2e_steps}
 
     cpu = None
+    parity_c1 = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline and not args.tabulated:
         cpu = cpu_baseline(P, bounds, shape, args.kernel)
+        if not args.no_parity and args.kernel == "cubic_spline" and args.precision == "fp64":
+            parity_c1 = cpu_baseline_c1(kiwi_b200, ctx)
 
     if rank == 0:
         g_ms = float(np.mean(gather_ms))
@@ -922,6 +963,8 @@ def main():
             line["roofline"] = tab_roofline
         if accuracy is not None:
             line["accuracy"] = accuracy
+        if parity_c1 is not None:
+            line["parity_c1"] = parity_c1
         if fp32_side is not None:
             # the FP32 kernel evaluates the same lattice work items as the FP64 one
             peak32 = kiwi_b200.measure_fp32_peak(ctx)

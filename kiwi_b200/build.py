@@ -3,7 +3,10 @@
 Each translation unit carries its own floating-point contract:
   * the plain all-FP64 form and the host/binning code: --fmad=false, so that products and sums round
     exactly as the reference's x86-64 build does;
-  * the FP32-mixed form: FMA contraction on (its error budget is stated against the FP64 oracle).
+  * the lattice forms (lattice.cu, the adjoint) and the FP32-mixed form: FMA contraction on -- they regroup
+    the reference's sum, so rounding each product on its own buys nothing; the quantities integer results
+    depend on (bounding boxes, lattice planes, cell centres, the pair counters' support test) use explicitly
+    rounded operations in every unit.
 
 Usage: python -m kiwi_b200.build [--verbose]   (or kiwi_b200.build.build())
 """
@@ -29,7 +32,7 @@ UNITS = [
     ("lattice.cu", []),
     ("noalloc.cu", ["--fmad=false"]),
     ("voronoi.cu", ["--fmad=false"]),
-    ("adjoint.cu", ["--fmad=false"]),
+    ("adjoint.cu", []),
     ("mixed.cu", []),
     ("batch.cu", ["--fmad=false"]),
     ("io.cu", []),

@@ -6,21 +6,20 @@
 //   dL/dm_p     = sum_c K_pc (gM_c + v_p . gP_c)
 //   dL/dv_p     = m_p sum_c K_pc gP_c
 //   dL/dtheta_p = m_p sum_c dK_pc/dtheta (gM_c + v_p . gP_c),   theta = x, y, z, h.
-// The per-pair cell integrals are recomputed, not stored: the forward kernel's lattice tiers (lattice_edge,
-// lattice_corner) are instantiated with the Dual4 type, which carries d/dx, d/dy, d/dz, d/dh of every
-// intermediate through the same operations, so the
-// value part equals the forward's Msum bit for bit and the derivative part is the exact derivative of the
-// evaluated formula (branch choices are taken on values).  A clamped pair (Msum < 0) has K = 0 and no
+// The per-pair cell integrals are recomputed, not stored: the forward kernel's lattice tiers
+// (lattice_edge_pair, lattice_point) are instantiated with the Dual3 type, which carries d/dx, d/dy, d/dz of
+// every intermediate through the same operations (d/dh follows from them, see k_cart_adjoint_lattice), so the
+// derivative part is the exact derivative of the evaluated formula (branch choices are taken on values).  A clamped pair (Msum < 0) has K = 0 and no
 // gradient.  The pairs are those of the forward's default evaluation: the cells of the particle's
 // support bounding box whose closest point lies within the support radius.
 //
-// The evaluation is the lattice form of the forward pass (lattice.cuh) in Dual4: one CTA per 8^3-cell
-// tile walks the tile's particles in chunks; (A) the edge tiers of every (plane, edge line) and (B) the
-// corner values of every (plane, lattice point) are computed once per particle with their derivatives;
-// (C) for each particle, each thread assembles the cells it owns from the 24 corner values (value and
-// derivatives alike), weighs them with the cells' cotangents, and a fixed-order block reduction writes the
-// particle's partial gradient for this tile to its (tile, particle) entry.  (D) Each particle's entries
-// are then added in tile order.  Deterministic, no atomics on the gradients.
+// The evaluation is the lattice form of the forward pass (lattice_tile.cuh) with derivatives: one CTA per
+// 8^3-cell tile walks the tile's particles in chunks; (A) the edge tiers of every (plane, edge line), in
+// swapped pairs, and (B) the octant value of every lattice point are computed once per particle with their
+// derivatives; (C) for each particle, each thread assembles the cells it owns from their 8 corners' octant
+// values (value and derivatives alike), weighs them with the cells' cotangents, and a fixed-order block
+// reduction writes the particle's partial gradient for this tile to its (tile, particle) entry.  (D) Each
+// particle's entries are then added in tile order.  Deterministic, no atomics on the gradients.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,40 +41,47 @@ namespace {
 constexpr int kAdjLatThreads = 256;
 constexpr int kAdjCellsPerThread = kTileCells / kAdjLatThreads;
 constexpr int kAdjPMax = 32;
-constexpr int kAdjECap = 512;   // edge entries per chunk (a full 8^3 particle box needs 486)
-constexpr int kAdjSCap = 2304;  // corner entries per chunk (a full 8^3 particle box needs 2187)
-constexpr int kAdjERec = 10;    // D2, D3 as Dual4
-constexpr int kAdjSRec = 5;     // S as Dual4
-constexpr size_t kAdjDynSmem = sizeof(double) * (kAdjERec * kAdjECap + kAdjSRec * kAdjSCap);
-constexpr int kAdjPtCap = kAdjSCap / 3;  // lattice points per chunk (three corner items each)
+constexpr int kAdjECap = 1536;  // edge slots per chunk (a full 8^3 particle box has 486)
+constexpr int kAdjPtCap = 2304; // lattice points per chunk (a full 8^3 particle box has 729)
+constexpr int kAdjERec = 8;     // D2, D3 as Dual3
+constexpr int kAdjTRec = 5;     // octant value and its derivatives with respect to x, y, z, h
+constexpr size_t kAdjDynSmem = sizeof(double) * (kAdjERec * kAdjECap + kAdjTRec * kAdjPtCap);
+static_assert(kAdjECap <= 2048, "packed edge-pair entries (11-bit slots)");
 
 struct AdjGrads {
     double *x, *y, *z, *h, *m, *vx, *vy, *vz;
 };
 
-__device__ __forceinline__ Dual4 dual_abs_offset(double off, int axis) {
-    // |plane - x_axis| and its derivative with respect to the particle's coordinate on that axis
-    Dual4 r(fabs(off));
+// |plane - x_axis| with its derivative with respect to the particle's coordinate on that axis
+__device__ __forceinline__ Dual3 dual_abs_offset(double off, int axis) {
+    Dual3 r(fabs(off));
     r.d[axis] = off > 0.0 ? -1.0 : (off < 0.0 ? 1.0 : 0.0);
     return r;
 }
 
-__device__ __forceinline__ Dual4 load_dual(const double* p) {
-    Dual4 r(p[0]);
+__device__ __forceinline__ Dual3 load_dual(const double* p) {
+    Dual3 r(p[0]);
     r.d[0] = p[1];
     r.d[1] = p[2];
     r.d[2] = p[3];
-    r.d[3] = p[4];
     return r;
 }
 
-__device__ __forceinline__ void store_dual(double* p, const Dual4& v) {
+__device__ __forceinline__ void store_dual(double* p, const Dual3& v) {
     p[0] = v.v;
     p[1] = v.d[0];
     p[2] = v.d[1];
     p[3] = v.d[2];
-    p[4] = v.d[3];
 }
+
+// The six edge tiers (with derivatives) of a lattice point, read from the chunk's table where lattice_point
+// uses them: slots in PointEdge order, D2 at +0 and D3 at +4 of each record.
+struct SmemDualEdges {
+    const double* rec;
+    int slot[6];
+    __device__ __forceinline__ Dual3 D2(int e) const { return load_dual(rec + kAdjERec * slot[e]); }
+    __device__ __forceinline__ Dual3 D3(int e) const { return load_dual(rec + kAdjERec * slot[e] + 4); }
+};
 
 __device__ __forceinline__ unsigned long long block_count(unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -85,6 +91,13 @@ __device__ __forceinline__ unsigned long long block_count(unsigned long long v) 
 // (A)-(C) for one tile: list holds (tile, particle) entry indices (the entries of particle p are
 // offs[p] .. offs[p+1]-1); part receives 8 doubles per entry: dL/dm, dL/d(x, y, z, h), dL/d(vx, vy, vz)
 // over this tile's cells.
+//
+// The octant value T of a lattice point at offsets u = (ux, uy, uz) from the particle is sgn(ux) sgn(uy)
+// sgn(uz) G(|ux|, |uy|, |uz|), with G the kernel mass of the box spanned by the particle and the point
+// (lattice_point).  G is a mass fraction of a kernel of scale h, so G(a, b, c; h) = G(a/h, b/h, c/h; 1): it is
+// homogeneous of degree 0 in (a, b, c, h), whence dT/dh = (ux dT/dx + uy dT/dy + uz dT/dz) / h with the
+// derivatives taken with respect to the particle's coordinates (u = plane - particle).  The tiers are
+// therefore evaluated with three forward derivatives (Dual3, h held fixed) and dT/dh follows from them.
 __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(CartGeom g, DevParticles P,
                                                                           const uint32_t* __restrict__ list,
                                                                           const int64_t* __restrict__ range,
@@ -92,17 +105,19 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                                                                           const double* __restrict__ cot,
                                                                           double* __restrict__ part,
                                                                           DevStats* __restrict__ st) {
-    __shared__ double s_x[kAdjPMax], s_y[kAdjPMax], s_z[kAdjPMax], s_h[kAdjPMax], s_m[kAdjPMax], s_vx[kAdjPMax],
-        s_vy[kAdjPMax], s_vz[kAdjPMax];
-    __shared__ int s_lo[kAdjPMax][3], s_dim[kAdjPMax][3], s_eoff[kAdjPMax], s_soff[kAdjPMax];
+    __shared__ double s_x[kAdjPMax], s_y[kAdjPMax], s_z[kAdjPMax], s_h[kAdjPMax], s_ih[kAdjPMax], s_m[kAdjPMax],
+        s_vx[kAdjPMax], s_vy[kAdjPMax], s_vz[kAdjPMax];
+    __shared__ int s_lo[kAdjPMax][3], s_dim[kAdjPMax][3], s_eoff[kAdjPMax], s_poff[kAdjPMax];
     __shared__ uint32_t s_entry[kAdjPMax];
-    __shared__ uint32_t s_mag[kAdjPMax][4];  // div_magic of n0, n1, n2 and n1 n2
-    __shared__ uint32_t s_blist[kAdjPtCap];
-    __shared__ int s_np, s_etot, s_stot, s_nexp, s_ncheap;
+    __shared__ uint32_t s_mag[kAdjPMax][4];  // div_magic of n0', n1', n2' and n1' n2'
+    __shared__ uint32_t s_plist[kAdjPtCap];
+    __shared__ uint32_t s_hlist[kAdjECap / 2];
+    __shared__ int s_np, s_etot, s_ptot, s_nexp, s_ncheap, s_nheavy;
     __shared__ double s_red[kAdjLatThreads / 32][8];
+    __shared__ double s_pl[3][kTileX + 1];
     extern __shared__ double s_adj[];
     double* s_E = s_adj;
-    double* s_S = s_adj + kAdjERec * kAdjECap;
+    double* s_T = s_adj + kAdjERec * kAdjECap;
 
     const int64_t t = blockIdx.x;
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
@@ -111,11 +126,16 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
     const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
     unsigned long long n_eval = 0, n_neg = 0;
     const int64_t beg = range[2 * t], end = range[2 * t + 1];
+    if (threadIdx.x < 3 * (kTileX + 1)) {
+        const int a = threadIdx.x / (kTileX + 1), l = threadIdx.x % (kTileX + 1);
+        const double mn = a == 0 ? g.x_min : (a == 1 ? g.y_min : g.z_min), d = a == 0 ? g.dpx : (a == 1 ? g.dpy : g.dpz);
+        s_pl[a][l] = add_rn(mn, mul_rn((double)((a == 0 ? bx : (a == 1 ? by : bz)) + l), d));
+    }
 
     for (int64_t pos = beg; pos < end;) {
         if (warp == 0) {
             const int64_t idx = pos + lane;
-            int ne = 0, ns = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+            int ne = 0, npt = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
             double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
             uint32_t e = 0;
             if (idx < end) {
@@ -137,25 +157,25 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
                 const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
                 ne = 2 * (n0 * n1 + n0 * n2 + n1 * n2);
-                ns = 3 * n0 * n1 * n2;
+                npt = n0 * n1 * n2;
             }
-            int ie = ne, is = ns;
+            int ie = ne, ip = npt;
             for (int o = 1; o < 32; o <<= 1) {
-                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vs = __shfl_up_sync(0xffffffffu, is, o);
+                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vp = __shfl_up_sync(0xffffffffu, ip, o);
                 if (lane >= o) {
                     ie += ve;
-                    is += vs;
+                    ip += vp;
                 }
             }
-            const bool take = (idx < end) && ie <= kAdjECap && is <= kAdjSCap;
+            const bool take = (idx < end) && ie <= kAdjECap && ip <= kAdjPtCap;
             const int np = __popc(__ballot_sync(0xffffffffu, take));
             if (take) {
-                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph;
+                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph; s_ih[lane] = 1.0 / ph;
                 s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
                 s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
                 s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
                 s_eoff[lane] = ie - ne;
-                s_soff[lane] = is - ns;
+                s_poff[lane] = ip - npt;
                 s_entry[lane] = e;
                 s_mag[lane][0] = div_magic(d0 + 1);
                 s_mag[lane][1] = div_magic(d1 + 1);
@@ -165,56 +185,67 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
             if (lane == np - 1) {
                 s_np = np;
                 s_etot = ie;
-                s_stot = is;
-                s_nexp = s_ncheap = 0;
+                s_ptot = ip;
+                s_nexp = s_ncheap = s_nheavy = 0;
             }
         }
         __syncthreads();
-        const int np = s_np, etot = s_etot, stot = s_stot;
+        const int np = s_np, etot = s_etot, ptot = s_ptot;
 
-        // (A) edge tiers with derivatives
-        for (int it = threadIdx.x; it < etot; it += kAdjLatThreads) {
-            const int j = chunk_search(s_eoff, np, it);
-            int e = it - s_eoff[j];
-            const int n[3] = {s_dim[j][0] + 1, s_dim[j][1] + 1, s_dim[j][2] + 1};
-            int a = 0, bax = 1;
-            {
-                const int sz[6] = {n[0] * n[1], n[0] * n[2], n[1] * n[0], n[1] * n[2], n[2] * n[0], n[2] * n[1]};
-                const int aa[6] = {0, 0, 1, 1, 2, 2}, bb[6] = {1, 2, 0, 2, 0, 1};
-                int blk = 0;
-                while (e >= sz[blk]) {
-                    e -= sz[blk];
-                    ++blk;
+        // (A) edge pairs, as the forward kernel walks them: pairs beyond 2h (or zero) get D2 = D3 = 0; the
+        // others are listed (slot ab | slot ba << 11 | particle << 22 | pair block << 27) with the two signed
+        // offsets parked in slot ab, and evaluated in (A2) by full warps.
+        {
+            const int qtot = etot >> 1;
+            const int qoff_l = lane < np ? (s_eoff[lane] >> 1) : INT_MAX;
+            for (int base = warp * 32; base < qtot; base += kAdjLatThreads) {
+                const int it = base + lane;
+                bool heavy = false;
+                uint32_t hrec = 0;
+                const int j = warp_owner(base, qoff_l, lane);
+                const int qoff = __shfl_sync(0xffffffffu, qoff_l, j & 31);
+                if (it < qtot) {
+                    int e = it - qoff;
+                    const int n0 = s_dim[j][0] + 1, n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
+                    const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
+                    const int blk = (e >= nxy) + (e >= nxy + nxz);
+                    e -= blk == 0 ? 0 : (blk == 1 ? nxy : nxy + nxz);
+                    const int a = blk == 2 ? 1 : 0, b = blk == 0 ? 1 : 2;
+                    const int nb = b == 1 ? n1 : n2, na = a == 0 ? n0 : n1;
+                    const int pi = div_by(e, s_mag[j][b]), qi = e - pi * nb;
+                    const int eb = s_eoff[j];
+                    const int sab = eb + (blk == 0 ? 0 : (blk == 1 ? nxy : 2 * nxy + nxz)) + pi * nb + qi;
+                    const int sba = eb + (blk == 0 ? nxy + nxz : (blk == 1 ? 2 * nxy + nxz + nyz : 2 * nxy + 2 * nxz + nyz)) +
+                                    qi * na + pi;
+                    const int la = s_lo[j][a] - (a == 0 ? bx : by), lb = s_lo[j][b] - (b == 1 ? by : bz);
+                    const double oa = s_pl[a][la + pi] - (a == 0 ? s_x[j] : s_y[j]);
+                    const double ob = s_pl[b][lb + qi] - (b == 1 ? s_y[j] : s_z[j]);
+                    const double h = s_h[j];
+                    heavy = oa != 0.0 && ob != 0.0 && oa * oa + ob * ob <= 4.0 * (h * h);
+                    if (heavy) {
+                        s_E[kAdjERec * sab] = oa;
+                        s_E[kAdjERec * sab + 1] = ob;
+                        hrec = (uint32_t)sab | (uint32_t)sba << 11 | (uint32_t)j << 22 | (uint32_t)blk << 27;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < kAdjERec; ++k) s_E[kAdjERec * sab + k] = s_E[kAdjERec * sba + k] = 0.0;
+                    }
                 }
-                a = aa[blk];
-                bax = bb[blk];
+                const unsigned m = __ballot_sync(0xffffffffu, heavy);
+                int hp = 0;
+                if (lane == 0 && m) hp = atomicAdd(&s_nheavy, __popc(m));
+                hp = __shfl_sync(0xffffffffu, hp, 0);
+                if (heavy) s_hlist[hp + __popc(m & ((1u << lane) - 1))] = hrec;
             }
-            const int p = e / n[bax], q = e % n[bax];
-            const double mn[3] = {g.x_min, g.y_min, g.z_min}, dd[3] = {g.dpx, g.dpy, g.dpz};
-            const double pc[3] = {s_x[j], s_y[j], s_z[j]};
-            const Dual4 r0 = dual_abs_offset(lattice_offset(mn[a], dd[a], s_lo[j][a] + p, pc[a]), a);
-            const Dual4 R0 = dual_abs_offset(lattice_offset(mn[bax], dd[bax], s_lo[j][bax] + q, pc[bax]), bax);
-            const Dual4 hD = Dual4::seed(s_h[j], 3);
-            // the forward kernel's edge tier (lattice_edge) in Dual4; zero beyond 2h and for zero offsets
-            Dual4 D2(0.0), D3(0.0);
-            if (r0 != 0.0 && R0 != 0.0 && r0.v * r0.v + R0.v * R0.v <= 4.0 * (s_h[j] * s_h[j])) {
-                const LatticeEdgeT<Dual4> ed = lattice_edge(hD, 1.0 / hD, r0, R0);
-                D2 = ed.D2;
-                D3 = ed.D3;
-            }
-            store_dual(s_E + kAdjERec * it, D2);
-            store_dual(s_E + kAdjERec * it + 5, D3);
         }
 
-        // (B0) the corner items, listed lattice point by lattice point as in the forward kernel: corners
-        // that no evaluated cell reads left out (the same padded test), corners beyond 2h (or zero) from
-        // the end of s_blist so that they run in warps of their own; a list entry packs (particle, i, j, k).
+        // (B0) the lattice points some evaluated cell reads, listed as in the forward kernel (the same padded
+        // test); a point on a particle plane has octant value 0 and no derivative, written here.
         {
-            const int ptot = stot / 3;
-            const int poff_l = lane < np ? s_soff[lane] / 3 : INT_MAX;
+            const int poff_l = lane < np ? s_poff[lane] : INT_MAX;
             for (int base = warp * 32; base < ptot; base += kAdjLatThreads) {
                 const int pt = base + lane;
-                int cls = -1;  // -1 none, 0 general, 1 cheap
+                int cls = -1;  // -1 none, 0 within 2h, 1 beyond
                 uint32_t rec = 0;
                 const int jp = warp_owner(base, poff_l, lane);
                 const int poff = __shfl_sync(0xffffffffu, poff_l, jp & 31);
@@ -223,17 +254,21 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                     const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
                     const int i = div_by(lp, s_mag[jp][3]), rem = lp - i * n12;
                     const int jj = div_by(rem, s_mag[jp][2]), k = rem - jj * n2;
-                    const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
-                    const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
-                    const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+                    const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
+                    const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
+                    const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
                     const double h = s_h[jp], radius = mul_rn(g.support_in_h, h);
                     const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
                     const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
                     const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
                     if (ex * ex + ey * ey + ez * ez < radius * radius) {
-                        const bool zero = ux == 0.0 || uy == 0.0 || uz == 0.0;
-                        cls = (zero || !(ux * ux + uy * uy + uz * uz < 4.0 * (h * h))) ? 1 : 0;
-                        rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
+                        if (ux == 0.0 || uy == 0.0 || uz == 0.0) {
+#pragma unroll
+                            for (int c = 0; c < kAdjTRec; ++c) s_T[kAdjTRec * pt + c] = 0.0;
+                        } else {
+                            cls = (ux * ux + uy * uy + uz * uz < 4.0 * (h * h)) ? 0 : 1;
+                            rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
+                        }
                     }
                 }
                 const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
@@ -245,66 +280,69 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 pe = __shfl_sync(0xffffffffu, pe, 0);
                 pcb = __shfl_sync(0xffffffffu, pcb, 0);
                 const unsigned below = (1u << lane) - 1;
-                if (cls >= 0) s_blist[cls == 0 ? pe + __popc(me & below) : kAdjPtCap - 1 - pcb - __popc(mc & below)] = rec;
+                if (cls >= 0) s_plist[cls == 0 ? pe + __popc(me & below) : kAdjPtCap - 1 - pcb - __popc(mc & below)] = rec;
             }
         }
         __syncthreads();
 
-        // (B) corner values with derivatives
+        // (A2) the listed edge pairs with their derivatives (the forward kernel's lattice_edge_pair in Dual3)
+        {
+            const int nheavy = s_nheavy;
+            for (int li = threadIdx.x; li < nheavy; li += kAdjLatThreads) {
+                const uint32_t rec = s_hlist[li];
+                const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)((rec >> 22) & 31u);
+                const int blk = (int)(rec >> 27);
+                const int a = blk == 2 ? 1 : 0, b = blk == 0 ? 1 : 2;
+                const Dual3 pD = dual_abs_offset(s_E[kAdjERec * sab], a);
+                const Dual3 qD = dual_abs_offset(s_E[kAdjERec * sab + 1], b);
+                LatticeEdgeT<Dual3> e_pq, e_qp;
+                lattice_edge_pair(Dual3(s_h[j]), Dual3(s_ih[j]), pD, qD, e_pq, e_qp);
+                store_dual(s_E + kAdjERec * sab, e_pq.D2);
+                store_dual(s_E + kAdjERec * sab + 4, e_pq.D3);
+                store_dual(s_E + kAdjERec * sba, e_qp.D2);
+                store_dual(s_E + kAdjERec * sba + 4, e_qp.D3);
+            }
+        }
+        __syncthreads();
+
+        // (B) octant values with their derivatives
         const int nexp = s_nexp, ncheap = s_ncheap;
-        for (int li = threadIdx.x; li < 3 * (nexp + ncheap); li += kAdjLatThreads) {
-            const int pli = li / 3, axis = li - 3 * pli;
-            const uint32_t rec = s_blist[pli < nexp ? pli : kAdjPtCap - ncheap + (pli - nexp)];
+        for (int li = threadIdx.x; li < nexp + ncheap; li += kAdjLatThreads) {
+            const uint32_t rec = s_plist[li < nexp ? li : kAdjPtCap - ncheap + (li - nexp)];
             const int jp = (int)(rec & 31u), i = (int)((rec >> 5) & 15u), jj = (int)((rec >> 9) & 15u),
                       k = (int)((rec >> 13) & 15u);
             const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
-            const int it = s_soff[jp] + axis * (n0 * n1 * n2) + (i * n1 + jj) * n2 + k;
-            const double ux = lattice_offset(g.x_min, g.dpx, s_lo[jp][0] + i, s_x[jp]);
-            const double uy = lattice_offset(g.y_min, g.dpy, s_lo[jp][1] + jj, s_y[jp]);
-            const double uz = lattice_offset(g.z_min, g.dpz, s_lo[jp][2] + k, s_z[jp]);
+            const int it = s_poff[jp] + (i * n1 + jj) * n2 + k;
+            const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
+            const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
+            const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
             const int eb = s_eoff[jp];
             const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
-            double ua, u1, u2;
-            int ax1, ax2, e1, e2;
-            if (axis == 0) {
-                ua = ux; u1 = uy; u2 = uz; ax1 = 1; ax2 = 2;
-                e1 = eb + i * n1 + jj;
-                e2 = eb + nxy + i * n2 + k;
-            } else if (axis == 1) {
-                ua = uy; u1 = ux; u2 = uz; ax1 = 0; ax2 = 2;
-                e1 = eb + nxy + nxz + jj * n0 + i;
-                e2 = eb + 2 * nxy + nxz + jj * n2 + k;
-            } else {
-                ua = uz; u1 = ux; u2 = uy; ax1 = 0; ax2 = 1;
-                e1 = eb + 2 * nxy + nxz + nyz + k * n0 + i;
-                e2 = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
-            }
-            Dual4 f(0.0);
-            const double sg = sgn(u1) * sgn(u2);
-            if (sg != 0.0 && ua != 0.0) {
-                const Dual4 r0 = dual_abs_offset(ua, axis);
-                const Dual4 a1 = dual_abs_offset(u1, ax1), a2 = dual_abs_offset(u2, ax2);
-                const Dual4 hD = Dual4::seed(s_h[jp], 3);
-                // the forward kernel's corner pair (lattice_corner) in Dual4
-                f = lattice_corner(hD, 1.0 / hD, r0, a1, a2, load_dual(s_E + kAdjERec * e1), load_dual(s_E + kAdjERec * e1 + 5),
-                                   load_dual(s_E + kAdjERec * e2), load_dual(s_E + kAdjERec * e2 + 5));
-            }
-            store_dual(s_S + kAdjSRec * it, sg * f);
+            const SmemDualEdges PE{s_E,
+                                   {eb + i * n1 + jj, eb + nxy + i * n2 + k, eb + nxy + nxz + jj * n0 + i,
+                                    eb + 2 * nxy + nxz + jj * n2 + k, eb + 2 * nxy + nxz + nyz + k * n0 + i,
+                                    eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj}};
+            const double sg = sgn(ux) * sgn(uy) * sgn(uz);
+            const Dual3 f = sg * lattice_point(Dual3(s_h[jp]), Dual3(s_ih[jp]), dual_abs_offset(ux, 0),
+                                               dual_abs_offset(uy, 1), dual_abs_offset(uz, 2), PE);
+            double* o = s_T + kAdjTRec * it;
+            o[0] = f.v;
+            o[1] = f.d[0];
+            o[2] = f.d[1];
+            o[3] = f.d[2];
+            o[4] = (ux * f.d[0] + uy * f.d[1] + uz * f.d[2]) * s_ih[jp];
         }
         __syncthreads();
 
-        // (C) per particle: the cells' values and derivatives from the corners, weighed by the cotangents
+        // (C) per particle: each cell's value and derivatives as the alternating sum of its 8 corners,
+        // weighed by the cell's cotangents
         for (int j = 0; j < np; ++j) {
             double acc[8];
 #pragma unroll
             for (int c = 0; c < 8; ++c) acc[c] = 0.0;
             const double x0 = s_x[j], y0 = s_y[j], z0 = s_z[j];
             const double radius = mul_rn(g.support_in_h, s_h[j]);
-            const int n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
-            const int L = (s_dim[j][0] + 1) * n1 * n2;
-            const double* Sx = s_S + kAdjSRec * s_soff[j];
-            const double* Sy = Sx + kAdjSRec * L;
-            const double* Sz = Sy + kAdjSRec * L;
+            const int n2 = s_dim[j][2] + 1, n12 = (s_dim[j][1] + 1) * n2;
 #pragma unroll
             for (int c = 0; c < kAdjCellsPerThread; ++c) {
                 const int li = threadIdx.x + c * kAdjLatThreads;
@@ -314,22 +352,15 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 const double ex = fmax(fabs(x0 - cell_centre(g.x_min, gx, g.dpx)) - g.hpx, 0.0);
                 const double ey = fmax(fabs(y0 - cell_centre(g.y_min, gy, g.dpy)) - g.hpy, 0.0);
                 const double ez = fmax(fabs(z0 - cell_centre(g.z_min, gz, g.dpz)) - g.hpz, 0.0);
-                if (!(ex * ex + ey * ey + ez * ez < radius * radius)) continue;
+                if (!(add_rn(add_rn(mul_rn(ex, ex), mul_rn(ey, ey)), mul_rn(ez, ez)) < mul_rn(radius, radius))) continue;
                 ++n_eval;
-                const double sx1 = sgn(lattice_offset(g.x_min, g.dpx, gx + 1, x0)), sx0 = sgn(lattice_offset(g.x_min, g.dpx, gx, x0));
-                const double sy1 = sgn(lattice_offset(g.y_min, g.dpy, gy + 1, y0)), sy0 = sgn(lattice_offset(g.y_min, g.dpy, gy, y0));
-                const double sz1 = sgn(lattice_offset(g.z_min, g.dpz, gz + 1, z0)), sz0 = sgn(lattice_offset(g.z_min, g.dpz, gz, z0));
-                // component comp of the cell's Msum: 0 the value (the forward's sum, same order), 1..4 d/d(x, y, z, h)
+                const double* Tp = s_T + kAdjTRec * (s_poff[j] + (i * (s_dim[j][1] + 1) + jj) * n2 + k);
+                // component comp of the cell's Msum: 0 the value, 1..4 d/d(x, y, z, h)
                 auto cell_sum = [&](int comp) {
-                    auto at = [&](const double* S, int a, int b, int cc) { return S[kAdjSRec * ((a * n1 + b) * n2 + cc) + comp]; };
-                    double m = 0.0;
-                    m += sx1 * (at(Sx, i + 1, jj + 1, k + 1) - at(Sx, i + 1, jj, k + 1) - at(Sx, i + 1, jj + 1, k) + at(Sx, i + 1, jj, k));
-                    m -= sx0 * (at(Sx, i, jj + 1, k + 1) - at(Sx, i, jj, k + 1) - at(Sx, i, jj + 1, k) + at(Sx, i, jj, k));
-                    m += sy1 * (at(Sy, i + 1, jj + 1, k + 1) - at(Sy, i, jj + 1, k + 1) - at(Sy, i + 1, jj + 1, k) + at(Sy, i, jj + 1, k));
-                    m -= sy0 * (at(Sy, i + 1, jj, k + 1) - at(Sy, i, jj, k + 1) - at(Sy, i + 1, jj, k) + at(Sy, i, jj, k));
-                    m += sz1 * (at(Sz, i + 1, jj + 1, k + 1) - at(Sz, i, jj + 1, k + 1) - at(Sz, i + 1, jj, k + 1) + at(Sz, i, jj, k + 1));
-                    m -= sz0 * (at(Sz, i + 1, jj + 1, k) - at(Sz, i, jj + 1, k) - at(Sz, i + 1, jj, k) + at(Sz, i, jj, k));
-                    return m;
+                    auto at = [&](int off) { return Tp[kAdjTRec * off + comp]; };
+                    const double m1 = (at(n12 + n2 + 1) - at(n12 + n2)) - (at(n12 + 1) - at(n12));
+                    const double m0 = (at(n2 + 1) - at(n2)) - (at(1) - at(0));
+                    return m1 - m0;
                 };
                 const double msum = cell_sum(0);
                 if (msum < 0.0) {
@@ -341,7 +372,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 const double gM = cot[i3], gx_ = cot[ncell + i3], gy_ = cot[2 * ncell + i3], gz_ = cot[3 * ncell + i3];
                 const double gs = gM + s_vx[j] * gx_ + s_vy[j] * gy_ + s_vz[j] * gz_;
                 acc[0] += msum * gs;
-#pragma unroll 1
+#pragma unroll
                 for (int comp = 1; comp <= 4; ++comp) acc[comp] += cell_sum(comp) * gs;
                 acc[5] += msum * gx_;
                 acc[6] += msum * gy_;

@@ -257,10 +257,15 @@ KIWI_LAT_CORNER T lattice_corner(T h, T ih, T r0, T a1, T a2, T D2a, T D3a, T D2
 // carry no flux), so a cell's mass is the 8-term difference of its corners' octant values.
 
 // The six edge tiers a lattice point reads: wall x with edge lines at |uy| (xy) and |uz| (xz), wall y with
-// lines at |ux| (yx) and |uz| (yz), wall z with lines at |ux| (zx) and |uy| (zy).
+// lines at |ux| (yx) and |uz| (yz), wall z with lines at |ux| (zx) and |uy| (zy).  lattice_point reads them
+// through an accessor with D2(e) and D3(e), e one of these, so that each is loaded where it is used; this
+// one holds them as values.
+enum PointEdge { kEdgeXY = 0, kEdgeXZ, kEdgeYX, kEdgeYZ, kEdgeZX, kEdgeZY };
 template <class T>
 struct PointEdges {
-    T xy2, xy3, xz2, xz3, yx2, yx3, yz2, yz3, zx2, zx3, zy2, zy3;  // D2, D3 of each
+    T d2[6], d3[6];
+    KIWI_HD T D2(int e) const { return d2[e]; }
+    KIWI_HD T D3(int e) const { return d3[e]; }
 };
 
 // One vertex pyramid of the series inside 2h (lattice_corner's loop body): legs `leg` (towards the edge line
@@ -280,12 +285,12 @@ KIWI_LAT T point_pyramid(const LatticeWall<T>& w, bool inner, T b1, T b2, T a, T
 }
 
 // One wall's corner value inside 2h (lattice_corner) from the point's shared quantities: wall distance r0
-// and its reciprocal, in-plane legs a1 (edge tier D2a) and a2 (D2b) with reciprocals, s2 = a1^2 + a2^2,
-// r and its reciprocal, the log terms of u = a2 / r (first pyramid) and u = a1 / r (second), their
-// 1 / (1 - u^2), and r0 r / (a1 a2).
-template <class T>
-KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T ia2, T s2,
-                                               T ir, T log_a2, T iom_a2, T log_a1, T iom_a1, T r0r_a1a2, T D2a, T D2b) {
+// and its reciprocal, in-plane legs a1 (edge tier E.D2(ea)) and a2 (E.D2(eb)) with reciprocals,
+// s2 = a1^2 + a2^2, r and its reciprocal, the log terms of u = a2 / r (first pyramid) and u = a1 / r
+// (second), their 1 / (1 - u^2), and r0 r / (a1 a2).
+template <class T, class Edges>
+KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T ia2, T s2, T ir, T log_a2, T iom_a2,
+                      T log_a1, T iom_a1, T r0r_a1a2, const Edges& E, int ea, int eb) {
     const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
     T pa, pb;
     if (a2 <= a1) {
@@ -297,31 +302,33 @@ KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T i
     }
     const T b1 = inner ? wall_b1_in(w) : 0.0;
     const T b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
-    T sum = point_pyramid(w, inner, b1, b2, a1 * ir0, a2 * ir, a2 * ia1, s2 * ia1 * ia1, iom_a2, log_a2, pa, D2a);
-    sum += point_pyramid(w, inner, b1, b2, a2 * ir0, a1 * ir, a1 * ia2, s2 * ia2 * ia2, iom_a1, log_a1, pb, D2b);
+    T sum = point_pyramid(w, inner, b1, b2, a1 * ir0, a2 * ir, a2 * ia1, s2 * ia1 * ia1, iom_a2, log_a2, pa,
+                          inner ? T(0.0) : E.D2(ea));
+    sum += point_pyramid(w, inner, b1, b2, a2 * ir0, a1 * ir, a1 * ia2, s2 * ia2 * ia2, iom_a1, log_a1, pb,
+                         inner ? T(0.0) : E.D2(eb));
     const T I1s = atan(r0r_a1a2);
     const T c1 = inner ? 1. / 40. * w.r0h3 : 0.25 * (-w.r0h - 1. / 30. * w.r0h3 + 1. / 15. * w.r0h_3);
     return w.r0h3 * (1.0 / kPi) * (sum + c1 * I1s);
 }
 
 // One wall's corner value beyond 2h (lattice_corner's first branch): x = r0 / h, the arctangent argument
-// q = r0 r / (a1 a2), and its inverse qi.
-template <class T>
-KIWI_LAT T point_wall_far(T h, T ih, T r0, T q, T qi, T D3a, T D3b) {
+// q = r0 r / (a1 a2), its inverse qi, and the edge tiers E.D3(ea), E.D3(eb) of the wall's two edge lines.
+template <class T, class Edges>
+KIWI_LAT T point_wall_far(T h, T ih, T r0, T q, T qi, const Edges& E, int ea, int eb) {
     const T x = r0 * ih, x2 = x * x, x3 = x2 * x;
     const T K = x3 * (1.0 / kPi);
-    if (r0 >= 2.0 * h) return 0.25 / kPi * atan(qi) + K * (D3a + D3b);
+    if (r0 >= 2.0 * h) return 0.25 / kPi * atan(qi) + K * (E.D3(ea) + E.D3(eb));
     const T x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
     const T p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
                        : -2. / 3. * x3 + 0.3 * x5 - 0.1 * x6 + 7. / 5. * x;
-    return -0.25 / kPi * atan(q) + 0.125 * p + K * (D3a + D3b);
+    return -0.25 / kPi * atan(q) + 0.125 * p + K * (E.D3(ea) + E.D3(eb));
 }
 
 // The sum of the three corner values of a lattice point at absolute offsets ax, ay, az > 0 from the
 // particle (unsigned; the octant value is sgn(ux) sgn(uy) sgn(uz) times it).  Equal to
 // lattice_corner(ax; ay, az) + lattice_corner(ay; ax, az) + lattice_corner(az; ax, ay) up to rounding.
-template <class T>
-KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const PointEdges<T>& E) {
+template <class T, class Edges>
+KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const Edges& E) {
     const T ax2 = ax * ax, ay2 = ay * ay, az2 = az * az;
     const T sxy = ax2 + ay2, sxz = ax2 + az2, syz = ay2 + az2;
     const T r2 = sxy + az2;
@@ -332,8 +339,9 @@ KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const PointEdges<T>
     const T qx = ax2 * r2 * iP, qy = ay2 * r2 * iP, qz = az2 * r2 * iP;
     if (!(r2 < 4.0 * (h * h))) {
         const T qxi = ay2 * az2 * iP, qyi = ax2 * az2 * iP, qzi = ax2 * ay2 * iP;
-        return point_wall_far(h, ih, ax, qx, qxi, E.xy3, E.xz3) + point_wall_far(h, ih, ay, qy, qyi, E.yx3, E.yz3) +
-               point_wall_far(h, ih, az, qz, qzi, E.zx3, E.zy3);
+        return point_wall_far(h, ih, ax, qx, qxi, E, kEdgeXY, kEdgeXZ) +
+               point_wall_far(h, ih, ay, qy, qyi, E, kEdgeYX, kEdgeYZ) +
+               point_wall_far(h, ih, az, qz, qzi, E, kEdgeZX, kEdgeZY);
     }
     const T ir = axyz * iP;
     const T iax = r * (ay * az) * iP, iay = r * (ax * az) * iP, iaz = r * (ax * ay) * iP;
@@ -345,9 +353,9 @@ KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const PointEdges<T>
     const T Ly = log1p(2.0 * uy * (1.0 + uy) * iomy);
     const T Lz = log1p(2.0 * uz * (1.0 + uz) * iomz);
     const bool inner = r2 < h * h;
-    T s = point_wall(h, ih, inner, ax, iax, ay, iay, az, iaz, syz, ir, Lz, iomz, Ly, iomy, qx, E.xy2, E.xz2);
-    s += point_wall(h, ih, inner, ay, iay, ax, iax, az, iaz, sxz, ir, Lz, iomz, Lx, iomx, qy, E.yx2, E.yz2);
-    s += point_wall(h, ih, inner, az, iaz, ax, iax, ay, iay, sxy, ir, Ly, iomy, Lx, iomx, qz, E.zx2, E.zy2);
+    T s = point_wall(h, ih, inner, ax, iax, ay, iay, az, iaz, syz, ir, Lz, iomz, Ly, iomy, qx, E, kEdgeXY, kEdgeXZ);
+    s += point_wall(h, ih, inner, ay, iay, ax, iax, az, iaz, sxz, ir, Lz, iomz, Lx, iomx, qy, E, kEdgeYX, kEdgeYZ);
+    s += point_wall(h, ih, inner, az, iaz, ax, iax, ay, iay, sxy, ir, Ly, iomy, Lx, iomx, qz, E, kEdgeZX, kEdgeZY);
     return s;
 }
 

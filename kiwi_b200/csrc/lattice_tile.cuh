@@ -33,6 +33,16 @@ constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap2 + kLatPtCap);
 constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatPtCap);
 constexpr size_t kLatTabDynSmem = sizeof(double) * kLatPtCap;
 
+// The six edge tiers of a lattice point (slots of the chunk's D2 / D3 tables in PointEdge order), read where
+// lattice_point uses them.
+struct SmemPointEdges {
+    const double* d2;
+    const double* d3;
+    int slot[6];
+    __device__ __forceinline__ double D2(int e) const { return d2[slot[e]]; }
+    __device__ __forceinline__ double D3(int e) const { return d3[slot[e]]; }
+};
+
 __device__ __forceinline__ void lat_add_stat(unsigned long long* dst, unsigned long long v) {
     // warp-aggregate, then one atomic per warp
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -340,8 +350,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                             lattice_generic_corner(K, H, ay, ax, az, s_E + kLatGenERec * eyx, s_E + kLatGenERec * eyz) +
                             lattice_generic_corner(K, H, az, ax, ay, s_E + kLatGenERec * ezx, s_E + kLatGenERec * ezy);
                     } else {
-                        const PointEdges<double> E{s_D2[exy], s_D3[exy], s_D2[exz], s_D3[exz], s_D2[eyx], s_D3[eyx],
-                                                   s_D2[eyz], s_D3[eyz], s_D2[ezx], s_D3[ezx], s_D2[ezy], s_D3[ezy]};
+                        const SmemPointEdges E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};
                         f = lattice_point(s_h[jp], s_ih[jp], ax, ay, az, E);
                     }
                 }

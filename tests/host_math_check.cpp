@@ -75,7 +75,11 @@ double hm_lattice_corner(double h, double r0, double a1, double a2, const double
 
 // edges: D2, D3 of xy, xz, yx, yz, zx, zy
 double hm_lattice_point(double h, double ax, double ay, double az, const double* e) {
-    PointEdges<double> E{e[0], e[1], e[2], e[3], e[4], e[5], e[6], e[7], e[8], e[9], e[10], e[11]};
+    PointEdges<double> E;
+    for (int k = 0; k < 6; ++k) {
+        E.d2[k] = e[2 * k];
+        E.d3[k] = e[2 * k + 1];
+    }
     return lattice_point(h, 1.0 / h, ax, ay, az, E);
 }
 }

@@ -28,34 +28,13 @@ import os
 import numpy as np
 import pytest
 
-from gpu_checks import BANDS
+from oracle.compare import band_stats
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 # 4x the reference's own error against the exact integral on the column workload, per band
 # (tests/golden/column_envelope.py: 5.7e-9, 5.5e-6, 4.9e-4, 1.1e-9)
 ENVELOPE = (2.3e-8, 2.2e-5, 2.0e-3, 4.4e-9)
-
-
-def band_stats(x, ref):
-    """Per band of the reference's density: cells, fraction within 1e-12 relative, median and max relative
-    difference (the last band: cells at or below 1e-6 of the peak, differences relative to the peak)."""
-    x, ref = np.asarray(x), np.asarray(ref)
-    peak = float(np.abs(ref).max())
-    out = []
-    for lo, hi in BANDS:
-        m = (np.abs(ref) > lo * peak) & (np.abs(ref) <= hi * peak)
-        rel = np.abs(x[m] - ref[m]) / np.abs(ref[m])
-        out.append({"band": f">{lo:g} of peak" if hi == np.inf else f"{lo:g}..{hi:g} of peak", "cells": int(m.sum()),
-                    "frac_le_1e-12": float(np.mean(rel <= 1e-12)) if m.any() else None,
-                    "median": float(np.median(rel)) if m.any() else None,
-                    "max": float(rel.max()) if m.any() else None})
-    low = np.abs(ref) <= BANDS[-1][0] * peak
-    rel = np.abs(x[low] - ref[low]) / peak
-    out.append({"band": f"<={BANDS[-1][0]:g} of peak (abs/peak)", "cells": int(low.sum()),
-                "frac_le_1e-12": float(np.mean(rel <= 1e-12)) if low.any() else None,
-                "median": float(np.median(rel)) if low.any() else None, "max": float(rel.max()) if low.any() else None})
-    return out
 
 
 def _workload(case):
