@@ -89,7 +89,7 @@ def parse():
     ap.add_argument("--multi", default="tiles", choices=["tiles", "replicas"],
                     help="with N > 1 GPUs: split one grid by cell tiles (strong scaling) or map one snapshot per "
                          "rank (weak scaling)")
-    ap.add_argument("--fd-particles", type=int, default=40, help="adjoint workload: particles checked by FD")
+    ap.add_argument("--fd-particles", type=int, default=200, help="adjoint workload: particles checked by FD")
     ap.add_argument("--adj-n", type=int, default=500_000, help="adjoint workload: particles")
     ap.add_argument("--adj-res", type=int, default=128, help="adjoint workload: grid cells per axis")
     ap.add_argument("--vor-n", type=int, default=200_000, help="voronoi workload: particles")
@@ -674,6 +674,7 @@ def run_batch(args):
         t_single += st["total_ms"]
         single_pairs += st["sphere_pairs"]
     batch.close()
+    errors = batch_item_errors(items, args) if not args.no_cpu_baseline else None
     tot_ms = float(np.sum(ms))
     line = {
         "metric": "particle-cell integrals/s (support pairs), batched sph-to-grid", "value": pairs / (tot_ms * 1e-3),
@@ -693,8 +694,65 @@ def run_batch(args):
                       "note": "the same items as one kiwi_sph_to_grid_device call each, binning included"},
         "fp64_peak_tflops": peak_fp64, "clocks": clk, "gpu_launches": int(per[0]["launches"]) if per else 0,
     }
+    if errors is not None:
+        line["per_snapshot_error"] = errors
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batch_item_errors(items, args, pair_cap=200_000):
+    """Per snapshot of the batch: a seeded subset of its particles (random order, taken while the subset's
+    bounding-box pairs stay under pair_cap) mapped on the snapshot's own grid by the GPU (one call, FP64 and,
+    for the cubic spline, FP32-mixed) and by the CPU oracle (the C restatement of the reference, bit-identical
+    to it); per density band of the oracle's grid, the largest relative difference.  The batch's own outputs
+    equal one call per item bit for bit (tests/test_gpu_batch.py), so this is the batch's error."""
+    import kiwi_b200
+    from oracle.compare import band_stats
+    from oracle.oracle import Oracle
+
+    orc = Oracle()
+    ctx = kiwi_b200.Context(0)
+    rng = np.random.default_rng(77)
+    out, worst64, worst32 = [], [0.0] * 4, [0.0] * 4
+    for it in items:
+        P = {k: v.cpu().numpy() for k, v in it["particles"].items()}
+        b, shape = it["bounds"], it["shape"]
+        d = [(b[2 * a + 1] - b[2 * a]) / shape[a] for a in range(3)]
+        kidx = it["kernel"].kernel
+        spec = kiwi_b200.KernelSpec(kidx)
+        sup = it["kernel"].support_in_h or spec.radkern
+        box = np.ones(len(P["x"]))
+        for a, k in enumerate("xyz"):
+            lo = np.clip(np.floor((P[k] - sup * P["h"] - b[2 * a]) / d[a]), 0, shape[a] - 1)
+            hi = np.clip(np.floor((P[k] + sup * P["h"] - b[2 * a]) / d[a]), 0, shape[a] - 1)
+            box *= np.maximum(hi - lo + 1, 0)
+        take, tot = [], 0.0
+        for i in rng.permutation(len(box)):
+            if tot + box[i] > pair_cap:
+                continue
+            take.append(i)
+            tot += box[i]
+            if len(take) >= 64:
+                break
+        sub = {k: np.ascontiguousarray(v[np.sort(take)]) for k, v in P.items()}
+        cubic = kidx == 0 and sup == 2.0
+        dens = orc.sph_to_grid(sub, b, shape, kernel=-1 if cubic else kidx, support_in_h=sup)[0]
+        rec = {"kernel": spec.key, "grid": shape[0], "particles": len(P["x"]), "subset": len(take),
+               "subset_bbox_pairs": int(tot)}
+        for prec, worst in (("fp64", worst64), ("fp32_mixed", worst32)):
+            if prec == "fp32_mixed" and not cubic:
+                continue
+            g = kiwi_b200.sph_to_grid(sub, b, shape, kernel=it["kernel"], precision=prec, ctx=ctx).density
+            st = band_stats(g, dens)
+            rec[prec] = [s["max"] for s in st]
+            for k in range(4):
+                if st[k]["max"] is not None:
+                    worst[k] = max(worst[k], st[k]["max"])
+        out.append(rec)
+    return {"against": "the CPU oracle (the reference's algorithm restated, bit-identical to it) on a seeded "
+                       "particle subset of each snapshot, the snapshot's grid and kernel",
+            "bands": [">1e-2 of peak", "1e-4..1e-2", "1e-6..1e-4", "<=1e-6 (abs/peak)"],
+            "max_over_snapshots_fp64": worst64, "max_over_snapshots_fp32_mixed_cubic": worst32, "items": out}
 
 
 def main():

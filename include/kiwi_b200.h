@@ -328,6 +328,15 @@ int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t
                      const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
                      double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
 
+/* kiwi_map_voronoi with every array in device memory -- particles, home cells, the cell geometry and the
+ * outputs -- on the context's stream (returns when done): a caller that maps several snapshots, or several
+ * quantities, on one tessellation copies its geometry to the GPU once.  The geometry's offsets and
+ * neighbour indices are not checked here (kiwi_map_voronoi checks them on the host); they must satisfy the
+ * same rules: face_off and vert_off start at 0 and do not decrease, face_nbr < n_cells, home_cell < n_cells. */
+int kiwi_map_voronoi_device(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                            const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
+                            double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
+
 /* The inverse-mapping check (run_inverse_mapping_test_stage's particle loop, src/mapping.cpp:540-701): the
  * same cell walk and cell integrals as kiwi_map_voronoi, summed per particle instead of per cell, in the
  * walk's order: m_recovered[i] = sum over the cells i reaches of (integral m_i' / M_c) M_c over cells with

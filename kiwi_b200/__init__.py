@@ -653,6 +653,34 @@ def map_voronoi(particles: dict, home_cell, cells: dict, kernel=None, precision=
     return MappingResult(*outs, raw=rawa.reshape(4, nc) if raw else None, stats=d)
 
 
+def map_voronoi_device(particles: dict, home_cell, cells: dict, out: dict, kernel=None, precision="fp64",
+                       ctx=None):
+    """Device variant of map_voronoi: `particles` (x y z vx vy vz m h), `home_cell` (int32), `cells`
+    (face_off, vert_off int64; vxyz, volume float64; face_nbr int32) and `out` (density, vx, vy, vz[, raw4])
+    are contiguous CUDA tensors, so that one tessellation staged on the GPU serves many calls.  Runs on the
+    context's stream and returns the call's stats."""
+    ctx = ctx or default_context()
+    ki = kernel or KernelIntegrator()
+    Ps, _ = _particles_struct(particles, device=True)
+
+    def ptr(t, typ):
+        return C.cast(C.c_void_p(int(t.data_ptr())), typ) if t is not None else None
+
+    nc = int(cells["volume"].numel())
+    cs = KiwiVoronoiCells(nc, ptr(cells["face_off"], _i64p), ptr(cells["vert_off"], _i64p), ptr(cells["vxyz"], _dp),
+                          ptr(cells["face_nbr"], _i32p), ptr(cells["volume"], _dp))
+    st = KiwiStats()
+    sel = ki.sel()
+    outs = [ptr(out.get(k), _dp) for k in ("density", "vx", "vy", "vz", "raw4")]
+    ctx.check(ctx._L.kiwi_map_voronoi_device(ctx.handle, C.byref(Ps), ptr(home_cell, _i32p), C.byref(cs), C.byref(sel),
+                                             precision_code(precision), *outs, C.byref(st)), "map (device)")
+    d = st.as_dict()
+    d["unresolved"] = d["skipped_outside"]
+    d["unmapped"] = d["tile_pairs"]
+    d["visited_pairs"] = d["evaluated_pairs"]
+    return d
+
+
 @dataclass
 class InverseMappingResult:
     """run_inverse_mapping_test_stage's results (include/kiwi/mapping.hpp:88-106): per particle, in snapshot

@@ -702,6 +702,37 @@ int kiwi_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t
                             nullptr);
 }
 
+int kiwi_map_voronoi_device(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                            const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
+                            double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats) {
+    KIWI_TRY(check_ctx(ctx));
+    int rc = KIWI_OK;
+    if (!particles_ok(ctx, particles, &rc)) return rc;
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    if ((precision & KIWI_FORM_MASK) != KIWI_FP64 && (precision & KIWI_FORM_MASK) != KIWI_FP64_REFERENCE_ORDER)
+        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "the Voronoi map is available in the FP64 form only");
+    if (kc.tabulated) KIWI_TRY(table_ensure(ctx, &kc.tab));
+    if (!cells || cells->n_cells < 0 || (cells->n_cells > 0 && (!cells->face_off || !cells->vert_off ||
+                                                                 !cells->vxyz || !cells->face_nbr || !cells->volume)))
+        return set_err(ctx, KIWI_ERR_ARG, "cell geometry is incomplete");
+    if (particles->n > 0 && !home_cell) return set_err(ctx, KIWI_ERR_ARG, "home_cell is null");
+    if (cells->n_cells >= (1LL << 31)) return set_err(ctx, KIWI_ERR_ARG, "too many cells");
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[2], ctx->stream));
+    DevParticles P{particles->n, particles->x, particles->y, particles->z, particles->vx,
+                   particles->vy, particles->vz, particles->m, particles->h};
+    CartOutputs out{density, vx, vy, vz, raw4, nullptr};
+    KIWI_TRY(voronoi_map_dev(ctx, P, home_cell, *cells, kc, out, stats));
+    KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
+    KIWI_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        stats->total_ms = ms;
+    }
+    return KIWI_OK;
+}
+
 int kiwi_inverse_map_voronoi(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
                              const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision,
                              const double* cell_mass, double* m_recovered, double* coverage, double* totals3,
