@@ -194,7 +194,10 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
             KIWI_TRY(scratch_t(ctx, S_CELL_ERR, (size_t)ncell, &cerr));
             KIWI_TRY(scratch_t(ctx, S_CELL_MASS, (size_t)ncell, &cmass));
         }
-        KIWI_TRY(mixed_cart_gather(ctx, g, P, tl, out, cerr, cmass, d_stats));
+        if (guarantee)
+            KIWI_TRY(mixed_cart_gather(ctx, g, P, tl, out, cerr, cmass, d_stats));
+        else
+            KIWI_TRY(lattice_mixed_gather(ctx, g, P, tl, out, d_stats));
         if (guarantee) {
             int32_t* map = nullptr;
             int64_t* d_nmap = nullptr;

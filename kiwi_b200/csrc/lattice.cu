@@ -25,10 +25,11 @@ int lattice_init_tables(KiwiCtx* ctx) {
 
 namespace {
 
-// Resident CTAs per SM the register budget is sized for: three for the cubic kernel (its shared memory
-// fits three times), two for the generic one (its table-driven series needs the registers).
+// Resident CTAs per SM the register budget is sized for: two for both kernels (128 registers).  The cubic
+// kernel's shared memory would fit three, but at the 80 registers three need, its point-wise tiers spill:
+// 3.59 G support pairs/s at three against 3.84 G at two on the 2 M-particle log-normal cube.
 #ifndef KIWI_LATTICE_MIN_BLOCKS
-#define KIWI_LATTICE_MIN_BLOCKS 3
+#define KIWI_LATTICE_MIN_BLOCKS 2
 #endif
 #ifndef KIWI_LATTICE_GEN_MIN_BLOCKS
 #define KIWI_LATTICE_GEN_MIN_BLOCKS 2
@@ -44,6 +45,19 @@ __global__ void __launch_bounds__(kLatThreads, kLatMinBlocks) k_cart_lattice(Car
                                                                              CartOutputs out, DevStats* __restrict__ st) {
     const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
     lattice_tile<CULL>(g, P, list, range, t, t, out, st);
+}
+
+// The FP32-mixed form of the cubic lattice kernel (support cells only): edge pairs and lattice points
+// evaluated with FP32 tiers (FP64 islands where a plane lies within 1e-3 h of the particle), cell assembly
+// and per-cell sums in FP64.
+__global__ void __launch_bounds__(kLatThreads, kLatMinBlocks) k_cart_lattice_mixed(CartGeom g, DevParticles P,
+                                                                                const uint32_t* __restrict__ list,
+                                                                                const int64_t* __restrict__ range,
+                                                                                const int32_t* __restrict__ tile_map,
+                                                                                CartOutputs out,
+                                                                                DevStats* __restrict__ st) {
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    lattice_tile<true, false, false, true>(g, P, list, range, t, t, out, st);
 }
 
 // The lattice form for the generic kernels (support cells only).
@@ -113,6 +127,20 @@ int lattice_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, 
         k_cart_lattice_generic<<<grid, kLatThreads, kLatGenDynSmem, ctx->stream>>>(g, P, k.kernel, tl.list, tl.range,
                                                                                    tl.map, out, d_stats);
     }
+    KIWI_LAUNCHED(ctx);
+    return KIWI_OK;
+}
+
+int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const TileLists& tl,
+                         const CartOutputs& out, DevStats* d_stats) {
+    if (tl.ntiles <= 0 || (tl.map && tl.nmap <= 0)) return KIWI_OK;
+    const dim3 grid((unsigned)(tl.map ? tl.nmap : tl.ntiles));
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kLatDynSmem));
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_mixed, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared));
+    k_cart_lattice_mixed<<<grid, kLatThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
+                                                                          d_stats);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

@@ -17,6 +17,7 @@
 #include <climits>
 
 #include "engine.hpp"
+#include "f32.cuh"
 #include "lattice.cuh"
 #include "tabulated.cuh"
 
@@ -25,8 +26,16 @@ namespace kiwi_b200 {
 constexpr int kLatThreads = 256;
 constexpr int kLatCellsPerThread = kTileCells / kLatThreads;
 static_assert(kTileCells % kLatThreads == 0, "tile cells must split evenly over the threads");
-constexpr int kLatPtCap = 2304;   // lattice points per chunk (a full 8^3 particle box has 729)
-constexpr int kLatECap2 = 2048;   // cubic edge tiers per chunk (a full 8^3 particle box has 486)
+// Chunk capacities (defaults sized for two CTAs per SM; a full 8^3 particle box has 729 lattice points and
+// 486 edge lines).
+#ifndef KIWI_LAT_PT_CAP
+#define KIWI_LAT_PT_CAP 2304
+#endif
+#ifndef KIWI_LAT_E_CAP
+#define KIWI_LAT_E_CAP 2048
+#endif
+constexpr int kLatPtCap = KIWI_LAT_PT_CAP;  // lattice points per chunk
+constexpr int kLatECap2 = KIWI_LAT_E_CAP;   // cubic edge tiers per chunk
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed point-list entries");
 static_assert(kLatECap2 <= 2048 && kLatGenECap <= 2048, "packed edge-pair entries (11-bit slots)");
 constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap2 + kLatPtCap);
@@ -34,14 +43,19 @@ constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + 
 constexpr size_t kLatTabDynSmem = sizeof(double) * kLatPtCap;
 
 // The six edge tiers of a lattice point (slots of the chunk's D2 / D3 tables in PointEdge order), read where
-// lattice_point uses them.
+// lattice_point uses them, as the real type T it is evaluated in.
+template <class T>
 struct SmemPointEdges {
     const double* d2;
     const double* d3;
     int slot[6];
-    __device__ __forceinline__ double D2(int e) const { return d2[slot[e]]; }
-    __device__ __forceinline__ double D3(int e) const { return d3[slot[e]]; }
+    __device__ __forceinline__ T D2(int e) const { return T(d2[slot[e]]); }
+    __device__ __forceinline__ T D3(int e) const { return T(d3[slot[e]]); }
 };
+
+// FP32-mixed form: planes closer to the particle than this fraction of h are evaluated in FP64 (the wall
+// tier's (h/r0)^3 and the edge ratio R_0/r0 grow without bound as r0 -> 0).
+constexpr double kMixedIslandFrac = 1e-3;
 
 __device__ __forceinline__ void lat_add_stat(unsigned long long* dst, unsigned long long v) {
     // warp-aggregate, then one atomic per warp
@@ -58,7 +72,7 @@ __device__ __forceinline__ void lat_add_stat(unsigned long long* dst, unsigned l
 // GENERIC: the table-driven tiers of kernel K (support radius support_in_h x h) instead of the cubic closed
 // form; edge tiers are lattice_generic_edge records.  TAB: the tabulated cubic integral (lookups in `tab`):
 // no edge tiers, and the points run in their natural order.  List order never affects the results.
-template <bool CULL, bool GENERIC = false, bool TAB = false>
+template <bool CULL, bool GENERIC = false, bool TAB = false, bool MIXED = false>
 __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticles& P,
                                              const uint32_t* __restrict__ list, const int64_t* __restrict__ range,
                                              int64_t t_range, int64_t t, const CartOutputs& out,
@@ -101,7 +115,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     // work counters: 32-bit per thread (a chunk adds at most a few hundred to any of them), flushed to the
     // 64-bit totals every 2^16 chunks and at the end
     unsigned n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
-    unsigned n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0, n_clamp = 0, n_chunks = 0;
+    unsigned n_eo = 0, n_em = 0, n_ei = 0, n_vp = 0, n_clamp = 0, n_chunks = 0, n_island = 0;
     auto flush = [&]() {
         lat_add_stat(&st->bbox_pairs, n_bbox);
         lat_add_stat(&st->sphere_pairs, n_sphere);
@@ -113,7 +127,8 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         lat_add_stat(&st->edge_inner, n_ei);
         lat_add_stat(&st->vertex_pyramids, n_vp);
         if (TAB) lat_add_stat(&st->table_clamps, n_clamp);
-        n_bbox = n_sphere = n_eval = n_neg = n_warn = n_eo = n_em = n_ei = n_vp = n_clamp = 0;
+        if (MIXED) lat_add_stat(&st->fp64_fallback, n_island);
+        n_bbox = n_sphere = n_eval = n_neg = n_warn = n_eo = n_em = n_ei = n_vp = n_clamp = n_island = 0;
     };
     const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
     const double sup_in_h = g.support_in_h;
@@ -294,7 +309,15 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 const uint32_t rec = s_hlist[li];
                 const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)(rec >> 22);
                 LatticeEdge e_pq, e_qp;
-                lattice_edge_pair(s_h[j], s_ih[j], s_D2[sab], s_D3[sab], e_pq, e_qp);
+                const double vp = s_D2[sab], vq = s_D3[sab];
+                if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * s_h[j]) {
+                    LatticeEdgeT<F32> f_pq, f_qp;
+                    lattice_edge_pair(F32(s_h[j]), F32(s_ih[j]), F32(vp), F32(vq), f_pq, f_qp);
+                    e_pq = {(double)f_pq.D2.v, (double)f_pq.D3.v};
+                    e_qp = {(double)f_qp.D2.v, (double)f_qp.D3.v};
+                } else {
+                    lattice_edge_pair(s_h[j], s_ih[j], vp, vq, e_pq, e_qp);
+                }
                 s_D2[sab] = e_pq.D2;
                 s_D3[sab] = e_pq.D3;
                 s_D2[sba] = e_qp.D2;
@@ -350,8 +373,14 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                             lattice_generic_corner(K, H, ay, ax, az, s_E + kLatGenERec * eyx, s_E + kLatGenERec * eyz) +
                             lattice_generic_corner(K, H, az, ax, ay, s_E + kLatGenERec * ezx, s_E + kLatGenERec * ezy);
                     } else {
-                        const SmemPointEdges E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};
-                        f = lattice_point(s_h[jp], s_ih[jp], ax, ay, az, E);
+                        if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * s_h[jp]) {
+                            const SmemPointEdges<F32> E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};
+                            f = (double)lattice_point(F32(s_h[jp]), F32(s_ih[jp]), F32(ax), F32(ay), F32(az), E).v;
+                        } else {
+                            const SmemPointEdges<double> E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};
+                            f = lattice_point(s_h[jp], s_ih[jp], ax, ay, az, E);
+                            if (MIXED) ++n_island;
+                        }
                     }
                 }
                 n_vp += 6;
