@@ -267,8 +267,8 @@ def cpu_baseline_c1(kiwi_b200, ctx):
     reference's own run_sph_to_grid_stage (oracle/_ref) on all host cores -- its stage wall time is the CPU
     baseline of this configuration, and its grid is the checker of the GPU's, cell by cell per density band
     (parity_c1)."""
-    from oracle.compare import band_stats
-    from oracle.oracle import load_ref
+    from oracle.compare import band_stats, exact_check
+    from oracle.oracle import load_ref, load_truth
 
     ref = load_ref()
     if ref is None:
@@ -287,6 +287,7 @@ def cpu_baseline_c1(kiwi_b200, ctx):
     sig = rd[0] > 1e-6 * rd[0].max()
     dv = max(float(np.max(np.abs(getattr(r, k)[sig] - v[sig]))) for k, v in zip(("vx", "vy", "vz"), rd[1:]))
     pairs, bbox = r.stats["sphere_pairs"], r.stats["bbox_pairs"]
+    exact = exact_check(P, b, shape, (r.density, r.vx, r.vy, r.vz), rd, load_truth())
     return {"workload": "column n=7300 (60% uniform + 40% filament, h from 57-NN), grid 100x100x410 of 0.02 pc",
             "support_pairs": int(pairs), "bbox_pairs": int(bbox),
             "gpu_e2e_s": gpu_s, "gpu_e2e_pairs_per_s": pairs / gpu_s,
@@ -294,7 +295,10 @@ def cpu_baseline_c1(kiwi_b200, ctx):
             "against": "the reference's run_sph_to_grid_stage (oracle/_ref) on the same particles, every cell",
             "density_bands": band_stats(r.density, rd[0]),
             "max_abs_velocity_diff_above_1e-6_peak_km_s": dv,
-            "total_mass_rel_diff": float(abs(r.density.sum() - rd[0].sum()) / rd[0].sum())}
+            "total_mass_rel_diff": float(abs(r.density.sum() - rd[0].sum()) / rd[0].sum()),
+            "vs_exact": {"how": "__float128 evaluation of the reference's algorithm, each cell alone over the "
+                                "particles covering it; relative density error of the GPU and of the reference",
+                         **exact}}
 
 
 def run_reference(args):
