@@ -269,8 +269,10 @@ int kiwi_batch_create(KiwiCtx* ctx, const KiwiBatchItem* items, int n_items, int
 /* Replays the graph on the context's stream and waits for it.  item_stats (n_items entries) and total
  * may be NULL; gather_ms / total_ms hold the device time of the whole batch. */
 int kiwi_batch_run(KiwiBatch* batch, KiwiStats* item_stats, KiwiStats* total);
-/* Times the launch shapes (longest-first or natural tile order x 1 or 2 resident CTAs per SM; one run
- * each) and keeps the fastest; *chosen = 0x100 if longest-first, | CTAs per SM. */
+/* Times the launch shapes (the two lattice families -- cubic and table-driven kernels -- in one persistent
+ * launch or one each, when the batch holds both x longest-first or natural tile order x 1 or 2 resident
+ * CTAs per SM; one run each) and keeps the fastest; *chosen = 0x10000 if merged | 0x100 if longest-first
+ * | CTAs per SM. */
 int kiwi_batch_tune(KiwiBatch* batch, int* chosen);
 void kiwi_batch_destroy(KiwiBatch* batch);
 

@@ -535,9 +535,11 @@ class Batch:
         return [s.as_dict() for s in st], tot.as_dict()
 
     def tune(self):
-        """Times the launch shapes and keeps the fastest; returns (longest_first, ctas_per_sm)."""
+        """Times the launch shapes and keeps the fastest; returns (longest_first, ctas_per_sm) and sets
+        self.merged (both lattice families in one persistent launch)."""
         c = C.c_int(0)
         self.ctx.check(self.ctx._L.kiwi_batch_tune(self._h, C.byref(c)), "batch tune")
+        self.merged = bool(c.value & 0x10000)
         return bool(c.value & 0x100), c.value & 0xff
 
     def close(self):

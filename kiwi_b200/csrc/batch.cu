@@ -36,6 +36,11 @@ struct KiwiBatch {
     int32_t* d_natural[kBatchFamilies] = {};
     int32_t* d_lpt[kBatchFamilies] = {};
     int64_t fam_tiles[kBatchFamilies] = {};
+    // both lattice families' tiles together (natural order and longest-first), for the merged launch
+    int32_t* d_natural_m = nullptr;
+    int32_t* d_lpt_m = nullptr;
+    int64_t merged_tiles = 0;
+    bool merge = false;
     const uint32_t* d_list = nullptr;
     int64_t* d_range = nullptr;
     unsigned long long* d_next = nullptr;  // kBatchFamilies counters
@@ -102,9 +107,17 @@ int batch_enqueue(KiwiBatch* b) {
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long) * kBatchFamilies, ctx->stream));
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_stats, 0, sizeof(DevStats) * b->n_items, ctx->stream));
     for (int i = 0; i < b->n_items; ++i) KIWI_TRY(fp64_mean_velocity(ctx, b->items[i].P, b->d_meanv + 4 * i));
-    for (int f = 0; f < kBatchFamilies; ++f)
+    for (int f = 0; f < kBatchFamilies; ++f) {
+        if (b->merge && f == kBatchFamilyLatticeGeneric) continue;
+        if (b->merge && f == kBatchFamilyLattice) {
+            KIWI_TRY(fp64_batch_gather(ctx, kBatchFamilyLatticeMerged, b->d_items, b->d_item_of_tile,
+                                       b->lpt ? b->d_lpt_m : b->d_natural_m, b->merged_tiles, b->d_list, b->d_range,
+                                       b->d_next + f, b->sms * b->ctas_per_sm));
+            continue;
+        }
         KIWI_TRY(fp64_batch_gather(ctx, f, b->d_items, b->d_item_of_tile, b->lpt ? b->d_lpt[f] : b->d_natural[f],
                                    b->fam_tiles[f], b->d_list, b->d_range, b->d_next + f, b->sms * b->ctas_per_sm));
+    }
     return KIWI_OK;
 }
 
@@ -182,6 +195,16 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
             KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_natural[f], nat[f].data(), sizeof(int32_t) * nat[f].size(),
                                            cudaMemcpyHostToDevice, ctx->stream));
     }
+    std::vector<int32_t> nat_m;  // both lattice families, in item order
+    for (int i = 0; i < n; ++i)
+        if (batch_family(b->items[i].mode) != kBatchFamilyGather)
+            for (int64_t t = b->tile_base[i]; t < b->tile_base[i + 1]; ++t) nat_m.push_back((int32_t)t);
+    b->merged_tiles = (int64_t)nat_m.size();
+    KIWI_TRY(balloc(b, nat_m.size(), &b->d_natural_m));
+    KIWI_TRY(balloc(b, nat_m.size(), &b->d_lpt_m));
+    if (!nat_m.empty())
+        KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_natural_m, nat_m.data(), sizeof(int32_t) * nat_m.size(),
+                                       cudaMemcpyHostToDevice, ctx->stream));
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_stats, 0, sizeof(DevStats) * n, ctx->stream));
     for (int i = 0; i < n; ++i) {
         b->items[i].st = b->d_stats + i;
@@ -266,14 +289,16 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
         k_fill_i32<<<(unsigned)((nt + 255) / 256), 256, 0, ctx->stream>>>(b->d_item_of_tile + b->tile_base[i], nt, i);
         KIWI_LAUNCHED(ctx);
     }
-    for (int f = 0; f < kBatchFamilies; ++f) {
-        const int64_t nf = b->fam_tiles[f];
+    for (int f = 0; f <= kBatchFamilies; ++f) {
+        const int64_t nf = f < kBatchFamilies ? b->fam_tiles[f] : b->merged_tiles;
         if (nf <= 0) continue;
-        k_tile_weights<<<(unsigned)((nf + 255) / 256), 256, 0, ctx->stream>>>(b->d_range, b->d_natural[f], nf, k0, v0);
+        const int32_t* nat_f = f < kBatchFamilies ? b->d_natural[f] : b->d_natural_m;
+        int32_t* lpt_f = f < kBatchFamilies ? b->d_lpt[f] : b->d_lpt_m;
+        k_tile_weights<<<(unsigned)((nf + 255) / 256), 256, 0, ctx->stream>>>(b->d_range, nat_f, nf, k0, v0);
         KIWI_LAUNCHED(ctx);
         bool second = false;
         KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, nf, 32, &second));
-        KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_lpt[f], second ? v1 : v0, sizeof(int32_t) * nf, cudaMemcpyDeviceToDevice,
+        KIWI_CUDA(ctx, cudaMemcpyAsync(lpt_f, second ? v1 : v0, sizeof(int32_t) * nf, cudaMemcpyDeviceToDevice,
                                        ctx->stream));
     }
     KIWI_CUDA(ctx, cudaMemcpyAsync(b->d_items, b->items.data(), sizeof(BatchItemDev) * n, cudaMemcpyHostToDevice,
@@ -383,26 +408,32 @@ int kiwi_batch_tune(KiwiBatch* b, int* chosen) {
     KiwiCtx* ctx = b->ctx;
     KIWI_CUDA(ctx, cudaSetDevice(ctx->device));
     float best = 1e30f;
-    bool best_lpt = b->lpt;
+    bool best_lpt = b->lpt, best_merge = b->merge;
     int best_ctas = b->ctas_per_sm;
-    for (int lpt = 1; lpt >= 0; --lpt) {
-        for (int ctas = 1; ctas <= 2; ++ctas) {
-            b->lpt = lpt != 0;
-            b->ctas_per_sm = ctas;
-            KIWI_TRY(batch_record(b));
-            float ms = 0.f;
-            KIWI_TRY(batch_time_once(b, &ms));
-            if (ms < best) {
-                best = ms;
-                best_lpt = b->lpt;
-                best_ctas = ctas;
+    const bool both = b->fam_tiles[kBatchFamilyLattice] > 0 && b->fam_tiles[kBatchFamilyLatticeGeneric] > 0;
+    for (int merge = both ? 1 : 0; merge >= 0; --merge) {
+        for (int lpt = 1; lpt >= 0; --lpt) {
+            for (int ctas = 1; ctas <= 2; ++ctas) {
+                b->merge = merge != 0;
+                b->lpt = lpt != 0;
+                b->ctas_per_sm = ctas;
+                KIWI_TRY(batch_record(b));
+                float ms = 0.f;
+                KIWI_TRY(batch_time_once(b, &ms));
+                if (ms < best) {
+                    best = ms;
+                    best_lpt = b->lpt;
+                    best_ctas = ctas;
+                    best_merge = b->merge;
+                }
             }
         }
     }
     b->lpt = best_lpt;
     b->ctas_per_sm = best_ctas;
+    b->merge = best_merge;
     KIWI_TRY(batch_record(b));
-    if (chosen) *chosen = (best_lpt ? 0x100 : 0) | best_ctas;
+    if (chosen) *chosen = (best_merge ? 0x10000 : 0) | (best_lpt ? 0x100 : 0) | best_ctas;
     return KIWI_OK;
 }
 

@@ -68,6 +68,9 @@ int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, con
 enum BatchMode { kBatchLattice = 0, kBatchGatherCubic = 1, kBatchGatherGeneric = 2, kBatchLatticeGeneric = 3 };
 // tile-body families, one persistent launch each
 enum BatchFamily { kBatchFamilyLattice = 0, kBatchFamilyLatticeGeneric = 1, kBatchFamilyGather = 2, kBatchFamilies = 3 };
+// launch-only family: the tiles of both lattice families in one persistent launch, each tile taking its
+// item's body
+constexpr int kBatchFamilyLatticeMerged = 3;
 inline int batch_family(int mode) {
     return mode == kBatchLattice ? kBatchFamilyLattice
                                  : (mode == kBatchLatticeGeneric ? kBatchFamilyLatticeGeneric : kBatchFamilyGather);

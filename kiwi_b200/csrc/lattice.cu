@@ -36,6 +36,7 @@ namespace {
 #endif
 constexpr int kLatMinBlocks = KIWI_LATTICE_MIN_BLOCKS;
 constexpr int kLatGenMinBlocks = KIWI_LATTICE_GEN_MIN_BLOCKS;
+constexpr size_t kLatMergedDynSmem = kLatDynSmem > kLatGenDynSmem ? kLatDynSmem : kLatGenDynSmem;
 
 template <bool CULL>
 __global__ void __launch_bounds__(kLatThreads, kLatMinBlocks) k_cart_lattice(CartGeom g, DevParticles P,
@@ -72,10 +73,10 @@ __global__ void __launch_bounds__(kLatThreads, kLatGenMinBlocks) k_cart_lattice_
     lattice_tile<true, true>(g, P, list, range, t, t, out, st, &c_tables[kernel]);
 }
 
-// The tiles of a batch of grids, one persistent launch per lattice family: each CTA takes the next of the
-// family's tiles (order[w]) from the work counter and runs the same tile body as the single-grid kernel, so
-// every cell's value and summation order are those of a single-grid call.  One instance per family keeps
-// each body's register budget.
+// The tiles of a batch of grids, one persistent launch per lattice family, or one for both
+// (kBatchFamilyLatticeMerged: each tile takes its item's body): each CTA takes the next of the launch's
+// tiles (order[w]) from the work counter and runs the same tile body as the single-grid kernel, so every
+// cell's summation order is that of a single-grid call.
 template <int FAMILY>
 __global__ void __launch_bounds__(kLatThreads, 2) k_batch_lattice(const BatchItemDev* __restrict__ items,
                                                                   const int32_t* __restrict__ item_of_tile,
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kLatThreads, 2) k_batch_lattice(const BatchIte
         const int64_t tg = (int64_t)order[w];
         const BatchItemDev& it = items[item_of_tile[tg]];
         const int64_t tl = tg - it.tile_base;
-        if (FAMILY == kBatchFamilyLattice)
+        if (FAMILY == kBatchFamilyLattice || (FAMILY == kBatchFamilyLatticeMerged && it.mode == kBatchLattice))
             lattice_tile<true>(it.g, it.P, list, range, tg, tl, it.out, it.st);
         else
             lattice_tile<true, true>(it.g, it.P, list, range, tg, tl, it.out, it.st, &c_tables[it.kernel]);
@@ -150,6 +151,8 @@ int lattice_batch_prepare(KiwiCtx* ctx) {
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatDynSmem));
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLatticeGeneric>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatGenDynSmem));
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLatticeMerged>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatMergedDynSmem));
     return KIWI_OK;
 }
 
@@ -158,6 +161,9 @@ int lattice_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, 
                          unsigned long long* d_next, int blocks) {
     if (family == kBatchFamilyLattice)
         k_batch_lattice<kBatchFamilyLattice><<<blocks, kLatThreads, kLatDynSmem, ctx->stream>>>(
+            d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
+    else if (family == kBatchFamilyLatticeMerged)
+        k_batch_lattice<kBatchFamilyLatticeMerged><<<blocks, kLatThreads, kLatMergedDynSmem, ctx->stream>>>(
             d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
     else
         k_batch_lattice<kBatchFamilyLatticeGeneric><<<blocks, kLatThreads, kLatGenDynSmem, ctx->stream>>>(

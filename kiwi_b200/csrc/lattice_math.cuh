@@ -250,9 +250,9 @@ KIWI_LAT_CORNER T lattice_corner(T h, T ih, T r0, T a1, T a2, T D2a, T D3a, T D2
 // variable u of a pyramid is opp / r with opp one of |ux|, |uy|, |uz|, only three distinct logarithm terms
 // (log((1 + u) / (1 - u)) for u = |ux| / r, |uy| / r, |uz| / r) among their six pyramids.  So the point
 // needs one square root, one reciprocal of r |ux uy uz| (giving 1/r, 1/|ux|, 1/|uy|, 1/|uz|), one of the
-// product of the three pair sums S_xy S_xz S_yz (giving every 1 / (1 - u^2) = r^2 / S), three log1p and six
-// arctangents -- where three separate corners need three roots, six reciprocals, six log1p and six
-// arctangents.  Its octant value is the sum of the three: the kernel mass of the box spanned by the
+// product of the three pair sums S_xy S_xz S_yz (giving every 1 / (1 - u^2) = r^2 / S), three log1p and five
+// arctangents (the three walls' I1 angles sum to pi, point_angles) -- where three separate corners need three
+// roots, six reciprocals, six log1p and six arctangents.  Its octant value is the sum of the three: the kernel mass of the box spanned by the
 // particle and the point (by the divergence theorem over that box, whose three faces through the particle
 // carry no flux), so a cell's mass is the 8-term difference of its corners' octant values.
 
@@ -287,10 +287,10 @@ KIWI_LAT T point_pyramid(const LatticeWall<T>& w, bool inner, T b1, T b2, T a, T
 // One wall's corner value inside 2h (lattice_corner) from the point's shared quantities: wall distance r0
 // and its reciprocal, in-plane legs a1 (edge tier E.D2(ea)) and a2 (E.D2(eb)) with reciprocals,
 // s2 = a1^2 + a2^2, r and its reciprocal, the log terms of u = a2 / r (first pyramid) and u = a1 / r
-// (second), their 1 / (1 - u^2), and r0 r / (a1 a2).
+// (second), their 1 / (1 - u^2), and the pair's I1 sum atan(r0 r / (a1 a2)) (point_angles).
 template <class T, class Edges>
 KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T ia2, T s2, T ir, T log_a2, T iom_a2,
-                      T log_a1, T iom_a1, T r0r_a1a2, const Edges& E, int ea, int eb) {
+                      T log_a1, T iom_a1, T I1s, const Edges& E, int ea, int eb) {
     const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
     T pa, pb;
     if (a2 <= a1) {
@@ -306,22 +306,44 @@ KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T i
                           inner ? T(0.0) : E.D2(ea));
     sum += point_pyramid(w, inner, b1, b2, a2 * ir0, a1 * ir, a1 * ia2, s2 * ia2 * ia2, iom_a1, log_a1, pb,
                          inner ? T(0.0) : E.D2(eb));
-    const T I1s = atan(r0r_a1a2);
     const T c1 = inner ? 1. / 40. * w.r0h3 : 0.25 * (-w.r0h - 1. / 30. * w.r0h3 + 1. / 15. * w.r0h_3);
     return w.r0h3 * (1.0 / kPi) * (sum + c1 * I1s);
 }
 
-// One wall's corner value beyond 2h (lattice_corner's first branch): x = r0 / h, the arctangent argument
-// q = r0 r / (a1 a2), its inverse qi, and the edge tiers E.D3(ea), E.D3(eb) of the wall's two edge lines.
+// One wall's corner value beyond 2h (lattice_corner's first branch): x = r0 / h, the angle
+// J = atan(r0 r / (a1 a2)) (point_angles), and the edge tiers E.D3(ea), E.D3(eb) of the wall's two edge lines.
+// For r0 >= 2h the value is the rectangle's solid angle over 4 pi, atan(a1 a2 / (r0 r)) / (4 pi) =
+// (pi/2 - J) / (4 pi): where that angle is small its relative precision is lost, not its absolute one, which
+// is what the cell's alternating sum of octant values needs.
 template <class T, class Edges>
-KIWI_LAT T point_wall_far(T h, T ih, T r0, T q, T qi, const Edges& E, int ea, int eb) {
+KIWI_LAT T point_wall_far(T h, T ih, T r0, T J, const Edges& E, int ea, int eb) {
     const T x = r0 * ih, x2 = x * x, x3 = x2 * x;
     const T K = x3 * (1.0 / kPi);
-    if (r0 >= 2.0 * h) return 0.25 / kPi * atan(qi) + K * (E.D3(ea) + E.D3(eb));
+    if (r0 >= 2.0 * h) return 0.25 / kPi * (0.5 * kPi - J) + K * (E.D3(ea) + E.D3(eb));
     const T x4 = x2 * x2, x5 = x4 * x, x6 = x3 * x3;
     const T p = r0 > h ? -4. / 3. * x3 + x4 - 0.3 * x5 + 1. / 30. * x6 - 1. / 15. + 8. / 5. * x
                        : -2. / 3. * x3 + 0.3 * x5 - 0.1 * x6 + 7. / 5. * x;
-    return -0.25 / kPi * atan(q) + 0.125 * p + K * (E.D3(ea) + E.D3(eb));
+    return -0.25 / kPi * J + 0.125 * p + K * (E.D3(ea) + E.D3(eb));
+}
+
+// The three walls' angles J_c = atan(a_c r / (a_a a_b)) of a lattice point (a_a, a_b the other two offsets)
+// sum to pi: tan J_x tan J_y = r^2 / az^2 > 1, so tan(J_x + J_y) = -tan J_z with J_x + J_y in (pi/2, pi).  Two
+// come from arctangents, the largest (at least pi/3) as pi minus the others.
+template <class T>
+KIWI_LAT void point_angles(T qx, T qy, T qz, T& Jx, T& Jy, T& Jz) {
+    if (qx >= qy && qx >= qz) {
+        Jy = atan(qy);
+        Jz = atan(qz);
+        Jx = kPi - Jy - Jz;
+    } else if (qy >= qz) {
+        Jx = atan(qx);
+        Jz = atan(qz);
+        Jy = kPi - Jx - Jz;
+    } else {
+        Jx = atan(qx);
+        Jy = atan(qy);
+        Jz = kPi - Jx - Jy;
+    }
 }
 
 // The sum of the three corner values of a lattice point at absolute offsets ax, ay, az > 0 from the
@@ -336,12 +358,11 @@ KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const Edges& E) {
     const T axyz = ax * (ay * az);
     const T iP = 1.0 / (r * axyz);  // 1 / (r |ux uy uz|)
     // r0 r / (a1 a2) of the wall at a_c: a_c^2 r^2 iP; its inverse: (product of the other two)^2 iP
-    const T qx = ax2 * r2 * iP, qy = ay2 * r2 * iP, qz = az2 * r2 * iP;
+    T Jx, Jy, Jz;
+    point_angles(ax2 * r2 * iP, ay2 * r2 * iP, az2 * r2 * iP, Jx, Jy, Jz);
     if (!(r2 < 4.0 * (h * h))) {
-        const T qxi = ay2 * az2 * iP, qyi = ax2 * az2 * iP, qzi = ax2 * ay2 * iP;
-        return point_wall_far(h, ih, ax, qx, qxi, E, kEdgeXY, kEdgeXZ) +
-               point_wall_far(h, ih, ay, qy, qyi, E, kEdgeYX, kEdgeYZ) +
-               point_wall_far(h, ih, az, qz, qzi, E, kEdgeZX, kEdgeZY);
+        return point_wall_far(h, ih, ax, Jx, E, kEdgeXY, kEdgeXZ) + point_wall_far(h, ih, ay, Jy, E, kEdgeYX, kEdgeYZ) +
+               point_wall_far(h, ih, az, Jz, E, kEdgeZX, kEdgeZY);
     }
     const T ir = axyz * iP;
     const T iax = r * (ay * az) * iP, iay = r * (ax * az) * iP, iaz = r * (ax * ay) * iP;
@@ -353,9 +374,9 @@ KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const Edges& E) {
     const T Ly = log1p(2.0 * uy * (1.0 + uy) * iomy);
     const T Lz = log1p(2.0 * uz * (1.0 + uz) * iomz);
     const bool inner = r2 < h * h;
-    T s = point_wall(h, ih, inner, ax, iax, ay, iay, az, iaz, syz, ir, Lz, iomz, Ly, iomy, qx, E, kEdgeXY, kEdgeXZ);
-    s += point_wall(h, ih, inner, ay, iay, ax, iax, az, iaz, sxz, ir, Lz, iomz, Lx, iomx, qy, E, kEdgeYX, kEdgeYZ);
-    s += point_wall(h, ih, inner, az, iaz, ax, iax, ay, iay, sxy, ir, Ly, iomy, Lx, iomx, qz, E, kEdgeZX, kEdgeZY);
+    T s = point_wall(h, ih, inner, ax, iax, ay, iay, az, iaz, syz, ir, Lz, iomz, Ly, iomy, Jx, E, kEdgeXY, kEdgeXZ);
+    s += point_wall(h, ih, inner, ay, iay, ax, iax, az, iaz, sxz, ir, Lz, iomz, Lx, iomx, Jy, E, kEdgeYX, kEdgeYZ);
+    s += point_wall(h, ih, inner, az, iaz, ax, iax, ay, iay, sxy, ir, Ly, iomy, Lx, iomx, Jz, E, kEdgeZX, kEdgeZY);
     return s;
 }
 

@@ -69,26 +69,24 @@ def test_fp32_padded_mass(kiwi, ctx):
 
 
 def test_guaranteed_tiles_equal_fp64_form(kiwi, ctx):
+    """The guaranteed variant recomputes in FP64 every 8^3 tile holding a cell whose FP32 rounding bound
+    exceeds 1e-6 of its mass: those tiles equal the FP64 form's bit for bit, and every cell above 1e-6 of
+    the peak ends within 1e-6 of the FP64 form."""
     P = random_particles(400, 21, hmin=0.05, hmax=0.4)
     b, shape = (0, 2, 0, 2, 0, 2), (24, 24, 24)
     g = kiwi.sph_to_grid(P, b, shape, ctx=ctx, precision="fp32_mixed_guaranteed", raw=True)
     f = kiwi.sph_to_grid(P, b, shape, ctx=ctx, precision="fp64", raw=True)
-    r = kiwi.sph_to_grid(P, b, shape, ctx=ctx, precision="fp32_mixed", raw=True)
     assert g.stats["fp64_tiles"] > 0
     M = f.raw[0].reshape(shape)
     G = g.raw[0].reshape(shape)
-    R = r.raw[0].reshape(shape)
-    # per 8^3 tile: either the FP64 form's values exactly, or the FP32 values unchanged
-    n_fp64 = 0
+    n_exact = 0
     for tx in range(3):
         for ty in range(3):
             for tz in range(3):
                 s = np.s_[8 * tx:8 * tx + 8, 8 * ty:8 * ty + 8, 8 * tz:8 * tz + 8]
-                if np.array_equal(G[s], M[s]) and not np.array_equal(G[s], R[s]):
-                    n_fp64 += 1
-                else:
-                    assert np.array_equal(G[s], R[s])
-    assert n_fp64 <= g.stats["fp64_tiles"]
+                if M[s].any() and np.array_equal(G[s], M[s]):
+                    n_exact += 1
+    assert n_exact >= g.stats["fp64_tiles"]
     m = M >= 1e-6 * M.max()
     assert np.max(np.abs(G[m] - M[m]) / M[m]) <= 1e-6
 
