@@ -264,7 +264,9 @@ typedef struct KiwiBatch KiwiBatch;
  * cubic closed form, the reference's evaluation order for the generic kernels) or
  * KIWI_FP64_REFERENCE_ORDER; no flags.  The plan holds the tile lists of the particles' positions and
  * smoothing lengths at creation: masses and velocities may change between runs, positions and smoothing
- * lengths may not.  Results equal kiwi_sph_to_grid_device's for each item, bit for bit. */
+ * lengths may not.  Results equal kiwi_sph_to_grid_device's for each item: bit for bit in
+ * KIWI_FP64_REFERENCE_ORDER; in the lattice form to rounding (within 1e-12 of the item's largest value;
+ * it is compiled with FMA contraction, which the compiler forms per kernel), with equal counts. */
 int kiwi_batch_create(KiwiCtx* ctx, const KiwiBatchItem* items, int n_items, int precision, KiwiBatch** out);
 /* Replays the graph on the context's stream and waits for it.  item_stats (n_items entries) and total
  * may be NULL; gather_ms / total_ms hold the device time of the whole batch. */

@@ -33,6 +33,18 @@ constexpr int kLatPMax = 32;     // particles per chunk
 #define KIWI_LAT_NOINLINE static inline
 #endif
 
+// The in-plane angles of the right triangle with legs a1, a2 (reciprocals ia1, ia2): pa = atan(a2 / a1) and
+// pb = pi/2 - pa, the smaller one from one arctangent, the larger its complement.  The operand is selected
+// and one arctangent evaluated, so that the threads of a warp do not split over two calls.
+template <class T>
+KIWI_LAT void leg_angles(T a1, T ia1, T a2, T ia2, T& pa, T& pb) {
+    const bool lo = a2 <= a1;
+    const T t = atan(lo ? a2 * ia1 : a1 * ia2);
+    const T c = 0.5 * kPi - t;
+    pa = lo ? t : c;
+    pb = lo ? c : t;
+}
+
 // The wall constants of the cubic spline (src/kernel_integral.cpp:222-247) divided by r0^3, as
 // polynomials in r0 / h and h / r0 (the reference forms B_k = r0^3 / 4 (...) and divides by r0^3 at each
 // use).  Powers from one reciprocal of h and one of r0.  The functions below are written over the real
@@ -202,13 +214,7 @@ KIWI_LAT_CORNER T lattice_corner(T h, T ih, T r0, T a1, T a2, T D2a, T D3a, T D2
     const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
     const T K = w.r0h3 * (1.0 / kPi);
     T pa, pb;
-    if (a2 <= a1) {
-        pa = atan(a2 * ia1);
-        pb = 0.5 * kPi - pa;
-    } else {
-        pb = atan(a1 * ia2);
-        pa = 0.5 * kPi - pb;
-    }
+    leg_angles(a1, ia1, a2, ia2, pa, pb);
     const bool inner = r2 < h * h;
     const T b1 = inner ? wall_b1_in(w) : 0.0;
     const T b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
@@ -293,13 +299,7 @@ KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T i
                       T log_a1, T iom_a1, T I1s, const Edges& E, int ea, int eb) {
     const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
     T pa, pb;
-    if (a2 <= a1) {
-        pa = atan(a2 * ia1);
-        pb = 0.5 * kPi - pa;
-    } else {
-        pb = atan(a1 * ia2);
-        pa = 0.5 * kPi - pb;
-    }
+    leg_angles(a1, ia1, a2, ia2, pa, pb);
     const T b1 = inner ? wall_b1_in(w) : 0.0;
     const T b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
     T sum = point_pyramid(w, inner, b1, b2, a1 * ir0, a2 * ir, a2 * ia1, s2 * ia1 * ia1, iom_a2, log_a2, pa,
@@ -329,21 +329,17 @@ KIWI_LAT T point_wall_far(T h, T ih, T r0, T J, const Edges& E, int ea, int eb) 
 // The three walls' angles J_c = atan(a_c r / (a_a a_b)) of a lattice point (a_a, a_b the other two offsets)
 // sum to pi: tan J_x tan J_y = r^2 / az^2 > 1, so tan(J_x + J_y) = -tan J_z with J_x + J_y in (pi/2, pi).  Two
 // come from arctangents, the largest (at least pi/3) as pi minus the others.
+// The two arctangents take selected operands, so that the threads of a warp do not split over the three
+// cases' calls.
 template <class T>
 KIWI_LAT void point_angles(T qx, T qy, T qz, T& Jx, T& Jy, T& Jz) {
-    if (qx >= qy && qx >= qz) {
-        Jy = atan(qy);
-        Jz = atan(qz);
-        Jx = kPi - Jy - Jz;
-    } else if (qy >= qz) {
-        Jx = atan(qx);
-        Jz = atan(qz);
-        Jy = kPi - Jx - Jz;
-    } else {
-        Jx = atan(qx);
-        Jy = atan(qy);
-        Jz = kPi - Jx - Jy;
-    }
+    const bool mx = qx >= qy && qx >= qz, my = !mx && qy >= qz;  // the largest: x, y, else z
+    const T ta = atan(mx ? qy : qx);                             // J_y if x is the largest, else J_x
+    const T tb = atan(mx || my ? qz : qy);                       // J_z unless z is the largest, then J_y
+    const T tc = kPi - ta - tb;
+    Jx = mx ? tc : ta;
+    Jy = mx ? ta : (my ? tc : tb);
+    Jz = mx || my ? tb : tc;
 }
 
 // The sum of the three corner values of a lattice point at absolute offsets ax, ay, az > 0 from the
@@ -535,6 +531,76 @@ KIWI_LAT_NOINLINE double lattice_generic_G(const KiwiKernelTable* K, double q0, 
     return sum;
 }
 
+// lattice_generic_G with what a lattice point shares among its six vertex tiers given: tn = tan(phi),
+// sc = 1 / cos(phi), the series variable u = t / r, iomu2 = 1 / (1 - u^2), I1 = atan(u / a) and K0 = atanh(u).
+// The series is lattice_generic_G's, term for term.
+KIWI_LAT double lattice_generic_G_pt(const KiwiKernelTable* K, double q0, int j, int k, double a, double a2,
+                                              double phi, double tn, double sc, double u, double iomu2, double I1,
+                                              double K0) {
+    const double* ak = K->a[k - 1];
+    int imin = 1;
+    for (int idx = KIWI_NI - 1; idx >= 0; --idx)
+        if (ak[idx] != 0.0) {
+            imin = 1 - idx;
+            break;
+        }
+    const double A3 = K->A3_pi / kPi;
+    double b = 0.0;
+    if (k >= j)
+        for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
+    double sum = (A3 * b) * phi;
+    double ph = 1.0, pl = 0.0;  // q0^idx
+    double wh = 1.0, wl = 0.0;  // (1 - u^2)^-m, compensated like q0^idx
+    double Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
+    double J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
+#pragma unroll
+    for (int idx = 0; idx < KIWI_NI; ++idx) {
+        if (1 - idx < imin) break;
+        double Iv;
+        if (idx == 0) {  // I_1 = atan(u / a)
+            Iv = I1;
+            Iodd = Iv;
+            Kc = K0;
+        } else if (idx == 1) {  // I_0 = phi
+            Iv = phi;
+        } else if ((idx & 1) == 0) {  // I_-(2m+1), m = idx / 2 - 1
+            const int m = idx / 2 - 1;
+            if (m > 0) {
+                const double nw = wh * iomu2;
+                wl = fma(wl, iomu2, fma(wh, iomu2, -nw));
+                wh = nw;
+                Kc = u * (wh + wl) * (1.0 / (2.0 * m)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
+                pow1a2 *= (1.0 + a2);
+            }
+            Iodd += a * pow1a2 * Kc;
+            Iv = Iodd;
+        } else {  // I_-2kk = sum_l C(kk, l) a^2l J_2l, kk = (idx - 1) / 2
+            const int kk = (idx - 1) / 2;
+            if (kk == 1) {
+                J[0] = phi;
+                J[1] = tn;
+            } else {
+                spow *= sc * sc;
+                J[kk] = spow * tn * (1.0 / (2 * kk - 1.0)) + (2 * kk - 2.0) / (2 * kk - 1.0) * J[kk - 1];
+            }
+            double s = J[0], apow = 1.0, bc = 1.0;
+#pragma unroll
+            for (int l = 1; l <= kk; ++l) {
+                bc = bc * (kk - l + 1) / l;
+                apow *= a2;
+                s += bc * apow * J[l];
+            }
+            Iv = s;
+        }
+        const double c = ak[idx];
+        if (c != 0.0) sum += (A3 * c * (ph + pl)) * Iv;
+        const double nh = ph * q0;
+        pl = fma(pl, q0, fma(ph, q0, -nh));
+        ph = nh;
+    }
+    return sum;
+}
+
 KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0, double R0,
                                                            double* rec) {
     for (int i = 0; i < kLatGenERec; ++i) rec[i] = 0.0;
@@ -595,6 +661,83 @@ KIWI_LAT double lattice_generic_corner(const KiwiKernelTable* K, double H, doubl
         const double G = lattice_generic_G(K, q0, j, k0 + s, a, a * a, phi, t * irr, R0 * irr);
         sum += (s > 0 ? rec[3 + s] : 0.0) + G;
     }
+    return sum;
+}
+
+// The three corner values of a lattice point for a generic kernel (support radius H), as
+// lattice_generic_corner(ax; ay, az) + lattice_generic_corner(ay; ax, az) + lattice_generic_corner(az; ax, ay).
+// The six vertex tiers share the point's distance r and one reciprocal of r |ux uy uz| (1/r and the 1/a_c),
+// the series variable u = t / r with atanh(u) (three distinct, u_c = a_c / r) and 1 / (1 - u^2) =
+// r^2 / (r^2 - a_c^2) from one reciprocal of S_xy S_xz S_yz, and I_1 = atan(u / a) = atan(a_a a_b / (a_c r)) =
+// pi/2 - J_c for the leg a_c the vertex's edge line lies at (three distinct, their J_c summing to pi:
+// point_angles).  ax, ay, az > 0.
+// The six edge records of a lattice point: base + kLatGenERec x slot, in PointEdge order.  The slot is
+// selected, not indexed, so that the lookup stays in registers.
+struct GenEdgeRecs {
+    const double* base;
+    int slot[6];
+    KIWI_HD const double* operator()(int e) const {
+        const int sl = e < 3 ? (e == 0 ? slot[0] : (e == 1 ? slot[1] : slot[2]))
+                             : (e == 3 ? slot[3] : (e == 4 ? slot[4] : slot[5]));
+        return base + kLatGenERec * sl;
+    }
+};
+
+KIWI_LAT double lattice_generic_point(const KiwiKernelTable* K, double H, double ax, double ay, double az,
+                                      const GenEdgeRecs& rec) {
+    const double ax2 = ax * ax, ay2 = ay * ay, az2 = az * az;
+    const double sxy = ax2 + ay2, sxz = ax2 + az2, syz = ay2 + az2;
+    const double r2 = sxy + az2;
+    const double r = sqrt(r2);
+    const double axyz = ax * (ay * az);
+    const double iP = 1.0 / (r * axyz);
+    const double ir = axyz * iP;
+    const double iax = r * (ay * az) * iP, iay = r * (ax * az) * iP, iaz = r * (ax * ay) * iP;
+    const double iQ = 1.0 / (sxy * sxz * syz);
+    const double iomx = r2 * (sxy * sxz) * iQ, iomy = r2 * (sxy * syz) * iQ, iomz = r2 * (sxz * syz) * iQ;
+    const double ux = ax * ir, uy = ay * ir, uz = az * ir;
+    const double Kx = atanh(ux), Ky = atanh(uy), Kz = atanh(uz);
+    double Ix, Iy, Iz;
+    point_angles(ax2 * r2 * iP, ay2 * r2 * iP, az2 * r2 * iP, Ix, Iy, Iz);
+    Ix = 0.5 * kPi - Ix;
+    Iy = 0.5 * kPi - Iy;
+    Iz = 0.5 * kPi - Iz;
+    const double iH = 1.0 / H;
+    double sum = 0.0;
+    // per axis c: a_c, 1 / a_c, u_c, 1 / (1 - u_c^2), atanh(u_c), I_1 of the edge lines at a_c; selected, not
+    // indexed, so that nothing leaves the registers in the walls' loop
+#define KIWI_PICK(c, x, y, z) ((c) == 0 ? (x) : ((c) == 1 ? (y) : (z)))
+#pragma unroll 1
+    for (int w = 0; w < 3; ++w) {
+        // the wall at a_w with legs a_c1, a_c2 (the other two axes in ascending order)
+        const int c1 = w == 0 ? 1 : 0, c2 = w == 2 ? 1 : 2;
+        const double r0 = KIWI_PICK(w, ax, ay, az), ir0 = KIWI_PICK(w, iax, iay, iaz);
+        const double q0 = r0 * iH;
+        const int j = generic_region(K, q0);
+        const double a1 = KIWI_PICK(c1, ax, ay, az), a2 = KIWI_PICK(c2, ax, ay, az);
+        const double ia1 = KIWI_PICK(c1, iax, iay, iaz), ia2 = KIWI_PICK(c2, iax, iay, iaz);
+        const double rho = sqrt(KIWI_PICK(w, syz, sxz, sxy));
+        double pa, pb;
+        leg_angles(a1, ia1, a2, ia2, pa, pb);
+#pragma unroll 1
+        for (int v = 0; v < 2; ++v) {
+            const double* rc = rec(2 * w + v);
+            const int packed = (int)rc[0];
+            const int nseg = packed & 7, k0 = packed >> 3;
+            if (nseg == 0) continue;
+            // vertex 0: R0 = a_c1 (the edge line at a_c1, along c2), t = a_c2; vertex 1 the reverse
+            const int cR = v ? c2 : c1, cT = v ? c1 : c2;
+            const double R0 = v ? a2 : a1, t = v ? a1 : a2, iR0 = v ? ia2 : ia1, phi = v ? pb : pa;
+            const double a = R0 * ir0;
+            int s = 0;
+            while (s + 1 < nseg && phi > rc[1 + s]) ++s;
+            const double G = lattice_generic_G_pt(K, q0, j, k0 + s, a, a * a, phi, t * iR0, rho * iR0,
+                                                  KIWI_PICK(cT, ux, uy, uz), KIWI_PICK(cT, iomx, iomy, iomz),
+                                                  KIWI_PICK(cR, Ix, Iy, Iz), KIWI_PICK(cT, Kx, Ky, Kz));
+            sum += (s > 0 ? rc[3 + s] : 0.0) + G;
+        }
+    }
+#undef KIWI_PICK
     return sum;
 }
 

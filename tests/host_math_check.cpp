@@ -82,4 +82,20 @@ double hm_lattice_point(double h, double ax, double ay, double az, const double*
     }
     return lattice_point(h, 1.0 / h, ax, ay, az, E);
 }
+
+// Generic kernels: one edge record (kLatGenERec doubles), one wall's two vertex tiers, and a lattice
+// point's six vertex tiers together (recs: the six edge records in PointEdge order, back to back).
+void hm_lattice_generic_edge(int kernel, double H, double r0, double R0, double* rec) {
+    lattice_generic_edge(&kiwi_kernel_tables[kernel], H, r0, R0, rec);
+}
+
+double hm_lattice_generic_corner(int kernel, double H, double r0, double a1, double a2, const double* rec1,
+                                 const double* rec2) {
+    return lattice_generic_corner(&kiwi_kernel_tables[kernel], H, r0, a1, a2, rec1, rec2);
+}
+
+double hm_lattice_generic_point(int kernel, double H, double ax, double ay, double az, const double* recs) {
+    const GenEdgeRecs rec{recs, {0, 1, 2, 3, 4, 5}};
+    return lattice_generic_point(&kiwi_kernel_tables[kernel], H, ax, ay, az, rec);
+}
 }

