@@ -215,8 +215,9 @@ int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, c
  * dL/dPy, dL/dPz (4 * ncells doubles, the raw4 layout), it writes per particle dL/dx, dL/dy, dL/dz,
  * dL/dh, dL/dm, dL/dvx, dL/dvy, dL/dvz (any output may be NULL).  The per-pair integrals are recomputed
  * in FP64 with forward-mode derivatives, over the pairs of the default (support-culled) evaluation.
- * Every pointer is in device memory; runs on the context's stream and returns when done.  Cubic spline
- * with support 2h only (KIWI_ERR_UNSUPPORTED otherwise). */
+ * Every pointer is in device memory; runs on the context's stream and returns when done.  The cubic
+ * closed form and the generic kernels' tables (every kernel of kiwi_kernel_spec); the tabulated integral
+ * returns KIWI_ERR_UNSUPPORTED. */
 int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                                     const KiwiKernelSel* kernel, const double* raw4, double* dx, double* dy,
                                     double* dz, double* dh, double* dm, double* dvx, double* dvy, double* dvz,

@@ -32,6 +32,7 @@
 #include "engine.hpp"
 #include "kiwi_math.cuh"
 #include "lattice.cuh"
+#include "lattice_dual.cuh"
 #include "prims.cuh"
 
 namespace kiwi_b200 {
@@ -47,6 +48,12 @@ constexpr int kAdjERec = 8;     // D2, D3 as Dual3
 constexpr int kAdjTRec = 5;     // octant value and its derivatives with respect to x, y, z, h
 constexpr size_t kAdjDynSmem = sizeof(double) * (kAdjERec * kAdjECap + kAdjTRec * kAdjPtCap);
 static_assert(kAdjECap <= 2048, "packed edge-pair entries (11-bit slots)");
+// generic kernels: edge records of lattice_generic_edge in Dual3 (offsets with derivatives)
+constexpr int kAdjGenECap = kLatGenECap;
+constexpr int kAdjGenERec = lat_gen_dual_rec<3>();
+constexpr size_t kAdjGenDynSmem = sizeof(double) * (kAdjGenERec * kAdjGenECap + kAdjTRec * kAdjPtCap);
+
+static __constant__ KiwiKernelTable c_adj_tables[KIWI_NUM_KERNELS];
 
 struct AdjGrads {
     double *x, *y, *z, *h, *m, *vx, *vy, *vz;
@@ -98,7 +105,12 @@ __device__ __forceinline__ unsigned long long block_count(unsigned long long v) 
 // homogeneous of degree 0 in (a, b, c, h), whence dT/dh = (ux dT/dx + uy dT/dy + uz dT/dz) / h with the
 // derivatives taken with respect to the particle's coordinates (u = plane - particle).  The tiers are
 // therefore evaluated with three forward derivatives (Dual3, h held fixed) and dT/dh follows from them.
-__global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(CartGeom g, DevParticles P,
+//
+// GENERIC: the table-driven tiers of kernel `kernel` (support g.support_in_h x h): every edge line's record
+// (lattice_generic_edge in Dual3) in (A), the points' six vertex tiers together (lattice_generic_point in
+// Dual3) in (B).  The same homogeneity gives d/dh.
+template <bool GENERIC>
+__global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(CartGeom g, DevParticles P, int kernel,
                                                                           const uint32_t* __restrict__ list,
                                                                           const int64_t* __restrict__ range,
                                                                           const int64_t* __restrict__ offs,
@@ -116,8 +128,11 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
     __shared__ double s_red[kAdjLatThreads / 32][8];
     __shared__ double s_pl[3][kTileX + 1];
     extern __shared__ double s_adj[];
+    constexpr int kERec = GENERIC ? kAdjGenERec : kAdjERec;
+    constexpr int kECap = GENERIC ? kAdjGenECap : kAdjECap;
+    const KiwiKernelTable* K = GENERIC ? &c_adj_tables[kernel] : nullptr;
     double* s_E = s_adj;
-    double* s_T = s_adj + kAdjERec * kAdjECap;
+    double* s_T = s_adj + kERec * kECap;
 
     const int64_t t = blockIdx.x;
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
@@ -167,7 +182,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                     ip += vp;
                 }
             }
-            const bool take = (idx < end) && ie <= kAdjECap && ip <= kAdjPtCap;
+            const bool take = (idx < end) && ie <= kECap && ip <= kAdjPtCap;
             const int np = __popc(__ballot_sync(0xffffffffu, take));
             if (take) {
                 s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph; s_ih[lane] = 1.0 / ph;
@@ -221,6 +236,13 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                     const double oa = s_pl[a][la + pi] - (a == 0 ? s_x[j] : s_y[j]);
                     const double ob = s_pl[b][lb + qi] - (b == 1 ? s_y[j] : s_z[j]);
                     const double h = s_h[j];
+                    if (GENERIC) {
+                        // both orientations' records, evaluated here (no pair list)
+                        const double H = mul_rn(g.support_in_h, h);
+                        const Dual3 pD = dual_abs_offset(oa, a), qD = dual_abs_offset(ob, b);
+                        lattice_generic_edge_dual<3>(K, H, pD, qD, s_E + kERec * sab);
+                        lattice_generic_edge_dual<3>(K, H, qD, pD, s_E + kERec * sba);
+                    } else {
                     heavy = oa != 0.0 && ob != 0.0 && oa * oa + ob * ob <= 4.0 * (h * h);
                     if (heavy) {
                         s_E[kAdjERec * sab] = oa;
@@ -229,6 +251,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                     } else {
 #pragma unroll
                         for (int k = 0; k < kAdjERec; ++k) s_E[kAdjERec * sab + k] = s_E[kAdjERec * sba + k] = 0.0;
+                    }
                     }
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, heavy);
@@ -266,7 +289,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
 #pragma unroll
                             for (int c = 0; c < kAdjTRec; ++c) s_T[kAdjTRec * pt + c] = 0.0;
                         } else {
-                            cls = (ux * ux + uy * uy + uz * uz < 4.0 * (h * h)) ? 0 : 1;
+                            cls = (ux * ux + uy * uy + uz * uz < (GENERIC ? radius * radius : 4.0 * (h * h))) ? 0 : 1;
                             rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
                         }
                     }
@@ -318,13 +341,20 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
             const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
             const int eb = s_eoff[jp];
             const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
-            const SmemDualEdges PE{s_E,
-                                   {eb + i * n1 + jj, eb + nxy + i * n2 + k, eb + nxy + nxz + jj * n0 + i,
-                                    eb + 2 * nxy + nxz + jj * n2 + k, eb + 2 * nxy + nxz + nyz + k * n0 + i,
-                                    eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj}};
+            const int slots[6] = {eb + i * n1 + jj, eb + nxy + i * n2 + k, eb + nxy + nxz + jj * n0 + i,
+                                  eb + 2 * nxy + nxz + jj * n2 + k, eb + 2 * nxy + nxz + nyz + k * n0 + i,
+                                  eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj};
             const double sg = sgn(ux) * sgn(uy) * sgn(uz);
-            const Dual3 f = sg * lattice_point(Dual3(s_h[jp]), Dual3(s_ih[jp]), dual_abs_offset(ux, 0),
-                                               dual_abs_offset(uy, 1), dual_abs_offset(uz, 2), PE);
+            Dual3 f;
+            if (GENERIC) {
+                const GenEdgeRecsDual<3> R{s_E, {slots[0], slots[1], slots[2], slots[3], slots[4], slots[5]}};
+                f = sg * lattice_generic_point(K, mul_rn(g.support_in_h, s_h[jp]), dual_abs_offset(ux, 0),
+                                               dual_abs_offset(uy, 1), dual_abs_offset(uz, 2), R);
+            } else {
+                const SmemDualEdges PE{s_E, {slots[0], slots[1], slots[2], slots[3], slots[4], slots[5]}};
+                f = sg * lattice_point(Dual3(s_h[jp]), Dual3(s_ih[jp]), dual_abs_offset(ux, 0),
+                                       dual_abs_offset(uy, 1), dual_abs_offset(uz, 2), PE);
+            }
             double* o = s_T + kAdjTRec * it;
             o[0] = f.v;
             o[1] = f.d[0];
@@ -427,12 +457,17 @@ __global__ void k_adjoint_reduce(int64_t n, const int64_t* __restrict__ offs, co
 
 }  // namespace
 
+int adjoint_init_tables(KiwiCtx* ctx) {
+    KIWI_CUDA(ctx, cudaMemcpyToSymbol(c_adj_tables, kiwi_kernel_tables, sizeof(kiwi_kernel_tables)));
+    return KIWI_OK;
+}
+
 int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, const KernelChoice& kc,
                      const double* d_cot, const AdjointOutputs& out, KiwiStats* stats) {
-    if (!kc.cubic || kc.tabulated)
+    if (kc.tabulated)
         return set_err(ctx, KIWI_ERR_UNSUPPORTED,
-                       "the adjoint is available for the analytic cubic spline integral with support 2h (generic_path "
-                       "and tabulated unset)");
+                       "the adjoint is available for the analytic integrals (cubic closed form and the generic "
+                       "kernels' tables), not for the tabulated one");
     DevStats* d_st = nullptr;
     KIWI_TRY(scratch_t(ctx, S_STATS, 1, &d_st));
     KIWI_CUDA(ctx, cudaMemsetAsync(d_st, 0, sizeof(DevStats), ctx->stream));
@@ -474,10 +509,17 @@ int cart_adjoint_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, con
         KIWI_TRY(radix_sort_pairs(ctx, k0, v0, k1, v1, total, key_bits, &second));
         k_tile_ranges<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(second ? k1 : k0, total, range);
         KIWI_LAUNCHED(ctx);
-        KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_adjoint_lattice, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)kAdjDynSmem));
-        k_cart_adjoint_lattice<<<(unsigned)ntiles, kAdjLatThreads, kAdjDynSmem, ctx->stream>>>(
-            g, P, second ? v1 : v0, range, offs, d_cot, part, d_st);
+        if (kc.cubic) {
+            KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_adjoint_lattice<false>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjDynSmem));
+            k_cart_adjoint_lattice<false><<<(unsigned)ntiles, kAdjLatThreads, kAdjDynSmem, ctx->stream>>>(
+                g, P, 0, second ? v1 : v0, range, offs, d_cot, part, d_st);
+        } else {
+            KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_adjoint_lattice<true>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kAdjGenDynSmem));
+            k_cart_adjoint_lattice<true><<<(unsigned)ntiles, kAdjLatThreads, kAdjGenDynSmem, ctx->stream>>>(
+                g, P, kc.kernel, second ? v1 : v0, range, offs, d_cot, part, d_st);
+        }
         KIWI_LAUNCHED(ctx);
     }
     if (n > 0) {

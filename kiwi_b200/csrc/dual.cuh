@@ -158,7 +158,20 @@ template <int N>
 KIWI_DD DualN<N> log1p(const DualN<N>& x) { return chain(x, ::log1p(x.v), 1.0 / (1.0 + x.v)); }
 // max with a constant: the constant (no derivative) where it wins
 template <int N>
+KIWI_DD DualN<N> atanh(const DualN<N>& x) { return chain(x, ::atanh(x.v), 1.0 / (1.0 - x.v * x.v)); }
+template <int N>
 KIWI_DD DualN<N> fmax(const DualN<N>& x, double c) { return x.v >= c ? x : DualN<N>(c); }
+template <int N>
+KIWI_DD DualN<N> fmin(double c, const DualN<N>& x) { return x.v <= c ? x : DualN<N>(c); }
+// a * b + c with the value fused (one rounding) and the derivative of a * b + c
+template <int N>
+KIWI_DD DualN<N> fma(const DualN<N>& a, const DualN<N>& b, const DualN<N>& c) {
+    DualN<N> r;
+    r.v = ::fma(a.v, b.v, c.v);
+#pragma unroll
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k] + c.d[k];
+    return r;
+}
 template <int N>
 KIWI_DD DualN<N> sin(const DualN<N>& x) { return chain(x, ::sin(x.v), ::cos(x.v)); }
 template <int N>

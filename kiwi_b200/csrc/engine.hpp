@@ -134,6 +134,7 @@ int fp64_measure_peak(KiwiCtx* ctx, double* tflops);
 // support boxes with full_box, else the cells the supports reach) and the generic kernels (the cells the
 // supports reach), and the batch's persistent launches of those two families.
 int lattice_init_tables(KiwiCtx* ctx);
+int adjoint_init_tables(KiwiCtx* ctx);
 int lattice_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
                         const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box);
 // The FP32-mixed form of the cubic lattice gather (FP32 tiers with FP64 islands, FP64 assembly); the number

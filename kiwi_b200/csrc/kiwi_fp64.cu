@@ -16,7 +16,8 @@ __constant__ KiwiKernelTable c_tables[KIWI_NUM_KERNELS];
 
 int fp64_init_tables(KiwiCtx* ctx) {
     KIWI_CUDA(ctx, cudaMemcpyToSymbol(c_tables, kiwi_kernel_tables, sizeof(kiwi_kernel_tables)));
-    return lattice_init_tables(ctx);
+    KIWI_TRY(lattice_init_tables(ctx));
+    return adjoint_init_tables(ctx);
 }
 
 }  // namespace kiwi_b200

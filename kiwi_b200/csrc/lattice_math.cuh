@@ -450,93 +450,28 @@ KIWI_LAT_EDGE void lattice_edge_pair(T h, T ih, T p, T q, LatticeEdgeT<T>& e_pq,
 constexpr int kLatGenERec = 7;
 constexpr int kLatGenECap = 640;  // edge records per chunk (a full 8^3 particle box needs 486)
 
-// G_k(phi) = bphi_k phi + sum_i coef_k,i I_i(phi) for a wall at q0 = r0 / H in region j of the kernel
-// (generic_G, src/kernel_integral_generic.cpp:82-92), a = R0 / r0, with sin(phi) and cos(phi) given.
-// The wall coefficients A3 a_k,i q0^i are formed on the fly and each basis integral I_i (the recurrences
-// of :19-66) is added as soon as it is formed, in ascending index order: every loop is unrolled over the
-// table's fixed width and predicated on the region's lowest index, so the basis values, the sec-power
-// integrals J_2l and the powers of q0 stay in registers.  q0^i is a compensated running product (hi + lo,
-// the product's rounding error carried exactly by fma): the terms can cancel heavily, and a plain running
-// product's rounding (up to ~i ulp) measurably raised the error of low-density cells; this is within an
-// ulp, like pow, at a fraction of its cost; (1 - u^2)^-m in the K recurrence is formed the same way.
-KIWI_LAT_NOINLINE double lattice_generic_G(const KiwiKernelTable* K, double q0, int j, int k, double a,
-                                                        double a2, double phi, double sinp, double cosp) {
-    const double* ak = K->a[k - 1];
-    int imin = 1;
-    for (int idx = KIWI_NI - 1; idx >= 0; --idx)
-        if (ak[idx] != 0.0) {
-            imin = 1 - idx;
-            break;
-        }
-    const double A3 = K->A3_pi / kPi;
-    double b = 0.0;
-    if (k >= j)
-        for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
-    double sum = (A3 * b) * phi;
-    // u = a sin(phi) / sqrt(a^2 + cos^2(phi)), so u / a = sin(phi) / sqrt(...) and
-    // 1 / (1 - u^2) = (a^2 + cos^2(phi)) / (cos^2(phi) (1 + a^2)): three reciprocals in all
-    const double den = a2 + cosp * cosp, iden = 1.0 / den;
-    const double ua = sinp * sqrt(iden), u = a * ua;
-    const double iomu2 = den / (cosp * cosp * (1.0 + a2));
-    const double sc = imin <= -2 ? 1.0 / cosp : 0.0, tn = sinp * sc;
-    double ph = 1.0, pl = 0.0;  // q0^idx
-    double wh = 1.0, wl = 0.0;  // (1 - u^2)^-m, compensated like q0^idx
-    double Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
-    double J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
-#pragma unroll
-    for (int idx = 0; idx < KIWI_NI; ++idx) {
-        if (1 - idx < imin) break;
-        double Iv;
-        if (idx == 0) {  // I_1 = atan(u / a)
-            Iv = atan(ua);
-            Iodd = Iv;
-            Kc = atanh(u);
-        } else if (idx == 1) {  // I_0 = phi
-            Iv = phi;
-        } else if ((idx & 1) == 0) {  // I_-(2m+1), m = idx / 2 - 1
-            const int m = idx / 2 - 1;
-            if (m > 0) {
-                const double nw = wh * iomu2;
-                wl = fma(wl, iomu2, fma(wh, iomu2, -nw));
-                wh = nw;
-                Kc = u * (wh + wl) * (1.0 / (2.0 * m)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
-                pow1a2 *= (1.0 + a2);
-            }
-            Iodd += a * pow1a2 * Kc;
-            Iv = Iodd;
-        } else {  // I_-2kk = sum_l C(kk, l) a^2l J_2l, kk = (idx - 1) / 2
-            const int kk = (idx - 1) / 2;
-            if (kk == 1) {
-                J[0] = phi;
-                J[1] = tn;
-            } else {
-                spow *= sc * sc;
-                J[kk] = spow * tn * (1.0 / (2 * kk - 1.0)) + (2 * kk - 2.0) / (2 * kk - 1.0) * J[kk - 1];
-            }
-            double s = J[0], apow = 1.0, bc = 1.0;
-#pragma unroll
-            for (int l = 1; l <= kk; ++l) {
-                bc = bc * (kk - l + 1) / l;
-                apow *= a2;
-                s += bc * apow * J[l];
-            }
-            Iv = s;
-        }
-        const double c = ak[idx];
-        if (c != 0.0) sum += (A3 * c * (ph + pl)) * Iv;
-        const double nh = ph * q0;
-        pl = fma(pl, q0, fma(ph, q0, -nh));
-        ph = nh;
-    }
-    return sum;
+// The value of a real number of any of the tiers' types (double, the FP32 type, a dual number), for the
+// decisions taken on values: kernel regions and segment choices.
+KIWI_LAT double lat_value(double x) { return x; }
+template <class T>
+KIWI_LAT double lat_value(const T& x) {
+    return (double)x.v;
 }
 
-// lattice_generic_G with what a lattice point shares among its six vertex tiers given: tn = tan(phi),
-// sc = 1 / cos(phi), the series variable u = t / r, iomu2 = 1 / (1 - u^2), I1 = atan(u / a) and K0 = atanh(u).
-// The series is lattice_generic_G's, term for term.
-KIWI_LAT double lattice_generic_G_pt(const KiwiKernelTable* K, double q0, int j, int k, double a, double a2,
-                                              double phi, double tn, double sc, double u, double iomu2, double I1,
-                                              double K0) {
+// G_k(phi) = bphi_k phi + sum_i coef_k,i I_i(phi) for a wall at q0 = r0 / H in region j of the kernel
+// (generic_G, src/kernel_integral_generic.cpp:82-92), a = R0 / r0, with what the basis integrals are built
+// from given: tn = tan(phi), sc = 1 / cos(phi), the series variable u = a sin(phi) / sqrt(a^2 + cos^2(phi))
+// (= t / r for the vertex at distance r whose leg along the edge is t), iomu2 = 1 / (1 - u^2), I1 = atan(u / a)
+// and K0 = atanh(u).  The wall coefficients A3 a_k,i q0^i are formed on the fly and each basis integral I_i
+// (the recurrences of :19-66) is added as soon as it is formed, in ascending index order: every loop is
+// unrolled over the table's fixed width and predicated on the region's lowest index, so the basis values,
+// the sec-power integrals J_2l and the powers of q0 stay in registers.  q0^i is a compensated running
+// product (hi + lo, the product's rounding error carried exactly by fma): the terms can cancel heavily, and a
+// plain running product's rounding (up to ~i ulp) measurably raised the error of low-density cells; this is
+// within an ulp, like pow, at a fraction of its cost; (1 - u^2)^-m in the K recurrence is formed the same way.
+template <class T>
+KIWI_LAT_NOINLINE T lattice_generic_G_pt(const KiwiKernelTable* K, T q0, int j, int k, T a, T a2, T phi, T tn,
+                                         T sc, T u, T iomu2, T I1, T K0) {
     const double* ak = K->a[k - 1];
     int imin = 1;
     for (int idx = KIWI_NI - 1; idx >= 0; --idx)
@@ -545,18 +480,18 @@ KIWI_LAT double lattice_generic_G_pt(const KiwiKernelTable* K, double q0, int j,
             break;
         }
     const double A3 = K->A3_pi / kPi;
-    double b = 0.0;
+    T b = 0.0;
     if (k >= j)
         for (int p = KIWI_NB - 1; p >= 0; --p) b = b * q0 + K->B[j - 1][k - 1][p];
-    double sum = (A3 * b) * phi;
-    double ph = 1.0, pl = 0.0;  // q0^idx
-    double wh = 1.0, wl = 0.0;  // (1 - u^2)^-m, compensated like q0^idx
-    double Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
-    double J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
+    T sum = (A3 * b) * phi;
+    T ph = 1.0, pl = 0.0;  // q0^idx
+    T wh = 1.0, wl = 0.0;  // (1 - u^2)^-m, compensated like q0^idx
+    T Iodd = 0.0, Kc = 0.0, pow1a2 = 1.0, spow = 1.0;
+    T J[(KIWI_NI + 1) / 2];  // J[l] = int_0^phi sec^(2l)
 #pragma unroll
     for (int idx = 0; idx < KIWI_NI; ++idx) {
         if (1 - idx < imin) break;
-        double Iv;
+        T Iv;
         if (idx == 0) {  // I_1 = atan(u / a)
             Iv = I1;
             Iodd = Iv;
@@ -566,7 +501,7 @@ KIWI_LAT double lattice_generic_G_pt(const KiwiKernelTable* K, double q0, int j,
         } else if ((idx & 1) == 0) {  // I_-(2m+1), m = idx / 2 - 1
             const int m = idx / 2 - 1;
             if (m > 0) {
-                const double nw = wh * iomu2;
+                const T nw = wh * iomu2;
                 wl = fma(wl, iomu2, fma(wh, iomu2, -nw));
                 wh = nw;
                 Kc = u * (wh + wl) * (1.0 / (2.0 * m)) + (2.0 * m - 1.0) / (2.0 * m) * Kc;
@@ -583,7 +518,8 @@ KIWI_LAT double lattice_generic_G_pt(const KiwiKernelTable* K, double q0, int j,
                 spow *= sc * sc;
                 J[kk] = spow * tn * (1.0 / (2 * kk - 1.0)) + (2 * kk - 2.0) / (2 * kk - 1.0) * J[kk - 1];
             }
-            double s = J[0], apow = 1.0, bc = 1.0;
+            T s = J[0], apow = 1.0;
+            double bc = 1.0;
 #pragma unroll
             for (int l = 1; l <= kk; ++l) {
                 bc = bc * (kk - l + 1) / l;
@@ -594,34 +530,63 @@ KIWI_LAT double lattice_generic_G_pt(const KiwiKernelTable* K, double q0, int j,
         }
         const double c = ak[idx];
         if (c != 0.0) sum += (A3 * c * (ph + pl)) * Iv;
-        const double nh = ph * q0;
+        const T nh = ph * q0;
         pl = fma(pl, q0, fma(ph, q0, -nh));
         ph = nh;
     }
     return sum;
 }
 
-KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0, double R0,
-                                                           double* rec) {
-    for (int i = 0; i < kLatGenERec; ++i) rec[i] = 0.0;
+// G_k(phi) with sin(phi) and cos(phi) given: u / a = sin(phi) / sqrt(a^2 + cos^2(phi)) and
+// 1 / (1 - u^2) = (a^2 + cos^2(phi)) / (cos^2(phi) (1 + a^2)): three reciprocals in all.
+template <class T>
+KIWI_LAT T lattice_generic_G(const KiwiKernelTable* K, T q0, int j, int k, T a, T a2, T phi, T sinp, T cosp) {
+    const T den = a2 + cosp * cosp, iden = 1.0 / den;
+    const T ua = sinp * sqrt(iden), u = a * ua;
+    const T iomu2 = den / (cosp * cosp * (1.0 + a2));
+    const T sc = 1.0 / cosp, tn = sinp * sc;
+    return lattice_generic_G_pt(K, q0, j, k, a, a2, phi, tn, sc, u, iomu2, atan(ua), atanh(u));
+}
+
+// The edge record of a generic kernel for the edge line at in-plane distance R0 in the wall at r0 (support
+// radius H): the kernel regions crossed along the line and the angles where it leaves each
+// (generic_edge, :119-148): w.set(nseg + 8 x first region), then per segment boundary s = 0..nseg-2 the
+// angle phi_end(s) and the continuity offset of segment s + 1.
+template <class T, class W>
+KIWI_LAT void lattice_generic_edge_t(const KiwiKernelTable* K, double H, T r0, T R0, W& w) {
     if (r0 == 0.0 || R0 == 0.0) return;
-    // the regions crossed along the edge line and the angles where it leaves them (generic_edge, :119-148)
-    const double q0 = r0 / H, qR = R0 / H;
-    const double a = R0 / r0, a2 = a * a;
-    const int j = generic_region(K, q0);
-    const int k0 = generic_region(K, sqrt(q0 * q0 + qR * qR));
+    const T q0 = r0 / H, qR = R0 / H;
+    const T a = R0 / r0, a2 = a * a;
+    const int j = generic_region(K, lat_value(q0));
+    const int k0 = generic_region(K, lat_value(sqrt(q0 * q0 + qR * qR)));
     const int nseg = K->nreg - k0 + 1;
-    rec[0] = (double)(nseg + 8 * k0);
-    double off = 0.0;
+    w.set_packed((double)(nseg + 8 * k0));
+    T off = 0.0;
     for (int s = 0; s + 1 < nseg; ++s) {
         const int k = k0 + s;
         const double c = K->c[k - 1];
-        const double pb = acos(fmin(1.0, qR / sqrt(c * c - q0 * q0)));
-        if (s < 3) rec[1 + s] = pb;
-        const double sp = sin(pb), cp = cos(pb);
+        const T pb = acos(fmin(1.0, qR / sqrt(c * c - q0 * q0)));
+        const T sp = sin(pb), cp = cos(pb);
         off = off + lattice_generic_G(K, q0, j, k, a, a2, pb, sp, cp) - lattice_generic_G(K, q0, j, k + 1, a, a2, pb, sp, cp);
-        if (s < 3) rec[4 + s] = off;
+        if (s < 3) w.set_segment(s, pb, off);
     }
+}
+
+// The double record: [0] = nseg + 8 x first region, [1..3] = phi_end of segments 0..2, [4..6] = offset of
+// segments 1..3.
+struct GenEdgeWriter {
+    double* rec;
+    KIWI_HD void set_packed(double v) { rec[0] = v; }
+    KIWI_HD void set_segment(int s, double phi_end, double off) {
+        rec[1 + s] = phi_end;
+        rec[4 + s] = off;
+    }
+};
+
+KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0, double R0, double* rec) {
+    for (int i = 0; i < kLatGenERec; ++i) rec[i] = 0.0;
+    GenEdgeWriter w{rec};
+    lattice_generic_edge_t(K, H, r0, R0, w);
 }
 
 
@@ -632,21 +597,20 @@ KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0
 // a1 line and rec2 of the a2 line: vertex 1 has R0 = a1, t = a2 and vertex 2 the reverse) share what the
 // pair has in common: the distance sqrt(a1^2 + a2^2) and its reciprocal, 1 / r0, q0 = r0 / H and its
 // kernel region, and the angle pair (the smaller one from atan2, the larger its complement, as in
-// lattice_corner).  r0, a1, a2 > 0.
+// lattice_corner).  r0, a1, a2 > 0.  (lattice_generic_point evaluates a point's three walls together; it
+// is the adjoint's form: in double it measured slower than three corners and less accurate in low-density
+// cells of the generic fixtures.)
 KIWI_LAT double lattice_generic_corner(const KiwiKernelTable* K, double H, double r0,
                                                                double a1, double a2, const double* rec1,
                                                                const double* rec2) {
     const double ir0 = 1.0 / r0, irr = 1.0 / sqrt(a1 * a1 + a2 * a2);
     const double q0 = r0 / H;
     const int j = generic_region(K, q0);
-    double pa, pb;
-    if (a2 <= a1) {
-        pa = atan2(a2, a1);
-        pb = 0.5 * kPi - pa;
-    } else {
-        pb = atan2(a1, a2);
-        pa = 0.5 * kPi - pb;
-    }
+    // the smaller angle from one atan2 with selected operands (no warp split over two calls), the larger
+    // its complement
+    const bool lo = a2 <= a1;
+    const double tq = atan2(lo ? a2 : a1, lo ? a1 : a2), tc = 0.5 * kPi - tq;
+    const double pa = lo ? tq : tc, pb = lo ? tc : tq;
     double sum = 0.0;
 #pragma unroll 1
     for (int v = 0; v < 2; ++v) {
@@ -676,34 +640,45 @@ KIWI_LAT double lattice_generic_corner(const KiwiKernelTable* K, double H, doubl
 struct GenEdgeRecs {
     const double* base;
     int slot[6];
-    KIWI_HD const double* operator()(int e) const {
+    KIWI_HD const double* rec(int e) const {
         const int sl = e < 3 ? (e == 0 ? slot[0] : (e == 1 ? slot[1] : slot[2]))
                              : (e == 3 ? slot[3] : (e == 4 ? slot[4] : slot[5]));
         return base + kLatGenERec * sl;
     }
+    KIWI_HD int packed(const double* r) const { return (int)r[0]; }
+    KIWI_HD double phi_end(const double* r, int s) const { return r[1 + s]; }
+    KIWI_HD double offset(const double* r, int s) const { return r[3 + s]; }  // segment s >= 1
 };
 
-KIWI_LAT double lattice_generic_point(const KiwiKernelTable* K, double H, double ax, double ay, double az,
-                                      const GenEdgeRecs& rec) {
-    const double ax2 = ax * ax, ay2 = ay * ay, az2 = az * az;
-    const double sxy = ax2 + ay2, sxz = ax2 + az2, syz = ay2 + az2;
-    const double r2 = sxy + az2;
-    const double r = sqrt(r2);
-    const double axyz = ax * (ay * az);
-    const double iP = 1.0 / (r * axyz);
-    const double ir = axyz * iP;
-    const double iax = r * (ay * az) * iP, iay = r * (ax * az) * iP, iaz = r * (ax * ay) * iP;
-    const double iQ = 1.0 / (sxy * sxz * syz);
-    const double iomx = r2 * (sxy * sxz) * iQ, iomy = r2 * (sxy * syz) * iQ, iomz = r2 * (sxz * syz) * iQ;
-    const double ux = ax * ir, uy = ay * ir, uz = az * ir;
-    const double Kx = atanh(ux), Ky = atanh(uy), Kz = atanh(uz);
-    double Ix, Iy, Iz;
+// The three corner values of a lattice point for a generic kernel (support radius H), as
+// lattice_generic_corner(ax; ay, az) + lattice_generic_corner(ay; ax, az) + lattice_generic_corner(az; ax, ay).
+// The six vertex tiers share the point's distance r and one reciprocal of r |ux uy uz| (1/r and the 1/a_c),
+// the series variable u = t / r with atanh(u) (three distinct, u_c = a_c / r) and 1 / (1 - u^2) =
+// r^2 / (r^2 - a_c^2) from one reciprocal of S_xy S_xz S_yz, and I_1 = atan(u / a) = atan(a_a a_b / (a_c r)) =
+// pi/2 - J_c for the leg a_c the vertex's edge line lies at (three distinct, their J_c summing to pi:
+// point_angles).  R reads the six edge records (rec(e) in PointEdge order; packed, phi_end, offset).
+// ax, ay, az > 0.
+template <class T, class R>
+KIWI_LAT T lattice_generic_point(const KiwiKernelTable* K, double H, T ax, T ay, T az, const R& recs) {
+    const T ax2 = ax * ax, ay2 = ay * ay, az2 = az * az;
+    const T sxy = ax2 + ay2, sxz = ax2 + az2, syz = ay2 + az2;
+    const T r2 = sxy + az2;
+    const T r = sqrt(r2);
+    const T axyz = ax * (ay * az);
+    const T iP = 1.0 / (r * axyz);
+    const T ir = axyz * iP;
+    const T iax = r * (ay * az) * iP, iay = r * (ax * az) * iP, iaz = r * (ax * ay) * iP;
+    const T iQ = 1.0 / (sxy * sxz * syz);
+    const T iomx = r2 * (sxy * sxz) * iQ, iomy = r2 * (sxy * syz) * iQ, iomz = r2 * (sxz * syz) * iQ;
+    const T ux = ax * ir, uy = ay * ir, uz = az * ir;
+    const T Kx = atanh(ux), Ky = atanh(uy), Kz = atanh(uz);
+    T Ix, Iy, Iz;
     point_angles(ax2 * r2 * iP, ay2 * r2 * iP, az2 * r2 * iP, Ix, Iy, Iz);
     Ix = 0.5 * kPi - Ix;
     Iy = 0.5 * kPi - Iy;
     Iz = 0.5 * kPi - Iz;
     const double iH = 1.0 / H;
-    double sum = 0.0;
+    T sum = 0.0;
     // per axis c: a_c, 1 / a_c, u_c, 1 / (1 - u_c^2), atanh(u_c), I_1 of the edge lines at a_c; selected, not
     // indexed, so that nothing leaves the registers in the walls' loop
 #define KIWI_PICK(c, x, y, z) ((c) == 0 ? (x) : ((c) == 1 ? (y) : (z)))
@@ -711,30 +686,30 @@ KIWI_LAT double lattice_generic_point(const KiwiKernelTable* K, double H, double
     for (int w = 0; w < 3; ++w) {
         // the wall at a_w with legs a_c1, a_c2 (the other two axes in ascending order)
         const int c1 = w == 0 ? 1 : 0, c2 = w == 2 ? 1 : 2;
-        const double r0 = KIWI_PICK(w, ax, ay, az), ir0 = KIWI_PICK(w, iax, iay, iaz);
-        const double q0 = r0 * iH;
-        const int j = generic_region(K, q0);
-        const double a1 = KIWI_PICK(c1, ax, ay, az), a2 = KIWI_PICK(c2, ax, ay, az);
-        const double ia1 = KIWI_PICK(c1, iax, iay, iaz), ia2 = KIWI_PICK(c2, iax, iay, iaz);
-        const double rho = sqrt(KIWI_PICK(w, syz, sxz, sxy));
-        double pa, pb;
+        const T r0 = KIWI_PICK(w, ax, ay, az), ir0 = KIWI_PICK(w, iax, iay, iaz);
+        const T q0 = r0 * iH;
+        const int j = generic_region(K, lat_value(q0));
+        const T a1 = KIWI_PICK(c1, ax, ay, az), a2 = KIWI_PICK(c2, ax, ay, az);
+        const T ia1 = KIWI_PICK(c1, iax, iay, iaz), ia2 = KIWI_PICK(c2, iax, iay, iaz);
+        const T rho = sqrt(KIWI_PICK(w, syz, sxz, sxy));
+        T pa, pb;
         leg_angles(a1, ia1, a2, ia2, pa, pb);
 #pragma unroll 1
         for (int v = 0; v < 2; ++v) {
-            const double* rc = rec(2 * w + v);
-            const int packed = (int)rc[0];
+            const auto rc = recs.rec(2 * w + v);
+            const int packed = recs.packed(rc);
             const int nseg = packed & 7, k0 = packed >> 3;
             if (nseg == 0) continue;
             // vertex 0: R0 = a_c1 (the edge line at a_c1, along c2), t = a_c2; vertex 1 the reverse
             const int cR = v ? c2 : c1, cT = v ? c1 : c2;
-            const double R0 = v ? a2 : a1, t = v ? a1 : a2, iR0 = v ? ia2 : ia1, phi = v ? pb : pa;
-            const double a = R0 * ir0;
+            const T R0 = v ? a2 : a1, t = v ? a1 : a2, iR0 = v ? ia2 : ia1, phi = v ? pb : pa;
+            const T a = R0 * ir0;
             int s = 0;
-            while (s + 1 < nseg && phi > rc[1 + s]) ++s;
-            const double G = lattice_generic_G_pt(K, q0, j, k0 + s, a, a * a, phi, t * iR0, rho * iR0,
-                                                  KIWI_PICK(cT, ux, uy, uz), KIWI_PICK(cT, iomx, iomy, iomz),
-                                                  KIWI_PICK(cR, Ix, Iy, Iz), KIWI_PICK(cT, Kx, Ky, Kz));
-            sum += (s > 0 ? rc[3 + s] : 0.0) + G;
+            while (s + 1 < nseg && lat_value(phi) > recs.phi_end(rc, s)) ++s;
+            const T G = lattice_generic_G_pt(K, q0, j, k0 + s, a, a * a, phi, t * iR0, rho * iR0,
+                                             KIWI_PICK(cT, ux, uy, uz), KIWI_PICK(cT, iomx, iomy, iomz),
+                                             KIWI_PICK(cR, Ix, Iy, Iz), KIWI_PICK(cT, Kx, Ky, Kz));
+            sum += (s > 0 ? recs.offset(rc, s) : T(0.0)) + G;
         }
     }
 #undef KIWI_PICK

@@ -369,8 +369,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     const int ezx = eb + 2 * nxy + nxz + nyz + k * n0 + i, ezy = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
                     if (GENERIC) {
                         const double H = mul_rn(sup_in_h, s_h[jp]);
-                        const GenEdgeRecs rec{s_E, {exy, exz, eyx, eyz, ezx, ezy}};
-                        f = lattice_generic_point(K, H, ax, ay, az, rec);
+                        f = lattice_generic_corner(K, H, ax, ay, az, s_E + kLatGenERec * exy, s_E + kLatGenERec * exz) +
+                            lattice_generic_corner(K, H, ay, ax, az, s_E + kLatGenERec * eyx, s_E + kLatGenERec * eyz) +
+                            lattice_generic_corner(K, H, az, ax, ay, s_E + kLatGenERec * ezx, s_E + kLatGenERec * ezy);
                     } else {
                         if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * s_h[jp]) {
                             const SmemPointEdges<F32> E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};

@@ -7,6 +7,7 @@
 #include "../kiwi_b200/csrc/kiwi_math.cuh"
 #include "../kiwi_b200/csrc/dual.cuh"
 #include "../kiwi_b200/csrc/lattice_math.cuh"
+#include "../kiwi_b200/csrc/lattice_dual.cuh"
 
 using namespace kiwi_b200;
 
@@ -97,5 +98,20 @@ double hm_lattice_generic_corner(int kernel, double H, double r0, double a1, dou
 double hm_lattice_generic_point(int kernel, double H, double ax, double ay, double az, const double* recs) {
     const GenEdgeRecs rec{recs, {0, 1, 2, 3, 4, 5}};
     return lattice_generic_point(&kiwi_kernel_tables[kernel], H, ax, ay, az, rec);
+}
+
+// The same point in Dual3 (d/dax, d/day, d/daz): the six edge records with derivatives
+// (lattice_generic_edge_dual) and the point value.  out4 = value, d/dax, d/day, d/daz.
+void hm_lattice_generic_point_grad(int kernel, double H, double ax, double ay, double az, double* out4) {
+    const KiwiKernelTable* K = &kiwi_kernel_tables[kernel];
+    const Dual3 X = Dual3::seed(ax, 0), Y = Dual3::seed(ay, 1), Z = Dual3::seed(az, 2);
+    constexpr int R = lat_gen_dual_rec<3>();
+    double recs[6 * R];
+    const Dual3 r0s[6] = {X, X, Y, Y, Z, Z}, R0s[6] = {Y, Z, X, Z, X, Y};
+    for (int e = 0; e < 6; ++e) lattice_generic_edge_dual<3>(K, H, r0s[e], R0s[e], recs + R * e);
+    const GenEdgeRecsDual<3> rd{recs, {0, 1, 2, 3, 4, 5}};
+    const Dual3 f = lattice_generic_point(K, H, X, Y, Z, rd);
+    out4[0] = f.v;
+    for (int k = 0; k < 3; ++k) out4[1 + k] = f.d[k];
 }
 }

@@ -189,12 +189,63 @@ def test_adjoint_deterministic_and_edge_cases(kiwi, ctx):
     assert st["evaluated_pairs"] == 0
 
 
-def test_adjoint_rejects_generic_kernels(kiwi, ctx):
+@pytest.mark.parametrize("kname", ["wendland_c4", "quintic_spline", "cubic_generic"])
+def test_generic_kernel_adjoint_matches_fd(kiwi, ctx, kname):
+    """The generic kernels' adjoint (edge records and lattice points in dual numbers over the kernel's
+    tables) against central differences of the GPU forward with the same kernel, and of the FP64 oracle on
+    a small grid."""
+    ki = (kiwi.make_kernel_integrator("cubic_spline", generic_path=True) if kname == "cubic_generic"
+          else kiwi.make_kernel_integrator(kname))
+    bounds, shape = (0.0, 2.0, 0.0, 2.0, 0.0, 2.0), (16, 16, 16)
+    P = random_particles(120, seed=43, hmin=0.06, hmax=0.3)
+    rng = np.random.default_rng(17)
+    cot = rng.standard_normal(4 * int(np.prod(shape)))
+    Pd = _dev(P)
+    g = {k: torch.empty_like(Pd[k]) for k in KEYS}
+    st = kiwi.sph_to_grid_adjoint_device(Pd, bounds, shape, torch.tensor(cot, device="cuda"), g, kernel=ki, ctx=ctx)
+    ad = {k: g[k].cpu().numpy() for k in KEYS}
+    assert st["evaluated_pairs"] > 0
+
+    def loss(P1):
+        r = kiwi.sph_to_grid(P1, bounds, shape, raw=True, ctx=ctx, precision="fp64", kernel=ki)
+        return float(r.raw.reshape(-1) @ cot)
+
+    worst = np.zeros(3)
+    for i in rng.choice(len(P["x"]), 20, replace=False):
+        fd = _fd(loss, _one(P, i), float(P["h"][i]))
+        worst = np.maximum(worst, _rel_errors(ad, fd, i))
+    print(f"{kname}: adjoint vs FD of the GPU forward (x/y/z/h, m, v): {worst}")
+    assert worst.max() <= FD_TOL, worst
+
+
+def test_generic_kernel_adjoint_matches_fd_of_oracle(kiwi, ctx, oracle):
+    bounds, shape = (0.0, 1.0, 0.0, 1.0, 0.0, 1.0), (8, 8, 8)
+    P = random_particles(5, seed=6, box=(0.15, 0.85), hmin=0.06, hmax=0.2)
+    rng = np.random.default_rng(9)
+    cot = rng.standard_normal(4 * 512)
+    ki = kiwi.make_kernel_integrator("wendland_c4")
+    Pd = _dev(P)
+    g = {k: torch.empty_like(Pd[k]) for k in KEYS}
+    kiwi.sph_to_grid_adjoint_device(Pd, bounds, shape, torch.tensor(cot, device="cuda"), g, kernel=ki, ctx=ctx)
+    ad = {k: g[k].cpu().numpy() for k in KEYS}
+    spec = kiwi.get_kernel("wendland_c4")
+    worst = np.zeros(3)
+    for i in range(len(P["x"])):
+        fd = _fd(lambda P1: float(oracle.sph_to_grid(P1, bounds, shape, kernel=spec.index,
+                                                     support_in_h=spec.radkern)[4].reshape(-1) @ cot),
+                 _one(P, i), float(P["h"][i]))
+        worst = np.maximum(worst, _rel_errors(ad, fd, i))
+    print(f"wendland_c4: adjoint vs FD of the FP64 oracle: {worst}")
+    assert worst.max() <= FD_TOL, worst
+
+
+def test_adjoint_rejects_tabulated(kiwi, ctx):
     P = random_particles(4, seed=1)
     Pd = _dev(P)
     g = {"x": torch.empty_like(Pd["x"])}
     cot = torch.zeros(4 * 8 ** 3, dtype=torch.float64, device="cuda")
     with pytest.raises(kiwi.KiwiError) as e:
         kiwi.sph_to_grid_adjoint_device(Pd, (0, 2, 0, 2, 0, 2), (8, 8, 8), cot, g,
-                                        kernel=kiwi.make_kernel_integrator("wendland_c4"), ctx=ctx)
+                                        kernel=kiwi.make_kernel_integrator("cubic_spline", use_tabulated_integral=True),
+                                        ctx=ctx)
     assert e.value.code == -6

@@ -39,6 +39,7 @@ def hm(tmp_path_factory):
     L.hm_lattice_generic_corner.argtypes = [C.c_int] + [C.c_double] * 4 + [dp, dp]
     L.hm_lattice_generic_point.restype = C.c_double
     L.hm_lattice_generic_point.argtypes = [C.c_int] + [C.c_double] * 4 + [dp]
+    L.hm_lattice_generic_point_grad.argtypes = [C.c_int] + [C.c_double] * 4 + [dp]
     return L
 
 
@@ -200,3 +201,42 @@ def test_lattice_generic_point(hm):
               f"corner rounding max {noise.max():.2e} q99 {np.quantile(noise, 0.99):.2e}")
         assert diff.max() <= 1.5 * noise.max() + 1e-15, kern
         assert np.quantile(diff, 0.99) <= 1.5 * np.quantile(noise, 0.99) + 1e-15, kern
+
+
+def test_lattice_generic_point_derivatives(hm):
+    """The generic lattice point in dual numbers (the adjoint's instantiation: edge records with derivatives
+    of their continuity offsets, the point's six vertex tiers) has the double form's value and derivatives
+    that match central differences of the double form (records recomputed at each offset)."""
+    dp = C.POINTER(C.c_double)
+
+    def value(kern, H, a):
+        recs = np.zeros(6 * 7)
+        for e, (r0, R0) in enumerate(((a[0], a[1]), (a[0], a[2]), (a[1], a[0]), (a[1], a[2]), (a[2], a[0]),
+                                      (a[2], a[1]))):
+            hm.hm_lattice_generic_edge(kern, H, r0, R0, recs[7 * e:].ctypes.data_as(dp))
+        return hm.hm_lattice_generic_point(kern, H, a[0], a[1], a[2], recs.ctypes.data_as(dp))
+
+    def fd(kern, H, a, c, d):
+        ap, am = a.copy(), a.copy()
+        ap[c] += d
+        am[c] -= d
+        return (value(kern, H, ap) - value(kern, H, am)) / (2 * d)
+
+    rng = np.random.default_rng(61)
+    worst_v, worst_d = 0.0, 0.0
+    for kern in range(6):
+        for _ in range(150):
+            H = 1.6
+            a = H * (0.05 + 0.9 * rng.random(3))
+            out = np.zeros(4)
+            hm.hm_lattice_generic_point_grad(kern, H, a[0], a[1], a[2], out.ctypes.data_as(dp))
+            worst_v = max(worst_v, abs(out[0] - value(kern, H, a)))
+            for c in range(3):
+                # Richardson-extrapolated central differences (step 1e-4 H and half of it): truncation ~1e-13,
+                # rounding (the generic tiers' ~1e-13 noise over the step) ~1e-9
+                d = 1e-4 * H
+                est = (4.0 * fd(kern, H, a, c, d / 2) - fd(kern, H, a, c, d)) / 3.0
+                worst_d = max(worst_d, abs(out[1 + c] - est) * H)
+    print(f"dual vs double value {worst_v:.2e}; derivative vs central differences (x H) {worst_d:.2e}")
+    assert worst_v < 1e-13
+    assert worst_d < 1e-8
