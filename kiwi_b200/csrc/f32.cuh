@@ -63,6 +63,12 @@ KIWI_FF F32 atan(F32 x) { return mk(atanf(x.v)); }
 KIWI_FF F32 atan2(F32 y, F32 x) { return mk(atan2f(y.v, x.v)); }
 KIWI_FF F32 log1p(F32 x) { return mk(log1pf(x.v)); }
 KIWI_FF F32 fmax(F32 x, double c) { return mk(fmaxf(x.v, (float)c)); }
+KIWI_FF F32 fmin(double c, F32 x) { return mk(fminf((float)c, x.v)); }
+KIWI_FF F32 acos(F32 x) { return mk(acosf(x.v)); }
+KIWI_FF F32 sin(F32 x) { return mk(sinf(x.v)); }
+KIWI_FF F32 cos(F32 x) { return mk(cosf(x.v)); }
+KIWI_FF F32 atanh(F32 x) { return mk(atanhf(x.v)); }
+KIWI_FF F32 fma(F32 a, F32 b, F32 c) { return mk(fmaf(a.v, b.v, c.v)); }
 
 #undef KIWI_FF
 

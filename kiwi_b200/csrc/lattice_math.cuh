@@ -470,7 +470,7 @@ KIWI_LAT double lat_value(const T& x) {
 // plain running product's rounding (up to ~i ulp) measurably raised the error of low-density cells; this is
 // within an ulp, like pow, at a fraction of its cost; (1 - u^2)^-m in the K recurrence is formed the same way.
 template <class T>
-KIWI_LAT_NOINLINE T lattice_generic_G_pt(const KiwiKernelTable* K, T q0, int j, int k, T a, T a2, T phi, T tn,
+KIWI_LAT T lattice_generic_G_pt(const KiwiKernelTable* K, T q0, int j, int k, T a, T a2, T phi, T tn,
                                          T sc, T u, T iomu2, T I1, T K0) {
     const double* ak = K->a[k - 1];
     int imin = 1;
@@ -540,7 +540,8 @@ KIWI_LAT_NOINLINE T lattice_generic_G_pt(const KiwiKernelTable* K, T q0, int j, 
 // G_k(phi) with sin(phi) and cos(phi) given: u / a = sin(phi) / sqrt(a^2 + cos^2(phi)) and
 // 1 / (1 - u^2) = (a^2 + cos^2(phi)) / (cos^2(phi) (1 + a^2)): three reciprocals in all.
 template <class T>
-KIWI_LAT T lattice_generic_G(const KiwiKernelTable* K, T q0, int j, int k, T a, T a2, T phi, T sinp, T cosp) {
+KIWI_LAT_NOINLINE T lattice_generic_G(const KiwiKernelTable* K, T q0, int j, int k, T a, T a2, T phi, T sinp,
+                                      T cosp) {
     const T den = a2 + cosp * cosp, iden = 1.0 / den;
     const T ua = sinp * sqrt(iden), u = a * ua;
     const T iomu2 = den / (cosp * cosp * (1.0 + a2));
@@ -600,30 +601,30 @@ KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0
 // lattice_corner).  r0, a1, a2 > 0.  (lattice_generic_point evaluates a point's three walls together; it
 // is the adjoint's form: in double it measured slower than three corners and less accurate in low-density
 // cells of the generic fixtures.)
-KIWI_LAT double lattice_generic_corner(const KiwiKernelTable* K, double H, double r0,
-                                                               double a1, double a2, const double* rec1,
-                                                               const double* rec2) {
-    const double ir0 = 1.0 / r0, irr = 1.0 / sqrt(a1 * a1 + a2 * a2);
-    const double q0 = r0 / H;
-    const int j = generic_region(K, q0);
+template <class T>
+KIWI_LAT T lattice_generic_corner(const KiwiKernelTable* K, double H, T r0, T a1, T a2, const double* rec1,
+                                  const double* rec2) {
+    const T ir0 = 1.0 / r0, irr = 1.0 / sqrt(a1 * a1 + a2 * a2);
+    const T q0 = r0 / H;
+    const int j = generic_region(K, lat_value(q0));
     // the smaller angle from one atan2 with selected operands (no warp split over two calls), the larger
     // its complement
     const bool lo = a2 <= a1;
-    const double tq = atan2(lo ? a2 : a1, lo ? a1 : a2), tc = 0.5 * kPi - tq;
-    const double pa = lo ? tq : tc, pb = lo ? tc : tq;
-    double sum = 0.0;
+    const T tq = atan2(lo ? a2 : a1, lo ? a1 : a2), tc = 0.5 * kPi - tq;
+    const T pa = lo ? tq : tc, pb = lo ? tc : tq;
+    T sum = 0.0;
 #pragma unroll 1
     for (int v = 0; v < 2; ++v) {
         const double* rec = v ? rec2 : rec1;
         const int packed = (int)rec[0];
         const int nseg = packed & 7, k0 = packed >> 3;
         if (nseg == 0) continue;
-        const double R0 = v ? a2 : a1, t = v ? a1 : a2, phi = v ? pb : pa;
-        const double a = R0 * ir0;
+        const T R0 = v ? a2 : a1, t = v ? a1 : a2, phi = v ? pb : pa;
+        const T a = R0 * ir0;
         int s = 0;
         while (s + 1 < nseg && phi > rec[1 + s]) ++s;
-        const double G = lattice_generic_G(K, q0, j, k0 + s, a, a * a, phi, t * irr, R0 * irr);
-        sum += (s > 0 ? rec[3 + s] : 0.0) + G;
+        const T G = lattice_generic_G(K, q0, j, k0 + s, a, a * a, phi, t * irr, R0 * irr);
+        sum += (s > 0 ? T(rec[3 + s]) : T(0.0)) + G;
     }
     return sum;
 }

@@ -23,7 +23,10 @@
 
 namespace kiwi_b200 {
 
-constexpr int kLatThreads = 256;
+#ifndef KIWI_LAT_THREADS
+#define KIWI_LAT_THREADS 256
+#endif
+constexpr int kLatThreads = KIWI_LAT_THREADS;
 constexpr int kLatCellsPerThread = kTileCells / kLatThreads;
 static_assert(kTileCells % kLatThreads == 0, "tile cells must split evenly over the threads");
 // Chunk capacities (defaults sized for two CTAs per SM; a full 8^3 particle box has 729 lattice points and
@@ -38,9 +41,11 @@ constexpr int kLatPtCap = KIWI_LAT_PT_CAP;  // lattice points per chunk
 constexpr int kLatECap2 = KIWI_LAT_E_CAP;   // cubic edge tiers per chunk
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed point-list entries");
 static_assert(kLatECap2 <= 2048 && kLatGenECap <= 2048, "packed edge-pair entries (11-bit slots)");
-constexpr size_t kLatDynSmem = sizeof(double) * (2 * kLatECap2 + kLatPtCap);
-constexpr size_t kLatGenDynSmem = sizeof(double) * (kLatGenERec * kLatGenECap + kLatPtCap);
-constexpr size_t kLatTabDynSmem = sizeof(double) * kLatPtCap;
+// dynamic shared memory: the owned cells' sums (4 per cell), then the chunk's edge tiers and octant values
+constexpr size_t kLatAccSmem = sizeof(double) * 4 * kTileCells;
+constexpr size_t kLatDynSmem = kLatAccSmem + sizeof(double) * (2 * kLatECap2 + kLatPtCap);
+constexpr size_t kLatGenDynSmem = kLatAccSmem + sizeof(double) * (kLatGenERec * kLatGenECap + kLatPtCap);
+constexpr size_t kLatTabDynSmem = kLatAccSmem + sizeof(double) * kLatPtCap;
 
 // The six edge tiers of a lattice point (slots of the chunk's D2 / D3 tables in PointEdge order), read where
 // lattice_point uses them, as the real type T it is evaluated in.
@@ -89,10 +94,14 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     __shared__ uint32_t s_hlist[(GENERIC || TAB) ? 1 : kLatECap2 / 2];
     extern __shared__ double s_dyn[];
     constexpr int kECap = GENERIC ? kLatGenECap : (TAB ? 0 : kLatECap2);
-    double* s_D2 = s_dyn;
-    double* s_D3 = s_dyn + kLatECap2;
-    double* s_E = s_dyn;  // generic edge records
-    double* s_T = s_dyn + (GENERIC ? kLatGenERec * kLatGenECap : (TAB ? 0 : 2 * kLatECap2));
+    // the owned cells' sums M, Px, Py, Pz: each thread's own entries (no sharing, no barrier), held in
+    // registers only while (C) adds a chunk -- the point phase needs the registers
+    double* s_acc = s_dyn;
+    double* s_chunk = s_dyn + 4 * kTileCells;
+    double* s_D2 = s_chunk;
+    double* s_D3 = s_chunk + kLatECap2;
+    double* s_E = s_chunk;  // generic edge records
+    double* s_T = s_chunk + (GENERIC ? kLatGenERec * kLatGenECap : (TAB ? 0 : 2 * kLatECap2));
 
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
@@ -109,9 +118,11 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         if (l < kTileX) s_cc[a][l] = cell_centre(mn, b0 + l, d);
     }
 
-    double acc[kLatCellsPerThread][4];
 #pragma unroll
-    for (int c = 0; c < kLatCellsPerThread; ++c) acc[c][0] = acc[c][1] = acc[c][2] = acc[c][3] = 0.0;
+    for (int c = 0; c < kLatCellsPerThread; ++c) {
+        const int li = threadIdx.x + c * kLatThreads;
+        s_acc[li] = s_acc[kTileCells + li] = s_acc[2 * kTileCells + li] = s_acc[3 * kTileCells + li] = 0.0;
+    }
     // work counters: 32-bit per thread (a chunk adds at most a few hundred to any of them), flushed to the
     // 64-bit totals every 2^16 chunks and at the end
     unsigned n_bbox = 0, n_sphere = 0, n_eval = 0, n_neg = 0, n_warn = 0;
@@ -395,6 +406,8 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const int li = threadIdx.x + c * kLatThreads;
             const int lx = li / (kTileZ * kTileY), ly = (li / kTileZ) % kTileY, lz = li % kTileZ;
             const int gx = bx + lx, gy = by + ly, gz = bz + lz;
+            double a0 = s_acc[li], a1 = s_acc[kTileCells + li];
+            double a2 = s_acc[2 * kTileCells + li], a3 = s_acc[3 * kTileCells + li];
             for (int j = 0; j < np; ++j) {
                 const int i = gx - s_lo[j][0], jj = gy - s_lo[j][1], k = gz - s_lo[j][2];
                 if (i < 0 || jj < 0 || k < 0 || i >= s_dim[j][0] || jj >= s_dim[j][1] || k >= s_dim[j][2]) continue;
@@ -420,11 +433,15 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 }
                 if (msum == 0.0) continue;
                 const double mm = msum * s_m[j];
-                acc[c][0] += mm;
-                acc[c][1] += mm * s_vx[j];
-                acc[c][2] += mm * s_vy[j];
-                acc[c][3] += mm * s_vz[j];
+                a0 += mm;
+                a1 += mm * s_vx[j];
+                a2 += mm * s_vy[j];
+                a3 += mm * s_vz[j];
             }
+            s_acc[li] = a0;
+            s_acc[kTileCells + li] = a1;
+            s_acc[2 * kTileCells + li] = a2;
+            s_acc[3 * kTileCells + li] = a3;
         }
         __syncthreads();
         pos += np;
@@ -442,17 +459,18 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         const int ix = bx + li / (kTileZ * kTileY), iy = by + (li / kTileZ) % kTileY, iz = bz + li % kTileZ;
         if (ix >= g.nx || iy >= g.ny || iz >= g.nz) continue;
         const int64_t i3 = ((int64_t)ix * g.ny + iy) * g.nz + iz;
-        const double M = acc[c][0];
+        const double M = s_acc[li];
         if (out.density) out.density[i3] = M / g.cell_volume;
         const bool has = M > 0.0;
-        if (out.vx) out.vx[i3] = has ? acc[c][1] / M : mvx;
-        if (out.vy) out.vy[i3] = has ? acc[c][2] / M : mvy;
-        if (out.vz) out.vz[i3] = has ? acc[c][3] / M : mvz;
+        const double P1 = s_acc[kTileCells + li], P2 = s_acc[2 * kTileCells + li], P3 = s_acc[3 * kTileCells + li];
+        if (out.vx) out.vx[i3] = has ? P1 / M : mvx;
+        if (out.vy) out.vy[i3] = has ? P2 / M : mvy;
+        if (out.vz) out.vz[i3] = has ? P3 / M : mvz;
         if (out.raw4) {
             out.raw4[i3] = M;
-            out.raw4[ncell + i3] = acc[c][1];
-            out.raw4[2 * ncell + i3] = acc[c][2];
-            out.raw4[3 * ncell + i3] = acc[c][3];
+            out.raw4[ncell + i3] = P1;
+            out.raw4[2 * ncell + i3] = P2;
+            out.raw4[3 * ncell + i3] = P3;
         }
     }
     flush();

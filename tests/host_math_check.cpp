@@ -8,6 +8,7 @@
 #include "../kiwi_b200/csrc/dual.cuh"
 #include "../kiwi_b200/csrc/lattice_math.cuh"
 #include "../kiwi_b200/csrc/lattice_dual.cuh"
+#include "../kiwi_b200/csrc/f32.cuh"
 
 using namespace kiwi_b200;
 
@@ -113,5 +114,53 @@ void hm_lattice_generic_point_grad(int kernel, double H, double ax, double ay, d
     const Dual3 f = lattice_generic_point(K, H, X, Y, Z, rd);
     out4[0] = f.v;
     for (int k = 0; k < 3; ++k) out4[1 + k] = f.d[k];
+}
+
+// FP32 instances (the FP32 type of f32.cuh): a cubic lattice point with FP32 edge pairs, and a generic
+// lattice point as three FP32 corners over FP32 edge records -- for measuring what FP32 does to the
+// octant values.
+double hm_lattice_point_f32(double h, double ax, double ay, double az) {
+    const F32 H(h), IH(1.0 / h);
+    const F32 a[3] = {F32(ax), F32(ay), F32(az)};
+    PointEdges<F32> E;
+    // PointEdge order xy, xz, yx, yz, zx, zy: (wall, edge line) = (p, q) pairs of axes
+    const int pw[6] = {0, 0, 1, 1, 2, 2}, pq[6] = {1, 2, 0, 2, 0, 1};
+    for (int e = 0; e < 6; ++e) {
+        const F32 p = a[pw[e]], q = a[pq[e]];
+        if ((double)(p.v * p.v + q.v * q.v) <= 4.0 * h * h) {
+            LatticeEdgeT<F32> ab, ba;
+            lattice_edge_pair(H, IH, p, q, ab, ba);
+            E.d2[e] = ab.D2;
+            E.d3[e] = ab.D3;
+        } else {
+            E.d2[e] = E.d3[e] = F32(0.0);
+        }
+    }
+    return (double)lattice_point(H, IH, a[0], a[1], a[2], E).v;
+}
+
+struct GenEdgeWriterF32 {
+    double* rec;
+    void set_packed(double v) { rec[0] = v; }
+    void set_segment(int s, F32 phi_end, F32 off) {
+        rec[1 + s] = (double)phi_end.v;
+        rec[4 + s] = (double)off.v;
+    }
+};
+
+double hm_lattice_generic_point_f32(int kernel, double H, double ax, double ay, double az) {
+    const KiwiKernelTable* K = &kiwi_kernel_tables[kernel];
+    const F32 a[3] = {F32(ax), F32(ay), F32(az)};
+    double recs[6][kLatGenERec];
+    const int pw[6] = {0, 0, 1, 1, 2, 2}, pq[6] = {1, 2, 0, 2, 0, 1};
+    for (int e = 0; e < 6; ++e) {
+        for (int i = 0; i < kLatGenERec; ++i) recs[e][i] = 0.0;
+        GenEdgeWriterF32 w{recs[e]};
+        lattice_generic_edge_t(K, H, a[pw[e]], a[pq[e]], w);
+    }
+    const F32 f = lattice_generic_corner(K, H, a[0], a[1], a[2], recs[0], recs[1]) +
+                  lattice_generic_corner(K, H, a[1], a[0], a[2], recs[2], recs[3]) +
+                  lattice_generic_corner(K, H, a[2], a[0], a[1], recs[4], recs[5]);
+    return (double)f.v;
 }
 }
