@@ -88,6 +88,10 @@ struct SmemDualEdges {
     int slot[6];
     __device__ __forceinline__ Dual3 D2(int e) const { return load_dual(rec + kAdjERec * slot[e]); }
     __device__ __forceinline__ Dual3 D3(int e) const { return load_dual(rec + kAdjERec * slot[e] + 4); }
+    __device__ __forceinline__ void leg_angles(int, const Dual3& a1, const Dual3& ia1, const Dual3& a2,
+                                               const Dual3& ia2, Dual3& pa, Dual3& pb) const {
+        kiwi_b200::leg_angles(a1, ia1, a2, ia2, pa, pb);
+    }
 };
 
 __device__ __forceinline__ unsigned long long block_count(unsigned long long v) {

@@ -183,11 +183,11 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
     if (form == KIWI_FP64 || form == KIWI_FP64_REFERENCE_ORDER) {
         KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl, out, d_stats, full_box, form == KIWI_FP64_REFERENCE_ORDER));
     } else if (form == KIWI_FP32_MIXED) {
-        if (!kc.cubic)
-            return set_err(ctx, KIWI_ERR_UNSUPPORTED,
-                           "the FP32-mixed form is available for the cubic spline kernel with support 2h");
         if (full_box) return set_err(ctx, KIWI_ERR_ARG, "KIWI_FULL_BOX is available with the FP64 forms only");
         const bool guarantee = (precision & KIWI_FP32_GUARANTEE) != 0;
+        if (guarantee && !kc.cubic)
+            return set_err(ctx, KIWI_ERR_UNSUPPORTED,
+                           "KIWI_FP32_GUARANTEE is available for the cubic spline kernel with support 2h");
         const int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
         double *cerr = nullptr, *cmass = nullptr;
         if (guarantee) {
@@ -197,7 +197,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         if (guarantee)
             KIWI_TRY(mixed_cart_gather(ctx, g, P, tl, out, cerr, cmass, d_stats));
         else
-            KIWI_TRY(lattice_mixed_gather(ctx, g, P, tl, out, d_stats));
+            KIWI_TRY(lattice_mixed_gather(ctx, g, P, kc, tl, out, d_stats));
         if (guarantee) {
             int32_t* map = nullptr;
             int64_t* d_nmap = nullptr;

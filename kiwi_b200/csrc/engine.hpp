@@ -139,8 +139,8 @@ int lattice_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, 
                         const TileLists& tl, const CartOutputs& out, DevStats* d_stats, bool full_box);
 // The FP32-mixed form of the cubic lattice gather (FP32 tiers with FP64 islands, FP64 assembly); the number
 // of lattice points evaluated in FP64 (islands) is added to d_stats->fp64_fallback.
-int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const TileLists& tl,
-                         const CartOutputs& out, DevStats* d_stats);
+int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
+                         const TileLists& tl, const CartOutputs& out, DevStats* d_stats);
 int lattice_batch_prepare(KiwiCtx* ctx);
 int lattice_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
                          const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,

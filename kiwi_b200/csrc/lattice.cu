@@ -73,6 +73,16 @@ __global__ void __launch_bounds__(kLatThreads, kLatGenMinBlocks) k_cart_lattice_
     lattice_tile<true, true>(g, P, list, range, t, t, out, st, &c_tables[kernel]);
 }
 
+// The FP32-mixed form of the generic lattice kernel: edge records and vertex tiers in FP32 (FP64 islands
+// where a plane lies within 1e-3 h of the particle), records, cell assembly and per-cell sums in FP64.
+__global__ void __launch_bounds__(kLatThreads, kLatGenMinBlocks)
+    k_cart_lattice_generic_mixed(CartGeom g, DevParticles P, int kernel, const uint32_t* __restrict__ list,
+                                 const int64_t* __restrict__ range, const int32_t* __restrict__ tile_map,
+                                 CartOutputs out, DevStats* __restrict__ st) {
+    const int64_t t = tile_map ? (int64_t)tile_map[blockIdx.x] : (int64_t)blockIdx.x;
+    lattice_tile<true, true, false, true>(g, P, list, range, t, t, out, st, &c_tables[kernel]);
+}
+
 // The tiles of a batch of grids, one persistent launch per lattice family, or one for both
 // (kBatchFamilyLatticeMerged: each tile takes its item's body): each CTA takes the next of the launch's
 // tiles (order[w]) from the work counter and runs the same tile body as the single-grid kernel, so every
@@ -132,10 +142,21 @@ int lattice_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, 
     return KIWI_OK;
 }
 
-int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const TileLists& tl,
-                         const CartOutputs& out, DevStats* d_stats) {
+int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, const KernelChoice& k,
+                         const TileLists& tl, const CartOutputs& out, DevStats* d_stats) {
     if (tl.ntiles <= 0 || (tl.map && tl.nmap <= 0)) return KIWI_OK;
     const dim3 grid((unsigned)(tl.map ? tl.nmap : tl.ntiles));
+    if (!k.cubic) {
+        KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_generic_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kLatGenDynSmem));
+        KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_generic_mixed,
+                                            cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            (int)cudaSharedmemCarveoutMaxShared));
+        k_cart_lattice_generic_mixed<<<grid, kLatThreads, kLatGenDynSmem, ctx->stream>>>(
+            g, P, k.kernel, tl.list, tl.range, tl.map, out, d_stats);
+        KIWI_LAUNCHED(ctx);
+        return KIWI_OK;
+    }
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kLatDynSmem));
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_mixed, cudaFuncAttributePreferredSharedMemoryCarveout,

@@ -272,6 +272,10 @@ struct PointEdges {
     T d2[6], d3[6];
     KIWI_HD T D2(int e) const { return d2[e]; }
     KIWI_HD T D3(int e) const { return d3[e]; }
+    // the in-plane angles of the wall whose legs lie along edge pair e's two axes (leg_angles)
+    KIWI_HD void leg_angles(int e, T a1, T ia1, T a2, T ia2, T& pa, T& pb) const {
+        kiwi_b200::leg_angles(a1, ia1, a2, ia2, pa, pb);
+    }
 };
 
 // One vertex pyramid of the series inside 2h (lattice_corner's loop body): legs `leg` (towards the edge line
@@ -293,13 +297,15 @@ KIWI_LAT T point_pyramid(const LatticeWall<T>& w, bool inner, T b1, T b2, T a, T
 // One wall's corner value inside 2h (lattice_corner) from the point's shared quantities: wall distance r0
 // and its reciprocal, in-plane legs a1 (edge tier E.D2(ea)) and a2 (E.D2(eb)) with reciprocals,
 // s2 = a1^2 + a2^2, r and its reciprocal, the log terms of u = a2 / r (first pyramid) and u = a1 / r
-// (second), their 1 / (1 - u^2), and the pair's I1 sum atan(r0 r / (a1 a2)) (point_angles).
+// (second), their 1 / (1 - u^2), and the pair's I1 sum atan(r0 r / (a1 a2)) (point_angles).  The in-plane
+// angles depend on a1 and a2 alone, so the Edges reader may hold them per edge pair: ec is the pair (the
+// edge line along a2 at a1) whose angles they are.
 template <class T, class Edges>
 KIWI_LAT T point_wall(T h, T ih, bool inner, T r0, T ir0, T a1, T ia1, T a2, T ia2, T s2, T ir, T log_a2, T iom_a2,
-                      T log_a1, T iom_a1, T I1s, const Edges& E, int ea, int eb) {
+                      T log_a1, T iom_a1, T I1s, const Edges& E, int ea, int eb, int ec) {
     const LatticeWall<T> w = lattice_wall(ih, h, ir0, r0);
     T pa, pb;
-    leg_angles(a1, ia1, a2, ia2, pa, pb);
+    E.leg_angles(ec, a1, ia1, a2, ia2, pa, pb);
     const T b1 = inner ? wall_b1_in(w) : 0.0;
     const T b2 = r0 > h ? wall_b2_mid(w) : wall_b2_in(w);
     T sum = point_pyramid(w, inner, b1, b2, a1 * ir0, a2 * ir, a2 * ia1, s2 * ia1 * ia1, iom_a2, log_a2, pa,
@@ -370,9 +376,12 @@ KIWI_LAT_CORNER T lattice_point(T h, T ih, T ax, T ay, T az, const Edges& E) {
     const T Ly = log1p(2.0 * uy * (1.0 + uy) * iomy);
     const T Lz = log1p(2.0 * uz * (1.0 + uz) * iomz);
     const bool inner = r2 < h * h;
-    T s = point_wall(h, ih, inner, ax, iax, ay, iay, az, iaz, syz, ir, Lz, iomz, Ly, iomy, Jx, E, kEdgeXY, kEdgeXZ);
-    s += point_wall(h, ih, inner, ay, iay, ax, iax, az, iaz, sxz, ir, Lz, iomz, Lx, iomx, Jy, E, kEdgeYX, kEdgeYZ);
-    s += point_wall(h, ih, inner, az, iaz, ax, iax, ay, iay, sxy, ir, Ly, iomy, Lx, iomx, Jz, E, kEdgeZX, kEdgeZY);
+    T s = point_wall(h, ih, inner, ax, iax, ay, iay, az, iaz, syz, ir, Lz, iomz, Ly, iomy, Jx, E, kEdgeXY, kEdgeXZ,
+                     kEdgeYZ);
+    s += point_wall(h, ih, inner, ay, iay, ax, iax, az, iaz, sxz, ir, Lz, iomz, Lx, iomx, Jy, E, kEdgeYX, kEdgeYZ,
+                    kEdgeXZ);
+    s += point_wall(h, ih, inner, az, iaz, ax, iax, ay, iay, sxy, ir, Ly, iomy, Lx, iomx, Jz, E, kEdgeZX, kEdgeZY,
+                    kEdgeXY);
     return s;
 }
 
@@ -575,16 +584,19 @@ KIWI_LAT void lattice_generic_edge_t(const KiwiKernelTable* K, double H, T r0, T
 
 // The double record: [0] = nseg + 8 x first region, [1..3] = phi_end of segments 0..2, [4..6] = offset of
 // segments 1..3.
+// (The record is stored in doubles whatever type the tiers were evaluated in.)
 struct GenEdgeWriter {
     double* rec;
     KIWI_HD void set_packed(double v) { rec[0] = v; }
-    KIWI_HD void set_segment(int s, double phi_end, double off) {
-        rec[1 + s] = phi_end;
-        rec[4 + s] = off;
+    template <class T>
+    KIWI_HD void set_segment(int s, T phi_end, T off) {
+        rec[1 + s] = lat_value(phi_end);
+        rec[4 + s] = lat_value(off);
     }
 };
 
-KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, double r0, double R0, double* rec) {
+template <class T>
+KIWI_LAT void lattice_generic_edge(const KiwiKernelTable* K, double H, T r0, T R0, double* rec) {
     for (int i = 0; i < kLatGenERec; ++i) rec[i] = 0.0;
     GenEdgeWriter w{rec};
     lattice_generic_edge_t(K, H, r0, R0, w);

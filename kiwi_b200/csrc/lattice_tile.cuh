@@ -43,7 +43,7 @@ static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "p
 static_assert(kLatECap2 <= 2048 && kLatGenECap <= 2048, "packed edge-pair entries (11-bit slots)");
 // dynamic shared memory: the owned cells' sums (4 per cell), then the chunk's edge tiers and octant values
 constexpr size_t kLatAccSmem = sizeof(double) * 4 * kTileCells;
-constexpr size_t kLatDynSmem = kLatAccSmem + sizeof(double) * (2 * kLatECap2 + kLatPtCap);
+constexpr size_t kLatDynSmem = kLatAccSmem + sizeof(double) * (3 * kLatECap2 + kLatPtCap);
 constexpr size_t kLatGenDynSmem = kLatAccSmem + sizeof(double) * (kLatGenERec * kLatGenECap + kLatPtCap);
 constexpr size_t kLatTabDynSmem = kLatAccSmem + sizeof(double) * kLatPtCap;
 
@@ -53,9 +53,23 @@ template <class T>
 struct SmemPointEdges {
     const double* d2;
     const double* d3;
+    const double* ang;  // per edge pair (at its ab slot): the smaller in-plane angle, or < 0 if not formed
     int slot[6];
     __device__ __forceinline__ T D2(int e) const { return T(d2[slot[e]]); }
     __device__ __forceinline__ T D3(int e) const { return T(d3[slot[e]]); }
+    // leg_angles from the pair's stored angle atan(min(a1, a2) / max(a1, a2)); a pair that (A2) did not
+    // evaluate (its legs' rounded square sum beyond 2h while the point's is within) forms it here
+    __device__ __forceinline__ void leg_angles(int e, T a1, T ia1, T a2, T ia2, T& pa, T& pb) const {
+        const double t = ang[slot[e]];
+        if (t < 0.0) {
+            kiwi_b200::leg_angles(a1, ia1, a2, ia2, pa, pb);
+            return;
+        }
+        const bool lo = a2 <= a1;
+        const T tq = T(t), tc = 0.5 * kPi - tq;
+        pa = lo ? tq : tc;
+        pb = lo ? tc : tq;
+    }
 };
 
 // FP32-mixed form: planes closer to the particle than this fraction of h are evaluated in FP64 (the wall
@@ -102,6 +116,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     double* s_D3 = s_chunk + kLatECap2;
     double* s_E = s_chunk;  // generic edge records
     double* s_T = s_chunk + (GENERIC ? kLatGenERec * kLatGenECap : (TAB ? 0 : 2 * kLatECap2));
+    double* s_A = s_T + kLatPtCap;  // cubic: each edge pair's smaller in-plane angle (at its ab slot)
 
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
@@ -227,8 +242,13 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     const double vp = fabs(s_pl[a][la + pi] - pa), vq = fabs(s_pl[b][lb + qi] - pb);
                     if (GENERIC) {
                         const double H = mul_rn(sup_in_h, s_h[j]);
-                        lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
-                        lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+                        if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * s_h[j]) {
+                            lattice_generic_edge(K, H, F32(vp), F32(vq), s_E + kLatGenERec * sab);
+                            lattice_generic_edge(K, H, F32(vq), F32(vp), s_E + kLatGenERec * sba);
+                        } else {
+                            lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
+                            lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+                        }
                         n_ei += 2;
                     } else {
                         const double h2 = s_h[j] * s_h[j];
@@ -244,6 +264,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                             n_eo += 2;
                             s_D2[sab] = s_D3[sab] = 0.0;
                             s_D2[sba] = s_D3[sba] = 0.0;
+                            s_A[sab] = -1.0;
                         }
                     }
                 }
@@ -321,7 +342,11 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)(rec >> 22);
                 LatticeEdge e_pq, e_qp;
                 const double vp = s_D2[sab], vq = s_D3[sab];
-                if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * s_h[j]) {
+                // the pair's smaller in-plane angle (FP64 in every form: FP64 island points read it too),
+                // which the walls with legs along a and b read
+                const double vmin = fmin(vp, vq), vmax = fmax(vp, vq);
+                s_A[sab] = atan(vmin / vmax);
+                if (MIXED && vmin >= kMixedIslandFrac * s_h[j]) {
                     LatticeEdgeT<F32> f_pq, f_qp;
                     lattice_edge_pair(F32(s_h[j]), F32(s_ih[j]), F32(vp), F32(vq), f_pq, f_qp);
                     e_pq = {(double)f_pq.D2.v, (double)f_pq.D3.v};
@@ -380,15 +405,26 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     const int ezx = eb + 2 * nxy + nxz + nyz + k * n0 + i, ezy = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
                     if (GENERIC) {
                         const double H = mul_rn(sup_in_h, s_h[jp]);
-                        f = lattice_generic_corner(K, H, ax, ay, az, s_E + kLatGenERec * exy, s_E + kLatGenERec * exz) +
-                            lattice_generic_corner(K, H, ay, ax, az, s_E + kLatGenERec * eyx, s_E + kLatGenERec * eyz) +
-                            lattice_generic_corner(K, H, az, ax, ay, s_E + kLatGenERec * ezx, s_E + kLatGenERec * ezy);
+                        const double *rxy = s_E + kLatGenERec * exy, *rxz = s_E + kLatGenERec * exz;
+                        const double *ryx = s_E + kLatGenERec * eyx, *ryz = s_E + kLatGenERec * eyz;
+                        const double *rzx = s_E + kLatGenERec * ezx, *rzy = s_E + kLatGenERec * ezy;
+                        if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * s_h[jp]) {
+                            const F32 fx(ax), fy(ay), fz(az);
+                            f = (double)(lattice_generic_corner(K, H, fx, fy, fz, rxy, rxz) +
+                                         lattice_generic_corner(K, H, fy, fx, fz, ryx, ryz) +
+                                         lattice_generic_corner(K, H, fz, fx, fy, rzx, rzy)).v;
+                        } else {
+                            f = lattice_generic_corner(K, H, ax, ay, az, rxy, rxz) +
+                                lattice_generic_corner(K, H, ay, ax, az, ryx, ryz) +
+                                lattice_generic_corner(K, H, az, ax, ay, rzx, rzy);
+                            if (MIXED) ++n_island;
+                        }
                     } else {
                         if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * s_h[jp]) {
-                            const SmemPointEdges<F32> E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};
+                            const SmemPointEdges<F32> E{s_D2, s_D3, s_A, {exy, exz, eyx, eyz, ezx, ezy}};
                             f = (double)lattice_point(F32(s_h[jp]), F32(s_ih[jp]), F32(ax), F32(ay), F32(az), E).v;
                         } else {
-                            const SmemPointEdges<double> E{s_D2, s_D3, {exy, exz, eyx, eyz, ezx, ezy}};
+                            const SmemPointEdges<double> E{s_D2, s_D3, s_A, {exy, exz, eyx, eyz, ezx, ezy}};
                             f = lattice_point(s_h[jp], s_ih[jp], ax, ay, az, E);
                             if (MIXED) ++n_island;
                         }

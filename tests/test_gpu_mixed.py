@@ -102,7 +102,33 @@ def test_fp32_deterministic_and_edge_cases(kiwi, ctx):
     r = kiwi.sph_to_grid(P0, b, (4, 4, 4), ctx=ctx, precision="fp32_mixed_guaranteed")
     assert np.all(r.density == 0) and r.stats["fp64_tiles"] == 0
     with pytest.raises(kiwi.KiwiError):
-        kiwi.sph_to_grid(P, b, (8, 8, 8), ctx=ctx, precision="fp32_mixed",
+        kiwi.sph_to_grid(P, b, (8, 8, 8), ctx=ctx, precision="fp32_mixed_guaranteed",
                          kernel=kiwi.make_kernel_integrator("wendland_c4"))
     with pytest.raises(kiwi.KiwiError):
         kiwi.sph_to_grid(P, b, (8, 8, 8), ctx=ctx, precision="fp32_mixed", full_box=True)
+
+
+GENERIC = [os.path.join(ROOT, "tests", "golden", f"grid_{k}.npz")
+           for k in ("generic_m4", "quartic_spline", "quintic_spline", "wendland_c2", "wendland_c4", "wendland_c6")]
+
+
+@pytest.mark.parametrize("fn", GENERIC, ids=[os.path.basename(f)[5:-4] for f in GENERIC])
+def test_fp32_generic_error_level_against_truth(kiwi, ctx, fn):
+    """The FP32-mixed form of the generic kernels (edge records and vertex tiers in FP32 over the kernel's
+    tables, FP64 islands and assembly): its error against the exact integral, per density band, with the
+    FP64 form's beside it; deterministic; total mass to FP32-term accuracy."""
+    d, P = _load(fn)
+    k = int(d["kernel_index"])
+    ki = kiwi.KernelIntegrator(kernel=k, support_in_h=0.0, generic_path=bool(d["generic"]) and k == 0)
+    r32 = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=ki, raw=True, ctx=ctx, precision="fp32_mixed")
+    r32b = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=ki, raw=True, ctx=ctx, precision="fp32_mixed")
+    r64 = kiwi.sph_to_grid(P, d["bounds"], tuple(d["shape"]), kernel=ki, ctx=ctx, precision="fp64")
+    assert np.array_equal(r32.raw, r32b.raw)
+    truth = d["truth_raw"][0] / _vol(d)
+    b32, b64 = band_max_rel(r32.density, truth), band_max_rel(r64.density, truth)
+    mass = abs(r32.density.sum() - r64.density.sum()) / r64.density.sum()
+    print(f"{os.path.basename(fn)}: FP32-mixed max rel err by band {b32} (FP64 form {b64}); "
+          f"total mass vs FP64 {mass:.2e}; FP64 island points {r32.stats['fp64_fallback']}")
+    assert np.all(np.isfinite(r32.density)) and r32.density.min() >= 0.0
+    assert b32[0] <= 1e-2
+    assert mass <= 1e-5
