@@ -113,6 +113,11 @@ void kiwi_ctx_destroy(KiwiCtx* ctx);
 const char* kiwi_last_error(const KiwiCtx* ctx); /* message of the last failed call on ctx */
 void* kiwi_ctx_stream(KiwiCtx* ctx);             /* the context's cudaStream_t */
 int kiwi_ctx_synchronize(KiwiCtx* ctx);
+/* Voronoi maps on this context: enable = 1 (the default) evaluates every face value once per particle
+ * through per-(pair, face) tables (12 bytes per face of every visited cell; a map whose tables would
+ * exceed 48 GB runs without them); enable = 0 runs one launch that evaluates a face shared by two visited
+ * cells on both sides.  Both give the same results bit for bit.  No counterpart in the reference. */
+int kiwi_ctx_set_voronoi_face_tables(KiwiCtx* ctx, int enable);
 const char* kiwi_version(void);
 /* Measured FP64 FMA throughput of the context's GPU in TFLOP/s (a short probe kernel).  No counterpart in
  * the reference: it provides the roofline denominator of the FP64 cell-integral kernels. */

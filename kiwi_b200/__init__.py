@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH):
     L.kiwi_ctx_stream.restype = C.c_void_p
     L.kiwi_ctx_stream.argtypes = [C.c_void_p]
     L.kiwi_ctx_synchronize.argtypes = [C.c_void_p]
+    L.kiwi_ctx_set_voronoi_face_tables.argtypes = [C.c_void_p, C.c_int]
     L.kiwi_kernel_index.argtypes = [C.c_char_p]
     L.kiwi_kernel_info.argtypes = [C.c_int, _dp]
     L.kiwi_full_integral_batch.argtypes = [C.c_void_p, C.c_int, C.c_int64, _dp, _dp, _dp, _dp, _dp]
@@ -203,6 +204,11 @@ class Context:
 
     def synchronize(self):
         self.check(self._L.kiwi_ctx_synchronize(self._h))
+
+    def set_voronoi_face_tables(self, enable: bool):
+        """Voronoi maps: each face value evaluated once through per-(pair, face) tables (True, the default)
+        or in one launch that evaluates a shared face on both sides (False); the results are equal."""
+        self.check(self._L.kiwi_ctx_set_voronoi_face_tables(self._h, int(bool(enable))))
 
     def close(self):
         if getattr(self, "_h", None):

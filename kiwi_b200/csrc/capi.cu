@@ -317,6 +317,12 @@ int kiwi_ctx_synchronize(KiwiCtx* ctx) {
     return KIWI_OK;
 }
 
+int kiwi_ctx_set_voronoi_face_tables(KiwiCtx* ctx, int enable) {
+    KIWI_TRY(check_ctx(ctx));
+    ctx->face_tables = enable != 0;
+    return KIWI_OK;
+}
+
 int kiwi_measure_fp64_peak(KiwiCtx* ctx, double* tflops) {
     KIWI_TRY(check_ctx(ctx));
     if (!tflops) return set_err(ctx, KIWI_ERR_ARG, "tflops is null");

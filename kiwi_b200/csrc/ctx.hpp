@@ -37,6 +37,8 @@ struct KiwiCtx {
     // tab_bytes of device memory).
     kiwi_b200::TabDev tab;
     size_t tab_bytes = 0;
+    // Voronoi maps: each face value evaluated once through per-(pair, face) tables (kiwi_ctx_set_voronoi_face_tables)
+    bool face_tables = true;
 };
 
 namespace kiwi_b200 {
@@ -160,7 +162,12 @@ enum ScratchSlot {
     S_FLAG_FLAGS,    // FP32-mixed guarantee: tiles to recompute
     S_FLAG_OFFS,     // FP32-mixed guarantee: compaction offsets
     S_NMAP,          // FP32-mixed guarantee: number of tiles to recompute
+    S_VOR_FCOUNT,    // Voronoi walk: per particle, the faces of its visited cells
+    S_VOR_FOFFS,     // Voronoi walk: their prefix sums
+    S_VOR_PFOFF,     // Voronoi walk: per pair, the offset of its cell's faces in the face tables
+    S_VOR_FSRC,      // Voronoi walk: per (pair, face), where its value comes from
+    S_VOR_FVAL,      // Voronoi map: per (pair, face), the face's integral
 };
-static_assert(S_NMAP < KiwiCtx::kSlots, "scratch slots");
+static_assert(S_VOR_FVAL < KiwiCtx::kSlots, "scratch slots");
 
 }  // namespace kiwi_b200

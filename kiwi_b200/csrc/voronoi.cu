@@ -71,6 +71,13 @@ __device__ __forceinline__ int marker(int64_t p, int pass) { return (int)(2 * p 
 // Cells of more than 128 faces are refused (KIWI_ERR_LIMIT).
 // Pass 1 also records per (particle, cell) the faces whose neighbour the walk processed earlier (bit i:
 // face i of the cell, first 64 faces): the reference reuses that neighbour's cached, negated face value.
+// With face tables (fcounts in pass 0; foffs, pair_foff, fsrc in pass 1), pass 0 also counts the faces of
+// each particle's visited cells, and pass 1 gives every (pair, face) its place in the face tables
+// (pair_foff: the pair's first face, the particle's cells back to back in walk order) and its source
+// (fsrc): -1 the face is evaluated for this pair; q >= 0 it takes, negated, the value of the neighbour's
+// first face towards this cell, the neighbour being the particle's q-th visited cell; -2 - e it takes the
+// value of this cell's earlier face e towards the same neighbour -- the reference's face cache
+// (src/mapping.cpp:56-93), decided here once so that the map evaluates each face value once.
 __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, DevParticles P,
                                                                     const int32_t* __restrict__ home,
                                                                     double support_in_h, int pass,
@@ -81,7 +88,11 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                                                                     const int64_t* __restrict__ offs,
                                                                     int32_t* __restrict__ pair_cells,
                                                                     unsigned long long* __restrict__ pair_mask,
-                                                                    DevStats* __restrict__ st) {
+                                                                    DevStats* __restrict__ st,
+                                                                    int64_t* __restrict__ fcounts,
+                                                                    const int64_t* __restrict__ foffs,
+                                                                    int64_t* __restrict__ pair_foff,
+                                                                    int32_t* __restrict__ fsrc) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * kBfsWarpsPerBlock + warp;
     long long* mark = mark_base + slot * C.n_cells;
@@ -97,6 +108,7 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
         if (!(h > 0.0) || k0 < 0 || k0 >= C.n_cells) {
             if (lane == 0) {
                 if (pass == 0) counts[p] = 0;
+                if (pass == 0 && fcounts) fcounts[p] = 0;
                 if (h > 0.0) ++n_unresolved;
             }
             continue;
@@ -111,6 +123,8 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
         }
         __syncwarp();
         int head = 0, tail = 1;
+        int64_t nface = 0;                                  // pass 0: this lane's share of the face count
+        int64_t fcarry = (pass == 1 && fsrc) ? foffs[p] : 0;  // pass 1: the next cell's first face
         while (head < tail) {
             if (head > C.n_cells) {  // cannot happen: each cell enters the queue once
                 n_limit += (lane == 0);
@@ -122,13 +136,15 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
             // reference, which discovers nothing).  Lane 0 then appends the candidates in (cell, face)
             // order, skipping neighbours queued meanwhile: the reference's sequential queue.
             const int batch = min(32, tail - head);
-            int64_t fa = 0;
+            int64_t fa = 0, nf = 0;
             unsigned long long cand0 = 0, cand1 = 0, earlier = 0;
             if (lane < batch) {
                 const int rank = head + lane;
                 const int32_t cell = queue[rank];
                 fa = C.face_off[cell];
                 const int64_t fz = C.face_off[cell + 1];
+                nf = fz - fa;
+                nface += nf;
                 if (fz - fa > 128) n_limit += 1;  // a cell of more than 128 faces is not supported
                 for (int64_t f = fa; f < fz && f - fa < 128; ++f) {
                     const int32_t nb = C.face_nbr[f];
@@ -156,6 +172,41 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                     pair_mask[o + rank] = earlier;
                 }
             }
+            if (pass == 1 && fsrc) {
+                // the cells' places in the face tables (a warp prefix sum in walk order) and each face's source
+                int64_t incl = nf;
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int64_t v = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                if (lane < batch) {
+                    const int rank = head + lane;
+                    const int32_t cell = queue[rank];
+                    const int64_t pf = fcarry + incl - nf;
+                    pair_foff[o + rank] = pf;
+                    for (int64_t f = fa; f < fa + nf; ++f) {
+                        const int32_t nb = C.face_nbr[f];
+                        int32_t code = -1;
+                        if (nb >= 0 && nb < C.n_cells) {
+                            const long long mv = mark[nb];
+                            if ((mv >> 32) == mk && (int)(mv & 0xffffffffLL) < rank)
+                                for (int64_t e = C.face_off[nb]; e < C.face_off[nb + 1]; ++e)
+                                    if (C.face_nbr[e] == cell) {
+                                        code = (int32_t)(mv & 0xffffffffLL);
+                                        break;
+                                    }
+                            if (code < 0)
+                                for (int64_t e = fa; e < f; ++e)
+                                    if (C.face_nbr[e] == nb) {
+                                        code = -2 - (int32_t)(e - fa);
+                                        break;
+                                    }
+                        }
+                        fsrc[pf + (f - fa)] = code;
+                    }
+                }
+                fcarry += __shfl_sync(0xffffffffu, incl, 31);
+            }
             int t = tail;
             for (int L = 0; L < batch; ++L) {
                 unsigned long long c0 = __shfl_sync(0xffffffffu, cand0, L);
@@ -179,6 +230,10 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
             tail = __shfl_sync(0xffffffffu, t, 0);
             head += batch;
             __syncwarp();
+        }
+        if (pass == 0 && fcounts) {
+            for (int d = 16; d > 0; d >>= 1) nface += __shfl_down_sync(0xffffffffu, nface, d);
+            if (lane == 0) fcounts[p] = nface;
         }
         if (pass == 0 && lane == 0) {
             counts[p] = tail;
@@ -375,6 +430,133 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
     }
 }
 
+// The face-table form of k_vor_gather, in two launches.  (a) k_vor_faces, one CTA per cell: each of the
+// cell's pairs evaluates the faces whose source is the pair itself (fsrc = -1) and stores their values.
+// (b) k_vor_sum, one CTA per cell: each pair adds its faces' values from the tables -- its own, an earlier
+// face's of its own cell, or the neighbour pair's value negated -- in face order, clamps at 0 and the
+// cell's pairs are added in particle order: the same operations on the same values as k_vor_gather, with
+// every face value evaluated once per particle instead of once per side.
+template <int MODE>
+__global__ void __launch_bounds__(kGatherThreads) k_vor_faces(VorCells C, DevParticles P, int kernel,
+                                                               double support_in_h, const TabDev tab,
+                                                               const uint32_t* __restrict__ plist,
+                                                               const int64_t* __restrict__ range,
+                                                               const int64_t* __restrict__ pair_foff,
+                                                               const int32_t* __restrict__ fsrc,
+                                                               const int64_t* __restrict__ offs,
+                                                               double* __restrict__ fval, DevStats* __restrict__ st) {
+    __shared__ double s_v[3 * kGatherVertCap];
+    const int64_t cell = blockIdx.x;
+    const int64_t f0 = C.face_off[cell], f1 = C.face_off[cell + 1];
+    const int64_t v0 = C.vert_off[f0], v1 = C.vert_off[f1];
+    const bool staged = (v1 - v0) <= kGatherVertCap;
+    if (staged)
+        for (int64_t i = threadIdx.x; i < 3 * (v1 - v0); i += kGatherThreads) s_v[i] = C.vxyz[3 * v0 + i];
+    __syncthreads();
+    const int64_t beg = range[2 * cell], end = range[2 * cell + 1];
+    unsigned n_clamp = 0;
+    for (int64_t k = beg + threadIdx.x; k < end; k += kGatherThreads) {
+        const int64_t pk = plist[k];
+        const int64_t p = pair_particle(offs, P.n, pk);
+        const double x0 = P.x[p], y0 = P.y[p], z0 = P.z[p], h = P.h[p];
+        const double radius = mul_rn(support_in_h, h);
+        const int64_t pf = pair_foff[pk];
+#pragma unroll 1
+        for (int64_t f = f0; f < f1; ++f) {
+            if (fsrc[pf + (f - f0)] != -1) continue;
+            const int nv = (int)(C.vert_off[f + 1] - C.vert_off[f]);
+            const double* verts = staged ? s_v + 3 * (C.vert_off[f] - v0) : C.vxyz + 3 * C.vert_off[f];
+            fval[pf + (f - f0)] = vor_face<MODE>(verts, nv, x0, y0, z0, h, radius, kernel, tab, &n_clamp);
+        }
+    }
+    const unsigned long long n_cl = warp_sum_u64(n_clamp);
+    if ((threadIdx.x & 31) == 0 && n_cl) atomicAdd(&st->table_clamps, n_cl);
+}
+
+__global__ void __launch_bounds__(kGatherThreads) k_vor_sum(VorCells C, DevParticles P,
+                                                             const uint32_t* __restrict__ plist,
+                                                             const int64_t* __restrict__ range,
+                                                             const int64_t* __restrict__ offs,
+                                                             const int64_t* __restrict__ pair_foff,
+                                                             const int32_t* __restrict__ fsrc,
+                                                             const double* __restrict__ fval, CartOutputs out,
+                                                             DevStats* __restrict__ st, double* __restrict__ pair_val) {
+    __shared__ double s_val[kGatherThreads], s_m[kGatherThreads], s_vx[kGatherThreads], s_vy[kGatherThreads],
+        s_vz[kGatherThreads];
+    const int64_t cell = blockIdx.x;
+    const int64_t f0 = C.face_off[cell], f1 = C.face_off[cell + 1];
+    const int64_t beg = range[2 * cell], end = range[2 * cell + 1];
+    double M = 0.0, Px = 0.0, Py = 0.0, Pz = 0.0;
+    unsigned long long n_neg = 0, n_warn = 0;
+    for (int64_t base = beg; base < end; base += kGatherThreads) {
+        const int64_t k = base + threadIdx.x;
+        double msum = 0.0;
+        if (k < end) {
+            const int64_t pk = plist[k];
+            const int64_t p = pair_particle(offs, P.n, pk);
+            const int64_t seg = offs[p];
+            const int64_t pf = pair_foff[pk];
+#pragma unroll 1
+            for (int64_t f = f0; f < f1; ++f) {
+                const int32_t code = fsrc[pf + (f - f0)];
+                if (code >= 0) {
+                    // the neighbour's first face towards this cell, from the neighbour's pair
+                    const int32_t nb = C.face_nbr[f];
+                    const int64_t g0 = C.face_off[nb], g1 = C.face_off[nb + 1];
+                    int64_t g = g0;
+                    while (g < g1 && C.face_nbr[g] != (int32_t)cell) ++g;  // found: the walk checked it
+                    if (g < g1) msum -= fval[pair_foff[seg + code] + (g - g0)];
+                } else {
+                    msum += fval[pf + (code == -1 ? f - f0 : (int64_t)(-2 - code))];
+                }
+            }
+            if (msum < 0.0) {
+                ++n_neg;
+                if (msum <= -0.01) ++n_warn;
+                msum = 0.0;
+            }
+            if (pair_val) pair_val[pk] = msum;
+            s_m[threadIdx.x] = P.m[p];
+            s_vx[threadIdx.x] = P.vx[p];
+            s_vy[threadIdx.x] = P.vy[p];
+            s_vz[threadIdx.x] = P.vz[p];
+        }
+        s_val[threadIdx.x] = msum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int cnt = (end - base < kGatherThreads) ? (int)(end - base) : kGatherThreads;
+            for (int i = 0; i < cnt; ++i) {  // in particle order, as the reference's loop adds them
+                const double mm = s_val[i] * s_m[i];
+                M += mm;
+                Px += mm * s_vx[i];
+                Py += mm * s_vy[i];
+                Pz += mm * s_vz[i];
+            }
+        }
+        __syncthreads();
+    }
+    n_neg = warp_sum_u64(n_neg);
+    n_warn = warp_sum_u64(n_warn);
+    if ((threadIdx.x & 31) == 0) {
+        if (n_neg) atomicAdd(&st->neg_clamped, n_neg);
+        if (n_warn) atomicAdd(&st->neg_warned, n_warn);
+    }
+    if (threadIdx.x == 0) {
+        const double vol = C.volume[cell];
+        if (out.density) out.density[cell] = (vol > 0.0) ? M / vol : 0.0;
+        const bool has = M > 0.0;
+        if (out.vx) out.vx[cell] = has ? Px / M : out.meanv[0];
+        if (out.vy) out.vy[cell] = has ? Py / M : out.meanv[1];
+        if (out.vz) out.vz[cell] = has ? Pz / M : out.meanv[2];
+        if (out.raw4) {
+            out.raw4[cell] = M;
+            out.raw4[C.n_cells + cell] = Px;
+            out.raw4[2 * C.n_cells + cell] = Py;
+            out.raw4[3 * C.n_cells + cell] = Pz;
+        }
+    }
+}
+
 // m_i = density * volume per cell (the forward map's cell mass, as run_inverse_mapping_test_stage forms
 // it from the mapping's rows, src/mapping.cpp:554-561).
 __global__ void k_vor_cell_mass(int64_t nc, const double* __restrict__ density, const double* __restrict__ volume,
@@ -441,17 +623,36 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_CUDA(ctx, cudaMemsetAsync(range, 0, sizeof(int64_t) * 2 * nc, ctx->stream));
 
     const double sup = kc.support_in_h;
-    // pass 0: count
+    // pass 0: count the visited cells and their faces
+    int64_t *fcounts = nullptr, *foffs = nullptr;
+    KIWI_TRY(scratch_t(ctx, S_VOR_FCOUNT, (size_t)std::max<int64_t>(n, 1), &fcounts));
+    KIWI_TRY(scratch_t(ctx, S_VOR_FOFFS, (size_t)std::max<int64_t>(n, 1) + 1, &foffs));
+    int64_t* d_ftotal = foffs + std::max<int64_t>(n, 1);
     KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
     if (n > 0) {
         k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 0, d_next, mark, queue,
-                                                                     counts, nullptr, nullptr, nullptr, d_stats);
+                                                                     counts, nullptr, nullptr, nullptr, d_stats,
+                                                                     fcounts, nullptr, nullptr, nullptr);
         KIWI_LAUNCHED(ctx);
     }
     KIWI_TRY(exclusive_scan<int64_t>(ctx, counts, n, offs, d_total));
-    int64_t total = 0;
+    KIWI_TRY(exclusive_scan<int64_t>(ctx, fcounts, n, foffs, d_ftotal));
+    int64_t total = 0, total_faces = 0;
     KIWI_CUDA(ctx, cudaMemcpyAsync(&total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    KIWI_CUDA(ctx, cudaMemcpyAsync(&total_faces, d_ftotal, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
     KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    // the face tables (each (pair, face) value evaluated once) when they fit a memory budget; else the
+    // single-launch gather, which evaluates a shared face on both sides
+    const int64_t face_bytes = total_faces * (int64_t)(sizeof(double) + sizeof(int32_t)) + total * 8;
+    const bool tables = ctx->face_tables && face_bytes <= ((int64_t)48 << 30);
+    int64_t* pair_foff = nullptr;
+    int32_t* fsrc = nullptr;
+    double* fval = nullptr;
+    if (tables && total > 0) {
+        KIWI_TRY(scratch_t(ctx, S_VOR_PFOFF, (size_t)total, &pair_foff));
+        KIWI_TRY(scratch_t(ctx, S_VOR_FSRC, (size_t)std::max<int64_t>(total_faces, 1), &fsrc));
+        KIWI_TRY(scratch_t(ctx, S_VOR_FVAL, (size_t)std::max<int64_t>(total_faces, 1), &fval));
+    }
     if (total >= (1LL << 32)) return set_err(ctx, KIWI_ERR_LIMIT, "too many (cell, particle) pairs: %lld", (long long)total);
     int32_t* pair_cells = nullptr;
     unsigned long long* pair_mask = nullptr;
@@ -467,7 +668,8 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
         // pass 1: write each particle's visited cells at its offset
         KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
         k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 1, d_next, mark, queue,
-                                                                     counts, offs, pair_cells, pair_mask, d_stats);
+                                                                     counts, offs, pair_cells, pair_mask, d_stats,
+                                                                     nullptr, foffs, pair_foff, fsrc);
         KIWI_LAUNCHED(ctx);
         k_vor_pairs<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(pair_cells, total, k0, v0);
         KIWI_LAUNCHED(ctx);
@@ -484,16 +686,32 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     if (nc > 0x7fffffffLL) return set_err(ctx, KIWI_ERR_ARG, "too many cells (%lld)", (long long)nc);
     double* pair_val = nullptr;
     if (inv) KIWI_TRY(scratch_t(ctx, S_VOR_PVAL, (size_t)std::max<int64_t>(total, 1), &pair_val));
-    if (kc.tabulated)
-        k_vor_gather<kVorTab><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
-            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
-    else if (kc.cubic)
-        k_vor_gather<kVorCubic><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
-            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
-    else
-        k_vor_gather<kVorGeneric><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
-            C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
-    KIWI_LAUNCHED(ctx);
+    if (fsrc) {
+        if (kc.tabulated)
+            k_vor_faces<kVorTab><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+                C, P, kc.kernel, sup, kc.tab, plist, range, pair_foff, fsrc, offs, fval, d_stats);
+        else if (kc.cubic)
+            k_vor_faces<kVorCubic><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+                C, P, kc.kernel, sup, kc.tab, plist, range, pair_foff, fsrc, offs, fval, d_stats);
+        else
+            k_vor_faces<kVorGeneric><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+                C, P, kc.kernel, sup, kc.tab, plist, range, pair_foff, fsrc, offs, fval, d_stats);
+        KIWI_LAUNCHED(ctx);
+        k_vor_sum<<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(C, P, plist, range, offs, pair_foff, fsrc, fval,
+                                                                     out, d_stats, pair_val);
+        KIWI_LAUNCHED(ctx);
+    } else {
+        if (kc.tabulated)
+            k_vor_gather<kVorTab><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+                C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
+        else if (kc.cubic)
+            k_vor_gather<kVorCubic><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+                C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
+        else
+            k_vor_gather<kVorGeneric><<<(unsigned)nc, kGatherThreads, 0, ctx->stream>>>(
+                C, P, kc.kernel, sup, kc.tab, plist, range, offs, pair_cells, pair_mask, out, d_stats, pair_val);
+        KIWI_LAUNCHED(ctx);
+    }
     if (inv && n > 0) {
         const double* cmass = inv->cell_mass;
         if (!cmass) {

@@ -206,3 +206,46 @@ def test_device_resident_geometry_equals_host_entry(kiwi, ctx, fn):
             assert np.array_equal(out[name].cpu().numpy(), getattr(res, name))
         assert np.array_equal(out["raw4"].cpu().numpy().reshape(4, nc), res.raw)
         assert st["visited_pairs"] == res.stats["visited_pairs"]
+
+
+def test_face_tables_equal_single_launch(kiwi, ctx):
+    """The face-table map (every face value evaluated once per particle, read back by both of its cells)
+    equals the single-launch gather (a shared face evaluated on both sides) bit for bit: every fixture and
+    kernel, the tabulated integral, and a geometry with the face cache's two special cases (a shared face
+    whose copies differ, a face split in two towards one neighbour)."""
+    cases = []
+    for fn in GOLDEN:
+        d, P, geo = _load(fn)
+        cases.append((P, d["home"], geo, kiwi.KernelIntegrator(kernel=int(d["kernel_index"]))))
+    d, P, geo = _load(GOLDEN[0])
+    cases.append((P, d["home"], geo, kiwi.make_kernel_integrator("cubic_spline", use_tabulated_integral=True)))
+    n, lo, hi = 6, 0.0, 1.2
+    lgeo, dd = lattice_cells(n, lo, hi)
+    cells = _cells_as_lists(lgeo)
+    idx = lambda i, j, k: (i * n + j) * n + k
+    for v, b in cells[idx(3, 2, 2)]:
+        if b == idx(2, 2, 2):
+            v[0, 1] += 1e-5
+    faces = []
+    for v, b in cells[idx(2, 3, 2)]:
+        if b == idx(2, 3, 3):
+            faces += [(v[[0, 1, 2]].copy(), b), (v[[0, 2, 3]].copy(), b)]
+        else:
+            faces.append((v, b))
+    cells[idx(2, 3, 2)] = faces
+    P = random_particles(80, 29, box=(0.35, 0.85), hmin=0.08, hmax=0.3)
+    home = ((np.floor(P["x"] / dd) * n + np.floor(P["y"] / dd)) * n + np.floor(P["z"] / dd)).astype(np.int32)
+    cases.append((P, home, _lists_as_cells(cells, lgeo["volume"]), None))
+    try:
+        for P, home, geo, k in cases:
+            ctx.set_voronoi_face_tables(True)
+            a = kiwi.map_voronoi(P, home, geo, kernel=k, raw=True, ctx=ctx)
+            ctx.set_voronoi_face_tables(False)
+            b = kiwi.map_voronoi(P, home, geo, kernel=k, raw=True, ctx=ctx)
+            assert np.array_equal(a.raw, b.raw)
+            for name in ("density", "vx", "vy", "vz"):
+                assert np.array_equal(getattr(a, name), getattr(b, name)), name
+            assert a.stats["visited_pairs"] == b.stats["visited_pairs"]
+            assert a.stats["neg_clamped"] == b.stats["neg_clamped"]
+    finally:
+        ctx.set_voronoi_face_tables(True)
