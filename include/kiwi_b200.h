@@ -32,19 +32,18 @@ extern "C" {
 #define KIWI_ERR_UNSUPPORTED (-6) /* option not available in this build */
 
 /* Arithmetic forms of the cell integrals (the low byte of a `precision` argument).
- * KIWI_FP64: all FP64.  For the cubic closed form the vertex-pyramid tiers are shared between the cells
- * of a particle's box (each edge tier once per plane and edge line, each vertex pyramid once per lattice
- * point), which is algebraically the reference's per-cell sum; for the generic kernels it is the
- * reference's per-cell evaluation order.
+ * KIWI_FP64: all FP64.  The tiers are shared between the cells of a particle's box (each edge tier once
+ * per plane and edge line, each lattice point's octant value once, a cell the alternating sum of its 8
+ * corners' values), which is algebraically the reference's per-cell sum; the cubic closed form and the
+ * generic kernels' tables alike.
  * KIWI_FP64_REFERENCE_ORDER: all FP64 in the reference's per-cell evaluation order, operation by
  * operation (6 faces x 4 edges x 2 vertices per cell, src/kernel_integral.cpp:471-647).
- * KIWI_FP32_MIXED (cubic spline with support 2h): the edge tiers and vertex pyramids of the lattice
- * form in FP32, evaluated from FP64 plane offsets relative to the particle; the per-cell assembly and the
- * per-cell totals in FP64; planes within 1e-3 h of the particle in FP64 throughout.  Each cell also gets a
- * bound on its rounding error (4 x 2^-24 x the summed magnitudes of the FP32 terms it was assembled
- * from).  The closed form subtracts pyramid masses that
- * can exceed the cell's mass by orders of magnitude, so the FP32 error grows with the support size in
- * cells; fp64_fallback in KiwiStats counts the cells whose bound exceeds 1e-6 of their mass. */
+ * KIWI_FP32_MIXED: the edge tiers and octant values of the lattice form in FP32 (cubic closed form or the
+ * generic kernels' tables), evaluated from FP64 plane offsets relative to the particle; the cell assembly
+ * and the per-cell totals in FP64; lattice points and edge lines with a plane within 1e-3 h of the
+ * particle in FP64 throughout (fp64_fallback in KiwiStats counts those points).  The closed form
+ * subtracts octant values that can exceed the cell's mass by orders of magnitude, so the FP32 error grows
+ * in the cells far from the particle: an approximate form with a stated error, not within 1e-6. */
 #define KIWI_FP64 0
 #define KIWI_FP32_MIXED 1
 #define KIWI_FP64_REFERENCE_ORDER 2
@@ -54,9 +53,12 @@ extern "C" {
  * radius are evaluated; the others hold no kernel mass and the reference's values for them are
  * rounding noise around zero (clamped at 0). */
 #define KIWI_FULL_BOX 0x100
-/* Flag for KIWI_FP32_MIXED: recompute in FP64 (lattice form) every 8x8x8 cell tile holding a cell whose
- * mass is at least 1e-6 of the peak cell mass and whose FP32 rounding bound exceeds 1e-6 of its mass, so
- * that those cells are within 1e-6 relative by construction.  KiwiStats.fp64_tiles counts the tiles. */
+/* Flag for KIWI_FP32_MIXED (cubic spline with support 2h): evaluate the FP32 terms with their magnitudes,
+ * so that each cell gets a bound on its rounding error (4 x 2^-24 x the summed magnitudes of its FP32
+ * terms), and recompute in FP64 (lattice form) every 8x8x8 cell tile holding a cell whose mass is at least
+ * 1e-6 of the peak cell mass and whose bound exceeds 1e-6 of its mass, so that those cells are within 1e-6
+ * relative by construction.  KiwiStats.fp64_tiles counts the tiles, fp64_fallback the cells whose bound
+ * exceeds 1e-6 of their mass. */
 #define KIWI_FP32_GUARANTEE 0x200
 
 typedef struct KiwiCtx KiwiCtx;
@@ -94,7 +96,9 @@ typedef struct KiwiStats {
     int64_t skipped_outside; /* particles whose support misses the grid (src/cartesian_grid.cpp:234-237) */
     int64_t neg_clamped;     /* pair integrals < 0 clamped to 0 (src/cartesian_grid.cpp:264-269) */
     int64_t neg_warned;      /* of those, <= -0.01 (the reference prints a warning for each) */
-    int64_t fp64_fallback;   /* FP32-mixed form: cells whose FP32 rounding bound exceeds 1e-6 of their mass */
+    int64_t fp64_fallback;   /* KIWI_FP32_MIXED: lattice points evaluated in FP64 (a plane within 1e-3 h);
+                              * with KIWI_FP32_GUARANTEE: cells whose FP32 rounding bound exceeds 1e-6 of
+                              * their mass */
     int64_t tile_pairs;      /* (tile, particle) list entries built by the binning step */
     int64_t launches;        /* GPU kernels launched by this call */
     double gather_ms;        /* device time of the cell-integral kernel(s) of this call (CUDA events) */

@@ -82,12 +82,25 @@ __device__ __forceinline__ void lat_add_stat(unsigned long long* dst, unsigned l
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
 }
 
+// One chunk of a tile's particle list as the lattice tile holds it in shared memory: the particles' data,
+// their cell boxes clipped to the tile (lo, dim), their edge-slot and point offsets, the magic divisors of
+// their lattice dimensions, and the chunk's counts.
+struct LatChunk {
+    double x[kLatPMax], y[kLatPMax], z[kLatPMax], h[kLatPMax], m[kLatPMax], vx[kLatPMax], vy[kLatPMax], vz[kLatPMax],
+        ih[kLatPMax];
+    int lo[kLatPMax][3], dim[kLatPMax][3], eoff[kLatPMax], poff[kLatPMax];
+    uint32_t mag[kLatPMax][4];  // div_magic of n0', n1', n2' and n1' n2'
+    int np, etot, ptot;
+};
+
 // The chunk of a tile's particle list (ascending particle index) is walked in four phases separated by
 // barriers: (A) classify every edge pair, listing those within the support; (B0) list the lattice points
 // that some evaluated cell reads (the cheap ones -- beyond the support -- from the end of the list) and set
 // the octant value of the points on a particle plane to 0; (A2) the listed edge pairs; (B) the listed
 // points' octant values; (C) each thread adds, for the cells it owns, the chunk's particles in list order
-// -- every cell's sum runs over its particles in ascending index order with no atomics.
+// -- every cell's sum runs over its particles in ascending index order with no atomics.  The chunks are
+// double-buffered: while warps 1-7 classify the current chunk's edge pairs and points, warp 0 loads the next
+// chunk (the particles' data, boxes and offsets) into the other buffer.
 // GENERIC: the table-driven tiers of kernel K (support radius support_in_h x h) instead of the cubic closed
 // form; edge tiers are lattice_generic_edge records.  TAB: the tabulated cubic integral (lookups in `tab`):
 // no edge tiers, and the points run in their natural order.  List order never affects the results.
@@ -97,13 +110,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                                              int64_t t_range, int64_t t, const CartOutputs& out,
                                              DevStats* __restrict__ st, const KiwiKernelTable* K = nullptr,
                                              const TabDev tab = TabDev{}) {
-    __shared__ double s_x[kLatPMax], s_y[kLatPMax], s_z[kLatPMax], s_h[kLatPMax], s_m[kLatPMax], s_vx[kLatPMax],
-        s_vy[kLatPMax], s_vz[kLatPMax], s_ih[kLatPMax];
-    __shared__ int s_lo[kLatPMax][3], s_dim[kLatPMax][3], s_eoff[kLatPMax], s_poff[kLatPMax];
-    __shared__ uint32_t s_mag[kLatPMax][4];  // div_magic of n0', n1', n2' and n1' n2'
+    __shared__ LatChunk s_cp[2];
     __shared__ TabWidths s_tw;               // TAB: the table's bin widths and their reciprocals
     if (TAB && threadIdx.x == 0) s_tw = tab_widths(tab);  // read after the chunk load's barrier
-    __shared__ int s_np, s_etot, s_ptot, s_nexp, s_ncheap, s_nheavy;
+    __shared__ int s_nexp, s_ncheap, s_nheavy;
     __shared__ uint32_t s_plist[TAB ? 1 : kLatPtCap];
     __shared__ uint32_t s_hlist[(GENERIC || TAB) ? 1 : kLatECap2 / 2];
     extern __shared__ double s_dyn[];
@@ -159,177 +169,188 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     const int64_t beg = range[2 * t_range], end = range[2 * t_range + 1];
     const double sup_in_h = g.support_in_h;
 
+    // warp 0: the chunk of the particle list starting at `at` into *dst (as many particles as the edge and
+    // point capacities take, at most 32)
+    auto load_chunk = [&](LatChunk* dst, int64_t at) {
+        const int64_t idx = at + lane;
+        int ne = 0, npt = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+        double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
+        if (idx < end) {
+            const uint32_t p = list[idx];
+            px = P.x[p]; py = P.y[p]; pz = P.z[p]; ph = P.h[p];
+            pm = P.m[p]; pvx = P.vx[p]; pvy = P.vy[p]; pvz = P.vz[p];
+            CellBox b;
+            bool outside;
+            particle_cell_box(g, px, py, pz, ph, b, &outside);
+            lo0 = max(b.x0, bx); lo1 = max(b.y0, by); lo2 = max(b.z0, bz);
+            d0 = min(b.x1, bx + kTileX - 1) - lo0 + 1;
+            d1 = min(b.y1, by + kTileY - 1) - lo1 + 1;
+            d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
+            const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
+            ne = TAB ? 0 : 2 * (n0 * n1 + n0 * n2 + n1 * n2);
+            npt = n0 * n1 * n2;
+        }
+        int ie = ne, ip = npt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ve = __shfl_up_sync(0xffffffffu, ie, o), vp = __shfl_up_sync(0xffffffffu, ip, o);
+            if (lane >= o) {
+                ie += ve;
+                ip += vp;
+            }
+        }
+        const bool take = (idx < end) && ie <= kECap && ip <= kLatPtCap;
+        const int np = __popc(__ballot_sync(0xffffffffu, take));
+        if (take) {
+            dst->x[lane] = px; dst->y[lane] = py; dst->z[lane] = pz; dst->h[lane] = ph; dst->ih[lane] = 1.0 / ph;
+            dst->m[lane] = pm; dst->vx[lane] = pvx; dst->vy[lane] = pvy; dst->vz[lane] = pvz;
+            dst->lo[lane][0] = lo0; dst->lo[lane][1] = lo1; dst->lo[lane][2] = lo2;
+            dst->dim[lane][0] = d0; dst->dim[lane][1] = d1; dst->dim[lane][2] = d2;
+            dst->eoff[lane] = ie - ne;
+            dst->poff[lane] = ip - npt;
+            dst->mag[lane][0] = div_magic(d0 + 1);
+            dst->mag[lane][1] = div_magic(d1 + 1);
+            dst->mag[lane][2] = div_magic(d2 + 1);
+            dst->mag[lane][3] = div_magic((d1 + 1) * (d2 + 1));
+        }
+        if (lane == np - 1) {
+            dst->np = np;
+            dst->etot = ie;
+            dst->ptot = ip;
+        }
+    };
+    LatChunk* cp = &s_cp[0];
+    if (warp == 0 && beg < end) load_chunk(cp, beg);
+    if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = 0;
+    __syncthreads();
+
     for (int64_t pos = beg; pos < end;) {
+        LatChunk* const nx = cp == &s_cp[0] ? &s_cp[1] : &s_cp[0];
+        const int np = cp->np, etot = cp->etot, ptot = cp->ptot;
+
         if (warp == 0) {
-            const int64_t idx = pos + lane;
-            int ne = 0, npt = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
-            double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
-            if (idx < end) {
-                const uint32_t p = list[idx];
-                px = P.x[p]; py = P.y[p]; pz = P.z[p]; ph = P.h[p];
-                pm = P.m[p]; pvx = P.vx[p]; pvy = P.vy[p]; pvz = P.vz[p];
-                CellBox b;
-                bool outside;
-                particle_cell_box(g, px, py, pz, ph, b, &outside);
-                lo0 = max(b.x0, bx); lo1 = max(b.y0, by); lo2 = max(b.z0, bz);
-                d0 = min(b.x1, bx + kTileX - 1) - lo0 + 1;
-                d1 = min(b.y1, by + kTileY - 1) - lo1 + 1;
-                d2 = min(b.z1, bz + kTileZ - 1) - lo2 + 1;
-                const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
-                ne = TAB ? 0 : 2 * (n0 * n1 + n0 * n2 + n1 * n2);
-                npt = n0 * n1 * n2;
-            }
-            int ie = ne, ip = npt;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int ve = __shfl_up_sync(0xffffffffu, ie, o), vp = __shfl_up_sync(0xffffffffu, ip, o);
-                if (lane >= o) {
-                    ie += ve;
-                    ip += vp;
+            // the next chunk, into the other buffer (read after the barrier that ends the current chunk)
+            if (pos + np < end) load_chunk(nx, pos + np);
+        } else {
+            // (A) edge pairs: pair block 0 = (x, y) over n0' x n1', 1 = (x, z) over n0' x n2', 2 = (y, z) over
+            // n1' x n2'; pair (p, q) of block (a, b) is edge ab[p][q] and edge ba[q][p].  Cubic: pairs beyond 2h
+            // (and zero ones) get D2 = D3 = 0 here; the others are listed (slot ab | slot ba << 11 | particle <<
+            // 22) with |u_a|, |u_b| parked in slot ab, and evaluated in (A2).  Generic: both records here.
+            if (!TAB) {
+                const int qtot = etot >> 1;
+                const int qoff_l = lane < np ? (cp->eoff[lane] >> 1) : INT_MAX;
+                for (int base = (warp - 1) * 32; base < qtot; base += kLatThreads - 32) {
+                    const int it = base + lane;
+                    bool heavy = false;
+                    uint32_t hrec = 0;
+                    const int j = warp_owner(base, qoff_l, lane);
+                    const int qoff = __shfl_sync(0xffffffffu, qoff_l, j & 31);
+                    if (it < qtot) {
+                        int e = it - qoff;
+                        const int n0 = cp->dim[j][0] + 1, n1 = cp->dim[j][1] + 1, n2 = cp->dim[j][2] + 1;
+                        const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
+                        const int blk = (e >= nxy) + (e >= nxy + nxz);
+                        e -= blk == 0 ? 0 : (blk == 1 ? nxy : nxy + nxz);
+                        const int a = blk == 2 ? 1 : 0, b = blk == 0 ? 1 : 2;
+                        const int nb = b == 1 ? n1 : n2, na = a == 0 ? n0 : n1;
+                        const int pi = div_by(e, cp->mag[j][b]), qi = e - pi * nb;
+                        const int eb = cp->eoff[j];
+                        const int sab = eb + (blk == 0 ? 0 : (blk == 1 ? nxy : 2 * nxy + nxz)) + pi * nb + qi;
+                        const int sba = eb + (blk == 0 ? nxy + nxz : (blk == 1 ? 2 * nxy + nxz + nyz : 2 * nxy + 2 * nxz + nyz)) +
+                                        qi * na + pi;
+                        const int la = cp->lo[j][a] - (a == 0 ? bx : by), lb = cp->lo[j][b] - (b == 1 ? by : bz);
+                        const double pa = a == 0 ? cp->x[j] : cp->y[j], pb = b == 1 ? cp->y[j] : cp->z[j];
+                        const double vp = fabs(s_pl[a][la + pi] - pa), vq = fabs(s_pl[b][lb + qi] - pb);
+                        if (GENERIC) {
+                            const double H = mul_rn(sup_in_h, cp->h[j]);
+                            if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * cp->h[j]) {
+                                lattice_generic_edge(K, H, F32(vp), F32(vq), s_E + kLatGenERec * sab);
+                                lattice_generic_edge(K, H, F32(vq), F32(vp), s_E + kLatGenERec * sba);
+                            } else {
+                                lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
+                                lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+                            }
+                            n_ei += 2;
+                        } else {
+                            const double h2 = cp->h[j] * cp->h[j];
+                            const double ld2 = add_rn(mul_rn(vp, vp), mul_rn(vq, vq));
+                            heavy = vp != 0.0 && vq != 0.0 && ld2 <= 4.0 * h2;
+                            if (heavy) {
+                                if (ld2 > h2) n_em += 2;
+                                else n_ei += 2;
+                                s_D2[sab] = vp;
+                                s_D3[sab] = vq;
+                                hrec = (uint32_t)sab | (uint32_t)sba << 11 | (uint32_t)j << 22;
+                            } else {
+                                n_eo += 2;
+                                s_D2[sab] = s_D3[sab] = 0.0;
+                                s_D2[sba] = s_D3[sba] = 0.0;
+                                s_A[sab] = -1.0;
+                            }
+                        }
+                    }
+                    if (!GENERIC) {
+                        const unsigned m = __ballot_sync(0xffffffffu, heavy);
+                        int hp = 0;
+                        if (lane == 0 && m) hp = atomicAdd(&s_nheavy, __popc(m));
+                        hp = __shfl_sync(0xffffffffu, hp, 0);
+                        if (heavy) s_hlist[hp + __popc(m & ((1u << lane) - 1))] = hrec;
+                    }
                 }
             }
-            const bool take = (idx < end) && ie <= kECap && ip <= kLatPtCap;
-            const int np = __popc(__ballot_sync(0xffffffffu, take));
-            if (take) {
-                s_x[lane] = px; s_y[lane] = py; s_z[lane] = pz; s_h[lane] = ph; s_ih[lane] = 1.0 / ph;
-                s_m[lane] = pm; s_vx[lane] = pvx; s_vy[lane] = pvy; s_vz[lane] = pvz;
-                s_lo[lane][0] = lo0; s_lo[lane][1] = lo1; s_lo[lane][2] = lo2;
-                s_dim[lane][0] = d0; s_dim[lane][1] = d1; s_dim[lane][2] = d2;
-                s_eoff[lane] = ie - ne;
-                s_poff[lane] = ip - npt;
-                s_mag[lane][0] = div_magic(d0 + 1);
-                s_mag[lane][1] = div_magic(d1 + 1);
-                s_mag[lane][2] = div_magic(d2 + 1);
-                s_mag[lane][3] = div_magic((d1 + 1) * (d2 + 1));
-            }
-            if (lane == np - 1) {
-                s_np = np;
-                s_etot = ie;
-                s_ptot = ip;
-                s_nexp = s_ncheap = s_nheavy = 0;
-            }
-        }
-        __syncthreads();
-        const int np = s_np, etot = s_etot, ptot = s_ptot;
 
-        // (A) edge pairs: pair block 0 = (x, y) over n0' x n1', 1 = (x, z) over n0' x n2', 2 = (y, z) over
-        // n1' x n2'; pair (p, q) of block (a, b) is edge ab[p][q] and edge ba[q][p].  Cubic: pairs beyond 2h
-        // (and zero ones) get D2 = D3 = 0 here; the others are listed (slot ab | slot ba << 11 | particle <<
-        // 22) with |u_a|, |u_b| parked in slot ab, and evaluated in (A2).  Generic: both records here.
-        if (!TAB) {
-            const int qtot = etot >> 1;
-            const int qoff_l = lane < np ? (s_eoff[lane] >> 1) : INT_MAX;
-            for (int base = warp * 32; base < qtot; base += kLatThreads) {
-                const int it = base + lane;
-                bool heavy = false;
-                uint32_t hrec = 0;
-                const int j = warp_owner(base, qoff_l, lane);
-                const int qoff = __shfl_sync(0xffffffffu, qoff_l, j & 31);
-                if (it < qtot) {
-                    int e = it - qoff;
-                    const int n0 = s_dim[j][0] + 1, n1 = s_dim[j][1] + 1, n2 = s_dim[j][2] + 1;
-                    const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
-                    const int blk = (e >= nxy) + (e >= nxy + nxz);
-                    e -= blk == 0 ? 0 : (blk == 1 ? nxy : nxy + nxz);
-                    const int a = blk == 2 ? 1 : 0, b = blk == 0 ? 1 : 2;
-                    const int nb = b == 1 ? n1 : n2, na = a == 0 ? n0 : n1;
-                    const int pi = div_by(e, s_mag[j][b]), qi = e - pi * nb;
-                    const int eb = s_eoff[j];
-                    const int sab = eb + (blk == 0 ? 0 : (blk == 1 ? nxy : 2 * nxy + nxz)) + pi * nb + qi;
-                    const int sba = eb + (blk == 0 ? nxy + nxz : (blk == 1 ? 2 * nxy + nxz + nyz : 2 * nxy + 2 * nxz + nyz)) +
-                                    qi * na + pi;
-                    const int la = s_lo[j][a] - (a == 0 ? bx : by), lb = s_lo[j][b] - (b == 1 ? by : bz);
-                    const double pa = a == 0 ? s_x[j] : s_y[j], pb = b == 1 ? s_y[j] : s_z[j];
-                    const double vp = fabs(s_pl[a][la + pi] - pa), vq = fabs(s_pl[b][lb + qi] - pb);
-                    if (GENERIC) {
-                        const double H = mul_rn(sup_in_h, s_h[j]);
-                        if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * s_h[j]) {
-                            lattice_generic_edge(K, H, F32(vp), F32(vq), s_E + kLatGenERec * sab);
-                            lattice_generic_edge(K, H, F32(vq), F32(vp), s_E + kLatGenERec * sba);
-                        } else {
-                            lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
-                            lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+            // (B0) the lattice points some evaluated cell reads: with CULL, a point none of whose eight cells
+            // meets the support sphere is left out (the test bounds the distance to the 2 x 2 x 2 cells around
+            // the point, their half-widths padded by 1e-6 of a cell so that rounding never drops a point an
+            // evaluated cell reads).  A point on a particle plane (an offset of 0) has octant value 0, written
+            // here; the others are listed, those within the support from the front of s_plist, those beyond it
+            // from the end, so that each kind runs in warps of its own.  An entry packs (particle, i, j, k):
+            // 5 + 3 x 4 bits.
+            if (!TAB) {
+                const int poff_l = lane < np ? cp->poff[lane] : INT_MAX;
+                for (int base = (warp - 1) * 32; base < ptot; base += kLatThreads - 32) {
+                    const int pt = base + lane;
+                    int cls = -1;  // -1 none, 0 within the support, 1 beyond
+                    uint32_t rec = 0;
+                    const int jp = warp_owner(base, poff_l, lane);
+                    const int poff = __shfl_sync(0xffffffffu, poff_l, jp & 31);
+                    if (pt < ptot) {
+                        const int lp = pt - poff;
+                        const int n2 = cp->dim[jp][2] + 1, n12 = (cp->dim[jp][1] + 1) * n2;
+                        const int i = div_by(lp, cp->mag[jp][3]), rem = lp - i * n12;
+                        const int jj = div_by(rem, cp->mag[jp][2]), k = rem - jj * n2;
+                        const double ux = s_pl[0][cp->lo[jp][0] - bx + i] - cp->x[jp];
+                        const double uy = s_pl[1][cp->lo[jp][1] - by + jj] - cp->y[jp];
+                        const double uz = s_pl[2][cp->lo[jp][2] - bz + k] - cp->z[jp];
+                        const double h = cp->h[jp];
+                        bool keep = true;
+                        if (CULL) {
+                            const double radius = mul_rn(sup_in_h, h);
+                            const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
+                            const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
+                            const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
+                            keep = ex * ex + ey * ey + ez * ez < radius * radius;
                         }
-                        n_ei += 2;
-                    } else {
-                        const double h2 = s_h[j] * s_h[j];
-                        const double ld2 = add_rn(mul_rn(vp, vp), mul_rn(vq, vq));
-                        heavy = vp != 0.0 && vq != 0.0 && ld2 <= 4.0 * h2;
-                        if (heavy) {
-                            if (ld2 > h2) n_em += 2;
-                            else n_ei += 2;
-                            s_D2[sab] = vp;
-                            s_D3[sab] = vq;
-                            hrec = (uint32_t)sab | (uint32_t)sba << 11 | (uint32_t)j << 22;
-                        } else {
-                            n_eo += 2;
-                            s_D2[sab] = s_D3[sab] = 0.0;
-                            s_D2[sba] = s_D3[sba] = 0.0;
-                            s_A[sab] = -1.0;
+                        if (keep) {
+                            if (ux == 0.0 || uy == 0.0 || uz == 0.0) {
+                                s_T[pt] = 0.0;
+                            } else {
+                                const double H = GENERIC ? mul_rn(sup_in_h, h) : 2.0 * h;
+                                cls = (ux * ux + uy * uy + uz * uz < H * H) ? 0 : 1;
+                                rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
+                            }
                         }
                     }
-                }
-                if (!GENERIC) {
-                    const unsigned m = __ballot_sync(0xffffffffu, heavy);
-                    int hp = 0;
-                    if (lane == 0 && m) hp = atomicAdd(&s_nheavy, __popc(m));
-                    hp = __shfl_sync(0xffffffffu, hp, 0);
-                    if (heavy) s_hlist[hp + __popc(m & ((1u << lane) - 1))] = hrec;
-                }
-            }
-        }
-
-        // (B0) the lattice points some evaluated cell reads: with CULL, a point none of whose eight cells
-        // meets the support sphere is left out (the test bounds the distance to the 2 x 2 x 2 cells around
-        // the point, their half-widths padded by 1e-6 of a cell so that rounding never drops a point an
-        // evaluated cell reads).  A point on a particle plane (an offset of 0) has octant value 0, written
-        // here; the others are listed, those within the support from the front of s_plist, those beyond it
-        // from the end, so that each kind runs in warps of its own.  An entry packs (particle, i, j, k):
-        // 5 + 3 x 4 bits.
-        if (!TAB) {
-            const int poff_l = lane < np ? s_poff[lane] : INT_MAX;
-            for (int base = warp * 32; base < ptot; base += kLatThreads) {
-                const int pt = base + lane;
-                int cls = -1;  // -1 none, 0 within the support, 1 beyond
-                uint32_t rec = 0;
-                const int jp = warp_owner(base, poff_l, lane);
-                const int poff = __shfl_sync(0xffffffffu, poff_l, jp & 31);
-                if (pt < ptot) {
-                    const int lp = pt - poff;
-                    const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
-                    const int i = div_by(lp, s_mag[jp][3]), rem = lp - i * n12;
-                    const int jj = div_by(rem, s_mag[jp][2]), k = rem - jj * n2;
-                    const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
-                    const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
-                    const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
-                    const double h = s_h[jp];
-                    bool keep = true;
-                    if (CULL) {
-                        const double radius = mul_rn(sup_in_h, h);
-                        const double ex = fmax(fabs(ux) - kNeedPad * g.dpx, 0.0);
-                        const double ey = fmax(fabs(uy) - kNeedPad * g.dpy, 0.0);
-                        const double ez = fmax(fabs(uz) - kNeedPad * g.dpz, 0.0);
-                        keep = ex * ex + ey * ey + ez * ez < radius * radius;
+                    const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
+                    int pe = 0, pcb = 0;
+                    if (lane == 0) {
+                        if (me) pe = atomicAdd(&s_nexp, __popc(me));
+                        if (mc) pcb = atomicAdd(&s_ncheap, __popc(mc));
                     }
-                    if (keep) {
-                        if (ux == 0.0 || uy == 0.0 || uz == 0.0) {
-                            s_T[pt] = 0.0;
-                        } else {
-                            const double H = GENERIC ? mul_rn(sup_in_h, h) : 2.0 * h;
-                            cls = (ux * ux + uy * uy + uz * uz < H * H) ? 0 : 1;
-                            rec = (uint32_t)jp | (uint32_t)i << 5 | (uint32_t)jj << 9 | (uint32_t)k << 13;
-                        }
-                    }
+                    pe = __shfl_sync(0xffffffffu, pe, 0);
+                    pcb = __shfl_sync(0xffffffffu, pcb, 0);
+                    const unsigned below = (1u << lane) - 1;
+                    if (cls >= 0) s_plist[cls == 0 ? pe + __popc(me & below) : kLatPtCap - 1 - pcb - __popc(mc & below)] = rec;
                 }
-                const unsigned me = __ballot_sync(0xffffffffu, cls == 0), mc = __ballot_sync(0xffffffffu, cls == 1);
-                int pe = 0, pcb = 0;
-                if (lane == 0) {
-                    if (me) pe = atomicAdd(&s_nexp, __popc(me));
-                    if (mc) pcb = atomicAdd(&s_ncheap, __popc(mc));
-                }
-                pe = __shfl_sync(0xffffffffu, pe, 0);
-                pcb = __shfl_sync(0xffffffffu, pcb, 0);
-                const unsigned below = (1u << lane) - 1;
-                if (cls >= 0) s_plist[cls == 0 ? pe + __popc(me & below) : kLatPtCap - 1 - pcb - __popc(mc & below)] = rec;
             }
         }
         __syncthreads();
@@ -346,13 +367,13 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 // which the walls with legs along a and b read
                 const double vmin = fmin(vp, vq), vmax = fmax(vp, vq);
                 s_A[sab] = atan(vmin / vmax);
-                if (MIXED && vmin >= kMixedIslandFrac * s_h[j]) {
+                if (MIXED && vmin >= kMixedIslandFrac * cp->h[j]) {
                     LatticeEdgeT<F32> f_pq, f_qp;
-                    lattice_edge_pair(F32(s_h[j]), F32(s_ih[j]), F32(vp), F32(vq), f_pq, f_qp);
+                    lattice_edge_pair(F32(cp->h[j]), F32(cp->ih[j]), F32(vp), F32(vq), f_pq, f_qp);
                     e_pq = {(double)f_pq.D2.v, (double)f_pq.D3.v};
                     e_qp = {(double)f_qp.D2.v, (double)f_qp.D3.v};
                 } else {
-                    lattice_edge_pair(s_h[j], s_ih[j], vp, vq, e_pq, e_qp);
+                    lattice_edge_pair(cp->h[j], cp->ih[j], vp, vq, e_pq, e_qp);
                 }
                 s_D2[sab] = e_pq.D2;
                 s_D3[sab] = e_pq.D3;
@@ -369,12 +390,12 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             int jp, i, jj, k, it;
             if (TAB) {
                 it = li;
-                jp = chunk_search(s_poff, np, it);
-                const int lp = it - s_poff[jp];
-                const int n2 = s_dim[jp][2] + 1, n12 = (s_dim[jp][1] + 1) * n2;
-                i = div_by(lp, s_mag[jp][3]);
+                jp = chunk_search(cp->poff, np, it);
+                const int lp = it - cp->poff[jp];
+                const int n2 = cp->dim[jp][2] + 1, n12 = (cp->dim[jp][1] + 1) * n2;
+                i = div_by(lp, cp->mag[jp][3]);
                 const int rem = lp - i * n12;
-                jj = div_by(rem, s_mag[jp][2]);
+                jj = div_by(rem, cp->mag[jp][2]);
                 k = rem - jj * n2;
             } else {
                 const uint32_t rec = s_plist[li < nexp ? li : kLatPtCap - ncheap + (li - nexp)];
@@ -382,33 +403,33 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 i = (int)((rec >> 5) & 15u);
                 jj = (int)((rec >> 9) & 15u);
                 k = (int)((rec >> 13) & 15u);
-                it = s_poff[jp] + (i * (s_dim[jp][1] + 1) + jj) * (s_dim[jp][2] + 1) + k;
+                it = cp->poff[jp] + (i * (cp->dim[jp][1] + 1) + jj) * (cp->dim[jp][2] + 1) + k;
             }
-            const double ux = s_pl[0][s_lo[jp][0] - bx + i] - s_x[jp];
-            const double uy = s_pl[1][s_lo[jp][1] - by + jj] - s_y[jp];
-            const double uz = s_pl[2][s_lo[jp][2] - bz + k] - s_z[jp];
+            const double ux = s_pl[0][cp->lo[jp][0] - bx + i] - cp->x[jp];
+            const double uy = s_pl[1][cp->lo[jp][1] - by + jj] - cp->y[jp];
+            const double uz = s_pl[2][cp->lo[jp][2] - bz + k] - cp->z[jp];
             const double sg = sgn(ux) * sgn(uy) * sgn(uz);
             double f = 0.0;
             if (sg != 0.0) {
                 const double ax = fabs(ux), ay = fabs(uy), az = fabs(uz);
                 if (TAB) {
                     // two right-triangle vertex pyramids per wall; cos(phi) from the legs
-                    const double ih = s_ih[jp];
+                    const double ih = cp->ih[jp];
                     f = tab_pair(tab, s_tw, ih, ax, ay, az, n_clamp) + tab_pair(tab, s_tw, ih, ay, ax, az, n_clamp) +
                         tab_pair(tab, s_tw, ih, az, ax, ay, n_clamp);
                 } else {
-                    const int n0 = s_dim[jp][0] + 1, n1 = s_dim[jp][1] + 1, n2 = s_dim[jp][2] + 1;
+                    const int n0 = cp->dim[jp][0] + 1, n1 = cp->dim[jp][1] + 1, n2 = cp->dim[jp][2] + 1;
                     const int nxy = n0 * n1, nxz = n0 * n2, nyz = n1 * n2;
-                    const int eb = s_eoff[jp];
+                    const int eb = cp->eoff[jp];
                     const int exy = eb + i * n1 + jj, exz = eb + nxy + i * n2 + k;
                     const int eyx = eb + nxy + nxz + jj * n0 + i, eyz = eb + 2 * nxy + nxz + jj * n2 + k;
                     const int ezx = eb + 2 * nxy + nxz + nyz + k * n0 + i, ezy = eb + 2 * nxy + 2 * nxz + nyz + k * n1 + jj;
                     if (GENERIC) {
-                        const double H = mul_rn(sup_in_h, s_h[jp]);
+                        const double H = mul_rn(sup_in_h, cp->h[jp]);
                         const double *rxy = s_E + kLatGenERec * exy, *rxz = s_E + kLatGenERec * exz;
                         const double *ryx = s_E + kLatGenERec * eyx, *ryz = s_E + kLatGenERec * eyz;
                         const double *rzx = s_E + kLatGenERec * ezx, *rzy = s_E + kLatGenERec * ezy;
-                        if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * s_h[jp]) {
+                        if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * cp->h[jp]) {
                             const F32 fx(ax), fy(ay), fz(az);
                             f = (double)(lattice_generic_corner(K, H, fx, fy, fz, rxy, rxz) +
                                          lattice_generic_corner(K, H, fy, fx, fz, ryx, ryz) +
@@ -420,12 +441,12 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                             if (MIXED) ++n_island;
                         }
                     } else {
-                        if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * s_h[jp]) {
+                        if (MIXED && fmin(ax, fmin(ay, az)) >= kMixedIslandFrac * cp->h[jp]) {
                             const SmemPointEdges<F32> E{s_D2, s_D3, s_A, {exy, exz, eyx, eyz, ezx, ezy}};
-                            f = (double)lattice_point(F32(s_h[jp]), F32(s_ih[jp]), F32(ax), F32(ay), F32(az), E).v;
+                            f = (double)lattice_point(F32(cp->h[jp]), F32(cp->ih[jp]), F32(ax), F32(ay), F32(az), E).v;
                         } else {
                             const SmemPointEdges<double> E{s_D2, s_D3, s_A, {exy, exz, eyx, eyz, ezx, ezy}};
-                            f = lattice_point(s_h[jp], s_ih[jp], ax, ay, az, E);
+                            f = lattice_point(cp->h[jp], cp->ih[jp], ax, ay, az, E);
                             if (MIXED) ++n_island;
                         }
                     }
@@ -436,6 +457,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         }
         __syncthreads();
 
+        // the next chunk's list counters (the lists of this one are read)
+        if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = 0;
+
         // (C) cells: the alternating sum of the 8 corners' octant values, in particle order
 #pragma unroll
         for (int c = 0; c < kLatCellsPerThread; ++c) {
@@ -445,20 +469,20 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             double a0 = s_acc[li], a1 = s_acc[kTileCells + li];
             double a2 = s_acc[2 * kTileCells + li], a3 = s_acc[3 * kTileCells + li];
             for (int j = 0; j < np; ++j) {
-                const int i = gx - s_lo[j][0], jj = gy - s_lo[j][1], k = gz - s_lo[j][2];
-                if (i < 0 || jj < 0 || k < 0 || i >= s_dim[j][0] || jj >= s_dim[j][1] || k >= s_dim[j][2]) continue;
+                const int i = gx - cp->lo[j][0], jj = gy - cp->lo[j][1], k = gz - cp->lo[j][2];
+                if (i < 0 || jj < 0 || k < 0 || i >= cp->dim[j][0] || jj >= cp->dim[j][1] || k >= cp->dim[j][2]) continue;
                 ++n_bbox;
-                const double radius = mul_rn(sup_in_h, s_h[j]);
-                const double ex = fmax(fabs(s_x[j] - s_cc[0][lx]) - g.hpx, 0.0);
-                const double ey = fmax(fabs(s_y[j] - s_cc[1][ly]) - g.hpy, 0.0);
-                const double ez = fmax(fabs(s_z[j] - s_cc[2][lz]) - g.hpz, 0.0);
+                const double radius = mul_rn(sup_in_h, cp->h[j]);
+                const double ex = fmax(fabs(cp->x[j] - s_cc[0][lx]) - g.hpx, 0.0);
+                const double ey = fmax(fabs(cp->y[j] - s_cc[1][ly]) - g.hpy, 0.0);
+                const double ez = fmax(fabs(cp->z[j] - s_cc[2][lz]) - g.hpz, 0.0);
                 // the support test of the pair counters, rounded as the host restatement rounds it
                 const bool in = add_rn(add_rn(mul_rn(ex, ex), mul_rn(ey, ey)), mul_rn(ez, ez)) < mul_rn(radius, radius);
                 n_sphere += in;
                 if (CULL && !in) continue;
                 ++n_eval;
-                const int n2 = s_dim[j][2] + 1, n12 = (s_dim[j][1] + 1) * n2;
-                const double* Tp = s_T + s_poff[j] + (i * (s_dim[j][1] + 1) + jj) * n2 + k;
+                const int n2 = cp->dim[j][2] + 1, n12 = (cp->dim[j][1] + 1) * n2;
+                const double* Tp = s_T + cp->poff[j] + (i * (cp->dim[j][1] + 1) + jj) * n2 + k;
                 const double m1 = (Tp[n12 + n2 + 1] - Tp[n12 + n2]) - (Tp[n12 + 1] - Tp[n12]);
                 const double m0 = (Tp[n2 + 1] - Tp[n2]) - (Tp[1] - Tp[0]);
                 double msum = m1 - m0;
@@ -468,11 +492,11 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                     msum = 0.0;
                 }
                 if (msum == 0.0) continue;
-                const double mm = msum * s_m[j];
+                const double mm = msum * cp->m[j];
                 a0 += mm;
-                a1 += mm * s_vx[j];
-                a2 += mm * s_vy[j];
-                a3 += mm * s_vz[j];
+                a1 += mm * cp->vx[j];
+                a2 += mm * cp->vy[j];
+                a3 += mm * cp->vz[j];
             }
             s_acc[li] = a0;
             s_acc[kTileCells + li] = a1;
@@ -481,6 +505,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         }
         __syncthreads();
         pos += np;
+        cp = nx;
         if (++n_chunks == (1u << 16)) {
             flush();
             n_chunks = 0;
