@@ -167,7 +167,8 @@ enum ScratchSlot {
     S_VOR_PFOFF,     // Voronoi walk: per pair, the offset of its cell's faces in the face tables
     S_VOR_FSRC,      // Voronoi walk: per (pair, face), where its value comes from
     S_VOR_FVAL,      // Voronoi map: per (pair, face), the face's integral
+    S_VOR_LINKS,     // Voronoi map: per face, its earlier twin in the cell and the neighbour's face back
 };
-static_assert(S_VOR_FVAL < KiwiCtx::kSlots, "scratch slots");
+static_assert(S_VOR_LINKS < KiwiCtx::kSlots, "scratch slots");
 
 }  // namespace kiwi_b200

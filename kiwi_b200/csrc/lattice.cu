@@ -121,14 +121,14 @@ int lattice_cart_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P, 
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                                (int)cudaSharedmemCarveoutMaxShared));
+                                                (int)kLatCarveout));
             k_cart_lattice<false><<<grid, kLatThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map,
                                                                                    out, d_stats);
         } else {
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)kLatDynSmem));
             KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                                (int)cudaSharedmemCarveoutMaxShared));
+                                                (int)kLatCarveout));
             k_cart_lattice<true><<<grid, kLatThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map,
                                                                                   out, d_stats);
         }
@@ -151,7 +151,7 @@ int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P,
                                             (int)kLatGenDynSmem));
         KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_generic_mixed,
                                             cudaFuncAttributePreferredSharedMemoryCarveout,
-                                            (int)cudaSharedmemCarveoutMaxShared));
+                                            (int)kLatCarveout));
         k_cart_lattice_generic_mixed<<<grid, kLatThreads, kLatGenDynSmem, ctx->stream>>>(
             g, P, k.kernel, tl.list, tl.range, tl.map, out, d_stats);
         KIWI_LAUNCHED(ctx);
@@ -160,7 +160,7 @@ int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P,
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)kLatDynSmem));
     KIWI_CUDA(ctx, cudaFuncSetAttribute(k_cart_lattice_mixed, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        (int)cudaSharedmemCarveoutMaxShared));
+                                        (int)kLatCarveout));
     k_cart_lattice_mixed<<<grid, kLatThreads, kLatDynSmem, ctx->stream>>>(g, P, tl.list, tl.range, tl.map, out,
                                                                           d_stats);
     KIWI_LAUNCHED(ctx);

@@ -41,9 +41,20 @@ constexpr int kLatPtCap = KIWI_LAT_PT_CAP;  // lattice points per chunk
 constexpr int kLatECap2 = KIWI_LAT_E_CAP;   // cubic edge tiers per chunk
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed point-list entries");
 static_assert(kLatECap2 <= 2048 && kLatGenECap <= 2048, "packed edge-pair entries (11-bit slots)");
+// Each edge pair's in-plane angle formed once (1) or every point's walls forming theirs (0).
+#ifndef KIWI_LAT_ANGLES
+#define KIWI_LAT_ANGLES 1
+#endif
+constexpr bool kLatAngles = KIWI_LAT_ANGLES != 0;
+// Shared-memory carveout preference of the lattice kernels, percent of the SM's maximum (what is not
+// carved out is L1, which holds the tiers' register spills).
+#ifndef KIWI_LAT_CARVEOUT
+#define KIWI_LAT_CARVEOUT 100
+#endif
+constexpr int kLatCarveout = KIWI_LAT_CARVEOUT;
 // dynamic shared memory: the owned cells' sums (4 per cell), then the chunk's edge tiers and octant values
 constexpr size_t kLatAccSmem = sizeof(double) * 4 * kTileCells;
-constexpr size_t kLatDynSmem = kLatAccSmem + sizeof(double) * (3 * kLatECap2 + kLatPtCap);
+constexpr size_t kLatDynSmem = kLatAccSmem + sizeof(double) * ((kLatAngles ? 3 : 2) * kLatECap2 + kLatPtCap);
 constexpr size_t kLatGenDynSmem = kLatAccSmem + sizeof(double) * (kLatGenERec * kLatGenECap + kLatPtCap);
 constexpr size_t kLatTabDynSmem = kLatAccSmem + sizeof(double) * kLatPtCap;
 
@@ -60,7 +71,7 @@ struct SmemPointEdges {
     // leg_angles from the pair's stored angle atan(min(a1, a2) / max(a1, a2)); a pair that (A2) did not
     // evaluate (its legs' rounded square sum beyond 2h while the point's is within) forms it here
     __device__ __forceinline__ void leg_angles(int e, T a1, T ia1, T a2, T ia2, T& pa, T& pb) const {
-        const double t = ang[slot[e]];
+        const double t = ang ? ang[slot[e]] : -1.0;
         if (t < 0.0) {
             kiwi_b200::leg_angles(a1, ia1, a2, ia2, pa, pb);
             return;
@@ -126,7 +137,8 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     double* s_D3 = s_chunk + kLatECap2;
     double* s_E = s_chunk;  // generic edge records
     double* s_T = s_chunk + (GENERIC ? kLatGenERec * kLatGenECap : (TAB ? 0 : 2 * kLatECap2));
-    double* s_A = s_T + kLatPtCap;  // cubic: each edge pair's smaller in-plane angle (at its ab slot)
+    // cubic: each edge pair's smaller in-plane angle (at its ab slot), or none
+    double* s_A = kLatAngles ? s_T + kLatPtCap : nullptr;
 
     const int tz = (int)(t % g.ntz), ty = (int)((t / g.ntz) % g.nty), tx = (int)(t / ((int64_t)g.ntz * g.nty));
     const int bx = tx * kTileX, by = ty * kTileY, bz = tz * kTileZ;
@@ -284,7 +296,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                                 n_eo += 2;
                                 s_D2[sab] = s_D3[sab] = 0.0;
                                 s_D2[sba] = s_D3[sba] = 0.0;
-                                s_A[sab] = -1.0;
+                                if (kLatAngles) s_A[sab] = -1.0;
                             }
                         }
                     }
@@ -366,7 +378,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 // the pair's smaller in-plane angle (FP64 in every form: FP64 island points read it too),
                 // which the walls with legs along a and b read
                 const double vmin = fmin(vp, vq), vmax = fmax(vp, vq);
-                s_A[sab] = atan(vmin / vmax);
+                if (kLatAngles) s_A[sab] = atan(vmin / vmax);
                 if (MIXED && vmin >= kMixedIslandFrac * cp->h[j]) {
                     LatticeEdgeT<F32> f_pq, f_qp;
                     lattice_edge_pair(F32(cp->h[j]), F32(cp->ih[j]), F32(vp), F32(vq), f_pq, f_qp);

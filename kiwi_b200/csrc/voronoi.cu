@@ -48,7 +48,41 @@ struct VorCells {
     const double* vxyz;
     const int32_t* face_nbr;
     const double* volume;
+    // per face f of cell c towards a cell nb (k_face_links): twin[f] the local index of c's first face
+    // before f towards nb, or -1; back[f] the index of nb's first face towards c, or -1 (both -1 when nb
+    // is no cell)
+    const int32_t* twin;
+    const int64_t* back;
 };
+
+// The face links of every cell (one thread per cell): what the walk and the gathers would otherwise look
+// up by scanning a cell's faces for every (particle, face).
+__global__ void k_face_links(int64_t n_cells, const int64_t* __restrict__ face_off,
+                             const int32_t* __restrict__ face_nbr, int32_t* __restrict__ twin,
+                             int64_t* __restrict__ back) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    const int64_t f0 = face_off[c], f1 = face_off[c + 1];
+    for (int64_t f = f0; f < f1; ++f) {
+        const int32_t nb = face_nbr[f];
+        int32_t tw = -1;
+        int64_t bk = -1;
+        if (nb >= 0 && nb < n_cells) {
+            for (int64_t e = f0; e < f; ++e)
+                if (face_nbr[e] == nb) {
+                    tw = (int32_t)(e - f0);
+                    break;
+                }
+            for (int64_t g = face_off[nb]; g < face_off[nb + 1]; ++g)
+                if (face_nbr[g] == (int32_t)c) {
+                    bk = g;
+                    break;
+                }
+        }
+        twin[f] = tw;
+        back[f] = bk;
+    }
+}
 
 constexpr int kBfsWarpsPerBlock = 4;
 constexpr int kGatherThreads = 128;
@@ -155,13 +189,7 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                         if ((int)(mv & 0xffffffffLL) < rank && f - fa < 64) earlier |= 1ull << (f - fa);
                         continue;
                     }
-                    bool dup = false;
-                    for (int64_t e = fa; e < f; ++e)
-                        if (C.face_nbr[e] == nb) {
-                            dup = true;
-                            break;
-                        }
-                    if (dup) continue;
+                    if (C.twin[f] >= 0) continue;  // an earlier face of this cell named nb already
                     const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
                     if (!face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]))) continue;
                     if (f - fa < 64) cand0 |= 1ull << (f - fa);
@@ -189,18 +217,9 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                         int32_t code = -1;
                         if (nb >= 0 && nb < C.n_cells) {
                             const long long mv = mark[nb];
-                            if ((mv >> 32) == mk && (int)(mv & 0xffffffffLL) < rank)
-                                for (int64_t e = C.face_off[nb]; e < C.face_off[nb + 1]; ++e)
-                                    if (C.face_nbr[e] == cell) {
-                                        code = (int32_t)(mv & 0xffffffffLL);
-                                        break;
-                                    }
-                            if (code < 0)
-                                for (int64_t e = fa; e < f; ++e)
-                                    if (C.face_nbr[e] == nb) {
-                                        code = -2 - (int32_t)(e - fa);
-                                        break;
-                                    }
+                            if ((mv >> 32) == mk && (int)(mv & 0xffffffffLL) < rank && C.back[f] >= 0)
+                                code = (int32_t)(mv & 0xffffffffLL);
+                            if (code < 0 && C.twin[f] >= 0) code = -2 - C.twin[f];
                         }
                         fsrc[pf + (f - fa)] = code;
                     }
@@ -357,22 +376,12 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
                                 break;
                             }
                     }
-                    int64_t g = -1;
-                    if (before)
-                        for (int64_t e = C.face_off[nb]; e < C.face_off[nb + 1]; ++e)
-                            if (C.face_nbr[e] == (int32_t)cell) {
-                                g = e;
-                                break;
-                            }
+                    const int64_t g = before ? C.back[f] : -1;
                     if (g >= 0) {
                         src = g;
                         sign = -1.0;
-                    } else {
-                        for (int64_t e = f0; e < f; ++e)
-                            if (C.face_nbr[e] == nb) {
-                                src = e;
-                                break;
-                            }
+                    } else if (C.twin[f] >= 0) {
+                        src = f0 + C.twin[f];
                     }
                 }
                 const int nv = (int)(C.vert_off[src + 1] - C.vert_off[src]);
@@ -502,10 +511,7 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_sum(VorCells C, DevParti
                 if (code >= 0) {
                     // the neighbour's first face towards this cell, from the neighbour's pair
                     const int32_t nb = C.face_nbr[f];
-                    const int64_t g0 = C.face_off[nb], g1 = C.face_off[nb + 1];
-                    int64_t g = g0;
-                    while (g < g1 && C.face_nbr[g] != (int32_t)cell) ++g;  // found: the walk checked it
-                    if (g < g1) msum -= fval[pair_foff[seg + code] + (g - g0)];
+                    msum -= fval[pair_foff[seg + code] + (C.back[f] - C.face_off[nb])];
                 } else {
                     msum += fval[pf + (code == -1 ? f - f0 : (int64_t)(-2 - code))];
                 }
@@ -589,7 +595,7 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
                     const KernelChoice& kc, const CartOutputs& out_in, KiwiStats* stats, const VorInverse* inv) {
     const int64_t launches0 = ctx->launches;
     const int64_t n = P.n, nc = cells.n_cells;
-    VorCells C{nc, cells.face_off, cells.vert_off, cells.vxyz, cells.face_nbr, cells.volume};
+    VorCells C{nc, cells.face_off, cells.vert_off, cells.vxyz, cells.face_nbr, cells.volume, nullptr, nullptr};
     DevStats* d_stats = nullptr;
     double* d_meanv = nullptr;
     unsigned long long* d_next = nullptr;
@@ -601,6 +607,22 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     out.meanv = d_meanv;
     KIWI_TRY(fp64_mean_velocity(ctx, P, d_meanv));
     if (nc <= 0) return KIWI_OK;
+
+    // the faces' links (earlier twin, the neighbour's face back)
+    int64_t n_faces = 0;
+    KIWI_CUDA(ctx, cudaMemcpyAsync(&n_faces, cells.face_off + nc, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned char* links = nullptr;
+    const size_t nf_alloc = (size_t)std::max<int64_t>(n_faces, 1);
+    KIWI_TRY(scratch_t(ctx, S_VOR_LINKS, nf_alloc * (sizeof(int64_t) + sizeof(int32_t)), &links));
+    int64_t* d_back = reinterpret_cast<int64_t*>(links);
+    int32_t* d_twin = reinterpret_cast<int32_t*>(links + nf_alloc * sizeof(int64_t));
+    k_face_links<<<(unsigned)((nc + 255) / 256), 256, 0, ctx->stream>>>(nc, cells.face_off, cells.face_nbr, d_twin,
+                                                                        d_back);
+    KIWI_LAUNCHED(ctx);
+    C.twin = d_twin;
+    C.back = d_back;
 
     // BFS work slots: a visited marker and a queue of n_cells entries each
     int sms = 0;
