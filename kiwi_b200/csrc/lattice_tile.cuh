@@ -41,6 +41,9 @@ constexpr int kLatPtCap = KIWI_LAT_PT_CAP;  // lattice points per chunk
 constexpr int kLatECap2 = KIWI_LAT_E_CAP;   // cubic edge tiers per chunk
 static_assert(kTileX <= 15 && kTileY <= 15 && kTileZ <= 15 && kLatPMax <= 32, "packed point-list entries");
 static_assert(kLatECap2 <= 2048 && kLatGenECap <= 2048, "packed edge-pair entries (11-bit slots)");
+// (C1) keeps a chunk's (particle, cell) pair values in its edge-tier buffer: a box has fewer cells than
+// lattice points, so ctot < ptot <= kLatPtCap
+static_assert(2 * kLatECap2 >= kLatPtCap && kLatGenERec * kLatGenECap >= kLatPtCap, "pair values fit the edge buffer");
 // Each edge pair's in-plane angle formed once (1) or every point's walls forming theirs (0).
 #ifndef KIWI_LAT_ANGLES
 #define KIWI_LAT_ANGLES 1
@@ -99,9 +102,10 @@ __device__ __forceinline__ void lat_add_stat(unsigned long long* dst, unsigned l
 struct LatChunk {
     double x[kLatPMax], y[kLatPMax], z[kLatPMax], h[kLatPMax], m[kLatPMax], vx[kLatPMax], vy[kLatPMax], vz[kLatPMax],
         ih[kLatPMax];
-    int lo[kLatPMax][3], dim[kLatPMax][3], eoff[kLatPMax], poff[kLatPMax];
-    uint32_t mag[kLatPMax][4];  // div_magic of n0', n1', n2' and n1' n2'
-    int np, etot, ptot;
+    int lo[kLatPMax][3], dim[kLatPMax][3], eoff[kLatPMax], poff[kLatPMax], coff[kLatPMax];
+    uint32_t mag[kLatPMax][4];   // div_magic of n0', n1', n2' and n1' n2'
+    uint32_t cmag[kLatPMax][2];  // div_magic of n2 and n1 n2 (the box's cells)
+    int np, etot, ptot, ctot;
 };
 
 // The chunk of a tile's particle list (ascending particle index) is walked in four phases separated by
@@ -185,7 +189,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     // point capacities take, at most 32)
     auto load_chunk = [&](LatChunk* dst, int64_t at) {
         const int64_t idx = at + lane;
-        int ne = 0, npt = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
+        int ne = 0, npt = 0, ncl = 0, lo0 = 0, lo1 = 0, lo2 = 0, d0 = 0, d1 = 0, d2 = 0;
         double px = 0, py = 0, pz = 0, ph = 0, pm = 0, pvx = 0, pvy = 0, pvz = 0;
         if (idx < end) {
             const uint32_t p = list[idx];
@@ -201,13 +205,16 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             const int n0 = d0 + 1, n1 = d1 + 1, n2 = d2 + 1;
             ne = TAB ? 0 : 2 * (n0 * n1 + n0 * n2 + n1 * n2);
             npt = n0 * n1 * n2;
+            ncl = d0 * d1 * d2;
         }
-        int ie = ne, ip = npt;
+        int ie = ne, ip = npt, ic = ncl;
         for (int o = 1; o < 32; o <<= 1) {
             const int ve = __shfl_up_sync(0xffffffffu, ie, o), vp = __shfl_up_sync(0xffffffffu, ip, o);
+            const int vc = __shfl_up_sync(0xffffffffu, ic, o);
             if (lane >= o) {
                 ie += ve;
                 ip += vp;
+                ic += vc;
             }
         }
         const bool take = (idx < end) && ie <= kECap && ip <= kLatPtCap;
@@ -223,11 +230,15 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
             dst->mag[lane][1] = div_magic(d1 + 1);
             dst->mag[lane][2] = div_magic(d2 + 1);
             dst->mag[lane][3] = div_magic((d1 + 1) * (d2 + 1));
+            dst->coff[lane] = ic - ncl;
+            dst->cmag[lane][0] = div_magic(d2);
+            dst->cmag[lane][1] = div_magic(d1 * d2);
         }
         if (lane == np - 1) {
             dst->np = np;
             dst->etot = ie;
             dst->ptot = ip;
+            dst->ctot = ic;
         }
     };
     LatChunk* cp = &s_cp[0];
@@ -472,48 +483,118 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         // the next chunk's list counters (the lists of this one are read)
         if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = 0;
 
-        // (C) cells: the alternating sum of the 8 corners' octant values, in particle order
+        // (C) cells: the alternating sum of the 8 corners' octant values, added in particle order.  (C1) every
+        // (particle, cell of its box) pair of the chunk, as one flat list over all threads: the support test,
+        // the counters and the clamped alternating sum, into the chunk's edge-tier buffer (dead after (B));
+        // (C2) each thread adds, for the cells it owns, the chunk's pairs in particle order.  The tabulated
+        // body (no edge buffer) does both in the owners' loop.
+        if (TAB) {
 #pragma unroll
-        for (int c = 0; c < kLatCellsPerThread; ++c) {
-            const int li = threadIdx.x + c * kLatThreads;
-            const int lx = li / (kTileZ * kTileY), ly = (li / kTileZ) % kTileY, lz = li % kTileZ;
-            const int gx = bx + lx, gy = by + ly, gz = bz + lz;
-            double a0 = s_acc[li], a1 = s_acc[kTileCells + li];
-            double a2 = s_acc[2 * kTileCells + li], a3 = s_acc[3 * kTileCells + li];
-            for (int j = 0; j < np; ++j) {
-                const int i = gx - cp->lo[j][0], jj = gy - cp->lo[j][1], k = gz - cp->lo[j][2];
-                if (i < 0 || jj < 0 || k < 0 || i >= cp->dim[j][0] || jj >= cp->dim[j][1] || k >= cp->dim[j][2]) continue;
-                ++n_bbox;
-                const double radius = mul_rn(sup_in_h, cp->h[j]);
-                const double ex = fmax(fabs(cp->x[j] - s_cc[0][lx]) - g.hpx, 0.0);
-                const double ey = fmax(fabs(cp->y[j] - s_cc[1][ly]) - g.hpy, 0.0);
-                const double ez = fmax(fabs(cp->z[j] - s_cc[2][lz]) - g.hpz, 0.0);
-                // the support test of the pair counters, rounded as the host restatement rounds it
-                const bool in = add_rn(add_rn(mul_rn(ex, ex), mul_rn(ey, ey)), mul_rn(ez, ez)) < mul_rn(radius, radius);
-                n_sphere += in;
-                if (CULL && !in) continue;
-                ++n_eval;
-                const int n2 = cp->dim[j][2] + 1, n12 = (cp->dim[j][1] + 1) * n2;
-                const double* Tp = s_T + cp->poff[j] + (i * (cp->dim[j][1] + 1) + jj) * n2 + k;
-                const double m1 = (Tp[n12 + n2 + 1] - Tp[n12 + n2]) - (Tp[n12 + 1] - Tp[n12]);
-                const double m0 = (Tp[n2 + 1] - Tp[n2]) - (Tp[1] - Tp[0]);
-                double msum = m1 - m0;
-                if (msum < 0.0) {
-                    ++n_neg;
-                    if (msum <= -0.01) ++n_warn;
-                    msum = 0.0;
+    #pragma unroll
+            for (int c = 0; c < kLatCellsPerThread; ++c) {
+                const int li = threadIdx.x + c * kLatThreads;
+                const int lx = li / (kTileZ * kTileY), ly = (li / kTileZ) % kTileY, lz = li % kTileZ;
+                const int gx = bx + lx, gy = by + ly, gz = bz + lz;
+                double a0 = s_acc[li], a1 = s_acc[kTileCells + li];
+                double a2 = s_acc[2 * kTileCells + li], a3 = s_acc[3 * kTileCells + li];
+                for (int j = 0; j < np; ++j) {
+                    const int i = gx - cp->lo[j][0], jj = gy - cp->lo[j][1], k = gz - cp->lo[j][2];
+                    if (i < 0 || jj < 0 || k < 0 || i >= cp->dim[j][0] || jj >= cp->dim[j][1] || k >= cp->dim[j][2]) continue;
+                    ++n_bbox;
+                    const double radius = mul_rn(sup_in_h, cp->h[j]);
+                    const double ex = fmax(fabs(cp->x[j] - s_cc[0][lx]) - g.hpx, 0.0);
+                    const double ey = fmax(fabs(cp->y[j] - s_cc[1][ly]) - g.hpy, 0.0);
+                    const double ez = fmax(fabs(cp->z[j] - s_cc[2][lz]) - g.hpz, 0.0);
+                    // the support test of the pair counters, rounded as the host restatement rounds it
+                    const bool in = add_rn(add_rn(mul_rn(ex, ex), mul_rn(ey, ey)), mul_rn(ez, ez)) < mul_rn(radius, radius);
+                    n_sphere += in;
+                    if (CULL && !in) continue;
+                    ++n_eval;
+                    const int n2 = cp->dim[j][2] + 1, n12 = (cp->dim[j][1] + 1) * n2;
+                    const double* Tp = s_T + cp->poff[j] + (i * (cp->dim[j][1] + 1) + jj) * n2 + k;
+                    const double m1 = (Tp[n12 + n2 + 1] - Tp[n12 + n2]) - (Tp[n12 + 1] - Tp[n12]);
+                    const double m0 = (Tp[n2 + 1] - Tp[n2]) - (Tp[1] - Tp[0]);
+                    double msum = m1 - m0;
+                    if (msum < 0.0) {
+                        ++n_neg;
+                        if (msum <= -0.01) ++n_warn;
+                        msum = 0.0;
+                    }
+                    if (msum == 0.0) continue;
+                    const double mm = msum * cp->m[j];
+                    a0 += mm;
+                    a1 += mm * cp->vx[j];
+                    a2 += mm * cp->vy[j];
+                    a3 += mm * cp->vz[j];
                 }
-                if (msum == 0.0) continue;
-                const double mm = msum * cp->m[j];
-                a0 += mm;
-                a1 += mm * cp->vx[j];
-                a2 += mm * cp->vy[j];
-                a3 += mm * cp->vz[j];
+                s_acc[li] = a0;
+                s_acc[kTileCells + li] = a1;
+                s_acc[2 * kTileCells + li] = a2;
+                s_acc[3 * kTileCells + li] = a3;
             }
-            s_acc[li] = a0;
-            s_acc[kTileCells + li] = a1;
-            s_acc[2 * kTileCells + li] = a2;
-            s_acc[3 * kTileCells + li] = a3;
+        } else {
+            double* const s_cm = s_chunk;  // (particle, cell) pair values at coff[j] + the cell's box index
+            const int ctot = cp->ctot;
+            const int coff_l = lane < np ? cp->coff[lane] : INT_MAX;
+            for (int base = warp * 32; base < ctot; base += kLatThreads) {
+                const int it = base + lane;
+                const int j = warp_owner(base, coff_l, lane);
+                const int cof = __shfl_sync(0xffffffffu, coff_l, j & 31);
+                if (it < ctot) {
+                    const int lc = it - cof;
+                    const int d1 = cp->dim[j][1], d2 = cp->dim[j][2];
+                    const int i = div_by(lc, cp->cmag[j][1]), rem = lc - i * (d1 * d2);
+                    const int jj = div_by(rem, cp->cmag[j][0]), k = rem - jj * d2;
+                    const int lx = cp->lo[j][0] - bx + i, ly = cp->lo[j][1] - by + jj, lz = cp->lo[j][2] - bz + k;
+                    ++n_bbox;
+                    const double radius = mul_rn(sup_in_h, cp->h[j]);
+                    const double ex = fmax(fabs(cp->x[j] - s_cc[0][lx]) - g.hpx, 0.0);
+                    const double ey = fmax(fabs(cp->y[j] - s_cc[1][ly]) - g.hpy, 0.0);
+                    const double ez = fmax(fabs(cp->z[j] - s_cc[2][lz]) - g.hpz, 0.0);
+                    // the support test of the pair counters, rounded as the host restatement rounds it
+                    const bool in = add_rn(add_rn(mul_rn(ex, ex), mul_rn(ey, ey)), mul_rn(ez, ez)) < mul_rn(radius, radius);
+                    n_sphere += in;
+                    double msum = 0.0;
+                    if (!CULL || in) {
+                        ++n_eval;
+                        const int n2 = d2 + 1, n12 = (d1 + 1) * n2;
+                        const double* Tp = s_T + cp->poff[j] + (i * (d1 + 1) + jj) * n2 + k;
+                        const double m1 = (Tp[n12 + n2 + 1] - Tp[n12 + n2]) - (Tp[n12 + 1] - Tp[n12]);
+                        const double m0 = (Tp[n2 + 1] - Tp[n2]) - (Tp[1] - Tp[0]);
+                        msum = m1 - m0;
+                        if (msum < 0.0) {
+                            ++n_neg;
+                            if (msum <= -0.01) ++n_warn;
+                            msum = 0.0;
+                        }
+                    }
+                    s_cm[it] = msum;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int c = 0; c < kLatCellsPerThread; ++c) {
+                const int li = threadIdx.x + c * kLatThreads;
+                const int gx = bx + li / (kTileZ * kTileY), gy = by + (li / kTileZ) % kTileY, gz = bz + li % kTileZ;
+                double a0 = s_acc[li], a1 = s_acc[kTileCells + li];
+                double a2 = s_acc[2 * kTileCells + li], a3 = s_acc[3 * kTileCells + li];
+                for (int j = 0; j < np; ++j) {
+                    const int i = gx - cp->lo[j][0], jj = gy - cp->lo[j][1], k = gz - cp->lo[j][2];
+                    const int d1 = cp->dim[j][1], d2 = cp->dim[j][2];
+                    if (i < 0 || jj < 0 || k < 0 || i >= cp->dim[j][0] || jj >= d1 || k >= d2) continue;
+                    const double msum = s_cm[cp->coff[j] + (i * d1 + jj) * d2 + k];
+                    if (msum == 0.0) continue;
+                    const double mm = msum * cp->m[j];
+                    a0 += mm;
+                    a1 += mm * cp->vx[j];
+                    a2 += mm * cp->vy[j];
+                    a3 += mm * cp->vz[j];
+                }
+                s_acc[li] = a0;
+                s_acc[kTileCells + li] = a1;
+                s_acc[2 * kTileCells + li] = a2;
+                s_acc[3 * kTileCells + li] = a3;
+            }
         }
         __syncthreads();
         pos += np;
