@@ -470,12 +470,18 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_faces(VorCells C, DevPar
         const double x0 = P.x[p], y0 = P.y[p], z0 = P.z[p], h = P.h[p];
         const double radius = mul_rn(support_in_h, h);
         const int64_t pf = pair_foff[pk];
+        // each lane advances to its own next face to evaluate, so that the lanes of a warp (different
+        // particles, whose walks borrow different faces) evaluate their i-th own faces together instead of
+        // idling through the faces the others evaluate
+        int64_t f = f0;
 #pragma unroll 1
-        for (int64_t f = f0; f < f1; ++f) {
-            if (fsrc[pf + (f - f0)] != -1) continue;
+        for (;;) {
+            while (f < f1 && fsrc[pf + (f - f0)] != -1) ++f;
+            if (f >= f1) break;
             const int nv = (int)(C.vert_off[f + 1] - C.vert_off[f]);
             const double* verts = staged ? s_v + 3 * (C.vert_off[f] - v0) : C.vxyz + 3 * C.vert_off[f];
             fval[pf + (f - f0)] = vor_face<MODE>(verts, nv, x0, y0, z0, h, radius, kernel, tab, &n_clamp);
+            ++f;
         }
     }
     const unsigned long long n_cl = warp_sum_u64(n_clamp);
