@@ -39,6 +39,8 @@ struct KiwiCtx {
     size_t tab_bytes = 0;
     // Voronoi maps: each face value evaluated once through per-(pair, face) tables (kiwi_ctx_set_voronoi_face_tables)
     bool face_tables = true;
+    // Voronoi maps: the pair and face totals of the last map, the sizes the next map's single walk reserves
+    int64_t vor_pairs_hint = 0, vor_faces_hint = 0;
 };
 
 namespace kiwi_b200 {
@@ -168,7 +170,8 @@ enum ScratchSlot {
     S_VOR_FSRC,      // Voronoi walk: per (pair, face), where its value comes from
     S_VOR_FVAL,      // Voronoi map: per (pair, face), the face's integral
     S_VOR_LINKS,     // Voronoi map: per face, its earlier twin in the cell and the neighbour's face back
+    S_VOR_STAGE,     // Voronoi walk: the single walk's staging area
 };
-static_assert(S_VOR_LINKS < KiwiCtx::kSlots, "scratch slots");
+static_assert(S_VOR_STAGE < KiwiCtx::kSlots, "scratch slots");
 
 }  // namespace kiwi_b200

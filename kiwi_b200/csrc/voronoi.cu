@@ -93,8 +93,21 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
     return v;
 }
 
-// marker value of particle p in pass `pass`: distinct for every (particle, pass), never -1
-__device__ __forceinline__ int marker(int64_t p, int pass) { return (int)(2 * p + pass); }
+// marker value of particle p in pass `pass` (0, 1 or 2): distinct for every (particle, pass), never -1
+__device__ __forceinline__ int marker(int64_t p, int pass) { return (int)(3 * p + pass); }
+
+// The single walk's staging area (pass 2): each particle's pairs and face sources, at places reserved in
+// walk-completion order with two atomic counters; k_vor_remap then lays them out particle by particle.
+struct VorStage {
+    unsigned long long* ctr;  // [0] pairs reserved, [1] faces reserved, [2] overflow
+    int64_t cap_pairs, cap_faces;
+    int32_t* cells;
+    unsigned long long* mask;
+    int64_t* floc;   // the pair's first face, relative to its particle's first face
+    int32_t* fsrc;
+    int64_t* start;  // per particle: its first pair and its first face in the staging area
+    int64_t* fstart;
+};
 
 // One warp per particle: the particle's BFS over the cell graph in the reference's order
 // (src/mapping.cpp:441-460): cells are processed first in, first out; a processed cell's faces are taken
@@ -126,7 +139,7 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                                                                     int64_t* __restrict__ fcounts,
                                                                     const int64_t* __restrict__ foffs,
                                                                     int64_t* __restrict__ pair_foff,
-                                                                    int32_t* __restrict__ fsrc) {
+                                                                    int32_t* __restrict__ fsrc, VorStage stg) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * kBfsWarpsPerBlock + warp;
     long long* mark = mark_base + slot * C.n_cells;
@@ -141,8 +154,8 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
         const int32_t k0 = home[p];
         if (!(h > 0.0) || k0 < 0 || k0 >= C.n_cells) {
             if (lane == 0) {
-                if (pass == 0) counts[p] = 0;
-                if (pass == 0 && fcounts) fcounts[p] = 0;
+                if (pass != 1) counts[p] = 0;
+                if (pass != 1 && fcounts) fcounts[p] = 0;
                 if (h > 0.0) ++n_unresolved;
             }
             continue;
@@ -250,24 +263,103 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
             head += batch;
             __syncwarp();
         }
-        if (pass == 0 && fcounts) {
+        if (pass != 1 && fcounts) {
             for (int d = 16; d > 0; d >>= 1) nface += __shfl_down_sync(0xffffffffu, nface, d);
+            nface = __shfl_sync(0xffffffffu, nface, 0);
             if (lane == 0) fcounts[p] = nface;
         }
-        if (pass == 0 && lane == 0) {
+        if (pass != 1 && lane == 0) {
             counts[p] = tail;
             if (tail == 1) ++n_unmapped;
+        }
+        if (pass == 2) {
+            // the single walk: reserve this particle's pairs and faces, then write them.  The marks hold
+            // every visited cell's queue position, so each face's source is decided as pass 1 decides it
+            // during its walk (a neighbour processed earlier is one with a smaller queue position).
+            unsigned long long s0 = 0, fs0 = 0;
+            if (lane == 0) {
+                s0 = atomicAdd(&stg.ctr[0], (unsigned long long)tail);
+                fs0 = atomicAdd(&stg.ctr[1], (unsigned long long)nface);
+            }
+            s0 = __shfl_sync(0xffffffffu, s0, 0);
+            fs0 = __shfl_sync(0xffffffffu, fs0, 0);
+            if (s0 + tail > (unsigned long long)stg.cap_pairs || fs0 + nface > (unsigned long long)stg.cap_faces) {
+                if (lane == 0) atomicOr(&stg.ctr[2], 1ull);
+            } else {
+                if (lane == 0) {
+                    stg.start[p] = (int64_t)s0;
+                    stg.fstart[p] = (int64_t)fs0;
+                }
+                int64_t fc = 0;
+                for (int base = 0; base < tail; base += 32) {
+                    const int r = base + lane;
+                    int32_t cell = 0;
+                    int64_t fa = 0, nf = 0;
+                    if (r < tail) {
+                        cell = queue[r];
+                        fa = C.face_off[cell];
+                        nf = C.face_off[cell + 1] - fa;
+                    }
+                    int64_t incl = nf;
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const int64_t v = __shfl_up_sync(0xffffffffu, incl, d);
+                        if (lane >= d) incl += v;
+                    }
+                    if (r < tail) {
+                        const int64_t fl = fc + incl - nf;
+                        unsigned long long earlier = 0;
+                        for (int64_t f = fa; f < fa + nf; ++f) {
+                            const int32_t nb = C.face_nbr[f];
+                            int32_t code = -1;
+                            if (nb >= 0 && nb < C.n_cells) {
+                                const long long mv = mark[nb];
+                                const bool before = (mv >> 32) == mk && (int)(mv & 0xffffffffLL) < r;
+                                if (before && f - fa < 64) earlier |= 1ull << (f - fa);
+                                if (before && C.back[f] >= 0) code = (int32_t)(mv & 0xffffffffLL);
+                                if (code < 0 && C.twin[f] >= 0) code = -2 - C.twin[f];
+                            }
+                            stg.fsrc[fs0 + fl + (f - fa)] = code;
+                        }
+                        stg.cells[s0 + r] = cell;
+                        stg.mask[s0 + r] = earlier;
+                        stg.floc[s0 + r] = fl;
+                    }
+                    fc += __shfl_sync(0xffffffffu, incl, 31);
+                }
+            }
         }
         __syncwarp();
     }
     n_unresolved = warp_sum_u64(n_unresolved);
     n_unmapped = warp_sum_u64(n_unmapped);
     n_limit = warp_sum_u64(n_limit);
-    if (lane == 0 && pass == 0) {
+    if (lane == 0 && pass != 1) {
         if (n_unresolved) atomicAdd(&st->skipped_outside, n_unresolved);
         if (n_unmapped) atomicAdd(&st->tile_pairs, n_unmapped);  // reported as "unmapped" by the caller
     }
     if (lane == 0 && n_limit) atomicAdd(&st->limit_hit, n_limit);
+}
+
+// The single walk's staging area laid out particle by particle (one warp per particle): the same arrays as
+// the two-pass walk writes -- pair_cells, pair_mask, pair_foff at offs[p], the face sources at foffs[p].
+__global__ void k_vor_remap(int64_t n, VorStage stg, const int64_t* __restrict__ counts,
+                            const int64_t* __restrict__ fcounts, const int64_t* __restrict__ offs,
+                            const int64_t* __restrict__ foffs, int32_t* __restrict__ pair_cells,
+                            unsigned long long* __restrict__ pair_mask, int64_t* __restrict__ pair_foff,
+                            int32_t* __restrict__ fsrc) {
+    const int64_t p = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (p >= n) return;
+    const int64_t cnt = counts[p], fcnt = fcounts[p];
+    if (cnt == 0) return;
+    const int64_t s0 = stg.start[p], d0 = offs[p], fs0 = stg.fstart[p], fd0 = foffs[p];
+    for (int64_t r = lane; r < cnt; r += 32) {
+        pair_cells[d0 + r] = stg.cells[s0 + r];
+        pair_mask[d0 + r] = stg.mask[s0 + r];
+        if (pair_foff) pair_foff[d0 + r] = fd0 + stg.floc[s0 + r];
+    }
+    if (fsrc)
+        for (int64_t q = lane; q < fcnt; q += 32) fsrc[fd0 + q] = stg.fsrc[fs0 + q];
 }
 
 // pair k (particle p's visited cells in BFS order, at offs[p]) -> (key = cell, value = k)
@@ -656,12 +748,52 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_TRY(scratch_t(ctx, S_VOR_FCOUNT, (size_t)std::max<int64_t>(n, 1), &fcounts));
     KIWI_TRY(scratch_t(ctx, S_VOR_FOFFS, (size_t)std::max<int64_t>(n, 1) + 1, &foffs));
     int64_t* d_ftotal = foffs + std::max<int64_t>(n, 1);
-    KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
-    if (n > 0) {
-        k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 0, d_next, mark, queue,
-                                                                     counts, nullptr, nullptr, nullptr, d_stats,
-                                                                     fcounts, nullptr, nullptr, nullptr);
-        KIWI_LAUNCHED(ctx);
+    // One walk when an earlier map on this context gave the totals to reserve (with room to spare): each
+    // particle's pairs and face sources go to a staging area and are laid out particle by particle after;
+    // otherwise (or if the reservation overflows) one walk counts and a second writes.
+    VorStage stg{};
+    bool single = false;
+    if (n > 0 && ctx->face_tables && ctx->vor_pairs_hint > 0) {
+        const int64_t cap_p = ctx->vor_pairs_hint + ctx->vor_pairs_hint / 4 + 4096;
+        const int64_t cap_f = ctx->vor_faces_hint + ctx->vor_faces_hint / 4 + 65536;
+        const size_t bytes = 3 * sizeof(unsigned long long) + 2 * sizeof(int64_t) * (size_t)n +
+                             (size_t)cap_p * (sizeof(unsigned long long) + sizeof(int64_t) + sizeof(int32_t)) +
+                             (size_t)cap_f * sizeof(int32_t);
+        if (bytes <= ((size_t)24 << 30)) {
+            unsigned char* blob = nullptr;
+            KIWI_TRY(scratch_t(ctx, S_VOR_STAGE, bytes, &blob));
+            unsigned char* q = blob;
+            stg.ctr = reinterpret_cast<unsigned long long*>(q), q += 3 * sizeof(unsigned long long);
+            stg.start = reinterpret_cast<int64_t*>(q), q += sizeof(int64_t) * (size_t)n;
+            stg.fstart = reinterpret_cast<int64_t*>(q), q += sizeof(int64_t) * (size_t)n;
+            stg.mask = reinterpret_cast<unsigned long long*>(q), q += sizeof(unsigned long long) * (size_t)cap_p;
+            stg.floc = reinterpret_cast<int64_t*>(q), q += sizeof(int64_t) * (size_t)cap_p;
+            stg.cells = reinterpret_cast<int32_t*>(q), q += sizeof(int32_t) * (size_t)cap_p;
+            stg.fsrc = reinterpret_cast<int32_t*>(q);
+            stg.cap_pairs = cap_p;
+            stg.cap_faces = cap_f;
+            KIWI_CUDA(ctx, cudaMemsetAsync(stg.ctr, 0, 3 * sizeof(unsigned long long), ctx->stream));
+            KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
+            k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 2, d_next, mark, queue,
+                                                                         counts, nullptr, nullptr, nullptr, d_stats,
+                                                                         fcounts, nullptr, nullptr, nullptr, stg);
+            KIWI_LAUNCHED(ctx);
+            unsigned long long ovf = 0;
+            KIWI_CUDA(ctx, cudaMemcpyAsync(&ovf, stg.ctr + 2, sizeof ovf, cudaMemcpyDeviceToHost, ctx->stream));
+            KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            single = ovf == 0;
+            if (!single) KIWI_CUDA(ctx, cudaMemsetAsync(d_stats, 0, sizeof(DevStats), ctx->stream));
+        }
+    }
+    if (!single) {
+        KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
+        if (n > 0) {
+            k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 0, d_next, mark, queue,
+                                                                         counts, nullptr, nullptr, nullptr, d_stats,
+                                                                         fcounts, nullptr, nullptr, nullptr,
+                                                                         VorStage{});
+            KIWI_LAUNCHED(ctx);
+        }
     }
     KIWI_TRY(exclusive_scan<int64_t>(ctx, counts, n, offs, d_total));
     KIWI_TRY(exclusive_scan<int64_t>(ctx, fcounts, n, foffs, d_ftotal));
@@ -669,6 +801,8 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_CUDA(ctx, cudaMemcpyAsync(&total, d_total, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
     KIWI_CUDA(ctx, cudaMemcpyAsync(&total_faces, d_ftotal, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx->stream));
     KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->vor_pairs_hint = total;
+    ctx->vor_faces_hint = total_faces;
     // the face tables (each (pair, face) value evaluated once) when they fit a memory budget; else the
     // single-launch gather, which evaluates a shared face on both sides
     const int64_t face_bytes = total_faces * (int64_t)(sizeof(double) + sizeof(int32_t)) + total * 8;
@@ -693,12 +827,19 @@ int voronoi_map_dev(KiwiCtx* ctx, const DevParticles& P, const int32_t* d_home, 
     KIWI_TRY(scratch_t(ctx, S_VALS1, (size_t)std::max<int64_t>(total, 1), &v1));
     const uint32_t* plist = v0;
     if (total > 0) {
-        // pass 1: write each particle's visited cells at its offset
-        KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
-        k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 1, d_next, mark, queue,
-                                                                     counts, offs, pair_cells, pair_mask, d_stats,
-                                                                     nullptr, foffs, pair_foff, fsrc);
-        KIWI_LAUNCHED(ctx);
+        if (single) {
+            // the staged pairs and face sources, particle by particle
+            k_vor_remap<<<(unsigned)((n * 32 + 255) / 256), 256, 0, ctx->stream>>>(
+                n, stg, counts, fcounts, offs, foffs, pair_cells, pair_mask, pair_foff, fsrc);
+            KIWI_LAUNCHED(ctx);
+        } else {
+            // pass 1: write each particle's visited cells at its offset
+            KIWI_CUDA(ctx, cudaMemsetAsync(d_next, 0, sizeof(unsigned long long), ctx->stream));
+            k_vor_bfs<<<blocks, 32 * kBfsWarpsPerBlock, 0, ctx->stream>>>(C, P, d_home, sup, 1, d_next, mark, queue,
+                                                                         counts, offs, pair_cells, pair_mask, d_stats,
+                                                                         nullptr, foffs, pair_foff, fsrc, VorStage{});
+            KIWI_LAUNCHED(ctx);
+        }
         k_vor_pairs<<<(unsigned)((total + 255) / 256), 256, 0, ctx->stream>>>(pair_cells, total, k0, v0);
         KIWI_LAUNCHED(ctx);
         int key_bits = 1;

@@ -249,3 +249,33 @@ def test_face_tables_equal_single_launch(kiwi, ctx):
             assert a.stats["neg_clamped"] == b.stats["neg_clamped"]
     finally:
         ctx.set_voronoi_face_tables(True)
+
+
+def test_single_walk_equals_two_walks(kiwi):
+    """After a first map, a context reserves the next map's pairs from the last totals and walks once (the
+    particles' pairs and face sources staged, then laid out particle by particle); a map whose pairs exceed
+    the reservation falls back to counting and writing in two walks.  Every path gives the same results bit
+    for bit: a fresh context's first map (two walks), the second map on it (one walk), and a larger map
+    after a smaller one (reservation overflows, two walks)."""
+    d, P, geo = _load(GOLDEN[0])
+    fresh = kiwi.Context(0)
+    a = kiwi.map_voronoi(P, d["home"], geo, raw=True, ctx=fresh)
+    b = kiwi.map_voronoi(P, d["home"], geo, raw=True, ctx=fresh)
+    c = kiwi.map_voronoi(P, d["home"], geo, raw=True, ctx=fresh)
+    for r in (b, c):
+        assert np.array_equal(a.raw, r.raw)
+        assert r.stats["visited_pairs"] == a.stats["visited_pairs"]
+        assert r.stats["neg_clamped"] == a.stats["neg_clamped"]
+        assert r.stats["skipped_outside"] == a.stats["skipped_outside"]
+    # a map of a few particles sets a small reservation; the full map after it overflows it
+    small = {k: v[:5].copy() for k, v in P.items()}
+    other = kiwi.Context(0)
+    kiwi.map_voronoi(small, d["home"][:5], geo, raw=True, ctx=other)
+    e = kiwi.map_voronoi(P, d["home"], geo, raw=True, ctx=other)
+    assert np.array_equal(a.raw, e.raw)
+    assert e.stats["visited_pairs"] == a.stats["visited_pairs"]
+    # and the inverse map (pair values kept) after a single walk
+    i1 = kiwi.inverse_map_voronoi(P, d["home"], geo, ctx=fresh)
+    i2 = kiwi.inverse_map_voronoi(P, d["home"], geo, ctx=kiwi.Context(0))
+    assert np.array_equal(i1.m_recovered, i2.m_recovered)
+    assert np.array_equal(i1.coverage, i2.coverage)
