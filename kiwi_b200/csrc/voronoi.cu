@@ -87,6 +87,9 @@ __global__ void k_face_links(int64_t n_cells, const int64_t* __restrict__ face_o
 constexpr int kBfsWarpsPerBlock = 4;
 constexpr int kGatherThreads = 128;
 constexpr int kGatherVertCap = 1536;  // vertices staged in shared memory per cell (36 KB)
+// k_vor_faces: a face item packs (pair slot << 7 | face), for cells of at most 128 faces
+constexpr int kFaceItemMaxFaces = 128;
+constexpr int kFaceItemCap = 2048;  // 4 KB of items beside the 36 KB of staged vertices
 
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -555,25 +558,78 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_faces(VorCells C, DevPar
         for (int64_t i = threadIdx.x; i < 3 * (v1 - v0); i += kGatherThreads) s_v[i] = C.vxyz[3 * v0 + i];
     __syncthreads();
     const int64_t beg = range[2 * cell], end = range[2 * cell + 1];
+    const int nf = (int)(f1 - f0);
     unsigned n_clamp = 0;
-    for (int64_t k = beg + threadIdx.x; k < end; k += kGatherThreads) {
-        const int64_t pk = plist[k];
-        const int64_t p = pair_particle(offs, P.n, pk);
-        const double x0 = P.x[p], y0 = P.y[p], z0 = P.z[p], h = P.h[p];
-        const double radius = mul_rn(support_in_h, h);
-        const int64_t pf = pair_foff[pk];
-        // each lane advances to its own next face to evaluate, so that the lanes of a warp (different
-        // particles, whose walks borrow different faces) evaluate their i-th own faces together instead of
-        // idling through the faces the others evaluate
-        int64_t f = f0;
+    if (nf > kFaceItemMaxFaces) {
+        // (a cell of more faces than an item packs; the walk refuses such a map afterwards)
+        for (int64_t k = beg + threadIdx.x; k < end; k += kGatherThreads) {
+            const int64_t pk = plist[k];
+            const int64_t p = pair_particle(offs, P.n, pk);
+            const double h = P.h[p];
+            const int64_t pf = pair_foff[pk];
 #pragma unroll 1
-        for (;;) {
-            while (f < f1 && fsrc[pf + (f - f0)] != -1) ++f;
-            if (f >= f1) break;
-            const int nv = (int)(C.vert_off[f + 1] - C.vert_off[f]);
-            const double* verts = staged ? s_v + 3 * (C.vert_off[f] - v0) : C.vxyz + 3 * C.vert_off[f];
-            fval[pf + (f - f0)] = vor_face<MODE>(verts, nv, x0, y0, z0, h, radius, kernel, tab, &n_clamp);
-            ++f;
+            for (int64_t f = f0; f < f1; ++f) {
+                if (fsrc[pf + (f - f0)] != -1) continue;
+                const int nv = (int)(C.vert_off[f + 1] - C.vert_off[f]);
+                fval[pf + (f - f0)] = vor_face<MODE>(C.vxyz + 3 * C.vert_off[f], nv, P.x[p], P.y[p], P.z[p], h,
+                                                     mul_rn(support_in_h, h), kernel, tab, &n_clamp);
+            }
+        }
+    } else {
+        // The cell's pairs in groups: each thread takes one pair and lists the faces it evaluates itself
+        // (its walk did not borrow them); the group's list is then evaluated by all threads at once, so
+        // that no lane idles through a face another pair evaluates.
+        __shared__ double s_px[kGatherThreads], s_py[kGatherThreads], s_pz[kGatherThreads], s_ph[kGatherThreads];
+        __shared__ int64_t s_pf[kGatherThreads];
+        __shared__ uint16_t s_items[kFaceItemCap];
+        __shared__ int s_wsum[kGatherThreads / 32];
+        const int group = min(kGatherThreads, kFaceItemCap / max(nf, 1));
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int64_t base = beg; base < end; base += group) {
+            const int64_t k = base + threadIdx.x;
+            int own = 0;
+            int64_t pf = 0;
+            if (threadIdx.x < group && k < end) {
+                const int64_t pk = plist[k];
+                const int64_t p = pair_particle(offs, P.n, pk);
+                pf = pair_foff[pk];
+                s_px[threadIdx.x] = P.x[p];
+                s_py[threadIdx.x] = P.y[p];
+                s_pz[threadIdx.x] = P.z[p];
+                s_ph[threadIdx.x] = P.h[p];
+                s_pf[threadIdx.x] = pf;
+                for (int f = 0; f < nf; ++f) own += fsrc[pf + f] == -1;
+            }
+            // block exclusive scan of the own-face counts
+            int incl = own;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                if (lane >= d) incl += v;
+            }
+            if (lane == 31) s_wsum[warp] = incl;
+            __syncthreads();
+            int wbase = 0, total = 0;
+            for (int w = 0; w < kGatherThreads / 32; ++w) {
+                if (w < warp) wbase += s_wsum[w];
+                total += s_wsum[w];
+            }
+            if (own > 0) {
+                int o = wbase + incl - own;
+                for (int f = 0; f < nf; ++f)
+                    if (fsrc[pf + f] == -1) s_items[o++] = (uint16_t)(threadIdx.x << 7 | f);
+            }
+            __syncthreads();
+            for (int it = threadIdx.x; it < total; it += kGatherThreads) {
+                const int item = s_items[it];
+                const int t = item >> 7, fl = item & 127;
+                const int64_t f = f0 + fl;
+                const int nv = (int)(C.vert_off[f + 1] - C.vert_off[f]);
+                const double* verts = staged ? s_v + 3 * (C.vert_off[f] - v0) : C.vxyz + 3 * C.vert_off[f];
+                const double h = s_ph[t];
+                fval[s_pf[t] + fl] = vor_face<MODE>(verts, nv, s_px[t], s_py[t], s_pz[t], h,
+                                                    mul_rn(support_in_h, h), kernel, tab, &n_clamp);
+            }
+            __syncthreads();
         }
     }
     const unsigned long long n_cl = warp_sum_u64(n_clamp);
