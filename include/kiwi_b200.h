@@ -119,8 +119,11 @@ void* kiwi_ctx_stream(KiwiCtx* ctx);             /* the context's cudaStream_t *
 int kiwi_ctx_synchronize(KiwiCtx* ctx);
 /* Voronoi maps on this context: enable = 1 (the default) evaluates every face value once per particle
  * through per-(pair, face) tables (12 bytes per face of every visited cell; a map whose tables would
- * exceed 48 GB runs without them); enable = 0 runs one launch that evaluates a face shared by two visited
- * cells on both sides.  Both give the same results bit for bit.  No counterpart in the reference. */
+ * exceed 48 GB runs without them), and a map after an earlier one on the same context walks the cell
+ * graph once, into space reserved from the earlier map's totals (another ~24 bytes per visited pair and
+ * 4 per face; a map that outgrows the reservation walks twice); enable = 0 walks twice and runs one
+ * launch that evaluates a face shared by two visited cells on both sides.  Every path gives the same
+ * results bit for bit.  No counterpart in the reference. */
 int kiwi_ctx_set_voronoi_face_tables(KiwiCtx* ctx, int enable);
 const char* kiwi_version(void);
 /* Measured FP64 FMA throughput of the context's GPU in TFLOP/s (a short probe kernel).  No counterpart in
