@@ -19,6 +19,22 @@ using namespace kiwi_b200;
 
 namespace {
 
+// Heaviest-first order of a grid's tiles (build parameter; 1 in the default build).
+#ifndef KIWI_TILE_LPT
+#define KIWI_TILE_LPT 1
+#endif
+constexpr bool kTileLpt = KIWI_TILE_LPT != 0;
+
+// sort keys of the heaviest-first tile order: descending (tile, particle) entry count, value the tile
+__global__ void k_tile_order_keys(const int64_t* __restrict__ range, int64_t ntiles, uint32_t* __restrict__ keys,
+                                  uint32_t* __restrict__ vals) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const int64_t e = range[2 * t + 1] - range[2 * t];
+    keys[t] = 0xffffffffu - (uint32_t)(e < 0xffffffffLL ? e : 0xffffffffLL);
+    vals[t] = (uint32_t)t;
+}
+
 }  // namespace
 
 namespace kiwi_b200 {
@@ -172,6 +188,20 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
         KIWI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         tl.map = map;
         tl.nmap = nmap;
+    } else if (kTileLpt && !ctx->arena && ntiles > 1 && total > 0) {
+        // the whole grid, heaviest tiles first (by (tile, particle) entry count; ties in tile order), so that
+        // the dense tiles of a clustered field do not start last and leave the SMs a tail
+        uint32_t *lk0, *lv0, *lk1, *lv1;
+        KIWI_TRY(scratch_t(ctx, S_LPT_K0, (size_t)ntiles, &lk0));
+        KIWI_TRY(scratch_t(ctx, S_LPT_V0, (size_t)ntiles, &lv0));
+        KIWI_TRY(scratch_t(ctx, S_LPT_K1, (size_t)ntiles, &lk1));
+        KIWI_TRY(scratch_t(ctx, S_LPT_V1, (size_t)ntiles, &lv1));
+        k_tile_order_keys<<<(unsigned)((ntiles + 255) / 256), 256, 0, ctx->stream>>>(range, ntiles, lk0, lv0);
+        KIWI_LAUNCHED(ctx);
+        bool second = false;
+        KIWI_TRY(radix_sort_pairs(ctx, lk0, lv0, lk1, lv1, ntiles, 32, &second));
+        tl.map = reinterpret_cast<const int32_t*>(second ? lv1 : lv0);
+        tl.nmap = ntiles;
     }
 
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));

@@ -26,7 +26,7 @@ struct KiwiCtx {
     std::string err;
     int64_t launches = 0;  // kernels launched on this context (for the stats of a call)
     // Scratch slots: each is grown on demand and reused by later calls on this context.
-    static constexpr int kSlots = 48;
+    static constexpr int kSlots = 64;
     void* slot_ptr[kSlots] = {};
     size_t slot_bytes[kSlots] = {};
     // Fixed arena mode (used only by the allocation-free entry point): when `arena` is set, scratch
@@ -171,7 +171,11 @@ enum ScratchSlot {
     S_VOR_FVAL,      // Voronoi map: per (pair, face), the face's integral
     S_VOR_LINKS,     // Voronoi map: per face, its earlier twin in the cell and the neighbour's face back
     S_VOR_STAGE,     // Voronoi walk: the single walk's staging area
+    S_LPT_K0,        // heaviest-first tile order: sort keys and values (two buffers each)
+    S_LPT_V0,
+    S_LPT_K1,
+    S_LPT_V1,
 };
-static_assert(S_VOR_STAGE < KiwiCtx::kSlots, "scratch slots");
+static_assert(S_LPT_V1 < KiwiCtx::kSlots, "scratch slots");
 
 }  // namespace kiwi_b200
