@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
     __shared__ uint32_t s_mag[kAdjPMax][4];  // div_magic of n0', n1', n2' and n1' n2'
     __shared__ uint32_t s_plist[kAdjPtCap];
     __shared__ uint32_t s_hlist[kAdjECap / 2];
-    __shared__ int s_np, s_etot, s_ptot, s_nexp, s_ncheap, s_nheavy;
+    __shared__ int s_np, s_etot, s_ptot, s_nexp, s_ncheap, s_nheavy, s_ninner;
     __shared__ double s_red[kAdjLatThreads / 32][8];
     __shared__ double s_pl[3][kTileX + 1];
     extern __shared__ double s_adj[];
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                 s_np = np;
                 s_etot = ie;
                 s_ptot = ip;
-                s_nexp = s_ncheap = s_nheavy = 0;
+                s_nexp = s_ncheap = s_nheavy = s_ninner = 0;
             }
         }
         __syncthreads();
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
             const int qoff_l = lane < np ? (s_eoff[lane] >> 1) : INT_MAX;
             for (int base = warp * 32; base < qtot; base += kAdjLatThreads) {
                 const int it = base + lane;
-                bool heavy = false;
+                bool heavy = false, inner = false;
                 uint32_t hrec = 0;
                 const int j = warp_owner(base, qoff_l, lane);
                 const int qoff = __shfl_sync(0xffffffffu, qoff_l, j & 31);
@@ -248,6 +248,7 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                         lattice_generic_edge_dual<3>(K, H, qD, pD, s_E + kERec * sba);
                     } else {
                     heavy = oa != 0.0 && ob != 0.0 && oa * oa + ob * ob <= 4.0 * (h * h);
+                    inner = heavy && oa * oa + ob * ob <= h * h;
                     if (heavy) {
                         s_E[kAdjERec * sab] = oa;
                         s_E[kAdjERec * sab + 1] = ob;
@@ -258,11 +259,19 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
                     }
                     }
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, heavy);
-                int hp = 0;
-                if (lane == 0 && m) hp = atomicAdd(&s_nheavy, __popc(m));
+                // pairs within h (two passes of the edge tiers) from the end of the list, the others from the
+                // front, so that each kind runs in warps of its own
+                const unsigned mm = __ballot_sync(0xffffffffu, heavy && !inner);
+                const unsigned mi = __ballot_sync(0xffffffffu, inner);
+                int hp = 0, hi = 0;
+                if (lane == 0) {
+                    if (mm) hp = atomicAdd(&s_nheavy, __popc(mm));
+                    if (mi) hi = atomicAdd(&s_ninner, __popc(mi));
+                }
                 hp = __shfl_sync(0xffffffffu, hp, 0);
-                if (heavy) s_hlist[hp + __popc(m & ((1u << lane) - 1))] = hrec;
+                hi = __shfl_sync(0xffffffffu, hi, 0);
+                const unsigned below = (1u << lane) - 1;
+                if (heavy) s_hlist[inner ? kAdjECap / 2 - 1 - hi - __popc(mi & below) : hp + __popc(mm & below)] = hrec;
             }
         }
 
@@ -314,9 +323,9 @@ __global__ void __launch_bounds__(kAdjLatThreads, 1) k_cart_adjoint_lattice(Cart
 
         // (A2) the listed edge pairs with their derivatives (the forward kernel's lattice_edge_pair in Dual3)
         {
-            const int nheavy = s_nheavy;
-            for (int li = threadIdx.x; li < nheavy; li += kAdjLatThreads) {
-                const uint32_t rec = s_hlist[li];
+            const int nmid = s_nheavy, ninner = s_ninner;
+            for (int li = threadIdx.x; li < nmid + ninner; li += kAdjLatThreads) {
+                const uint32_t rec = s_hlist[li < nmid ? li : kAdjECap / 2 - ninner + (li - nmid)];
                 const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)((rec >> 22) & 31u);
                 const int blk = (int)(rec >> 27);
                 const int a = blk == 2 ? 1 : 0, b = blk == 0 ? 1 : 2;

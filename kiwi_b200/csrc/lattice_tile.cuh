@@ -128,7 +128,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     __shared__ LatChunk s_cp[2];
     __shared__ TabWidths s_tw;               // TAB: the table's bin widths and their reciprocals
     if (TAB && threadIdx.x == 0) s_tw = tab_widths(tab);  // read after the chunk load's barrier
-    __shared__ int s_nexp, s_ncheap, s_nheavy;
+    __shared__ int s_nexp, s_ncheap, s_nheavy, s_ninner;
     __shared__ uint32_t s_plist[TAB ? 1 : kLatPtCap];
     __shared__ uint32_t s_hlist[(GENERIC || TAB) ? 1 : kLatECap2 / 2];
     extern __shared__ double s_dyn[];
@@ -243,7 +243,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     };
     LatChunk* cp = &s_cp[0];
     if (warp == 0 && beg < end) load_chunk(cp, beg);
-    if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = 0;
+    if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = s_ninner = 0;
     __syncthreads();
 
     for (int64_t pos = beg; pos < end;) {
@@ -263,7 +263,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                 const int qoff_l = lane < np ? (cp->eoff[lane] >> 1) : INT_MAX;
                 for (int base = (warp - 1) * 32; base < qtot; base += kLatThreads - 32) {
                     const int it = base + lane;
-                    bool heavy = false;
+                    bool heavy = false, inner = false;
                     uint32_t hrec = 0;
                     const int j = warp_owner(base, qoff_l, lane);
                     const int qoff = __shfl_sync(0xffffffffu, qoff_l, j & 31);
@@ -297,6 +297,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                             const double h2 = cp->h[j] * cp->h[j];
                             const double ld2 = add_rn(mul_rn(vp, vp), mul_rn(vq, vq));
                             heavy = vp != 0.0 && vq != 0.0 && ld2 <= 4.0 * h2;
+                            inner = heavy && !(ld2 > h2);
                             if (heavy) {
                                 if (ld2 > h2) n_em += 2;
                                 else n_ei += 2;
@@ -312,11 +313,20 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                         }
                     }
                     if (!GENERIC) {
-                        const unsigned m = __ballot_sync(0xffffffffu, heavy);
-                        int hp = 0;
-                        if (lane == 0 && m) hp = atomicAdd(&s_nheavy, __popc(m));
+                        // pairs within h (two passes of the edge tiers) from the end of the list, the others
+                        // (one pass) from the front, so that each kind runs in warps of its own
+                        const unsigned mm = __ballot_sync(0xffffffffu, heavy && !inner);
+                        const unsigned mi = __ballot_sync(0xffffffffu, inner);
+                        int hp = 0, hi = 0;
+                        if (lane == 0) {
+                            if (mm) hp = atomicAdd(&s_nheavy, __popc(mm));
+                            if (mi) hi = atomicAdd(&s_ninner, __popc(mi));
+                        }
                         hp = __shfl_sync(0xffffffffu, hp, 0);
-                        if (heavy) s_hlist[hp + __popc(m & ((1u << lane) - 1))] = hrec;
+                        hi = __shfl_sync(0xffffffffu, hi, 0);
+                        const unsigned below = (1u << lane) - 1;
+                        if (heavy)
+                            s_hlist[inner ? kLatECap2 / 2 - 1 - hi - __popc(mi & below) : hp + __popc(mm & below)] = hrec;
                     }
                 }
             }
@@ -380,9 +390,9 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
 
         // (A2) the listed edge pairs (cubic)
         if (!GENERIC && !TAB) {
-            const int nheavy = s_nheavy;
-            for (int li = threadIdx.x; li < nheavy; li += kLatThreads) {
-                const uint32_t rec = s_hlist[li];
+            const int nmid = s_nheavy, ninner = s_ninner;
+            for (int li = threadIdx.x; li < nmid + ninner; li += kLatThreads) {
+                const uint32_t rec = s_hlist[li < nmid ? li : kLatECap2 / 2 - ninner + (li - nmid)];
                 const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)(rec >> 22);
                 LatticeEdge e_pq, e_qp;
                 const double vp = s_D2[sab], vq = s_D3[sab];
@@ -481,7 +491,7 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         __syncthreads();
 
         // the next chunk's list counters (the lists of this one are read)
-        if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = 0;
+        if (threadIdx.x == 0) s_nexp = s_ncheap = s_nheavy = s_ninner = 0;
 
         // (C) cells: the alternating sum of the 8 corners' octant values, added in particle order.  (C1) every
         // (particle, cell of its box) pair of the chunk, as one flat list over all threads: the support test,
