@@ -85,6 +85,7 @@ __global__ void k_face_links(int64_t n_cells, const int64_t* __restrict__ face_o
 }
 
 constexpr int kBfsWarpsPerBlock = 4;
+constexpr int kBfsCandCap = 512;  // a batch's discovery candidates listed per warp (larger batches: lane 0)
 constexpr int kGatherThreads = 128;
 constexpr int kGatherVertCap = 1536;  // vertices staged in shared memory per cell (36 KB)
 // k_vor_faces: a face item packs (pair slot << 7 | face), for cells of at most 128 faces
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                                                                     const int64_t* __restrict__ foffs,
                                                                     int64_t* __restrict__ pair_foff,
                                                                     int32_t* __restrict__ fsrc, VorStage stg) {
+    __shared__ int32_t s_cand[kBfsWarpsPerBlock][kBfsCandCap];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * kBfsWarpsPerBlock + warp;
     long long* mark = mark_base + slot * C.n_cells;
@@ -243,6 +245,46 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                 fcarry += __shfl_sync(0xffffffffu, incl, 31);
             }
             int t = tail;
+            // the batch's candidates in (cell, face) order; each is queued if no earlier candidate names the
+            // same cell and it is not queued yet -- the sequential appends' queue, with every lane at work
+            const int nc_l = __popcll(cand0) + __popcll(cand1);
+            int c_incl = nc_l;
+            for (int d = 1; d < 32; d <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, c_incl, d);
+                if (lane >= d) c_incl += v;
+            }
+            const int n_cand = __shfl_sync(0xffffffffu, c_incl, 31);
+            if (n_cand <= kBfsCandCap) {
+                int32_t* cl = s_cand[warp];
+                int o = c_incl - nc_l;
+                for (int w = 0; w < 2; ++w) {
+                    unsigned long long bits = w == 0 ? cand0 : cand1;
+                    while (bits) {
+                        const int b = __ffsll((long long)bits) - 1;
+                        bits &= bits - 1;
+                        cl[o++] = C.face_nbr[fa + 64 * w + b];
+                    }
+                }
+                __syncwarp();
+                for (int base = 0; base < n_cand; base += 32) {
+                    const int i = base + lane;
+                    int32_t nb = -1;
+                    bool keep = false;
+                    if (i < n_cand) {
+                        nb = cl[i];
+                        keep = (mark[nb] >> 32) != mk;
+                        for (int j = 0; keep && j < i; ++j) keep = cl[j] != nb;
+                    }
+                    const unsigned kb = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
+                        const int pos = t + __popc(kb & ((1u << lane) - 1));
+                        mark[nb] = (mk << 32) | (long long)pos;
+                        queue[pos] = nb;
+                    }
+                    t += __popc(kb);
+                }
+                __syncwarp();
+            } else {
             for (int L = 0; L < batch; ++L) {
                 unsigned long long c0 = __shfl_sync(0xffffffffu, cand0, L);
                 unsigned long long c1 = __shfl_sync(0xffffffffu, cand1, L);
@@ -261,6 +303,7 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                         }
                     }
                 }
+            }
             }
             tail = __shfl_sync(0xffffffffu, t, 0);
             head += batch;
