@@ -130,7 +130,8 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
     if (TAB && threadIdx.x == 0) s_tw = tab_widths(tab);  // read after the chunk load's barrier
     __shared__ int s_nexp, s_ncheap, s_nheavy, s_ninner;
     __shared__ uint32_t s_plist[TAB ? 1 : kLatPtCap];
-    __shared__ uint32_t s_hlist[(GENERIC || TAB) ? 1 : kLatECap2 / 2];
+    __shared__ uint32_t s_hlist[TAB ? 1 : kLatECap2 / 2];
+    static_assert(kLatGenECap / 2 <= kLatECap2 / 2, "generic edge pairs fit the pair list");
     extern __shared__ double s_dyn[];
     constexpr int kECap = GENERIC ? kLatGenECap : (TAB ? 0 : kLatECap2);
     // the owned cells' sums M, Px, Py, Pz: each thread's own entries (no sharing, no barrier), held in
@@ -284,13 +285,25 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                         const double pa = a == 0 ? cp->x[j] : cp->y[j], pb = b == 1 ? cp->y[j] : cp->z[j];
                         const double vp = fabs(s_pl[a][la + pi] - pa), vq = fabs(s_pl[b][lb + qi] - pb);
                         if (GENERIC) {
+                            // the records of a pair whose edge line crosses a region boundary (the expensive
+                            // ones: per boundary an arccosine, a sine and cosine and two series) are listed
+                            // and evaluated in (A2) by all warps, those crossing two or more from the end of
+                            // the list; the others (zero, or one region) here
                             const double H = mul_rn(sup_in_h, cp->h[j]);
-                            if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * cp->h[j]) {
-                                lattice_generic_edge(K, H, F32(vp), F32(vq), s_E + kLatGenERec * sab);
-                                lattice_generic_edge(K, H, F32(vq), F32(vp), s_E + kLatGenERec * sba);
-                            } else {
+                            int nseg = 0;
+                            if (vp != 0.0 && vq != 0.0) {
+                                const double q0 = vp / H, qR = vq / H;
+                                nseg = K->nreg - generic_region(K, sqrt(q0 * q0 + qR * qR)) + 1;
+                            }
+                            if (nseg <= 1) {
                                 lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
                                 lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+                            } else {
+                                heavy = true;
+                                inner = nseg >= 3;
+                                s_E[kLatGenERec * sab] = vp;
+                                s_E[kLatGenERec * sab + 1] = vq;
+                                hrec = (uint32_t)sab | (uint32_t)sba << 11 | (uint32_t)j << 22;
                             }
                             n_ei += 2;
                         } else {
@@ -312,9 +325,10 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
                             }
                         }
                     }
-                    if (!GENERIC) {
-                        // pairs within h (two passes of the edge tiers) from the end of the list, the others
-                        // (one pass) from the front, so that each kind runs in warps of its own
+                    {
+                        // pairs within h (two passes of the edge tiers; generic: two or more region
+                        // boundaries) from the end of the list, the others from the front, so that each kind
+                        // runs in warps of its own
                         const unsigned mm = __ballot_sync(0xffffffffu, heavy && !inner);
                         const unsigned mi = __ballot_sync(0xffffffffu, inner);
                         int hp = 0, hi = 0;
@@ -388,7 +402,24 @@ __device__ __forceinline__ void lattice_tile(const CartGeom& g, const DevParticl
         }
         __syncthreads();
 
-        // (A2) the listed edge pairs (cubic)
+        // (A2) the listed edge pairs
+        if (GENERIC) {
+            const int nmid = s_nheavy, ninner = s_ninner;
+            for (int li = threadIdx.x; li < nmid + ninner; li += kLatThreads) {
+                const uint32_t rec = s_hlist[li < nmid ? li : kLatECap2 / 2 - ninner + (li - nmid)];
+                const int sab = (int)(rec & 2047u), sba = (int)((rec >> 11) & 2047u), j = (int)(rec >> 22);
+                const double vp = s_E[kLatGenERec * sab], vq = s_E[kLatGenERec * sab + 1];
+                const double H = mul_rn(sup_in_h, cp->h[j]);
+                if (MIXED && fmin(vp, vq) >= kMixedIslandFrac * cp->h[j]) {
+                    lattice_generic_edge(K, H, F32(vp), F32(vq), s_E + kLatGenERec * sab);
+                    lattice_generic_edge(K, H, F32(vq), F32(vp), s_E + kLatGenERec * sba);
+                } else {
+                    lattice_generic_edge(K, H, vp, vq, s_E + kLatGenERec * sab);
+                    lattice_generic_edge(K, H, vq, vp, s_E + kLatGenERec * sba);
+                }
+            }
+            __syncthreads();
+        }
         if (!GENERIC && !TAB) {
             const int nmid = s_nheavy, ninner = s_ninner;
             for (int li = threadIdx.x; li < nmid + ninner; li += kLatThreads) {
