@@ -273,10 +273,9 @@ typedef struct KiwiBatchItem {
 typedef struct KiwiBatch KiwiBatch;
 
 /* Bins every item's particles into the cell tiles of its grid (one scan and one sort over all items),
- * orders the tiles longest-first, and records the graph.  precision: KIWI_FP64 (lattice form for the
- * cubic closed form, the reference's evaluation order for the generic kernels) or
- * KIWI_FP64_REFERENCE_ORDER; no flags.  The plan holds the tile lists of the particles' positions and
- * smoothing lengths at creation: masses and velocities may change between runs, positions and smoothing
+ * orders the tiles longest-first, and records the graph.  precision: KIWI_FP64 (lattice form),
+ * KIWI_FP64_REFERENCE_ORDER or KIWI_FP32_MIXED (the lattice form's FP32-mixed tiles); no flags.  The plan
+ * holds the tile lists of the particles' positions and smoothing lengths at creation: masses and velocities may change between runs, positions and smoothing
  * lengths may not.  Results equal kiwi_sph_to_grid_device's for each item: bit for bit in
  * KIWI_FP64_REFERENCE_ORDER; in the lattice form to rounding (within 1e-12 of the item's largest value;
  * it is compiled with FMA contraction, which the compiler forms per kernel), with equal counts. */

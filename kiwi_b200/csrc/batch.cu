@@ -104,6 +104,7 @@ void batch_free(KiwiBatch* b) {
 // The replayed work: reset the counters, the mean velocities, one persistent launch per family present.
 int batch_enqueue(KiwiBatch* b) {
     KiwiCtx* ctx = b->ctx;
+    const bool mixed = (b->precision & KIWI_FORM_MASK) == KIWI_FP32_MIXED;
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_next, 0, sizeof(unsigned long long) * kBatchFamilies, ctx->stream));
     KIWI_CUDA(ctx, cudaMemsetAsync(b->d_stats, 0, sizeof(DevStats) * b->n_items, ctx->stream));
     for (int i = 0; i < b->n_items; ++i) KIWI_TRY(fp64_mean_velocity(ctx, b->items[i].P, b->d_meanv + 4 * i));
@@ -112,11 +113,12 @@ int batch_enqueue(KiwiBatch* b) {
         if (b->merge && f == kBatchFamilyLattice) {
             KIWI_TRY(fp64_batch_gather(ctx, kBatchFamilyLatticeMerged, b->d_items, b->d_item_of_tile,
                                        b->lpt ? b->d_lpt_m : b->d_natural_m, b->merged_tiles, b->d_list, b->d_range,
-                                       b->d_next + f, b->sms * b->ctas_per_sm));
+                                       b->d_next + f, b->sms * b->ctas_per_sm, mixed));
             continue;
         }
         KIWI_TRY(fp64_batch_gather(ctx, f, b->d_items, b->d_item_of_tile, b->lpt ? b->d_lpt[f] : b->d_natural[f],
-                                   b->fam_tiles[f], b->d_list, b->d_range, b->d_next + f, b->sms * b->ctas_per_sm));
+                                   b->fam_tiles[f], b->d_list, b->d_range, b->d_next + f, b->sms * b->ctas_per_sm,
+                                   mixed));
     }
     return KIWI_OK;
 }
@@ -163,7 +165,7 @@ int batch_build(KiwiBatch* b, const KiwiBatchItem* in) {
         d.out = CartOutputs{it.density, it.vx, it.vy, it.vz, it.raw4, nullptr};
         d.kernel = kc.kernel;
         const int form = b->precision & KIWI_FORM_MASK;
-        if (form == KIWI_FP64) d.mode = kc.cubic ? kBatchLattice : kBatchLatticeGeneric;
+        if (form == KIWI_FP64 || form == KIWI_FP32_MIXED) d.mode = kc.cubic ? kBatchLattice : kBatchLatticeGeneric;
         else d.mode = kc.cubic ? kBatchGatherCubic : kBatchGatherGeneric;
         d.tile_base = b->tile_base[i];
         b->tile_base[i + 1] = b->tile_base[i] + (int64_t)d.g.ntx * d.g.nty * d.g.ntz;
@@ -338,8 +340,8 @@ int kiwi_batch_create(KiwiCtx* ctx, const KiwiBatchItem* items, int n_items, int
     const int form = precision & KIWI_FORM_MASK;
     if (precision & ~KIWI_FORM_MASK)
         return set_err(ctx, KIWI_ERR_ARG, "batch: flags (KIWI_FULL_BOX, KIWI_FP32_GUARANTEE) are not supported");
-    if (form != KIWI_FP64 && form != KIWI_FP64_REFERENCE_ORDER)
-        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "batch: only the FP64 forms are available");
+    if (form != KIWI_FP64 && form != KIWI_FP64_REFERENCE_ORDER && form != KIWI_FP32_MIXED)
+        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "batch: precision %d is not available", precision);
     KiwiBatch* b = new KiwiBatch();
     b->ctx = ctx;
     b->n_items = n_items;

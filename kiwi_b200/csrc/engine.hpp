@@ -86,11 +86,12 @@ struct BatchItemDev {
 };
 
 // kiwi_fp64.cu: one persistent launch over the tiles order[0 .. ntiles) (global tile indices) of the items
-// of one family, taken from the work counter *next (zero before the launch).
+// of one family, taken from the work counter *next (zero before the launch); mixed: the lattice families'
+// FP32-mixed tile bodies.
 int fp64_batch_prepare(KiwiCtx* ctx);
 int fp64_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
                       const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
-                      unsigned long long* d_next, int blocks);
+                      unsigned long long* d_next, int blocks, bool mixed);
 
 // mixed.cu: the FP32-mixed form (cubic spline).  cell_err (device, ncell doubles) receives each cell's
 // rounding-error bound and cell_mass (ncell doubles) its raw mass sum M.
@@ -144,6 +145,6 @@ int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P,
 int lattice_batch_prepare(KiwiCtx* ctx);
 int lattice_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
                          const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
-                         unsigned long long* d_next, int blocks);
+                         unsigned long long* d_next, int blocks, bool mixed);
 
 }  // namespace kiwi_b200

@@ -530,10 +530,11 @@ int fp64_batch_prepare(KiwiCtx* ctx) { return lattice_batch_prepare(ctx); }
 
 int fp64_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
                       const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
-                      unsigned long long* d_next, int blocks) {
+                      unsigned long long* d_next, int blocks, bool mixed) {
     if (ntiles <= 0) return KIWI_OK;
     if (family != kBatchFamilyGather)
-        return lattice_batch_gather(ctx, family, d_items, d_item_of_tile, d_order, ntiles, list, range, d_next, blocks);
+        return lattice_batch_gather(ctx, family, d_items, d_item_of_tile, d_order, ntiles, list, range, d_next, blocks,
+                                    mixed);
     k_batch_gather_persistent<<<blocks, kThreads, 0, ctx->stream>>>(d_items, d_item_of_tile, d_order, ntiles, list,
                                                                    range, d_next);
     KIWI_LAUNCHED(ctx);

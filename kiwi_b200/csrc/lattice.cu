@@ -86,8 +86,8 @@ __global__ void __launch_bounds__(kLatThreads, kLatGenMinBlocks)
 // The tiles of a batch of grids, one persistent launch per lattice family, or one for both
 // (kBatchFamilyLatticeMerged: each tile takes its item's body): each CTA takes the next of the launch's
 // tiles (order[w]) from the work counter and runs the same tile body as the single-grid kernel, so every
-// cell's summation order is that of a single-grid call.
-template <int FAMILY>
+// cell's summation order is that of a single-grid call.  MIXED: the FP32-mixed tile bodies.
+template <int FAMILY, bool MIXED>
 __global__ void __launch_bounds__(kLatThreads, 2) k_batch_lattice(const BatchItemDev* __restrict__ items,
                                                                   const int32_t* __restrict__ item_of_tile,
                                                                   const int32_t* __restrict__ order, int64_t ntiles,
@@ -104,9 +104,10 @@ __global__ void __launch_bounds__(kLatThreads, 2) k_batch_lattice(const BatchIte
         const BatchItemDev& it = items[item_of_tile[tg]];
         const int64_t tl = tg - it.tile_base;
         if (FAMILY == kBatchFamilyLattice || (FAMILY == kBatchFamilyLatticeMerged && it.mode == kBatchLattice))
-            lattice_tile<true>(it.g, it.P, list, range, tg, tl, it.out, it.st);
+            lattice_tile<true, false, false, MIXED>(it.g, it.P, list, range, tg, tl, it.out, it.st);
         else
-            lattice_tile<true, true>(it.g, it.P, list, range, tg, tl, it.out, it.st, &c_tables[it.kernel]);
+            lattice_tile<true, true, false, MIXED>(it.g, it.P, list, range, tg, tl, it.out, it.st,
+                                                   &c_tables[it.kernel]);
         __syncthreads();
     }
 }
@@ -167,28 +168,44 @@ int lattice_mixed_gather(KiwiCtx* ctx, const CartGeom& g, const DevParticles& P,
     return KIWI_OK;
 }
 
-int lattice_batch_prepare(KiwiCtx* ctx) {
-    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLattice>,
+template <bool MIXED>
+static int batch_prepare_t(KiwiCtx* ctx) {
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLattice, MIXED>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatDynSmem));
-    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLatticeGeneric>,
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLatticeGeneric, MIXED>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatGenDynSmem));
-    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLatticeMerged>,
+    KIWI_CUDA(ctx, cudaFuncSetAttribute(k_batch_lattice<kBatchFamilyLatticeMerged, MIXED>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLatMergedDynSmem));
     return KIWI_OK;
 }
 
-int lattice_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
-                         const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
-                         unsigned long long* d_next, int blocks) {
+int lattice_batch_prepare(KiwiCtx* ctx) {
+    KIWI_TRY(batch_prepare_t<false>(ctx));
+    return batch_prepare_t<true>(ctx);
+}
+
+template <bool MIXED>
+static void batch_launch_t(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
+                           const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
+                           unsigned long long* d_next, int blocks) {
     if (family == kBatchFamilyLattice)
-        k_batch_lattice<kBatchFamilyLattice><<<blocks, kLatThreads, kLatDynSmem, ctx->stream>>>(
+        k_batch_lattice<kBatchFamilyLattice, MIXED><<<blocks, kLatThreads, kLatDynSmem, ctx->stream>>>(
             d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
     else if (family == kBatchFamilyLatticeMerged)
-        k_batch_lattice<kBatchFamilyLatticeMerged><<<blocks, kLatThreads, kLatMergedDynSmem, ctx->stream>>>(
+        k_batch_lattice<kBatchFamilyLatticeMerged, MIXED><<<blocks, kLatThreads, kLatMergedDynSmem, ctx->stream>>>(
             d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
     else
-        k_batch_lattice<kBatchFamilyLatticeGeneric><<<blocks, kLatThreads, kLatGenDynSmem, ctx->stream>>>(
+        k_batch_lattice<kBatchFamilyLatticeGeneric, MIXED><<<blocks, kLatThreads, kLatGenDynSmem, ctx->stream>>>(
             d_items, d_item_of_tile, d_order, ntiles, list, range, d_next);
+}
+
+int lattice_batch_gather(KiwiCtx* ctx, int family, const BatchItemDev* d_items, const int32_t* d_item_of_tile,
+                         const int32_t* d_order, int64_t ntiles, const uint32_t* list, const int64_t* range,
+                         unsigned long long* d_next, int blocks, bool mixed) {
+    if (mixed)
+        batch_launch_t<true>(ctx, family, d_items, d_item_of_tile, d_order, ntiles, list, range, d_next, blocks);
+    else
+        batch_launch_t<false>(ctx, family, d_items, d_item_of_tile, d_order, ntiles, list, range, d_next, blocks);
     KIWI_LAUNCHED(ctx);
     return KIWI_OK;
 }

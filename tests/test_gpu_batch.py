@@ -3,8 +3,9 @@ one persistent, graph-recorded launch.  The batch runs the same tile bodies with
 order as a single-grid call: in the reference-order form (compiled without FMA contraction) each item's
 output equals the single call's bit for bit; the lattice form is compiled with FMA contraction, which the
 compiler forms per kernel, so the batch kernel's results agree with the single-grid kernel's to rounding
-(within 1e-12 of the item's largest value), every count is equal, and the clamped-cell count (cells whose
-sum rounds below zero) agrees to within the cells whose sum is within rounding of zero."""
+(within 1e-12 of the item's largest value; the FP32-mixed form within its own error level), every count is
+equal, and the clamped-cell count (cells whose sum rounds below zero) agrees to within the cells whose sum
+is within rounding of zero."""
 import numpy as np
 import pytest
 
@@ -42,19 +43,26 @@ def _items(kiwi):
     return items
 
 
+# agreement of a batch item with the single-grid call, relative to the item's largest value: the FP64
+# lattice form to rounding; the FP32-mixed form within its own error level (the densest cells are within
+# 1e-3 of the exact integral in either kernel)
+TOL = {"fp64": 1e-12, "fp32_mixed": 2e-3}
+VTOL = {"fp64": 1e-9, "fp32_mixed": 2e-2}
+
+
 def _same(a, b, precision):
-    """Bitwise equal in the reference-order form; within 1e-12 of the largest value in the lattice form."""
+    """Bitwise equal in the reference-order form; within TOL of the largest value in the lattice forms."""
     if precision == "fp64_reference_order":
         return torch.equal(a, b)
     scale = float(b.abs().max()) if b.numel() else 0.0
     d = float((a - b).abs().max()) if b.numel() else 0.0
-    return d <= 1e-12 * scale
+    return d <= TOL[precision] * scale
 
 
 def _same_outputs(out, ref, precision):
     """Every output of an item against the single-grid call's: the raw sums and densities as _same; the
     finalised velocities (ratios of two sums, as sensitive as the cell's mass is small) bitwise in the
-    reference-order form, and in the lattice form within 1e-9 of the largest velocity where the density is
+    reference-order form, and in the lattice forms within VTOL of the largest velocity where the density is
     above 1e-3 of its peak."""
     bad = [k for k in ("density", "raw4") if not _same(out[k], ref[k], precision)]
     if precision == "fp64_reference_order":
@@ -63,7 +71,7 @@ def _same_outputs(out, ref, precision):
         m = ref["density"] >= 1e-3 * ref["density"].max()
         for k in ("vx", "vy", "vz"):
             scale = float(ref[k].abs().max())
-            if m.any() and float((out[k][m] - ref[k][m]).abs().max()) > 1e-9 * scale:
+            if m.any() and float((out[k][m] - ref[k][m]).abs().max()) > VTOL[precision] * scale:
                 bad.append(k)
     return bad
 
@@ -77,7 +85,7 @@ def _single(kiwi, ctx, it, precision):
     return out, st
 
 
-@pytest.mark.parametrize("precision", ["fp64", "fp64_reference_order"])
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reference_order", "fp32_mixed"])
 def test_batch_equals_single_calls(kiwi, ctx, precision):
     items = _items(kiwi)
     batch = kiwi.Batch(items, precision=precision, ctx=ctx)
@@ -93,7 +101,8 @@ def test_batch_equals_single_calls(kiwi, ctx, precision):
                     assert per[i][k] == st[k], (rep, i, k, per[i][k], st[k])
                 # a clamped cell is one whose alternating sum rounds below zero: in the lattice form, cells
                 # at the support's edge whose sum is within rounding of zero may round to either side
-                tol = 0 if precision == "fp64_reference_order" else max(8, st["neg_clamped"] // 50)
+                tol = {"fp64_reference_order": 0, "fp64": max(8, st["neg_clamped"] // 50),
+                       "fp32_mixed": max(64, st["neg_clamped"] // 5)}[precision]
                 assert abs(per[i]["neg_clamped"] - st["neg_clamped"]) <= tol, (rep, i, per[i]["neg_clamped"],
                                                                             st["neg_clamped"])
             assert tot["sphere_pairs"] == sum(p["sphere_pairs"] for p in per)
@@ -130,7 +139,7 @@ def test_batch_masses_may_change_between_runs(kiwi, ctx):
 def test_batch_rejects_bad_arguments(kiwi, ctx):
     items = _items(kiwi)[:1]
     with pytest.raises(kiwi.KiwiError):
-        kiwi.Batch(items, precision="fp32_mixed", ctx=ctx)
+        kiwi.Batch(items, precision="fp32_mixed_guaranteed", ctx=ctx)
     bad = dict(items[0])
     bad["bounds"] = (1.0, 0.0, 0.0, 1.0, 0.0, 1.0)
     with pytest.raises(kiwi.KiwiError):
