@@ -503,6 +503,10 @@ KIWI_HD bool face_reachable(double x0, double y0, double z0, double support_radi
     const double norm = sqrt(A * A + B * B + C * C);
     const double r0 = (A * x0 + B * y0 + C * z0 + D) / norm;
     const double ar0 = fabs(r0);
+    // The face is no closer than its plane: face_dist below is ar0 or sqrt(r0^2 + d^2), and a correctly
+    // rounded sqrt(r0 * r0) is |r0| in binary floating point, so sqrt(r0^2 + d^2) >= ar0 as rounded too.
+    // (A NaN ar0 goes on to the walk, as in the reference.)
+    if (ar0 >= support_radius) return false;
     const double xp = x0 - r0 * A / norm;
     const double yp = y0 - r0 * B / norm;
     const double zp = z0 - r0 * C / norm;

@@ -145,6 +145,7 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                                                                     int64_t* __restrict__ pair_foff,
                                                                     int32_t* __restrict__ fsrc, VorStage stg) {
     __shared__ int32_t s_cand[kBfsWarpsPerBlock][kBfsCandCap];
+    __shared__ unsigned long long s_reach[kBfsWarpsPerBlock][32][2];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t slot = (int64_t)blockIdx.x * kBfsWarpsPerBlock + warp;
     long long* mark = mark_base + slot * C.n_cells;
@@ -182,14 +183,15 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                 n_limit += (lane == 0);
                 break;
             }
-            // The lanes take the next (up to) 32 queued cells, one each, and mark their discovery
-            // candidates: faces towards a neighbour not yet in the queue that the kernel reaches, skipping
-            // a face whose neighbour an earlier face of the same cell already named (a face-cache hit in the
-            // reference, which discovers nothing).  Lane 0 then appends the candidates in (cell, face)
-            // order, skipping neighbours queued meanwhile: the reference's sequential queue.
+            // The lanes take the next (up to) 32 queued cells, one each, and mark the faces to test: faces
+            // towards a neighbour not yet in the queue, skipping a face whose neighbour an earlier face of
+            // the same cell already named (a face-cache hit in the reference, which discovers nothing).  The
+            // warp tests them (the kernel reaches the face or not); the reachable ones are the discovery
+            // candidates, appended in (cell, face) order, skipping neighbours queued meanwhile: the
+            // reference's sequential queue.
             const int batch = min(32, tail - head);
             int64_t fa = 0, nf = 0;
-            unsigned long long cand0 = 0, cand1 = 0, earlier = 0;
+            unsigned long long cand0 = 0, cand1 = 0, earlier = 0, test0 = 0, test1 = 0;
             if (lane < batch) {
                 const int rank = head + lane;
                 const int32_t cell = queue[rank];
@@ -208,14 +210,69 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                         continue;
                     }
                     if (C.twin[f] >= 0) continue;  // an earlier face of this cell named nb already
-                    const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
-                    if (!face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]))) continue;
-                    if (f - fa < 64) cand0 |= 1ull << (f - fa);
-                    else cand1 |= 1ull << (f - fa - 64);
+                    if (f - fa < 64) test0 |= 1ull << (f - fa);
+                    else test1 |= 1ull << (f - fa - 64);
                 }
                 if (pass == 1) {
                     pair_cells[o + rank] = cell;
                     pair_mask[o + rank] = earlier;
+                }
+            }
+            {
+                // The faces left to test (neighbour not queued, not a twin) as one list over the warp, in
+                // (cell, face) order, each lane testing every 32nd: a lane's own cell would leave the others
+                // idle through its faces, and the early batches hold one cell or a few.  A batch of more
+                // tests than the list holds is tested lane by lane.
+                const int nt_l = __popcll(test0) + __popcll(test1);
+                int t_incl = nt_l;
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, t_incl, d);
+                    if (lane >= d) t_incl += v;
+                }
+                const int n_test = __shfl_sync(0xffffffffu, t_incl, 31);
+                if (n_test <= kBfsCandCap) {
+                    int32_t* items = s_cand[warp];
+                    int o_t = t_incl - nt_l;
+                    for (int w = 0; w < 2; ++w) {
+                        unsigned long long bits = w == 0 ? test0 : test1;
+                        while (bits) {
+                            const int b = __ffsll((long long)bits) - 1;
+                            bits &= bits - 1;
+                            items[o_t++] = lane << 7 | (64 * w + b);
+                        }
+                    }
+                    s_reach[warp][lane][0] = 0;
+                    s_reach[warp][lane][1] = 0;
+                    __syncwarp();
+                    for (int base = 0; base < n_test; base += 32) {
+                        const int i = base + lane;
+                        const int item = i < n_test ? items[i] : 0;
+                        const int src = item >> 7, fl = item & 127;
+                        const int64_t f = __shfl_sync(0xffffffffu, fa, src) + fl;
+                        if (i < n_test) {
+                            const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
+                            if (face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f])))
+                                atomicOr(&s_reach[warp][src][fl >> 6], 1ull << (fl & 63));
+                        }
+                    }
+                    __syncwarp();
+                    cand0 = s_reach[warp][lane][0];
+                    cand1 = s_reach[warp][lane][1];
+                    __syncwarp();
+                } else {
+                    for (int w = 0; w < 2; ++w) {
+                        unsigned long long bits = w == 0 ? test0 : test1;
+                        while (bits) {
+                            const int b = __ffsll((long long)bits) - 1;
+                            bits &= bits - 1;
+                            const int64_t f = fa + 64 * w + b;
+                            const FlatVerts V{C.vxyz + 3 * C.vert_off[f]};
+                            if (face_reachable(x0, y0, z0, radius, V, (int)(C.vert_off[f + 1] - C.vert_off[f]))) {
+                                if (w == 0) cand0 |= 1ull << b;
+                                else cand1 |= 1ull << b;
+                            }
+                        }
+                    }
                 }
             }
             if (pass == 1 && fsrc) {
