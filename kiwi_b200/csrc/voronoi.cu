@@ -91,6 +91,11 @@ constexpr int kGatherVertCap = 1536;  // vertices staged in shared memory per ce
 // k_vor_faces: a face item packs (pair slot << 7 | face), for cells of at most 128 faces
 constexpr int kFaceItemMaxFaces = 128;
 constexpr int kFaceItemCap = 2048;  // 4 KB of items beside the 36 KB of staged vertices
+// k_vor_faces: CTAs per SM the register allocation leaves room for (4: 128 registers a thread, a few
+// spilled; 8 % faster than 3 CTAs at 166 registers)
+#ifndef KIWI_VOR_FACES_MIN_BLOCKS
+#define KIWI_VOR_FACES_MIN_BLOCKS 4
+#endif
 
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -641,14 +646,11 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_gather(VorCells C, DevPa
 // cell's pairs are added in particle order: the same operations on the same values as k_vor_gather, with
 // every face value evaluated once per particle instead of once per side.
 template <int MODE>
-__global__ void __launch_bounds__(kGatherThreads) k_vor_faces(VorCells C, DevParticles P, int kernel,
-                                                               double support_in_h, const TabDev tab,
-                                                               const uint32_t* __restrict__ plist,
-                                                               const int64_t* __restrict__ range,
-                                                               const int64_t* __restrict__ pair_foff,
-                                                               const int32_t* __restrict__ fsrc,
-                                                               const int64_t* __restrict__ offs,
-                                                               double* __restrict__ fval, DevStats* __restrict__ st) {
+__global__ void __launch_bounds__(kGatherThreads, KIWI_VOR_FACES_MIN_BLOCKS)
+    k_vor_faces(VorCells C, DevParticles P, int kernel, double support_in_h, const TabDev tab,
+                const uint32_t* __restrict__ plist, const int64_t* __restrict__ range,
+                const int64_t* __restrict__ pair_foff, const int32_t* __restrict__ fsrc,
+                const int64_t* __restrict__ offs, double* __restrict__ fval, DevStats* __restrict__ st) {
     __shared__ double s_v[3 * kGatherVertCap];
     const int64_t cell = blockIdx.x;
     const int64_t f0 = C.face_off[cell], f1 = C.face_off[cell + 1];
@@ -676,47 +678,71 @@ __global__ void __launch_bounds__(kGatherThreads) k_vor_faces(VorCells C, DevPar
             }
         }
     } else {
-        // The cell's pairs in groups: each thread takes one pair and lists the faces it evaluates itself
-        // (its walk did not borrow them); the group's list is then evaluated by all threads at once, so
-        // that no lane idles through a face another pair evaluates.
+        // The cell's pairs in groups: each thread takes one pair and marks the faces it evaluates itself
+        // (its walk did not borrow them); the group's (pair, face) items are listed face by face (a
+        // counting sort by face) and evaluated by all threads at once, so that no lane idles through a
+        // face another pair evaluates and a warp's lanes walk the same face (same vertex count, same
+        // staged vertices) for different particles.  Each value goes to its own place in the tables, so
+        // the order within a face's bucket does not matter.
         __shared__ double s_px[kGatherThreads], s_py[kGatherThreads], s_pz[kGatherThreads], s_ph[kGatherThreads];
         __shared__ int64_t s_pf[kGatherThreads];
         __shared__ uint16_t s_items[kFaceItemCap];
-        __shared__ int s_wsum[kGatherThreads / 32];
+        __shared__ int s_fpos[kFaceItemMaxFaces];
+        __shared__ int s_total;
         const int group = min(kGatherThreads, kFaceItemCap / max(nf, 1));
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         for (int64_t base = beg; base < end; base += group) {
+            for (int f = threadIdx.x; f < nf; f += kGatherThreads) s_fpos[f] = 0;
+            __syncthreads();
             const int64_t k = base + threadIdx.x;
-            int own = 0;
-            int64_t pf = 0;
+            unsigned long long own0 = 0, own1 = 0;  // faces 0..63 and 64..127 this pair evaluates
             if (threadIdx.x < group && k < end) {
                 const int64_t pk = plist[k];
                 const int64_t p = pair_particle(offs, P.n, pk);
-                pf = pair_foff[pk];
+                const int64_t pf = pair_foff[pk];
                 s_px[threadIdx.x] = P.x[p];
                 s_py[threadIdx.x] = P.y[p];
                 s_pz[threadIdx.x] = P.z[p];
                 s_ph[threadIdx.x] = P.h[p];
                 s_pf[threadIdx.x] = pf;
-                for (int f = 0; f < nf; ++f) own += fsrc[pf + f] == -1;
-            }
-            // block exclusive scan of the own-face counts
-            int incl = own;
-            for (int d = 1; d < 32; d <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, d);
-                if (lane >= d) incl += v;
-            }
-            if (lane == 31) s_wsum[warp] = incl;
-            __syncthreads();
-            int wbase = 0, total = 0;
-            for (int w = 0; w < kGatherThreads / 32; ++w) {
-                if (w < warp) wbase += s_wsum[w];
-                total += s_wsum[w];
-            }
-            if (own > 0) {
-                int o = wbase + incl - own;
                 for (int f = 0; f < nf; ++f)
-                    if (fsrc[pf + f] == -1) s_items[o++] = (uint16_t)(threadIdx.x << 7 | f);
+                    if (fsrc[pf + f] == -1) {
+                        if (f < 64) own0 |= 1ull << f;
+                        else own1 |= 1ull << (f - 64);
+                        atomicAdd(&s_fpos[f], 1);
+                    }
+            }
+            __syncthreads();
+            if (warp == 0) {
+                // exclusive scan of the per-face counts (nf <= 128: four faces per lane)
+                int c[4], sum = 0;
+                for (int q = 0; q < 4; ++q) {
+                    const int f = 4 * lane + q;
+                    c[q] = f < nf ? s_fpos[f] : 0;
+                    sum += c[q];
+                }
+                int incl = sum;
+                for (int d = 1; d < 32; d <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, d);
+                    if (lane >= d) incl += v;
+                }
+                int run = incl - sum;
+                for (int q = 0; q < 4; ++q) {
+                    const int f = 4 * lane + q;
+                    if (f < nf) s_fpos[f] = run;
+                    run += c[q];
+                }
+                if (lane == 31) s_total = incl;
+            }
+            __syncthreads();
+            const int total = s_total;
+            for (int w = 0; w < 2; ++w) {
+                unsigned long long bits = w == 0 ? own0 : own1;
+                while (bits) {
+                    const int f = 64 * w + __ffsll((long long)bits) - 1;
+                    bits &= bits - 1;
+                    s_items[atomicAdd(&s_fpos[f], 1)] = (uint16_t)(threadIdx.x << 7 | f);
+                }
             }
             __syncthreads();
             for (int it = threadIdx.x; it < total; it += kGatherThreads) {
