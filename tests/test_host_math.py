@@ -240,3 +240,43 @@ def test_lattice_generic_point_derivatives(hm):
     print(f"dual vs double value {worst_v:.2e}; derivative vs central differences (x H) {worst_d:.2e}")
     assert worst_v < 1e-13
     assert worst_d < 1e-8
+
+
+def _plane_distance(p, v):
+    """|r0| of the face walk (src/kernel_integral.cpp:481-495) in the same IEEE operations, in numpy."""
+    (x1, y1, z1), (x2, y2, z2), (x3, y3, z3) = (tuple(float(c) for c in v[i]) for i in range(3))
+    A = (y2 - y1) * (z3 - z1) - (y3 - y1) * (z2 - z1)
+    B = (z2 - z1) * (x3 - x1) - (z3 - z1) * (x2 - x1)
+    Cc = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1)
+    D = -A * x1 - B * y1 - Cc * z1
+    norm = np.sqrt(A * A + B * B + Cc * Cc)
+    return abs((A * p[0] + B * p[1] + Cc * p[2] + D) / norm)
+
+
+def test_reachability_at_the_plane_distance(hm, oracle):
+    """face_reachable rejects a face whose plane lies at or beyond the support before its vertex loop.  On
+    convex polygons of 3 to 9 vertices in random orientations, with the support equal to the plane
+    distance, one ulp either side of it and 1e-12 .. 1e-3 relative either side, and with the foot of the
+    perpendicular inside and outside the polygon, its decision is the reference's (out_vert != n) every time."""
+    rng = np.random.default_rng(13)
+    dp = C.POINTER(C.c_double)
+    checked = 0
+    for _ in range(400):
+        n = int(rng.integers(3, 10))
+        ang = np.sort(rng.random(n)) * 2 * np.pi
+        rad = 0.2 + rng.random()
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        off = rng.normal(size=3)
+        verts = np.ascontiguousarray(np.stack([rad * np.cos(ang), rad * np.sin(ang), np.zeros(n)], axis=1) @ q.T
+                                     + off)
+        local = np.array([rng.normal() * rad, rng.normal() * rad, (0.05 + rng.random()) * rng.choice([-1, 1])])
+        p = q @ local + off
+        d = _plane_distance(p, verts)
+        sups = [d, np.nextafter(d, 0), np.nextafter(d, np.inf)]
+        sups += [d * (1 + s * e) for e in (1e-12, 1e-9, 1e-6, 1e-3) for s in (-1, 1)]
+        for sup in sups:
+            r = hm.hm_face_reachable(*p, sup, verts.ctypes.data_as(dp), n)
+            _, ov = oracle.face_integral(*p, verts, kernel=0, h=sup / 2, support=sup)
+            assert r == (ov != n), (n, sup / d - 1)
+            checked += 1
+    assert checked == 400 * 11
