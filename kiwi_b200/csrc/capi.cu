@@ -245,7 +245,7 @@ int sph_to_grid_dev(KiwiCtx* ctx, const DevParticles& P, const CartGeom& g, cons
             KIWI_TRY(fp64_cart_gather(ctx, g, P, kc, tl2, out, d_st2, false, false));
         }
     } else {
-        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "precision %d is not available in this build", precision);
+        return set_err(ctx, KIWI_ERR_UNSUPPORTED, "precision %d is not available in this library", precision);
     }
     KIWI_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
 
