@@ -21,11 +21,10 @@ def tile_grid(shape):
     return (nx + TILE - 1) // TILE, (ny + TILE - 1) // TILE, (nz + TILE - 1) // TILE
 
 
-def tile_entry_counts(particles: dict, bounds, shape, support_in_h: float) -> np.ndarray:
-    """(tile, particle) entries per tile, in tile order: the number of particles whose clamped support
-    box (src/cartesian_grid.cpp:211-237) touches the tile."""
+def _support_tiles(particles: dict, bounds, shape, support_in_h: float):
+    """Per particle: whether its clamped support box (src/cartesian_grid.cpp:211-237) holds a cell, and
+    the tile range [t0, t1) of that box on each axis."""
     nx, ny, nz = (int(s) for s in shape)
-    ntx, nty, ntz = tile_grid(shape)
     x, y, z, h = (np.asarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "h"))
     b = [float(v) for v in bounds]
     d = [(b[1] - b[0]) / nx, (b[3] - b[2]) / ny, (b[5] - b[4]) / nz]
@@ -41,9 +40,31 @@ def tile_entry_counts(particles: dict, bounds, shape, support_in_h: float) -> np
         ok &= a0 <= a1
         lo.append(a0)
         hi.append(a1)
+    t0 = [np.where(ok, lo[i], 0).astype(np.int64) // TILE for i in range(3)]
+    t1 = [np.where(ok, hi[i], 0).astype(np.int64) // TILE + 1 for i in range(3)]
+    return ok, t0, t1
+
+
+def _box_sums(table: np.ndarray, t0, t1) -> np.ndarray:
+    """Sum of table[t0x:t1x, t0y:t1y, t0z:t1z] per box, from the 3-D prefix sums (inclusion-exclusion)."""
+    S = np.zeros(tuple(n + 1 for n in table.shape), dtype=np.int64)
+    S[1:, 1:, 1:] = table.astype(np.int64).cumsum(0).cumsum(1).cumsum(2)
+    out = np.zeros(len(t0[0]), dtype=np.int64)
+    for sx, ix in ((1, t1[0]), (-1, t0[0])):
+        for sy, iy in ((1, t1[1]), (-1, t0[1])):
+            for sz, iz in ((1, t1[2]), (-1, t0[2])):
+                out += sx * sy * sz * S[ix, iy, iz]
+    return out
+
+
+def tile_entry_counts(particles: dict, bounds, shape, support_in_h: float) -> np.ndarray:
+    """(tile, particle) entries per tile, in tile order: the number of particles whose clamped support
+    box (src/cartesian_grid.cpp:211-237) touches the tile."""
+    ntx, nty, ntz = tile_grid(shape)
+    ok, t0, t1 = _support_tiles(particles, bounds, shape, support_in_h)
+    t0 = [t[ok] for t in t0]
+    t1 = [t[ok] for t in t1]
     cnt = np.zeros((ntx + 1, nty + 1, ntz + 1), dtype=np.int64)
-    t0 = [(lo[i][ok] // TILE).astype(np.int64) for i in range(3)]
-    t1 = [(hi[i][ok] // TILE).astype(np.int64) + 1 for i in range(3)]
     # 3-D difference array: +1 on the box's corners with inclusion-exclusion signs
     for sx, ix in ((1, t0[0]), (-1, t1[0])):
         for sy, iy in ((1, t0[1]), (-1, t1[1])):
@@ -51,6 +72,21 @@ def tile_entry_counts(particles: dict, bounds, shape, support_in_h: float) -> np
                 np.add.at(cnt, (ix, iy, iz), sx * sy * sz)
     cnt = cnt.cumsum(0).cumsum(1).cumsum(2)[:ntx, :nty, :ntz]
     return cnt.reshape(-1)
+
+
+def part_particles(particles: dict, bounds, shape, support_in_h: float, owner: np.ndarray,
+                   part: int) -> np.ndarray:
+    """Indices (ascending) of the particles whose clamped support box touches a tile of `part`: every
+    particle that contributes to a cell of the part.  A rank that maps only these particles (in this
+    order) gets its own cells' sums exactly as the whole snapshot gives them -- each cell adds its
+    particles in ascending order and the others add nothing -- and keeps `cells_of_part` of the result.
+    A cell no particle reaches takes the snapshot's mean velocity (src/cartesian_grid.cpp:302-315), which
+    needs the whole snapshot."""
+    ntx, nty, ntz = tile_grid(shape)
+    ok, t0, t1 = _support_tiles(particles, bounds, shape, support_in_h)
+    mine = (np.asarray(owner) == part).reshape(ntx, nty, ntz)
+    hit = _box_sums(mine, t0, t1) > 0
+    return np.nonzero(ok & hit)[0]
 
 
 def tile_owners(weights: np.ndarray, n_parts: int) -> np.ndarray:

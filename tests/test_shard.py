@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import random_particles
+from kiwi_b200 import shard
 
 
 def _brute_counts(P, bounds, shape, sup):
@@ -123,3 +124,83 @@ def test_two_ranks_agree_on_the_split_gloo():
         cover = masks[0] + masks[1]
         assert np.all(cover == 1)  # disjoint and complete
         assert ms == 11.0 and pairs == 300.0  # max of the times, sum of the pairs
+
+
+def test_part_particles_cover_the_part():
+    """part_particles holds every particle whose support box reaches a cell of the part (brute force over
+    the cells), in ascending order, and no particle that reaches none of its tiles."""
+    P = random_particles(300, 21, hmin=0.02, hmax=0.25)
+    bounds, shape, sup = (0, 2, 0, 2, 0, 2), (40, 24, 20), 2.0
+    own = shard.tile_owners(shard.tile_entry_counts(P, bounds, shape, sup), 3)
+    ntx, nty, ntz = shard.tile_grid(shape)
+    d = [2.0 / s for s in shape]
+    for part in range(3):
+        idx = shard.part_particles(P, bounds, shape, sup, own, part)
+        assert np.all(np.diff(idx) > 0)
+        mine = (own == part).reshape(ntx, nty, ntz)
+        want = []
+        for i in range(len(P["x"])):
+            r = sup * P["h"][i]
+            lo = [max(int(np.floor((P[k][i] - r) / d[a])), 0) for a, k in enumerate("xyz")]
+            hi = [min(int(np.floor((P[k][i] + r) / d[a])), shape[a] - 1) for a, k in enumerate("xyz")]
+            if any(lo[a] > hi[a] for a in range(3)):
+                continue
+            if mine[lo[0] // 8:hi[0] // 8 + 1, lo[1] // 8:hi[1] // 8 + 1, lo[2] // 8:hi[2] // 8 + 1].any():
+                want.append(i)
+        assert np.array_equal(idx, np.array(want, dtype=idx.dtype))
+
+
+def _rank_compute(rank, world, port, q):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import torch
+
+        from kiwi_b200 import shard
+        from oracle.oracle import Oracle
+
+        # every rank builds the snapshot, derives the split, and maps only the particles that reach its
+        # tiles (the oracle stands in for the per-part device call), then the cells are gathered on rank 0
+        P = random_particles(500, 17, hmin=0.02, hmax=0.15)
+        bounds, shape, sup = (0, 2, 0, 2, 0, 2), (40, 24, 16), 2.0
+        own = shard.tile_owners(shard.tile_entry_counts(P, bounds, shape, sup), world)
+        idx = shard.part_particles(P, bounds, shape, sup, own, rank)
+        sub = {k: np.ascontiguousarray(v[idx]) for k, v in P.items()}
+        dens, vx, vy, vz, raw, _ = Oracle().sph_to_grid(sub, bounds, shape)
+        cells = shard.cells_of_part(own, rank, shape)
+        mine = torch.tensor(np.stack([np.where(cells, a, 0.0) for a in (dens, vx, vy, vz, *raw.reshape(4, -1))]))
+        parts = [torch.zeros_like(mine) for _ in range(world)]
+        dist.all_gather(parts, mine)
+        q.put((rank, len(idx), [t.numpy() for t in parts] if rank == 0 else None))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_map_their_parts_gloo(oracle):
+    """Two gloo ranks each map the particles of their own part and keep their own cells; the assembled
+    grid equals the whole snapshot's map bit for bit (densities and raw sums everywhere, velocities in
+    every cell a particle reaches)."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_compute, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in procs], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    P = random_particles(500, 17, hmin=0.02, hmax=0.15)
+    dens, vx, vy, vz, raw, _ = oracle.sph_to_grid(P, (0, 2, 0, 2, 0, 2), (40, 24, 16))
+    assert out[0][1] < 500 and out[1][1] < 500  # each rank maps a proper subset
+    assembled = out[0][2][0] + out[0][2][1]  # the parts' cells are disjoint, zero elsewhere
+    whole = np.stack([dens, vx, vy, vz, *raw.reshape(4, -1)])
+    reached = raw.reshape(4, -1)[0] > 0
+    for f in (0, 4, 5, 6, 7):
+        assert np.array_equal(assembled[f], whole[f])
+    for f in (1, 2, 3):
+        assert np.array_equal(assembled[f][reached], whole[f][reached])
