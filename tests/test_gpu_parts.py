@@ -58,3 +58,36 @@ def test_part_arguments_are_checked(kiwi, ctx):
     with pytest.raises(kiwi.KiwiError):
         kiwi.sph_to_grid_device(dP, (0, 2, 0, 2, 0, 2), (8, 8, 8), out, ctx=ctx, precision="fp32_mixed_guaranteed",
                                 part=0, n_parts=2)
+
+
+@pytest.mark.parametrize("precision,kname", [("fp64", "cubic_spline"), ("fp64", "wendland_c4"),
+                                             ("fp64_reference_order", "cubic_spline"), ("fp32_mixed", "cubic_spline")])
+def test_part_particles_reproduce_their_cells(kiwi, ctx, precision, kname):
+    """A rank that holds only the particles reaching its tiles (shard.part_particles) and maps them with the
+    whole-grid call gets its own cells bit for bit as the whole snapshot gives them (densities everywhere,
+    velocities wherever a particle reaches the cell)."""
+    from kiwi_b200 import shard
+
+    P = random_particles(500, 32, hmin=0.02, hmax=0.35)
+    b, shape, n_parts = (0.0, 2.0, 0.0, 2.0, 0.0, 2.0), (40, 24, 33), 3
+    ki = kiwi.make_kernel_integrator(kname)
+    sup = ki.support_in_h or kiwi.get_kernel(kname).radkern
+    nc = int(np.prod(shape))
+
+    def run(Q):
+        dQ = {k: torch.tensor(np.ascontiguousarray(Q[k]), device="cuda") for k in KEYS}
+        out = {k: torch.zeros(nc, dtype=torch.float64, device="cuda") for k in ("density", "vx", "vy", "vz")}
+        kiwi.sph_to_grid_device(dQ, b, shape, out, kernel=ki, precision=precision, ctx=ctx)
+        return {k: v.cpu().numpy() for k, v in out.items()}
+
+    whole = run(P)
+    own = shard.tile_owners(shard.tile_entry_counts(P, b, shape, sup), n_parts)
+    for p in range(n_parts):
+        idx = shard.part_particles(P, b, shape, sup, own, p)
+        assert 0 < len(idx) < len(P["x"])
+        part = run({k: v[idx] for k, v in P.items()})
+        cells = shard.cells_of_part(own, p, shape)
+        assert np.array_equal(part["density"][cells], whole["density"][cells]), p
+        reached = cells & (whole["density"] > 0)
+        for k in ("vx", "vy", "vz"):
+            assert np.array_equal(part[k][reached], whole[k][reached]), (p, k)
