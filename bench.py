@@ -83,7 +83,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true",
-                    help="skip parity_c1: config 1 on the GPU and through the reference's stage (~3 min of host CPU)")
+                    help="skip parity_c1: the 7,300-particle column on the GPU and through the reference's stage "
+                         "(~3 min of host CPU)")
     ap.add_argument("--no-fp32-compare", action="store_true",
                     help="with --precision fp64: skip timing the FP32-mixed form beside it")
     ap.add_argument("--multi", default="tiles", choices=["tiles", "replicas"],
@@ -262,10 +263,10 @@ def cpu_baseline(P, bounds, shape, kernel_name):
 
 
 def cpu_baseline_c1(kiwi_b200, ctx):
-    """Config 1 (the 7,300-particle column on its 100 x 100 x 410 grid of 0.02 pc cells, the CPU-runnable
-    configuration) mapped twice: on the GPU through the public host API (host arrays in and out), and by the
+    """The 7,300-particle column on its 100 x 100 x 410 grid of 0.02 pc cells (the workload small enough for
+    the reference's own stage) mapped twice: on the GPU through the public host API (host arrays in and out), and by the
     reference's own run_sph_to_grid_stage (oracle/_ref) on all host cores -- its stage wall time is the CPU
-    baseline of this configuration, and its grid is the checker of the GPU's, cell by cell per density band
+    baseline of this workload, and its grid is compared with the GPU's, cell by cell per density band
     (parity_c1)."""
     from oracle.compare import band_stats, exact_check
     from oracle.oracle import load_ref, load_truth
@@ -1041,7 +1042,9 @@ def main():
         line = {
             "metric": "particle-cell integrals/s (support pairs), sph-to-grid", "value": value,
             "unit": "pair-integrals/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": job_ms / args.steps, "higher_is_better": True, "scaling": "strong" if split else "weak",
+            "ms_per_step": job_ms / args.steps, "higher_is_better": True,
+            # --multi tiles: the same grid at every N (total work fixed); replicas: one grid per rank
+            "scaling": "strong" if args.multi == "tiles" else "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": workload_config(args, nc, ws, split),

@@ -1,1 +1,1 @@
-"""CPU checkers of the kernel-integral path -- test infrastructure only (see oracle/oracle.py)."""
+"""CPU oracles of the kernel-integral path -- test infrastructure only (see oracle/oracle.py)."""

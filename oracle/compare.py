@@ -1,5 +1,5 @@
 """Cell-by-cell comparison of two density grids, per density band -- TEST INFRASTRUCTURE ONLY (used by the
-GPU parity tests and by bench.py's CPU-baseline leg, which runs the reference as the checker).
+GPU parity tests and by bench.py's CPU-baseline leg, which compares the GPU with the reference).
 
 Bands are fractions of the reference grid's peak density: > 1e-2, 1e-4..1e-2, 1e-6..1e-4, and the cells at
 or below 1e-6 of the peak, whose differences are taken relative to the peak."""

@@ -1,4 +1,4 @@
-"""ctypes bindings of the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+"""ctypes bindings of the CPU oracles -- TEST INFRASTRUCTURE ONLY.
 
 ``Oracle`` wraps oracle/liboracle.so (the C restatement of the reference's algorithm) and ``RefLib``
 wraps oracle/_ref/libkiwi_ref.so (the reference KIWI library built from its own sources by

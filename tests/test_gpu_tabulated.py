@@ -34,7 +34,7 @@ def _tab(kiwi):
 
 def _expected_clamps(h, phi, r0, R0, s):
     """How many of the three lookup indices of each item fall outside the table (numpy restatement of the
-    index arithmetic, the checker for the GPU's count)."""
+    index arithmetic, the expected value of the GPU's count)."""
     n = 0
     for hh, p, a, b in zip(h, phi, r0, R0):
         if a == 0.0 or b == 0.0 or p == 0.0:
@@ -53,7 +53,7 @@ def _expected_clamps(h, phi, r0, R0, s):
 
 def _entry_args(flat):
     """(phi, r0, R_0) of canonical-table entries by flat index (the grid of generate_density_table,
-    src/kernel_integral.cpp:84-112, restated as the checker)."""
+    src/kernel_integral.cpp:84-112, restated in numpy)."""
     i, rem = np.divmod(flat, 301 * 301)
     j, k = np.divmod(rem, 301)
     n, rl, mul, cphil = 150, 0.1, 0.98, 0.98
