@@ -1,4 +1,5 @@
-"""Splitting one grid over several GPUs: the host side of kiwi_sph_to_grid_device_part.
+"""Splitting work over several GPUs: the host side of kiwi_sph_to_grid_device_part, the Voronoi map's
+spatial slabs, and snapshots dealt to GPUs.
 
 The library splits a grid's 8x8x8-cell tiles into n parts, each a contiguous run of the tile order
 (tile (tx, ty, tz) at index (tx * nty + ty) * ntz + tz) with a near-equal number of (tile, particle)
@@ -6,8 +7,10 @@ entries: tile t belongs to part floor(prefix(t) * n / W) (capped at n - 1), pref
 the tiles before t and W their total; with W = 0 the tiles split evenly by number.  This module restates
 that rule on the host -- the entry counts from the particles' clamped support boxes, exactly as the
 binning computes them -- so that a rank knows which x rows of the grid it owns (to copy back only those)
-before the GPU has run, and every rank agrees on the split without talking to the others.  It also
-holds the max-over-ranks reduction of a step's timing.
+before the GPU has run, and every rank agrees on the split without talking to the others.  A Voronoi
+map splits by spatial slabs of cells (each rank maps the particles that can reach its slab and keeps its
+cells), and a batch of snapshots by whole snapshots, longest first.  It also holds the max-over-ranks
+reduction of a step's timing.
 """
 from __future__ import annotations
 
@@ -121,6 +124,94 @@ def cells_of_part(owner: np.ndarray, part: int, shape) -> np.ndarray:
     t = (owner == part).reshape(ntx, nty, ntz)
     m = np.repeat(np.repeat(np.repeat(t, TILE, 0), TILE, 1), TILE, 2)[:nx, :ny, :nz]
     return m.reshape(-1)
+
+
+def _cell_vertex_rows(cells: dict):
+    """Per cell, its vertex rows [start, end) in vxyz (a cell's faces, and their vertices, are contiguous)."""
+    fo = np.asarray(cells["face_off"], dtype=np.int64)
+    vo = np.asarray(cells["vert_off"], dtype=np.int64)
+    return vo[fo[:-1]], vo[fo[1:]]
+
+
+def voronoi_cell_owners(cells: dict, n_parts: int, axis: int = 0) -> np.ndarray:
+    """Voronoi cells split into n_parts spatial slabs along `axis`: the cells ordered by the mean of their
+    vertices' coordinate (ties by cell index), cut into runs of near-equal cell counts (cell of rank k goes
+    to part floor(k n / n_cells))."""
+    start, end = _cell_vertex_rows(cells)
+    nc = len(start)
+    if nc == 0:
+        return np.zeros(0, dtype=np.int64)
+    coord = np.asarray(cells["vxyz"], dtype=np.float64).reshape(-1, 3)[:, axis]
+    cs = np.concatenate([[0.0], np.cumsum(coord)])
+    cnt = end - start
+    centre = np.where(cnt > 0, (cs[end] - cs[start]) / np.maximum(cnt, 1), 0.0)
+    order = np.argsort(centre, kind="stable")
+    owner = np.empty(nc, dtype=np.int64)
+    owner[order] = (np.arange(nc, dtype=np.int64) * n_parts) // nc
+    return owner
+
+
+def voronoi_part_particles(particles: dict, home_cell, cells: dict, owner: np.ndarray, part: int,
+                           support_in_h: float) -> np.ndarray:
+    """Indices (ascending) of the particles whose cell walk can reach a cell of `part`: those whose home
+    cell is the part's, and those whose support sphere comes within 1.001 radii of the box around the
+    part's cell vertices.  A walk visits the home cell and otherwise only cells behind a face within the
+    support radius (src/mapping.cpp:187-193), so every (cell, particle) pair of the part's cells comes from
+    these particles; a walk depends on its particle alone and a cell adds its pairs in particle order, so a
+    rank that maps only these particles (in this order) gets its own cells bit for bit as the whole
+    snapshot gives them.  A cell no particle reaches takes the snapshot's mean velocity
+    (src/mapping.cpp:490-500), which needs the whole snapshot."""
+    start, end = _cell_vertex_rows(cells)
+    owner = np.asarray(owner)
+    v = np.asarray(cells["vxyz"], dtype=np.float64).reshape(-1, 3)
+    rows = np.repeat(owner == part, end - start)
+    home = np.asarray(home_cell, dtype=np.int64)
+    n = len(home)
+    valid = (home >= 0) & (home < len(owner))
+    sel = np.zeros(n, dtype=bool)
+    sel[valid] = owner[home[valid]] == part
+    if rows.any():
+        lo, hi = v[rows].min(axis=0), v[rows].max(axis=0)
+        d2 = np.zeros(n)
+        for a, k in enumerate("xyz"):
+            c = np.asarray(particles[k], dtype=np.float64)
+            d2 += np.maximum(np.maximum(lo[a] - c, c - hi[a]), 0.0) ** 2
+        r = 1.001 * support_in_h * np.asarray(particles["h"], dtype=np.float64)
+        sel |= d2 <= r * r
+    return np.nonzero(sel)[0]
+
+
+def snapshot_work(particles: dict, bounds, shape, support_in_h: float) -> int:
+    """A snapshot's (particle, cell) pairs within the particles' clamped support boxes
+    (src/cartesian_grid.cpp:211-237): the work estimate by which snapshots are dealt to GPUs."""
+    nx, ny, nz = (int(s) for s in shape)
+    x, y, z, h = (np.asarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "h"))
+    b = [float(v) for v in bounds]
+    d = [(b[1] - b[0]) / nx, (b[3] - b[2]) / ny, (b[5] - b[4]) / nz]
+    radius = support_in_h * h
+    ok = h > 0
+    cells = np.ones(len(h), dtype=np.int64)
+    for c, mn, dd, n in ((x, b[0], d[0], nx), (y, b[2], d[1], ny), (z, b[4], d[2], nz)):
+        with np.errstate(invalid="ignore", over="ignore"):
+            a0 = np.maximum(np.clip(np.floor((c - radius - mn) / dd), -2e9, 2e9), 0)
+            a1 = np.minimum(np.clip(np.floor((c + radius - mn) / dd), -2e9, 2e9), n - 1)
+        ok &= a0 <= a1
+        cells *= np.where(ok, a1 - a0 + 1, 0).astype(np.int64)
+    return int(cells[ok].sum())
+
+
+def assign_snapshots_lpt(work, n_parts: int) -> list[np.ndarray]:
+    """Whole snapshots dealt to n_parts GPUs, longest processing time first: by work descending (ties by
+    index), each to the part with the least work so far (ties to the lowest part).  Every rank computes
+    the same assignment from the same work list.  Returns each part's snapshot indices, ascending."""
+    work = np.asarray(work, dtype=np.int64)
+    load = np.zeros(n_parts, dtype=np.int64)
+    parts = [[] for _ in range(n_parts)]
+    for i in np.argsort(-work, kind="stable"):
+        p = int(np.argmin(load))
+        parts[p].append(int(i))
+        load[p] += work[i]
+    return [np.array(sorted(q), dtype=np.int64) for q in parts]
 
 
 def reduce_step(ms: float, pairs: float, device=None):

@@ -146,3 +146,38 @@ def test_batch_rejects_bad_arguments(kiwi, ctx):
         kiwi.Batch([bad], ctx=ctx)
     with pytest.raises(kiwi.KiwiError):
         kiwi.Batch([], ctx=ctx)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp64_reference_order"])
+def test_snapshots_dealt_to_gpus_equal_the_whole_batch(kiwi, ctx, precision):
+    """A batch split over GPUs by whole snapshots, longest first (shard.assign_snapshots_lpt on
+    shard.snapshot_work), run here part after part: each part's batch gives its items' outputs as the
+    whole batch does."""
+    from kiwi_b200 import shard
+
+    items = _items(kiwi)
+    full = kiwi.Batch(items, precision=precision, ctx=ctx)
+    try:
+        full.run()
+        torch.cuda.synchronize()
+        ref = [{k: v.clone() for k, v in it["out"].items()} for it in items]
+    finally:
+        full.close()
+    work = [shard.snapshot_work({k: it["particles"][k].cpu().numpy() for k in ("x", "y", "z", "h")}, it["bounds"],
+                                it["shape"], it["kernel"].support_in_h or 2.0) for it in items]
+    parts = shard.assign_snapshots_lpt(work, 2)
+    assert all(len(q) for q in parts)
+    for q in parts:
+        sub = [items[i] for i in q]
+        for it in sub:
+            for k in it["out"]:
+                it["out"][k].fill_(123.0)
+        b = kiwi.Batch(sub, precision=precision, ctx=ctx)
+        try:
+            b.run()
+            torch.cuda.synchronize()
+        finally:
+            b.close()
+        for i in q:
+            assert not _same_outputs(items[i]["out"], ref[i], precision), (i, _same_outputs(items[i]["out"], ref[i],
+                                                                                            precision))

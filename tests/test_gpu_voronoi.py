@@ -279,3 +279,49 @@ def test_single_walk_equals_two_walks(kiwi):
     i2 = kiwi.inverse_map_voronoi(P, d["home"], geo, ctx=kiwi.Context(0))
     assert np.array_equal(i1.m_recovered, i2.m_recovered)
     assert np.array_equal(i1.coverage, i2.coverage)
+
+
+@pytest.mark.parametrize("fn", GOLDEN, ids=[os.path.basename(f)[4:-4] for f in GOLDEN])
+def test_slab_particles_reproduce_their_cells(kiwi, ctx, fn):
+    """A Voronoi map split over GPUs by spatial slabs of cells (shard.voronoi_cell_owners), each slab
+    mapping only the particles that can reach it (shard.voronoi_part_particles), run here slab after slab:
+    every slab's cells equal the whole map's bit for bit (raw sums and densities everywhere, velocities where
+    a particle reaches the cell)."""
+    from kiwi_b200 import shard
+
+    d, P, geo = _load(fn)
+    ki = kiwi.KernelIntegrator(kernel=int(d["kernel_index"]))
+    sup = float(d["support_in_h"])
+    whole = kiwi.map_voronoi(P, d["home"], geo, kernel=ki, raw=True, ctx=ctx)
+    for n in (2, 3):
+        own = shard.voronoi_cell_owners(geo, n)
+        for p in range(n):
+            idx = shard.voronoi_part_particles(P, d["home"], geo, own, p, sup)
+            part = kiwi.map_voronoi({k: v[idx] for k, v in P.items()}, d["home"][idx], geo, kernel=ki, raw=True,
+                                    ctx=ctx)
+            cells = own == p
+            assert np.array_equal(part.raw[:, cells], whole.raw[:, cells]), (n, p)
+            assert np.array_equal(part.density[cells], whole.density[cells]), (n, p)
+            reached = cells & (whole.raw[0] > 0)
+            for k in ("vx", "vy", "vz"):
+                assert np.array_equal(getattr(part, k)[reached], getattr(whole, k)[reached]), (n, p, k)
+
+
+def test_slab_particles_on_a_larger_tessellation(kiwi, ctx, reflib):
+    """2,000 particles with small supports on the reference's own Voro++ tessellation, four slabs: every
+    slab maps a proper subset of the particles and its cells equal the whole map's bit for bit."""
+    from kiwi_b200 import shard
+
+    P = random_particles(2000, 23, hmin=0.02, hmax=0.06)
+    geo, _ = reflib.voronoi(P, (0, 2, 0, 2, 0, 2), run_map=False)
+    cells = {k: geo[k] for k in ("face_off", "vert_off", "vxyz", "face_nbr", "volume")}
+    whole = kiwi.map_voronoi(P, geo["home"], cells, raw=True, ctx=ctx)
+    own = shard.voronoi_cell_owners(cells, 4)
+    for p in range(4):
+        idx = shard.voronoi_part_particles(P, geo["home"], cells, own, p, 2.0)
+        assert 0 < len(idx) < 2000
+        part = kiwi.map_voronoi({k: v[idx] for k, v in P.items()}, geo["home"][idx], cells, raw=True, ctx=ctx)
+        mine = own == p
+        assert np.array_equal(part.raw[:, mine], whole.raw[:, mine]), p
+        reached = mine & (whole.raw[0] > 0)
+        assert np.array_equal(part.vx[reached], whole.vx[reached]), p

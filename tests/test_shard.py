@@ -1,5 +1,6 @@
 """Host side of splitting one grid over several GPUs (kiwi_b200.shard): the tile entry counts, the
 ownership rule, and the multi-rank agreement and timing reduction over gloo with two ranks on the CPU."""
+import glob
 import os
 import socket
 
@@ -204,3 +205,84 @@ def test_two_ranks_map_their_parts_gloo(oracle):
         assert np.array_equal(assembled[f], whole[f])
     for f in (1, 2, 3):
         assert np.array_equal(assembled[f][reached], whole[f][reached])
+
+
+VOR_GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "vor_*.npz")))
+
+
+def _vor_fixture(fn):
+    d = np.load(fn)
+    P = {k: d[k] for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+    geo = {k[4:]: d[k] for k in d.files if k.startswith("geo_")}
+    k = int(d["kernel_index"])
+    return d, P, geo, (k if k > 0 else -1), float(d["support_in_h"])
+
+
+def test_voronoi_slabs_are_balanced_and_ordered():
+    _, _, geo, _, _ = _vor_fixture(VOR_GOLDEN[0])
+    start, end = shard._cell_vertex_rows(geo)
+    v = geo["vxyz"].reshape(-1, 3)
+    centre = np.array([v[a:b, 0].mean() for a, b in zip(start, end)])
+    for n in (2, 3, 5):
+        own = shard.voronoi_cell_owners(geo, n)
+        counts = np.bincount(own, minlength=n)
+        assert counts.max() - counts.min() <= 1
+        for p in range(n - 1):
+            assert centre[own == p].max() <= centre[own == p + 1].min() + 1e-12
+
+
+def _check_voronoi_slabs(oracle, P, home, geo, k, sup, parts=(2, 3)):
+    """Each slab's particles, mapped on their own (the oracle, the reference's algorithm), give the slab's
+    cells bit for bit as the whole snapshot gives them (raw sums and densities everywhere, velocities where
+    a particle reaches the cell).  Returns the slabs' particle counts."""
+    whole = oracle.map_voronoi(P, home, geo, kernel=k, support_in_h=sup)
+    sizes = []
+    for n in parts:
+        own = shard.voronoi_cell_owners(geo, n)
+        for p in range(n):
+            idx = shard.voronoi_part_particles(P, home, geo, own, p, sup)
+            sizes.append(len(idx))
+            part = oracle.map_voronoi({q: v[idx] for q, v in P.items()}, home[idx], geo, kernel=k, support_in_h=sup)
+            cells = own == p
+            assert np.array_equal(part[4][:, cells], whole[4][:, cells]), (n, p)
+            assert np.array_equal(part[0][cells], whole[0][cells]), (n, p)
+            reached = cells & (whole[4][0] > 0)
+            for i in (1, 2, 3):
+                assert np.array_equal(part[i][reached], whole[i][reached]), (n, p, i)
+    return sizes
+
+
+@pytest.mark.parametrize("fn", VOR_GOLDEN, ids=[os.path.basename(f)[4:-4] for f in VOR_GOLDEN])
+def test_voronoi_part_particles_reproduce_their_cells(oracle, fn):
+    d, P, geo, k, sup = _vor_fixture(fn)
+    _check_voronoi_slabs(oracle, P, d["home"], geo, k, sup)
+
+
+def test_voronoi_slab_particles_on_a_larger_tessellation(oracle, reflib):
+    """2,000 particles with small supports on the reference's own Voro++ tessellation: every slab maps a
+    proper subset of the particles and its cells come out bit for bit."""
+    P = random_particles(2000, 23, hmin=0.02, hmax=0.06)
+    geo, _ = reflib.voronoi(P, (0, 2, 0, 2, 0, 2), run_map=False)
+    sizes = _check_voronoi_slabs(oracle, P, geo["home"], geo, -1, 2.0, parts=(2, 4))
+    assert max(sizes) < 2000 and min(sizes) > 0
+
+
+def test_snapshot_work_is_the_bounding_box_pair_count(oracle):
+    for seed in (3, 4):
+        P = random_particles(200, seed, hmin=0.02, hmax=0.3)
+        b, shape = (0, 2, 0, 2, 0, 2), (20, 12, 9)
+        st = oracle.sph_to_grid(P, b, shape)[5]
+        assert shard.snapshot_work(P, b, shape, 2.0) == st.bbox_pairs
+
+
+def test_snapshots_dealt_longest_first():
+    rng = np.random.default_rng(5)
+    work = rng.integers(1, 10_000, 64) ** 2
+    for n in (1, 2, 3, 8):
+        parts = shard.assign_snapshots_lpt(work, n)
+        allp = np.concatenate(parts)
+        assert np.array_equal(np.sort(allp), np.arange(64))  # disjoint and complete
+        loads = [int(work[q].sum()) for q in parts]
+        assert max(loads) <= work.sum() / n + work.max()  # the greedy bound
+        again = shard.assign_snapshots_lpt(work.copy(), n)  # deterministic: every rank derives the same
+        assert all(np.array_equal(a, b) for a, b in zip(parts, again))
