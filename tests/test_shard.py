@@ -286,3 +286,49 @@ def test_snapshots_dealt_longest_first():
         assert max(loads) <= work.sum() / n + work.max()  # the greedy bound
         again = shard.assign_snapshots_lpt(work.copy(), n)  # deterministic: every rank derives the same
         assert all(np.array_equal(a, b) for a, b in zip(parts, again))
+
+
+def _rank_voronoi(rank, world, port, fn, q):
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import torch
+
+        from oracle.oracle import Oracle
+
+        # every rank loads the tessellation, derives the slabs, and maps only the particles that can reach
+        # its own slab (the oracle standing in for the device call); the slabs' raw sums go to rank 0
+        d, P, geo, k, sup = _vor_fixture(fn)
+        own = shard.voronoi_cell_owners(geo, world)
+        idx = shard.voronoi_part_particles(P, d["home"], geo, own, rank, sup)
+        raw = Oracle().map_voronoi({q_: v[idx] for q_, v in P.items()}, d["home"][idx], geo, kernel=k,
+                                   support_in_h=sup)[4]
+        mine = torch.tensor(np.where(own == rank, raw, 0.0))
+        parts = [torch.zeros_like(mine) for _ in range(world)]
+        dist.all_gather(parts, mine)
+        q.put((rank, [t.numpy() for t in parts] if rank == 0 else None))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_map_their_voronoi_slabs_gloo(oracle):
+    """Two gloo ranks each map their slab's particles; the gathered raw sums equal the whole map's bit for
+    bit."""
+    import multiprocessing as mp
+
+    fn = VOR_GOLDEN[0]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_voronoi, args=(r, 2, port, fn, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = sorted([q.get(timeout=300) for _ in procs], key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    d, P, geo, k, sup = _vor_fixture(fn)
+    whole = oracle.map_voronoi(P, d["home"], geo, kernel=k, support_in_h=sup)[4]
+    assert np.array_equal(out[0][1][0] + out[0][1][1], whole)
