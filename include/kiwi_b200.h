@@ -221,6 +221,13 @@ int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, c
                                  const KiwiKernelSel* kernel, int precision, int part, int n_parts, double* density,
                                  double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
 
+/* Host only, no GPU work: the x rows [*ix0, *ix1) of cells that part `part` of kiwi_sph_to_grid_device_part
+ * writes (its tiles' cells lie in these rows, contiguous in the output layout), from HOST arrays x, y, z,
+ * h of the same particles: the same support boxes and ownership rule, so that each rank knows which rows
+ * to copy back before it runs.  *ix0 = *ix1 = 0 if the part owns no tile.  ctx may be NULL (no message). */
+int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                   const KiwiKernelSel* kernel, int part, int n_parts, int* ix0, int* ix1);
+
 /* Adjoint of the sph-to-grid raw sums.  It has no counterpart in the reference (which has no gradients).
  * With M_c = sum_p m_p K_pc and P_c = sum_p m_p K_pc v_p the raw sums of kiwi_sph_to_grid_device
  * (K_pc the particle's kernel mass in cell c, clamped at 0), and raw4 the cotangents dL/dM, dL/dPx,

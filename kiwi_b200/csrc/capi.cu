@@ -521,6 +521,76 @@ int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, c
     return KIWI_OK;
 }
 
+// Host only: the split of kiwi_sph_to_grid_device_part restated over host arrays -- the same clamped
+// support boxes (particle_cell_box), the (tile, particle) entries per tile from a 3-D difference array
+// over the particles' tile boxes, and the same integer ownership rule as k_tile_part_flags -- so that a
+// rank knows the x rows its part writes before any GPU work.
+int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                   const KiwiKernelSel* kernel, int part, int n_parts, int* ix0, int* ix1) {
+    if (!particles || !ix0 || !ix1) return set_err(ctx, KIWI_ERR_ARG, "particles, ix0 and ix1 must not be null");
+    if (particles->n < 0 || (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h)))
+        return set_err(ctx, KIWI_ERR_ARG, "particles need n >= 0 and host arrays x, y, z, h");
+    if (n_parts < 1 || n_parts > 65536 || part < 0 || part >= n_parts)
+        return set_err(ctx, KIWI_ERR_ARG, "part %d of %d parts is out of range (1 <= n_parts <= 65536)", part,
+                       n_parts);
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    CartGeom g;
+    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+    const int64_t ntx = g.ntx, nty = g.nty, ntz = g.ntz, nt = ntx * nty * ntz;
+    std::vector<int64_t> d((size_t)((ntx + 1) * (nty + 1) * (ntz + 1)), 0);
+    auto at = [&](int64_t x, int64_t y, int64_t z) -> int64_t& { return d[(size_t)((x * (nty + 1) + y) * (ntz + 1) + z)]; };
+    for (int64_t i = 0; i < particles->n; ++i) {
+        CellBox b;
+        bool outside = false;
+        if (!particle_cell_box(g, particles->x[i], particles->y[i], particles->z[i], particles->h[i], b, &outside))
+            continue;
+        const int64_t x0 = b.x0 / kTileX, x1 = b.x1 / kTileX + 1, y0 = b.y0 / kTileY, y1 = b.y1 / kTileY + 1,
+                      z0 = b.z0 / kTileZ, z1 = b.z1 / kTileZ + 1;
+        at(x0, y0, z0) += 1;
+        at(x1, y0, z0) -= 1;
+        at(x0, y1, z0) -= 1;
+        at(x0, y0, z1) -= 1;
+        at(x1, y1, z0) += 1;
+        at(x1, y0, z1) += 1;
+        at(x0, y1, z1) += 1;
+        at(x1, y1, z1) -= 1;
+    }
+    for (int64_t x = 0; x <= ntx; ++x)  // prefix sums along z, y, x give each tile's entry count
+        for (int64_t y = 0; y <= nty; ++y)
+            for (int64_t z = 1; z <= ntz; ++z) at(x, y, z) += at(x, y, z - 1);
+    for (int64_t x = 0; x <= ntx; ++x)
+        for (int64_t y = 1; y <= nty; ++y)
+            for (int64_t z = 0; z <= ntz; ++z) at(x, y, z) += at(x, y - 1, z);
+    for (int64_t x = 1; x <= ntx; ++x)
+        for (int64_t y = 0; y <= nty; ++y)
+            for (int64_t z = 0; z <= ntz; ++z) at(x, y, z) += at(x - 1, y, z);
+    std::vector<int64_t> w((size_t)nt);
+    int64_t W = 0;
+    for (int64_t t = 0; t < nt; ++t) {
+        const int64_t tx = t / (nty * ntz), ty = (t / ntz) % nty, tz = t % ntz;
+        w[(size_t)t] = std::min<int64_t>(at(tx, ty, tz), 0xFFFFFFFFLL);  // the device counts tiles in 32 bits
+        W += w[(size_t)t];
+    }
+    int64_t first = -1, last = -1, prefix = 0;
+    for (int64_t t = 0; t < nt; ++t) {
+        int64_t owner = W > 0 ? (prefix * n_parts) / W : (t * n_parts) / nt;
+        if (owner > n_parts - 1) owner = n_parts - 1;
+        if (owner == part) {
+            if (first < 0) first = t;
+            last = t;
+        }
+        prefix += w[(size_t)t];
+    }
+    if (first < 0) {
+        *ix0 = *ix1 = 0;
+    } else {
+        *ix0 = (int)(first / (nty * ntz)) * kTileX;
+        *ix1 = std::min<int>(g.nx, (int)(last / (nty * ntz) + 1) * kTileX);
+    }
+    return KIWI_OK;
+}
+
 int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                                     const KiwiKernelSel* kernel, const double* d_raw4, double* d_x, double* d_y,
                                     double* d_z, double* d_h, double* d_m, double* d_vx, double* d_vy, double* d_vz,

@@ -332,3 +332,45 @@ def test_two_ranks_map_their_voronoi_slabs_gloo(oracle):
     d, P, geo, k, sup = _vor_fixture(fn)
     whole = oracle.map_voronoi(P, d["home"], geo, kernel=k, support_in_h=sup)[4]
     assert np.array_equal(out[0][1][0] + out[0][1][1], whole)
+
+
+def test_c_abi_part_rows_match_the_host_rule():
+    """kiwi_part_rows (host only, no GPU) gives the rows of shard.part_rows: the C ABI's restatement of the
+    split for C and C++ callers, on random, clustered and out-of-domain particles and several kernels."""
+    import ctypes as C
+
+    import kiwi_b200 as kb
+
+    lib = C.CDLL(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "kiwi_b200",
+                              "libkiwi_b200.so"))
+    lib.kiwi_part_rows.argtypes = [C.c_void_p, C.POINTER(kb.KiwiParticles), C.POINTER(kb.KiwiCartGrid),
+                                   C.POINTER(kb.KiwiKernelSel), C.c_int, C.c_int, C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)]
+    rng = np.random.default_rng(9)
+    dp = C.POINTER(C.c_double)
+    for case in range(12):
+        n = int(rng.integers(0, 3000))
+        P = random_particles(n, 40 + case, hmin=0.01, hmax=0.4)
+        if case % 3 == 1:  # clustered
+            for k in "xyz":
+                P[k] = 1.0 + 0.1 * rng.standard_normal(n)
+        if case % 3 == 2 and n:  # some outside the domain, some with h <= 0
+            P["x"][: n // 5] += 5.0
+            P["h"][n // 5: n // 4] = 0.0
+        shape = tuple(int(v) for v in rng.integers(5, 70, 3))
+        b = (0.0, 2.0, -0.3, 2.1, 0.1, 1.7)
+        kernel, sup = [(0, 2.0), (4, 2.0), (2, 0.0)][case % 3]
+        sup_h = sup or kb.get_kernel("quintic_spline").radkern
+        arrs = {k: np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+        parts = kb.KiwiParticles(n, *[arrs[k].ctypes.data_as(dp) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")])
+        grid = kb.KiwiCartGrid((C.c_double * 6)(*b), *shape)
+        sel = kb.KiwiKernelSel(kernel, sup, 0, 0)
+        for n_parts in (1, 2, 3, 7):
+            own = shard.tile_owners(shard.tile_entry_counts(arrs, b, shape, sup_h), n_parts)
+            for p in range(n_parts):
+                a0, a1 = C.c_int(-1), C.c_int(-1)
+                assert lib.kiwi_part_rows(None, C.byref(parts), C.byref(grid), C.byref(sel), p, n_parts,
+                                          C.byref(a0), C.byref(a1)) == 0
+                assert (a0.value, a1.value) == shard.part_rows(own, p, shape), (case, n_parts, p)
+    a0, a1 = C.c_int(), C.c_int()
+    assert lib.kiwi_part_rows(None, C.byref(parts), C.byref(grid), C.byref(sel), 3, 3, C.byref(a0), C.byref(a1)) < 0
