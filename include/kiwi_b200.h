@@ -360,6 +360,20 @@ int kiwi_map_voronoi_device(KiwiCtx* ctx, const KiwiParticles* particles, const 
                             const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, int precision, double* density,
                             double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
 
+/* A Voronoi map over several GPUs (no counterpart in the reference), host only, no GPU work.
+ * kiwi_voronoi_cell_owners: owner[c] in [0, n_parts), the cells split into spatial slabs along `axis`
+ * (0, 1, 2): ordered by the midpoint (lo + hi) / 2 of their vertices' extent along it (ties by cell index;
+ * coordinates must be finite) and cut into runs of near-equal counts (rank k -> part k n_parts / n_cells).
+ * kiwi_voronoi_part_particles: select[i] = 1 for the particles whose walk can reach a cell of `part` --
+ * home cell owned by it, or support sphere within 1.001 radii of the box around its cells' vertices --
+ * and the count in *n_selected.  A rank that maps these particles (in their order) with kiwi_map_voronoi
+ * gets its own cells bit for bit as the whole snapshot gives them; a cell no particle reaches takes the
+ * whole snapshot's mean velocity.  Every array is a HOST array; ctx may be NULL (no message). */
+int kiwi_voronoi_cell_owners(KiwiCtx* ctx, const KiwiVoronoiCells* cells, int n_parts, int axis, int32_t* owner);
+int kiwi_voronoi_part_particles(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                                const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, const int32_t* owner,
+                                int part, uint8_t* select, int64_t* n_selected);
+
 /* The inverse-mapping check (run_inverse_mapping_test_stage's particle loop, src/mapping.cpp:540-701): the
  * same cell walk and cell integrals as kiwi_map_voronoi, summed per particle instead of per cell, in the
  * walk's order: m_recovered[i] = sum over the cells i reaches of (integral m_i' / M_c) M_c over cells with

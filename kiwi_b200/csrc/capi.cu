@@ -591,6 +591,102 @@ int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartG
     return KIWI_OK;
 }
 
+namespace {
+// A cell's vertex rows [vert_off[face_off[c]], vert_off[face_off[c + 1]]) (its faces, and their vertices,
+// are back to back), checked against the geometry's sizes.
+int voronoi_host_rows(KiwiCtx* ctx, const KiwiVoronoiCells* cells, std::vector<int64_t>* start,
+                      std::vector<int64_t>* end) {
+    if (!cells || cells->n_cells < 0 || (cells->n_cells > 0 && (!cells->face_off || !cells->vert_off || !cells->vxyz)))
+        return set_err(ctx, KIWI_ERR_ARG, "cells need n_cells >= 0 and host arrays face_off, vert_off, vxyz");
+    const int64_t nc = cells->n_cells;
+    start->resize((size_t)nc);
+    end->resize((size_t)nc);
+    int64_t prev = 0;
+    for (int64_t c = 0; c < nc; ++c) {
+        const int64_t f0 = cells->face_off[c], f1 = cells->face_off[c + 1];
+        if (f0 < 0 || f1 < f0) return set_err(ctx, KIWI_ERR_ARG, "face_off must start at 0 and not decrease");
+        const int64_t a = cells->vert_off[f0], b = cells->vert_off[f1];
+        if (a < prev || b < a) return set_err(ctx, KIWI_ERR_ARG, "vert_off must not decrease");
+        (*start)[(size_t)c] = a;
+        (*end)[(size_t)c] = b;
+        prev = b;
+    }
+    return KIWI_OK;
+}
+}  // namespace
+
+int kiwi_voronoi_cell_owners(KiwiCtx* ctx, const KiwiVoronoiCells* cells, int n_parts, int axis, int32_t* owner) {
+    if (n_parts < 1 || axis < 0 || axis > 2 || (!owner && cells && cells->n_cells > 0))
+        return set_err(ctx, KIWI_ERR_ARG, "n_parts must be >= 1, axis 0, 1 or 2, owner non-null");
+    std::vector<int64_t> start, end;
+    KIWI_TRY(voronoi_host_rows(ctx, cells, &start, &end));
+    const int64_t nc = cells->n_cells;
+    std::vector<double> mid((size_t)nc, 0.0);
+    for (int64_t c = 0; c < nc; ++c) {
+        if (end[(size_t)c] <= start[(size_t)c]) continue;
+        double lo = cells->vxyz[3 * start[(size_t)c] + axis], hi = lo;
+        for (int64_t r = start[(size_t)c] + 1; r < end[(size_t)c]; ++r) {
+            const double v = cells->vxyz[3 * r + axis];
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+        }
+        mid[(size_t)c] = (lo + hi) * 0.5;
+    }
+    std::vector<int64_t> order((size_t)nc);
+    for (int64_t c = 0; c < nc; ++c) order[(size_t)c] = c;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return mid[(size_t)a] < mid[(size_t)b]; });
+    for (int64_t k = 0; k < nc; ++k) owner[(size_t)order[(size_t)k]] = (int32_t)((k * n_parts) / nc);
+    return KIWI_OK;
+}
+
+int kiwi_voronoi_part_particles(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
+                                const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, const int32_t* owner,
+                                int part, uint8_t* select, int64_t* n_selected) {
+    if (!particles || !n_selected || particles->n < 0 ||
+        (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h || !home_cell ||
+                              !select)))
+        return set_err(ctx, KIWI_ERR_ARG, "particles (host x, y, z, h), home_cell, select and n_selected are needed");
+    std::vector<int64_t> start, end;
+    KIWI_TRY(voronoi_host_rows(ctx, cells, &start, &end));
+    if (cells->n_cells > 0 && !owner) return set_err(ctx, KIWI_ERR_ARG, "owner is null");
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    const int64_t nc = cells->n_cells;
+    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool any = false;
+    for (int64_t c = 0; c < nc; ++c) {
+        if (owner[(size_t)c] != part) continue;
+        for (int64_t r = start[(size_t)c]; r < end[(size_t)c]; ++r)
+            for (int a = 0; a < 3; ++a) {
+                const double v = cells->vxyz[3 * r + a];
+                lo[a] = any ? std::min(lo[a], v) : v;
+                hi[a] = any ? std::max(hi[a], v) : v;
+                if (a == 2) any = true;
+            }
+    }
+    const double rscale = 1.001 * kc.support_in_h;
+    int64_t count = 0;
+    for (int64_t i = 0; i < particles->n; ++i) {
+        const int32_t hc = home_cell[i];
+        bool s = hc >= 0 && hc < nc && owner[hc] == part;
+        if (!s && any) {
+            const double c3[3] = {particles->x[i], particles->y[i], particles->z[i]};
+            double d2 = 0.0;
+            for (int a = 0; a < 3; ++a) {
+                const double t = std::max(std::max(lo[a] - c3[a], c3[a] - hi[a]), 0.0);
+                d2 += t * t;
+            }
+            const double r = rscale * particles->h[i];
+            s = d2 <= r * r;
+        }
+        select[i] = s ? 1 : 0;
+        count += s;
+    }
+    *n_selected = count;
+    return KIWI_OK;
+}
+
 int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                                     const KiwiKernelSel* kernel, const double* d_raw4, double* d_x, double* d_y,
                                     double* d_z, double* d_h, double* d_m, double* d_vx, double* d_vy, double* d_vz,

@@ -133,18 +133,28 @@ def _cell_vertex_rows(cells: dict):
     return vo[fo[:-1]], vo[fo[1:]]
 
 
-def voronoi_cell_owners(cells: dict, n_parts: int, axis: int = 0) -> np.ndarray:
-    """Voronoi cells split into n_parts spatial slabs along `axis`: the cells ordered by the mean of their
-    vertices' coordinate (ties by cell index), cut into runs of near-equal cell counts (cell of rank k goes
-    to part floor(k n / n_cells))."""
+def _cell_midpoints(cells: dict, axis: int) -> np.ndarray:
+    """Per cell, the midpoint (lo + hi) / 2 of its vertices' extent along `axis` (0 for a cell without
+    vertices): min, max and one sum, so that every restatement of it rounds alike."""
     start, end = _cell_vertex_rows(cells)
-    nc = len(start)
-    if nc == 0:
-        return np.zeros(0, dtype=np.int64)
     coord = np.asarray(cells["vxyz"], dtype=np.float64).reshape(-1, 3)[:, axis]
-    cs = np.concatenate([[0.0], np.cumsum(coord)])
-    cnt = end - start
-    centre = np.where(cnt > 0, (cs[end] - cs[start]) / np.maximum(cnt, 1), 0.0)
+    mid = np.zeros(len(start))
+    has = end > start
+    if has.any():
+        # the cells' rows are back to back in cell order (CSR), so the non-empty cells' starts delimit them
+        s = start[has]
+        mid[has] = (np.minimum.reduceat(coord, s) + np.maximum.reduceat(coord, s)) * 0.5
+    return mid
+
+
+def voronoi_cell_owners(cells: dict, n_parts: int, axis: int = 0) -> np.ndarray:
+    """Voronoi cells split into n_parts spatial slabs along `axis`: the cells ordered by the midpoint of
+    their vertices' extent along it (ties by cell index), cut into runs of near-equal cell counts (the cell
+    of rank k goes to part floor(k n / n_cells))."""
+    nc = len(np.asarray(cells["face_off"])) - 1
+    if nc <= 0:
+        return np.zeros(0, dtype=np.int64)
+    centre = _cell_midpoints(cells, axis)
     order = np.argsort(centre, kind="stable")
     owner = np.empty(nc, dtype=np.int64)
     owner[order] = (np.arange(nc, dtype=np.int64) * n_parts) // nc

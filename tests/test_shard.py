@@ -222,7 +222,7 @@ def test_voronoi_slabs_are_balanced_and_ordered():
     _, _, geo, _, _ = _vor_fixture(VOR_GOLDEN[0])
     start, end = shard._cell_vertex_rows(geo)
     v = geo["vxyz"].reshape(-1, 3)
-    centre = np.array([v[a:b, 0].mean() for a, b in zip(start, end)])
+    centre = np.array([(v[a:b, 0].min() + v[a:b, 0].max()) * 0.5 for a, b in zip(start, end)])
     for n in (2, 3, 5):
         own = shard.voronoi_cell_owners(geo, n)
         counts = np.bincount(own, minlength=n)
@@ -374,3 +374,55 @@ def test_c_abi_part_rows_match_the_host_rule():
                 assert (a0.value, a1.value) == shard.part_rows(own, p, shape), (case, n_parts, p)
     a0, a1 = C.c_int(), C.c_int()
     assert lib.kiwi_part_rows(None, C.byref(parts), C.byref(grid), C.byref(sel), 3, 3, C.byref(a0), C.byref(a1)) < 0
+
+
+def test_c_abi_voronoi_slabs_match_the_host_rule(reflib):
+    """kiwi_voronoi_cell_owners and kiwi_voronoi_part_particles (host only, no GPU) give the owners and
+    particle sets of shard.voronoi_cell_owners / voronoi_part_particles, on every axis and several part
+    counts, on the Voronoi fixtures and on a 2,000-particle Voro++ tessellation."""
+    import ctypes as C
+
+    import kiwi_b200 as kb
+
+    lib = C.CDLL(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "kiwi_b200",
+                              "libkiwi_b200.so"))
+    i32p, i64p, dp = C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double)
+    lib.kiwi_voronoi_cell_owners.argtypes = [C.c_void_p, C.POINTER(kb.KiwiVoronoiCells), C.c_int, C.c_int, i32p]
+    lib.kiwi_voronoi_part_particles.argtypes = [C.c_void_p, C.POINTER(kb.KiwiParticles), i32p,
+                                                C.POINTER(kb.KiwiVoronoiCells), C.POINTER(kb.KiwiKernelSel), i32p,
+                                                C.c_int, C.POINTER(C.c_uint8), i64p]
+    cases = []
+    for fn in VOR_GOLDEN:
+        d, P, geo, _, sup = _vor_fixture(fn)
+        cases.append((P, d["home"], geo, int(d["kernel_index"]), sup))
+    P = random_particles(2000, 23, hmin=0.02, hmax=0.06)
+    g, _ = reflib.voronoi(P, (0, 2, 0, 2, 0, 2), run_map=False)
+    cases.append((P, g["home"], g, 0, 2.0))
+    for P, home, geo, kernel, sup in cases:
+        fo = np.ascontiguousarray(geo["face_off"], dtype=np.int64)
+        vo = np.ascontiguousarray(geo["vert_off"], dtype=np.int64)
+        vx = np.ascontiguousarray(geo["vxyz"], dtype=np.float64).reshape(-1)
+        nb = np.ascontiguousarray(geo["face_nbr"], dtype=np.int32)
+        vol = np.ascontiguousarray(geo["volume"], dtype=np.float64)
+        cells = kb.KiwiVoronoiCells(len(vol), fo.ctypes.data_as(i64p), vo.ctypes.data_as(i64p), vx.ctypes.data_as(dp),
+                                    nb.ctypes.data_as(i32p), vol.ctypes.data_as(dp))
+        arrs = {k: np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+        parts = kb.KiwiParticles(len(arrs["x"]), *[arrs[k].ctypes.data_as(dp)
+                                                   for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")])
+        hm = np.ascontiguousarray(home, dtype=np.int32)
+        sel = kb.KiwiKernelSel(kernel, 0.0, 0, 0)
+        for axis in (0, 1, 2):
+            for n in (1, 2, 3, 5):
+                own_c = np.zeros(len(vol), dtype=np.int32)
+                assert lib.kiwi_voronoi_cell_owners(None, C.byref(cells), n, axis, own_c.ctypes.data_as(i32p)) == 0
+                own = shard.voronoi_cell_owners(geo, n, axis=axis)
+                assert np.array_equal(own_c, own), (axis, n)
+                for p in range(n):
+                    s = np.zeros(len(arrs["x"]), dtype=np.uint8)
+                    cnt = C.c_int64(-1)
+                    assert lib.kiwi_voronoi_part_particles(None, C.byref(parts), hm.ctypes.data_as(i32p),
+                                                           C.byref(cells), C.byref(sel), own_c.ctypes.data_as(i32p),
+                                                           p, s.ctypes.data_as(C.POINTER(C.c_uint8)),
+                                                           C.byref(cnt)) == 0
+                    want = shard.voronoi_part_particles(P, home, geo, own, p, sup)
+                    assert np.array_equal(np.nonzero(s)[0], want) and cnt.value == len(want), (axis, n, p)
