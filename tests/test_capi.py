@@ -112,3 +112,37 @@ int main() {
 ''')
     subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-o", str(tmp_path / "use"), str(src),
                     "-L", os.path.join(ROOT, "kiwi_b200"), "-lkiwi_b200"], check=True)
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/kiwi_b200.h compiles as strict C99 and a plain C program links against the library and calls
+    its host-only entry points (kernel lookup, the split of one grid over parts) without a GPU."""
+    import subprocess
+
+    src = tmp_path / "use.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "kiwi_b200.h"
+int main(void) {
+    double x[2] = {0.5, 1.5}, y[2] = {0.5, 1.5}, z[2] = {0.5, 1.5}, v[2] = {0, 0}, m[2] = {1, 1}, h[2] = {0.2, 0.2};
+    KiwiParticles p = {2, x, y, z, v, v, v, m, h};
+    KiwiCartGrid g = {{0.0, 2.0, 0.0, 2.0, 0.0, 2.0}, 32, 16, 16};
+    KiwiKernelSel k = {0, 0.0, 0, 0};
+    int a0 = -1, a1 = -1, b0 = -1, b1 = -1;
+    if (kiwi_kernel_index("cubic_spline") != 0) return 1;
+    if (kiwi_part_rows(NULL, &p, &g, &k, 0, 2, &a0, &a1) != 0) return 2;
+    if (kiwi_part_rows(NULL, &p, &g, &k, 1, 2, &b0, &b1) != 0) return 3;
+    printf("%d %d %d %d\n", a0, a1, b0, b1);
+    return 0;
+}
+''')
+    exe = tmp_path / "use"
+    libdir = os.path.dirname(LIB)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"), str(src),
+                    "-o", str(exe), "-L", libdir, "-lkiwi_b200", "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out
+    a0, a1, b0, b1 = (int(t) for t in out.stdout.split())
+    # two particles touching tiles 0, 4 and 11, 15 of the 4 x 2 x 2 tiles: part 0 owns tiles 0-4 (x rows
+    # 0-15), part 1 tiles 5-15 (x rows 8-31)
+    assert (a0, a1) == (0, 16) and (b0, b1) == (8, 32)
