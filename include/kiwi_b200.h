@@ -228,6 +228,13 @@ int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, c
 int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                    const KiwiKernelSel* kernel, int part, int n_parts, int* ix0, int* ix1);
 
+/* Host only, no GPU work: a snapshot's (particle, cell) pairs within the particles' clamped support boxes
+ * (src/cartesian_grid.cpp:211-237; KiwiStats.bbox_pairs of the reference-order form), from HOST arrays x, y,
+ * z, h -- the work estimate by which a batch of snapshots is dealt to GPUs, longest first.  ctx may be
+ * NULL (no message). */
+int kiwi_snapshot_work(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                       const KiwiKernelSel* kernel, int64_t* bbox_pairs);
+
 /* Adjoint of the sph-to-grid raw sums.  It has no counterpart in the reference (which has no gradients).
  * With M_c = sum_p m_p K_pc and P_c = sum_p m_p K_pc v_p the raw sums of kiwi_sph_to_grid_device
  * (K_pc the particle's kernel mass in cell c, clamped at 0), and raw4 the cotangents dL/dM, dL/dPx,

@@ -591,6 +591,27 @@ int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartG
     return KIWI_OK;
 }
 
+int kiwi_snapshot_work(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
+                       const KiwiKernelSel* kernel, int64_t* bbox_pairs) {
+    if (!particles || !bbox_pairs || particles->n < 0 ||
+        (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h)))
+        return set_err(ctx, KIWI_ERR_ARG, "particles (host x, y, z, h) and bbox_pairs are needed");
+    KernelChoice kc;
+    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+    CartGeom g;
+    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+    int64_t total = 0;
+    for (int64_t i = 0; i < particles->n; ++i) {
+        CellBox b;
+        bool outside = false;
+        if (!particle_cell_box(g, particles->x[i], particles->y[i], particles->z[i], particles->h[i], b, &outside))
+            continue;
+        total += (int64_t)(b.x1 - b.x0 + 1) * (b.y1 - b.y0 + 1) * (b.z1 - b.z0 + 1);
+    }
+    *bbox_pairs = total;
+    return KIWI_OK;
+}
+
 namespace {
 // A cell's vertex rows [vert_off[face_off[c]], vert_off[face_off[c + 1]]) (its faces, and their vertices,
 // are back to back), checked against the geometry's sizes.

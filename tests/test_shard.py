@@ -268,11 +268,31 @@ def test_voronoi_slab_particles_on_a_larger_tessellation(oracle, reflib):
 
 
 def test_snapshot_work_is_the_bounding_box_pair_count(oracle):
-    for seed in (3, 4):
+    """shard.snapshot_work and kiwi_snapshot_work (C ABI, host only) both equal the oracle's bounding-box
+    pair count."""
+    import ctypes as C
+
+    import kiwi_b200 as kb
+
+    lib = C.CDLL(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "kiwi_b200",
+                              "libkiwi_b200.so"))
+    lib.kiwi_snapshot_work.argtypes = [C.c_void_p, C.POINTER(kb.KiwiParticles), C.POINTER(kb.KiwiCartGrid),
+                                       C.POINTER(kb.KiwiKernelSel), C.POINTER(C.c_int64)]
+    dp = C.POINTER(C.c_double)
+    for seed in (3, 4, 5):
         P = random_particles(200, seed, hmin=0.02, hmax=0.3)
+        if seed == 5:
+            P["x"][:50] += 3.0  # outside the domain
         b, shape = (0, 2, 0, 2, 0, 2), (20, 12, 9)
         st = oracle.sph_to_grid(P, b, shape)[5]
         assert shard.snapshot_work(P, b, shape, 2.0) == st.bbox_pairs
+        arrs = {k: np.ascontiguousarray(P[k], dtype=np.float64) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")}
+        parts = kb.KiwiParticles(200, *[arrs[k].ctypes.data_as(dp) for k in ("x", "y", "z", "vx", "vy", "vz", "m", "h")])
+        grid = kb.KiwiCartGrid((C.c_double * 6)(*b), *shape)
+        w = C.c_int64(-1)
+        assert lib.kiwi_snapshot_work(None, C.byref(parts), C.byref(grid), C.byref(kb.KiwiKernelSel(0, 0.0, 0, 0)),
+                                      C.byref(w)) == 0
+        assert w.value == st.bbox_pairs
 
 
 def test_snapshots_dealt_longest_first():
