@@ -11,7 +11,9 @@
  *     ends in _device, in which case it is stream-ordered on the context's stream;
  *   - results are deterministic: each cell's sum is taken over its particles in ascending particle
  *     order, with no floating-point atomics, so repeated calls are bitwise identical;
- *   - there is no CPU fallback: without a usable sm_100 GPU every call fails with KIWI_ERR_NODEV.
+ *   - there is no CPU fallback: without a usable sm_100 GPU every compute call fails with
+ *     KIWI_ERR_NODEV.  The host-only helpers (kernel lookups, kiwi_part_rows, kiwi_snapshot_work,
+ *     kiwi_voronoi_cell_owners, kiwi_voronoi_part_particles, the file readers and writers) need no GPU.
  */
 #ifndef KIWI_B200_H
 #define KIWI_B200_H
@@ -27,9 +29,9 @@ extern "C" {
 #define KIWI_ERR_ARG (-1)         /* invalid argument (the reference's ConfigError / runtime_error) */
 #define KIWI_ERR_CUDA (-2)        /* a CUDA call failed */
 #define KIWI_ERR_NODEV (-3)       /* no usable GPU */
-#define KIWI_ERR_ALLOC (-4)       /* device memory allocation failed */
+#define KIWI_ERR_ALLOC (-4)       /* memory allocation failed (device; host in the host-only helpers) */
 #define KIWI_ERR_LIMIT (-5)       /* a bounded device loop hit its iteration cap */
-#define KIWI_ERR_UNSUPPORTED (-6) /* option not available in this build */
+#define KIWI_ERR_UNSUPPORTED (-6) /* option not available in this library */
 
 /* Arithmetic forms of the cell integrals (the low byte of a `precision` argument).
  * KIWI_FP64: all FP64.  The tiers are shared between the cells of a particle's box (each edge tier once

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <new>
 #include <vector>
 
 #include "../../include/kiwi_b200.h"
@@ -527,68 +528,72 @@ int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, c
 // rank knows the x rows its part writes before any GPU work.
 int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                    const KiwiKernelSel* kernel, int part, int n_parts, int* ix0, int* ix1) {
-    if (!particles || !ix0 || !ix1) return set_err(ctx, KIWI_ERR_ARG, "particles, ix0 and ix1 must not be null");
-    if (particles->n < 0 || (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h)))
-        return set_err(ctx, KIWI_ERR_ARG, "particles need n >= 0 and host arrays x, y, z, h");
-    if (n_parts < 1 || n_parts > 65536 || part < 0 || part >= n_parts)
-        return set_err(ctx, KIWI_ERR_ARG, "part %d of %d parts is out of range (1 <= n_parts <= 65536)", part,
-                       n_parts);
-    KernelChoice kc;
-    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
-    CartGeom g;
-    KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
-    const int64_t ntx = g.ntx, nty = g.nty, ntz = g.ntz, nt = ntx * nty * ntz;
-    std::vector<int64_t> d((size_t)((ntx + 1) * (nty + 1) * (ntz + 1)), 0);
-    auto at = [&](int64_t x, int64_t y, int64_t z) -> int64_t& { return d[(size_t)((x * (nty + 1) + y) * (ntz + 1) + z)]; };
-    for (int64_t i = 0; i < particles->n; ++i) {
-        CellBox b;
-        bool outside = false;
-        if (!particle_cell_box(g, particles->x[i], particles->y[i], particles->z[i], particles->h[i], b, &outside))
-            continue;
-        const int64_t x0 = b.x0 / kTileX, x1 = b.x1 / kTileX + 1, y0 = b.y0 / kTileY, y1 = b.y1 / kTileY + 1,
-                      z0 = b.z0 / kTileZ, z1 = b.z1 / kTileZ + 1;
-        at(x0, y0, z0) += 1;
-        at(x1, y0, z0) -= 1;
-        at(x0, y1, z0) -= 1;
-        at(x0, y0, z1) -= 1;
-        at(x1, y1, z0) += 1;
-        at(x1, y0, z1) += 1;
-        at(x0, y1, z1) += 1;
-        at(x1, y1, z1) -= 1;
-    }
-    for (int64_t x = 0; x <= ntx; ++x)  // prefix sums along z, y, x give each tile's entry count
-        for (int64_t y = 0; y <= nty; ++y)
-            for (int64_t z = 1; z <= ntz; ++z) at(x, y, z) += at(x, y, z - 1);
-    for (int64_t x = 0; x <= ntx; ++x)
-        for (int64_t y = 1; y <= nty; ++y)
-            for (int64_t z = 0; z <= ntz; ++z) at(x, y, z) += at(x, y - 1, z);
-    for (int64_t x = 1; x <= ntx; ++x)
-        for (int64_t y = 0; y <= nty; ++y)
-            for (int64_t z = 0; z <= ntz; ++z) at(x, y, z) += at(x - 1, y, z);
-    std::vector<int64_t> w((size_t)nt);
-    int64_t W = 0;
-    for (int64_t t = 0; t < nt; ++t) {
-        const int64_t tx = t / (nty * ntz), ty = (t / ntz) % nty, tz = t % ntz;
-        w[(size_t)t] = std::min<int64_t>(at(tx, ty, tz), 0xFFFFFFFFLL);  // the device counts tiles in 32 bits
-        W += w[(size_t)t];
-    }
-    int64_t first = -1, last = -1, prefix = 0;
-    for (int64_t t = 0; t < nt; ++t) {
-        int64_t owner = W > 0 ? (prefix * n_parts) / W : (t * n_parts) / nt;
-        if (owner > n_parts - 1) owner = n_parts - 1;
-        if (owner == part) {
-            if (first < 0) first = t;
-            last = t;
+    try {
+        if (!particles || !ix0 || !ix1) return set_err(ctx, KIWI_ERR_ARG, "particles, ix0 and ix1 must not be null");
+        if (particles->n < 0 || (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h)))
+            return set_err(ctx, KIWI_ERR_ARG, "particles need n >= 0 and host arrays x, y, z, h");
+        if (n_parts < 1 || n_parts > 65536 || part < 0 || part >= n_parts)
+            return set_err(ctx, KIWI_ERR_ARG, "part %d of %d parts is out of range (1 <= n_parts <= 65536)", part,
+                           n_parts);
+        KernelChoice kc;
+        KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+        CartGeom g;
+        KIWI_TRY(make_geom(ctx, grid, kc.support_in_h, &g));
+        const int64_t ntx = g.ntx, nty = g.nty, ntz = g.ntz, nt = ntx * nty * ntz;
+        std::vector<int64_t> d((size_t)((ntx + 1) * (nty + 1) * (ntz + 1)), 0);
+        auto at = [&](int64_t x, int64_t y, int64_t z) -> int64_t& { return d[(size_t)((x * (nty + 1) + y) * (ntz + 1) + z)]; };
+        for (int64_t i = 0; i < particles->n; ++i) {
+            CellBox b;
+            bool outside = false;
+            if (!particle_cell_box(g, particles->x[i], particles->y[i], particles->z[i], particles->h[i], b, &outside))
+                continue;
+            const int64_t x0 = b.x0 / kTileX, x1 = b.x1 / kTileX + 1, y0 = b.y0 / kTileY, y1 = b.y1 / kTileY + 1,
+                          z0 = b.z0 / kTileZ, z1 = b.z1 / kTileZ + 1;
+            at(x0, y0, z0) += 1;
+            at(x1, y0, z0) -= 1;
+            at(x0, y1, z0) -= 1;
+            at(x0, y0, z1) -= 1;
+            at(x1, y1, z0) += 1;
+            at(x1, y0, z1) += 1;
+            at(x0, y1, z1) += 1;
+            at(x1, y1, z1) -= 1;
         }
-        prefix += w[(size_t)t];
+        for (int64_t x = 0; x <= ntx; ++x)  // prefix sums along z, y, x give each tile's entry count
+            for (int64_t y = 0; y <= nty; ++y)
+                for (int64_t z = 1; z <= ntz; ++z) at(x, y, z) += at(x, y, z - 1);
+        for (int64_t x = 0; x <= ntx; ++x)
+            for (int64_t y = 1; y <= nty; ++y)
+                for (int64_t z = 0; z <= ntz; ++z) at(x, y, z) += at(x, y - 1, z);
+        for (int64_t x = 1; x <= ntx; ++x)
+            for (int64_t y = 0; y <= nty; ++y)
+                for (int64_t z = 0; z <= ntz; ++z) at(x, y, z) += at(x - 1, y, z);
+        std::vector<int64_t> w((size_t)nt);
+        int64_t W = 0;
+        for (int64_t t = 0; t < nt; ++t) {
+            const int64_t tx = t / (nty * ntz), ty = (t / ntz) % nty, tz = t % ntz;
+            w[(size_t)t] = std::min<int64_t>(at(tx, ty, tz), 0xFFFFFFFFLL);  // the device counts tiles in 32 bits
+            W += w[(size_t)t];
+        }
+        int64_t first = -1, last = -1, prefix = 0;
+        for (int64_t t = 0; t < nt; ++t) {
+            int64_t owner = W > 0 ? (prefix * n_parts) / W : (t * n_parts) / nt;
+            if (owner > n_parts - 1) owner = n_parts - 1;
+            if (owner == part) {
+                if (first < 0) first = t;
+                last = t;
+            }
+            prefix += w[(size_t)t];
+        }
+        if (first < 0) {
+            *ix0 = *ix1 = 0;
+        } else {
+            *ix0 = (int)(first / (nty * ntz)) * kTileX;
+            *ix1 = std::min<int>(g.nx, (int)(last / (nty * ntz) + 1) * kTileX);
+        }
+        return KIWI_OK;
+    } catch (const std::bad_alloc&) {
+        return set_err(ctx, KIWI_ERR_ALLOC, "host memory allocation failed");
     }
-    if (first < 0) {
-        *ix0 = *ix1 = 0;
-    } else {
-        *ix0 = (int)(first / (nty * ntz)) * kTileX;
-        *ix1 = std::min<int>(g.nx, (int)(last / (nty * ntz) + 1) * kTileX);
-    }
-    return KIWI_OK;
 }
 
 int kiwi_snapshot_work(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
@@ -637,75 +642,83 @@ int voronoi_host_rows(KiwiCtx* ctx, const KiwiVoronoiCells* cells, std::vector<i
 }  // namespace
 
 int kiwi_voronoi_cell_owners(KiwiCtx* ctx, const KiwiVoronoiCells* cells, int n_parts, int axis, int32_t* owner) {
-    if (n_parts < 1 || axis < 0 || axis > 2 || (!owner && cells && cells->n_cells > 0))
-        return set_err(ctx, KIWI_ERR_ARG, "n_parts must be >= 1, axis 0, 1 or 2, owner non-null");
-    std::vector<int64_t> start, end;
-    KIWI_TRY(voronoi_host_rows(ctx, cells, &start, &end));
-    const int64_t nc = cells->n_cells;
-    std::vector<double> mid((size_t)nc, 0.0);
-    for (int64_t c = 0; c < nc; ++c) {
-        if (end[(size_t)c] <= start[(size_t)c]) continue;
-        double lo = cells->vxyz[3 * start[(size_t)c] + axis], hi = lo;
-        for (int64_t r = start[(size_t)c] + 1; r < end[(size_t)c]; ++r) {
-            const double v = cells->vxyz[3 * r + axis];
-            lo = std::min(lo, v);
-            hi = std::max(hi, v);
+    try {
+        if (n_parts < 1 || axis < 0 || axis > 2 || (!owner && cells && cells->n_cells > 0))
+            return set_err(ctx, KIWI_ERR_ARG, "n_parts must be >= 1, axis 0, 1 or 2, owner non-null");
+        std::vector<int64_t> start, end;
+        KIWI_TRY(voronoi_host_rows(ctx, cells, &start, &end));
+        const int64_t nc = cells->n_cells;
+        std::vector<double> mid((size_t)nc, 0.0);
+        for (int64_t c = 0; c < nc; ++c) {
+            if (end[(size_t)c] <= start[(size_t)c]) continue;
+            double lo = cells->vxyz[3 * start[(size_t)c] + axis], hi = lo;
+            for (int64_t r = start[(size_t)c] + 1; r < end[(size_t)c]; ++r) {
+                const double v = cells->vxyz[3 * r + axis];
+                lo = std::min(lo, v);
+                hi = std::max(hi, v);
+            }
+            mid[(size_t)c] = (lo + hi) * 0.5;
         }
-        mid[(size_t)c] = (lo + hi) * 0.5;
+        std::vector<int64_t> order((size_t)nc);
+        for (int64_t c = 0; c < nc; ++c) order[(size_t)c] = c;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int64_t a, int64_t b) { return mid[(size_t)a] < mid[(size_t)b]; });
+        for (int64_t k = 0; k < nc; ++k) owner[(size_t)order[(size_t)k]] = (int32_t)((k * n_parts) / nc);
+        return KIWI_OK;
+    } catch (const std::bad_alloc&) {
+        return set_err(ctx, KIWI_ERR_ALLOC, "host memory allocation failed");
     }
-    std::vector<int64_t> order((size_t)nc);
-    for (int64_t c = 0; c < nc; ++c) order[(size_t)c] = c;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int64_t a, int64_t b) { return mid[(size_t)a] < mid[(size_t)b]; });
-    for (int64_t k = 0; k < nc; ++k) owner[(size_t)order[(size_t)k]] = (int32_t)((k * n_parts) / nc);
-    return KIWI_OK;
 }
 
 int kiwi_voronoi_part_particles(KiwiCtx* ctx, const KiwiParticles* particles, const int32_t* home_cell,
                                 const KiwiVoronoiCells* cells, const KiwiKernelSel* kernel, const int32_t* owner,
                                 int part, uint8_t* select, int64_t* n_selected) {
-    if (!particles || !n_selected || particles->n < 0 ||
-        (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h || !home_cell ||
-                              !select)))
-        return set_err(ctx, KIWI_ERR_ARG, "particles (host x, y, z, h), home_cell, select and n_selected are needed");
-    std::vector<int64_t> start, end;
-    KIWI_TRY(voronoi_host_rows(ctx, cells, &start, &end));
-    if (cells->n_cells > 0 && !owner) return set_err(ctx, KIWI_ERR_ARG, "owner is null");
-    KernelChoice kc;
-    KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
-    const int64_t nc = cells->n_cells;
-    double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    bool any = false;
-    for (int64_t c = 0; c < nc; ++c) {
-        if (owner[(size_t)c] != part) continue;
-        for (int64_t r = start[(size_t)c]; r < end[(size_t)c]; ++r)
-            for (int a = 0; a < 3; ++a) {
-                const double v = cells->vxyz[3 * r + a];
-                lo[a] = any ? std::min(lo[a], v) : v;
-                hi[a] = any ? std::max(hi[a], v) : v;
-                if (a == 2) any = true;
-            }
-    }
-    const double rscale = 1.001 * kc.support_in_h;
-    int64_t count = 0;
-    for (int64_t i = 0; i < particles->n; ++i) {
-        const int32_t hc = home_cell[i];
-        bool s = hc >= 0 && hc < nc && owner[hc] == part;
-        if (!s && any) {
-            const double c3[3] = {particles->x[i], particles->y[i], particles->z[i]};
-            double d2 = 0.0;
-            for (int a = 0; a < 3; ++a) {
-                const double t = std::max(std::max(lo[a] - c3[a], c3[a] - hi[a]), 0.0);
-                d2 += t * t;
-            }
-            const double r = rscale * particles->h[i];
-            s = d2 <= r * r;
+    try {
+        if (!particles || !n_selected || particles->n < 0 ||
+            (particles->n > 0 && (!particles->x || !particles->y || !particles->z || !particles->h || !home_cell ||
+                                  !select)))
+            return set_err(ctx, KIWI_ERR_ARG, "particles (host x, y, z, h), home_cell, select and n_selected are needed");
+        std::vector<int64_t> start, end;
+        KIWI_TRY(voronoi_host_rows(ctx, cells, &start, &end));
+        if (cells->n_cells > 0 && !owner) return set_err(ctx, KIWI_ERR_ARG, "owner is null");
+        KernelChoice kc;
+        KIWI_TRY(resolve_kernel(ctx, kernel, &kc));
+        const int64_t nc = cells->n_cells;
+        double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        bool any = false;
+        for (int64_t c = 0; c < nc; ++c) {
+            if (owner[(size_t)c] != part) continue;
+            for (int64_t r = start[(size_t)c]; r < end[(size_t)c]; ++r)
+                for (int a = 0; a < 3; ++a) {
+                    const double v = cells->vxyz[3 * r + a];
+                    lo[a] = any ? std::min(lo[a], v) : v;
+                    hi[a] = any ? std::max(hi[a], v) : v;
+                    if (a == 2) any = true;
+                }
         }
-        select[i] = s ? 1 : 0;
-        count += s;
+        const double rscale = 1.001 * kc.support_in_h;
+        int64_t count = 0;
+        for (int64_t i = 0; i < particles->n; ++i) {
+            const int32_t hc = home_cell[i];
+            bool s = hc >= 0 && hc < nc && owner[hc] == part;
+            if (!s && any) {
+                const double c3[3] = {particles->x[i], particles->y[i], particles->z[i]};
+                double d2 = 0.0;
+                for (int a = 0; a < 3; ++a) {
+                    const double t = std::max(std::max(lo[a] - c3[a], c3[a] - hi[a]), 0.0);
+                    d2 += t * t;
+                }
+                const double r = rscale * particles->h[i];
+                s = d2 <= r * r;
+            }
+            select[i] = s ? 1 : 0;
+            count += s;
+        }
+        *n_selected = count;
+        return KIWI_OK;
+    } catch (const std::bad_alloc&) {
+        return set_err(ctx, KIWI_ERR_ALLOC, "host memory allocation failed");
     }
-    *n_selected = count;
-    return KIWI_OK;
 }
 
 int kiwi_sph_to_grid_adjoint_device(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
