@@ -31,3 +31,26 @@ def test_reference_arm_json_line():
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
     assert "workload" in line["config"]
+
+
+def test_reference_arm_loads_nothing_of_the_engine():
+    """The reference arm runs the reference's own code only: after `bench.py --impl reference` the process
+    has not imported kiwi_b200 and has not mapped libkiwi_b200.so."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libkiwi_ref.so")):
+        pytest.skip("oracle/_ref is not built (it needs the reference checkout)")
+    code = (
+        "import runpy, sys\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '1', '--n', '20000', "
+        "'--res', '64']\n"
+        "try:\n"
+        "    runpy.run_path('bench.py', run_name='__main__')\n"
+        "except SystemExit:\n"
+        "    pass\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print('ENGINE_IMPORTED' if any(m.startswith('kiwi_b200') for m in sys.modules) else 'NO_ENGINE_IMPORT')\n"
+        "print('ENGINE_MAPPED' if 'libkiwi_b200' in maps else 'NO_ENGINE_MAPPED')\n"
+        "print('REF_MAPPED' if 'libkiwi_ref' in maps else 'NO_REF_MAPPED')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    tail = r.stdout.strip().splitlines()[-3:]
+    assert tail == ["NO_ENGINE_IMPORT", "NO_ENGINE_MAPPED", "REF_MAPPED"], tail
