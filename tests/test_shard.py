@@ -446,3 +446,28 @@ def test_c_abi_voronoi_slabs_match_the_host_rule(reflib):
                                                            C.byref(cnt)) == 0
                     want = shard.voronoi_part_particles(P, home, geo, own, p, sup)
                     assert np.array_equal(np.nonzero(s)[0], want) and cnt.value == len(want), (axis, n, p)
+
+
+def test_voronoi_split_edge_cases(oracle):
+    """More parts than cells (some parts own none and map no particle), a snapshot without particles, and
+    particles with h <= 0 or no home cell: the parts still reproduce the whole map."""
+    d, P, geo, k, sup = _vor_fixture(VOR_GOLDEN[0])
+    nc = len(geo["volume"])
+    own = shard.voronoi_cell_owners(geo, nc + 3)
+    assert np.bincount(own, minlength=nc + 3).max() == 1  # at most one cell per part
+    empty = [p for p in range(nc + 3) if not np.any(own == p)]
+    assert len(empty) == 3
+    for p in empty:
+        assert len(shard.voronoi_part_particles(P, d["home"], geo, own, p, sup)) == 0
+    P0 = {q: v[:0] for q, v in P.items()}
+    assert len(shard.voronoi_part_particles(P0, d["home"][:0], geo, shard.voronoi_cell_owners(geo, 2), 0, sup)) == 0
+    home = d["home"].copy()
+    home[:10] = -1
+    P2 = {q: v.copy() for q, v in P.items()}
+    P2["h"][10:20] = 0.0
+    whole = oracle.map_voronoi(P2, home, geo, kernel=k, support_in_h=sup)[4]
+    own = shard.voronoi_cell_owners(geo, 3, axis=2)
+    for p in range(3):
+        idx = shard.voronoi_part_particles(P2, home, geo, own, p, sup)
+        part = oracle.map_voronoi({q: v[idx] for q, v in P2.items()}, home[idx], geo, kernel=k, support_in_h=sup)[4]
+        assert np.array_equal(part[:, own == p], whole[:, own == p]), p
