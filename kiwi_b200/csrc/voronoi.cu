@@ -289,7 +289,6 @@ __global__ void __launch_bounds__(32 * kBfsWarpsPerBlock) k_vor_bfs(VorCells C, 
                 }
                 if (lane < batch) {
                     const int rank = head + lane;
-                    const int32_t cell = queue[rank];
                     const int64_t pf = fcarry + incl - nf;
                     pair_foff[o + rank] = pf;
                     for (int64_t f = fa; f < fa + nf; ++f) {
