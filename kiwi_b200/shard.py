@@ -24,9 +24,9 @@ def tile_grid(shape):
     return (nx + TILE - 1) // TILE, (ny + TILE - 1) // TILE, (nz + TILE - 1) // TILE
 
 
-def _support_tiles(particles: dict, bounds, shape, support_in_h: float):
+def _support_boxes(particles: dict, bounds, shape, support_in_h: float):
     """Per particle: whether its clamped support box (src/cartesian_grid.cpp:211-237) holds a cell, and
-    the tile range [t0, t1) of that box on each axis."""
+    the box's inclusive cell range [lo, hi] on each axis (as floats; meaningful where it holds a cell)."""
     nx, ny, nz = (int(s) for s in shape)
     x, y, z, h = (np.asarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "h"))
     b = [float(v) for v in bounds]
@@ -43,6 +43,13 @@ def _support_tiles(particles: dict, bounds, shape, support_in_h: float):
         ok &= a0 <= a1
         lo.append(a0)
         hi.append(a1)
+    return ok, lo, hi
+
+
+def _support_tiles(particles: dict, bounds, shape, support_in_h: float):
+    """Per particle: whether its clamped support box holds a cell, and the tile range [t0, t1) of that box
+    on each axis."""
+    ok, lo, hi = _support_boxes(particles, bounds, shape, support_in_h)
     t0 = [np.where(ok, lo[i], 0).astype(np.int64) // TILE for i in range(3)]
     t1 = [np.where(ok, hi[i], 0).astype(np.int64) // TILE + 1 for i in range(3)]
     return ok, t0, t1
@@ -194,20 +201,11 @@ def voronoi_part_particles(particles: dict, home_cell, cells: dict, owner: np.nd
 def snapshot_work(particles: dict, bounds, shape, support_in_h: float) -> int:
     """A snapshot's (particle, cell) pairs within the particles' clamped support boxes
     (src/cartesian_grid.cpp:211-237): the work estimate by which snapshots are dealt to GPUs."""
-    nx, ny, nz = (int(s) for s in shape)
-    x, y, z, h = (np.asarray(particles[k], dtype=np.float64) for k in ("x", "y", "z", "h"))
-    b = [float(v) for v in bounds]
-    d = [(b[1] - b[0]) / nx, (b[3] - b[2]) / ny, (b[5] - b[4]) / nz]
-    radius = support_in_h * h
-    ok = h > 0
-    cells = np.ones(len(h), dtype=np.int64)
-    for c, mn, dd, n in ((x, b[0], d[0], nx), (y, b[2], d[1], ny), (z, b[4], d[2], nz)):
-        with np.errstate(invalid="ignore", over="ignore"):
-            a0 = np.maximum(np.clip(np.floor((c - radius - mn) / dd), -2e9, 2e9), 0)
-            a1 = np.minimum(np.clip(np.floor((c + radius - mn) / dd), -2e9, 2e9), n - 1)
-        ok &= a0 <= a1
-        cells *= np.where(ok, a1 - a0 + 1, 0).astype(np.int64)
-    return int(cells[ok].sum())
+    ok, lo, hi = _support_boxes(particles, bounds, shape, support_in_h)
+    cells = np.ones(int(ok.sum()), dtype=np.int64)
+    for a in range(3):
+        cells *= (hi[a][ok] - lo[a][ok] + 1).astype(np.int64)
+    return int(cells.sum())
 
 
 def assign_snapshots_lpt(work, n_parts: int) -> list[np.ndarray]:
