@@ -223,17 +223,18 @@ int kiwi_sph_to_grid_device_part(KiwiCtx* ctx, const KiwiParticles* particles, c
                                  const KiwiKernelSel* kernel, int precision, int part, int n_parts, double* density,
                                  double* vx, double* vy, double* vz, double* raw4, KiwiStats* stats);
 
-/* Host only, no GPU work: the x rows [*ix0, *ix1) of cells that part `part` of kiwi_sph_to_grid_device_part
- * writes (its tiles' cells lie in these rows, contiguous in the output layout), from HOST arrays x, y, z,
- * h of the same particles: the same support boxes and ownership rule, so that each rank knows which rows
- * to copy back before it runs.  *ix0 = *ix1 = 0 if the part owns no tile.  ctx may be NULL (no message). */
+/* Host only, no GPU work (no counterpart in the reference): the x rows [*ix0, *ix1) of cells that part
+ * `part` of kiwi_sph_to_grid_device_part writes (its tiles' cells lie in these rows, contiguous in the
+ * output layout), from HOST arrays x, y, z, h of the same particles: the same support boxes and ownership
+ * rule, so that each rank knows which rows to copy back before it runs.  *ix0 = *ix1 = 0 if the part owns
+ * no tile.  ctx may be NULL (no message). */
 int kiwi_part_rows(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                    const KiwiKernelSel* kernel, int part, int n_parts, int* ix0, int* ix1);
 
-/* Host only, no GPU work: a snapshot's (particle, cell) pairs within the particles' clamped support boxes
- * (src/cartesian_grid.cpp:211-237; KiwiStats.bbox_pairs of the reference-order form), from HOST arrays x, y,
- * z, h -- the work estimate by which a batch of snapshots is dealt to GPUs, longest first.  ctx may be
- * NULL (no message). */
+/* Host only, no GPU work (no counterpart in the reference): a snapshot's (particle, cell) pairs within the
+ * particles' clamped support boxes (src/cartesian_grid.cpp:211-237; KiwiStats.bbox_pairs of the
+ * reference-order form), from HOST arrays x, y, z, h -- the work estimate by which a batch of snapshots is
+ * dealt to GPUs, longest first.  ctx may be NULL (no message). */
 int kiwi_snapshot_work(KiwiCtx* ctx, const KiwiParticles* particles, const KiwiCartGrid* grid,
                        const KiwiKernelSel* kernel, int64_t* bbox_pairs);
 
